@@ -1,0 +1,379 @@
+#!/usr/bin/env python3
+"""Benchmark: MD steps/s on the 65536-atom liquid-vapour LJ slab.
+
+Workload (one step = one Langevin NPT MD step of the whole slab through the
+graph-captured driver): 40 x 40 x 160 sigma box, liquid rho* 0.78 for
+|z - 80| < 24.84, vapour 0.02, adaptive per-slab LJ cutoff in [2.5, 5.0],
+skin 0.3, Langevin NPT with P_zz = 0 (x, y fixed), dt 0.005, T* 0.85.
+`value` is the mixed-precision path (FP32 pair math, FP64 accumulation);
+the plain FP64 path runs the same steps and is reported beside it together
+with the force RMS error of mixed against FP64 on the same configuration.
+
+python bench.py --gpus N --steps K --warmup W [--impl reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "md.error_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "MD steps/s at 64k-atom slab, force RMS err <=1e-4 vs FP64; mixed vs plain FP64"
+DT = 0.005
+TEMP = 0.85
+SKIN = 0.3
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def build_slab(mdf):
+    s = mdf.systems.lj_slab()
+    return s
+
+
+def rc_lattice(mdf, s):
+    """Adaptive rc lattice from the AdaptRCut estimate when available."""
+    est = getattr(mdf, "adapt_rcut_lattice", None)
+    if est is None:
+        return None, "uniform 2.5 (adaptive estimate not built)"
+    lat, info = est(s)
+    return lat, info
+
+
+def make_sim(mdf, s, prec, lattice, seed=1):
+    sys_ = mdf.MDSystem(s.pos, s.box, vel=s.vel, precision=prec)
+    if lattice is None:
+        sys_.set_rcut(np.full(s.n, 2.5, np.float32))
+    else:
+        mdf.AssignRCut(lattice).assign(sys_)
+    eng = mdf.InteractionEngine(sys_)
+    eng.registNonBondedInteraction(1.0, 1.0, 0.0)
+    lv = mdf.langevin_params(dt=DT, temperature=TEMP, gamma_t=1.0, tau_p=2.0, kappa_t=0.1,
+                             p_ref=(0.0, 0.0, 0.0), npt_dirs=4, seed=seed)
+    sim = mdf.Simulation(sys_, eng, skin=SKIN, cell_size=2.8, lv=lv, expansion=1.5, use_graph=True)
+    return sys_, eng, sim
+
+
+def time_steps(torch, sim, stream, steps, flush):
+    """Per-step CUDA-event timing; L2 is flushed between timed steps."""
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for a, b in ev:
+            flush.zero_()
+            a.record(stream)
+            sim.run(1)
+            b.record(stream)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in ev) / 1e3
+
+
+def time_lj_kernel(torch, mdf, sys_, eng, sim, stream, reps=50):
+    """Average duration of the dominant kernel (LJ forces) on the bench state."""
+    # the simulation owns its list; time the kernel on a list built the same way
+    cl = mdf.CellList(sys_, 2.8)
+    cl.rebuild()
+    rc = sys_.rcut()
+    nl = mdf.NeighborList(sys_, float(rc.max()) + SKIN, SKIN, expansion=1.5)
+    nl.fit(sys_, cl)
+    counts, _ = nl.lists()
+    P = int(counts.sum())
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        for _ in range(5):
+            eng.applyNonBondedInteraction(sys_, nl, with_stats=True)
+        a.record(stream)
+        for _ in range(reps):
+            eng.applyNonBondedInteraction(sys_, nl, with_stats=True)
+        b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / 1e3 / reps, P
+
+
+def force_error(mdf, s, lattice):
+    """RMS force error of mixed against FP64 on the same configuration."""
+    out = {}
+    for prec in (0, 1):
+        sys_ = mdf.MDSystem(s.pos, s.box, precision=prec)
+        if lattice is None:
+            sys_.set_rcut(np.full(s.n, 2.5, np.float32))
+        else:
+            mdf.AssignRCut(lattice).assign(sys_)
+        cl = mdf.CellList(sys_, 2.8)
+        cl.rebuild()
+        nl = mdf.NeighborList(sys_, float(sys_.rcut().max()) + SKIN, SKIN, expansion=1.5)
+        nl.fit(sys_, cl)
+        eng = mdf.InteractionEngine(sys_)
+        eng.registNonBondedInteraction(1.0, 1.0, 0.0)
+        eng.clearInteraction()
+        eng.applyNonBondedInteraction(sys_, nl, with_stats=True)
+        out[prec] = sys_.forces()
+    d = out[0] - out[1]
+    rms_abs = float(np.sqrt((d ** 2).sum(1).mean()))
+    rms_rel = float(np.sqrt((d ** 2).sum() / (out[1] ** 2).sum()))
+    return rms_abs, rms_rel
+
+
+def cpu_baseline(s, lattice, nsteps):
+    from oracle import oracle as orc
+    rc = None if lattice is not None else np.full(s.n, 2.5, np.float32)
+    kw = dict(dt=DT, temperature=TEMP, gamma_t=1.0, skin=SKIN, rcut=rc, lattice=lattice, tau_p=2.0,
+              kappa_t=0.1, p_ref=(0, 0, 0), npt_dirs=4, seed=1, cap=1024)
+    orc.md_langevin_run(s.pos, s.vel, s.box, 1, **kw)  # warm (page in, list build)
+    t = time.perf_counter()
+    out = orc.md_langevin_run(s.pos, s.vel, s.box, nsteps, **kw)
+    el = time.perf_counter() - t
+    # the run includes one initial list build + force evaluation; count it as a step
+    return (nsteps / el), orc.num_threads(), out
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    import mdforce as mdf
+    s = build_slab(mdf)
+    lattice, rcinfo = rc_lattice(mdf, s)
+    from oracle import oracle as orc
+    # bounded sample: estimate one step, cap the whole run at ~150 s
+    sps0, cores, _ = cpu_baseline(s, lattice, 3)
+    budget_steps = max(3, min(args.steps, int(150 * sps0)))
+    for _ in range(1):
+        pass
+    sps, cores, out = cpu_baseline(s, lattice, budget_steps)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": sps, "unit": "steps/s", "n_gpus": args.gpus,
+        "steps": budget_steps, "warmup": args.warmup, "ms_per_step": 1e3 / sps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "lj_slab_65536_npt", "n_atoms": s.n, "box": s.box.tolist(),
+                   "rc": rcinfo, "skin": SKIN, "dt": DT, "parallelism": "replicas"},
+        "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": cores, "kind": "port",
+                         "sample": f"{budget_steps} Langevin NPT steps of the full 65536-atom slab "
+                                   "(oracle CPU FP64 cell+Verlet list LJ, OpenMP)"},
+        "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank, world, local = dist_env()
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    import mdforce as mdf
+
+    s = build_slab(mdf)
+    lattice, rcinfo = rc_lattice(mdf, s)
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    # ---- mixed precision path (the headline value)
+    sys_m, eng_m, sim_m = make_sim(mdf, s, 0, lattice, seed=1 + rank)
+    sys_m.set_stream(stream.cuda_stream)
+    sim_m.run(args.warmup)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        t_mixed = time_steps(torch, sim_m, stream, args.steps, flush)
+    steps_done, rebuilds, flags = sim_m.counters()
+    t_max = t_mixed
+    if world > 1:
+        tt = torch.tensor([t_mixed], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_max = float(tt.item())
+        torch.distributed.barrier()
+    value = world * args.steps / t_max
+
+    # back-to-back (warm L2) throughput of the same loop, for reference
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        a.record(stream)
+        sim_m.run(args.steps)
+        b.record(stream)
+    torch.cuda.synchronize()
+    warm_sps = args.steps / (a.elapsed_time(b) / 1e3)
+
+    # ---- FP64 path, same steps
+    fp64_sps = None
+    if not args.no_fp64:
+        sys_d, eng_d, sim_d = make_sim(mdf, s, 1, lattice, seed=1 + rank)
+        sys_d.set_stream(stream.cuda_stream)
+        sim_d.run(args.warmup)
+        t64 = time_steps(torch, sim_d, stream, args.steps, flush)
+        fp64_sps = args.steps / t64
+        del sim_d, eng_d, sys_d
+
+    # ---- dominant kernel: LJ forces, algorithmic bytes / CUDA-event duration
+    t_lj, P = time_lj_kernel(torch, mdf, sys_m, eng_m, sim_m, stream)
+    N = s.n
+    alg_bytes = N * 16 + N * 4 + P * 4 + N * 24  # positions, rcut, list indices, FP64 forces
+    peak, peak_kind = measured_peak_hbm()
+    achieved = alg_bytes / t_lj / 1e9
+    rms_abs, rms_rel = force_error(mdf, s, lattice)
+
+    # ---- end to end through the C ABI with host buffers
+    e2e_steps = min(args.steps, 500)
+    pin_pos = torch.from_numpy(np.ascontiguousarray(s.pos)).pin_memory()
+    pin_vel = torch.from_numpy(np.ascontiguousarray(s.vel)).pin_memory()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sys_e, eng_e, sim_e = None, None, None
+    sys_e = mdf.MDSystem(pin_pos.numpy(), s.box, vel=pin_vel.numpy(), precision=0)
+    if lattice is None:
+        sys_e.set_rcut(np.full(N, 2.5, np.float32))
+    else:
+        mdf.AssignRCut(lattice).assign(sys_e)
+    eng_e = mdf.InteractionEngine(sys_e)
+    eng_e.registNonBondedInteraction(1.0, 1.0, 0.0)
+    lv = mdf.langevin_params(dt=DT, temperature=TEMP, gamma_t=1.0, tau_p=2.0, kappa_t=0.1,
+                             p_ref=(0.0, 0.0, 0.0), npt_dirs=4, seed=1)
+    sim_e = mdf.Simulation(sys_e, eng_e, skin=SKIN, cell_size=2.8, lv=lv, expansion=1.5)
+    t_setup = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sim_e.run(1)
+        sys_e.stats()  # D2H of the step's energy / virial / kinetic tensor
+    fin_pos = sys_e.positions()
+    fin_f = sys_e.forces()
+    t_e2e = time.perf_counter() - t1 + t_setup
+    e2e_sps = e2e_steps / t_e2e
+    h2d = (pin_pos.numel() + pin_vel.numel()) * 8 / e2e_steps
+    d2h = 16 * 8 + (fin_pos.size + fin_f.size) * 8 / e2e_steps
+
+    kernels_per_step = 12  # box, step1, bin, scan, scatter, order, gather, copyback, list, clear, lj, step2
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        n_cpu = 30
+        sps_cpu, cores, _ = cpu_baseline(s, lattice, n_cpu)
+        cpu = {"value": sps_cpu, "unit": "steps/s", "cores": cores, "kind": "port",
+               "sample": f"{n_cpu} Langevin NPT steps of the full 65536-atom slab "
+                         "(oracle CPU FP64 cell+Verlet list LJ, OpenMP)"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair math / f64 accumulation",
+            "data": "synthetic",
+            "config": {"workload": "lj_slab_65536_npt", "n_atoms": N, "box": s.box.tolist(),
+                       "rc": rcinfo, "skin": SKIN, "dt": DT, "T": TEMP, "ensemble": "Langevin NPT Pzz=0",
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "flushed (256 MB write) between timed steps"},
+            "fp64_steps_per_s": fp64_sps,
+            "speedup_vs_fp64": (value / world / fp64_sps) if fp64_sps else None,
+            "warm_l2_steps_per_s": warm_sps,
+            "force_rms_err_vs_fp64": {"abs": rms_abs, "rel": rms_rel},
+            "list_rebuilds": rebuilds, "tau_per_day": value / world * DT * 86400,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "k_lj_mixed",
+                         "kernel_us": t_lj * 1e6, "alg_bytes": alg_bytes, "peak_kind": peak_kind},
+            "e2e": {"value": e2e_sps, "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": kernels_per_step * args.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,142 @@
+// Device helpers: binary32 arithmetic without contraction (for the
+// bit-exact cell / neighbour criteria), deterministic last-block
+// reductions in FP64, and a counter-based normal generator.
+#pragma once
+#include "md_internal.cuh"
+
+// ---- binary32 / binary64 arithmetic with no FMA contraction ------------
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float floor_r(float a) { return floorf(a); }
+__device__ __forceinline__ double floor_r(double a) { return floor(a); }
+
+// Box accessors in the working precision: binary32 uses the float copies
+// (box.size / box.sizei of the reference), binary64 the double ones.
+template <class R> __device__ __forceinline__ R boxL(const DevState* s, int d);
+template <> __device__ __forceinline__ float boxL<float>(const DevState* s, int d) { return s->Lf[d]; }
+template <> __device__ __forceinline__ double boxL<double>(const DevState* s, int d) { return s->L[d]; }
+template <class R> __device__ __forceinline__ R boxLi(const DevState* s, int d);
+template <> __device__ __forceinline__ float boxLi<float>(const DevState* s, int d) { return s->Lif[d]; }
+template <> __device__ __forceinline__ double boxLi<double>(const DevState* s, int d) { return s->Li[d]; }
+
+// shortestImage (ENG/include/BoxGeometry.h:176-179): x -= floorf(x*Li + 0.5)*L
+template <class R>
+__device__ __forceinline__ R min_image_exact(R x, R L, R Li) {
+  R k = floor_r(add_rn(mul_rn(x, Li), R(0.5)));
+  return sub_rn(x, mul_rn(k, L));
+}
+
+// ---- deterministic reductions ------------------------------------------
+template <int NV>
+__device__ __forceinline__ void warp_sum(double (&v)[NV]) {
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  }
+}
+
+// Block-reduce v (all threads participate, blockDim.x multiple of 32, <= 1024),
+// thread 0 stores the block partial; the last block to finish sums the partials
+// in block order (fixed, hence bit-reproducible) and adds them into out[k]
+// (or stores when `store`).  `counter` is reset by the last block.
+template <int NV>
+__device__ bool block_reduce_finish(double (&v)[NV], double* partials, unsigned* counter,
+                                    double* out, bool store) {
+  __shared__ double sh[32][NV];
+  __shared__ bool am_last;
+  warp_sum<NV>(v);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) sh[wid][k] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+    for (int w = 0; w < nw; ++w)
+#pragma unroll
+      for (int k = 0; k < NV; ++k) acc[k] += sh[w][k];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) partials[(size_t)blockIdx.x * NV + k] = acc[k];
+    __threadfence();
+    unsigned prev = atomicAdd(counter, 1u);
+    am_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+  double acc[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] += __ldcg(&partials[(size_t)b * NV + k]);
+  warp_sum<NV>(acc);
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) sh[wid][k] = acc[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < NV; ++k) {
+      double s = 0.0;
+      for (int w = 0; w < nw; ++w) s += sh[w][k];
+      if (store) out[k] = s; else out[k] += s;
+    }
+    *counter = 0u;
+    __threadfence();
+    return true;
+  }
+  return false;
+}
+
+// ---- Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) -----------------
+struct u32x4 { uint32_t a, b, c, d; };
+__device__ __forceinline__ void philox_round(u32x4& x, uint32_t k0, uint32_t k1) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  uint32_t hi0 = __umulhi(M0, x.a), lo0 = M0 * x.a;
+  uint32_t hi1 = __umulhi(M1, x.c), lo1 = M1 * x.c;
+  u32x4 y;
+  y.a = hi1 ^ x.b ^ k0;
+  y.b = lo1;
+  y.c = hi0 ^ x.d ^ k1;
+  y.d = lo0;
+  x = y;
+}
+__device__ __forceinline__ u32x4 philox4x32_10(u32x4 ctr, uint32_t k0, uint32_t k1) {
+  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    philox_round(ctr, k0, k1);
+    k0 += W0;
+    k1 += W1;
+  }
+  return ctr;
+}
+// four standard normals (Box-Muller on the two 32-bit pairs), FP64 math so
+// that both precisions draw the same numbers
+__device__ __forceinline__ void normals4(uint64_t seed, uint64_t step, uint32_t id, double out[4]) {
+  u32x4 c{id, (uint32_t)step, (uint32_t)(step >> 32), 0x6d646672u};
+  u32x4 r = philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const double inv = 2.3283064365386963e-10;  // 2^-32
+  double u1 = ((double)r.a + 0.5) * inv, u2 = ((double)r.b + 0.5) * inv;
+  double u3 = ((double)r.c + 0.5) * inv, u4 = ((double)r.d + 0.5) * inv;
+  double m1 = sqrt(-2.0 * log(u1)), m2 = sqrt(-2.0 * log(u3));
+  double s1, c1, s2, c2;
+  sincospi(2.0 * u2, &s1, &c1);
+  sincospi(2.0 * u4, &s2, &c2);
+  out[0] = m1 * c1; out[1] = m1 * s1; out[2] = m2 * c2; out[3] = m2 * s2;
+}
+
+template <class R> __device__ __forceinline__ typename V4<R>::T load4(const void* p, int i) {
+  return reinterpret_cast<const typename V4<R>::T*>(p)[i];
+}

@@ -1,0 +1,277 @@
+// Integrators: velocity Verlet and Langevin NVT / NPT (BAOAB splitting).
+// Reference: velocityVerlet_part1/part2 (ENG/src/Integrator.cu:273-436);
+// Langevin equations of motion, langevin.npt/writedown/paper.tex:355-369
+// (isotropic), :382-440 (choice of M and gamma_P), :586-600 (anisotropic box).
+//
+// Box-length Langevin piston for the directions d in npt_dirs (x and y fixed
+// for the slab, z free with target P_zz):
+//   dL_d/dt = p_d / M_d
+//   dp_d/dt = A_d (P_dd - P_ref) - gamma_P p_d + sqrt(2 kT gamma_P M_d) W'
+// with A_d = V / L_d (det h h^-T in paper.tex:586-600), and for the particles
+//   dr_d/dt = p_d/m + (dL_d/dt / L_d) r_d,  dp_d/dt = F_d - (dL_d/dt / L_d) p_d - gamma_T p_d + noise.
+// For fixed box velocity over a sub-step h the drift is solved exactly:
+//   L' = L + h v_L, lambda = L'/L, r_d' = lambda r_d + h p_d/m, p_d' = p_d/lambda.
+// One step: B(dt/2) A(dt/2) O(dt) A(dt/2) | forces | B(dt/2).  The box part of
+// B/A/O runs in a one-thread kernel before the particle update; the closing
+// box half kick runs in the last block of the closing particle kick, with
+// the pressure computed there from the FP64 kinetic and virial sums.
+#include <cmath>
+#include <cstring>
+#include "device_common.cuh"
+
+struct LvDev {
+  double dt, kT, c1, c2, c1p, c2p, pref[3], skin_half2;
+  int dirs;
+  uint64_t seed;
+};
+
+// box B/A/O/A for one step, plus reset of the rebuild flag
+__global__ void k_lv_box(DevState* st, LvDev p) {
+  if (st->flags & FLAG_REBUILD) st->rebuilds += 1ull;
+  st->flags &= ~FLAG_REBUILD;
+  st->step += 1ull;
+  double xi[4];
+  normals4(p.seed ^ 0x5bd1e995ull, st->step, 0xffffffffu, xi);
+  for (int d = 0; d < 3; ++d) { st->lam1[d] = 1.0; st->lam2[d] = 1.0; }
+  if (!p.dirs) return;
+  const double V = st->L[0] * st->L[1] * st->L[2];
+  for (int d = 0; d < 3; ++d) {
+    if (!(p.dirs & (1 << d))) continue;
+    const double A = V / st->L[d];
+    double ph = st->ph[d];
+    const double M = st->Mh[d];
+    ph += 0.5 * p.dt * A * (st->Pcur[d] - p.pref[d]);            // B
+    const double L0 = st->L[d];
+    const double L1 = L0 + 0.5 * p.dt * ph / M;                  // A
+    ph = p.c1p * ph + p.c2p * sqrt(M * p.kT) * xi[d];            // O
+    const double L2 = L1 + 0.5 * p.dt * ph / M;                  // A
+    st->lam1[d] = L1 / L0;
+    st->lam2[d] = L2 / L1;
+    st->ph[d] = ph;
+    st->L[d] = L2;
+    st->Li[d] = 1.0 / L2;
+    st->Lf[d] = (float)L2;
+    st->Lif[d] = 1.0f / st->Lf[d];
+  }
+}
+
+template <class R>
+__global__ void __launch_bounds__(256)
+k_lv_step1(int N, typename V4<R>::T* __restrict__ pos, typename V4<R>::T* __restrict__ vel,
+           const double4a* __restrict__ force, const int* __restrict__ id,
+           const typename V4<R>::T* __restrict__ backup, DevState* st, LvDev p) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  typename V4<R>::T x = pos[k], v = vel[k];
+  const double4a f = force[k];
+  const double im = (double)v.w;
+  const double h = 0.5 * p.dt;
+  double vx = v.x + h * f.x * im, vy = v.y + h * f.y * im, vz = v.z + h * f.z * im;  // B
+  double rx = x.x, ry = x.y, rz = x.z;
+  const double l1[3] = {st->lam1[0], st->lam1[1], st->lam1[2]};
+  const double l2[3] = {st->lam2[0], st->lam2[1], st->lam2[2]};
+  // A
+  rx = l1[0] * rx + h * vx; vx /= l1[0];
+  ry = l1[1] * ry + h * vy; vy /= l1[1];
+  rz = l1[2] * rz + h * vz; vz /= l1[2];
+  // O
+  double xi[4];
+  normals4(p.seed, st->step, (uint32_t)id[k], xi);
+  const double sd = p.c2 * sqrt(p.kT * im);
+  vx = p.c1 * vx + sd * xi[0];
+  vy = p.c1 * vy + sd * xi[1];
+  vz = p.c1 * vz + sd * xi[2];
+  // A
+  rx = l2[0] * rx + h * vx; vx /= l2[0];
+  ry = l2[1] * ry + h * vy; vy /= l2[1];
+  rz = l2[2] * rz + h * vz; vz /= l2[2];
+  x.x = (R)rx; x.y = (R)ry; x.z = (R)rz;
+  v.x = (R)vx; v.y = (R)vy; v.z = (R)vz;
+  pos[k] = x;
+  vel[k] = v;
+  // Displacement_max: rebuild when |r - r_backup| > skin/2
+  if (backup) {
+    const typename V4<R>::T b = backup[k];
+    const double dx = min_image_exact((double)x.x - (double)b.x, st->L[0], st->Li[0]);
+    const double dy = min_image_exact((double)x.y - (double)b.y, st->L[1], st->Li[1]);
+    const double dz = min_image_exact((double)x.z - (double)b.z, st->L[2], st->Li[2]);
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    const bool far = d2 > p.skin_half2;
+    const unsigned m = __ballot_sync(__activemask(), far);
+    if (m && (int)(threadIdx.x & 31) == __ffs(m) - 1) atomicOr(&st->flags, FLAG_REBUILD);
+  }
+}
+
+template <class R>
+__global__ void __launch_bounds__(256)
+k_lv_step2(int N, typename V4<R>::T* __restrict__ vel, const double4a* __restrict__ force,
+           DevState* st, LvDev p, double* partials, int with_box) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  double kin[3] = {0, 0, 0};
+  if (k < N) {
+    typename V4<R>::T v = vel[k];
+    const double4a f = force[k];
+    const double im = (double)v.w;
+    const double h = 0.5 * p.dt;
+    double vx = v.x + h * f.x * im, vy = v.y + h * f.y * im, vz = v.z + h * f.z * im;
+    v.x = (R)vx; v.y = (R)vy; v.z = (R)vz;
+    vel[k] = v;
+    const double m = 1.0 / im;
+    kin[0] = 0.5 * m * (double)v.x * (double)v.x;
+    kin[1] = 0.5 * m * (double)v.y * (double)v.y;
+    kin[2] = 0.5 * m * (double)v.z * (double)v.z;
+  }
+  const bool last = block_reduce_finish<3>(kin, partials, &st->red_counter[RED_KIN],
+                                           &st->stats[MD_STAT_KINETIC_XX], true);
+  if (last && with_box) {
+    // P_dd = 2/V (K_dd - W_dd/2) + tail correction (MDStatistic::pressureXX)
+    const double V = st->L[0] * st->L[1] * st->L[2];
+    for (int d = 0; d < 3; ++d) {
+      const double W = st->stats[MD_STAT_VIRIAL_XX + d];
+      const double K = st->stats[MD_STAT_KINETIC_XX + d];
+      st->Pcur[d] = 2.0 / V * (K - 0.5 * W) + st->stats[MD_STAT_PRESSURE_CORR_XX + d];
+      if (p.dirs & (1 << d)) st->ph[d] += 0.5 * p.dt * V / st->L[d] * (st->Pcur[d] - p.pref[d]);
+    }
+  }
+}
+
+static LvDev make_lv(const md_system* sys, const md_nlist* nl) {
+  const md_langevin_params& q = sys->lv;
+  LvDev p;
+  p.dt = q.dt;
+  p.kT = q.temperature;
+  p.c1 = exp(-q.gamma_t * q.dt);
+  p.c2 = sqrt(1.0 - p.c1 * p.c1);
+  double gp = q.tau_p > 0 ? 1.0 / q.tau_p : 0.0;  // gamma_P = 1/tau_P (paper.tex:430)
+  p.c1p = exp(-gp * q.dt);
+  p.c2p = sqrt(1.0 - p.c1p * p.c1p);
+  for (int d = 0; d < 3; ++d) p.pref[d] = q.p_ref[d];
+  p.dirs = q.npt_dirs;
+  p.seed = q.seed;
+  double s = nl ? 0.5 * nl->skin : 1e300;
+  p.skin_half2 = s * s;
+  return p;
+}
+
+int langevin_step1_impl(md_system* sys, md_nlist* nl, Recorder* rec) {
+  LvDev p = make_lv(sys, nl);
+  DevState* st = sys->st;
+  {
+    void* a[] = {&st, &p};
+    if (int r = rec_launch(rec, (const void*)k_lv_box, dim3(1), dim3(1), 0, a)) return r;
+  }
+  int N = sys->N;
+  void* bk = nl ? nl->backup : nullptr;
+  void* a[] = {&N, &sys->pos, &sys->vel, &sys->force, &sys->id, &bk, &st, &p};
+  const void* f = sys->prec == MD_PREC_FP64 ? (const void*)k_lv_step1<double> : (const void*)k_lv_step1<float>;
+  return rec_launch(rec, f, dim3(ceil_div(N, 256)), dim3(256), 0, a);
+}
+
+int langevin_step2_impl(md_system* sys, Recorder* rec) {
+  LvDev p = make_lv(sys, nullptr);
+  DevState* st = sys->st;
+  int N = sys->N;
+  int with_box = 1;
+  void* a[] = {&N, &sys->vel, &sys->force, &st, &p, &sys->partials, &with_box};
+  const void* f = sys->prec == MD_PREC_FP64 ? (const void*)k_lv_step2<double> : (const void*)k_lv_step2<float>;
+  return rec_launch(rec, f, dim3(ceil_div(N, 256)), dim3(256), 0, a);
+}
+
+// ------------------------------------------------------------ velocity Verlet
+template <class R>
+__global__ void k_vv1(int N, typename V4<R>::T* pos, typename V4<R>::T* vel, const double4a* force, double dt) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  typename V4<R>::T x = pos[k], v = vel[k];
+  const double4a f = force[k];
+  const double hi = 0.5 * dt * (double)v.w;
+  v.x = (R)(v.x + hi * f.x); v.y = (R)(v.y + hi * f.y); v.z = (R)(v.z + hi * f.z);
+  x.x = (R)(x.x + dt * v.x); x.y = (R)(x.y + dt * v.y); x.z = (R)(x.z + dt * v.z);
+  pos[k] = x;
+  vel[k] = v;
+}
+
+extern "C" int md_vv_step1(md_system* sys, double dt) {
+  if (!sys || !(dt > 0)) return MD_ERR_BADARG;
+  int nb = ceil_div(sys->N, 256);
+  if (sys->prec == MD_PREC_FP64)
+    k_vv1<double><<<nb, 256, 0, sys->stream>>>(sys->N, (double4a*)sys->pos, (double4a*)sys->vel, sys->force, dt);
+  else
+    k_vv1<float><<<nb, 256, 0, sys->stream>>>(sys->N, (float4*)sys->pos, (float4*)sys->vel, sys->force, dt);
+  MD_CHECK_LAUNCH("vv step1");
+  return MD_OK;
+}
+
+extern "C" int md_vv_step2(md_system* sys, double dt, int with_stats) {
+  if (!sys || !(dt > 0)) return MD_ERR_BADARG;
+  LvDev p;
+  memset(&p, 0, sizeof(p));
+  p.dt = dt;
+  int N = sys->N;
+  DevState* st = sys->st;
+  int nb = ceil_div(N, 256);
+  (void)with_stats;
+  if (sys->prec == MD_PREC_FP64)
+    k_lv_step2<double><<<nb, 256, 0, sys->stream>>>(N, (double4a*)sys->vel, sys->force, st, p, sys->partials, 0);
+  else
+    k_lv_step2<float><<<nb, 256, 0, sys->stream>>>(N, (float4*)sys->vel, sys->force, st, p, sys->partials, 0);
+  MD_CHECK_LAUNCH("vv step2");
+  return MD_OK;
+}
+
+// ------------------------------------------------------------ Langevin ABI
+__global__ void k_lv_init(DevState* st, double M0, double M1, double M2) {
+  st->Mh[0] = M0; st->Mh[1] = M1; st->Mh[2] = M2;
+  for (int d = 0; d < 3; ++d) { st->ph[d] = 0.0; st->Pcur[d] = 0.0; st->lam1[d] = st->lam2[d] = 1.0; }
+}
+
+extern "C" int md_langevin_setup(md_system* sys, const md_langevin_params* p) {
+  if (!sys || !p || !(p->dt > 0) || !(p->temperature >= 0) || !(p->gamma_t >= 0)) {
+    md_set_error("md_langevin_setup: bad arguments");
+    return MD_ERR_BADARG;
+  }
+  if (p->npt_dirs && (!(p->tau_p > 0) || !(p->kappa_t > 0))) {
+    md_set_error("md_langevin_setup: NPT needs tau_p > 0 and kappa_t > 0");
+    return MD_ERR_BADARG;
+  }
+  sys->lv = *p;
+  sys->lv_set = true;
+  DevState hs;
+  if (int r = sys->read_state(hs)) return r;
+  // M_V = (tau_P / 2pi)^2 / (kappa_T V0) (paper.tex:422-428), carried to a box
+  // length: the restoring force on p_d is A_d dP, dP = -dV/(kappa V), dV = A_d dL
+  double V = hs.L[0] * hs.L[1] * hs.L[2];
+  double M[3];
+  for (int d = 0; d < 3; ++d) {
+    double A = V / hs.L[d];
+    double w = 2.0 * M_PI / (p->tau_p > 0 ? p->tau_p : 1.0);
+    M[d] = A * A / (p->kappa_t > 0 ? p->kappa_t * V : 1.0) / (w * w);
+  }
+  k_lv_init<<<1, 1, 0, sys->stream>>>(sys->st, M[0], M[1], M[2]);
+  MD_CHECK_LAUNCH("lv init");
+  MD_CUDA(cudaStreamSynchronize(sys->stream));
+  return MD_OK;
+}
+
+extern "C" int md_langevin_step1(md_system* sys, md_nlist* nl) {
+  if (!sys || !sys->lv_set) { md_set_error("md_langevin_step1: call md_langevin_setup first"); return MD_ERR_BADARG; }
+  Recorder rec;
+  rec.stream = sys->stream;
+  return langevin_step1_impl(sys, nl, &rec);
+}
+
+extern "C" int md_langevin_step2(md_system* sys) {
+  if (!sys || !sys->lv_set) { md_set_error("md_langevin_step2: call md_langevin_setup first"); return MD_ERR_BADARG; }
+  Recorder rec;
+  rec.stream = sys->stream;
+  return langevin_step2_impl(sys, &rec);
+}
+
+extern "C" int md_langevin_get_state(md_system* sys, double* step, double p_h[3]) {
+  if (!sys) return MD_ERR_BADARG;
+  DevState hs;
+  if (int r = sys->read_state(hs)) return r;
+  if (step) *step = (double)hs.step;
+  if (p_h) for (int d = 0; d < 3; ++d) p_h[d] = hs.ph[d];
+  return MD_OK;
+}

@@ -1,0 +1,241 @@
+// Adaptive-cutoff Lennard-Jones non-bonded forces.
+// Reference: calNonBondedInteraction_neighbor, statistics variant
+// (ENG/src/InteractionEngine_interface.cu:1204-1281), LennardJones6_12::forcePoten
+// (ENG/include/NonBondedInteraction.h:867-893), InteractionEngine::
+// applyNonBondedInteraction (ENG/src/InteractionEngine_interface.cu:317-380).
+//
+// G lanes share one atom i and stride through its list row; the pair test is
+// the reference's binary32 |d|^2 < rcut_i^2 on the minimum-image vector
+// (same rounding as the list criterion), so the interacting pair set is
+// exactly the reference's.  Mixed precision: pair forces in FP32, each lane
+// keeps Kahan-compensated FP32 partial sums, lanes are combined in FP64 by
+// shuffles, the atom force is accumulated in FP64.  Energy and the diagonal
+// virial (1/2 sum over the full list, as the reference's per-atom buffers)
+// are block-reduced in FP64 and finished by the last block in a fixed order.
+#include <cmath>
+#include "device_common.cuh"
+
+struct LJParams {
+  float eps4f, sig2f, shiftf;
+  double eps4, sig2, shift;
+};
+
+struct Kahan {
+  float s = 0.f, c = 0.f;
+  __device__ __forceinline__ void add(float x) {
+    float y = x - c;
+    float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+  __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, G);
+  return v;
+}
+
+// ---------------------------------------------------------------- mixed
+template <int G, bool STATS>
+__global__ void __launch_bounds__(256)
+k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut,
+           const int* __restrict__ list, const int* __restrict__ nnb, int cap,
+           const DevState* __restrict__ st, LJParams p, double4a* __restrict__ force, int overwrite,
+           double* partials, unsigned* counter, double* stats) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / G;
+  const int lane = t & (G - 1);
+  const float L0 = st->Lf[0], L1 = st->Lf[1], L2 = st->Lf[2];
+  const float I0 = st->Lif[0], I1 = st->Lif[1], I2 = st->Lif[2];
+  Kahan fx, fy, fz;
+  float e = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+  if (i < N) {
+    const float4 pi = pos[i];
+    const float rc = rcut[i];
+    const float rc2 = __fmul_rn(rc, rc);
+    int n = nnb[i];
+    n = n < cap ? n : cap;
+    const int* row = list + (size_t)i * cap;
+    for (int k = lane; k < n; k += G) {
+      const int j = __ldg(row + k);
+      const float4 pj = __ldg(pos + j);
+      const float dx = min_image_exact(__fsub_rn(pj.x, pi.x), L0, I0);
+      const float dy = min_image_exact(__fsub_rn(pj.y, pi.y), L1, I1);
+      const float dz = min_image_exact(__fsub_rn(pj.z, pi.z), L2, I2);
+      const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+      if (r2 < rc2) {
+        const float ri2 = __fdividef(1.0f, r2);
+        const float s2 = p.sig2f * ri2;
+        const float s6 = s2 * s2 * s2;
+        const float fs = p.eps4f * (6.f * s6 - 12.f * s6 * s6) * ri2;
+        fx.add(fs * dx);
+        fy.add(fs * dy);
+        fz.add(fs * dz);
+        if (STATS) {
+          e += p.eps4f * (s6 * s6 - s6) + p.shiftf;
+          vx += fs * dx * dx;
+          vy += fs * dy * dy;
+          vz += fs * dz * dz;
+        }
+      }
+    }
+  }
+  double Fx = group_sum<G>(fx.value()), Fy = group_sum<G>(fy.value()), Fz = group_sum<G>(fz.value());
+  if (i < N && lane == 0) {
+    double4a f = overwrite ? double4a{0, 0, 0, 0} : force[i];
+    f.x += Fx; f.y += Fy; f.z += Fz;
+    force[i] = f;
+  }
+  if (STATS) {
+    double v[4] = {0.5 * (double)e, 0.5 * (double)vx, 0.5 * (double)vy, 0.5 * (double)vz};
+    block_reduce_finish<4>(v, partials, counter, stats, false);
+  }
+}
+
+// ---------------------------------------------------------------- FP64
+template <int G, bool STATS>
+__global__ void __launch_bounds__(256)
+k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcut,
+          const int* __restrict__ list, const int* __restrict__ nnb, int cap,
+          const DevState* __restrict__ st, LJParams p, double4a* __restrict__ force, int overwrite,
+          double* partials, unsigned* counter, double* stats) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / G;
+  const int lane = t & (G - 1);
+  const double L0 = st->L[0], L1 = st->L[1], L2 = st->L[2];
+  const double I0 = st->Li[0], I1 = st->Li[1], I2 = st->Li[2];
+  double fx = 0, fy = 0, fz = 0, e = 0, vx = 0, vy = 0, vz = 0;
+  if (i < N) {
+    const double4a pi = pos[i];
+    const double rc = (double)rcut[i];
+    const double rc2 = rc * rc;
+    int n = nnb[i];
+    n = n < cap ? n : cap;
+    const int* row = list + (size_t)i * cap;
+    for (int k = lane; k < n; k += G) {
+      const int j = __ldg(row + k);
+      const double4a pj = pos[j];
+      const double dx = min_image_exact(pj.x - pi.x, L0, I0);
+      const double dy = min_image_exact(pj.y - pi.y, L1, I1);
+      const double dz = min_image_exact(pj.z - pi.z, L2, I2);
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 < rc2) {
+        const double ri2 = 1.0 / r2;
+        const double s2 = p.sig2 * ri2;
+        const double s6 = s2 * s2 * s2;
+        const double fs = p.eps4 * (6.0 * s6 - 12.0 * s6 * s6) * ri2;
+        fx += fs * dx;
+        fy += fs * dy;
+        fz += fs * dz;
+        if (STATS) {
+          e += p.eps4 * (s6 * s6 - s6) + p.shift;
+          vx += fs * dx * dx;
+          vy += fs * dy * dy;
+          vz += fs * dz * dz;
+        }
+      }
+    }
+  }
+  double Fx = group_sum<G>(fx), Fy = group_sum<G>(fy), Fz = group_sum<G>(fz);
+  if (i < N && lane == 0) {
+    double4a f = overwrite ? double4a{0, 0, 0, 0} : force[i];
+    f.x += Fx; f.y += Fy; f.z += Fz;
+    force[i] = f;
+  }
+  if (STATS) {
+    double v[4] = {0.5 * e, 0.5 * vx, 0.5 * vy, 0.5 * vz};
+    block_reduce_finish<4>(v, partials, counter, stats, false);
+  }
+}
+
+__global__ void k_clear_force(int N, double4a* f) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < N) f[k] = double4a{0, 0, 0, 0};
+}
+
+static const int kLanes = 8;
+
+int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats, bool overwrite,
+                  Recorder* rec) {
+  if (!eng->has_lj) { md_set_error("no non-bonded interaction registered"); return MD_ERR_BADARG; }
+  LJParams p;
+  p.eps4 = 4.0 * eng->eps;
+  p.sig2 = eng->sigma * eng->sigma;
+  p.shift = eng->shift;
+  p.eps4f = (float)p.eps4;
+  p.sig2f = (float)p.sig2;
+  p.shiftf = (float)p.shift;
+  int N = sys->N;
+  int cap = nl->cap;
+  int ow = overwrite ? 1 : 0;
+  const int threads = 256;
+  dim3 grid(ceil_div((long long)N * kLanes, threads));
+  if ((int)grid.x > sys->max_partial_blocks) { md_set_error("partials buffer too small"); return MD_ERR_BADARG; }
+  DevState* st = sys->st;
+  unsigned* counter = &st->red_counter[RED_LJ];
+  double* stats = &st->stats[MD_STAT_NB_ENERGY];
+  void* a[] = {&N, &sys->pos, &sys->rcut, &nl->list, &nl->nnb, &cap, &st, &p, &sys->force, &ow,
+               &sys->partials, &counter, &stats};
+  const void* f;
+  if (sys->prec == MD_PREC_FP64)
+    f = with_stats ? (const void*)k_lj_fp64<kLanes, true> : (const void*)k_lj_fp64<kLanes, false>;
+  else
+    f = with_stats ? (const void*)k_lj_mixed<kLanes, true> : (const void*)k_lj_mixed<kLanes, false>;
+  return rec_launch(rec, f, grid, dim3(threads), 0, a);
+}
+
+// ------------------------------------------------------------------ C ABI
+extern "C" int md_engine_create(md_engine** out, md_system* sys) {
+  if (!out || !sys) { md_set_error("md_engine_create: bad arguments"); return MD_ERR_BADARG; }
+  md_engine* e = new md_engine();
+  e->sys = sys;
+  *out = e;
+  return MD_OK;
+}
+
+extern "C" int md_engine_destroy(md_engine* e) {
+  delete e;
+  return MD_OK;
+}
+
+extern "C" int md_engine_register_lj(md_engine* e, double eps, double sigma, double shift) {
+  if (!e || !(eps >= 0) || !(sigma > 0) || !std::isfinite(shift)) { md_set_error("md_engine_register_lj: bad arguments"); return MD_ERR_BADARG; }
+  e->has_lj = true;
+  e->eps = eps;
+  e->sigma = sigma;
+  e->shift = shift;
+  return MD_OK;
+}
+
+extern "C" int md_engine_register_bonded(md_engine* e, int n_bonds) {
+  if (!e || n_bonds < 0) return MD_ERR_BADARG;
+  if (n_bonds > 0) {
+    md_set_error("bonded interactions are not part of this force path (%d bonds given)", n_bonds);
+    return MD_ERR_UNSUPPORTED;
+  }
+  e->n_bonds = 0;
+  return MD_OK;
+}
+
+extern "C" int md_engine_apply_bonded(md_engine* e, md_system* sys) {
+  if (!e || !sys) return MD_ERR_BADARG;
+  return MD_OK;  // no bonded terms registered: nothing to add
+}
+
+extern "C" int md_engine_clear_forces(md_engine* e, md_system* sys) {
+  if (!e || !sys) return MD_ERR_BADARG;
+  k_clear_force<<<ceil_div(sys->N, 256), 256, 0, sys->stream>>>(sys->N, sys->force);
+  MD_CHECK_LAUNCH("clear force");
+  return MD_OK;
+}
+
+extern "C" int md_engine_apply_nonbonded(md_engine* e, md_system* sys, md_nlist* nl, int with_stats) {
+  if (!e || !sys || !nl) return MD_ERR_BADARG;
+  if (!nl->built) { md_set_error("neighbour list not built"); return MD_ERR_BADARG; }
+  Recorder rec;
+  rec.stream = sys->stream;
+  return lj_apply_impl(e, sys, nl, with_stats != 0, false, &rec);
+}

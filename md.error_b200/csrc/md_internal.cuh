@@ -1,0 +1,164 @@
+// Internal declarations shared by the translation units of libmdforce.
+// Device data layout (all per-atom arrays in CELL ORDER, slot k):
+//   pos[k]   Real4  x,y,z wrapped into the box at the last rebuild, w = charge
+//   vel[k]   Real4  vx,vy,vz, w = 1/m
+//   force[k] double4 accumulated force (FP64 in both precisions)
+//   image[k] int4   periodic image counters (coordNoi{x,y,z})
+//   id[k]    int    original atom index
+//   rcut[k]  float  per-atom cutoff (AssignRCut lattice value)
+// The box, the statistic slots, the rebuild/overflow flags and the barostat
+// state live in one device-resident DevState so that a captured step never
+// needs a host round trip.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+#include "../../include/mdforce.h"
+
+struct alignas(32) double4a {
+  double x, y, z, w;
+};
+
+template <class R> struct V4;
+template <> struct V4<float> { typedef float4 T; };
+template <> struct V4<double> { typedef double4a T; };
+
+// device flag bits
+enum : unsigned {
+  FLAG_REBUILD = 1u,        // displacement exceeded skin/2 (or forced)
+  FLAG_NL_OVERFLOW = 2u,    // mdErrorShortNeighborList
+  FLAG_CELL_INDEX = 4u,     // mdErrorOverFlowCellIdx
+  FLAG_NAN = 8u,            // non-finite coordinate met
+  FLAG_TIMEOUT = 16u
+};
+
+// reduction counters (one per kind of last-block reduction)
+enum { RED_LJ = 0, RED_KIN = 1, RED_DISP = 2, RED_SPME = 3, RED_MISC = 4, RED_COUNT = 8 };
+
+struct DevState {
+  double L[3];       // box edge, FP64 master copy
+  double Li[3];      // 1/L
+  float Lf[3];       // binary32 box.size (BoxGeometry.h setBoxSize)
+  float Lif[3];      // binary32 box.sizei = 1/x computed in float
+  double stats[MD_STAT_COUNT];
+  unsigned flags;
+  unsigned red_counter[RED_COUNT];
+  int max_nnb;       // largest list length seen at the last build
+  int pad0;
+  unsigned long long step;     // Langevin step counter (RNG counter)
+  unsigned long long rebuilds; // number of list builds
+  double max_disp2;            // last max squared displacement
+  // barostat (anisotropic Langevin piston on the box lengths)
+  double ph[3];      // box momentum p_h
+  double Mh[3];      // box mass
+  double lam1[3], lam2[3]; // scale factors of the two A half steps of this step
+  double Pcur[3];    // diagonal pressure at the end of the last step
+};
+
+// host helpers -------------------------------------------------------------
+void md_set_error(const char* fmt, ...);
+int md_cuda_fail(cudaError_t e, const char* what);
+#define MD_CUDA(call)                                   \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return md_cuda_fail(_e, #call); \
+  } while (0)
+#define MD_CHECK_LAUNCH(what)                           \
+  do {                                                  \
+    cudaError_t _e = cudaGetLastError();                \
+    if (_e != cudaSuccess) return md_cuda_fail(_e, what); \
+  } while (0)
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// box update on the host side copy
+void box_fill(DevState& s, const double L[3]);
+
+struct md_system {
+  int N = 0;
+  int prec = MD_PREC_MIXED;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  void* pos = nullptr;      // Real4
+  void* vel = nullptr;      // Real4
+  double4a* force = nullptr;
+  int4* image = nullptr;
+  int* id = nullptr;
+  float* rcut = nullptr;
+  // gather targets used by the cell sort
+  void* t_pos = nullptr;
+  void* t_vel = nullptr;
+  double4a* t_force = nullptr;
+  int4* t_image = nullptr;
+  int* t_id = nullptr;
+  float* t_rcut = nullptr;
+  DevState* st = nullptr;   // device state
+  double* partials = nullptr;  // block partial sums for reductions
+  int max_partial_blocks = 0;
+  // pinned host staging
+  void* h_stage = nullptr;
+  size_t h_stage_bytes = 0;
+  // rc lattice (AssignRCut)
+  float* d_lattice = nullptr;
+  int lat_n[3] = {0, 0, 0};
+  // Langevin parameters (md_langevin_setup)
+  md_langevin_params lv;
+  bool lv_set = false;
+  size_t real_size() const { return prec == MD_PREC_FP64 ? sizeof(double) : sizeof(float); }
+  size_t r4_size() const { return prec == MD_PREC_FP64 ? sizeof(double4a) : sizeof(float4); }
+  int read_state(DevState& s);
+};
+
+struct md_cell_list {
+  int ncell[3] = {1, 1, 1};
+  int ntot = 1;
+  double cell_size = 0;
+  int bdir = 7, divide = 1;
+  uint32_t* cell_of = nullptr;     // cell of slot k (after sort: sorted order)
+  uint32_t* t_cell = nullptr;      // cell of slot k before the sort
+  uint32_t* slot = nullptr;        // rank inside the cell from the atomic count
+  uint32_t* count = nullptr;       // atoms per cell
+  uint32_t* start = nullptr;       // exclusive scan, ntot+1
+  uint32_t* members = nullptr;     // cell member lists (current index)
+  uint32_t* perm = nullptr;        // perm[new] = old
+  bool built = false;
+};
+
+struct md_nlist {
+  double rlist = 0, skin = 0, expansion = 1;
+  int mode = MD_NL_MINIMAGE;
+  int cap = 0;
+  int N = 0;
+  int* list = nullptr;    // [N][cap] row-major (slot indices)
+  int* nnb = nullptr;     // [N]
+  void* backup = nullptr; // Real4 positions at the last build
+  bool built = false;
+};
+
+struct md_engine {
+  md_system* sys = nullptr;
+  bool has_lj = false;
+  double eps = 1, sigma = 1, shift = 0;
+  int n_bonds = 0;
+};
+
+// launch helper: direct launch or kernel-node recording ---------------------
+struct Recorder {
+  cudaGraph_t graph = nullptr;   // when non-null, launches become kernel nodes
+  cudaGraphNode_t last = nullptr;
+  bool has_last = false;
+  cudaStream_t stream = nullptr;
+};
+int rec_launch(Recorder* r, const void* func, dim3 grid, dim3 block, size_t smem, void** args);
+
+// kernels entry points implemented in the .cu files -------------------------
+int cells_rebuild_impl(md_cell_list* cl, md_system* sys, Recorder* rec, bool conditional);
+int nlist_build_impl(md_nlist* nl, md_system* sys, md_cell_list* cl, Recorder* rec, bool conditional);
+int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats, bool overwrite, Recorder* rec);
+int langevin_step1_impl(md_system* sys, md_nlist* nl, Recorder* rec);
+int langevin_step2_impl(md_system* sys, Recorder* rec);
+int clear_stats_impl(md_system* sys, Recorder* rec, int first, int count);
+int set_flag_impl(md_system* sys, unsigned bits, Recorder* rec);

@@ -1,0 +1,112 @@
+"""ctypes loader of libmdforce.so (the C ABI declared in include/mdforce.h).
+
+The library is built in-tree by ``make -C md.error_b200/csrc``.  There is no
+fallback: if the shared object is missing or cannot be loaded, importing
+this module raises, so nothing can silently run on the CPU instead.
+"""
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmdforce.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"libmdforce.so not found at {LIB_PATH}; build it with "
+        "`make -C md.error_b200/csrc` (nvcc, sm_100a)")
+
+lib = C.CDLL(LIB_PATH)
+
+vp = C.c_void_p
+i32 = C.c_int
+i64 = C.c_int64
+u64 = C.c_uint64
+f32 = C.c_float
+f64 = C.c_double
+P = C.POINTER
+
+
+class LangevinParams(C.Structure):
+    """md_langevin_params"""
+    _fields_ = [("dt", f64), ("temperature", f64), ("gamma_t", f64),
+                ("tau_p", f64), ("kappa_t", f64), ("p_ref", f64 * 3),
+                ("npt_dirs", i32), ("seed", u64)]
+
+
+class SimParams(C.Structure):
+    """md_sim_params"""
+    _fields_ = [("lv", LangevinParams), ("skin", f64), ("cell_size", f64),
+                ("expansion", f64), ("nl_mode", i32), ("use_graph", i32),
+                ("stats_every", i32)]
+
+
+_SIGS = {
+    "md_last_error_message": (C.c_char_p, []),
+    "md_version": (C.c_char_p, []),
+    "md_device_count": (i32, [P(i32)]),
+    "md_system_create": (i32, [P(vp), i32, P(f64), P(f64), P(f64), P(i32), P(f64), P(f64), i32, i32]),
+    "md_system_destroy": (i32, [vp]),
+    "md_system_set_stream": (i32, [vp, vp]),
+    "md_system_synchronize": (i32, [vp]),
+    "md_system_num_atoms": (i32, [vp, P(i32)]),
+    "md_system_set_positions": (i32, [vp, P(f64)]),
+    "md_system_get_positions": (i32, [vp, P(f64)]),
+    "md_system_get_unwrapped_positions": (i32, [vp, P(f64)]),
+    "md_system_set_velocities": (i32, [vp, P(f64)]),
+    "md_system_get_velocities": (i32, [vp, P(f64)]),
+    "md_system_get_forces": (i32, [vp, P(f64)]),
+    "md_system_get_box": (i32, [vp, P(f64)]),
+    "md_system_set_box": (i32, [vp, P(f64)]),
+    "md_system_set_rcut": (i32, [vp, P(f32)]),
+    "md_system_get_rcut": (i32, [vp, P(f32)]),
+    "md_system_normalize": (i32, [vp]),
+    "md_system_read_stats": (i32, [vp, P(f64)]),
+    "md_system_clear_stats": (i32, [vp]),
+    "md_cell_list_create": (i32, [P(vp), vp, f64, i32, i32]),
+    "md_cell_list_destroy": (i32, [vp]),
+    "md_cell_list_rebuild": (i32, [vp, vp]),
+    "md_cell_list_get_ncell": (i32, [vp, P(i32)]),
+    "md_cell_list_get_cell_index": (i32, [vp, vp, P(C.c_uint32)]),
+    "md_nlist_create": (i32, [P(vp), vp, f64, f64, f64, i32]),
+    "md_nlist_destroy": (i32, [vp]),
+    "md_nlist_rebuild": (i32, [vp, vp, vp]),
+    "md_nlist_fit": (i32, [vp, vp, vp]),
+    "md_nlist_capacity": (i32, [vp, P(i32)]),
+    "md_nlist_max_displacement": (i32, [vp, vp, P(f64)]),
+    "md_nlist_sum_neighbor": (i32, [vp, vp, P(i64)]),
+    "md_nlist_get": (i32, [vp, vp, P(C.c_int32), P(C.c_int32)]),
+    "md_engine_create": (i32, [P(vp), vp]),
+    "md_engine_destroy": (i32, [vp]),
+    "md_engine_register_lj": (i32, [vp, f64, f64, f64]),
+    "md_engine_register_bonded": (i32, [vp, i32]),
+    "md_engine_clear_forces": (i32, [vp, vp]),
+    "md_engine_apply_nonbonded": (i32, [vp, vp, vp, i32]),
+    "md_engine_apply_bonded": (i32, [vp, vp]),
+    "md_assign_rcut": (i32, [vp, P(f32), i32, i32, i32]),
+    "md_set_rcut_uniform": (i32, [vp, f32]),
+    "md_vv_step1": (i32, [vp, f64]),
+    "md_vv_step2": (i32, [vp, f64, i32]),
+    "md_langevin_setup": (i32, [vp, P(LangevinParams)]),
+    "md_langevin_step1": (i32, [vp, vp]),
+    "md_langevin_step2": (i32, [vp]),
+    "md_langevin_get_state": (i32, [vp, P(f64), P(f64)]),
+    "md_sim_create": (i32, [P(vp), vp, vp, P(SimParams)]),
+    "md_sim_destroy": (i32, [vp]),
+    "md_sim_run": (i32, [vp, i32]),
+    "md_sim_counters": (i32, [vp, P(i64), P(i64), P(i32)]),
+    "md_synth_fcc": (i32, [i32, i32, i32, P(f64), f64, u64, P(f64)]),
+    "md_synth_slab": (i32, [i32, i32, P(f64), i32, f64, f64, f64, u64, P(f64)]),
+    "md_synth_maxwell": (i32, [i32, P(f64), f64, u64, P(f64)]),
+    "md_synth_charges": (i32, [i32, u64, P(f64)]),
+}
+
+
+def _declare(sigs):
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+_declare(_SIGS)
+EXPORTED = tuple(_SIGS)

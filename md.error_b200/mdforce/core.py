@@ -1,0 +1,388 @@
+"""Host-side mirror of the md.error interaction-engine API over the C ABI.
+
+Class and method names follow the reference engine
+(shortRange.inhomo/template/tools/simulation.hetero.cutoff):
+  MDSystem            include/MDSystem_interface.h:18-104
+  CellList            include/CellList_interface.h:18-73 (rebuild)
+  NeighborList        include/NeighborList_interface.h:20-82 (rebuild)
+  InteractionEngine   include/InteractionEngine_interface.h:17-155
+                      (registNonBondedInteraction, clearInteraction,
+                       applyNonBondedInteraction, applyBondedInteraction)
+  AssignRCut          include/AssignRCut.h:10-42 (getRCut + assign)
+  VelocityVerlet      include/Integrator_interface.h:181-205 (step1/step2)
+Errors are raised as MDException subclasses named after the reference's
+exceptions / device flags (MDExcptCuda, mdErrorShortNeighborList, ...).
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._lib import lib, LangevinParams, SimParams
+
+MD_OK = 0
+MD_ERR_CELL_OVERFLOW = 1
+MD_ERR_NLIST_OVERFLOW = 2
+MD_ERR_CELL_INDEX = 3
+MD_ERR_CUDA = 10
+MD_ERR_BADARG = 11
+MD_ERR_UNSUPPORTED = 12
+MD_ERR_TIMEOUT = 13
+
+PREC_MIXED = 0
+PREC_FP64 = 1
+NL_MINIMAGE = 0
+NL_CELLSHIFT = 1
+
+STAT_NB_ENERGY, STAT_VIRIAL_XX, STAT_VIRIAL_YY, STAT_VIRIAL_ZZ = 0, 1, 2, 3
+STAT_KINETIC_XX, STAT_KINETIC_YY, STAT_KINETIC_ZZ = 4, 5, 6
+STAT_PRESSURE_CORR_XX = 7
+STAT_ELEC_DIR, STAT_ELEC_REC, STAT_ELEC_SELF = 10, 11, 12
+STAT_COUNT = 16
+
+
+class MDException(RuntimeError):
+    code = -1
+
+
+class MDExcptCuda(MDException):
+    code = MD_ERR_CUDA
+
+
+class MDExcptShortCellList(MDException):
+    code = MD_ERR_CELL_OVERFLOW
+
+
+class MDExcptShortNeighborList(MDException):
+    code = MD_ERR_NLIST_OVERFLOW
+
+
+class MDExcptCellIndexOverflow(MDException):
+    code = MD_ERR_CELL_INDEX
+
+
+class MDExcptBadArgument(MDException, ValueError):
+    code = MD_ERR_BADARG
+
+
+class MDExcptUnsupported(MDException):
+    code = MD_ERR_UNSUPPORTED
+
+
+class MDExcptTimeout(MDException):
+    code = MD_ERR_TIMEOUT
+
+
+_BY_CODE = {c.code: c for c in (MDExcptCuda, MDExcptShortCellList, MDExcptShortNeighborList,
+                                 MDExcptCellIndexOverflow, MDExcptBadArgument,
+                                 MDExcptUnsupported, MDExcptTimeout)}
+
+
+def check(status, what=""):
+    if status != MD_OK:
+        msg = lib.md_last_error_message().decode()
+        raise _BY_CODE.get(status, MDException)(f"{what}: {msg} (status {status})")
+
+
+def _p(a, ctype=C.c_double):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def _f64(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None:
+        a = a.reshape(shape)
+    return a
+
+
+def device_count():
+    n = C.c_int(0)
+    check(lib.md_device_count(C.byref(n)), "md_device_count")
+    return n.value
+
+
+class MDSystem:
+    """Per-atom SoA on the device (MDSystem / DeviceMDData)."""
+
+    def __init__(self, pos, box, vel=None, charge=None, mass=None, precision=PREC_MIXED, device=0):
+        pos = _f64(pos).reshape(-1, 3)
+        self.n = pos.shape[0]
+        box = _f64(box, (3,))
+        self.precision = precision
+        h = C.c_void_p()
+        args = [C.byref(h), self.n, _p(box), _p(pos)]
+        keep = []
+        for arr, shape in ((vel, (-1, 3)),):
+            if arr is None:
+                args.append(None)
+            else:
+                a = _f64(arr).reshape(shape)
+                keep.append(a)
+                args.append(_p(a))
+        args.append(None)  # type
+        for arr in (charge, mass):
+            if arr is None:
+                args.append(None)
+            else:
+                a = _f64(arr).reshape(-1)
+                keep.append(a)
+                args.append(_p(a))
+        args += [precision, device]
+        check(lib.md_system_create(*args), "MDSystem")
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.md_system_destroy(self.h)
+            self.h = None
+
+    def set_stream(self, stream_ptr):
+        check(lib.md_system_set_stream(self.h, C.c_void_p(stream_ptr)), "set_stream")
+
+    def synchronize(self):
+        check(lib.md_system_synchronize(self.h), "synchronize")
+
+    def _get3(self, fn):
+        out = np.empty((self.n, 3), np.float64)
+        check(fn(self.h, _p(out)), fn.__name__)
+        return out
+
+    def positions(self):
+        return self._get3(lib.md_system_get_positions)
+
+    def unwrapped_positions(self):
+        return self._get3(lib.md_system_get_unwrapped_positions)
+
+    def velocities(self):
+        return self._get3(lib.md_system_get_velocities)
+
+    def forces(self):
+        return self._get3(lib.md_system_get_forces)
+
+    def set_positions(self, pos):
+        a = _f64(pos).reshape(self.n, 3)
+        check(lib.md_system_set_positions(self.h, _p(a)), "set_positions")
+
+    def set_velocities(self, vel):
+        a = _f64(vel).reshape(self.n, 3)
+        check(lib.md_system_set_velocities(self.h, _p(a)), "set_velocities")
+
+    def box(self):
+        b = np.empty(3, np.float64)
+        check(lib.md_system_get_box(self.h, _p(b)), "get_box")
+        return b
+
+    def set_box(self, box):
+        b = _f64(box, (3,))
+        check(lib.md_system_set_box(self.h, _p(b)), "set_box")
+
+    def set_rcut(self, rcut):
+        a = np.ascontiguousarray(rcut, dtype=np.float32).reshape(self.n)
+        check(lib.md_system_set_rcut(self.h, _p(a, C.c_float)), "set_rcut")
+
+    def rcut(self):
+        a = np.empty(self.n, np.float32)
+        check(lib.md_system_get_rcut(self.h, _p(a, C.c_float)), "get_rcut")
+        return a
+
+    def normalizeDeviceData(self):
+        check(lib.md_system_normalize(self.h), "normalize")
+
+    def stats(self):
+        out = np.zeros(STAT_COUNT, np.float64)
+        check(lib.md_system_read_stats(self.h, _p(out)), "read_stats")
+        return out
+
+    def clear_stats(self):
+        check(lib.md_system_clear_stats(self.h), "clear_stats")
+
+    def pressure(self, stats=None):
+        """MDStatistic::pressureXX/YY/ZZ (ENG/include/Statistic_interface.h:92-121)."""
+        s = self.stats() if stats is None else stats
+        L = self.box()
+        V = L.prod()
+        return np.array([2.0 / V * (s[STAT_KINETIC_XX + d] - 0.5 * s[STAT_VIRIAL_XX + d])
+                         + s[STAT_PRESSURE_CORR_XX + d] for d in range(3)])
+
+
+class CellList:
+    def __init__(self, sys, cell_size, bdir=7, divide=1):
+        h = C.c_void_p()
+        check(lib.md_cell_list_create(C.byref(h), sys.h, float(cell_size), bdir, divide), "CellList")
+        self.h = h
+        self.sys = sys
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.md_cell_list_destroy(self.h)
+            self.h = None
+
+    def rebuild(self, sys=None):
+        check(lib.md_cell_list_rebuild(self.h, (sys or self.sys).h), "CellList::rebuild")
+
+    def ncell(self):
+        a = (C.c_int * 3)()
+        check(lib.md_cell_list_get_ncell(self.h, a), "ncell")
+        return tuple(a)
+
+    def cell_index(self):
+        out = np.empty(self.sys.n, np.uint32)
+        check(lib.md_cell_list_get_cell_index(self.h, self.sys.h, _p(out, C.c_uint32)), "cell_index")
+        return out
+
+
+class NeighborList:
+    def __init__(self, sys, rlist, skin, expansion=4.0, mode=NL_MINIMAGE):
+        h = C.c_void_p()
+        check(lib.md_nlist_create(C.byref(h), sys.h, float(rlist), float(skin), float(expansion), mode),
+              "NeighborList")
+        self.h = h
+        self.sys = sys
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.md_nlist_destroy(self.h)
+            self.h = None
+
+    def rebuild(self, sys, clist):
+        check(lib.md_nlist_rebuild(self.h, sys.h, clist.h), "NeighborList::rebuild")
+
+    def fit(self, sys, clist):
+        check(lib.md_nlist_fit(self.h, sys.h, clist.h), "NeighborList::fit")
+
+    def capacity(self):
+        c = C.c_int()
+        check(lib.md_nlist_capacity(self.h, C.byref(c)), "capacity")
+        return c.value
+
+    def calSumNeighbor(self):
+        s = C.c_int64()
+        check(lib.md_nlist_sum_neighbor(self.h, self.sys.h, C.byref(s)), "calSumNeighbor")
+        return s.value
+
+    def max_displacement(self):
+        d = C.c_double()
+        check(lib.md_nlist_max_displacement(self.h, self.sys.h, C.byref(d)), "max_displacement")
+        return d.value
+
+    def lists(self):
+        """(counts[N], pairs) in original atom indices (CSR order)."""
+        counts = np.empty(self.sys.n, np.int32)
+        total = self.calSumNeighbor()
+        pairs = np.empty(max(total, 1), np.int32)
+        check(lib.md_nlist_get(self.h, self.sys.h, _p(counts, C.c_int32), _p(pairs, C.c_int32)), "nlist_get")
+        return counts, pairs[:total]
+
+
+class InteractionEngine:
+    def __init__(self, sys):
+        h = C.c_void_p()
+        check(lib.md_engine_create(C.byref(h), sys.h), "InteractionEngine")
+        self.h = h
+        self.sys = sys
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.md_engine_destroy(self.h)
+            self.h = None
+
+    def registNonBondedInteraction(self, epsilon=1.0, sigma=1.0, shift=0.0):
+        check(lib.md_engine_register_lj(self.h, epsilon, sigma, shift), "registNonBondedInteraction")
+
+    def registBondedInteraction(self, n_bonds=0):
+        check(lib.md_engine_register_bonded(self.h, int(n_bonds)), "registBondedInteraction")
+
+    def clearInteraction(self, sys=None):
+        check(lib.md_engine_clear_forces(self.h, (sys or self.sys).h), "clearInteraction")
+
+    def applyNonBondedInteraction(self, sys, nlist, with_stats=True):
+        check(lib.md_engine_apply_nonbonded(self.h, sys.h, nlist.h, 1 if with_stats else 0),
+              "applyNonBondedInteraction")
+
+    def applyBondedInteraction(self, sys):
+        check(lib.md_engine_apply_bonded(self.h, sys.h), "applyBondedInteraction")
+
+
+class AssignRCut:
+    """Per-atom cutoff from an rc lattice (AssignRCut::getRCut + assign)."""
+
+    def __init__(self, lattice):
+        self.lattice = np.ascontiguousarray(lattice, dtype=np.float32)
+        assert self.lattice.ndim == 3
+
+    def uniform(self, sys, rc):
+        check(lib.md_set_rcut_uniform(sys.h, float(rc)), "AssignRCut::uniform")
+
+    def assign(self, sys):
+        nx, ny, nz = self.lattice.shape
+        check(lib.md_assign_rcut(sys.h, _p(self.lattice, C.c_float), nx, ny, nz), "AssignRCut::assign")
+
+
+class VelocityVerlet:
+    def __init__(self, sys):
+        self.sys = sys
+
+    def step1(self, sys, dt):
+        check(lib.md_vv_step1(sys.h, float(dt)), "VelocityVerlet::step1")
+
+    def step2(self, sys, dt, with_stats=True):
+        check(lib.md_vv_step2(sys.h, float(dt), 1 if with_stats else 0), "VelocityVerlet::step2")
+
+
+def langevin_params(dt, temperature, gamma_t, tau_p=0.0, kappa_t=0.0, p_ref=(0.0, 0.0, 0.0),
+                    npt_dirs=0, seed=1):
+    p = LangevinParams()
+    p.dt, p.temperature, p.gamma_t, p.tau_p, p.kappa_t = dt, temperature, gamma_t, tau_p, kappa_t
+    for d in range(3):
+        p.p_ref[d] = p_ref[d]
+    p.npt_dirs = npt_dirs
+    p.seed = seed
+    return p
+
+
+class Langevin:
+    """Langevin NVT / NPT (langevin.npt/writedown/paper.tex:355-369, 586-600)."""
+
+    def __init__(self, sys, **kw):
+        self.params = langevin_params(**kw)
+        check(lib.md_langevin_setup(sys.h, C.byref(self.params)), "Langevin")
+        self.sys = sys
+
+    def step1(self, nlist=None):
+        check(lib.md_langevin_step1(self.sys.h, nlist.h if nlist else None), "Langevin::step1")
+
+    def step2(self):
+        check(lib.md_langevin_step2(self.sys.h), "Langevin::step2")
+
+
+class Simulation:
+    """Graph-captured Langevin MD driver (the hot loop of ENG/app/lj.nhc-xtc.cu)."""
+
+    def __init__(self, sys, engine, skin, cell_size, lv, nl_mode=NL_MINIMAGE, expansion=1.5,
+                 use_graph=True):
+        p = SimParams()
+        p.lv = lv
+        p.skin = skin
+        p.cell_size = cell_size
+        p.expansion = expansion
+        p.nl_mode = nl_mode
+        p.use_graph = 1 if use_graph else 0
+        p.stats_every = 1
+        self.params = p
+        h = C.c_void_p()
+        check(lib.md_sim_create(C.byref(h), sys.h, engine.h, C.byref(p)), "Simulation")
+        self.h = h
+        self.sys = sys
+        self.engine = engine
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.md_sim_destroy(self.h)
+            self.h = None
+
+    def run(self, nsteps):
+        check(lib.md_sim_run(self.h, int(nsteps)), "Simulation::run")
+
+    def counters(self):
+        s, r, f = C.c_int64(), C.c_int64(), C.c_int()
+        check(lib.md_sim_counters(self.h, C.byref(s), C.byref(r), C.byref(f)), "counters")
+        return s.value, r.value, f.value

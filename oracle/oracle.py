@@ -1,0 +1,211 @@
+"""ORACLE -- test infrastructure only (ctypes wrapper of oracle/liboracle.so).
+
+Imported only by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+leg, as the checker; the product package never imports it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+
+def build():
+    subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+if not os.path.exists(LIB):
+    build()
+_lib = C.CDLL(LIB)
+
+P = C.POINTER
+f32, f64, i32, i64, u32, u64 = C.c_float, C.c_double, C.c_int, C.c_int64, C.c_uint32, C.c_uint64
+
+
+class LvParams(C.Structure):
+    _fields_ = [("dt", f64), ("temperature", f64), ("gamma_t", f64), ("tau_p", f64),
+                ("kappa_t", f64), ("p_ref", f64 * 3), ("npt_dirs", i32), ("seed", u64),
+                ("skin", f64), ("eps", f64), ("sigma", f64), ("shift", f64)]
+
+
+_sigs = {
+    "orc_box_inverse_f32": (None, [P(f32), P(f32)]),
+    "orc_decide_ncell": (i32, [P(f64), f64, i32, i32, P(i32)]),
+    "orc_bin_f32": (None, [i32, P(f32), P(i32), P(f32), P(i32), P(u32)]),
+    "orc_bin_f64": (None, [i32, P(f64), P(i32), P(f64), P(i32), P(u32)]),
+    "orc_nlist_allpair_f32": (None, [i32, P(f32), P(f32), f32, P(f32), i32, P(i32), P(i32)]),
+    "orc_nlist_allpair_f64": (None, [i32, P(f64), P(f64), f64, P(f64), i32, P(i32), P(i32)]),
+    "orc_nlist_cellshift_f32": (None, [i32, P(f32), P(u32), f32, P(f32), P(i32), i32, P(i32), P(i32)]),
+    "orc_lj_allpair_f64": (None, [i32, P(f64), P(f64), f64, f64, f64, P(f64), P(f32), P(f32), P(f64), P(f64)]),
+    "orc_lattice_rcut_f32": (f32, [f32, f32, f32, P(f32), P(f32), i32, i32, i32]),
+    "orc_assign_rcut_f32": (None, [i32, P(f32), P(f32), P(f32), i32, i32, i32, P(f32)]),
+    "orc_normals4": (None, [u64, u64, u32, P(f64)]),
+    "orc_md_langevin_run": (i32, [i32, P(f64), P(f64), P(f64), P(f32), P(f32), i32, i32, i32, P(f64),
+                                  P(LvParams), P(f64), i32, i32, P(f64), P(i64)]),
+    "orc_num_threads": (i32, []),
+    "orc_philox4x32_10": (None, [P(u32), P(u32), P(u32)]),
+}
+for _n, (_r, _a) in _sigs.items():
+    _f = getattr(_lib, _n)
+    _f.restype = _r
+    _f.argtypes = _a
+
+
+def _p(a, t):
+    return a.ctypes.data_as(P(t))
+
+
+def box_inverse_f32(box):
+    b = np.ascontiguousarray(box, np.float32)
+    out = np.empty(3, np.float32)
+    _lib.orc_box_inverse_f32(_p(b, f32), _p(out, f32))
+    return out
+
+
+def decide_ncell(box, cell_size, bdir=7, divide=1):
+    b = np.ascontiguousarray(box, np.float64)
+    nc = np.empty(3, np.int32)
+    mode = _lib.orc_decide_ncell(_p(b, f64), float(cell_size), bdir, divide, _p(nc, i32))
+    return tuple(int(x) for x in nc), bool(mode)
+
+
+def bin_f32(pos, box, ncell):
+    """normalise + cell index (binary32); returns (pos_wrapped, image, cell)."""
+    p = np.ascontiguousarray(pos, np.float32).copy()
+    n = p.shape[0]
+    img = np.zeros((n, 3), np.int32)
+    b = np.ascontiguousarray(box, np.float32)
+    nc = np.ascontiguousarray(ncell, np.int32)
+    cell = np.empty(n, np.uint32)
+    _lib.orc_bin_f32(n, _p(p, f32), _p(img, i32), _p(b, f32), _p(nc, i32), _p(cell, u32))
+    return p, img, cell
+
+
+def bin_f64(pos, box, ncell):
+    p = np.ascontiguousarray(pos, np.float64).copy()
+    n = p.shape[0]
+    img = np.zeros((n, 3), np.int32)
+    b = np.ascontiguousarray(box, np.float64)
+    nc = np.ascontiguousarray(ncell, np.int32)
+    cell = np.empty(n, np.uint32)
+    _lib.orc_bin_f64(n, _p(p, f64), _p(img, i32), _p(b, f64), _p(nc, i32), _p(cell, u32))
+    return p, img, cell
+
+
+def _csr(counts, pairs, cap):
+    n = counts.shape[0]
+    if (counts > cap).any():
+        raise RuntimeError("oracle list capacity exceeded")
+    rows = [pairs[i * cap:i * cap + counts[i]] for i in range(n)]
+    return counts.copy(), (np.concatenate(rows) if n else np.empty(0, np.int32))
+
+
+def nlist_allpair_f32(pos, rcut, skin, box, cap=1024):
+    p = np.ascontiguousarray(pos, np.float32)
+    n = p.shape[0]
+    rc = np.ascontiguousarray(rcut, np.float32)
+    b = np.ascontiguousarray(box, np.float32)
+    counts = np.empty(n, np.int32)
+    pairs = np.empty(n * cap, np.int32)
+    _lib.orc_nlist_allpair_f32(n, _p(p, f32), _p(rc, f32), float(np.float32(skin)), _p(b, f32), cap,
+                               _p(counts, i32), _p(pairs, i32))
+    return _csr(counts, pairs, cap)
+
+
+def nlist_allpair_f64(pos, rcut, skin, box, cap=1024):
+    p = np.ascontiguousarray(pos, np.float64)
+    n = p.shape[0]
+    rc = np.ascontiguousarray(rcut, np.float64)
+    b = np.ascontiguousarray(box, np.float64)
+    counts = np.empty(n, np.int32)
+    pairs = np.empty(n * cap, np.int32)
+    _lib.orc_nlist_allpair_f64(n, _p(p, f64), _p(rc, f64), float(skin), _p(b, f64), cap,
+                               _p(counts, i32), _p(pairs, i32))
+    return _csr(counts, pairs, cap)
+
+
+def nlist_cellshift_f32(pos, cell, rlist, box, ncell, cap=1024):
+    p = np.ascontiguousarray(pos, np.float32)
+    n = p.shape[0]
+    c = np.ascontiguousarray(cell, np.uint32)
+    b = np.ascontiguousarray(box, np.float32)
+    nc = np.ascontiguousarray(ncell, np.int32)
+    counts = np.empty(n, np.int32)
+    pairs = np.empty(n * cap, np.int32)
+    _lib.orc_nlist_cellshift_f32(n, _p(p, f32), _p(c, u32), float(np.float32(rlist)), _p(b, f32),
+                                 _p(nc, i32), cap, _p(counts, i32), _p(pairs, i32))
+    return _csr(counts, pairs, cap)
+
+
+def lj_allpair_f64(pos, rcut, box, eps=1.0, sigma=1.0, shift=0.0, pos32=None, box32=None):
+    """FP64 all-pairs LJ; returns (force[N,3], stats[E, Wxx, Wyy, Wzz])."""
+    p = np.ascontiguousarray(pos, np.float64)
+    n = p.shape[0]
+    rc = np.ascontiguousarray(rcut, np.float64)
+    b = np.ascontiguousarray(box, np.float64)
+    F = np.empty((n, 3), np.float64)
+    st = np.empty(4, np.float64)
+    p32 = None if pos32 is None else np.ascontiguousarray(pos32, np.float32)
+    b32 = None if box32 is None else np.ascontiguousarray(box32, np.float32)
+    _lib.orc_lj_allpair_f64(n, _p(p, f64), _p(rc, f64), eps, sigma, shift, _p(b, f64),
+                            None if p32 is None else _p(p32, f32), None if b32 is None else _p(b32, f32),
+                            _p(F, f64), _p(st, f64))
+    return F, st
+
+
+def assign_rcut_f32(pos, box, lattice):
+    p = np.ascontiguousarray(pos, np.float32)
+    b = np.ascontiguousarray(box, np.float32)
+    lat = np.ascontiguousarray(lattice, np.float32)
+    nx, ny, nz = lat.shape
+    out = np.empty(p.shape[0], np.float32)
+    _lib.orc_assign_rcut_f32(p.shape[0], _p(p, f32), _p(b, f32), _p(lat, f32), nx, ny, nz, _p(out, f32))
+    return out
+
+
+def normals4(seed, step, idx):
+    out = np.empty(4, np.float64)
+    _lib.orc_normals4(seed, step, idx, _p(out, f64))
+    return out
+
+
+def md_langevin_run(pos, vel, box, nsteps, *, dt, temperature, gamma_t, skin, rcut=None,
+                    lattice=None, tau_p=0.0, kappa_t=0.0, p_ref=(0, 0, 0), npt_dirs=0, seed=1,
+                    eps=1.0, sigma=1.0, shift=0.0, pcorr=None, cap=1024, mass=None):
+    """CPU FP64 Langevin MD; returns dict(pos, vel, box, stats, rebuilds, max_list, status)."""
+    p = np.ascontiguousarray(pos, np.float64).copy()
+    v = np.ascontiguousarray(vel, np.float64).copy()
+    n = p.shape[0]
+    b = np.ascontiguousarray(box, np.float64).copy()
+    prm = LvParams()
+    prm.dt, prm.temperature, prm.gamma_t, prm.tau_p, prm.kappa_t = dt, temperature, gamma_t, tau_p, kappa_t
+    for d in range(3):
+        prm.p_ref[d] = p_ref[d]
+    prm.npt_dirs, prm.seed, prm.skin, prm.eps, prm.sigma, prm.shift = npt_dirs, seed, skin, eps, sigma, shift
+    rc = None if rcut is None else np.ascontiguousarray(rcut, np.float32)
+    lat = None if lattice is None else np.ascontiguousarray(lattice, np.float32)
+    nx, ny, nz = (lat.shape if lat is not None else (0, 0, 0))
+    m = None if mass is None else np.ascontiguousarray(mass, np.float64)
+    pc = None if pcorr is None else np.ascontiguousarray(pcorr, np.float64)
+    stats = np.zeros(7, np.float64)
+    cnt = np.zeros(2, np.int64)
+    status = _lib.orc_md_langevin_run(n, _p(p, f64), _p(v, f64), None if m is None else _p(m, f64),
+                                      None if rc is None else _p(rc, f32), None if lat is None else _p(lat, f32),
+                                      nx, ny, nz, _p(b, f64), C.byref(prm), None if pc is None else _p(pc, f64),
+                                      int(nsteps), int(cap), _p(stats, f64), _p(cnt, i64))
+    return dict(pos=p, vel=v, box=b, stats=stats, rebuilds=int(cnt[0]), max_list=int(cnt[1]), status=status)
+
+
+def num_threads():
+    return _lib.orc_num_threads()
+
+
+def philox4x32_10(ctr, key):
+    c = np.ascontiguousarray(ctr, np.uint32)
+    k = np.ascontiguousarray(key, np.uint32)
+    out = np.empty(4, np.uint32)
+    _lib.orc_philox4x32_10(_p(c, u32), _p(k, u32), _p(out, u32))
+    return out

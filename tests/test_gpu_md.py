@@ -1,0 +1,232 @@
+"""GPU parity tests of the short-range path through the C ABI:
+cell binning (bit-exact), neighbour sets (bit-exact, order-independent),
+adaptive-cutoff LJ forces / energy / virial against the FP64 all-pairs
+oracle, list overflow handling, and the Langevin driver against the CPU
+FP64 oracle trajectory."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# tolerances: relative RMS force error of the mixed path (FP32 pair math,
+# compensated / FP64 accumulation) and of the FP64 path against the FP64 oracle
+TOL_MIXED = 1e-5
+TOL_FP64 = 1e-12
+
+
+def rel_rms(a, b):
+    return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+
+
+def as_sets(counts, pairs):
+    out, off = [], 0
+    for c in counts:
+        out.append(np.sort(pairs[off:off + c]))
+        off += c
+    return out
+
+
+def assert_same_sets(c1, p1, c2, p2):
+    assert np.array_equal(c1, c2), f"count mismatch at {np.nonzero(c1 != c2)[0][:10]}"
+    s1, s2 = as_sets(c1, p1), as_sets(c2, p2)
+    bad = [i for i in range(len(s1)) if not np.array_equal(s1[i], s2[i])]
+    assert not bad, f"neighbour sets differ for atoms {bad[:10]}"
+
+
+@pytest.fixture(scope="module")
+def fluid(mdf):
+    return mdf.systems.lj_fluid_fcc()
+
+
+@pytest.fixture(scope="module")
+def small_slab(mdf):
+    return mdf.systems.lj_slab(n=8192, box=(20.0, 20.0, 80.0))
+
+
+def adaptive_rcut(n, seed=0):
+    rng = np.random.default_rng(seed)
+    return rng.choice(np.arange(2.5, 5.01, 0.5), size=n).astype(np.float32)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_cell_binning_bit_exact(mdf, orc, fluid, prec):
+    rng = np.random.default_rng(5)
+    pos = fluid.pos + rng.uniform(-3, 3, size=fluid.pos.shape)  # many atoms outside the box
+    pos[0] = [fluid.box[0] * (1 - 1e-9), 0.0, -1e-7]
+    sys = mdf.MDSystem(pos, fluid.box, precision=prec)
+    cl = mdf.CellList(sys, 2.8)
+    cl.rebuild()
+    nc = cl.ncell()
+    assert nc == orc.decide_ncell(fluid.box, 2.8)[0]
+    if prec == 0:
+        p, img, cell = orc.bin_f32(pos.astype(np.float32), fluid.box.astype(np.float32), nc)
+    else:
+        p, img, cell = orc.bin_f64(pos, fluid.box, nc)
+    assert np.array_equal(cl.cell_index(), cell)
+    gp = sys.positions()
+    assert np.array_equal(gp, p.astype(np.float64))
+    un = sys.unwrapped_positions()
+    L = (fluid.box.astype(np.float32) if prec == 0 else fluid.box).astype(np.float64)
+    gimg = np.rint((un - gp) / L).astype(np.int32)
+    assert np.array_equal(gimg, img)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_nlist_uniform_minimage(mdf, orc, fluid, prec):
+    sys = mdf.MDSystem(fluid.pos, fluid.box, precision=prec)
+    eng = mdf.AssignRCut(np.full((3, 3, 3), 2.5, np.float32))
+    eng.uniform(sys, 2.5)
+    cl = mdf.CellList(sys, 2.8)
+    cl.rebuild()
+    nl = mdf.NeighborList(sys, 2.8, 0.3, expansion=2.0)
+    nl.rebuild(sys, cl)
+    c, p = nl.lists()
+    gp = sys.positions()
+    if prec == 0:
+        oc, op = orc.nlist_allpair_f32(gp.astype(np.float32), np.full(sys.n, 2.5, np.float32), 0.3,
+                                       fluid.box.astype(np.float32))
+    else:
+        oc, op = orc.nlist_allpair_f64(gp, np.full(sys.n, 2.5), 0.3, fluid.box)
+    assert_same_sets(c, p, oc, op)
+    assert 60 < c.mean() < 100
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_nlist_adaptive_minimage(mdf, orc, small_slab, prec):
+    s = small_slab
+    rc = adaptive_rcut(s.n)
+    sys = mdf.MDSystem(s.pos, s.box, precision=prec)
+    sys.set_rcut(rc)
+    cl = mdf.CellList(sys, 2.8)
+    cl.rebuild()
+    nl = mdf.NeighborList(sys, 5.3, 0.3, expansion=3.0)
+    nl.fit(sys, cl)
+    c, p = nl.lists()
+    gp = sys.positions()
+    grc = sys.rcut()
+    assert np.array_equal(grc, rc)
+    if prec == 0:
+        oc, op = orc.nlist_allpair_f32(gp.astype(np.float32), grc, 0.3, s.box.astype(np.float32))
+    else:
+        oc, op = orc.nlist_allpair_f64(gp, grc.astype(np.float64), 0.3, s.box)
+    assert_same_sets(c, p, oc, op)
+
+
+def test_nlist_cellshift_bit_exact(mdf, orc, fluid):
+    sys = mdf.MDSystem(fluid.pos, fluid.box, precision=0)
+    sys.set_rcut(np.full(sys.n, 2.5, np.float32))
+    cl = mdf.CellList(sys, 2.8)
+    cl.rebuild()
+    nl = mdf.NeighborList(sys, 2.8, 0.3, expansion=2.0, mode=mdf.NL_CELLSHIFT)
+    nl.rebuild(sys, cl)
+    c, p = nl.lists()
+    gp = sys.positions().astype(np.float32)
+    nc = cl.ncell()
+    _, _, cell = orc.bin_f32(gp, fluid.box.astype(np.float32), nc)
+    assert np.array_equal(cell, cl.cell_index())
+    oc, op = orc.nlist_cellshift_f32(gp, cell, 2.8, fluid.box.astype(np.float32), nc)
+    assert_same_sets(c, p, oc, op)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_lj_forces_vs_fp64_oracle(mdf, orc, small_slab, prec):
+    s = small_slab
+    rc = adaptive_rcut(s.n, seed=3)
+    sys = mdf.MDSystem(s.pos, s.box, precision=prec)
+    sys.set_rcut(rc)
+    cl = mdf.CellList(sys, 2.8)
+    cl.rebuild()
+    nl = mdf.NeighborList(sys, 5.3, 0.3, expansion=3.0)
+    nl.fit(sys, cl)
+    eng = mdf.InteractionEngine(sys)
+    eng.registNonBondedInteraction(1.0, 1.0, 0.0)
+    eng.clearInteraction()
+    sys.clear_stats()
+    eng.applyNonBondedInteraction(sys, nl, with_stats=True)
+    F = sys.forces()
+    st = sys.stats()
+    gp = sys.positions()
+    if prec == 0:
+        Fo, so = orc.lj_allpair_f64(gp, rc.astype(np.float64), s.box, pos32=gp.astype(np.float32),
+                                    box32=s.box.astype(np.float32))
+        tol = TOL_MIXED
+    else:
+        Fo, so = orc.lj_allpair_f64(gp, rc.astype(np.float64), s.box)
+        tol = TOL_FP64
+    err = rel_rms(F, Fo)
+    assert err < tol, err
+    assert np.allclose(st[:4], so, rtol=tol * 10, atol=0), (st[:4], so)
+
+
+def test_nlist_overflow_raises_and_fit_recovers(mdf, fluid):
+    sys = mdf.MDSystem(fluid.pos, fluid.box, precision=0)
+    sys.set_rcut(np.full(sys.n, 2.5, np.float32))
+    cl = mdf.CellList(sys, 2.8)
+    cl.rebuild()
+    nl = mdf.NeighborList(sys, 2.8, 0.3, expansion=0.2)  # far too small on purpose
+    with pytest.raises(mdf.MDExcptShortNeighborList):
+        nl.rebuild(sys, cl)
+    nl.fit(sys, cl)
+    c, _ = nl.lists()
+    assert c.max() <= nl.capacity() and c.mean() > 60
+
+
+def _run_gpu(mdf, s, prec, nsteps, use_graph=True, npt=False, rc=2.5, seed=11):
+    sys = mdf.MDSystem(s.pos, s.box, vel=s.vel, precision=prec)
+    sys.set_rcut(np.full(sys.n, rc, np.float32))
+    eng = mdf.InteractionEngine(sys)
+    eng.registNonBondedInteraction(1.0, 1.0, 0.0)
+    lv = mdf.langevin_params(dt=0.005, temperature=1.0, gamma_t=0.5, seed=seed,
+                             tau_p=1.0 if npt else 0.0, kappa_t=0.05 if npt else 0.0,
+                             p_ref=(0.0, 0.0, 0.5), npt_dirs=4 if npt else 0)
+    sim = mdf.Simulation(sys, eng, skin=0.3, cell_size=2.8, lv=lv, use_graph=use_graph)
+    sim.run(nsteps)
+    steps, rebuilds, flags = sim.counters()
+    return sys, sim, rebuilds
+
+
+@pytest.mark.parametrize("npt", [False, True])
+def test_langevin_fp64_trajectory_matches_oracle(mdf, orc, fluid, npt):
+    nsteps = 40
+    sys, sim, reb = _run_gpu(mdf, fluid, 1, nsteps, npt=npt)
+    out = orc.md_langevin_run(fluid.pos, fluid.vel, fluid.box, nsteps, dt=0.005, temperature=1.0,
+                              gamma_t=0.5, skin=0.3, rcut=np.full(fluid.n, 2.5, np.float32), seed=11,
+                              tau_p=1.0 if npt else 0.0, kappa_t=0.05 if npt else 0.0,
+                              p_ref=(0.0, 0.0, 0.5), npt_dirs=4 if npt else 0)
+    assert out["status"] == 0
+    assert reb == out["rebuilds"]
+    box = sys.box()
+    assert np.allclose(box, out["box"], rtol=1e-12, atol=0)
+    d = sys.positions() - out["pos"]
+    d -= np.round(d / box) * box
+    assert np.abs(d).max() < 1e-9
+    assert np.abs(sys.velocities() - out["vel"]).max() < 1e-8
+    st = sys.stats()
+    assert np.allclose(st[:4], out["stats"][:4], rtol=1e-10)
+
+
+def test_graph_and_direct_launch_agree(mdf, fluid):
+    a, _, ra = _run_gpu(mdf, fluid, 0, 30, use_graph=True)
+    b, _, rb = _run_gpu(mdf, fluid, 0, 30, use_graph=False)
+    assert ra == rb
+    assert np.array_equal(a.positions(), b.positions())
+    assert np.array_equal(a.velocities(), b.velocities())
+
+
+def test_mixed_tracks_fp64(mdf, fluid):
+    a, _, _ = _run_gpu(mdf, fluid, 0, 20)
+    b, _, _ = _run_gpu(mdf, fluid, 1, 20)
+    d = a.positions() - b.positions()
+    d -= np.round(d / fluid.box) * fluid.box
+    assert np.abs(d).max() < 1e-4
+
+
+def test_langevin_temperature(mdf, fluid):
+    sys, sim, _ = _run_gpu(mdf, fluid, 0, 400)
+    Ts = []
+    for _ in range(20):
+        sim.run(20)
+        st = sys.stats()
+        Ts.append(2 * st[4:7].sum() / (3 * sys.n))
+    T = np.mean(Ts)
+    assert abs(T - 1.0) < 0.05, T
