@@ -87,45 +87,47 @@ __global__ void k_bin(int N, typename V4<R>::T* pos, int4* image, DevState* st, 
   t_cell[i] = cell;
 }
 
-// single-block exclusive scan; zeroes count for the next rebuild
-__global__ void k_scan(int n, uint32_t* count, uint32_t* start, DevState* st, int gate) {
+// single-block exclusive scan (1024 threads, each owns a contiguous chunk);
+// zeroes count for the next rebuild
+__global__ void __launch_bounds__(1024) k_scan(int n, uint32_t* count, uint32_t* start, DevState* st, int gate) {
   if (gate && !(st->flags & FLAG_REBUILD)) return;
   __shared__ uint32_t wsum[32];
-  __shared__ uint32_t carry;
   const int T = blockDim.x;
-  if (threadIdx.x == 0) carry = 0;
+  const int chunk = (n + T - 1) / T;
+  const int b = threadIdx.x * chunk;
+  const int e = min(n, b + chunk);
+  uint32_t tot = 0;
+  for (int i = b; i < e; ++i) tot += count[i];
+  // exclusive block scan of the per-thread totals
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t x = tot;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[wid] = x;
   __syncthreads();
-  for (int base = 0; base < n; base += T) {
-    int i = base + threadIdx.x;
-    uint32_t v = (i < n) ? count[i] : 0u;
-    if (i < n) count[i] = 0u;
-    // inclusive warp scan
-    uint32_t x = v;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (wid == 0) {
+    uint32_t w = (lane < (T >> 5)) ? wsum[lane] : 0u;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
+      uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
     }
-    if (lane == 31) wsum[wid] = x;
-    __syncthreads();
-    if (wid == 0) {
-      uint32_t w = (lane < (T >> 5)) ? wsum[lane] : 0u;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-        if (lane >= o) w += y;
-      }
-      wsum[lane] = w;
-    }
-    __syncthreads();
-    uint32_t excl = carry + (wid > 0 ? wsum[wid - 1] : 0u) + x - v;
-    if (i < n) start[i] = excl;
-    __syncthreads();
-    if (threadIdx.x == T - 1) carry = excl + v;
-    __syncthreads();
+    wsum[lane] = w;
   }
-  if (threadIdx.x == 0) start[n] = carry;
+  __syncthreads();
+  uint32_t run = (wid > 0 ? wsum[wid - 1] : 0u) + x - tot;
+  for (int i = b; i < e; ++i) {
+    const uint32_t v = count[i];
+    start[i] = run;
+    count[i] = 0u;
+    run += v;
+  }
+  if (threadIdx.x == T - 1) start[n] = run;
+  // the thread owning the last chunk may be before T-1 when n < T*chunk
+  if (e == n && b < e) start[n] = run;
 }
 
 __global__ void k_scatter(int N, const uint32_t* t_cell, const uint32_t* slot, const uint32_t* start,
