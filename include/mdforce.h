@@ -232,12 +232,48 @@ typedef struct md_sim_params {
   int nl_mode;          /* md_nlist_mode                                   */
   int use_graph;        /* capture the step in a CUDA graph                */
   int stats_every;      /* energy/virial every n steps (NPT needs 1)       */
+  double max_rcut;      /* largest cutoff the run may assign (list capacity); 0 = current max */
 } md_sim_params;
 int md_sim_create(md_sim** out, md_system* sys, md_engine* eng, const md_sim_params* p);
 int md_sim_destroy(md_sim* sim);
 int md_sim_run(md_sim* sim, int nsteps);
 /* number of list rebuilds so far and the last status flags seen on the device */
 int md_sim_counters(md_sim* sim, int64_t* steps, int64_t* rebuilds, int* device_flags);
+/* 1 when the step graph skips the rebuild chain with a device-side conditional node */
+int md_sim_uses_conditional_graph(md_sim* sim, int* out);
+
+/* ------------------------------------------------------------ adaptive cutoff
+ * Replaces DensityProfile_PiecewiseConst (ENG/src/DensityProfile.cu:27-99),
+ * AdaptRCut (ENG/include/AdaptRCut.h:29-107, ENG/src/AdaptRCut.cu:96-508) and
+ * PressureCorrection (ENG/src/PressureCorrection.cu:27-340), FP64 on the GPU.
+ * Bins: unsigned(L_d/refh) made odd; cutoffs rcmin:rcstep:rcmax. */
+typedef struct md_adapt_rcut md_adapt_rcut;
+int md_arc_create(md_adapt_rcut** out, md_system* sys, double refh, double rcmin, double rcmax,
+                  double rcstep);
+int md_arc_destroy(md_adapt_rcut* arc);
+int md_arc_get_dims(md_adapt_rcut* arc, int n[3], int* nrc);
+/* DensityProfile::deposite of the current coordinates / clearData */
+int md_arc_deposit(md_adapt_rcut* arc, md_system* sys);
+int md_arc_clear_profile(md_adapt_rcut* arc);
+/* use an explicit density profile [nx][ny][nz] instead of deposited samples */
+int md_arc_set_profile(md_adapt_rcut* arc, const double* rho);
+int md_arc_get_profile(md_adapt_rcut* arc, double* rho);
+/* DensityProfile::calculate + AdaptRCut::calError + calRCut(prec) + refineRCut x nrefine
+   + PressureCorrection::correction, all on the device */
+int md_arc_update(md_adapt_rcut* arc, double prec, int nrefine);
+int md_arc_get_error(md_adapt_rcut* arc, double* error /* [nrc][nele] */);
+int md_arc_get_rcut(md_adapt_rcut* arc, double* rcut, int* index, double* result_error);
+/* k-space kernels: s1k [nrc][nele], s2k [3][nrc][nele] (imaginary parts),
+   pressure-correction kernels [3][nrc][nele] */
+int md_arc_get_tables(md_adapt_rcut* arc, double* s1k, double* s2k, double* pck);
+/* AssignRCut::getRCut + assign: lattice to the system, list rebuild at the next step */
+int md_arc_assign(md_adapt_rcut* arc, md_system* sys);
+/* tail pressure tensor into MD_STAT_PRESSURE_CORR_*; out (nullable) gets it too */
+int md_arc_pressure_correction(md_adapt_rcut* arc, md_system* sys, double out[3]);
+/* the reference's schedule inside md_sim_run: deposit every sample_every steps,
+   update + assign + pressure correction every update_every steps */
+int md_sim_attach_adapt_rcut(md_sim* sim, md_adapt_rcut* arc, int sample_every, int update_every,
+                             double prec, int nrefine);
 
 /* ------------------------------------------------------------ synthetic inputs
  * Seeded generators of the benchmark systems (host only, no GPU needed).  The

@@ -1,0 +1,592 @@
+// Adaptive cutoff estimate (AdaptRCut), its density profile and the tail
+// pressure correction, all in FP64 on the GPU.
+// Reference (ENG = shortRange.inhomo/template/tools/simulation.hetero.cutoff):
+//   DensityProfile_PiecewiseConst  ENG/src/DensityProfile.cu:27-99
+//   AdaptRCut::makeS1k/makeS2k     ENG/src/AdaptRCut.cu:265-416
+//   AdaptRCut::calError/calRCut/refineRCut  ENG/src/AdaptRCut.cu:182-508
+//   Integral1D Gauss4              ENG/src/Integral1D.cu:164-232
+//   PressureCorrection             ENG/src/PressureCorrection.cu:175-340
+//   AssignRCut::getRCut + assign   ENG/src/AssignRCut.cu:46-117
+//
+// k-space kernels: the radial integrals depend on |k| only, so one thread per
+// point of the k-grid octant runs the adaptive Gauss-4 quadrature (explicit
+// stack, same subdivision rule as the reference) for every rc interval and
+// writes the kernel values of all sign images.  The 3D transforms of the
+// (odd-sized) bin grid are batched direct DFTs along each axis with the line
+// and its twiddles in shared memory.  Error map, bisection and refinement are
+// element-wise kernels; nothing returns to the host until asked.
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "device_common.cuh"
+
+struct md_adapt_rcut {
+  int n[3] = {0, 0, 0};
+  long nele = 0;
+  int nrc = 0;
+  std::vector<double> rc;
+  double box_tab[3] = {0, 0, 0};  // box the kernel tables were built for
+  double* d_rc = nullptr;
+  double* counts = nullptr;   // deposited atom counts per bin
+  double* rho = nullptr;      // profile (calculate)
+  double2* rhok = nullptr;
+  double* s1k = nullptr;      // [nrc][nele] real
+  double* s2k = nullptr;      // [3][nrc][nele] imaginary
+  double* pck = nullptr;      // [3][nrc][nele] real (pressure-correction kernels)
+  double2* work = nullptr;    // [4*nrc][nele]
+  double* error = nullptr;    // [nrc][nele]
+  double* rcut = nullptr;     // [nele]
+  int* rcidx = nullptr;       // [nele]
+  int* rcidx2 = nullptr;
+  double* rerr = nullptr;
+  double* pcorr = nullptr;    // [3]
+  int ndata = 0;
+  cudaStream_t stream = nullptr;
+  md_system* sys = nullptr;
+};
+
+// ------------------------------------------------------------ quadrature
+__device__ __forceinline__ double pow_int_d(double x, int nn) {
+  unsigned n;
+  if (nn < 0) { x = 1.0 / x; n = (unsigned)(-nn); } else n = (unsigned)nn;
+  double v = 1.0;
+  do {
+    if (n & 1) v *= x;
+    n >>= 1;
+    x *= x;
+  } while (n);
+  return v;
+}
+
+// integrands: 13 -> x^-13 sin(2 pi k x); 5 -> x^-5 sin(2 pi k x);
+// 1 / 25 -> -24 x^-4.5 J_{1/2}(2 pi k x) / J_{5/2}(2 pi k x) (closed forms)
+__device__ __forceinline__ double fn_eval(int kind, double k, double x) {
+  double s, c;
+  sincospi(2.0 * k * x, &s, &c);
+  if (kind == 13) return pow_int_d(x, -13) * s;
+  if (kind == 5) return pow_int_d(x, -5) * s;
+  const double z = 2.0 * M_PI * k * x;
+  const double pre = -24.0 / (pow_int_d(x, 4) * sqrt(x));
+  if (z == 0.0) return 0.0;
+  const double r = sqrt(2.0 / (M_PI * z));
+  if (kind == 1) return pre * r * s;
+  return pre * r * ((3.0 / (z * z) - 1.0) * s - 3.0 * c / z);
+}
+
+__device__ double g4_coarse(int kind, double k, double xlo, double xup) {
+  const double v0 = 0.33998104358485626, v1 = 0.86113631159405258;   // Gauss-Legendre 4 nodes
+  const double w0 = 0.65214515486254614, w1 = 0.34785484513745386;   // and weights
+  const double hm = 0.5 * (xup - xlo), c = 0.5 * (xup + xlo);
+  return hm * (w1 * (fn_eval(kind, k, c - hm * v1) + fn_eval(kind, k, c + hm * v1)) +
+               w0 * (fn_eval(kind, k, c - hm * v0) + fn_eval(kind, k, c + hm * v0)));
+}
+
+// Integral1D::cal_int(Gauss4, f, xlo, xup, tol): bisect a box while
+// |coarse - (left + right)| >= 255 tol, children get tol/2; stop below
+// 1e-13 of the interval.  Depth-first with an explicit stack.
+__device__ double g4_adaptive(int kind, double k, double xlo, double xup, double tol, unsigned* flags) {
+  const int MAXD = 64;
+  double sa[MAXD], sb[MAXD], st[MAXD], sc[MAXD];
+  int top = 0;
+  const double ghx = xup - xlo;
+  sa[0] = xlo; sb[0] = xup; st[0] = tol; sc[0] = g4_coarse(kind, k, xlo, xup);
+  top = 1;
+  double total = 0.0;
+  while (top > 0) {
+    --top;
+    const double a = sa[top], b = sb[top], t = st[top], coarse = sc[top];
+    const double hh = 0.5 * (b - a);
+    const double c0 = g4_coarse(kind, k, a, a + hh), c1 = g4_coarse(kind, k, a + hh, b);
+    const double v = c0 + c1;
+    if (fabs(coarse - v) < t * 255 || hh * 2 < 1e-13 * ghx) { total += v; continue; }
+    if (top + 2 > MAXD) { atomicOr(flags, FLAG_QUADRATURE); total += v; continue; }
+    sa[top] = a + hh; sb[top] = b; st[top] = t * 0.5; sc[top] = c1; ++top;   // right, popped later
+    sa[top] = a; sb[top] = a + hh; st[top] = t * 0.5; sc[top] = c0; ++top;   // left first
+  }
+  return total;
+}
+
+__device__ __forceinline__ long lin(const int n[3], int x, int y, int z) { return z + (long)n[2] * (y + (long)n[1] * x); }
+
+struct ArcDims { int n[3]; int nrc; double box[3]; };
+
+// one thread per octant point (ax, ay, az) >= 0
+__global__ void k_arc_tables(ArcDims g, const double* rc, double* s1k, double* s2k, double* pck, unsigned* flags) {
+  const int hx = g.n[0] / 2 + 1, hy = g.n[1] / 2 + 1, hz = g.n[2] / 2 + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= hx * hy * hz) return;
+  const int az = t % hz, ay = (t / hz) % hy, ax = t / (hz * hy);
+  const int nrc = g.nrc;
+  const long nele = (long)g.n[0] * g.n[1] * g.n[2];
+  const double eps = 1.0, sigma = 1.0;
+  const double pref = 16. * 36. * pow_int_d(sigma, 12) * eps;
+  const double pre = 8. * eps * pow_int_d(sigma, 6);
+  const double kx0 = ax / g.box[0], ky0 = ay / g.box[1], kz0 = az / g.box[2];
+  const double k = sqrt(kx0 * kx0 + ky0 * ky0 + kz0 * kz0);
+  const int MAXRC = 32;
+  double S1[MAXRC], T[MAXRC], I1[MAXRC], I5[MAXRC];
+  // cumulative integrals from the top interval [rc_last, 30] down
+  double cum13 = 0, cum5 = 0;
+  for (int c = nrc - 1; c >= 0; --c) {
+    const double hi = (c == nrc - 1) ? 30.0 : rc[c + 1];
+    if (k != 0) {
+      cum13 += 2. / k * pref * g4_adaptive(13, k, rc[c], hi, 1e-12, flags);
+      S1[c] = cum13;
+      cum5 += g4_adaptive(5, k, rc[c], hi, 1e-16, flags) * pre / k * 2 * M_PI;
+      const double r = rc[c], r6 = pow_int_d(r, 6);
+      const double e = 2. * M_PI * k * r;
+      double size = -2. * M_PI * r * r * (4. * eps * pow_int_d(sigma, 6) / r6) * (2. * cos(e) / e - 2. * sin(e) / (e * e));
+      size /= k;
+      T[c] = cum5 + size;
+      I1[c] = g4_adaptive(1, k, rc[c], hi, 1e-7, flags);
+      I5[c] = g4_adaptive(25, k, rc[c], hi, 1e-7, flags);
+    } else {
+      S1[c] = 4. * M_PI * pref / 11. * pow_int_d(rc[c], -11);
+      T[c] = 0;
+      I1[c] = I5[c] = 0;
+    }
+  }
+  // write every sign image of this octant point
+  for (int sx = 0; sx < 2; ++sx) {
+    if (sx && ax == 0) continue;
+    for (int sy = 0; sy < 2; ++sy) {
+      if (sy && ay == 0) continue;
+      for (int sz = 0; sz < 2; ++sz) {
+        if (sz && az == 0) continue;
+        const int ix = sx ? -ax : ax, iy = sy ? -ay : ay, iz = sz ? -az : az;
+        const int lx = ix < 0 ? ix + g.n[0] : ix, ly = iy < 0 ? iy + g.n[1] : iy, lz = iz < 0 ? iz + g.n[2] : iz;
+        const long p = lin(g.n, lx, ly, lz);
+        const double kx = ix / g.box[0], ky = iy / g.box[1], kz = iz / g.box[2];
+        // angular factors of PressureCorrection::makeKernel
+        double cp = 0, sp = 0, c2t = 1;
+        if (k != 0) {
+          const double phi = acos(kz / k);
+          double theta = 0.;
+          if (phi != 0.) {
+            double tt = kx / (k * sin(phi));
+            tt = fmin(1.0, fmax(-1.0, tt));
+            theta = acos(tt);
+            if (ky < 0) theta = 2. * M_PI - theta;
+          }
+          cp = cos(phi); sp = sin(phi); c2t = cos(theta * 2);
+        }
+        const double sc = (k != 0) ? M_PI / sqrt(k) : 0.0;
+        double cx = 0, cy = 0, cz = 0;
+        for (int c = nrc - 1; c >= 0; --c) {
+          s1k[(long)c * nele + p] = S1[c];
+          s2k[(0L * nrc + c) * nele + p] = kx * T[c];
+          s2k[(1L * nrc + c) * nele + p] = ky * T[c];
+          s2k[(2L * nrc + c) * nele + p] = kz * T[c];
+          if (k != 0) {
+            cx += sc * (2. / 3. * I1[c] + (-1. / 3. + cp * cp - sp * sp * c2t) * I5[c]);
+            cy += sc * (2. / 3. * I1[c] + (-1. / 3. + cp * cp + sp * sp * c2t) * I5[c]);
+            cz += sc * 4. / 3. * (0.5 * I1[c] + (0.5 - 1.5 * cp * cp) * I5[c]);
+          }
+          pck[(0L * nrc + c) * nele + p] = cx;
+          pck[(1L * nrc + c) * nele + p] = cy;
+          pck[(2L * nrc + c) * nele + p] = cz;
+        }
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ batched DFT
+// One block per line; lines of all `batch` arrays of the grid along `axis`.
+// out[k] = sum_j in[j] exp(sign 2 pi i jk/n), in place.  n <= 1024.
+__global__ void k_dft_axis(double2* data, ArcDims g, int axis, int sign, int batch) {
+  extern __shared__ double2 sm[];
+  double2* line = sm;
+  double2* tw = sm + g.n[axis];
+  const int n = g.n[axis];
+  const long nele = (long)g.n[0] * g.n[1] * g.n[2];
+  const int a1 = (axis + 1) % 3, a2 = (axis + 2) % 3;
+  const long lines = (long)g.n[a1] * g.n[a2];
+  const long lid = blockIdx.x;
+  if (lid >= lines * batch) return;
+  const int b = (int)(lid / lines);
+  const long r = lid % lines;
+  const int i1 = (int)(r / g.n[a2]), i2 = (int)(r % g.n[a2]);
+  const long stride[3] = {(long)g.n[1] * g.n[2], (long)g.n[2], 1};
+  double2* base = data + (long)b * nele + i1 * stride[a1] + i2 * stride[a2];
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    line[j] = base[j * stride[axis]];
+    double s, c;
+    sincospi(2.0 * j / n, &s, &c);
+    tw[j] = make_double2(c, sign * s);
+  }
+  __syncthreads();
+  for (int kk = threadIdx.x; kk < n; kk += blockDim.x) {
+    double sr = 0, si = 0;
+    int m = 0;
+    for (int j = 0; j < n; ++j) {
+      const double2 x = line[j], w = tw[m];
+      sr += x.x * w.x - x.y * w.y;
+      si += x.x * w.y + x.y * w.x;
+      m += kk;
+      if (m >= n) m -= n;
+    }
+    base[kk * stride[axis]] = make_double2(sr, si);
+  }
+}
+
+static int dft3(md_adapt_rcut* a, double2* data, int sign, int batch) {
+  ArcDims g;
+  for (int d = 0; d < 3; ++d) g.n[d] = a->n[d];
+  for (int axis = 2; axis >= 0; --axis) {
+    long lines = (long)g.n[(axis + 1) % 3] * g.n[(axis + 2) % 3] * batch;
+    size_t smem = sizeof(double2) * 2 * g.n[axis];
+    k_dft_axis<<<(unsigned)lines, 128, smem, a->stream>>>(data, g, axis, sign, batch);
+    MD_CHECK_LAUNCH("dft axis");
+  }
+  return MD_OK;
+}
+
+// ------------------------------------------------------------ element-wise kernels
+template <class R>
+__global__ void k_arc_deposit(int N, const typename V4<R>::T* pos, const DevState* st, ArcDims g, double* counts) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const typename V4<R>::T p = pos[i];
+  const double c[3] = {(double)(float)p.x, (double)(float)p.y, (double)(float)p.z};
+  unsigned b[3];
+  for (int d = 0; d < 3; ++d) {
+    const double L = st->L[d];
+    double tmp = c[d];
+    if (c[d] >= L) tmp -= L; else if (c[d] < 0) tmp += L;
+    const double h = L / g.n[d];
+    double q = tmp / h;
+    b[d] = q > 0 ? (unsigned)q : 0u;
+    if (b[d] >= (unsigned)g.n[d]) b[d] = g.n[d] - 1;
+  }
+  atomicAdd(&counts[b[2] + (long)g.n[2] * (b[1] + (long)g.n[1] * b[0])], 1.0);
+}
+
+__global__ void k_arc_profile(long nele, const double* counts, double inv, double* rho, double2* out) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= nele) return;
+  const double r = counts ? counts[i] * inv : rho[i];
+  rho[i] = r;
+  out[i] = make_double2(r, 0.0);
+}
+
+__global__ void k_arc_multiply(long nele, int nrc, const double2* rhok, double scale, const double* s1k,
+                               const double* s2k, double2* work) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= nele) return;
+  const double2 r = make_double2(rhok[i].x * scale, rhok[i].y * scale);
+  for (int c = 0; c < nrc; ++c) {
+    const double s = s1k[(long)c * nele + i];
+    work[(long)(4 * c) * nele + i] = make_double2(r.x * s, r.y * s);
+    for (int d = 0; d < 3; ++d) {
+      const double b = s2k[((long)d * nrc + c) * nele + i];
+      work[(long)(4 * c + 1 + d) * nele + i] = make_double2(-r.y * b, r.x * b);
+    }
+  }
+}
+
+__global__ void k_arc_error(long nele, int nrc, const double2* work, double Vi, double* error) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= nele) return;
+  for (int c = 0; c < nrc; ++c) {
+    const double e1 = work[(long)(4 * c) * nele + i].x * Vi;
+    const double ex = work[(long)(4 * c + 1) * nele + i].x * Vi;
+    const double ey = work[(long)(4 * c + 2) * nele + i].x * Vi;
+    const double ez = work[(long)(4 * c + 3) * nele + i].x * Vi;
+    error[(long)c * nele + i] = sqrt(e1 + ex * ex + ey * ey + ez * ez);
+  }
+}
+
+// calRCutOnePoint (AdaptRCut.cu:418-460)
+__global__ void k_arc_rcut(long nele, int nrc, const double* rc, const double* error, double prec,
+                           double* rcut, int* idx, double* rerr) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= nele) return;
+  unsigned a = 0, b = nrc - 1;
+  const double ea = error[i], eb0 = error[(long)b * nele + i];
+  if (ea - prec <= 0) { rcut[i] = rc[a]; idx[i] = a; rerr[i] = ea; return; }
+  if (eb0 - prec >= 0) { rcut[i] = rc[b]; idx[i] = b; rerr[i] = eb0; return; }
+  double eb = eb0;
+  while (b - a > 1) {
+    const unsigned c = (a + b) / 2;
+    const double ec = error[(long)c * nele + i];
+    if (ec > prec) a = c; else { b = c; eb = ec; }
+  }
+  rcut[i] = rc[b]; idx[i] = b; rerr[i] = eb;
+}
+
+// refineRCut (AdaptRCut.cu:470-508)
+__global__ void k_arc_refine(ArcDims g, const int* in, int* out, const double* rc, const double* error,
+                             double* rcut, double* rerr) {
+  const long nele = (long)g.n[0] * g.n[1] * g.n[2];
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= nele) return;
+  const int z = (int)(i % g.n[2]), y = (int)((i / g.n[2]) % g.n[1]), x = (int)(i / ((long)g.n[2] * g.n[1]));
+  int m = 0;
+  for (int dx = -1; dx <= 1; ++dx)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dz = -1; dz <= 1; ++dz) {
+        const int jx = (x + dx + g.n[0]) % g.n[0], jy = (y + dy + g.n[1]) % g.n[1], jz = (z + dz + g.n[2]) % g.n[2];
+        m = max(m, in[lin(g.n, jx, jy, jz)]);
+      }
+  out[i] = m;
+  rcut[i] = rc[m];
+  rerr[i] = error[(long)m * nele + i];
+}
+
+__global__ void k_pc_multiply(long nele, int nrc, const double2* rhok, double scale, const double* pck, double2* work) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= nele) return;
+  const double2 r = make_double2(rhok[i].x * scale, rhok[i].y * scale);
+  for (int t = 0; t < 3 * nrc; ++t) {
+    const double kk = pck[(long)t * nele + i];
+    work[(long)t * nele + i] = make_double2(r.x * kk, r.y * kk);
+  }
+}
+
+// p_aa = sum_i 0.5 conv_aa[idx_i](i) rho_i dv / V^2 (PressureCorrection::correction)
+__global__ void k_pc_reduce(long nele, int nrc, const double2* work, const int* idx, const double* rho,
+                            double fac, double* partials, unsigned* counter, double* out) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  double v[3] = {0, 0, 0};
+  if (i < nele) {
+    const int c = idx[i];
+    for (int d = 0; d < 3; ++d) v[d] = 0.5 * work[((long)d * nrc + c) * nele + i].x * rho[i] * fac;
+  }
+  block_reduce_finish<3>(v, partials, counter, out, true);
+}
+
+__global__ void k_store_pcorr(const double* p, DevState* st) {
+  for (int d = 0; d < 3; ++d) st->stats[MD_STAT_PRESSURE_CORR_XX + d] = p[d];
+}
+
+__global__ void k_lattice_from_rcut(long nele, const double* rcut, float* lat, DevState* st) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < nele) lat[i] = (float)rcut[i];
+  if (i == 0) atomicOr(&st->flags, FLAG_FORCE_REBUILD);
+}
+
+// ------------------------------------------------------------ host side
+static int build_tables(md_adapt_rcut* a) {
+  DevState hs;
+  if (int r = a->sys->read_state(hs)) return r;
+  ArcDims g;
+  for (int d = 0; d < 3; ++d) { g.n[d] = a->n[d]; g.box[d] = hs.L[d]; a->box_tab[d] = hs.L[d]; }
+  g.nrc = a->nrc;
+  int oct = (g.n[0] / 2 + 1) * (g.n[1] / 2 + 1) * (g.n[2] / 2 + 1);
+  k_arc_tables<<<ceil_div(oct, 64), 64, 0, a->stream>>>(g, a->d_rc, a->s1k, a->s2k, a->pck, &a->sys->st->flags);
+  MD_CHECK_LAUNCH("arc tables");
+  return MD_OK;
+}
+
+extern "C" int md_arc_create(md_adapt_rcut** out, md_system* sys, double refh, double rcmin, double rcmax,
+                             double rcstep) {
+  if (!out || !sys || !(refh > 0) || !(rcmin > 0) || !(rcmax >= rcmin) || !(rcstep > 0)) {
+    md_set_error("md_arc_create: bad arguments");
+    return MD_ERR_BADARG;
+  }
+  DevState hs;
+  if (int r = sys->read_state(hs)) return r;
+  md_adapt_rcut* a = new md_adapt_rcut();
+  a->sys = sys;
+  a->stream = sys->stream;
+  for (int d = 0; d < 3; ++d) {  // DensityProfile_PiecewiseConst::reinit: odd bin counts
+    unsigned v = (unsigned)(hs.L[d] / refh);
+    if ((v - (v / 2) * 2) == 0) v++;
+    a->n[d] = (int)v;
+  }
+  if (a->n[0] > 1024 || a->n[1] > 1024 || a->n[2] > 1024) {
+    delete a;
+    md_set_error("md_arc_create: more than 1024 bins along one direction");
+    return MD_ERR_BADARG;
+  }
+  for (double r = rcmin; r <= rcmax; r += rcstep) a->rc.push_back(r);  // AdaptRCut::reinit rcList
+  a->nrc = (int)a->rc.size();
+  if (a->nrc > 32) { delete a; md_set_error("md_arc_create: at most 32 cutoffs"); return MD_ERR_BADARG; }
+  a->nele = (long)a->n[0] * a->n[1] * a->n[2];
+  const long ne = a->nele;
+  const int nrc = a->nrc;
+  bool ok = cudaMalloc(&a->d_rc, sizeof(double) * nrc) == cudaSuccess &&
+            cudaMalloc(&a->counts, sizeof(double) * ne) == cudaSuccess &&
+            cudaMalloc(&a->rho, sizeof(double) * ne) == cudaSuccess &&
+            cudaMalloc(&a->rhok, sizeof(double2) * ne) == cudaSuccess &&
+            cudaMalloc(&a->s1k, sizeof(double) * nrc * ne) == cudaSuccess &&
+            cudaMalloc(&a->s2k, sizeof(double) * 3 * nrc * ne) == cudaSuccess &&
+            cudaMalloc(&a->pck, sizeof(double) * 3 * nrc * ne) == cudaSuccess &&
+            cudaMalloc(&a->work, sizeof(double2) * 4 * nrc * ne) == cudaSuccess &&
+            cudaMalloc(&a->error, sizeof(double) * nrc * ne) == cudaSuccess &&
+            cudaMalloc(&a->rcut, sizeof(double) * ne) == cudaSuccess &&
+            cudaMalloc(&a->rcidx, sizeof(int) * ne) == cudaSuccess &&
+            cudaMalloc(&a->rcidx2, sizeof(int) * ne) == cudaSuccess &&
+            cudaMalloc(&a->rerr, sizeof(double) * ne) == cudaSuccess &&
+            cudaMalloc(&a->pcorr, sizeof(double) * 3) == cudaSuccess;
+  if (!ok) {
+    md_cuda_fail(cudaGetLastError(), "md_arc_create");
+    md_arc_destroy(a);
+    return MD_ERR_CUDA;
+  }
+  cudaMemcpyAsync(a->d_rc, a->rc.data(), sizeof(double) * nrc, cudaMemcpyHostToDevice, a->stream);
+  cudaMemsetAsync(a->counts, 0, sizeof(double) * ne, a->stream);
+  cudaMemsetAsync(a->rho, 0, sizeof(double) * ne, a->stream);
+  if (int r = build_tables(a)) { md_arc_destroy(a); return r; }
+  *out = a;
+  return MD_OK;
+}
+
+extern "C" int md_arc_destroy(md_adapt_rcut* a) {
+  if (!a) return MD_OK;
+  void* p[] = {a->d_rc, a->counts, a->rho, a->rhok, a->s1k, a->s2k, a->pck, a->work,
+               a->error, a->rcut, a->rcidx, a->rcidx2, a->rerr, a->pcorr};
+  for (void* q : p) if (q) cudaFree(q);
+  delete a;
+  return MD_OK;
+}
+
+extern "C" int md_arc_get_dims(md_adapt_rcut* a, int n[3], int* nrc) {
+  if (!a) return MD_ERR_BADARG;
+  if (n) for (int d = 0; d < 3; ++d) n[d] = a->n[d];
+  if (nrc) *nrc = a->nrc;
+  return MD_OK;
+}
+
+extern "C" int md_arc_deposit(md_adapt_rcut* a, md_system* sys) {
+  if (!a || !sys) return MD_ERR_BADARG;
+  ArcDims g;
+  for (int d = 0; d < 3; ++d) g.n[d] = a->n[d];
+  int nb = ceil_div(sys->N, 256);
+  if (sys->prec == MD_PREC_FP64)
+    k_arc_deposit<double><<<nb, 256, 0, a->stream>>>(sys->N, (double4a*)sys->pos, sys->st, g, a->counts);
+  else
+    k_arc_deposit<float><<<nb, 256, 0, a->stream>>>(sys->N, (float4*)sys->pos, sys->st, g, a->counts);
+  MD_CHECK_LAUNCH("arc deposit");
+  a->ndata++;
+  return MD_OK;
+}
+
+extern "C" int md_arc_clear_profile(md_adapt_rcut* a) {
+  if (!a) return MD_ERR_BADARG;
+  MD_CUDA(cudaMemsetAsync(a->counts, 0, sizeof(double) * a->nele, a->stream));
+  a->ndata = 0;
+  return MD_OK;
+}
+
+extern "C" int md_arc_set_profile(md_adapt_rcut* a, const double* rho) {
+  if (!a || !rho) return MD_ERR_BADARG;
+  MD_CUDA(cudaMemcpyAsync(a->rho, rho, sizeof(double) * a->nele, cudaMemcpyHostToDevice, a->stream));
+  MD_CUDA(cudaStreamSynchronize(a->stream));
+  a->ndata = -1;  // explicit profile: do not renormalise counts
+  return MD_OK;
+}
+
+extern "C" int md_arc_get_profile(md_adapt_rcut* a, double* rho) {
+  if (!a || !rho) return MD_ERR_BADARG;
+  MD_CUDA(cudaMemcpyAsync(rho, a->rho, sizeof(double) * a->nele, cudaMemcpyDeviceToHost, a->stream));
+  MD_CUDA(cudaStreamSynchronize(a->stream));
+  return MD_OK;
+}
+
+extern "C" int md_arc_update(md_adapt_rcut* a, double prec, int nrefine) {
+  if (!a || !(prec > 0) || nrefine < 0) { md_set_error("md_arc_update: bad arguments"); return MD_ERR_BADARG; }
+  md_system* sys = a->sys;
+  DevState hs;
+  if (int r = sys->read_state(hs)) return r;
+  bool box_changed = false;
+  for (int d = 0; d < 3; ++d) box_changed |= fabs(hs.L[d] - a->box_tab[d]) > 1e-9 * a->box_tab[d];
+  if (box_changed)
+    if (int r = build_tables(a)) return r;
+  const long ne = a->nele;
+  const int nb = (int)((ne + 255) / 256);
+  // DensityProfile::calculate: counts / (dv * ndata), or the explicit profile
+  if (a->ndata > 0) {
+    double dv = (hs.L[0] / a->n[0]) * (hs.L[1] / a->n[1]) * (hs.L[2] / a->n[2]);
+    k_arc_profile<<<nb, 256, 0, a->stream>>>(ne, a->counts, 1.0 / (dv * a->ndata), a->rho, a->rhok);
+  } else if (a->ndata < 0) {
+    k_arc_profile<<<nb, 256, 0, a->stream>>>(ne, nullptr, 0.0, a->rho, a->rhok);
+  } else {
+    md_set_error("md_arc_update: no density samples deposited");
+    return MD_ERR_BADARG;
+  }
+  MD_CHECK_LAUNCH("arc profile");
+  if (int r = dft3(a, a->rhok, -1, 1)) return r;
+  const double V = hs.L[0] * hs.L[1] * hs.L[2];
+  k_arc_multiply<<<nb, 256, 0, a->stream>>>(ne, a->nrc, a->rhok, V / ne, a->s1k, a->s2k, a->work);
+  MD_CHECK_LAUNCH("arc multiply");
+  if (int r = dft3(a, a->work, +1, 4 * a->nrc)) return r;
+  k_arc_error<<<nb, 256, 0, a->stream>>>(ne, a->nrc, a->work, 1.0 / V, a->error);
+  k_arc_rcut<<<nb, 256, 0, a->stream>>>(ne, a->nrc, a->d_rc, a->error, prec, a->rcut, a->rcidx, a->rerr);
+  MD_CHECK_LAUNCH("arc rcut");
+  ArcDims g;
+  for (int d = 0; d < 3; ++d) g.n[d] = a->n[d];
+  for (int it = 0; it < nrefine; ++it) {
+    k_arc_refine<<<nb, 256, 0, a->stream>>>(g, a->rcidx, a->rcidx2, a->d_rc, a->error, a->rcut, a->rerr);
+    MD_CHECK_LAUNCH("arc refine");
+    std::swap(a->rcidx, a->rcidx2);
+  }
+  // PressureCorrection::correction on the same profile and rc map
+  k_pc_multiply<<<nb, 256, 0, a->stream>>>(ne, a->nrc, a->rhok, V / ne, a->pck, a->work);
+  MD_CHECK_LAUNCH("pc multiply");
+  if (int r = dft3(a, a->work, +1, 3 * a->nrc)) return r;
+  const double dv = (hs.L[0] / a->n[0]) * (hs.L[1] / a->n[1]) * (hs.L[2] / a->n[2]);
+  if (nb > sys->max_partial_blocks) { md_set_error("partials buffer too small"); return MD_ERR_BADARG; }
+  k_pc_reduce<<<nb, 256, 0, a->stream>>>(ne, a->nrc, a->work, a->rcidx, a->rho, dv / (V * V), sys->partials,
+                                         &sys->st->red_counter[RED_MISC], a->pcorr);
+  MD_CHECK_LAUNCH("pc reduce");
+  return MD_OK;
+}
+
+extern "C" int md_arc_get_error(md_adapt_rcut* a, double* err) {
+  if (!a || !err) return MD_ERR_BADARG;
+  MD_CUDA(cudaMemcpyAsync(err, a->error, sizeof(double) * a->nrc * a->nele, cudaMemcpyDeviceToHost, a->stream));
+  MD_CUDA(cudaStreamSynchronize(a->stream));
+  return MD_OK;
+}
+
+extern "C" int md_arc_get_rcut(md_adapt_rcut* a, double* rcut, int* idx, double* result_error) {
+  if (!a) return MD_ERR_BADARG;
+  if (rcut) MD_CUDA(cudaMemcpyAsync(rcut, a->rcut, sizeof(double) * a->nele, cudaMemcpyDeviceToHost, a->stream));
+  if (idx) MD_CUDA(cudaMemcpyAsync(idx, a->rcidx, sizeof(int) * a->nele, cudaMemcpyDeviceToHost, a->stream));
+  if (result_error) MD_CUDA(cudaMemcpyAsync(result_error, a->rerr, sizeof(double) * a->nele, cudaMemcpyDeviceToHost, a->stream));
+  MD_CUDA(cudaStreamSynchronize(a->stream));
+  DevState hs;
+  if (int r = a->sys->read_state(hs)) return r;
+  if (hs.flags & FLAG_QUADRATURE) { md_set_error("adaptive quadrature reached its depth bound"); return MD_ERR_BADARG; }
+  return MD_OK;
+}
+
+extern "C" int md_arc_get_tables(md_adapt_rcut* a, double* s1k, double* s2k, double* pck) {
+  if (!a) return MD_ERR_BADARG;
+  const size_t m = (size_t)a->nrc * a->nele;
+  if (s1k) MD_CUDA(cudaMemcpyAsync(s1k, a->s1k, sizeof(double) * m, cudaMemcpyDeviceToHost, a->stream));
+  if (s2k) MD_CUDA(cudaMemcpyAsync(s2k, a->s2k, sizeof(double) * 3 * m, cudaMemcpyDeviceToHost, a->stream));
+  if (pck) MD_CUDA(cudaMemcpyAsync(pck, a->pck, sizeof(double) * 3 * m, cudaMemcpyDeviceToHost, a->stream));
+  MD_CUDA(cudaStreamSynchronize(a->stream));
+  return MD_OK;
+}
+
+// AssignRCut::getRCut + assign: the device lattice the cell sort reads, and a
+// forced list rebuild at the next step.  Lattice storage is reused when the
+// size matches so a captured step keeps a valid pointer.
+extern "C" int md_arc_assign(md_adapt_rcut* a, md_system* sys) {
+  if (!a || !sys) return MD_ERR_BADARG;
+  const long ne = a->nele;
+  if (!sys->d_lattice || (long)sys->lat_n[0] * sys->lat_n[1] * sys->lat_n[2] != ne) {
+    if (sys->d_lattice) cudaFree(sys->d_lattice);
+    sys->d_lattice = nullptr;
+    MD_CUDA(cudaMalloc(&sys->d_lattice, sizeof(float) * ne));
+  }
+  for (int d = 0; d < 3; ++d) sys->lat_n[d] = a->n[d];
+  k_lattice_from_rcut<<<(int)((ne + 255) / 256), 256, 0, a->stream>>>(ne, a->rcut, sys->d_lattice, sys->st);
+  MD_CHECK_LAUNCH("lattice");
+  return MD_OK;
+}
+
+extern "C" int md_arc_pressure_correction(md_adapt_rcut* a, md_system* sys, double out[3]) {
+  if (!a || !sys) return MD_ERR_BADARG;
+  k_store_pcorr<<<1, 1, 0, a->stream>>>(a->pcorr, sys->st);
+  MD_CHECK_LAUNCH("store pcorr");
+  if (out) {
+    MD_CUDA(cudaMemcpyAsync(out, a->pcorr, sizeof(double) * 3, cudaMemcpyDeviceToHost, a->stream));
+    MD_CUDA(cudaStreamSynchronize(a->stream));
+  }
+  return MD_OK;
+}

@@ -25,10 +25,13 @@ struct LvDev {
   uint64_t seed;
 };
 
-// box B/A/O/A for one step, plus reset of the rebuild flag
-__global__ void k_lv_box(DevState* st, LvDev p) {
-  if (st->flags & FLAG_REBUILD) st->rebuilds += 1ull;
-  st->flags &= ~FLAG_REBUILD;
+// Start of a step, one thread: rebuild accounting and flag reset, step
+// counter, and the box part of B(dt/2) A(dt/2) O(dt) A(dt/2).
+__device__ void box_advance(DevState* st, const LvDev& p) {
+  const unsigned f = st->flags;
+  if (f & FLAG_REBUILD) st->rebuilds += 1ull;
+  // a forced rebuild (new cutoff lattice) becomes this step's rebuild
+  st->flags = (f & ~(FLAG_REBUILD | FLAG_FORCE_REBUILD)) | ((f & FLAG_FORCE_REBUILD) ? FLAG_REBUILD : 0u);
   st->step += 1ull;
   double xi[4];
   normals4(p.seed ^ 0x5bd1e995ull, st->step, 0xffffffffu, xi);
@@ -55,13 +58,51 @@ __global__ void k_lv_box(DevState* st, LvDev p) {
   }
 }
 
+__global__ void k_lv_box(DevState* st, LvDev p) { box_advance(st, p); }
+
+// Particle part of B(dt/2) A(dt/2) O(dt) A(dt/2) and the rebuild test.  With
+// use_cond the last block to finish writes the rebuild decision into the CUDA
+// graph conditional that guards the cell sort + list build.
+template <class R>
+__device__ __forceinline__ void lv_particle_step1(int k, typename V4<R>::T* __restrict__ pos,
+                                                  typename V4<R>::T* __restrict__ vel,
+                                                  const double4a* __restrict__ force,
+                                                  const int* __restrict__ id,
+                                                  const typename V4<R>::T* __restrict__ backup,
+                                                  DevState* st, const LvDev& p);
+
 template <class R>
 __global__ void __launch_bounds__(256)
 k_lv_step1(int N, typename V4<R>::T* __restrict__ pos, typename V4<R>::T* __restrict__ vel,
            const double4a* __restrict__ force, const int* __restrict__ id,
-           const typename V4<R>::T* __restrict__ backup, DevState* st, LvDev p) {
+           const typename V4<R>::T* __restrict__ backup, DevState* st, LvDev p,
+           cudaGraphConditionalHandle cond, int use_cond) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= N) return;
+  if (k < N) lv_particle_step1<R>(k, pos, vel, force, id, backup, st, p);
+  if (use_cond) {
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      last = atomicAdd(&st->red_counter[RED_DISP], 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+      __threadfence();
+      const unsigned f = atomicOr(&st->flags, 0u);
+      cudaGraphSetConditional(cond, (f & FLAG_REBUILD) ? 1u : 0u);
+      st->red_counter[RED_DISP] = 0u;
+    }
+  }
+}
+
+template <class R>
+__device__ __forceinline__ void lv_particle_step1(int k, typename V4<R>::T* __restrict__ pos,
+                                                  typename V4<R>::T* __restrict__ vel,
+                                                  const double4a* __restrict__ force,
+                                                  const int* __restrict__ id,
+                                                  const typename V4<R>::T* __restrict__ backup,
+                                                  DevState* st, const LvDev& p) {
   typename V4<R>::T x = pos[k], v = vel[k];
   const double4a f = force[k];
   const double im = (double)v.w;
@@ -102,17 +143,20 @@ k_lv_step1(int N, typename V4<R>::T* __restrict__ pos, typename V4<R>::T* __rest
   }
 }
 
+// Closing B(dt/2) (kick = 0: no kick, used to prime the pressure), kinetic
+// tensor; the last block computes P, gives the box momentum its half kick
+// (with_box) and, with advance, runs box_advance for the next step.
 template <class R>
 __global__ void __launch_bounds__(256)
 k_lv_step2(int N, typename V4<R>::T* __restrict__ vel, const double4a* __restrict__ force,
-           DevState* st, LvDev p, double* partials, int with_box) {
+           DevState* st, LvDev p, double* partials, int with_box, int kick, int advance) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   double kin[3] = {0, 0, 0};
   if (k < N) {
     typename V4<R>::T v = vel[k];
     const double4a f = force[k];
     const double im = (double)v.w;
-    const double h = 0.5 * p.dt;
+    const double h = kick ? 0.5 * p.dt : 0.0;
     double vx = v.x + h * f.x * im, vy = v.y + h * f.y * im, vz = v.z + h * f.z * im;
     v.x = (R)vx; v.y = (R)vy; v.z = (R)vz;
     vel[k] = v;
@@ -130,8 +174,9 @@ k_lv_step2(int N, typename V4<R>::T* __restrict__ vel, const double4a* __restric
       const double W = st->stats[MD_STAT_VIRIAL_XX + d];
       const double K = st->stats[MD_STAT_KINETIC_XX + d];
       st->Pcur[d] = 2.0 / V * (K - 0.5 * W) + st->stats[MD_STAT_PRESSURE_CORR_XX + d];
-      if (p.dirs & (1 << d)) st->ph[d] += 0.5 * p.dt * V / st->L[d] * (st->Pcur[d] - p.pref[d]);
+      if (kick && (p.dirs & (1 << d))) st->ph[d] += 0.5 * p.dt * V / st->L[d] * (st->Pcur[d] - p.pref[d]);
     }
+    if (advance) box_advance(st, p);
   }
 }
 
@@ -153,26 +198,30 @@ static LvDev make_lv(const md_system* sys, const md_nlist* nl) {
   return p;
 }
 
-int langevin_step1_impl(md_system* sys, md_nlist* nl, Recorder* rec) {
+// with_box_kernel: launch k_lv_box first (manual stepping); the driver instead
+// advances the box in the previous step's closing kick.  cond/use_cond: see
+// k_lv_step1.
+int langevin_step1_impl(md_system* sys, md_nlist* nl, Recorder* rec, bool with_box_kernel,
+                        cudaGraphConditionalHandle cond, int use_cond) {
   LvDev p = make_lv(sys, nl);
   DevState* st = sys->st;
-  {
+  if (with_box_kernel) {
     void* a[] = {&st, &p};
     if (int r = rec_launch(rec, (const void*)k_lv_box, dim3(1), dim3(1), 0, a)) return r;
   }
   int N = sys->N;
   void* bk = nl ? nl->backup : nullptr;
-  void* a[] = {&N, &sys->pos, &sys->vel, &sys->force, &sys->id, &bk, &st, &p};
+  void* a[] = {&N, &sys->pos, &sys->vel, &sys->force, &sys->id, &bk, &st, &p, &cond, &use_cond};
   const void* f = sys->prec == MD_PREC_FP64 ? (const void*)k_lv_step1<double> : (const void*)k_lv_step1<float>;
   return rec_launch(rec, f, dim3(ceil_div(N, 256)), dim3(256), 0, a);
 }
 
-int langevin_step2_impl(md_system* sys, Recorder* rec) {
+int langevin_step2_impl(md_system* sys, Recorder* rec, int kick, int advance) {
   LvDev p = make_lv(sys, nullptr);
   DevState* st = sys->st;
   int N = sys->N;
   int with_box = 1;
-  void* a[] = {&N, &sys->vel, &sys->force, &st, &p, &sys->partials, &with_box};
+  void* a[] = {&N, &sys->vel, &sys->force, &st, &p, &sys->partials, &with_box, &kick, &advance};
   const void* f = sys->prec == MD_PREC_FP64 ? (const void*)k_lv_step2<double> : (const void*)k_lv_step2<float>;
   return rec_launch(rec, f, dim3(ceil_div(N, 256)), dim3(256), 0, a);
 }
@@ -212,9 +261,9 @@ extern "C" int md_vv_step2(md_system* sys, double dt, int with_stats) {
   int nb = ceil_div(N, 256);
   (void)with_stats;
   if (sys->prec == MD_PREC_FP64)
-    k_lv_step2<double><<<nb, 256, 0, sys->stream>>>(N, (double4a*)sys->vel, sys->force, st, p, sys->partials, 0);
+    k_lv_step2<double><<<nb, 256, 0, sys->stream>>>(N, (double4a*)sys->vel, sys->force, st, p, sys->partials, 0, 1, 0);
   else
-    k_lv_step2<float><<<nb, 256, 0, sys->stream>>>(N, (float4*)sys->vel, sys->force, st, p, sys->partials, 0);
+    k_lv_step2<float><<<nb, 256, 0, sys->stream>>>(N, (float4*)sys->vel, sys->force, st, p, sys->partials, 0, 1, 0);
   MD_CHECK_LAUNCH("vv step2");
   return MD_OK;
 }
@@ -257,14 +306,14 @@ extern "C" int md_langevin_step1(md_system* sys, md_nlist* nl) {
   if (!sys || !sys->lv_set) { md_set_error("md_langevin_step1: call md_langevin_setup first"); return MD_ERR_BADARG; }
   Recorder rec;
   rec.stream = sys->stream;
-  return langevin_step1_impl(sys, nl, &rec);
+  return langevin_step1_impl(sys, nl, &rec, true, 0, 0);
 }
 
 extern "C" int md_langevin_step2(md_system* sys) {
   if (!sys || !sys->lv_set) { md_set_error("md_langevin_step2: call md_langevin_setup first"); return MD_ERR_BADARG; }
   Recorder rec;
   rec.stream = sys->stream;
-  return langevin_step2_impl(sys, &rec);
+  return langevin_step2_impl(sys, &rec, 1, 0);
 }
 
 extern "C" int md_langevin_get_state(md_system* sys, double* step, double p_h[3]) {

@@ -59,26 +59,39 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
     int n = nnb[i];
     n = n < cap ? n : cap;
     const int* row = list + (size_t)i * cap;
-    for (int k = lane; k < n; k += G) {
-      const int j = __ldg(row + k);
-      const float4 pj = __ldg(pos + j);
-      const float dx = min_image_exact(__fsub_rn(pj.x, pi.x), L0, I0);
-      const float dy = min_image_exact(__fsub_rn(pj.y, pi.y), L1, I1);
-      const float dz = min_image_exact(__fsub_rn(pj.z, pi.z), L2, I2);
-      const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-      if (r2 < rc2) {
-        const float ri2 = __fdividef(1.0f, r2);
-        const float s2 = p.sig2f * ri2;
-        const float s6 = s2 * s2 * s2;
-        const float fs = p.eps4f * (6.f * s6 - 12.f * s6 * s6) * ri2;
-        fx.add(fs * dx);
-        fy.add(fs * dy);
-        fz.add(fs * dz);
-        if (STATS) {
-          e += p.eps4f * (s6 * s6 - s6) + p.shiftf;
-          vx += fs * dx * dx;
-          vy += fs * dy * dy;
-          vz += fs * dz * dz;
+    // U list entries per lane per pass: all index loads, then all position
+    // gathers, then the arithmetic -- U independent loads in flight per lane
+    constexpr int U = 4;
+    for (int k0 = lane; k0 < n; k0 += U * G) {
+      int jj[U];
+      float4 pj[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int kk = k0 + u * G;
+        jj[u] = kk < n ? __ldg(row + kk) : -1;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) pj[u] = __ldg(pos + (jj[u] >= 0 ? jj[u] : i));
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const float dx = min_image_exact(__fsub_rn(pj[u].x, pi.x), L0, I0);
+        const float dy = min_image_exact(__fsub_rn(pj[u].y, pi.y), L1, I1);
+        const float dz = min_image_exact(__fsub_rn(pj[u].z, pi.z), L2, I2);
+        const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+        if (jj[u] >= 0 && r2 < rc2) {
+          const float ri2 = __fdividef(1.0f, r2);
+          const float s2 = p.sig2f * ri2;
+          const float s6 = s2 * s2 * s2;
+          const float fs = p.eps4f * (6.f * s6 - 12.f * s6 * s6) * ri2;
+          fx.add(fs * dx);
+          fy.add(fs * dy);
+          fz.add(fs * dz);
+          if (STATS) {
+            e += p.eps4f * (s6 * s6 - s6) + p.shiftf;
+            vx += fs * dx * dx;
+            vy += fs * dy * dy;
+            vz += fs * dz * dz;
+          }
         }
       }
     }
@@ -91,7 +104,8 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
   }
   if (STATS) {
     double v[4] = {0.5 * (double)e, 0.5 * (double)vx, 0.5 * (double)vy, 0.5 * (double)vz};
-    block_reduce_finish<4>(v, partials, counter, stats, false);
+    // the first force term of a step (overwrite) stores the slots, later terms add
+    block_reduce_finish<4>(v, partials, counter, stats, overwrite != 0);
   }
 }
 
@@ -115,14 +129,25 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
     int n = nnb[i];
     n = n < cap ? n : cap;
     const int* row = list + (size_t)i * cap;
-    for (int k = lane; k < n; k += G) {
-      const int j = __ldg(row + k);
-      const double4a pj = pos[j];
+    constexpr int U = 4;
+    for (int k0 = lane; k0 < n; k0 += U * G) {
+      int jj[U];
+      double4a pq[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int kk = k0 + u * G;
+        jj[u] = kk < n ? __ldg(row + kk) : -1;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) pq[u] = pos[jj[u] >= 0 ? jj[u] : i];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+      const double4a pj = pq[u];
       const double dx = min_image_exact(pj.x - pi.x, L0, I0);
       const double dy = min_image_exact(pj.y - pi.y, L1, I1);
       const double dz = min_image_exact(pj.z - pi.z, L2, I2);
       const double r2 = dx * dx + dy * dy + dz * dz;
-      if (r2 < rc2) {
+      if (jj[u] >= 0 && r2 < rc2) {
         const double ri2 = 1.0 / r2;
         const double s2 = p.sig2 * ri2;
         const double s6 = s2 * s2 * s2;
@@ -137,6 +162,7 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
           vz += fs * dz * dz;
         }
       }
+      }
     }
   }
   double Fx = group_sum<G>(fx), Fy = group_sum<G>(fy), Fz = group_sum<G>(fz);
@@ -147,7 +173,8 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
   }
   if (STATS) {
     double v[4] = {0.5 * e, 0.5 * vx, 0.5 * vy, 0.5 * vz};
-    block_reduce_finish<4>(v, partials, counter, stats, false);
+    // the first force term of a step (overwrite) stores the slots, later terms add
+    block_reduce_finish<4>(v, partials, counter, stats, overwrite != 0);
   }
 }
 

@@ -31,7 +31,9 @@ enum : unsigned {
   FLAG_NL_OVERFLOW = 2u,    // mdErrorShortNeighborList
   FLAG_CELL_INDEX = 4u,     // mdErrorOverFlowCellIdx
   FLAG_NAN = 8u,            // non-finite coordinate met
-  FLAG_TIMEOUT = 16u
+  FLAG_TIMEOUT = 16u,
+  FLAG_FORCE_REBUILD = 32u, // rebuild at the next step (cutoffs or box changed)
+  FLAG_QUADRATURE = 64u     // adaptive quadrature hit its depth bound
 };
 
 // reduction counters (one per kind of last-block reduction)
@@ -158,7 +160,8 @@ int rec_launch(Recorder* r, const void* func, dim3 grid, dim3 block, size_t smem
 int cells_rebuild_impl(md_cell_list* cl, md_system* sys, Recorder* rec, bool conditional);
 int nlist_build_impl(md_nlist* nl, md_system* sys, md_cell_list* cl, Recorder* rec, bool conditional);
 int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats, bool overwrite, Recorder* rec);
-int langevin_step1_impl(md_system* sys, md_nlist* nl, Recorder* rec);
-int langevin_step2_impl(md_system* sys, Recorder* rec);
+int langevin_step1_impl(md_system* sys, md_nlist* nl, Recorder* rec, bool with_box_kernel,
+                        cudaGraphConditionalHandle cond, int use_cond);
+int langevin_step2_impl(md_system* sys, Recorder* rec, int kick, int advance);
 int clear_stats_impl(md_system* sys, Recorder* rec, int first, int count);
 int set_flag_impl(md_system* sys, unsigned bits, Recorder* rec);

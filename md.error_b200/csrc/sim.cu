@@ -1,15 +1,28 @@
 // Simulation driver: the hot loop of ENG/app/lj.nhc-xtc.cu:159-274 for the
 // Langevin path, with the rebuild decision taken on the device.
-// One step = k_lv_box, k_lv_step1 (B A O A + displacement flag), the gated
-// rebuild chain (bin, scan, scatter, order, gather, copy back, list build),
-// stats clear, LJ (overwrite, +stats), k_lv_step2 (B, kinetic tensor,
-// pressure, box half kick).  The step is recorded once as a CUDA graph of
-// kernel nodes and replayed; gated kernels return at once when the device
-// flag says no rebuild is due.
+//
+// One step, recorded once as a CUDA graph of kernel nodes:
+//   k_lv_step1   particle B A O A, displacement test; its last block writes
+//                the rebuild decision into a graph conditional
+//   IF(rebuild)  bin, scan, scatter, order, gather, copy back, list build
+//   LJ           forces (overwrite) + FP64 energy / virial (store)
+//   k_lv_step2   closing B, kinetic tensor, pressure, box momentum half kick,
+//                and the box B A O A of the next step
+// Where the driver cannot create conditional nodes the rebuild kernels are
+// recorded unconditionally and return at once unless the device flag is set.
+// Density sampling and the adaptive-cutoff update run between graph launches
+// on the same stream on the reference's schedule (every 40 / 2000 steps).
 #include <cmath>
 #include <cstring>
 #include <vector>
 #include "device_common.cuh"
+
+struct md_adapt_rcut;
+extern "C" int md_arc_deposit(md_adapt_rcut* a, md_system* sys);
+extern "C" int md_arc_update(md_adapt_rcut* a, double prec, int nrefine);
+extern "C" int md_arc_assign(md_adapt_rcut* a, md_system* sys);
+extern "C" int md_arc_pressure_correction(md_adapt_rcut* a, md_system* sys, double out[3]);
+extern "C" int md_arc_clear_profile(md_adapt_rcut* a);
 
 struct md_sim {
   md_system* sys = nullptr;
@@ -19,18 +32,59 @@ struct md_sim {
   md_nlist* nl = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  bool conditional = false;
+  float* lattice_in_graph = nullptr;
   int64_t steps = 0;
+  // adaptive cutoff schedule
+  md_adapt_rcut* arc = nullptr;
+  int sample_every = 0, update_every = 0, nrefine = 0;
+  double prec = 0;
 };
 
-static int record_step(md_sim* s, Recorder* rec) {
+static int record_step(md_sim* s, Recorder* rec, bool use_graph) {
   md_system* sys = s->sys;
-  bool stats = true;
-  if (int r = langevin_step1_impl(sys, s->nl, rec)) return r;
-  if (int r = cells_rebuild_impl(s->cl, sys, rec, true)) return r;
-  if (int r = nlist_build_impl(s->nl, sys, s->cl, rec, true)) return r;
-  if (int r = clear_stats_impl(sys, rec, MD_STAT_NB_ENERGY, 4)) return r;
-  if (int r = lj_apply_impl(s->eng, sys, s->nl, stats, true, rec)) return r;
-  if (int r = langevin_step2_impl(sys, rec)) return r;
+  cudaGraphConditionalHandle h = 0;
+  bool cond = false;
+  if (use_graph && rec->graph) {
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, rec->graph, 0, 0);
+    cond = (e == cudaSuccess);
+    if (!cond) cudaGetLastError();
+  }
+  if (int r = langevin_step1_impl(sys, s->nl, rec, false, h, cond ? 1 : 0)) return r;
+  if (cond) {
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    MD_CUDA(cudaGraphAddNode(&node, rec->graph, &rec->last, 1, &cp));
+    Recorder body;
+    body.graph = cp.conditional.phGraph_out[0];
+    body.stream = rec->stream;
+    if (int r = cells_rebuild_impl(s->cl, sys, &body, false)) return r;
+    if (int r = nlist_build_impl(s->nl, sys, s->cl, &body, false)) return r;
+    rec->last = node;
+    rec->has_last = true;
+  } else {
+    if (int r = cells_rebuild_impl(s->cl, sys, rec, true)) return r;
+    if (int r = nlist_build_impl(s->nl, sys, s->cl, rec, true)) return r;
+  }
+  s->conditional = cond;
+  if (int r = lj_apply_impl(s->eng, sys, s->nl, true, true, rec)) return r;
+  if (int r = langevin_step2_impl(sys, rec, 1, 1)) return r;
+  return MD_OK;
+}
+
+static int build_graph(md_sim* s) {
+  if (s->exec) { cudaGraphExecDestroy(s->exec); s->exec = nullptr; }
+  if (s->graph) { cudaGraphDestroy(s->graph); s->graph = nullptr; }
+  MD_CUDA(cudaGraphCreate(&s->graph, 0));
+  Recorder g;
+  g.graph = s->graph;
+  g.stream = s->sys->stream;
+  if (int r = record_step(s, &g, true)) return r;
+  MD_CUDA(cudaGraphInstantiate(&s->exec, s->graph, 0));
+  s->lattice_in_graph = s->sys->d_lattice;
   return MD_OK;
 }
 
@@ -64,61 +118,85 @@ extern "C" int md_sim_create(md_sim** out, md_system* sys, md_engine* eng, const
   float rmax = 0;
   for (float v : rc) rmax = v > rmax ? v : rmax;
   if (!(rmax > 0)) { md_set_error("md_sim_create: per-atom cutoffs not set"); return fail(MD_ERR_BADARG); }
+  if (p->max_rcut > rmax) rmax = (float)p->max_rcut;
   double rlist = rmax + p->skin;
   if ((r = md_nlist_create(&s->nl, sys, rlist, p->skin, p->expansion > 0 ? p->expansion : 1.0, p->nl_mode))) return fail(r);
   if ((r = md_cell_list_rebuild(s->cl, sys))) return fail(r);
-  if ((r = md_nlist_fit(s->nl, sys, s->cl))) return fail(r);
-  // head room for the run: 25% + 32 over the largest list of the start configuration
+  // capacity: lists of every atom at the largest cutoff the run may assign,
+  // 20% + 32 head room (a list that still outgrows it raises the overflow flag)
   {
+    std::vector<float> keep(sys->N);
+    if ((r = md_system_get_rcut(sys, keep.data()))) return fail(r);
+    std::vector<float> big(sys->N, rmax);
+    if ((r = md_system_set_rcut(sys, big.data()))) return fail(r);
+    if ((r = md_nlist_fit(s->nl, sys, s->cl))) return fail(r);
     DevState hs;
     if ((r = sys->read_state(hs))) return fail(r);
-    int want = ((int)(hs.max_nnb * 1.25) + 32 + 7) & ~7;
+    if ((r = md_system_set_rcut(sys, keep.data()))) return fail(r);
+    int want = ((int)(hs.max_nnb * 1.2) + 32 + 7) & ~7;
     if (want > s->nl->cap) {
       cudaFree(s->nl->list);
       s->nl->list = nullptr;
       s->nl->cap = want;
       if (cudaMalloc(&s->nl->list, sizeof(int) * (size_t)want * sys->N) != cudaSuccess) return fail(md_cuda_fail(cudaGetLastError(), "nlist realloc"));
-      if ((r = md_nlist_rebuild(s->nl, sys, s->cl))) return fail(r);
     }
+    if ((r = md_nlist_rebuild(s->nl, sys, s->cl))) return fail(r);
   }
-  // initial forces and pressure
+  // initial forces, pressure and the box move of the first step
   Recorder rec;
   rec.stream = sys->stream;
-  if ((r = clear_stats_impl(sys, &rec, MD_STAT_NB_ENERGY, 4))) return fail(r);
   if ((r = lj_apply_impl(eng, sys, s->nl, true, true, &rec))) return fail(r);
-  {
-    md_langevin_params keep = sys->lv;
-    sys->lv.dt = 1e-300;  // kinetic tensor and pressure with no kick
-    r = langevin_step2_impl(sys, &rec);
-    sys->lv = keep;
-    if (r) return fail(r);
-  }
+  if ((r = langevin_step2_impl(sys, &rec, 0, 1))) return fail(r);
   MD_CUDA(cudaStreamSynchronize(sys->stream));
-  if (p->use_graph) {
-    if (cudaGraphCreate(&s->graph, 0) != cudaSuccess) return fail(md_cuda_fail(cudaGetLastError(), "graph create"));
-    Recorder g;
-    g.graph = s->graph;
-    g.stream = sys->stream;
-    if ((r = record_step(s, &g))) return fail(r);
-    if (cudaGraphInstantiate(&s->exec, s->graph, 0) != cudaSuccess) return fail(md_cuda_fail(cudaGetLastError(), "graph instantiate"));
-  }
+  if (p->use_graph)
+    if ((r = build_graph(s))) return fail(r);
   *out = s;
+  return MD_OK;
+}
+
+extern "C" int md_sim_attach_adapt_rcut(md_sim* s, md_adapt_rcut* arc, int sample_every, int update_every,
+                                        double prec, int nrefine) {
+  if (!s || !arc || sample_every < 1 || update_every < 1 || !(prec > 0) || nrefine < 0) {
+    md_set_error("md_sim_attach_adapt_rcut: bad arguments");
+    return MD_ERR_BADARG;
+  }
+  s->arc = arc;
+  s->sample_every = sample_every;
+  s->update_every = update_every;
+  s->prec = prec;
+  s->nrefine = nrefine;
   return MD_OK;
 }
 
 extern "C" int md_sim_run(md_sim* s, int nsteps) {
   if (!s || nsteps < 0) return MD_ERR_BADARG;
   md_system* sys = s->sys;
+  if (s->exec && sys->d_lattice != s->lattice_in_graph)
+    if (int r = build_graph(s)) return r;
   for (int i = 0; i < nsteps; ++i) {
     if (s->exec) {
       MD_CUDA(cudaGraphLaunch(s->exec, sys->stream));
     } else {
       Recorder rec;
       rec.stream = sys->stream;
-      if (int r = record_step(s, &rec)) return r;
+      if (int r = record_step(s, &rec, false)) return r;
+    }
+    s->steps += 1;
+    if (s->arc) {
+      // lj.nhc-xtc.cu:226-254: deposit every sample_every steps, new rc map and
+      // tail correction every update_every steps
+      if (s->steps % s->sample_every == 0)
+        if (int r = md_arc_deposit(s->arc, sys)) return r;
+      if (s->steps % s->update_every == 0) {
+        if (int r = md_arc_update(s->arc, s->prec, s->nrefine)) return r;
+        if (int r = md_arc_assign(s->arc, sys)) return r;
+        if (int r = md_arc_pressure_correction(s->arc, sys, nullptr)) return r;
+        if (int r = md_arc_clear_profile(s->arc)) return r;
+        if (s->exec && sys->d_lattice != s->lattice_in_graph)
+          if (int r = build_graph(s)) return r;
+      }
     }
   }
-  s->steps += nsteps;
   return MD_OK;
 }
 
@@ -127,12 +205,18 @@ extern "C" int md_sim_counters(md_sim* s, int64_t* steps, int64_t* rebuilds, int
   DevState hs;
   if (int r = s->sys->read_state(hs)) return r;
   if (steps) *steps = s->steps;
-  if (rebuilds) *rebuilds = (int64_t)hs.rebuilds + ((hs.flags & FLAG_REBUILD) ? 1 : 0);
+  if (rebuilds) *rebuilds = (int64_t)hs.rebuilds;
   if (flags) *flags = (int)hs.flags;
   if (hs.flags & FLAG_NL_OVERFLOW) {
     md_set_error("neighbour list overflow during the run (largest list %d, capacity %d)", hs.max_nnb, s->nl->cap);
     return MD_ERR_NLIST_OVERFLOW;
   }
   if (hs.flags & FLAG_NAN) { md_set_error("non-finite coordinates during the run"); return MD_ERR_BADARG; }
+  return MD_OK;
+}
+
+extern "C" int md_sim_uses_conditional_graph(md_sim* s, int* out) {
+  if (!s || !out) return MD_ERR_BADARG;
+  *out = (s->exec && s->conditional) ? 1 : 0;
   return MD_OK;
 }

@@ -37,7 +37,7 @@ class SimParams(C.Structure):
     """md_sim_params"""
     _fields_ = [("lv", LangevinParams), ("skin", f64), ("cell_size", f64),
                 ("expansion", f64), ("nl_mode", i32), ("use_graph", i32),
-                ("stats_every", i32)]
+                ("stats_every", i32), ("max_rcut", f64)]
 
 
 _SIGS = {
@@ -94,6 +94,21 @@ _SIGS = {
     "md_sim_destroy": (i32, [vp]),
     "md_sim_run": (i32, [vp, i32]),
     "md_sim_counters": (i32, [vp, P(i64), P(i64), P(i32)]),
+    "md_sim_uses_conditional_graph": (i32, [vp, P(i32)]),
+    "md_sim_attach_adapt_rcut": (i32, [vp, vp, i32, i32, f64, i32]),
+    "md_arc_create": (i32, [P(vp), vp, f64, f64, f64, f64]),
+    "md_arc_destroy": (i32, [vp]),
+    "md_arc_get_dims": (i32, [vp, P(i32), P(i32)]),
+    "md_arc_deposit": (i32, [vp, vp]),
+    "md_arc_clear_profile": (i32, [vp]),
+    "md_arc_set_profile": (i32, [vp, P(f64)]),
+    "md_arc_get_profile": (i32, [vp, P(f64)]),
+    "md_arc_update": (i32, [vp, f64, i32]),
+    "md_arc_get_error": (i32, [vp, P(f64)]),
+    "md_arc_get_rcut": (i32, [vp, P(f64), P(i32), P(f64)]),
+    "md_arc_get_tables": (i32, [vp, P(f64), P(f64), P(f64)]),
+    "md_arc_assign": (i32, [vp, vp]),
+    "md_arc_pressure_correction": (i32, [vp, vp, P(f64)]),
     "md_synth_fcc": (i32, [i32, i32, i32, P(f64), f64, u64, P(f64)]),
     "md_synth_slab": (i32, [i32, i32, P(f64), i32, f64, f64, f64, u64, P(f64)]),
     "md_synth_maxwell": (i32, [i32, P(f64), f64, u64, P(f64)]),

@@ -354,11 +354,80 @@ class Langevin:
         check(lib.md_langevin_step2(self.sys.h), "Langevin::step2")
 
 
+class AdaptRCutEstimator:
+    """AdaptRCut + DensityProfile_PiecewiseConst + PressureCorrection on the GPU
+    (ENG/src/AdaptRCut.cu, ENG/src/DensityProfile.cu, ENG/src/PressureCorrection.cu)."""
+
+    def __init__(self, sys, refh=1.0, rcmin=2.5, rcmax=5.0, rcstep=0.5):
+        h = C.c_void_p()
+        check(lib.md_arc_create(C.byref(h), sys.h, refh, rcmin, rcmax, rcstep), "AdaptRCut")
+        self.h = h
+        self.sys = sys
+        n = (C.c_int * 3)()
+        nrc = C.c_int()
+        check(lib.md_arc_get_dims(h, n, C.byref(nrc)), "dims")
+        self.n = tuple(n)
+        self.nrc = nrc.value
+        self.nele = self.n[0] * self.n[1] * self.n[2]
+        self.rc_list = np.array([rcmin + i * rcstep for i in range(self.nrc)])
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.md_arc_destroy(self.h)
+            self.h = None
+
+    def deposite(self, sys=None):
+        check(lib.md_arc_deposit(self.h, (sys or self.sys).h), "deposite")
+
+    def clearData(self):
+        check(lib.md_arc_clear_profile(self.h), "clearData")
+
+    def set_profile(self, rho):
+        a = _f64(rho).reshape(self.n)
+        check(lib.md_arc_set_profile(self.h, _p(a)), "set_profile")
+
+    def profile(self):
+        a = np.empty(self.n, np.float64)
+        check(lib.md_arc_get_profile(self.h, _p(a)), "profile")
+        return a
+
+    def update(self, prec, nrefine=0):
+        """calError + calRCut(prec) + refineRCut x nrefine + PressureCorrection."""
+        check(lib.md_arc_update(self.h, float(prec), int(nrefine)), "AdaptRCut::update")
+
+    def error(self):
+        a = np.empty((self.nrc,) + self.n, np.float64)
+        check(lib.md_arc_get_error(self.h, _p(a)), "error")
+        return a
+
+    def rcut(self):
+        rc = np.empty(self.n, np.float64)
+        idx = np.empty(self.n, np.int32)
+        err = np.empty(self.n, np.float64)
+        check(lib.md_arc_get_rcut(self.h, _p(rc), _p(idx, C.c_int), _p(err)), "rcut")
+        return rc, idx, err
+
+    def tables(self):
+        s1 = np.empty((self.nrc,) + self.n)
+        s2 = np.empty((3, self.nrc) + self.n)
+        pc = np.empty((3, self.nrc) + self.n)
+        check(lib.md_arc_get_tables(self.h, _p(s1), _p(s2), _p(pc)), "tables")
+        return s1, s2, pc
+
+    def assign(self, sys=None):
+        check(lib.md_arc_assign(self.h, (sys or self.sys).h), "AssignRCut::assign")
+
+    def pressure_correction(self, sys=None):
+        out = np.zeros(3)
+        check(lib.md_arc_pressure_correction(self.h, (sys or self.sys).h, _p(out)), "pressure_correction")
+        return out
+
+
 class Simulation:
     """Graph-captured Langevin MD driver (the hot loop of ENG/app/lj.nhc-xtc.cu)."""
 
     def __init__(self, sys, engine, skin, cell_size, lv, nl_mode=NL_MINIMAGE, expansion=1.5,
-                 use_graph=True):
+                 use_graph=True, max_rcut=0.0):
         p = SimParams()
         p.lv = lv
         p.skin = skin
@@ -367,6 +436,7 @@ class Simulation:
         p.nl_mode = nl_mode
         p.use_graph = 1 if use_graph else 0
         p.stats_every = 1
+        p.max_rcut = max_rcut
         self.params = p
         h = C.c_void_p()
         check(lib.md_sim_create(C.byref(h), sys.h, engine.h, C.byref(p)), "Simulation")
@@ -386,3 +456,14 @@ class Simulation:
         s, r, f = C.c_int64(), C.c_int64(), C.c_int()
         check(lib.md_sim_counters(self.h, C.byref(s), C.byref(r), C.byref(f)), "counters")
         return s.value, r.value, f.value
+
+    def uses_conditional_graph(self):
+        v = C.c_int()
+        check(lib.md_sim_uses_conditional_graph(self.h, C.byref(v)), "conditional")
+        return bool(v.value)
+
+    def attach_adapt_rcut(self, arc, sample_every=40, update_every=2000, prec=0.02, nrefine=0):
+        """rcutAssignFeq / densityProfileSamplingFeq / rcutUpdateFeq of lj.nhc-xtc.cu."""
+        check(lib.md_sim_attach_adapt_rcut(self.h, arc.h, sample_every, update_every, prec, nrefine),
+              "attach_adapt_rcut")
+        self.arc = arc

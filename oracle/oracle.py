@@ -209,3 +209,149 @@ def philox4x32_10(ctr, key):
     out = np.empty(4, np.uint32)
     _lib.orc_philox4x32_10(_p(c, u32), _p(k, u32), _p(out, u32))
     return out
+
+
+# ---------------------------------------------------------------- AdaptRCut
+_lib2 = _lib
+_sigs2 = {
+    "orc_dp_bins": (None, [P(f64), f64, P(i32)]),
+    "orc_dp_deposit": (None, [i32, P(f32), P(f64), P(i32), P(f64)]),
+    "orc_dp_calculate": (None, [P(f64), P(i32), i32, P(f64)]),
+    "orc_dft3d": (None, [P(i32), P(f64), i32]),
+    "orc_gauss4": (f64, [i32, f64, f64, f64, f64]),
+    "orc_arc_kernels": (None, [P(f64), P(i32), P(f64), i32, f64, f64, P(f64), P(f64), P(f64), P(f64)]),
+    "orc_arc_error": (None, [P(f64), P(i32), i32, P(f64), P(f64), P(f64), P(f64), P(f64), P(f64)]),
+    "orc_arc_calrcut": (None, [i32, P(f64), C.c_long, P(f64), f64, P(f64), P(i32), P(f64)]),
+    "orc_arc_refine": (None, [P(i32), P(f64), C.c_long, P(f64), P(i32), P(f64), P(f64)]),
+    "orc_pc_kernels": (None, [P(f64), P(i32), P(f64), i32, P(f64), P(f64), P(f64)]),
+    "orc_pc_correction": (None, [P(f64), P(i32), i32, P(f64), P(f64), P(f64), P(f64), P(i32), P(f64)]),
+}
+for _n, (_r, _a) in _sigs2.items():
+    _f = getattr(_lib2, _n)
+    _f.restype = _r
+    _f.argtypes = _a
+
+
+def dp_bins(box, refh):
+    b = np.ascontiguousarray(box, np.float64)
+    n = np.empty(3, np.int32)
+    _lib.orc_dp_bins(_p(b, f64), float(refh), _p(n, i32))
+    return tuple(int(x) for x in n)
+
+
+def dp_deposit(coord, box, n, profile=None):
+    c = np.ascontiguousarray(coord, np.float32)
+    b = np.ascontiguousarray(box, np.float64)
+    nn = np.ascontiguousarray(n, np.int32)
+    prof = np.zeros(tuple(n), np.float64) if profile is None else profile
+    _lib.orc_dp_deposit(c.shape[0], _p(c, f32), _p(b, f64), _p(nn, i32), _p(prof, f64))
+    return prof
+
+
+def dft3d(data, sign):
+    """in-place unnormalised 3D DFT of a complex128 array"""
+    d = np.ascontiguousarray(data, np.complex128).copy()
+    n = np.array(d.shape, np.int32)
+    _lib.orc_dft3d(_p(n, i32), d.ctypes.data_as(P(f64)), int(sign))
+    return d
+
+
+def gauss4(kind, k, xlo, xup, tol):
+    return _lib.orc_gauss4(kind, k, xlo, xup, tol)
+
+
+def arc_kernels(box, n, rc, eps=1.0, sigma=1.0):
+    b = np.ascontiguousarray(box, np.float64)
+    nn = np.ascontiguousarray(n, np.int32)
+    rcl = np.ascontiguousarray(rc, np.float64)
+    nrc = len(rcl)
+    shp = (nrc,) + tuple(n)
+    s1, sx, sy, sz = (np.zeros(shp) for _ in range(4))
+    _lib.orc_arc_kernels(_p(b, f64), _p(nn, i32), _p(rcl, f64), nrc, eps, sigma, _p(s1, f64), _p(sx, f64),
+                         _p(sy, f64), _p(sz, f64))
+    return s1, np.stack([sx, sy, sz])
+
+
+def pc_kernels(box, n, rc):
+    b = np.ascontiguousarray(box, np.float64)
+    nn = np.ascontiguousarray(n, np.int32)
+    rcl = np.ascontiguousarray(rc, np.float64)
+    nrc = len(rcl)
+    shp = (nrc,) + tuple(n)
+    kx, ky, kz = (np.zeros(shp) for _ in range(3))
+    _lib.orc_pc_kernels(_p(b, f64), _p(nn, i32), _p(rcl, f64), nrc, _p(kx, f64), _p(ky, f64), _p(kz, f64))
+    return np.stack([kx, ky, kz])
+
+
+def adapt_rcut(box, n, rc, rho, prec, nrefine=0, with_pc=True):
+    """AdaptRCut::calError + calRCut + refineRCut (+ PressureCorrection) on profile rho."""
+    b = np.ascontiguousarray(box, np.float64)
+    nn = np.ascontiguousarray(n, np.int32)
+    rcl = np.ascontiguousarray(rc, np.float64)
+    nrc = len(rcl)
+    s1, s2 = arc_kernels(box, n, rc)
+    s1 = np.ascontiguousarray(s1)
+    sx, sy, sz = (np.ascontiguousarray(s2[d]) for d in range(3))
+    r = np.ascontiguousarray(rho, np.float64).reshape(n)
+    err = np.zeros((nrc,) + tuple(n))
+    _lib.orc_arc_error(_p(b, f64), _p(nn, i32), nrc, _p(s1, f64), _p(sx, f64), _p(sy, f64), _p(sz, f64),
+                       _p(r, f64), _p(err, f64))
+    nele = int(np.prod(n))
+    rcut = np.zeros(tuple(n)); idx = np.zeros(tuple(n), np.int32); rerr = np.zeros(tuple(n))
+    _lib.orc_arc_calrcut(nrc, _p(rcl, f64), nele, _p(err, f64), float(prec), _p(rcut, f64), _p(idx, i32),
+                         _p(rerr, f64))
+    for _ in range(nrefine):
+        _lib.orc_arc_refine(_p(nn, i32), _p(rcl, f64), nele, _p(err, f64), _p(idx, i32), _p(rcut, f64),
+                            _p(rerr, f64))
+    out = dict(error=err, rcut=rcut, index=idx, result_error=rerr, s1k=s1, s2k=s2)
+    if with_pc:
+        K = pc_kernels(box, n, rc)
+        kx, ky, kz = (np.ascontiguousarray(K[d]) for d in range(3))
+        p = np.zeros(3)
+        _lib.orc_pc_correction(_p(b, f64), _p(nn, i32), nrc, _p(kx, f64), _p(ky, f64), _p(kz, f64), _p(r, f64),
+                               _p(idx, i32), _p(p, f64))
+        out["pcorr"] = p
+        out["pck"] = K
+    return out
+
+
+# ---------------------------------------------------------------- reference (compiled from its sources)
+REF_DIR = os.path.join(HERE, "_ref")
+
+
+def ref_available(name):
+    return os.path.exists(os.path.join(REF_DIR, name))
+
+
+def ref_adapt_rcut(box, n, rcmin, rcmax, rcstep, rho, prec, nrefine=0):
+    """The reference's own AdaptRCut + PressureCorrection (oracle/_ref/libref_arc.so)."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libref_arc.so"))
+    lib.ref_arc_run.argtypes = [P(f64), P(i32), f64, f64, f64, P(f64), f64, i32, P(f64), P(f64), P(i32),
+                                P(f64), P(f64)]
+    b = np.ascontiguousarray(box, np.float64)
+    nn = np.ascontiguousarray(n, np.int32)
+    r = np.ascontiguousarray(rho, np.float64).reshape(n)
+    nrc = len(np.arange(rcmin, rcmax + 1e-12, rcstep))
+    err = np.zeros((nrc,) + tuple(n)); rcut = np.zeros(tuple(n)); idx = np.zeros(tuple(n), np.int32)
+    rerr = np.zeros(tuple(n)); pc = np.zeros(3)
+    lib.ref_arc_run(_p(b, f64), _p(nn, i32), rcmin, rcmax, rcstep, _p(r, f64), prec, nrefine, _p(err, f64),
+                    _p(rcut, f64), _p(idx, i32), _p(rerr, f64), _p(pc, f64))
+    return dict(error=err, rcut=rcut, index=idx, result_error=rerr, pcorr=pc)
+
+
+def ref_spme(pos, q, box, beta, K, rcut, method, order):
+    """The reference's own ElectrostaticInteraction (oracle/_ref/libref_spme.so):
+    method 0 ik B-spline SPME, 1 analytic-differentiation SPME, 2 exact Ewald."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libref_spme.so"))
+    lib.ref_spme_forces.argtypes = [i32, P(f64), P(f64), P(f64), f64, P(i32), f64, i32, i32, P(f64), P(f64),
+                                    P(f64), P(f64), P(f64), P(f64)]
+    p = np.ascontiguousarray(pos, np.float64)
+    n = p.shape[0]
+    qq = np.ascontiguousarray(q, np.float64)
+    b = np.ascontiguousarray(box, np.float64)
+    KK = np.ascontiguousarray(K, np.int32)
+    df = np.zeros((n, 3)); rf = np.zeros((n, 3))
+    e, ed, er, ei = f64(), f64(), f64(), f64()
+    lib.ref_spme_forces(n, _p(p, f64), _p(qq, f64), _p(b, f64), beta, _p(KK, i32), rcut, method, order,
+                        _p(df, f64), _p(rf, f64), C.byref(e), C.byref(ed), C.byref(er), C.byref(ei))
+    return dict(dir=df, rec=rf, energy=e.value, err_dir=ed.value, err_rec=er.value, err_interp=ei.value)

@@ -1,0 +1,97 @@
+// ORACLE build (test infrastructure only): extern "C" entry points that drive
+// the md.error reference sources compiled where they lie under the reference
+// tree (see oracle/ref/Makefile), so tests can compare our restatement with
+// the reference's own code on the same inputs.
+//   ref_spme_*: longRange.hetero/profile.test/template/tools/real.error
+//               ElectrostaticInteraction (EleRecBSpline / EleRecFBSpline / EleRecES / EleDir)
+//   ref_arc_*:  shortRange.inhomo/template/tools/simulation.hetero.cutoff
+//               AdaptRCut + PressureCorrection (host code)
+#include <cstring>
+#include <iostream>
+#include <sstream>
+#include <vector>
+
+#ifdef REF_SPME
+#include "ElectrostaticInteraction.h"
+#include "BoxGeometry.h"
+#include "Particle.h"
+
+extern "C" int ref_spme_forces(int n, const double* pos, const double* q, const double* box,
+                               double beta, const int* K, double rcut, int method, int order,
+                               double* dir_force, double* rec_force, double* energy,
+                               double* err_dir, double* err_rec, double* err_interp) {
+  TimeConstRectangularBoxGeometry bx(box[0], box[1], box[2]);
+  std::vector<StandardParticle> parts(n);
+  for (int i = 0; i < n; ++i) {
+    StandardParticle& p = parts[i];
+    for (int d = 0; d < 3; ++d) { p.r()[d] = pos[3 * i + d]; p.v()[d] = 0.; }
+    p.mass() = 1.;
+    p.id() = i;
+    p.type() = 0;
+    p.charge() = q[i];
+    bx.moveParticleToBox(p);
+  }
+  std::vector<unsigned> KK(3);
+  for (int d = 0; d < 3; ++d) KK[d] = (unsigned)K[d];
+  InterpolationInfo::Method m = method == 0 ? InterpolationInfo::BSpline
+                                : (method == 1 ? InterpolationInfo::FBSpline : InterpolationInfo::ES);
+  ElectrostaticInteraction ele;
+  ele.init(beta, KK, rcut, bx, m, (InterpolationInfo::Order)order);
+  for (int i = 0; i < n; ++i) ele.registerParticle(parts[i]);
+  ele.build();
+  std::vector<double> zero3(3, 0.);
+  std::vector<std::vector<double> > df(n, zero3), rf(n, zero3);
+  // the exact Ewald sum prints a progress line per k-vector: silence std::cout
+  std::ostringstream sink;
+  std::streambuf* keep = std::cout.rdbuf(sink.rdbuf());
+  double e = ele.applyInteractionCalPotential(df, rf);
+  std::cout.rdbuf(keep);
+  for (int i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) { dir_force[3 * i + d] = df[i][d]; rec_force[3 * i + d] = rf[i][d]; }
+  *energy = e;
+  if (err_dir && err_rec) ele.errorEstimatePME(*err_dir, *err_rec);
+  if (err_interp && method == 0) ele.errorEstimateInterpolRec(*err_interp);
+  return 0;
+}
+#endif
+
+#ifdef REF_ARC
+#include "AdaptRCut.h"
+#include "PressureCorrection.h"
+
+// AdaptRCut on a given density profile: error[nrc*nele], rcut[nele], rcidx[nele]
+extern "C" int ref_arc_run(const double* box, const int* nbin, double rcmin, double rcmax,
+                           double rcstep, const double* profile, double prec, int nrefine,
+                           double* error_out, double* rcut_out, int* rcidx_out,
+                           double* rerr_out, double* pcorr_out) {
+  DensityProfile_PiecewiseConst dp;
+  dp.set(box, nbin, profile);
+  AdaptRCut arc;
+  arc.reinit(rcmin, rcmax, rcstep, dp);
+  arc.calError(dp);
+  arc.calRCut(prec);
+  for (int i = 0; i < nrefine; ++i) arc.refineRCut();
+  const int nele = nbin[0] * nbin[1] * nbin[2];
+  int nrc = (int)arc.getRcList().size();
+  // error / result_error are private members; this translation unit is built
+  // with -Dprivate=public so the harness can read them
+  if (error_out)
+    for (int c = 0; c < nrc; ++c)
+      for (int i = 0; i < nele; ++i) error_out[(size_t)c * nele + i] = arc.error[c][i][0];
+  for (int i = 0; i < nele; ++i) {
+    rcut_out[i] = arc.getRCut()[i];
+    rcidx_out[i] = arc.getProfileIndex()[i];
+  }
+  if (rerr_out)
+    for (int i = 0; i < nele; ++i) rerr_out[i] = arc.result_error[i];
+  if (pcorr_out) {
+    PressureCorrection pc(arc, dp);
+    pc.correction(arc, dp);
+    pcorr_out[0] = pc.pxx;
+    pcorr_out[1] = pc.pyy;
+    pcorr_out[2] = pc.pzz;
+  }
+  (void)nrc;
+  return 0;
+}
+#endif
