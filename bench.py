@@ -117,19 +117,15 @@ def build_slab(mdf):
     return s
 
 
-def rc_lattice(mdf, s):
-    """Adaptive rc lattice from the AdaptRCut estimate when available."""
-    est = getattr(mdf, "adapt_rcut_lattice", None)
-    if est is None:
-        return None, "uniform 2.5 (adaptive estimate not built)"
-    lat, info = est(s)
-    return lat, info
+RC_MIN, RC_MAX, RC_STEP = 2.5, 5.0, 0.5
+TARGET_PREC = 0.02      # targetPrec of ENG/app/lj.nhc-xtc.cu:57
+SAMPLE_EVERY, UPDATE_EVERY = 40, 2000  # densityProfileSamplingFeq, rcutUpdateFeq (:49-51)
 
 
-def make_sim(mdf, s, prec, lattice, seed=1, npt=True, gamma=1.0):
+def make_sim(mdf, s, prec, lattice, seed=1, npt=True, gamma=1.0, adaptive=True):
     sys_ = mdf.MDSystem(s.pos, s.box, vel=s.vel, precision=prec)
     if lattice is None:
-        sys_.set_rcut(np.full(s.n, 2.5, np.float32))
+        sys_.set_rcut(np.full(s.n, RC_MIN, np.float32))
     else:
         mdf.AssignRCut(lattice).assign(sys_)
     eng = mdf.InteractionEngine(sys_)
@@ -137,23 +133,39 @@ def make_sim(mdf, s, prec, lattice, seed=1, npt=True, gamma=1.0):
     lv = mdf.langevin_params(dt=DT, temperature=TEMP, gamma_t=gamma, tau_p=2.0 if npt else 0.0,
                              kappa_t=0.1 if npt else 0.0, p_ref=(0.0, 0.0, 0.0),
                              npt_dirs=4 if npt else 0, seed=seed)
-    sim = mdf.Simulation(sys_, eng, skin=SKIN, cell_size=2.8, lv=lv, expansion=1.5, use_graph=True)
+    sim = mdf.Simulation(sys_, eng, skin=SKIN, cell_size=2.8, lv=lv, expansion=1.5, use_graph=True,
+                         max_rcut=RC_MAX)
+    if adaptive:
+        arc = mdf.AdaptRCutEstimator(sys_, refh=1.0, rcmin=RC_MIN, rcmax=RC_MAX, rcstep=RC_STEP)
+        sim.attach_adapt_rcut(arc, sample_every=SAMPLE_EVERY, update_every=UPDATE_EVERY, prec=TARGET_PREC)
     return sys_, eng, sim
 
 
 def equilibrate(mdf, s, nsteps):
     """Relax the random-sequential-addition start (0.8 sigma contacts) by
-    Langevin NVT at T*; returns a copy of s with the relaxed positions and
-    velocities.  Not timed."""
-    if nsteps <= 0:
-        return s
-    sys_, eng, sim = make_sim(mdf, s, 0, None, seed=12345, npt=False, gamma=2.0)
-    sim.run(nsteps)
+    Langevin NVT at T*, sampling the density profile every 40 steps; at the end
+    the adaptive-cutoff estimate (AdaptRCut, target 0.02, rc 2.5..5.0) of the
+    sampled profile gives the per-bin cutoff lattice.  Not timed."""
+    sys_, eng, sim = make_sim(mdf, s, 0, None, seed=12345, npt=False, gamma=2.0, adaptive=False)
+    arc = mdf.AdaptRCutEstimator(sys_, refh=1.0, rcmin=RC_MIN, rcmax=RC_MAX, rcstep=RC_STEP)
+    done = 0
+    while done < max(nsteps, SAMPLE_EVERY):
+        sim.run(SAMPLE_EVERY)
+        done += SAMPLE_EVERY
+        if done > nsteps // 2:
+            arc.deposite()
+    arc.update(TARGET_PREC)
+    rc, idx, err = arc.rcut()
+    lattice = rc.astype(np.float32)
     sys_.synchronize()
     out = mdf.systems.SyntheticSystem(s.name, sys_.positions(), sys_.box(), sys_.velocities(),
-                                      s.charge, dict(s.meta, equilibrated_steps=nsteps))
-    del sim, eng, sys_
-    return out
+                                      s.charge, dict(s.meta, equilibrated_steps=done))
+    counts = {float(v): int((rc == v).sum()) for v in np.unique(rc)}
+    info = (f"adaptive per-bin lattice {arc.n} from AdaptRCut at target {TARGET_PREC}, "
+            f"rc {RC_MIN}..{RC_MAX} step {RC_STEP}; bins per rc {counts}; "
+            f"re-estimated every {UPDATE_EVERY} steps from samples every {SAMPLE_EVERY}")
+    del sim, eng, sys_, arc
+    return out, lattice, info
 
 
 def time_steps(torch, sim, stream, steps, flush):
@@ -235,8 +247,9 @@ def run_reference(args):
     if rank != 0:
         return 0
     import mdforce as mdf
-    s = build_slab(mdf)
-    lattice, rcinfo = rc_lattice(mdf, s)
+    # the same seeded start, relaxation and cutoff lattice as the GPU arm; the
+    # preparation is not timed (it runs on the device when one is present)
+    s, lattice, rcinfo = equilibrate(mdf, build_slab(mdf), args.equil)
     from oracle import oracle as orc
     # bounded sample: estimate one step, cap the whole run at ~150 s
     sps0, cores, _ = cpu_baseline(s, lattice, 3)
@@ -273,8 +286,7 @@ def main():
     torch.cuda.set_device(local)
     import mdforce as mdf
 
-    s = equilibrate(mdf, build_slab(mdf), args.equil)
-    lattice, rcinfo = rc_lattice(mdf, s)
+    s, lattice, rcinfo = equilibrate(mdf, build_slab(mdf), args.equil)
     stream = torch.cuda.Stream()
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
@@ -286,9 +298,11 @@ def main():
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
+    _, rebuilds0, _ = sim_m.counters()
     with Clocks(local) as clk:
         t_mixed = time_steps(torch, sim_m, stream, args.steps, flush)
     steps_done, rebuilds, flags = sim_m.counters()
+    rebuilds_timed = rebuilds - rebuilds0
     t_max = t_mixed
     if world > 1:
         tt = torch.tensor([t_mixed], device="cuda", dtype=torch.float64)
@@ -354,7 +368,11 @@ def main():
     h2d = (pin_pos.numel() + pin_vel.numel()) * 8 / e2e_steps
     d2h = 16 * 8 + (fin_pos.size + fin_f.size) * 8 / e2e_steps
 
-    kernels_per_step = 12  # box, step1, bin, scan, scatter, order, gather, copyback, list, clear, lj, step2
+    # step1, LJ, step2 every step; bin, scan, scatter, order, gather, copy back,
+    # list build per rebuild; the density deposit every 40 steps; 3 + 3*3 DFT
+    # passes + 7 element-wise kernels per cutoff update (every 2000 steps)
+    n_updates = (args.warmup + args.steps) // UPDATE_EVERY - args.warmup // UPDATE_EVERY
+    launches = (3 * args.steps + 7 * rebuilds_timed + args.steps // SAMPLE_EVERY + 22 * n_updates)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         n_cpu = 30
@@ -383,7 +401,8 @@ def main():
                          "kernel_us": t_lj * 1e6, "alg_bytes": alg_bytes, "peak_kind": peak_kind},
             "e2e": {"value": e2e_sps, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "gpu_launches": kernels_per_step * args.steps,
+            "gpu_launches": launches,
+            "list_rebuilds_timed": rebuilds_timed,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }

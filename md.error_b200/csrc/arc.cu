@@ -236,7 +236,7 @@ static int dft3(md_adapt_rcut* a, double2* data, int sign, int batch) {
   for (int axis = 2; axis >= 0; --axis) {
     long lines = (long)g.n[(axis + 1) % 3] * g.n[(axis + 2) % 3] * batch;
     size_t smem = sizeof(double2) * 2 * g.n[axis];
-    k_dft_axis<<<(unsigned)lines, 128, smem, a->stream>>>(data, g, axis, sign, batch);
+    k_dft_axis<<<(unsigned)lines, 128, smem, a->sys->stream>>>(data, g, axis, sign, batch);
     MD_CHECK_LAUNCH("dft axis");
   }
   return MD_OK;
@@ -374,7 +374,7 @@ static int build_tables(md_adapt_rcut* a) {
   for (int d = 0; d < 3; ++d) { g.n[d] = a->n[d]; g.box[d] = hs.L[d]; a->box_tab[d] = hs.L[d]; }
   g.nrc = a->nrc;
   int oct = (g.n[0] / 2 + 1) * (g.n[1] / 2 + 1) * (g.n[2] / 2 + 1);
-  k_arc_tables<<<ceil_div(oct, 64), 64, 0, a->stream>>>(g, a->d_rc, a->s1k, a->s2k, a->pck, &a->sys->st->flags);
+  k_arc_tables<<<ceil_div(oct, 64), 64, 0, a->sys->stream>>>(g, a->d_rc, a->s1k, a->s2k, a->pck, &a->sys->st->flags);
   MD_CHECK_LAUNCH("arc tables");
   return MD_OK;
 }
@@ -389,7 +389,7 @@ extern "C" int md_arc_create(md_adapt_rcut** out, md_system* sys, double refh, d
   if (int r = sys->read_state(hs)) return r;
   md_adapt_rcut* a = new md_adapt_rcut();
   a->sys = sys;
-  a->stream = sys->stream;
+  a->sys->stream = sys->stream;
   for (int d = 0; d < 3; ++d) {  // DensityProfile_PiecewiseConst::reinit: odd bin counts
     unsigned v = (unsigned)(hs.L[d] / refh);
     if ((v - (v / 2) * 2) == 0) v++;
@@ -425,9 +425,9 @@ extern "C" int md_arc_create(md_adapt_rcut** out, md_system* sys, double refh, d
     md_arc_destroy(a);
     return MD_ERR_CUDA;
   }
-  cudaMemcpyAsync(a->d_rc, a->rc.data(), sizeof(double) * nrc, cudaMemcpyHostToDevice, a->stream);
-  cudaMemsetAsync(a->counts, 0, sizeof(double) * ne, a->stream);
-  cudaMemsetAsync(a->rho, 0, sizeof(double) * ne, a->stream);
+  cudaMemcpyAsync(a->d_rc, a->rc.data(), sizeof(double) * nrc, cudaMemcpyHostToDevice, a->sys->stream);
+  cudaMemsetAsync(a->counts, 0, sizeof(double) * ne, a->sys->stream);
+  cudaMemsetAsync(a->rho, 0, sizeof(double) * ne, a->sys->stream);
   if (int r = build_tables(a)) { md_arc_destroy(a); return r; }
   *out = a;
   return MD_OK;
@@ -455,9 +455,9 @@ extern "C" int md_arc_deposit(md_adapt_rcut* a, md_system* sys) {
   for (int d = 0; d < 3; ++d) g.n[d] = a->n[d];
   int nb = ceil_div(sys->N, 256);
   if (sys->prec == MD_PREC_FP64)
-    k_arc_deposit<double><<<nb, 256, 0, a->stream>>>(sys->N, (double4a*)sys->pos, sys->st, g, a->counts);
+    k_arc_deposit<double><<<nb, 256, 0, a->sys->stream>>>(sys->N, (double4a*)sys->pos, sys->st, g, a->counts);
   else
-    k_arc_deposit<float><<<nb, 256, 0, a->stream>>>(sys->N, (float4*)sys->pos, sys->st, g, a->counts);
+    k_arc_deposit<float><<<nb, 256, 0, a->sys->stream>>>(sys->N, (float4*)sys->pos, sys->st, g, a->counts);
   MD_CHECK_LAUNCH("arc deposit");
   a->ndata++;
   return MD_OK;
@@ -465,23 +465,23 @@ extern "C" int md_arc_deposit(md_adapt_rcut* a, md_system* sys) {
 
 extern "C" int md_arc_clear_profile(md_adapt_rcut* a) {
   if (!a) return MD_ERR_BADARG;
-  MD_CUDA(cudaMemsetAsync(a->counts, 0, sizeof(double) * a->nele, a->stream));
+  MD_CUDA(cudaMemsetAsync(a->counts, 0, sizeof(double) * a->nele, a->sys->stream));
   a->ndata = 0;
   return MD_OK;
 }
 
 extern "C" int md_arc_set_profile(md_adapt_rcut* a, const double* rho) {
   if (!a || !rho) return MD_ERR_BADARG;
-  MD_CUDA(cudaMemcpyAsync(a->rho, rho, sizeof(double) * a->nele, cudaMemcpyHostToDevice, a->stream));
-  MD_CUDA(cudaStreamSynchronize(a->stream));
+  MD_CUDA(cudaMemcpyAsync(a->rho, rho, sizeof(double) * a->nele, cudaMemcpyHostToDevice, a->sys->stream));
+  MD_CUDA(cudaStreamSynchronize(a->sys->stream));
   a->ndata = -1;  // explicit profile: do not renormalise counts
   return MD_OK;
 }
 
 extern "C" int md_arc_get_profile(md_adapt_rcut* a, double* rho) {
   if (!a || !rho) return MD_ERR_BADARG;
-  MD_CUDA(cudaMemcpyAsync(rho, a->rho, sizeof(double) * a->nele, cudaMemcpyDeviceToHost, a->stream));
-  MD_CUDA(cudaStreamSynchronize(a->stream));
+  MD_CUDA(cudaMemcpyAsync(rho, a->rho, sizeof(double) * a->nele, cudaMemcpyDeviceToHost, a->sys->stream));
+  MD_CUDA(cudaStreamSynchronize(a->sys->stream));
   return MD_OK;
 }
 
@@ -499,9 +499,9 @@ extern "C" int md_arc_update(md_adapt_rcut* a, double prec, int nrefine) {
   // DensityProfile::calculate: counts / (dv * ndata), or the explicit profile
   if (a->ndata > 0) {
     double dv = (hs.L[0] / a->n[0]) * (hs.L[1] / a->n[1]) * (hs.L[2] / a->n[2]);
-    k_arc_profile<<<nb, 256, 0, a->stream>>>(ne, a->counts, 1.0 / (dv * a->ndata), a->rho, a->rhok);
+    k_arc_profile<<<nb, 256, 0, a->sys->stream>>>(ne, a->counts, 1.0 / (dv * a->ndata), a->rho, a->rhok);
   } else if (a->ndata < 0) {
-    k_arc_profile<<<nb, 256, 0, a->stream>>>(ne, nullptr, 0.0, a->rho, a->rhok);
+    k_arc_profile<<<nb, 256, 0, a->sys->stream>>>(ne, nullptr, 0.0, a->rho, a->rhok);
   } else {
     md_set_error("md_arc_update: no density samples deposited");
     return MD_ERR_BADARG;
@@ -509,26 +509,26 @@ extern "C" int md_arc_update(md_adapt_rcut* a, double prec, int nrefine) {
   MD_CHECK_LAUNCH("arc profile");
   if (int r = dft3(a, a->rhok, -1, 1)) return r;
   const double V = hs.L[0] * hs.L[1] * hs.L[2];
-  k_arc_multiply<<<nb, 256, 0, a->stream>>>(ne, a->nrc, a->rhok, V / ne, a->s1k, a->s2k, a->work);
+  k_arc_multiply<<<nb, 256, 0, a->sys->stream>>>(ne, a->nrc, a->rhok, V / ne, a->s1k, a->s2k, a->work);
   MD_CHECK_LAUNCH("arc multiply");
   if (int r = dft3(a, a->work, +1, 4 * a->nrc)) return r;
-  k_arc_error<<<nb, 256, 0, a->stream>>>(ne, a->nrc, a->work, 1.0 / V, a->error);
-  k_arc_rcut<<<nb, 256, 0, a->stream>>>(ne, a->nrc, a->d_rc, a->error, prec, a->rcut, a->rcidx, a->rerr);
+  k_arc_error<<<nb, 256, 0, a->sys->stream>>>(ne, a->nrc, a->work, 1.0 / V, a->error);
+  k_arc_rcut<<<nb, 256, 0, a->sys->stream>>>(ne, a->nrc, a->d_rc, a->error, prec, a->rcut, a->rcidx, a->rerr);
   MD_CHECK_LAUNCH("arc rcut");
   ArcDims g;
   for (int d = 0; d < 3; ++d) g.n[d] = a->n[d];
   for (int it = 0; it < nrefine; ++it) {
-    k_arc_refine<<<nb, 256, 0, a->stream>>>(g, a->rcidx, a->rcidx2, a->d_rc, a->error, a->rcut, a->rerr);
+    k_arc_refine<<<nb, 256, 0, a->sys->stream>>>(g, a->rcidx, a->rcidx2, a->d_rc, a->error, a->rcut, a->rerr);
     MD_CHECK_LAUNCH("arc refine");
     std::swap(a->rcidx, a->rcidx2);
   }
   // PressureCorrection::correction on the same profile and rc map
-  k_pc_multiply<<<nb, 256, 0, a->stream>>>(ne, a->nrc, a->rhok, V / ne, a->pck, a->work);
+  k_pc_multiply<<<nb, 256, 0, a->sys->stream>>>(ne, a->nrc, a->rhok, V / ne, a->pck, a->work);
   MD_CHECK_LAUNCH("pc multiply");
   if (int r = dft3(a, a->work, +1, 3 * a->nrc)) return r;
   const double dv = (hs.L[0] / a->n[0]) * (hs.L[1] / a->n[1]) * (hs.L[2] / a->n[2]);
   if (nb > sys->max_partial_blocks) { md_set_error("partials buffer too small"); return MD_ERR_BADARG; }
-  k_pc_reduce<<<nb, 256, 0, a->stream>>>(ne, a->nrc, a->work, a->rcidx, a->rho, dv / (V * V), sys->partials,
+  k_pc_reduce<<<nb, 256, 0, a->sys->stream>>>(ne, a->nrc, a->work, a->rcidx, a->rho, dv / (V * V), sys->partials,
                                          &sys->st->red_counter[RED_MISC], a->pcorr);
   MD_CHECK_LAUNCH("pc reduce");
   return MD_OK;
@@ -536,17 +536,17 @@ extern "C" int md_arc_update(md_adapt_rcut* a, double prec, int nrefine) {
 
 extern "C" int md_arc_get_error(md_adapt_rcut* a, double* err) {
   if (!a || !err) return MD_ERR_BADARG;
-  MD_CUDA(cudaMemcpyAsync(err, a->error, sizeof(double) * a->nrc * a->nele, cudaMemcpyDeviceToHost, a->stream));
-  MD_CUDA(cudaStreamSynchronize(a->stream));
+  MD_CUDA(cudaMemcpyAsync(err, a->error, sizeof(double) * a->nrc * a->nele, cudaMemcpyDeviceToHost, a->sys->stream));
+  MD_CUDA(cudaStreamSynchronize(a->sys->stream));
   return MD_OK;
 }
 
 extern "C" int md_arc_get_rcut(md_adapt_rcut* a, double* rcut, int* idx, double* result_error) {
   if (!a) return MD_ERR_BADARG;
-  if (rcut) MD_CUDA(cudaMemcpyAsync(rcut, a->rcut, sizeof(double) * a->nele, cudaMemcpyDeviceToHost, a->stream));
-  if (idx) MD_CUDA(cudaMemcpyAsync(idx, a->rcidx, sizeof(int) * a->nele, cudaMemcpyDeviceToHost, a->stream));
-  if (result_error) MD_CUDA(cudaMemcpyAsync(result_error, a->rerr, sizeof(double) * a->nele, cudaMemcpyDeviceToHost, a->stream));
-  MD_CUDA(cudaStreamSynchronize(a->stream));
+  if (rcut) MD_CUDA(cudaMemcpyAsync(rcut, a->rcut, sizeof(double) * a->nele, cudaMemcpyDeviceToHost, a->sys->stream));
+  if (idx) MD_CUDA(cudaMemcpyAsync(idx, a->rcidx, sizeof(int) * a->nele, cudaMemcpyDeviceToHost, a->sys->stream));
+  if (result_error) MD_CUDA(cudaMemcpyAsync(result_error, a->rerr, sizeof(double) * a->nele, cudaMemcpyDeviceToHost, a->sys->stream));
+  MD_CUDA(cudaStreamSynchronize(a->sys->stream));
   DevState hs;
   if (int r = a->sys->read_state(hs)) return r;
   if (hs.flags & FLAG_QUADRATURE) { md_set_error("adaptive quadrature reached its depth bound"); return MD_ERR_BADARG; }
@@ -556,10 +556,10 @@ extern "C" int md_arc_get_rcut(md_adapt_rcut* a, double* rcut, int* idx, double*
 extern "C" int md_arc_get_tables(md_adapt_rcut* a, double* s1k, double* s2k, double* pck) {
   if (!a) return MD_ERR_BADARG;
   const size_t m = (size_t)a->nrc * a->nele;
-  if (s1k) MD_CUDA(cudaMemcpyAsync(s1k, a->s1k, sizeof(double) * m, cudaMemcpyDeviceToHost, a->stream));
-  if (s2k) MD_CUDA(cudaMemcpyAsync(s2k, a->s2k, sizeof(double) * 3 * m, cudaMemcpyDeviceToHost, a->stream));
-  if (pck) MD_CUDA(cudaMemcpyAsync(pck, a->pck, sizeof(double) * 3 * m, cudaMemcpyDeviceToHost, a->stream));
-  MD_CUDA(cudaStreamSynchronize(a->stream));
+  if (s1k) MD_CUDA(cudaMemcpyAsync(s1k, a->s1k, sizeof(double) * m, cudaMemcpyDeviceToHost, a->sys->stream));
+  if (s2k) MD_CUDA(cudaMemcpyAsync(s2k, a->s2k, sizeof(double) * 3 * m, cudaMemcpyDeviceToHost, a->sys->stream));
+  if (pck) MD_CUDA(cudaMemcpyAsync(pck, a->pck, sizeof(double) * 3 * m, cudaMemcpyDeviceToHost, a->sys->stream));
+  MD_CUDA(cudaStreamSynchronize(a->sys->stream));
   return MD_OK;
 }
 
@@ -575,18 +575,18 @@ extern "C" int md_arc_assign(md_adapt_rcut* a, md_system* sys) {
     MD_CUDA(cudaMalloc(&sys->d_lattice, sizeof(float) * ne));
   }
   for (int d = 0; d < 3; ++d) sys->lat_n[d] = a->n[d];
-  k_lattice_from_rcut<<<(int)((ne + 255) / 256), 256, 0, a->stream>>>(ne, a->rcut, sys->d_lattice, sys->st);
+  k_lattice_from_rcut<<<(int)((ne + 255) / 256), 256, 0, a->sys->stream>>>(ne, a->rcut, sys->d_lattice, sys->st);
   MD_CHECK_LAUNCH("lattice");
   return MD_OK;
 }
 
 extern "C" int md_arc_pressure_correction(md_adapt_rcut* a, md_system* sys, double out[3]) {
   if (!a || !sys) return MD_ERR_BADARG;
-  k_store_pcorr<<<1, 1, 0, a->stream>>>(a->pcorr, sys->st);
+  k_store_pcorr<<<1, 1, 0, a->sys->stream>>>(a->pcorr, sys->st);
   MD_CHECK_LAUNCH("store pcorr");
   if (out) {
-    MD_CUDA(cudaMemcpyAsync(out, a->pcorr, sizeof(double) * 3, cudaMemcpyDeviceToHost, a->stream));
-    MD_CUDA(cudaStreamSynchronize(a->stream));
+    MD_CUDA(cudaMemcpyAsync(out, a->pcorr, sizeof(double) * 3, cudaMemcpyDeviceToHost, a->sys->stream));
+    MD_CUDA(cudaStreamSynchronize(a->sys->stream));
   }
   return MD_OK;
 }

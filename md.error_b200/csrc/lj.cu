@@ -63,29 +63,38 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
     // gathers, then the arithmetic -- U independent loads in flight per lane
     constexpr int U = 4;
     for (int k0 = lane; k0 < n; k0 += U * G) {
-      int jj[U];
+      int ee[U];
       float4 pj[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int kk = k0 + u * G;
-        jj[u] = kk < n ? __ldg(row + kk) : -1;
+        ee[u] = kk < n ? __ldg(row + kk) : -1;
       }
 #pragma unroll
-      for (int u = 0; u < U; ++u) pj[u] = __ldg(pos + (jj[u] >= 0 ? jj[u] : i));
+      // -1 marks "past the end" (a packed entry never has all six image bits set)
+      for (int u = 0; u < U; ++u) pj[u] = __ldg(pos + (ee[u] != -1 ? (ee[u] & 0x03FFFFFF) : i));
+      // the U pair forces of this batch are summed in FP32, the batch sum is
+      // added to the lane's Kahan-compensated accumulator
+      float bx = 0.f, by = 0.f, bz = 0.f;
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const float dx = min_image_exact(__fsub_rn(pj[u].x, pi.x), L0, I0);
-        const float dy = min_image_exact(__fsub_rn(pj[u].y, pi.y), L1, I1);
-        const float dz = min_image_exact(__fsub_rn(pj[u].z, pi.z), L2, I2);
+        // d - k L with the image k stored at build time: the same binary32
+        // operations as shortestImage's x -= floorf(x/L + 0.5) L
+        const unsigned code = (unsigned)ee[u] >> 26;
+        const float kx = (float)((int)(code & 3u) - 1), ky = (float)((int)((code >> 2) & 3u) - 1),
+                    kz = (float)((int)(code >> 4) - 1);
+        const float dx = __fsub_rn(__fsub_rn(pj[u].x, pi.x), __fmul_rn(kx, L0));
+        const float dy = __fsub_rn(__fsub_rn(pj[u].y, pi.y), __fmul_rn(ky, L1));
+        const float dz = __fsub_rn(__fsub_rn(pj[u].z, pi.z), __fmul_rn(kz, L2));
         const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-        if (jj[u] >= 0 && r2 < rc2) {
+        if (ee[u] != -1 && r2 < rc2) {
           const float ri2 = __fdividef(1.0f, r2);
           const float s2 = p.sig2f * ri2;
           const float s6 = s2 * s2 * s2;
           const float fs = p.eps4f * (6.f * s6 - 12.f * s6 * s6) * ri2;
-          fx.add(fs * dx);
-          fy.add(fs * dy);
-          fz.add(fs * dz);
+          bx += fs * dx;
+          by += fs * dy;
+          bz += fs * dz;
           if (STATS) {
             e += p.eps4f * (s6 * s6 - s6) + p.shiftf;
             vx += fs * dx * dx;
@@ -94,7 +103,11 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
           }
         }
       }
+      fx.add(bx);
+      fy.add(by);
+      fz.add(bz);
     }
+    (void)I0; (void)I1; (void)I2;
   }
   double Fx = group_sum<G>(fx.value()), Fy = group_sum<G>(fy.value()), Fz = group_sum<G>(fz.value());
   if (i < N && lane == 0) {
@@ -139,15 +152,18 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
         jj[u] = kk < n ? __ldg(row + kk) : -1;
       }
 #pragma unroll
-      for (int u = 0; u < U; ++u) pq[u] = pos[jj[u] >= 0 ? jj[u] : i];
+      for (int u = 0; u < U; ++u) pq[u] = pos[jj[u] != -1 ? (jj[u] & 0x03FFFFFF) : i];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
       const double4a pj = pq[u];
-      const double dx = min_image_exact(pj.x - pi.x, L0, I0);
-      const double dy = min_image_exact(pj.y - pi.y, L1, I1);
-      const double dz = min_image_exact(pj.z - pi.z, L2, I2);
+      const unsigned code = (unsigned)jj[u] >> 26;
+      const double kx = (double)((int)(code & 3u) - 1), ky = (double)((int)((code >> 2) & 3u) - 1),
+                   kz = (double)((int)(code >> 4) - 1);
+      const double dx = __dsub_rn(__dsub_rn(pj.x, pi.x), __dmul_rn(kx, L0));
+      const double dy = __dsub_rn(__dsub_rn(pj.y, pi.y), __dmul_rn(ky, L1));
+      const double dz = __dsub_rn(__dsub_rn(pj.z, pi.z), __dmul_rn(kz, L2));
       const double r2 = dx * dx + dy * dy + dz * dz;
-      if (jj[u] >= 0 && r2 < rc2) {
+      if (jj[u] != -1 && r2 < rc2) {
         const double ri2 = 1.0 / r2;
         const double s2 = p.sig2 * ri2;
         const double s6 = s2 * s2 * s2;

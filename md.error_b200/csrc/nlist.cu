@@ -4,17 +4,22 @@
 // NeighborList::mallocDeviceNeighborList (UNI/src/NeighborList_interface.cu:187-208),
 // Displacement_max (ENG/src/Displacement_interface.cu:80-126).
 //
-// One warp builds the full list of one atom i (atoms are in cell order).  The
-// candidate cells are the ones whose box intersects the sphere of radius
-// rlist_i (+1e-3 margin), enumerated as (x,y) columns and contiguous z runs,
-// so every run of candidate j is one contiguous slice of the cell-sorted
-// arrays: 32 lanes test 32 consecutive j with coalesced float4/double4 loads,
-// and a ballot compacts the accepted ones into row i of the list.
+// One block per home cell.  The candidate cells of the home cell (every cell
+// whose box comes within the largest list radius of the home-cell box, or the
+// reference's c +- 1 stencil in cell-shift mode) are enumerated as (x, y)
+// columns of contiguous z runs -- each run one contiguous slice of the
+// cell-sorted arrays -- and staged into a shared-memory tile.  Each warp then
+// takes one home atom i at a time; its 32 lanes test 32 tile entries at once,
+// skipping runs whose box lies beyond rlist_i, and a ballot compacts the
+// accepted ones into row i of the list.  When the tile would not fit, the same
+// loop reads the runs from global memory.
 // The acceptance test repeats the reference's binary32 operations exactly
 // (no FMA contraction), so the neighbour SETS are bit-identical to the
 // reference criterion; only the enumeration (and list order) is ours.
-// List layout: list[i*cap + k], k < nnb[i] (row-major: the G lanes that
-// later share atom i read consecutive entries).
+// List layout: list[i*cap + k], k < nnb[i]; each entry packs the slot index j
+// (bits 0-25) and the periodic image k_d = floorf(d_d/L_d + 0.5) in {-1,0,1}
+// of the minimum-image vector, 2 bits per axis (bits 26-31, stored k+1), so
+// the force loop forms d - k L with the reference's exact operations.
 #include <cmath>
 #include <cstring>
 #include "device_common.cuh"
@@ -23,153 +28,208 @@ struct NlGeom {
   int nc[3];
 };
 
+#define NL_TILE_CAP 2304
+#define NL_MAX_RUNS 160
+
+struct RunInfo {
+  int jb, cnt, off;     // global start, length, tile offset
+  int sx, sy, sz;       // cell-shift images (cell-shift criterion)
+  float b0[3], b1[3];   // run box (unwrapped frame of the home cell)
+};
+
+__device__ __forceinline__ int img_code(int kx, int ky, int kz) {
+  return ((kx + 1) << 26) | ((ky + 1) << 28) | ((kz + 1) << 30);
+}
+
 template <class R, int MODE>
 __global__ void __launch_bounds__(128)
 k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __restrict__ rcut,
-           const uint32_t* __restrict__ start, const uint32_t* __restrict__ cell_of, NlGeom g,
-           const DevState* __restrict__ st,
+           const uint32_t* __restrict__ start, NlGeom g, const DevState* __restrict__ st,
            double rlist_uniform, double skin, int cap, int* __restrict__ list, int* __restrict__ nnb,
            typename V4<R>::T* __restrict__ backup, int force_minimage, DevState* stw, int gate) {
-  if (gate && !(st->flags & FLAG_REBUILD)) return;
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (i >= N) return;
   typedef typename V4<R>::T T4;
-  const T4 pi = pos[i];
+  extern __shared__ __align__(16) unsigned char nl_smem[];
+  T4* tile = reinterpret_cast<T4*>(nl_smem);
+  __shared__ RunInfo runs[NL_MAX_RUNS];
+  __shared__ int nruns, tile_n, use_global;
+  __shared__ float rl_max_sh;
+  if (gate && !(st->flags & FLAG_REBUILD)) return;
+  const int c = blockIdx.x;
+  const int i0 = (int)start[c], i1 = (int)start[c + 1];
+  if (i0 == i1) return;  // empty home cell (uniform exit for the whole block)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const R L[3] = {boxL<R>(st, 0), boxL<R>(st, 1), boxL<R>(st, 2)};
   const R Li[3] = {boxLi<R>(st, 0), boxLi<R>(st, 1), boxLi<R>(st, 2)};
-  // list radius: rcut[ii] + rlistExten (AllPair) or the uniform rlist (cell list)
-  R rl;
-  if (MODE == MD_NL_MINIMAGE) rl = add_rn((R)rcut[i], (R)skin);
-  else rl = (R)rlist_uniform;
-  const R rl2 = mul_rn(rl, rl);
   const bool minimg = (MODE == MD_NL_MINIMAGE) || force_minimage;
+  const int hc[3] = {c / (g.nc[2] * g.nc[1]), (c / g.nc[2]) % g.nc[1], c % g.nc[2]};
+  double h[3];
+  for (int d = 0; d < 3; ++d) h[d] = st->L[d] / g.nc[d];
 
-  // Candidate cells.  Minimum-image mode: every cell whose box meets the
-  // sphere of radius rl + 1e-3 around r_i (FP64, conservative), pruned per
-  // column.  Cell-shift mode: the reference stencil, cells c_i +- reach with
-  // reach = 1 when the cell edge is >= rlist (buildCellNeighborhood).
-  const bool cs = !minimg;
-  const double rle = (double)rl + 1e-3;
-  double h[3], xi[3] = {(double)pi.x, (double)pi.y, (double)pi.z};
-  bool full[3];
-  int ci[3] = {0, 0, 0}, reach[3] = {1, 1, 1};
-  if (cs) {
-    const uint32_t c = cell_of[i];
-    ci[2] = (int)(c % (uint32_t)g.nc[2]);
-    ci[1] = (int)((c / (uint32_t)g.nc[2]) % (uint32_t)g.nc[1]);
-    ci[0] = (int)(c / ((uint32_t)g.nc[2] * (uint32_t)g.nc[1]));
+  // largest list radius among the home atoms
+  if (threadIdx.x == 0) rl_max_sh = 0.f;
+  __syncthreads();
+  if (MODE == MD_NL_MINIMAGE) {
+    float m = 0.f;
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) m = fmaxf(m, __fadd_rn(rcut[i], (float)skin));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) atomicMax((int*)&rl_max_sh, __float_as_int(m));  // non-negative floats order as ints
+  } else if (threadIdx.x == 0) {
+    rl_max_sh = (float)rlist_uniform;
   }
-  bool finite = true;
-  for (int d = 0; d < 3; ++d) {
-    // enumeration coordinate wrapped into [0, L): keeps every candidate cell
-    // index inside the table even if atoms drifted since the last binning
-    finite = finite && isfinite(xi[d]);
-    xi[d] -= floor(xi[d] / st->L[d]) * st->L[d];
-    if (!(xi[d] >= 0.0) || xi[d] >= st->L[d]) xi[d] = 0.0;
-  }
-  if (!finite) {
-    if (lane == 0) { nnb[i] = 0; backup[i] = pi; atomicOr(&stw->flags, FLAG_NAN); }
-    return;
-  }
-  for (int d = 0; d < 3; ++d) {
-    h[d] = st->L[d] / g.nc[d];
-    if (cs) {
-      reach[d] = (h[d] >= rlist_uniform) ? 1 : (int)ceil(rlist_uniform / h[d]);
-      full[d] = false;  // the host guarantees 2*reach+1 <= nc in this mode
-    } else {
-      full[d] = (2.0 * ceil(rle / h[d]) + 1.0) >= (double)g.nc[d];
+  __syncthreads();
+
+  // runs of candidate cells (thread 0; at most a few dozen)
+  if (threadIdx.x == 0) {
+    const double rle = (double)rl_max_sh * (1.0 + 1e-6) + 2e-3;
+    int lo[3], hi[3];
+    bool full[3];
+    for (int d = 0; d < 3; ++d) {
+      if (!minimg) {
+        const int reach = (h[d] >= rlist_uniform) ? 1 : (int)ceil(rlist_uniform / h[d]);
+        lo[d] = hc[d] - reach; hi[d] = hc[d] + reach; full[d] = false;
+      } else {
+        lo[d] = (int)floor((hc[d] * h[d] - rle) / h[d]);
+        hi[d] = (int)floor(((hc[d] + 1) * h[d] + rle) / h[d]);
+        full[d] = (hi[d] - lo[d] + 1) >= g.nc[d];
+        if (full[d]) { lo[d] = 0; hi[d] = g.nc[d] - 1; }
+      }
     }
-  }
-  int n = 0;
-  const unsigned ltmask = (1u << lane) - 1u;
-  int xlo, xhi;
-  if (cs) { xlo = ci[0] - reach[0]; xhi = ci[0] + reach[0]; }
-  else if (full[0]) { xlo = 0; xhi = g.nc[0] - 1; }
-  else { xlo = (int)floor((xi[0] - rle) / h[0]); xhi = (int)floor((xi[0] + rle) / h[0]); }
-  for (int ix = xlo; ix <= xhi; ++ix) {
-    int cx = ix, sx = 0;
-    double dxm = 0.0;
-    if (!full[0]) {
+    int nr = 0, off = 0;
+    bool overflow_runs = false;
+    for (int ix = lo[0]; ix <= hi[0]; ++ix) {
+      int cx = ix, sx = 0;
       if (cx < 0) { cx += g.nc[0]; sx = 1; } else if (cx >= g.nc[0]) { cx -= g.nc[0]; sx = -1; }
-      if (!cs) {
-        dxm = fmax(0.0, fmax(ix * h[0] - xi[0], xi[0] - (ix + 1) * h[0]));
-        if (dxm > rle) continue;
-      }
-    }
-    const double ry = sqrt(fmax(0.0, rle * rle - dxm * dxm));
-    int ylo, yhi;
-    if (cs) { ylo = ci[1] - reach[1]; yhi = ci[1] + reach[1]; }
-    else if (full[1]) { ylo = 0; yhi = g.nc[1] - 1; }
-    else { ylo = (int)floor((xi[1] - ry) / h[1]); yhi = (int)floor((xi[1] + ry) / h[1]); }
-    for (int iy = ylo; iy <= yhi; ++iy) {
-      int cy = iy, sy = 0;
-      double dym = 0.0;
-      if (!full[1]) {
+      for (int iy = lo[1]; iy <= hi[1]; ++iy) {
+        int cy = iy, sy = 0;
         if (cy < 0) { cy += g.nc[1]; sy = 1; } else if (cy >= g.nc[1]) { cy -= g.nc[1]; sy = -1; }
-        if (!cs) {
-          dym = fmax(0.0, fmax(iy * h[1] - xi[1], xi[1] - (iy + 1) * h[1]));
-          if (dxm * dxm + dym * dym > rle * rle) continue;
+        const int colbase = g.nc[2] * (cy + g.nc[1] * cx);
+        int ra[3], rb[3], rs[3], rz0[3], nseg = 0;
+        if (full[2]) { ra[0] = 0; rb[0] = g.nc[2] - 1; rs[0] = 0; rz0[0] = 0; nseg = 1; }
+        else {
+          const int zlo = lo[2], zhi = hi[2];
+          if (zlo < 0) { ra[nseg] = zlo + g.nc[2]; rb[nseg] = g.nc[2] - 1; rs[nseg] = 1; rz0[nseg] = zlo; ++nseg; }
+          const int a = max(zlo, 0), b = min(zhi, g.nc[2] - 1);
+          if (a <= b) { ra[nseg] = a; rb[nseg] = b; rs[nseg] = 0; rz0[nseg] = a; ++nseg; }
+          if (zhi >= g.nc[2]) { ra[nseg] = 0; rb[nseg] = zhi - g.nc[2]; rs[nseg] = -1; rz0[nseg] = g.nc[2]; ++nseg; }
         }
-      }
-      const double rz = sqrt(fmax(0.0, rle * rle - dxm * dxm - dym * dym));
-      const int colbase = g.nc[2] * (cy + g.nc[1] * cx);
-      // up to three contiguous z runs: [a,b] with image shift sz
-      int ra[3], rb[3], rs[3], nr = 0;
-      if (full[2]) { ra[0] = 0; rb[0] = g.nc[2] - 1; rs[0] = 0; nr = 1; }
-      else {
-        int zlo, zhi;
-        if (cs) { zlo = ci[2] - reach[2]; zhi = ci[2] + reach[2]; }
-        else { zlo = (int)floor((xi[2] - rz) / h[2]); zhi = (int)floor((xi[2] + rz) / h[2]); }
-        if (zlo < 0) { ra[nr] = zlo + g.nc[2]; rb[nr] = g.nc[2] - 1; rs[nr] = 1; ++nr; }
-        int a = max(zlo, 0), b = min(zhi, g.nc[2] - 1);
-        if (a <= b) { ra[nr] = a; rb[nr] = b; rs[nr] = 0; ++nr; }
-        if (zhi >= g.nc[2]) { ra[nr] = 0; rb[nr] = zhi - g.nc[2]; rs[nr] = -1; ++nr; }
-      }
-      // image shifts of the cell list path: shift = shiftNoi * box.size (binary32)
-      const R shx = mul_rn((R)sx, L[0]), shy = mul_rn((R)sy, L[1]);
-      for (int r = 0; r < nr; ++r) {
-        const R shz = mul_rn((R)rs[r], L[2]);
-        const int jb = (int)start[colbase + ra[r]];
-        const int je = (int)start[colbase + rb[r] + 1];
-        for (int j0 = jb; j0 < je; j0 += 32) {
-          const int j = j0 + lane;
-          bool ok = false;
-          if (j < je) {
-            const T4 pj = pos[j];
-            R dx, dy, dz;
-            if (minimg) {
-              dx = min_image_exact(sub_rn(pj.x, pi.x), L[0], Li[0]);
-              dy = min_image_exact(sub_rn(pj.y, pi.y), L[1], Li[1]);
-              dz = min_image_exact(sub_rn(pj.z, pi.z), L[2], Li[2]);
-            } else {
-              dx = sub_rn(sub_rn(pj.x, shx), pi.x);
-              dy = sub_rn(sub_rn(pj.y, shy), pi.y);
-              dz = sub_rn(sub_rn(pj.z, shz), pi.z);
-            }
-            const R d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
-            ok = (d2 < rl2) && (j != i);
-          }
-          const unsigned m = __ballot_sync(0xffffffffu, ok);
-          if (ok) {
-            const int p = n + __popc(m & ltmask);
-            if (p < cap) list[(size_t)i * cap + p] = j;
-          }
-          n += __popc(m);
+        for (int s = 0; s < nseg; ++s) {
+          const int jb = (int)start[colbase + ra[s]], je = (int)start[colbase + rb[s] + 1];
+          if (je == jb) continue;
+          if (nr == NL_MAX_RUNS) { overflow_runs = true; continue; }
+          RunInfo& R_ = runs[nr++];
+          R_.jb = jb; R_.cnt = je - jb; R_.off = off;
+          R_.sx = sx; R_.sy = sy; R_.sz = rs[s];
+          const int zc0 = rz0[s], zc1 = rz0[s] + (rb[s] - ra[s]);
+          R_.b0[0] = full[0] ? -1e30f : (float)(ix * h[0]); R_.b1[0] = full[0] ? 1e30f : (float)((ix + 1) * h[0]);
+          R_.b0[1] = full[1] ? -1e30f : (float)(iy * h[1]); R_.b1[1] = full[1] ? 1e30f : (float)((iy + 1) * h[1]);
+          R_.b0[2] = full[2] ? -1e30f : (float)(zc0 * h[2]); R_.b1[2] = full[2] ? 1e30f : (float)((zc1 + 1) * h[2]);
+          off += je - jb;
         }
       }
     }
+    nruns = nr;
+    tile_n = off;
+    use_global = (off > NL_TILE_CAP) ? 1 : 0;
+    if (overflow_runs) atomicOr(&stw->flags, FLAG_NL_OVERFLOW);
   }
-  if (lane == 0) {
-    nnb[i] = n;
-    backup[i] = pi;
-    if (n > cap) atomicOr(&stw->flags, FLAG_NL_OVERFLOW);
-    atomicMax(&stw->max_nnb, n);
+  __syncthreads();
+  const int nr = nruns;
+  if (!use_global) {
+    for (int r = 0; r < nr; ++r) {
+      const RunInfo& R_ = runs[r];
+      for (int t = threadIdx.x; t < R_.cnt; t += blockDim.x) tile[R_.off + t] = pos[R_.jb + t];
+    }
   }
+  __syncthreads();
+  const bool glob = use_global;
+  const unsigned ltmask = (1u << lane) - 1u;
+
+  for (int i = i0 + warp; i < i1; i += nwarp) {
+    const T4 pi = pos[i];
+    R rl;
+    if (MODE == MD_NL_MINIMAGE) rl = add_rn((R)rcut[i], (R)skin);
+    else rl = (R)rlist_uniform;
+    const R rl2 = mul_rn(rl, rl);
+    // enumeration coordinates of i in the home cell's frame
+    float xe[3];
+    {
+      const double xi[3] = {(double)pi.x, (double)pi.y, (double)pi.z};
+      for (int d = 0; d < 3; ++d) {
+        double w = xi[d] - floor(xi[d] / st->L[d]) * st->L[d];
+        if (!(w >= 0.0) || w >= st->L[d]) w = 0.0;
+        xe[d] = (float)w;
+      }
+    }
+    const float rle_i = (float)rl * (1.0f + 1e-5f) + 2e-3f;
+    int n = 0;
+    for (int r = 0; r < nr; ++r) {
+      const RunInfo& R_ = runs[r];
+      if (minimg) {
+        float dd = 0.f;
+        for (int d = 0; d < 3; ++d) {
+          const float e = fmaxf(0.f, fmaxf(R_.b0[d] - xe[d], xe[d] - R_.b1[d]));
+          dd += e * e;
+        }
+        if (dd > rle_i * rle_i) continue;
+      }
+      const R shx = mul_rn((R)R_.sx, L[0]), shy = mul_rn((R)R_.sy, L[1]), shz = mul_rn((R)R_.sz, L[2]);
+      for (int t0 = 0; t0 < R_.cnt; t0 += 32) {
+        const int t = t0 + lane;
+        bool ok = false;
+        int code = 0;
+        const int j = R_.jb + t;
+        if (t < R_.cnt) {
+          const T4 pj = glob ? pos[j] : tile[R_.off + t];
+          const R rx = sub_rn(pj.x, pi.x), ry = sub_rn(pj.y, pi.y), rz = sub_rn(pj.z, pi.z);
+          const R kx = floor_r(add_rn(mul_rn(rx, Li[0]), R(0.5)));
+          const R ky = floor_r(add_rn(mul_rn(ry, Li[1]), R(0.5)));
+          const R kz = floor_r(add_rn(mul_rn(rz, Li[2]), R(0.5)));
+          R dx, dy, dz;
+          if (minimg) {
+            dx = sub_rn(rx, mul_rn(kx, L[0]));
+            dy = sub_rn(ry, mul_rn(ky, L[1]));
+            dz = sub_rn(rz, mul_rn(kz, L[2]));
+          } else {
+            dx = sub_rn(sub_rn(pj.x, shx), pi.x);
+            dy = sub_rn(sub_rn(pj.y, shy), pi.y);
+            dz = sub_rn(sub_rn(pj.z, shz), pi.z);
+          }
+          const R d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
+          ok = (d2 < rl2) && (j != i);
+          code = img_code((int)kx, (int)ky, (int)kz);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        if (ok) {
+          const int p = n + __popc(m & ltmask);
+          if (p < cap) list[(size_t)i * cap + p] = j | code;
+        }
+        n += __popc(m);
+      }
+    }
+    if (lane == 0) {
+      nnb[i] = n;
+      backup[i] = pi;
+      if (n > cap) atomicOr(&stw->flags, FLAG_NL_OVERFLOW);
+      atomicMax(&stw->max_nnb, n);
+    }
+  }
+}
+
+template <class R, int MODE>
+static const void* nl_kernel() {
+  static bool attr = false;
+  const void* f = (const void*)k_nl_build<R, MODE>;
+  if (!attr) {
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(NL_TILE_CAP * sizeof(typename V4<R>::T)));
+    attr = true;
+  }
+  return f;
 }
 
 int nlist_build_impl(md_nlist* nl, md_system* sys, md_cell_list* cl, Recorder* rec, bool gated) {
   int N = sys->N;
+  if (N >= (1 << 26)) { md_set_error("neighbour lists hold at most 2^26 atoms"); return MD_ERR_BADARG; }
   NlGeom g;
   for (int d = 0; d < 3; ++d) g.nc[d] = cl->ncell[d];
   int gate = gated ? 1 : 0;
@@ -189,17 +249,19 @@ int nlist_build_impl(md_nlist* nl, md_system* sys, md_cell_list* cl, Recorder* r
   double rl = nl->rlist, skin = nl->skin;
   DevState* st = sys->st;
   int cap = nl->cap;
-  dim3 grid(ceil_div((long long)N * 32, 128)), block(128);
-  void* a[] = {&N, &sys->pos, &sys->rcut, &cl->start, &cl->cell_of, &g, &st, &rl, &skin, &cap, &nl->list,
+  dim3 grid(cl->ntot), block(128);
+  void* a[] = {&N, &sys->pos, &sys->rcut, &cl->start, &g, &st, &rl, &skin, &cap, &nl->list,
                &nl->nnb, &nl->backup, &force_mi, &st, &gate};
   const void* f;
-  if (sys->prec == MD_PREC_FP64)
-    f = nl->mode == MD_NL_MINIMAGE ? (const void*)k_nl_build<double, MD_NL_MINIMAGE>
-                                   : (const void*)k_nl_build<double, MD_NL_CELLSHIFT>;
-  else
-    f = nl->mode == MD_NL_MINIMAGE ? (const void*)k_nl_build<float, MD_NL_MINIMAGE>
-                                   : (const void*)k_nl_build<float, MD_NL_CELLSHIFT>;
-  if (int r = rec_launch(rec, f, grid, block, 0, a)) return r;
+  size_t smem;
+  if (sys->prec == MD_PREC_FP64) {
+    f = nl->mode == MD_NL_MINIMAGE ? nl_kernel<double, MD_NL_MINIMAGE>() : nl_kernel<double, MD_NL_CELLSHIFT>();
+    smem = NL_TILE_CAP * sizeof(double4a);
+  } else {
+    f = nl->mode == MD_NL_MINIMAGE ? nl_kernel<float, MD_NL_MINIMAGE>() : nl_kernel<float, MD_NL_CELLSHIFT>();
+    smem = NL_TILE_CAP * sizeof(float4);
+  }
+  if (int r = rec_launch(rec, f, grid, block, smem, a)) return r;
   nl->built = true;
   return MD_OK;
 }
@@ -360,7 +422,7 @@ extern "C" int md_nlist_get(md_nlist* nl, md_system* sys, int32_t* counts, int32
     int c = nnb[k] < nl->cap ? nnb[k] : nl->cap;
     counts[o] = c;
     if (pairs)
-      for (int t = 0; t < c; ++t) pairs[off + t] = id[lst[(size_t)k * nl->cap + t]];
+      for (int t = 0; t < c; ++t) pairs[off + t] = id[lst[(size_t)k * nl->cap + t] & 0x03FFFFFF];
     off += c;
   }
   return MD_OK;
