@@ -67,14 +67,14 @@ enum md_stat_slot {
   MD_STAT_NB_ENERGY = 0,   /* mdStatisticNonBondedPotential  */
   MD_STAT_VIRIAL_XX = 1,   /* mdStatisticVirialXX (sum f.d)  */
   MD_STAT_VIRIAL_YY = 2,
-  MD_STAT_VIRIAL_ZZ = 3,
-  MD_STAT_KINETIC_XX = 4,  /* 1/2 sum m v_x^2                */
-  MD_STAT_KINETIC_YY = 5,
-  MD_STAT_KINETIC_ZZ = 6,
-  MD_STAT_PRESSURE_CORR_XX = 7, /* tail corrections added to P  */
-  MD_STAT_PRESSURE_CORR_YY = 8,
-  MD_STAT_PRESSURE_CORR_ZZ = 9,
-  MD_STAT_ELEC_DIR = 10,   /* real-space Ewald energy        */
+  MD_STAT_VIRIAL_ZZ = 3,   /* (virials include every force term of the step) */
+  MD_STAT_ELEC_DIR = 4,    /* real-space Ewald energy        */
+  MD_STAT_KINETIC_XX = 5,  /* 1/2 sum m v_x^2                */
+  MD_STAT_KINETIC_YY = 6,
+  MD_STAT_KINETIC_ZZ = 7,
+  MD_STAT_PRESSURE_CORR_XX = 8, /* tail corrections added to P  */
+  MD_STAT_PRESSURE_CORR_YY = 9,
+  MD_STAT_PRESSURE_CORR_ZZ = 10,
   MD_STAT_ELEC_REC = 11,   /* reciprocal (SPME) energy       */
   MD_STAT_ELEC_SELF = 12,  /* -beta/sqrt(pi) sum q^2         */
   MD_STAT_COUNT = 16
@@ -185,6 +185,29 @@ int md_engine_clear_forces(md_engine* eng, md_system* sys);
 int md_engine_apply_nonbonded(md_engine* eng, md_system* sys, md_nlist* nl, int with_stats);
 /* applyBondedInteraction: MD_OK with nothing to do when no bonds are registered. */
 int md_engine_apply_bonded(md_engine* eng, md_system* sys);
+/* Real-space Ewald (ElectrostaticInteraction_dir, RE/src/EleDir.cpp:43-61) fused into
+   the non-bonded kernel: E = 1/2 sum q_i q_j erfc(beta r)/r over the same list and
+   cutoff; energy into MD_STAT_ELEC_DIR. */
+int md_engine_register_coulomb(md_engine* eng, double beta);
+
+/* ------------------------------------------------------------ long range
+ * Reciprocal SPME, replaces ElectrostaticInteraction_rec_BSpline (ik differentiation,
+ * RE/src/EleRecBSpline.cpp:393-877) and ElectrostaticInteraction_rec_FBSpline
+ * (analytic differentiation, RE/src/EleRecFBSpline.cpp:771-1195): cardinal B-spline
+ * order `order`, mesh K (powers of two), splitting beta, rectangular box.
+ * method 0 = ik, 1 = analytic.  md_spme_apply adds the reciprocal forces and, with
+ * stats, stores the energy in MD_STAT_ELEC_REC and adds its virial. */
+typedef struct md_spme md_spme;
+int md_spme_create(md_spme** out, md_system* sys, const int K[3], int order, double beta, int method);
+int md_spme_destroy(md_spme* spme);
+int md_spme_apply(md_spme* spme, md_system* sys, int with_stats);
+/* the charge mesh Q of the last apply (calQ), [K0][K1][K2] */
+int md_spme_get_mesh(md_spme* spme, double* Q);
+/* -beta/sqrt(pi) sum q^2 (ElectrostaticInteraction.cpp:219-222) into MD_STAT_ELEC_SELF */
+int md_ewald_self_energy(md_system* sys, double beta, double* out);
+/* Exact reciprocal Ewald sum over |m_d| <= K_d/2 in FP64 (ElectrostaticInteraction_rec_ES,
+   RE/src/EleRecES.cpp:49-144): energy, and the forces added when add_forces != 0. */
+int md_ewald_exact(md_system* sys, const int K[3], double beta, double* energy, int add_forces);
 
 /* ------------------------------------------------------- per-atom cutoff
  * Replaces AssignRCut::getRCut + assign (ENG/src/AssignRCut.cu:46-117):

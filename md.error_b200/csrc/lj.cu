@@ -15,9 +15,12 @@
 #include <cmath>
 #include "device_common.cuh"
 
+// LJ 6-12 parameters and the real-space Ewald splitting (EleDir::
+// applyInteractionCalPotential, RE/src/EleDir.cpp:43-61):
+//   E_ij = q_i q_j erfc(beta r)/r,  F_i = -q_i q_j (erfc(beta r)/r + 2 beta/sqrt(pi) e^{-beta^2 r^2}) / r^2 (r_j - r_i)
 struct LJParams {
-  float eps4f, sig2f, shiftf;
-  double eps4, sig2, shift;
+  float eps4f, sig2f, shiftf, betaf, cbf;
+  double eps4, sig2, shift, beta, cb;  // cb = 2 beta / sqrt(pi)
 };
 
 struct Kahan {
@@ -39,7 +42,7 @@ __device__ __forceinline__ double group_sum(double v) {
 }
 
 // ---------------------------------------------------------------- mixed
-template <int G, bool STATS>
+template <int G, bool STATS, bool COUL>
 __global__ void __launch_bounds__(256)
 k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut,
            const int* __restrict__ list, const int* __restrict__ nnb, int cap,
@@ -51,7 +54,7 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
   const float L0 = st->Lf[0], L1 = st->Lf[1], L2 = st->Lf[2];
   const float I0 = st->Lif[0], I1 = st->Lif[1], I2 = st->Lif[2];
   Kahan fx, fy, fz;
-  float e = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+  float e = 0.f, vx = 0.f, vy = 0.f, vz = 0.f, ec = 0.f;
   if (i < N) {
     const float4 pi = pos[i];
     const float rc = rcut[i];
@@ -91,7 +94,14 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
           const float ri2 = __fdividef(1.0f, r2);
           const float s2 = p.sig2f * ri2;
           const float s6 = s2 * s2 * s2;
-          const float fs = p.eps4f * (6.f * s6 - 12.f * s6 * s6) * ri2;
+          float fs = p.eps4f * (6.f * s6 - 12.f * s6 * s6) * ri2;
+          if (COUL) {
+            const float qq = pi.w * pj[u].w;
+            const float rinv = rsqrtf(r2);
+            const float er = erfcf(p.betaf * r2 * rinv);
+            fs -= qq * (er * rinv + p.cbf * __expf(-p.betaf * p.betaf * r2)) * ri2;
+            if (STATS) ec += qq * er * rinv;
+          }
           bx += fs * dx;
           by += fs * dy;
           bz += fs * dz;
@@ -116,14 +126,15 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
     force[i] = f;
   }
   if (STATS) {
-    double v[4] = {0.5 * (double)e, 0.5 * (double)vx, 0.5 * (double)vy, 0.5 * (double)vz};
-    // the first force term of a step (overwrite) stores the slots, later terms add
-    block_reduce_finish<4>(v, partials, counter, stats, overwrite != 0);
+    // slots NB_ENERGY, VIRIAL_XX..ZZ, ELEC_DIR are contiguous; the first force
+    // term of a step (overwrite) stores them, later terms add
+    double v[5] = {0.5 * (double)e, 0.5 * (double)vx, 0.5 * (double)vy, 0.5 * (double)vz, 0.5 * (double)ec};
+    block_reduce_finish<5>(v, partials, counter, stats, overwrite != 0);
   }
 }
 
 // ---------------------------------------------------------------- FP64
-template <int G, bool STATS>
+template <int G, bool STATS, bool COUL>
 __global__ void __launch_bounds__(256)
 k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcut,
           const int* __restrict__ list, const int* __restrict__ nnb, int cap,
@@ -133,8 +144,7 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
   const int i = t / G;
   const int lane = t & (G - 1);
   const double L0 = st->L[0], L1 = st->L[1], L2 = st->L[2];
-  const double I0 = st->Li[0], I1 = st->Li[1], I2 = st->Li[2];
-  double fx = 0, fy = 0, fz = 0, e = 0, vx = 0, vy = 0, vz = 0;
+  double fx = 0, fy = 0, fz = 0, e = 0, vx = 0, vy = 0, vz = 0, ec = 0;
   if (i < N) {
     const double4a pi = pos[i];
     const double rc = (double)rcut[i];
@@ -167,7 +177,14 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
         const double ri2 = 1.0 / r2;
         const double s2 = p.sig2 * ri2;
         const double s6 = s2 * s2 * s2;
-        const double fs = p.eps4 * (6.0 * s6 - 12.0 * s6 * s6) * ri2;
+        double fs = p.eps4 * (6.0 * s6 - 12.0 * s6 * s6) * ri2;
+        if (COUL) {
+          const double qq = pi.w * pj.w;
+          const double r = sqrt(r2);
+          const double er = erfc(p.beta * r);
+          fs -= qq * (er / r + p.cb * exp(-p.beta * p.beta * r2)) * ri2;
+          if (STATS) ec += qq * er / r;
+        }
         fx += fs * dx;
         fy += fs * dy;
         fz += fs * dz;
@@ -188,9 +205,9 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
     force[i] = f;
   }
   if (STATS) {
-    double v[4] = {0.5 * e, 0.5 * vx, 0.5 * vy, 0.5 * vz};
+    double v[5] = {0.5 * e, 0.5 * vx, 0.5 * vy, 0.5 * vz, 0.5 * ec};
     // the first force term of a step (overwrite) stores the slots, later terms add
-    block_reduce_finish<4>(v, partials, counter, stats, overwrite != 0);
+    block_reduce_finish<5>(v, partials, counter, stats, overwrite != 0);
   }
 }
 
@@ -211,6 +228,11 @@ int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats,
   p.eps4f = (float)p.eps4;
   p.sig2f = (float)p.sig2;
   p.shiftf = (float)p.shift;
+  p.beta = eng->beta;
+  p.cb = 2.0 * eng->beta / sqrt(M_PI);
+  p.betaf = (float)p.beta;
+  p.cbf = (float)p.cb;
+  const bool coul = eng->has_coul;
   int N = sys->N;
   int cap = nl->cap;
   int ow = overwrite ? 1 : 0;
@@ -223,11 +245,23 @@ int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats,
   void* a[] = {&N, &sys->pos, &sys->rcut, &nl->list, &nl->nnb, &cap, &st, &p, &sys->force, &ow,
                &sys->partials, &counter, &stats};
   const void* f;
-  if (sys->prec == MD_PREC_FP64)
-    f = with_stats ? (const void*)k_lj_fp64<kLanes, true> : (const void*)k_lj_fp64<kLanes, false>;
-  else
-    f = with_stats ? (const void*)k_lj_mixed<kLanes, true> : (const void*)k_lj_mixed<kLanes, false>;
+  if (sys->prec == MD_PREC_FP64) {
+    if (coul) f = with_stats ? (const void*)k_lj_fp64<kLanes, true, true> : (const void*)k_lj_fp64<kLanes, false, true>;
+    else f = with_stats ? (const void*)k_lj_fp64<kLanes, true, false> : (const void*)k_lj_fp64<kLanes, false, false>;
+  } else {
+    if (coul) f = with_stats ? (const void*)k_lj_mixed<kLanes, true, true> : (const void*)k_lj_mixed<kLanes, false, true>;
+    else f = with_stats ? (const void*)k_lj_mixed<kLanes, true, false> : (const void*)k_lj_mixed<kLanes, false, false>;
+  }
   return rec_launch(rec, f, grid, dim3(threads), 0, a);
+}
+
+// ElectrostaticInteraction_dir: real-space Ewald with splitting beta inside the
+// non-bonded kernel (same list and per-atom cutoff as the LJ term)
+extern "C" int md_engine_register_coulomb(md_engine* e, double beta) {
+  if (!e || !(beta > 0)) { md_set_error("md_engine_register_coulomb: bad arguments"); return MD_ERR_BADARG; }
+  e->has_coul = true;
+  e->beta = beta;
+  return MD_OK;
 }
 
 // ------------------------------------------------------------------ C ABI

@@ -57,6 +57,7 @@ struct DevState {
   double Mh[3];      // box mass
   double lam1[3], lam2[3]; // scale factors of the two A half steps of this step
   double Pcur[3];    // diagonal pressure at the end of the last step
+  double scratch[8]; // reduction target of multi-slot sums merged afterwards
 };
 
 // host helpers -------------------------------------------------------------
@@ -144,6 +145,8 @@ struct md_engine {
   md_system* sys = nullptr;
   bool has_lj = false;
   double eps = 1, sigma = 1, shift = 0;
+  bool has_coul = false;
+  double beta = 0;
   int n_bonds = 0;
 };
 

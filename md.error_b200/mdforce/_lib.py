@@ -95,6 +95,13 @@ _SIGS = {
     "md_sim_run": (i32, [vp, i32]),
     "md_sim_counters": (i32, [vp, P(i64), P(i64), P(i32)]),
     "md_sim_uses_conditional_graph": (i32, [vp, P(i32)]),
+    "md_engine_register_coulomb": (i32, [vp, f64]),
+    "md_spme_create": (i32, [P(vp), vp, P(i32), i32, f64, i32]),
+    "md_spme_destroy": (i32, [vp]),
+    "md_spme_apply": (i32, [vp, vp, i32]),
+    "md_spme_get_mesh": (i32, [vp, P(f64)]),
+    "md_ewald_self_energy": (i32, [vp, f64, P(f64)]),
+    "md_ewald_exact": (i32, [vp, P(i32), f64, P(f64), i32]),
     "md_sim_attach_adapt_rcut": (i32, [vp, vp, i32, i32, f64, i32]),
     "md_arc_create": (i32, [P(vp), vp, f64, f64, f64, f64]),
     "md_arc_destroy": (i32, [vp]),

@@ -34,9 +34,10 @@ NL_MINIMAGE = 0
 NL_CELLSHIFT = 1
 
 STAT_NB_ENERGY, STAT_VIRIAL_XX, STAT_VIRIAL_YY, STAT_VIRIAL_ZZ = 0, 1, 2, 3
-STAT_KINETIC_XX, STAT_KINETIC_YY, STAT_KINETIC_ZZ = 4, 5, 6
-STAT_PRESSURE_CORR_XX = 7
-STAT_ELEC_DIR, STAT_ELEC_REC, STAT_ELEC_SELF = 10, 11, 12
+STAT_ELEC_DIR = 4
+STAT_KINETIC_XX, STAT_KINETIC_YY, STAT_KINETIC_ZZ = 5, 6, 7
+STAT_PRESSURE_CORR_XX = 8
+STAT_ELEC_REC, STAT_ELEC_SELF = 11, 12
 STAT_COUNT = 16
 
 
@@ -300,6 +301,53 @@ class InteractionEngine:
 
     def applyBondedInteraction(self, sys):
         check(lib.md_engine_apply_bonded(self.h, sys.h), "applyBondedInteraction")
+
+
+def registCoulomb(engine, beta):
+    """Real-space Ewald in the non-bonded kernel (ElectrostaticInteraction_dir)."""
+    check(lib.md_engine_register_coulomb(engine.h, float(beta)), "registCoulomb")
+
+
+class SPME:
+    """Reciprocal SPME on the device: ElectrostaticInteraction_rec_BSpline (method 'ik')
+    or ElectrostaticInteraction_rec_FBSpline (method 'analytic')."""
+
+    def __init__(self, sys, K, order, beta, method="ik"):
+        KK = (C.c_int * 3)(*[int(k) for k in K])
+        h = C.c_void_p()
+        m = {"ik": 0, "analytic": 1}[method]
+        check(lib.md_spme_create(C.byref(h), sys.h, KK, int(order), float(beta), m), "SPME")
+        self.h = h
+        self.sys = sys
+        self.K = tuple(int(k) for k in K)
+        self.beta = beta
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.md_spme_destroy(self.h)
+            self.h = None
+
+    def apply(self, sys=None, with_stats=True):
+        check(lib.md_spme_apply(self.h, (sys or self.sys).h, 1 if with_stats else 0), "SPME::apply")
+
+    def mesh(self):
+        Q = np.empty(self.K, np.float64)
+        check(lib.md_spme_get_mesh(self.h, _p(Q)), "mesh")
+        return Q
+
+
+def ewald_self_energy(sys, beta):
+    v = C.c_double()
+    check(lib.md_ewald_self_energy(sys.h, float(beta), C.byref(v)), "self energy")
+    return v.value
+
+
+def ewald_exact(sys, K, beta, add_forces=True):
+    """Exact reciprocal Ewald sum in FP64 (ElectrostaticInteraction_rec_ES)."""
+    KK = (C.c_int * 3)(*[int(k) for k in K])
+    e = C.c_double()
+    check(lib.md_ewald_exact(sys.h, KK, float(beta), C.byref(e), 1 if add_forces else 0), "ewald_exact")
+    return e.value
 
 
 class AssignRCut:

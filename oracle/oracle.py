@@ -355,3 +355,74 @@ def ref_spme(pos, q, box, beta, K, rcut, method, order):
     lib.ref_spme_forces(n, _p(p, f64), _p(qq, f64), _p(b, f64), beta, _p(KK, i32), rcut, method, order,
                         _p(df, f64), _p(rf, f64), C.byref(e), C.byref(ed), C.byref(er), C.byref(ei))
     return dict(dir=df, rec=rf, energy=e.value, err_dir=ed.value, err_rec=er.value, err_interp=ei.value)
+
+
+# ---------------------------------------------------------------- SPME / Ewald
+_sigs3 = {
+    "orc_bspline_weights": (None, [i32, f64, P(f64), P(f64)]),
+    "orc_bspline": (f64, [i32, f64]),
+    "orc_spme_bmod": (None, [i32, i32, P(f64)]),
+    "orc_spme_spread": (None, [i32, P(f64), P(f64), P(f64), P(i32), i32, P(f64)]),
+    "orc_spme_rec": (f64, [i32, P(f64), P(f64), P(f64), P(i32), i32, f64, i32, P(f64)]),
+    "orc_ewald_rec_exact": (f64, [i32, P(f64), P(f64), P(f64), P(i32), f64, P(f64)]),
+    "orc_ewald_dir": (f64, [i32, P(f64), P(f64), P(f64), f64, f64, P(f64)]),
+    "orc_ewald_self": (f64, [i32, P(f64), f64]),
+}
+for _n, (_r, _a) in _sigs3.items():
+    _f = getattr(_lib, _n)
+    _f.restype = _r
+    _f.argtypes = _a
+
+
+def bspline_weights(n, f):
+    w = np.zeros(n); dw = np.zeros(n)
+    _lib.orc_bspline_weights(n, float(f), _p(w, f64), _p(dw, f64))
+    return w, dw
+
+
+def bspline(n, x):
+    return _lib.orc_bspline(n, float(x))
+
+
+def spme_bmod(n, K):
+    b = np.zeros(K)
+    _lib.orc_spme_bmod(n, K, _p(b, f64))
+    return b
+
+
+def spme_spread(pos, q, box, K, n):
+    p = np.ascontiguousarray(pos, np.float64); qq = np.ascontiguousarray(q, np.float64)
+    b = np.ascontiguousarray(box, np.float64); KK = np.ascontiguousarray(K, np.int32)
+    Q = np.zeros(tuple(K))
+    _lib.orc_spme_spread(p.shape[0], _p(p, f64), _p(qq, f64), _p(b, f64), _p(KK, i32), n, _p(Q, f64))
+    return Q
+
+
+def spme_rec(pos, q, box, K, n, beta, method=0):
+    """reciprocal SPME energy and forces; method 0 ik, 1 analytic differentiation"""
+    p = np.ascontiguousarray(pos, np.float64); qq = np.ascontiguousarray(q, np.float64)
+    b = np.ascontiguousarray(box, np.float64); KK = np.ascontiguousarray(K, np.int32)
+    F = np.zeros_like(p)
+    E = _lib.orc_spme_rec(p.shape[0], _p(p, f64), _p(qq, f64), _p(b, f64), _p(KK, i32), n, beta, method, _p(F, f64))
+    return E, F
+
+
+def ewald_rec_exact(pos, q, box, K, beta):
+    p = np.ascontiguousarray(pos, np.float64); qq = np.ascontiguousarray(q, np.float64)
+    b = np.ascontiguousarray(box, np.float64); KK = np.ascontiguousarray(K, np.int32)
+    F = np.zeros_like(p)
+    E = _lib.orc_ewald_rec_exact(p.shape[0], _p(p, f64), _p(qq, f64), _p(b, f64), _p(KK, i32), beta, _p(F, f64))
+    return E, F
+
+
+def ewald_dir(pos, q, box, beta, rcut):
+    p = np.ascontiguousarray(pos, np.float64); qq = np.ascontiguousarray(q, np.float64)
+    b = np.ascontiguousarray(box, np.float64)
+    F = np.zeros_like(p)
+    E = _lib.orc_ewald_dir(p.shape[0], _p(p, f64), _p(qq, f64), _p(b, f64), beta, rcut, _p(F, f64))
+    return E, F
+
+
+def ewald_self(q, beta):
+    qq = np.ascontiguousarray(q, np.float64)
+    return _lib.orc_ewald_self(len(qq), _p(qq, f64), beta)

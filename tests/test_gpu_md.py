@@ -229,7 +229,7 @@ def test_langevin_temperature(mdf, fluid):
     for _ in range(40):
         sim.run(25)
         st = sys.stats()
-        Ts.append(2 * st[4:7].sum() / (3 * sys.n))
+        Ts.append(2 * st[mdf.STAT_KINETIC_XX:mdf.STAT_KINETIC_XX + 3].sum() / (3 * sys.n))
     T = np.mean(Ts)
     # BAOAB kinetic temperature is exact for harmonic forces and O(dt^2) here
     assert abs(T - 1.0) < 0.02, T

@@ -1,0 +1,151 @@
+"""GPU tests of the electrostatics path through the C ABI: SPME charge mesh,
+ik and analytic reciprocal forces/energies, real-space Ewald, self energy and
+the FP64 exact Ewald sum, each against the CPU oracle (pinned to the
+reference's own EleRecBSpline / EleRecFBSpline / EleRecES / EleDir built from
+its sources, tests/test_spme_oracle.py), plus the charged-fluid benchmark
+system (20736 charges, 64^3, order 6, beta 0.95) against an FP64 Ewald
+reference."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL = {0: 2e-5, 1: 1e-10}  # relative RMS force error, mixed / FP64
+
+
+def rel_rms(a, b):
+    return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+
+
+@pytest.fixture(scope="module")
+def small():
+    rng = np.random.default_rng(0)
+    n, L = 300, 9.0
+    pos = rng.uniform(0, L, (n, 3))
+    q = np.where(np.arange(n) < n // 2, 1.0, -1.0)
+    rng.shuffle(q)
+    return pos, q, np.array([L, L, L])
+
+
+def make(mdf, pos, q, box, prec):
+    sys = mdf.MDSystem(pos, box, charge=q, precision=prec)
+    return sys
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_spread_mesh(mdf, orc, small, prec):
+    pos, q, box = small
+    sys = make(mdf, pos, q, box, prec)
+    sp = mdf.SPME(sys, (16, 16, 32), 6, 1.3)
+    sys.clear_stats()
+    sp.apply()
+    Q = sp.mesh()
+    Qo = orc.spme_spread(pos, q, box, (16, 16, 32), 6)
+    assert np.abs(Q - Qo).max() < (1e-5 if prec == 0 else 1e-12)
+
+
+@pytest.mark.parametrize("method", ["ik", "analytic"])
+@pytest.mark.parametrize("prec", [0, 1])
+def test_reciprocal_forces_and_energy(mdf, orc, small, prec, method):
+    pos, q, box = small
+    K, order, beta = (16, 16, 32), 6, 1.3
+    sys = make(mdf, pos, q, box, prec)
+    sp = mdf.SPME(sys, K, order, beta, method)
+    eng = mdf.InteractionEngine(sys)
+    eng.clearInteraction()
+    sys.clear_stats()
+    sp.apply()
+    F = sys.forces()
+    E = sys.stats()[mdf.STAT_ELEC_REC]
+    Eo, Fo = orc.spme_rec(pos, q, box, K, order, beta, 0 if method == "ik" else 1)
+    assert rel_rms(F, Fo) < TOL[prec]
+    assert abs(E - Eo) < 1e-6 * abs(Eo) + (1e-12 if prec else 1e-6)
+
+
+def test_reciprocal_matches_reference_build(mdf, orc, small):
+    if not orc.ref_available("libref_spme.so"):
+        pytest.skip("reference SPME not built")
+    pos, q, box = small
+    sys = make(mdf, pos, q, box, 1)
+    for method, m in (("ik", 0), ("analytic", 1)):
+        sp = mdf.SPME(sys, (16, 16, 16), 6, 1.5, method)
+        eng = mdf.InteractionEngine(sys)
+        eng.clearInteraction()
+        sys.clear_stats()
+        sp.apply()
+        ref = orc.ref_spme(sys.positions(), q, box, 1.5, (16, 16, 16), 4.0, m, 6)
+        assert rel_rms(sys.forces(), ref["rec"]) < 1e-10
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_real_space_and_self(mdf, orc, small, prec):
+    pos, q, box = small
+    beta, rc = 1.3, 4.0
+    sys = make(mdf, pos, q, box, prec)
+    sys.set_rcut(np.full(len(q), rc, np.float32))
+    eng = mdf.InteractionEngine(sys)
+    eng.registNonBondedInteraction(0.0, 1.0, 0.0)  # LJ off (eps = 0)
+    mdf.registCoulomb(eng, beta)
+    cl = mdf.CellList(sys, rc + 0.3)
+    cl.rebuild()
+    nl = mdf.NeighborList(sys, rc + 0.3, 0.3, expansion=3.0)
+    nl.fit(sys, cl)
+    eng.clearInteraction()
+    sys.clear_stats()
+    eng.applyNonBondedInteraction(sys, nl, with_stats=True)
+    F = sys.forces()
+    E = sys.stats()[mdf.STAT_ELEC_DIR]
+    gp = sys.positions()
+    Eo, Fo = orc.ewald_dir(gp, q, box, beta, rc)
+    assert rel_rms(F, Fo) < TOL[prec]
+    assert abs(E - Eo) < (1e-5 if prec == 0 else 1e-10) * abs(Eo)
+    es = mdf.ewald_self_energy(sys, beta)
+    assert abs(es - orc.ewald_self(q, beta)) < 1e-10 * abs(es)
+
+
+def test_exact_ewald_fp64(mdf, orc, small):
+    pos, q, box = small
+    sys = make(mdf, pos, q, box, 1)
+    eng = mdf.InteractionEngine(sys)
+    eng.clearInteraction()
+    E = mdf.ewald_exact(sys, (10, 10, 10), 1.3)
+    Eo, Fo = orc.ewald_rec_exact(sys.positions(), q, box, (10, 10, 10), 1.3)
+    assert abs(E - Eo) < 1e-11 * abs(Eo)
+    assert rel_rms(sys.forces(), Fo) < 1e-11
+
+
+@pytest.mark.slow
+def test_charged_fluid_against_fp64_ewald(mdf):
+    """20736 +-1 charges, 30^3 box, mesh 64^3, order 6, beta 0.95, real-space
+    rc 3.0, ik: the mixed path against FP64 real space (rc = 14.9, all pairs)
+    plus the exact reciprocal sum (|m| <= 39, truncation < 1e-12)."""
+    s = mdf.systems.charged_fluid()
+    beta, K, order = 0.95, (64, 64, 64), 6
+    out = {}
+    for prec, rc, spme in ((0, 3.0, True), (1, 14.9, False)):
+        sys = mdf.MDSystem(s.pos, s.box, charge=s.charge, precision=prec)
+        sys.set_rcut(np.full(s.n, rc, np.float32))
+        eng = mdf.InteractionEngine(sys)
+        eng.registNonBondedInteraction(0.0, 1.0, 0.0)
+        mdf.registCoulomb(eng, beta)
+        cl = mdf.CellList(sys, 3.3)
+        cl.rebuild()
+        nl = mdf.NeighborList(sys, rc + 0.3, 0.3, expansion=1.2)
+        nl.fit(sys, cl)
+        eng.clearInteraction()
+        sys.clear_stats()
+        eng.applyNonBondedInteraction(sys, nl, with_stats=True)
+        if spme:
+            mdf.SPME(sys, K, order, beta, "ik").apply()
+            e_rec = sys.stats()[mdf.STAT_ELEC_REC]
+        else:
+            e_rec = mdf.ewald_exact(sys, (78, 78, 78), beta)
+        st = sys.stats()
+        out[prec] = (sys.forces(), st[mdf.STAT_ELEC_DIR] + e_rec + mdf.ewald_self_energy(sys, beta))
+    F, E = out[0]
+    Fo, Eo = out[1]
+    err = float(np.sqrt(((F - Fo) ** 2).sum(1).mean()))
+    # real-space truncation at 3.0 plus SPME interpolation: a-priori ~1e-3 for
+    # these parameters (errorEstimatePME / rec_BSpline::errorEstimate)
+    assert err < 5e-3, err
+    assert abs(E - Eo) / abs(Eo) < 1e-3

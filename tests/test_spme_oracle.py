@@ -1,0 +1,74 @@
+"""CPU tests of the electrostatics oracle: B-spline basics, and ik / analytic
+SPME, exact Ewald and real-space Ewald against the reference's own
+ElectrostaticInteraction built from its sources (oracle/_ref/libref_spme.so),
+on the same seeded inputs."""
+import numpy as np
+import pytest
+
+
+def test_bspline_partition_of_unity_and_derivative(orc):
+    for n in (2, 4, 6, 8):
+        for f in (0.0, 0.13, 0.5, 0.91):
+            w, dw = orc.bspline_weights(n, f)
+            assert abs(w.sum() - 1.0) < 1e-14
+            assert abs(dw.sum()) < 1e-13
+            # derivative against a central difference of M_n (off the knots, where
+            # M_2' jumps)
+            h = 1e-6
+            for j in range(n if f > 0 else 0):
+                x = f + j
+                fd = (orc.bspline(n, x + h) - orc.bspline(n, x - h)) / (2 * h) if 0 < x - h and x + h < n else None
+                if fd is not None:
+                    assert abs(dw[j] - fd) < 1e-6
+
+
+def test_bspline_order4_closed_form(orc):
+    # M_4 on [0,1): x^3/6
+    for x in (0.1, 0.5, 0.9):
+        assert abs(orc.bspline(4, x) - x ** 3 / 6) < 1e-15
+
+
+@pytest.fixture(scope="module")
+def charges():
+    rng = np.random.default_rng(0)
+    n, L = 200, 8.0
+    pos = rng.uniform(0, L, (n, 3))
+    q = np.where(np.arange(n) < n // 2, 1.0, -1.0)
+    return pos, q, np.array([L, L, L])
+
+
+@pytest.mark.parametrize("K,order,method", [((16, 16, 16), 6, 0), ((16, 16, 15), 4, 0), ((15, 15, 15), 6, 0),
+                                            ((16, 12, 20), 6, 1), ((16, 16, 16), 8, 0)])
+def test_spme_oracle_matches_reference_build(orc, charges, K, order, method):
+    if not orc.ref_available("libref_spme.so"):
+        pytest.skip("reference SPME not built (needs the reference tree at build time)")
+    pos, q, box = charges
+    ref = orc.ref_spme(pos, q, box, 1.5, K, 3.5, method, order)
+    E, F = orc.spme_rec(pos, q, box, K, order, 1.5, method)
+    Ed, Fd = orc.ewald_dir(pos, q, box, 1.5, 3.5)
+    Es = orc.ewald_self(q, 1.5)
+    tol = 1e-9 if order == 8 else 1e-11  # the reference evaluates M_8 from polynomial tables
+    assert np.abs(F - ref["rec"]).max() < tol * np.abs(F).max() * 10
+    assert np.abs(Fd - ref["dir"]).max() < 1e-12
+    assert abs(E + Ed + Es - ref["energy"]) < tol * abs(ref["energy"]) * 10
+
+
+def test_exact_ewald_oracle_matches_reference_build(orc, charges):
+    if not orc.ref_available("libref_spme.so"):
+        pytest.skip("reference SPME not built")
+    pos, q, box = charges
+    ref = orc.ref_spme(pos, q, box, 1.5, (10, 10, 10), 3.5, 2, 6)
+    E, F = orc.ewald_rec_exact(pos, q, box, (10, 10, 10), 1.5)
+    Ed, _ = orc.ewald_dir(pos, q, box, 1.5, 3.5)
+    assert np.abs(F - ref["rec"]).max() < 1e-12
+    assert abs(E + Ed + orc.ewald_self(q, 1.5) - ref["energy"]) < 1e-11 * abs(ref["energy"])
+
+
+def test_spme_converges_to_exact_ewald(orc, charges):
+    pos, q, box = charges
+    Ee, Fe = orc.ewald_rec_exact(pos, q, box, (24, 24, 24), 1.5)
+    errs = []
+    for K in (16, 32):
+        E, F = orc.spme_rec(pos, q, box, (K, K, K), 6, 1.5, 0)
+        errs.append(np.sqrt(((F - Fe) ** 2).sum(1).mean()))
+    assert errs[1] < errs[0] / 20
