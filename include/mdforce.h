@@ -209,6 +209,18 @@ int md_ewald_self_energy(md_system* sys, double beta, double* out);
    RE/src/EleRecES.cpp:49-144): energy, and the forces added when add_forces != 0. */
 int md_ewald_exact(md_system* sys, const int K[3], double beta, double* energy, int add_forces);
 
+/* ------------------------------------------------------------ error estimates
+ * ElectrostaticInteraction::errorEstimatePME (RE/src/ElectrostaticInteraction.cpp:349-401):
+ * real-space and Ewald-truncation estimates with c2 = sum q^2 of the system; FP64 sums
+ * on the device. */
+int md_error_estimate_pme(md_system* sys, const int K[3], double beta, double rcut, double* err_dir,
+                          double* err_rec);
+/* ElectrostaticInteraction_rec_BSpline::errorEstimate (RE/src/EleRecBSpline.cpp:154-206):
+ * homogeneous ik-SPME interpolation error for B-spline order `order`. */
+int md_error_estimate_spme_ik(md_system* sys, const int K[3], int order, double beta, double* err);
+/* splitting beta whose real-space estimate equals target at cutoff rcut */
+int md_choose_beta(md_system* sys, double rcut, double target, double* beta);
+
 /* ------------------------------------------------------- per-atom cutoff
  * Replaces AssignRCut::getRCut + assign (ENG/src/AssignRCut.cu:46-117):
  * rcut_i = lattice[iz + nz*(iy + ny*ix)], ix = int((x*nx)/Lx) etc. (binary32). */

@@ -350,6 +350,28 @@ def ewald_exact(sys, K, beta, add_forces=True):
     return e.value
 
 
+def errorEstimatePME(sys, K, beta, rcut):
+    """(err_dir, err_rec) of ElectrostaticInteraction::errorEstimatePME."""
+    KK = (C.c_int * 3)(*[int(k) for k in K])
+    d, r = C.c_double(), C.c_double()
+    check(lib.md_error_estimate_pme(sys.h, KK, float(beta), float(rcut), C.byref(d), C.byref(r)), "errorEstimatePME")
+    return d.value, r.value
+
+
+def errorEstimateInterpolRec(sys, K, order, beta):
+    """ik-SPME interpolation estimate of ElectrostaticInteraction_rec_BSpline::errorEstimate."""
+    KK = (C.c_int * 3)(*[int(k) for k in K])
+    e = C.c_double()
+    check(lib.md_error_estimate_spme_ik(sys.h, KK, int(order), float(beta), C.byref(e)), "errorEstimate")
+    return e.value
+
+
+def choose_beta(sys, rcut, target):
+    b = C.c_double()
+    check(lib.md_choose_beta(sys.h, float(rcut), float(target), C.byref(b)), "choose_beta")
+    return b.value
+
+
 class AssignRCut:
     """Per-atom cutoff from an rc lattice (AssignRCut::getRCut + assign)."""
 

@@ -426,3 +426,22 @@ def ewald_dir(pos, q, box, beta, rcut):
 def ewald_self(q, beta):
     qq = np.ascontiguousarray(q, np.float64)
     return _lib.orc_ewald_self(len(qq), _p(qq, f64), beta)
+
+
+# ---------------------------------------------------------------- error estimates
+_lib.orc_error_estimate_pme.restype = None
+_lib.orc_error_estimate_pme.argtypes = [P(f64), P(i32), f64, f64, f64, i32, P(f64), P(f64)]
+_lib.orc_error_estimate_spme_ik.restype = f64
+_lib.orc_error_estimate_spme_ik.argtypes = [P(f64), P(i32), i32, f64, f64, i32]
+
+
+def error_estimate_pme(box, K, beta, rcut, c2, natom):
+    b = np.ascontiguousarray(box, np.float64); KK = np.ascontiguousarray(K, np.int32)
+    d, r = f64(), f64()
+    _lib.orc_error_estimate_pme(_p(b, f64), _p(KK, i32), beta, rcut, c2, natom, C.byref(d), C.byref(r))
+    return d.value, r.value
+
+
+def error_estimate_spme_ik(box, K, order, beta, c2, natom):
+    b = np.ascontiguousarray(box, np.float64); KK = np.ascontiguousarray(K, np.int32)
+    return _lib.orc_error_estimate_spme_ik(_p(b, f64), _p(KK, i32), order, beta, c2, natom)

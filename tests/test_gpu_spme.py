@@ -149,3 +149,20 @@ def test_charged_fluid_against_fp64_ewald(mdf):
     # these parameters (errorEstimatePME / rec_BSpline::errorEstimate)
     assert err < 5e-3, err
     assert abs(E - Eo) / abs(Eo) < 1e-3
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_error_estimates_on_device(mdf, orc, small, prec):
+    pos, q, box = small
+    sys = make(mdf, pos, q, box, prec)
+    c2 = float((q * q).sum())
+    for K, order in (((16, 16, 32), 6), ((32, 32, 32), 4)):
+        d, r = mdf.errorEstimatePME(sys, K, 1.3, 4.0)
+        do, ro = orc.error_estimate_pme(box, K, 1.3, 4.0, c2, len(q))
+        assert abs(d - do) < 1e-12 * do and abs(r - ro) < 1e-10 * ro
+        e = mdf.errorEstimateInterpolRec(sys, K, order, 1.3)
+        eo = orc.error_estimate_spme_ik(box, K, order, 1.3, c2, len(q))
+        assert abs(e - eo) < 1e-10 * eo
+    beta = mdf.choose_beta(sys, 4.0, 1e-4)
+    d, _ = mdf.errorEstimatePME(sys, (16, 16, 16), beta, 4.0)
+    assert abs(d - 1e-4) < 1e-9

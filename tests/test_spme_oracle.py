@@ -72,3 +72,17 @@ def test_spme_converges_to_exact_ewald(orc, charges):
         E, F = orc.spme_rec(pos, q, box, (K, K, K), 6, 1.5, 0)
         errs.append(np.sqrt(((F - Fe) ** 2).sum(1).mean()))
     assert errs[1] < errs[0] / 20
+
+
+@pytest.mark.parametrize("K,order", [((16, 16, 16), 6), ((16, 12, 20), 4)])
+def test_error_estimates_match_reference_build(orc, charges, K, order):
+    if not orc.ref_available("libref_spme.so"):
+        pytest.skip("reference SPME not built")
+    pos, q, box = charges
+    ref = orc.ref_spme(pos, q, box, 1.5, K, 3.5, 0, order)
+    c2 = float((q * q).sum())
+    d, r = orc.error_estimate_pme(box, K, 1.5, 3.5, c2, len(q))
+    e = orc.error_estimate_spme_ik(box, K, order, 1.5, c2, len(q))
+    assert abs(d - ref["err_dir"]) <= 1e-14 * ref["err_dir"]
+    assert abs(r - ref["err_rec"]) <= 1e-13 * ref["err_rec"]
+    assert abs(e - ref["err_interp"]) <= 1e-13 * ref["err_interp"]
