@@ -27,7 +27,21 @@ struct LvDev {
 
 // Start of a step, one thread: rebuild accounting and flag reset, step
 // counter, and the box part of B(dt/2) A(dt/2) O(dt) A(dt/2).
-__device__ void box_advance(DevState* st, const LvDev& p) {
+__device__ void box_commit(DevState* st) {
+  if (!st->box_pending) return;
+  for (int d = 0; d < 3; ++d) {
+    st->L[d] = st->Lnext[d];
+    st->Li[d] = 1.0 / st->Lnext[d];
+    st->Lf[d] = (float)st->Lnext[d];
+    st->Lif[d] = 1.0f / st->Lf[d];
+  }
+  st->box_pending = 0;
+}
+
+// commit = false: the new box waits in Lnext until the particles of the step
+// are moved (k_lv_step1 commits it), so the box read between steps always
+// matches the positions
+__device__ void box_advance(DevState* st, const LvDev& p, bool commit) {
   const unsigned f = st->flags;
   if (f & FLAG_REBUILD) st->rebuilds += 1ull;
   // a forced rebuild (new cutoff lattice) becomes this step's rebuild
@@ -38,6 +52,7 @@ __device__ void box_advance(DevState* st, const LvDev& p) {
   for (int d = 0; d < 3; ++d) { st->lam1[d] = 1.0; st->lam2[d] = 1.0; }
   if (!p.dirs) return;
   const double V = st->L[0] * st->L[1] * st->L[2];
+  for (int d = 0; d < 3; ++d) st->Lnext[d] = st->L[d];
   for (int d = 0; d < 3; ++d) {
     if (!(p.dirs & (1 << d))) continue;
     const double A = V / st->L[d];
@@ -51,14 +66,13 @@ __device__ void box_advance(DevState* st, const LvDev& p) {
     st->lam1[d] = L1 / L0;
     st->lam2[d] = L2 / L1;
     st->ph[d] = ph;
-    st->L[d] = L2;
-    st->Li[d] = 1.0 / L2;
-    st->Lf[d] = (float)L2;
-    st->Lif[d] = 1.0f / st->Lf[d];
+    st->Lnext[d] = L2;
   }
+  st->box_pending = 1;
+  if (commit) box_commit(st);
 }
 
-__global__ void k_lv_box(DevState* st, LvDev p) { box_advance(st, p); }
+__global__ void k_lv_box(DevState* st, LvDev p) { box_advance(st, p, true); }
 
 // Particle part of B(dt/2) A(dt/2) O(dt) A(dt/2) and the rebuild test.  With
 // use_cond the last block to finish writes the rebuild decision into the CUDA
@@ -79,20 +93,22 @@ k_lv_step1(int N, typename V4<R>::T* __restrict__ pos, typename V4<R>::T* __rest
            cudaGraphConditionalHandle cond, int use_cond) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < N) lv_particle_step1<R>(k, pos, vel, force, id, backup, st, p);
-  if (use_cond) {
-    __shared__ bool last;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      __threadfence();
-      last = atomicAdd(&st->red_counter[RED_DISP], 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (last && threadIdx.x == 0) {
-      __threadfence();
-      const unsigned f = atomicOr(&st->flags, 0u);
-      cudaGraphSetConditional(cond, (f & FLAG_REBUILD) ? 1u : 0u);
-      st->red_counter[RED_DISP] = 0u;
-    }
+  // the last block to finish (every other block is done reading the box)
+  // commits the box of this step and hands the rebuild decision to the graph
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(&st->red_counter[RED_DISP], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    box_commit(st);
+    const unsigned f = atomicOr(&st->flags, 0u);
+    if (use_cond) cudaGraphSetConditional(cond, (f & FLAG_REBUILD) ? 1u : 0u);
+    st->red_counter[RED_DISP] = 0u;
+    __threadfence();
   }
 }
 
@@ -176,7 +192,7 @@ k_lv_step2(int N, typename V4<R>::T* __restrict__ vel, const double4a* __restric
       st->Pcur[d] = 2.0 / V * (K - 0.5 * W) + st->stats[MD_STAT_PRESSURE_CORR_XX + d];
       if (kick && (p.dirs & (1 << d))) st->ph[d] += 0.5 * p.dt * V / st->L[d] * (st->Pcur[d] - p.pref[d]);
     }
-    if (advance) box_advance(st, p);
+    if (advance) box_advance(st, p, false);
   }
 }
 

@@ -58,6 +58,9 @@ struct DevState {
   double lam1[3], lam2[3]; // scale factors of the two A half steps of this step
   double Pcur[3];    // diagonal pressure at the end of the last step
   double scratch[8]; // reduction target of multi-slot sums merged afterwards
+  double Lnext[3];   // box of the next step, committed by that step's first kernel
+  int box_pending;
+  int pad1;
 };
 
 // host helpers -------------------------------------------------------------
