@@ -218,6 +218,14 @@ int md_error_estimate_pme(md_system* sys, const int K[3], double beta, double rc
 /* ElectrostaticInteraction_rec_BSpline::errorEstimate (RE/src/EleRecBSpline.cpp:154-206):
  * homogeneous ik-SPME interpolation error for B-spline order `order`. */
 int md_error_estimate_spme_ik(md_system* sys, const int K[3], int order, double beta, double* err);
+/* Same estimate as md_error_estimate_spme_ik without allocating device memory, for
+ * callers that reserve all device memory in their own pool or must keep the stream
+ * allocator from growing between steps. No counterpart in the reference. Its scratch
+ * is one fixed 180 KiB array per device: meshes up to K0*K1*K2 = 4,194,304 points
+ * (larger ones give MD_ERR_BADARG); the first call on a device looks the array up
+ * and should come before any stream capture; calls that overlap in time on one
+ * device race on the shared scratch. */
+int md_error_estimate_spme_ik_noalloc(md_system* sys, const int K[3], int order, double beta, double* err);
 /* splitting beta whose real-space estimate equals target at cutoff rcut */
 int md_choose_beta(md_system* sys, double rcut, double target, double* beta);
 

@@ -5,6 +5,7 @@
 //   ElectrostaticInteraction_rec_BSpline::errorEstimate    RE/src/EleRecBSpline.cpp:154-206
 //   EleEcalculator (produce4Item)                          RE/src/EleEcalculator.cpp:100-220
 #include <cmath>
+#include <mutex>
 #include <vector>
 #include "device_common.cuh"
 
@@ -141,6 +142,87 @@ extern "C" int md_error_estimate_spme_ik(md_system* sys, const int K[3], int ord
   MD_CUDA(cudaFreeAsync(tab, sys->stream));
   DevState hs;
   if (int r = sys->read_state(hs)) return r;
+  *err = sqrt(hs.scratch[6] * c2 * c2 / (double)sys->N);
+  return MD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// md_error_estimate_spme_ik_noalloc: the ik-SPME interpolation estimate above,
+// computed by the same kernel, without any device allocation. The estimate is
+// re-evaluated whenever a barostat changes the box or a tuner tries another
+// mesh; a caller that reserves all device memory up front in its own pool, or
+// that must keep the stream-ordered allocator from growing between steps,
+// cannot let each evaluation allocate its aliasing tables and per-block
+// partial sums. This variant takes both from one fixed scratch array per
+// device instead:
+//   [0, 3*1025)            e1 tables of the three axes
+//   [3*1025, 6*1025)       e2 tables
+//   [6*1025, +max_blocks)  one partial sum per block of k_est_spme_ik
+// Nothing in it has to start at zero: the tables are rewritten by every call
+// and each block writes its own partial before the last block reads it (the
+// completion counter is the system's, reset by that last block). Meshes are
+// limited to K0*K1*K2 <= EST_NOALLOC_MAX_BLOCKS * 256 = 4,194,304 points
+// (160^3 fits; 256^3 does not) and larger ones are rejected with
+// MD_ERR_BADARG. All calls on one device share the scratch: two calls that
+// overlap in time (different streams or host threads on one device) race and
+// return wrong estimates; calls issued one after the other are safe.
+constexpr int EST_TAB = 3 * 1025;
+constexpr int EST_NOALLOC_MAX_BLOCKS = 16384;
+constexpr int EST_NOALLOC_MAX_DEVICES = 64;
+static __device__ __align__(256) double g_est_scratch[2 * EST_TAB + EST_NOALLOC_MAX_BLOCKS];  // 180 KiB
+
+// Device address of g_est_scratch on `device`, looked up once per device with
+// that device current (the first call on a device does this setup, so it
+// should come before any stream capture that includes the entry point).
+static int est_scratch(int device, double** out) {
+  static std::mutex mu;
+  static double* addr[EST_NOALLOC_MAX_DEVICES] = {};
+  if (device < 0 || device >= EST_NOALLOC_MAX_DEVICES) {
+    md_set_error("device %d outside the %d devices the estimate scratch supports", device, EST_NOALLOC_MAX_DEVICES);
+    return MD_ERR_BADARG;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[device]) {
+    int prev = 0;
+    MD_CUDA(cudaGetDevice(&prev));
+    MD_CUDA(cudaSetDevice(device));
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_est_scratch);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) return md_cuda_fail(e, "cudaGetSymbolAddress(g_est_scratch)");
+    addr[device] = (double*)p;
+  }
+  *out = addr[device];
+  return MD_OK;
+}
+
+extern "C" int md_error_estimate_spme_ik_noalloc(md_system* sys, const int K[3], int order, double beta,
+                                                 double* err) {
+  if (!sys || !K || !err || order < 2 || !(beta > 0)) return MD_ERR_BADARG;
+  for (int d = 0; d < 3; ++d)
+    if (K[d] < 2 || K[d] > 1024) { md_set_error("mesh size out of range"); return MD_ERR_BADARG; }
+  const long n = (long)K[0] * K[1] * K[2];
+  const long nb = (n + 255) / 256;
+  if (nb > EST_NOALLOC_MAX_BLOCKS) {
+    md_set_error("mesh %dx%dx%d has %ld points; the allocation-free estimate handles at most %d",
+                 K[0], K[1], K[2], n, EST_NOALLOC_MAX_BLOCKS * 256);
+    return MD_ERR_BADARG;
+  }
+  double* scratch = nullptr;
+  if (int r = est_scratch(sys->device, &scratch)) return r;
+  double c2;
+  if (int r = charge_sq(sys, &c2)) return r;
+  std::vector<double> tab(2 * EST_TAB, 0.0);
+  for (int d = 0; d < 3; ++d)
+    for (int m = -K[d] / 2; m <= K[d] / 2; ++m)
+      ecal(2 * M_PI * m / (double)K[d], order, tab[d * 1025 + m + K[d] / 2], tab[EST_TAB + d * 1025 + m + K[d] / 2]);
+  MD_CUDA(cudaMemcpyAsync(scratch, tab.data(), sizeof(double) * 2 * EST_TAB, cudaMemcpyHostToDevice, sys->stream));
+  k_est_spme_ik<<<(int)nb, 256, 0, sys->stream>>>(K[0], K[1], K[2], beta, scratch, scratch + EST_TAB, sys->st,
+                                                  scratch + 2 * EST_TAB, &sys->st->red_counter[RED_MISC],
+                                                  &sys->st->scratch[6]);
+  MD_CHECK_LAUNCH("est spme (no alloc)");
+  DevState hs;
+  if (int r = sys->read_state(hs)) return r;  // also keeps tab alive until the copy is done
   *err = sqrt(hs.scratch[6] * c2 * c2 / (double)sys->N);
   return MD_OK;
 }
