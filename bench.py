@@ -41,6 +41,10 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--equil", type=int, default=4000,
                     help="untimed NVT relaxation steps of the random start")
+    ap.add_argument("--launch", default="graph", choices=["graph", "direct"],
+                    help="direct: launch each step's kernels on the stream instead of one CUDA graph "
+                         "(rebuild kernels gated on the device flag); for profilers that do not "
+                         "descend into conditional graph nodes")
     return ap.parse_args()
 
 
@@ -112,6 +116,20 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+def profiled_traffic(kernel):
+    """DRAM bytes (read + write) per launch of `kernel` from its committed ncu
+    summary under profiles/, or None when there is none."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_slab65536.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 def build_slab(mdf):
     s = mdf.systems.lj_slab()
     return s
@@ -122,7 +140,7 @@ TARGET_PREC = 0.02      # targetPrec of ENG/app/lj.nhc-xtc.cu:57
 SAMPLE_EVERY, UPDATE_EVERY = 40, 2000  # densityProfileSamplingFeq, rcutUpdateFeq (:49-51)
 
 
-def make_sim(mdf, s, prec, lattice, seed=1, npt=True, gamma=1.0, adaptive=True):
+def make_sim(mdf, s, prec, lattice, seed=1, npt=True, gamma=1.0, adaptive=True, use_graph=True):
     sys_ = mdf.MDSystem(s.pos, s.box, vel=s.vel, precision=prec)
     if lattice is None:
         sys_.set_rcut(np.full(s.n, RC_MIN, np.float32))
@@ -133,7 +151,7 @@ def make_sim(mdf, s, prec, lattice, seed=1, npt=True, gamma=1.0, adaptive=True):
     lv = mdf.langevin_params(dt=DT, temperature=TEMP, gamma_t=gamma, tau_p=2.0 if npt else 0.0,
                              kappa_t=0.1 if npt else 0.0, p_ref=(0.0, 0.0, 0.0),
                              npt_dirs=4 if npt else 0, seed=seed)
-    sim = mdf.Simulation(sys_, eng, skin=SKIN, cell_size=2.8, lv=lv, expansion=1.5, use_graph=True,
+    sim = mdf.Simulation(sys_, eng, skin=SKIN, cell_size=2.8, lv=lv, expansion=1.5, use_graph=use_graph,
                          max_rcut=RC_MAX)
     if adaptive:
         arc = mdf.AdaptRCutEstimator(sys_, refh=1.0, rcmin=RC_MIN, rcmax=RC_MAX, rcstep=RC_STEP)
@@ -168,10 +186,14 @@ def equilibrate(mdf, s, nsteps):
     return out, lattice, info
 
 
-def time_steps(torch, sim, stream, steps, flush):
-    """Per-step CUDA-event timing; L2 is flushed between timed steps."""
+def time_steps(torch, sim, stream, steps, flush, nvtx_range=None):
+    """Per-step CUDA-event timing; L2 is flushed between timed steps.  The loop
+    is wrapped in an NVTX range when one is named, so that a profiler can be
+    restricted to the timed launches (ncu --nvtx --nvtx-include <name>/)."""
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     torch.cuda.synchronize()
+    if nvtx_range:
+        torch.cuda.nvtx.range_push(nvtx_range)
     with torch.cuda.stream(stream):
         for a, b in ev:
             flush.zero_()
@@ -179,6 +201,8 @@ def time_steps(torch, sim, stream, steps, flush):
             sim.run(1)
             b.record(stream)
     torch.cuda.synchronize()
+    if nvtx_range:
+        torch.cuda.nvtx.range_pop()
     return sum(a.elapsed_time(b) for a, b in ev) / 1e3
 
 
@@ -254,8 +278,6 @@ def run_reference(args):
     # bounded sample: estimate one step, cap the whole run at ~150 s
     sps0, cores, _ = cpu_baseline(s, lattice, 3)
     budget_steps = max(3, min(args.steps, int(150 * sps0)))
-    for _ in range(1):
-        pass
     sps, cores, out = cpu_baseline(s, lattice, budget_steps)
     line = {
         "impl": "reference", "metric": METRIC, "value": sps, "unit": "steps/s", "n_gpus": args.gpus,
@@ -291,7 +313,8 @@ def main():
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
     # ---- mixed precision path (the headline value)
-    sys_m, eng_m, sim_m = make_sim(mdf, s, 0, lattice, seed=1 + rank)
+    use_graph = args.launch == "graph"
+    sys_m, eng_m, sim_m = make_sim(mdf, s, 0, lattice, seed=1 + rank, use_graph=use_graph)
     sys_m.set_stream(stream.cuda_stream)
     sim_m.run(args.warmup)
     torch.cuda.synchronize()
@@ -300,7 +323,7 @@ def main():
     torch.cuda.synchronize()
     _, rebuilds0, _ = sim_m.counters()
     with Clocks(local) as clk:
-        t_mixed = time_steps(torch, sim_m, stream, args.steps, flush)
+        t_mixed = time_steps(torch, sim_m, stream, args.steps, flush, nvtx_range="timed")
     steps_done, rebuilds, flags = sim_m.counters()
     rebuilds_timed = rebuilds - rebuilds0
     t_max = t_mixed
@@ -324,7 +347,7 @@ def main():
     # ---- FP64 path, same steps
     fp64_sps = None
     if not args.no_fp64:
-        sys_d, eng_d, sim_d = make_sim(mdf, s, 1, lattice, seed=1 + rank)
+        sys_d, eng_d, sim_d = make_sim(mdf, s, 1, lattice, seed=1 + rank, use_graph=use_graph)
         sys_d.set_stream(stream.cuda_stream)
         sim_d.run(args.warmup)
         t64 = time_steps(torch, sim_d, stream, args.steps, flush)
@@ -372,7 +395,10 @@ def main():
     # list build per rebuild; the density deposit every 40 steps; 3 + 3*3 DFT
     # passes + 7 element-wise kernels per cutoff update (every 2000 steps)
     n_updates = (args.warmup + args.steps) // UPDATE_EVERY - args.warmup // UPDATE_EVERY
-    launches = (3 * args.steps + 7 * rebuilds_timed + args.steps // SAMPLE_EVERY + 22 * n_updates)
+    # (direct launch: the 7 rebuild kernels are launched every step and return
+    # early unless the device flag asks for a rebuild)
+    rebuild_launches = 7 * (rebuilds_timed if use_graph else args.steps)
+    launches = (3 * args.steps + rebuild_launches + args.steps // SAMPLE_EVERY + 22 * n_updates)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         n_cpu = 30
@@ -397,7 +423,8 @@ def main():
             "force_rms_err_vs_fp64": {"abs": rms_abs, "rel": rms_rel},
             "list_rebuilds": rebuilds, "tau_per_day": value / world * DT * 86400,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "kernel": "k_lj_mixed",
+                         "frac": achieved / peak, "traffic": profiled_traffic("k_lj_mixed"),
+                         "kernel": "k_lj_mixed",
                          "kernel_us": t_lj * 1e6, "alg_bytes": alg_bytes, "peak_kind": peak_kind},
             "e2e": {"value": e2e_sps, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},

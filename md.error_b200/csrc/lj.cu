@@ -42,8 +42,75 @@ __device__ __forceinline__ double group_sum(double v) {
 }
 
 // ---------------------------------------------------------------- mixed
+struct MixedAcc {
+  Kahan fx, fy, fz;
+  float e = 0.f, vx = 0.f, vy = 0.f, vz = 0.f, ec = 0.f;
+};
+
+// One pass of a lane over U list entries k0, k0+G, ..., k0+(U-1)G of row i:
+// all index loads, then all position gathers, then the arithmetic, so that U
+// independent loads are in flight per lane. TAIL: entries at or past n are
+// skipped (only the last pass of a row can reach them).
+// The image shift k L of an entry is read from the 64-entry table `shift`
+// indexed by the entry's six image bits; the table holds the binary32
+// products k_d * L_d (exactly -L_d, +0 or L_d), so d - shift is the same
+// binary32 operation as shortestImage's x -= floorf(x/L + 0.5) L.
+template <int G, int U, bool TAIL, bool STATS, bool COUL>
+__device__ __forceinline__ void lj_pass_mixed(int k0, int n, const int* __restrict__ row,
+                                              const float4* __restrict__ pos, int i, const float4& pi,
+                                              float rc2, const float4* shift, const LJParams& p,
+                                              MixedAcc& a) {
+  int ee[U];
+  float4 pj[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int kk = k0 + u * G;
+    ee[u] = (!TAIL || kk < n) ? __ldg(row + kk) : -1;
+  }
+#pragma unroll
+  // -1 marks "past the end" (a packed entry never has all six image bits set)
+  for (int u = 0; u < U; ++u) pj[u] = __ldg(pos + ((!TAIL || ee[u] != -1) ? (ee[u] & 0x03FFFFFF) : i));
+  // the U pair forces of this pass are summed in FP32, the pass sum is added
+  // to the lane's Kahan-compensated accumulator
+  float bx = 0.f, by = 0.f, bz = 0.f;
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const float4 sh = shift[(unsigned)ee[u] >> 26];
+    const float dx = __fsub_rn(__fsub_rn(pj[u].x, pi.x), sh.x);
+    const float dy = __fsub_rn(__fsub_rn(pj[u].y, pi.y), sh.y);
+    const float dz = __fsub_rn(__fsub_rn(pj[u].z, pi.z), sh.z);
+    const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    if ((!TAIL || ee[u] != -1) && r2 < rc2) {
+      const float ri2 = __fdividef(1.0f, r2);
+      const float s2 = p.sig2f * ri2;
+      const float s6 = s2 * s2 * s2;
+      // 4 eps (6 s^6 - 12 s^12) / r^2 = (4 eps / r^2) s^6 (6 - 12 s^6)
+      float fs = (p.eps4f * ri2) * s6 * fmaf(-12.f, s6, 6.f);
+      if (COUL) {
+        const float qq = pi.w * pj[u].w;
+        const float rinv = rsqrtf(r2);
+        const float er = erfcf(p.betaf * r2 * rinv);
+        fs -= qq * (er * rinv + p.cbf * __expf(-p.betaf * p.betaf * r2)) * ri2;
+        if (STATS) a.ec += qq * er * rinv;
+      }
+      bx += fs * dx;
+      by += fs * dy;
+      bz += fs * dz;
+      if (STATS) {
+        a.e += fmaf(p.eps4f, fmaf(s6, s6, -s6), p.shiftf);
+        a.vx += fs * dx * dx;
+        a.vy += fs * dy * dy;
+        a.vz += fs * dz * dz;
+      }
+    }
+  }
+  a.fx.add(bx);
+  a.fy.add(by);
+  a.fz.add(bz);
+}
+
 template <int G, bool STATS, bool COUL>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, COUL ? 4 : 5)
 k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut,
            const int* __restrict__ list, const int* __restrict__ nnb, int cap,
            const DevState* __restrict__ st, LJParams p, double4a* __restrict__ force, int overwrite,
@@ -51,10 +118,16 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = t / G;
   const int lane = t & (G - 1);
-  const float L0 = st->Lf[0], L1 = st->Lf[1], L2 = st->Lf[2];
-  const float I0 = st->Lif[0], I1 = st->Lif[1], I2 = st->Lif[2];
-  Kahan fx, fy, fz;
-  float e = 0.f, vx = 0.f, vy = 0.f, vz = 0.f, ec = 0.f;
+  // image shift table: entry c = (k_x+1) | (k_y+1) << 2 | (k_z+1) << 4
+  __shared__ float4 shift[64];
+  if (threadIdx.x < 64) {
+    const unsigned c = threadIdx.x;
+    shift[c] = make_float4(__fmul_rn((float)((int)(c & 3u) - 1), st->Lf[0]),
+                           __fmul_rn((float)((int)((c >> 2) & 3u) - 1), st->Lf[1]),
+                           __fmul_rn((float)((int)(c >> 4) - 1), st->Lf[2]), 0.f);
+  }
+  __syncthreads();
+  MixedAcc a;
   if (i < N) {
     const float4 pi = pos[i];
     const float rc = rcut[i];
@@ -62,63 +135,15 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
     int n = nnb[i];
     n = n < cap ? n : cap;
     const int* row = list + (size_t)i * cap;
-    // U list entries per lane per pass: all index loads, then all position
-    // gathers, then the arithmetic -- U independent loads in flight per lane
     constexpr int U = 4;
-    for (int k0 = lane; k0 < n; k0 += U * G) {
-      int ee[U];
-      float4 pj[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int kk = k0 + u * G;
-        ee[u] = kk < n ? __ldg(row + kk) : -1;
-      }
-#pragma unroll
-      // -1 marks "past the end" (a packed entry never has all six image bits set)
-      for (int u = 0; u < U; ++u) pj[u] = __ldg(pos + (ee[u] != -1 ? (ee[u] & 0x03FFFFFF) : i));
-      // the U pair forces of this batch are summed in FP32, the batch sum is
-      // added to the lane's Kahan-compensated accumulator
-      float bx = 0.f, by = 0.f, bz = 0.f;
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        // d - k L with the image k stored at build time: the same binary32
-        // operations as shortestImage's x -= floorf(x/L + 0.5) L
-        const unsigned code = (unsigned)ee[u] >> 26;
-        const float kx = (float)((int)(code & 3u) - 1), ky = (float)((int)((code >> 2) & 3u) - 1),
-                    kz = (float)((int)(code >> 4) - 1);
-        const float dx = __fsub_rn(__fsub_rn(pj[u].x, pi.x), __fmul_rn(kx, L0));
-        const float dy = __fsub_rn(__fsub_rn(pj[u].y, pi.y), __fmul_rn(ky, L1));
-        const float dz = __fsub_rn(__fsub_rn(pj[u].z, pi.z), __fmul_rn(kz, L2));
-        const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-        if (ee[u] != -1 && r2 < rc2) {
-          const float ri2 = __fdividef(1.0f, r2);
-          const float s2 = p.sig2f * ri2;
-          const float s6 = s2 * s2 * s2;
-          float fs = p.eps4f * (6.f * s6 - 12.f * s6 * s6) * ri2;
-          if (COUL) {
-            const float qq = pi.w * pj[u].w;
-            const float rinv = rsqrtf(r2);
-            const float er = erfcf(p.betaf * r2 * rinv);
-            fs -= qq * (er * rinv + p.cbf * __expf(-p.betaf * p.betaf * r2)) * ri2;
-            if (STATS) ec += qq * er * rinv;
-          }
-          bx += fs * dx;
-          by += fs * dy;
-          bz += fs * dz;
-          if (STATS) {
-            e += p.eps4f * (s6 * s6 - s6) + p.shiftf;
-            vx += fs * dx * dx;
-            vy += fs * dy * dy;
-            vz += fs * dz * dz;
-          }
-        }
-      }
-      fx.add(bx);
-      fy.add(by);
-      fz.add(bz);
-    }
-    (void)I0; (void)I1; (void)I2;
+    int k0 = lane;
+    // passes whose U entries are all inside the row, then at most one ragged pass
+    for (; k0 + (U - 1) * G < n; k0 += U * G)
+      lj_pass_mixed<G, U, false, STATS, COUL>(k0, n, row, pos, i, pi, rc2, shift, p, a);
+    if (k0 < n) lj_pass_mixed<G, U, true, STATS, COUL>(k0, n, row, pos, i, pi, rc2, shift, p, a);
   }
+  Kahan& fx = a.fx; Kahan& fy = a.fy; Kahan& fz = a.fz;
+  const float e = a.e, vx = a.vx, vy = a.vy, vz = a.vz, ec = a.ec;
   double Fx = group_sum<G>(fx.value()), Fy = group_sum<G>(fy.value()), Fz = group_sum<G>(fz.value());
   if (i < N && lane == 0) {
     double4a f = overwrite ? double4a{0, 0, 0, 0} : force[i];
