@@ -113,6 +113,9 @@ int md_system_get_unwrapped_positions(md_system* sys, double* pos);
 int md_system_set_velocities(md_system* sys, const double* vel);
 int md_system_get_velocities(md_system* sys, double* vel);
 int md_system_get_forces(md_system* sys, double* force);
+/* per-atom charges [N] in original order (MDSystem ddata.charge) */
+int md_system_set_charges(md_system* sys, const double* charge);
+int md_system_get_charges(md_system* sys, double* charge);
 int md_system_get_box(md_system* sys, double box[3]);
 int md_system_set_box(md_system* sys, const double box[3]);
 /* per-atom cutoff rcut_i in original order (MDSystem ddata.rcut) */
@@ -203,6 +206,26 @@ int md_spme_destroy(md_spme* spme);
 int md_spme_apply(md_spme* spme, md_system* sys, int with_stats);
 /* the charge mesh Q of the last apply (calQ), [K0][K1][K2] */
 int md_spme_get_mesh(md_spme* spme, double* Q);
+/* Adjoint of the reciprocal SPME energy E = 1/2 sum_m psi(m) |Q^(m)|^2 (the energy of
+ * ElectrostaticInteraction_rec_BSpline, RE/src/EleRecBSpline.cpp:393-536; no gradient
+ * counterpart in the reference).  Recomputes spread and forward transform, then one
+ * inverse transform of psi Q^ = Phi and a gather:
+ *   dE_dq[i]      = sum_k theta_i(k) Phi(k)                    (electrostatic potential)
+ *   dE_dr[i][d]   = q_i sum_k d theta_i(k)/du_d Phi(k) K_d/L_d  (exact gradient, = -F of
+ *                   analytic differentiation whatever the force method)
+ *   dE_dbeta      = sum_m 1/2 |Q^|^2 psi 2 pi^2 |m|^2 / beta^3
+ *   dE_dpsi[t]    = 1/2 |Q^|^2 on the half spectrum [K0][K1][K2/2+1], the interior z
+ *                   planes weighted 2 (each stands for m and -m), 0 at m = 0.
+ * Every output is nullable; host arrays in original atom order; synchronises. */
+int md_spme_energy_grad(md_spme* spme, md_system* sys, double* energy, double* dE_dq,
+                        double* dE_dr, double* dE_dbeta, double* dE_dpsi);
+/* influence function psi on the half spectrum [K0][K1][K2/2+1] (calPsiFPhiF, ik scaling) */
+int md_spme_get_influence(md_spme* spme, double* psi);
+/* Self-force correction of analytic differentiation (SelfCorr::reinit + correction,
+ * RE/src/SelfCorr.cpp:99-220, applied by RE/app/spme.cpp:266-270 for fbspline):
+ * F_id -= sum_{k=1..3} c_d(k) q_i^2 sin(2 pi k K_d x_id / L_d), the c_d(k) from the
+ * aliasing sums of the B-spline of the spme's order; added to the system's forces. */
+int md_spme_self_correction(md_spme* spme, md_system* sys);
 /* -beta/sqrt(pi) sum q^2 (ElectrostaticInteraction.cpp:219-222) into MD_STAT_ELEC_SELF */
 int md_ewald_self_energy(md_system* sys, double beta, double* out);
 /* Exact reciprocal Ewald sum over |m_d| <= K_d/2 in FP64 (ElectrostaticInteraction_rec_ES,
@@ -261,6 +284,46 @@ int md_langevin_step2(md_system* sys);
 /* barostat state: box length velocity and momentum for each direction */
 int md_langevin_get_state(md_system* sys, double* step, double p_h[3]);
 
+/* Nose-Hoover chain of 2 thermostats (NoseHoover_Chains2, ENG/include/Thermostat.h:77-120,
+ * ENG/src/Thermostat.cu:23-304): Q1 = tau_T^2 T 3N/(4 pi^2), Q2 = Q1/(3N), xi = 1, v_xi = 0
+ * at creation; chain arithmetic in FP64 on the device.  remove_com: subtract the
+ * centre-of-mass velocity at the start of every step (TranslationalFreedomRemover). */
+typedef struct md_nhc md_nhc;
+int md_nhc_create(md_nhc** out, md_system* sys, double ref_T, double tau_T, int remove_com);
+int md_nhc_destroy(md_nhc* nhc);
+/* NoseHoover_Chains2::operator_L(dt) on the current velocities; the kinetic tensor of the
+   scaled velocities goes to MD_STAT_KINETIC_* */
+int md_nhc_operator_L(md_nhc* nhc, md_system* sys, double dt, int with_stats);
+/* manual stepping of the lj.nhc-xtc step: step1 = [COM removal] operator_L(dt/2) + VV step1
+   + displacement test (nl nullable); step2 = VV step2 + operator_L(dt/2) */
+int md_nhc_step1(md_nhc* nhc, md_system* sys, md_nlist* nl, double dt);
+int md_nhc_step2(md_nhc* nhc, md_system* sys, double dt);
+/* xi1, xi2, v_xi1, v_xi2 and HamiltonianContribution
+   (Q1 v_xi1^2/2 + Q2 v_xi2^2/2 + 3N T xi1 + T xi2) */
+int md_nhc_get_state(md_nhc* nhc, double out[5]);
+
+/* Isobaric Nose-Hoover chain, isotropic box (NoseHoover_Chains2_Isobaric,
+ * ENG/include/Barostat.h:90-175, ENG/src/Barostat.cu:6-460): Nf = 3N - 3,
+ * Q1 = tau_T^2 T Nf, W = tau_P^2 T Nf, ep = ln(V)/3, vep = 0, xi1 = 1, vxi1 = 0.
+ * The operators are the reference's; the pressure is tr(2/V (K - W_vir/2))/3 +
+ * pressure_corr, from the current kinetic tensor and the virial slots of the last force
+ * evaluation.  The reference composes no step from them; the standard MTK step is
+ * L_CP(dt/2) L_v(dt/2) L_r(dt) L_box(dt) | forces | L_v(dt/2) L_CP(dt/2). */
+typedef struct md_nhc_npt md_nhc_npt;
+int md_nhc_npt_create(md_nhc_npt** out, md_system* sys, double ref_T, double tau_T, double ref_P,
+                      double tau_P, double pressure_corr);
+int md_nhc_npt_destroy(md_nhc_npt* h);
+/* thermostat + barostat propagator L_CP(dt); kinetic tensor after scaling to the stats */
+int md_nhc_npt_operator_L_CP(md_nhc_npt* h, md_system* sys, double dt);
+/* v += dt F/m, kinetic tensor to the stats */
+int md_nhc_npt_operator_L_v(md_nhc_npt* h, md_system* sys, double dt);
+/* x = e^{vep dt} x + dt e^{vep dt/2} sinh-series(vep dt/2) v */
+int md_nhc_npt_operator_L_r(md_nhc_npt* h, md_system* sys, double dt);
+/* box edges *= e^{vep dt}, ep += vep dt */
+int md_nhc_npt_operator_L_box(md_nhc_npt* h, md_system* sys, double dt);
+/* ep, vep, xi1, vxi1, HamiltonianContribution (W vep^2/2 + Q1 vxi1^2/2 + (Nf+1) T xi1 + P V) */
+int md_nhc_npt_get_state(md_nhc_npt* h, double out[5]);
+
 /* ------------------------------------------------------------ simulation driver
  * Replaces the hot loop of ENG/app/lj.nhc-xtc.cu:159-274 for the Langevin path:
  * per step  [B A O A] -> (device-side rebuild check -> cell sort + list build) ->
@@ -276,7 +339,16 @@ typedef struct md_sim_params {
   int use_graph;        /* capture the step in a CUDA graph                */
   int stats_every;      /* energy/virial every n steps (NPT needs 1)       */
   double max_rcut;      /* largest cutoff the run may assign (list capacity); 0 = current max */
+  int integrator;       /* md_integrator: Langevin (lv) or Nose-Hoover chain + velocity Verlet */
+  double nhc_tau;       /* NHC period tau_T (lv.temperature is the target, lv.dt the step) */
+  int remove_com;       /* NHC: remove the centre-of-mass velocity every step */
 } md_sim_params;
+enum md_integrator {
+  MD_INTEG_LANGEVIN = 0,
+  /* the step of ENG/app/lj.nhc-xtc.cu:159-200: COM removal, NoseHoover_Chains2::operator_L(dt/2),
+     VelocityVerlet::step1, rebuild check, forces, step2, operator_L(dt/2) */
+  MD_INTEG_NHC = 1
+};
 int md_sim_create(md_sim** out, md_system* sys, md_engine* eng, const md_sim_params* p);
 int md_sim_destroy(md_sim* sim);
 int md_sim_run(md_sim* sim, int nsteps);
@@ -284,6 +356,9 @@ int md_sim_run(md_sim* sim, int nsteps);
 int md_sim_counters(md_sim* sim, int64_t* steps, int64_t* rebuilds, int* device_flags);
 /* 1 when the step graph skips the rebuild chain with a device-side conditional node */
 int md_sim_uses_conditional_graph(md_sim* sim, int* out);
+/* MD_INTEG_NHC runs: md_nhc_get_state of the driver's chain (after the pending
+   start-of-step half of the next step) */
+int md_sim_get_nhc_state(md_sim* sim, double out[5]);
 
 /* ------------------------------------------------------------ adaptive cutoff
  * Replaces DensityProfile_PiecewiseConst (ENG/src/DensityProfile.cu:27-99),
@@ -333,6 +408,33 @@ int md_synth_slab(int n, int n_in, const double box[3], int axis, double center,
 int md_synth_maxwell(int n, const double* mass, double temperature, uint64_t seed, double* vel);
 /* n/2 charges +1 and n/2 charges -1 in seeded random order */
 int md_synth_charges(int n, uint64_t seed, double* q);
+
+/* ------------------------------------------------------------ optiBasis error functional
+ * Replaces HermiteLossFunc / HermiteLossFunc_Bound0 .value / .deriv
+ * (optiBasis/IkError.py:166-260) with IkError.prepare_sum / prepare_sum_deriv /
+ * estimate / estimate_deriv (optiBasis/IkError.py:32-136) and the hats of
+ * HermiteBasisHatComput_Norm1(_Bound0) (optiBasis/HatComput.py:155-300), FP64 on the GPU.
+ * Interpolation basis: symmetric piecewise cubic Hermite on nbin bins of [0, CC] (grid
+ * units), value 1 and slope 0 at 0; coefficients [v_1..v_n, d_1..d_n] with n = nbin, or
+ * n = nbin - 1 when bound0 (the basis vanishes at CC).  Mesh K, rectangular box L,
+ * splitting beta, aliasing sum |l| <= l_cut; over_smpl 0 = int(400 nbin / CC).
+ * q2 = sum of squared charges and natoms set the scale of the estimate. */
+typedef struct md_ikerr md_ikerr;
+int md_ikerr_create(md_ikerr** out, const int K[3], const double L[3], double beta, double CC,
+                    int nbin, int l_cut, int bound0, int over_smpl, double q2, double natoms,
+                    int device);
+int md_ikerr_destroy(md_ikerr* h);
+int md_ikerr_num_coeffs(md_ikerr* h, int* out);
+/* estimate (value) and its gradient for C candidate coefficient vectors coeffs[C][n];
+   grads[C][n] may be NULL.  Host arrays; synchronises. */
+int md_ikerr_evaluate(md_ikerr* h, int C, const double* coeffs, double* values, double* grads);
+/* the same on device arrays, asynchronous on `stream` (NULL = the handle's stream) */
+int md_ikerr_evaluate_device(md_ikerr* h, int C, const double* d_coeffs, double* d_values,
+                             double* d_grads, void* stream);
+/* basis hats along axis d at k = 0..K_d/2 + l_cut K_d: hat0[k] (knot 0) and hats[n][k] */
+int md_ikerr_get_hats(md_ikerr* h, int d, double* hat0, double* hats);
+/* W_d(m), m = -K_d/2..K_d/2: sum over the other two mesh indices of 2|G(m)|^2 */
+int md_ikerr_get_weights(md_ikerr* h, int d, double* W);
 
 #ifdef __cplusplus
 }

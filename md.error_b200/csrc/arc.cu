@@ -230,16 +230,22 @@ __global__ void k_dft_axis(double2* data, ArcDims g, int axis, int sign, int bat
   }
 }
 
-static int dft3(md_adapt_rcut* a, double2* data, int sign, int batch) {
+// unnormalised 3D DFT (sign -1 forward, +1 backward) of `batch` consecutive
+// complex grids [n0][n1][n2], in place, any sizes up to 1024 per axis
+int dft3_grid(double2* data, const int n[3], int sign, int batch, cudaStream_t stream) {
   ArcDims g;
-  for (int d = 0; d < 3; ++d) g.n[d] = a->n[d];
+  for (int d = 0; d < 3; ++d) g.n[d] = n[d];
   for (int axis = 2; axis >= 0; --axis) {
     long lines = (long)g.n[(axis + 1) % 3] * g.n[(axis + 2) % 3] * batch;
     size_t smem = sizeof(double2) * 2 * g.n[axis];
-    k_dft_axis<<<(unsigned)lines, 128, smem, a->sys->stream>>>(data, g, axis, sign, batch);
+    k_dft_axis<<<(unsigned)lines, 128, smem, stream>>>(data, g, axis, sign, batch);
     MD_CHECK_LAUNCH("dft axis");
   }
   return MD_OK;
+}
+
+static int dft3(md_adapt_rcut* a, double2* data, int sign, int batch) {
+  return dft3_grid(data, a->n, sign, batch, a->sys->stream);
 }
 
 // ------------------------------------------------------------ element-wise kernels

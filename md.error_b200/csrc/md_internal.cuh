@@ -133,6 +133,16 @@ struct md_cell_list {
   bool built = false;
 };
 
+// Row layout of the neighbour list: rows hold cap entries (a multiple of 32)
+// in 32-entry lines, each line stored transposed 8 x 4 so that a force
+// kernel with 8 lanes per atom reads one 16-byte vector per lane per line
+// and lane l holds the line's logical entries l, l+8, l+16, l+24 (the 8
+// lanes then gather 8 consecutive neighbours at a time).  Logical entry e of
+// a row sits at nl_slot(e).
+__host__ __device__ __forceinline__ int nl_slot(int e) {
+  return (e & ~31) | ((e & 7) << 2) | ((e >> 3) & 3);
+}
+
 struct md_nlist {
   double rlist = 0, skin = 0, expansion = 1;
   int mode = MD_NL_MINIMAGE;
@@ -170,4 +180,8 @@ int langevin_step1_impl(md_system* sys, md_nlist* nl, Recorder* rec, bool with_b
                         cudaGraphConditionalHandle cond, int use_cond);
 int langevin_step2_impl(md_system* sys, Recorder* rec, int kick, int advance);
 int clear_stats_impl(md_system* sys, Recorder* rec, int first, int count);
+int nhc_vv1_impl(md_nhc* h, md_nlist* nl, double dt, Recorder* rec, cudaGraphConditionalHandle cond,
+                 int use_cond);
+int nhc_vv2_impl(md_nhc* h, double dt, Recorder* rec, int kick, int end, int start, int account);
+int nhc_settle_impl(md_nhc* h);
 int set_flag_impl(md_system* sys, unsigned bits, Recorder* rec);

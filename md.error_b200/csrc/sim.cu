@@ -35,6 +35,8 @@ struct md_sim {
   bool conditional = false;
   float* lattice_in_graph = nullptr;
   int64_t steps = 0;
+  md_nhc* nhc = nullptr;  // MD_INTEG_NHC
+  bool nhc_settled = false;  // velocities / chain brought to the end of the last step
   // adaptive cutoff schedule
   md_adapt_rcut* arc = nullptr;
   int sample_every = 0, update_every = 0, nrefine = 0;
@@ -50,7 +52,12 @@ static int record_step(md_sim* s, Recorder* rec, bool use_graph) {
     cond = (e == cudaSuccess);
     if (!cond) cudaGetLastError();
   }
-  if (int r = langevin_step1_impl(sys, s->nl, rec, false, h, cond ? 1 : 0)) return r;
+  const bool nhc = s->nhc != nullptr;
+  if (nhc) {
+    if (int r = nhc_vv1_impl(s->nhc, s->nl, s->p.lv.dt, rec, h, cond ? 1 : 0)) return r;
+  } else {
+    if (int r = langevin_step1_impl(sys, s->nl, rec, false, h, cond ? 1 : 0)) return r;
+  }
   if (cond) {
     cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
     cp.conditional.handle = h;
@@ -71,7 +78,13 @@ static int record_step(md_sim* s, Recorder* rec, bool use_graph) {
   }
   s->conditional = cond;
   if (int r = lj_apply_impl(s->eng, sys, s->nl, true, true, rec)) return r;
-  if (int r = langevin_step2_impl(sys, rec, 1, 1)) return r;
+  if (nhc) {
+    // closing kick + operator_L(dt/2), then this step's successor's COM
+    // removal and operator_L(dt/2), as a pending velocity map
+    if (int r = nhc_vv2_impl(s->nhc, s->p.lv.dt, rec, 1, 1, 1, 1)) return r;
+  } else {
+    if (int r = langevin_step2_impl(sys, rec, 1, 1)) return r;
+  }
   return MD_OK;
 }
 
@@ -94,6 +107,7 @@ extern "C" int md_sim_destroy(md_sim* s) {
   if (s->graph) cudaGraphDestroy(s->graph);
   md_nlist_destroy(s->nl);
   md_cell_list_destroy(s->cl);
+  md_nhc_destroy(s->nhc);
   delete s;
   return MD_OK;
 }
@@ -133,7 +147,7 @@ extern "C" int md_sim_create(md_sim** out, md_system* sys, md_engine* eng, const
     DevState hs;
     if ((r = sys->read_state(hs))) return fail(r);
     if ((r = md_system_set_rcut(sys, keep.data()))) return fail(r);
-    int want = ((int)(hs.max_nnb * 1.2) + 32 + 7) & ~7;
+    int want = ((int)(hs.max_nnb * 1.2) + 32 + 31) & ~31;
     if (want > s->nl->cap) {
       cudaFree(s->nl->list);
       s->nl->list = nullptr;
@@ -146,7 +160,17 @@ extern "C" int md_sim_create(md_sim** out, md_system* sys, md_engine* eng, const
   Recorder rec;
   rec.stream = sys->stream;
   if ((r = lj_apply_impl(eng, sys, s->nl, true, true, &rec))) return fail(r);
-  if ((r = langevin_step2_impl(sys, &rec, 0, 1))) return fail(r);
+  if (p->integrator == MD_INTEG_NHC) {
+    if (!(p->nhc_tau > 0)) { md_set_error("md_sim_create: the Nose-Hoover chain needs nhc_tau > 0"); return fail(MD_ERR_BADARG); }
+    if ((r = md_nhc_create(&s->nhc, sys, p->lv.temperature, p->nhc_tau, p->remove_com))) return fail(r);
+    // step 0 opens with COM removal and operator_L(dt/2): pending velocity map
+    if ((r = nhc_vv2_impl(s->nhc, p->lv.dt, &rec, 0, 0, 1, 1))) return fail(r);
+  } else if (p->integrator != MD_INTEG_LANGEVIN) {
+    md_set_error("md_sim_create: unknown integrator %d", p->integrator);
+    return fail(MD_ERR_BADARG);
+  } else if ((r = langevin_step2_impl(sys, &rec, 0, 1))) {
+    return fail(r);
+  }
   MD_CUDA(cudaStreamSynchronize(sys->stream));
   if (p->use_graph)
     if ((r = build_graph(s))) return fail(r);
@@ -173,6 +197,13 @@ extern "C" int md_sim_run(md_sim* s, int nsteps) {
   md_system* sys = s->sys;
   if (s->exec && sys->d_lattice != s->lattice_in_graph)
     if (int r = build_graph(s)) return r;
+  if (s->nhc && s->nhc_settled && nsteps > 0) {
+    // re-open the step the last run closed: COM removal + operator_L(dt/2)
+    Recorder rec;
+    rec.stream = sys->stream;
+    if (int r = nhc_vv2_impl(s->nhc, s->p.lv.dt, &rec, 0, 0, 1, 0)) return r;
+    s->nhc_settled = false;
+  }
   for (int i = 0; i < nsteps; ++i) {
     if (s->exec) {
       MD_CUDA(cudaGraphLaunch(s->exec, sys->stream));
@@ -197,6 +228,11 @@ extern "C" int md_sim_run(md_sim* s, int nsteps) {
       }
     }
   }
+  if (s->nhc && !s->nhc_settled) {
+    // velocities and chain as the reference has them after the last step
+    if (int r = nhc_settle_impl(s->nhc)) return r;
+    s->nhc_settled = true;
+  }
   return MD_OK;
 }
 
@@ -213,6 +249,12 @@ extern "C" int md_sim_counters(md_sim* s, int64_t* steps, int64_t* rebuilds, int
   }
   if (hs.flags & FLAG_NAN) { md_set_error("non-finite coordinates during the run"); return MD_ERR_BADARG; }
   return MD_OK;
+}
+
+extern "C" int md_sim_get_nhc_state(md_sim* s, double out[5]) {
+  if (!s || !out) return MD_ERR_BADARG;
+  if (!s->nhc) { md_set_error("md_sim_get_nhc_state: the run does not use the Nose-Hoover chain"); return MD_ERR_BADARG; }
+  return md_nhc_get_state(s->nhc, out);
 }
 
 extern "C" int md_sim_uses_conditional_graph(md_sim* s, int* out) {

@@ -16,6 +16,7 @@
 // a block holds several lines that are adjacent in memory so that strided
 // axes load coalesced.  Mixed precision: mesh, FFT and gather in FP32,
 // energy/virial and force accumulation in FP64.  Power-of-two mesh sizes.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -37,7 +38,7 @@ struct md_spme {
   void* C = nullptr;      // complex half meshes: [0] Q^, [1..3] products
   void* G = nullptr;      // real convolution meshes (3 for ik, 1 analytic)
   void* psi = nullptr;    // influence function on the half spectrum (ik normalisation)
-  double box_tab[3] = {0, 0, 0};
+  double* d_box_tab = nullptr;  // box psi was computed for (device; 0 = never)
 };
 
 // ---------------------------------------------------------------- B-spline weights
@@ -220,11 +221,16 @@ __device__ __forceinline__ double bmod_d(int n, int K, int m) {
   return 1.0 / (re * re + im * im);
 }
 
+// psi is recomputed only when the box differs from `tab`, the box it was last
+// computed for (NPT); the comparison is made on the device so that no host
+// round trip is needed, and `tab` is updated by k_spme_box_tab afterwards
 template <class R>
-__global__ void k_spme_influence(int K0, int K1, int K2, int n, double beta, const DevState* st, R* psi) {
+__global__ void k_spme_influence(int K0, int K1, int K2, int n, double beta, const DevState* st, R* psi,
+                                 const double* tab) {
   const int K2h = K2 / 2 + 1;
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (t >= (long)K0 * K1 * K2h) return;
+  if (st->L[0] == tab[0] && st->L[1] == tab[1] && st->L[2] == tab[2]) return;
   const int k = (int)(t % K2h), j = (int)((t / K2h) % K1), i = (int)(t / ((long)K2h * K1));
   const int ip = i <= K0 / 2 ? i : i - K0, jp = j <= K1 / 2 ? j : j - K1, kp = k;
   if (!ip && !jp && !kp) { psi[t] = R(0); return; }
@@ -234,6 +240,10 @@ __global__ void k_spme_influence(int K0, int K1, int K2, int n, double beta, con
   const double B = bmod_d(n, K0, i) * bmod_d(n, K1, j) * bmod_d(n, K2, k);
   const double sc = M_PI * M_PI / beta / beta;
   psi[t] = (R)(exp(-sc * mm) / mm * B / (M_PI * V));
+}
+
+__global__ void k_spme_box_tab(const DevState* st, double* tab) {
+  for (int d = 0; d < 3; ++d) tab[d] = st->L[d];
 }
 
 // energy + diagonal virial and the products written into C[1..]
@@ -341,6 +351,188 @@ k_spme_gather(int N, const typename V4<R>::T* __restrict__ pos, int n, int K0, i
   }
 }
 
+// ---------------------------------------------------------------- adjoint
+// The reciprocal energy is the quadratic form E = 1/2 sum_m psi(m) |Q^(m)|^2
+// = 1/2 sum_k Q(k) Phi(k) with Phi = IFFT(psi Q^) (unnormalised transforms),
+// Q(k) = sum_i q_i theta_i(k), theta_i(k) = prod_d M_n(u_id - k_d), u = K x / L.
+// Hence
+//   dE/dq_i      = sum_k theta_i(k) Phi(k)                      (potential)
+//   dE/dx_id     = q_i sum_k d theta_i(k)/du_d Phi(k) K_d / L_d  (exact gradient,
+//                  the analytic-differentiation force with its sign flipped)
+//   dE/dpsi(m)   = 1/2 |Q^(m)|^2
+//   dE/dbeta     = sum_m 1/2 |Q^(m)|^2 psi(m) 2 pi^2 |m|^2 / beta^3
+// The adjoint recomputes the spread mesh and its transform instead of
+// keeping them from an earlier forward call.
+template <class R>
+__global__ void __launch_bounds__(256)
+k_spme_adj_kspace(int K0, int K1, int K2, double beta, const R* __restrict__ psi, typename C2<R>::T* __restrict__ C,
+                  size_t nhalf, DevState* st, double* partials, double* __restrict__ dpsi) {
+  typedef typename C2<R>::T T2;
+  const int K2h = K2 / 2 + 1;
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  double v[2] = {0, 0};
+  if (t < (long)nhalf) {
+    const int k = (int)(t % K2h), j = (int)((t / K2h) % K1), i = (int)(t / ((long)K2h * K1));
+    const int ip = i <= K0 / 2 ? i : i - K0, jp = j <= K1 / 2 ? j : j - K1, kp = k;
+    const T2 q = C[t];
+    const R ps = psi[t];
+    T2 g;
+    g.x = q.x * ps;
+    g.y = q.y * ps;
+    C[nhalf + t] = g;
+    // interior z planes of the half spectrum stand for two full-spectrum modes
+    const double wgt = (k == 0 || (2 * k == K2)) ? 1.0 : 2.0;
+    const double q2 = 0.5 * wgt * ((double)q.x * q.x + (double)q.y * q.y);
+    if (dpsi) dpsi[t] = (ip || jp || kp) ? q2 : 0.0;
+    if (ip || jp || kp) {
+      const double m0 = ip * st->Li[0], m1 = jp * st->Li[1], m2 = kp * st->Li[2];
+      const double mm = m0 * m0 + m1 * m1 + m2 * m2;
+      v[0] = q2 * (double)ps;
+      v[1] = v[0] * 2.0 * M_PI * M_PI * mm / (beta * beta * beta);
+    }
+  }
+  block_reduce_finish<2>(v, partials, &st->red_counter[RED_SPME], st->scratch, true);
+}
+
+template <class R>
+__global__ void __launch_bounds__(256)
+k_spme_adj_gather(int N, const typename V4<R>::T* __restrict__ pos, const int* __restrict__ id, int n, int K0,
+                  int K1, int K2, const DevState* __restrict__ st, const R* __restrict__ Phi,
+                  double* __restrict__ dq, double* __restrict__ dr) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= N) return;
+  const typename V4<R>::T p = pos[warp];
+  int b0, b1, b2;
+  R f0, f1, f2;
+  grid_coord<R>(p.x, (R)st->Li[0], K0, b0, f0);
+  grid_coord<R>(p.y, (R)st->Li[1], K1, b1, f1);
+  grid_coord<R>(p.z, (R)st->Li[2], K2, b2, f2);
+  R w0[16], w1[16], w2[16], d0[16], d1[16], d2[16];
+  bspline_w<R>(n, f0, w0, d0);
+  bspline_w<R>(n, f1, w1, d1);
+  bspline_w<R>(n, f2, w2, d2);
+  double pot = 0, gx = 0, gy = 0, gz = 0;
+  for (int ab = lane; ab < n * n; ab += 32) {
+    const int a = ab / n, b = ab % n;
+    const long row = ((long)wrapk(b0 - a, K0) * K1 + wrapk(b1 - b, K1)) * K2;
+    for (int c = 0; c < n; ++c) {
+      const R g = Phi[row + wrapk(b2 - c, K2)];
+      pot += (double)(g * w0[a] * w1[b] * w2[c]);
+      gx += (double)(g * d0[a] * w1[b] * w2[c]);
+      gy += (double)(g * w0[a] * d1[b] * w2[c]);
+      gz += (double)(g * w0[a] * w1[b] * d2[c]);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    pot += __shfl_xor_sync(0xffffffffu, pot, o);
+    gx += __shfl_xor_sync(0xffffffffu, gx, o);
+    gy += __shfl_xor_sync(0xffffffffu, gy, o);
+    gz += __shfl_xor_sync(0xffffffffu, gz, o);
+  }
+  if (lane == 0) {
+    const double q = (double)p.w;
+    const int o = id[warp];  // results in the caller's atom order
+    if (dq) dq[o] = pot;
+    if (dr) {
+      dr[3 * o] = q * gx * K0 * st->Li[0];
+      dr[3 * o + 1] = q * gy * K1 * st->Li[1];
+      dr[3 * o + 2] = q * gz * K2 * st->Li[2];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- self-force correction
+// SelfCorr (RE/src/SelfCorr.cpp:99-220), analytic differentiation, |k| <= 3:
+//   c_d(k) = sum_{m != 0} f(m) (-2) g_d(m_d, k) (-4 pi k K_d / L_d),
+//   f(m) = e^{-pi^2 |m|^2 / beta^2} / |m|^2 / (2 pi V)
+//   g_d(m, k) = (u + 2 pi k)^-n / sum_{l=-3..3} (u + 2 pi l)^-n, u = 2 pi m / K_d
+//   (0 at the Nyquist index of an even K_d);
+//   F_id -= sum_{k=1..3} c_d(k) q_i^2 sin(2 pi k K_d x_id / L_d).
+// g_d depends on m_d alone, so the K^3 sum is regrouped per axis: W_d(i) is
+// the sum of f over the other two indices (one block per (i, d)), then the
+// nine c_d(k) are 1-D sums.
+__global__ void __launch_bounds__(256)
+k_selfcorr_weights(int K0, int K1, int K2, double beta, const DevState* st, double* W /* [3][Kmax] */, int Kmax) {
+  const int d = blockIdx.y, i = blockIdx.x;
+  const int K[3] = {K0, K1, K2};
+  if (i >= K[d]) return;
+  const int a = (d + 1) % 3, b = (d + 2) % 3;
+  int p[3];
+  p[d] = i > (K[d] >> 1) ? i - K[d] : i;
+  const double V = st->L[0] * st->L[1] * st->L[2];
+  const double t = M_PI / beta, scal = 1.0 / (2.0 * M_PI * V);
+  double acc = 0.0;
+  for (int e = threadIdx.x; e < K[a] * K[b]; e += blockDim.x) {
+    const int ia = e / K[b], ib = e % K[b];
+    p[a] = ia > (K[a] >> 1) ? ia - K[a] : ia;
+    p[b] = ib > (K[b] >> 1) ? ib - K[b] : ib;
+    const double m0 = p[0] * st->Li[0], m1 = p[1] * st->Li[1], m2 = p[2] * st->Li[2];
+    const double mm = m0 * m0 + m1 * m1 + m2 * m2;
+    if (mm == 0.0) continue;
+    acc += exp(-t * t * mm) / mm * scal;
+  }
+  __shared__ double sh[8];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += sh[w];
+    W[d * Kmax + i] = s;
+  }
+}
+
+__device__ __forceinline__ double ipow_dev(double x, int n) {
+  double r = 1.0;
+  for (int k = 0; k < n; ++k) r *= x;
+  return r;
+}
+
+// one warp per (d, k), k = 1..3: c[d][k]
+__global__ void k_selfcorr_coef(int K0, int K1, int K2, int order, const DevState* st, const double* W, int Kmax,
+                                double* coef /* [3][4] */) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (w >= 9) return;
+  const int d = w / 3, kk = 1 + w % 3;
+  const int K[3] = {K0, K1, K2};
+  double acc = 0.0;
+  for (int i = lane; i < K[d]; i += 32) {
+    if (i == (K[d] >> 1) && (K[d] % 2 == 0)) continue;
+    const int p = i > (K[d] >> 1) ? i - K[d] : i;
+    const double u = 2.0 * M_PI * p / K[d];
+    double s = 1.0 / ipow_dev(u, order), up = u, un = u;
+    for (int l = 0; l < 3; ++l) {
+      up += 2.0 * M_PI;
+      un -= 2.0 * M_PI;
+      s += 1.0 / ipow_dev(up, order);
+      s += 1.0 / ipow_dev(un, order);
+    }
+    const double g = 1.0 / ipow_dev(u + 2.0 * M_PI * kk, order) / s;
+    acc += W[d * Kmax + i] * (-2.0 * g) * (-4.0) * M_PI * kk * (double)K[d] * st->Li[d];
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) coef[d * 4 + kk] = acc;
+}
+
+template <class R>
+__global__ void __launch_bounds__(256)
+k_selfcorr_apply(int N, const typename V4<R>::T* __restrict__ pos, int K0, int K1, int K2, const DevState* st,
+                 const double* __restrict__ coef, double4a* __restrict__ force) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const typename V4<R>::T p = pos[i];
+  const double q2 = (double)p.w * (double)p.w;
+  const double x[3] = {(double)p.x, (double)p.y, (double)p.z};
+  const int K[3] = {K0, K1, K2};
+  double f[3] = {0, 0, 0};
+  for (int d = 0; d < 3; ++d)
+    for (int kk = 1; kk <= 3; ++kk)
+      f[d] -= coef[d * 4 + kk] * q2 * sinpi(2.0 * kk * K[d] * st->Li[d] * x[d]);
+  double4a F = force[i];
+  F.x += f[0]; F.y += f[1]; F.z += f[2];
+  force[i] = F;
+}
+
 // ---------------------------------------------------------------- exact Ewald (FP64)
 // S(m) = sum_i q_i exp(2 pi i m.r_i) for every m of the |m_d| <= K_d/2 box
 // (EleRecES::calPotential), then E = sum_m e^{-pi^2 m^2/beta^2}/m^2 |S|^2 / (2 pi V)
@@ -446,28 +638,21 @@ static int fft_launch(md_spme* s, const void* in, void* out, int mode, int axis,
   return MD_OK;
 }
 
+// influence refresh (only when the box changed), spread and the forward
+// transform: C[0] = Q^ on the half spectrum
 template <class R>
-static int spme_run(md_spme* s, bool with_stats) {
+static int spme_forward_mesh(md_spme* s) {
   typedef typename C2<R>::T T2;
   md_system* sys = s->sys;
   cudaStream_t st_ = sys->stream;
   const int K0 = s->K[0], K1 = s->K[1], K2 = s->K[2], n = s->order;
   R* Q = (R*)s->Q;
   T2* C = (T2*)s->C;
-  R* G = (R*)s->G;
-  // influence function: recomputed when the box changed (NPT)
-  DevState hs;
-  bool box_changed = false;
-  if (with_stats || true) {
-    MD_CUDA(cudaMemcpyAsync(&hs.L, sys->st->L, sizeof(double) * 3, cudaMemcpyDeviceToHost, st_));
-    MD_CUDA(cudaStreamSynchronize(st_));
-    for (int d = 0; d < 3; ++d) box_changed |= hs.L[d] != s->box_tab[d];
-  }
-  if (box_changed) {
-    k_spme_influence<R><<<(unsigned)((s->nhalf + 255) / 256), 256, 0, st_>>>(K0, K1, K2, n, s->beta, sys->st, (R*)s->psi);
-    MD_CHECK_LAUNCH("spme influence");
-    for (int d = 0; d < 3; ++d) s->box_tab[d] = hs.L[d];
-  }
+  k_spme_influence<R><<<(unsigned)((s->nhalf + 255) / 256), 256, 0, st_>>>(K0, K1, K2, n, s->beta, sys->st,
+                                                                           (R*)s->psi, s->d_box_tab);
+  MD_CHECK_LAUNCH("spme influence");
+  k_spme_box_tab<<<1, 1, 0, st_>>>(sys->st, s->d_box_tab);
+  MD_CHECK_LAUNCH("spme box tab");
   MD_CUDA(cudaMemsetAsync(Q, 0, sizeof(R) * s->nreal, st_));
   const long nt = (long)sys->N * n * n;
   k_spme_spread<R><<<(unsigned)((nt + 255) / 256), 256, 0, st_>>>(sys->N, (const typename V4<R>::T*)sys->pos, n, K0,
@@ -476,6 +661,18 @@ static int spme_run(md_spme* s, bool with_stats) {
   if (int r = fft_launch<R>(s, Q, C, 0, 2, -1, 1)) return r;
   if (int r = fft_launch<R>(s, C, C, 1, 1, -1, 1)) return r;
   if (int r = fft_launch<R>(s, C, C, 1, 0, -1, 1)) return r;
+  return MD_OK;
+}
+
+template <class R>
+static int spme_run(md_spme* s, bool with_stats) {
+  typedef typename C2<R>::T T2;
+  md_system* sys = s->sys;
+  cudaStream_t st_ = sys->stream;
+  const int K0 = s->K[0], K1 = s->K[1], K2 = s->K[2], n = s->order;
+  T2* C = (T2*)s->C;
+  R* G = (R*)s->G;
+  if (int r = spme_forward_mesh<R>(s)) return r;
   const int nb = (int)((s->nhalf + 255) / 256);
   if (with_stats && nb > sys->max_partial_blocks) { md_set_error("partials buffer too small for the mesh"); return MD_ERR_BADARG; }
   k_spme_kspace<R><<<nb, 256, 0, st_>>>(K0, K1, K2, s->method, s->beta, (const R*)s->psi, C, s->nhalf, sys->st,
@@ -493,6 +690,50 @@ static int spme_run(md_spme* s, bool with_stats) {
   k_spme_gather<R><<<(unsigned)(((long)sys->N * 32 + 255) / 256), 256, 0, st_>>>(
       sys->N, (const typename V4<R>::T*)sys->pos, n, K0, K1, K2, s->method, sys->st, G, s->nreal, sys->force);
   MD_CHECK_LAUNCH("spme gather");
+  return MD_OK;
+}
+
+// energy and gradient: recompute the mesh and its transform, influence
+// multiply (energy, dE/dbeta, dE/dpsi), one inverse transform to Phi, gather
+template <class R>
+static int spme_energy_grad(md_spme* s, double* energy, double* dq, double* dr, double* dbeta, double* dpsi) {
+  typedef typename C2<R>::T T2;
+  md_system* sys = s->sys;
+  cudaStream_t st_ = sys->stream;
+  const int K0 = s->K[0], K1 = s->K[1], K2 = s->K[2], n = s->order;
+  T2* C = (T2*)s->C;
+  R* G = (R*)s->G;
+  const int nb = (int)((s->nhalf + 255) / 256);
+  if (nb > sys->max_partial_blocks) { md_set_error("partials buffer too small for the mesh"); return MD_ERR_BADARG; }
+  // device outputs: dq [N], dr [N][3], dpsi [nhalf] (FP64, caller's atom order)
+  const size_t nq = dq ? (size_t)sys->N : 0, nr = dr ? 3 * (size_t)sys->N : 0, np = dpsi ? s->nhalf : 0;
+  double* d = nullptr;
+  if (nq + nr + np) MD_CUDA(cudaMallocAsync((void**)&d, sizeof(double) * (nq + nr + np), st_));
+  double* d_q = dq ? d : nullptr;
+  double* d_r = dr ? d + nq : nullptr;
+  double* d_p = dpsi ? d + nq + nr : nullptr;
+  if (int r = spme_forward_mesh<R>(s)) return r;
+  k_spme_adj_kspace<R><<<nb, 256, 0, st_>>>(K0, K1, K2, s->beta, (const R*)s->psi, C, s->nhalf, sys->st,
+                                             sys->partials, d_p);
+  MD_CHECK_LAUNCH("spme adjoint kspace");
+  if (dq || dr) {
+    T2* Cp = C + s->nhalf;
+    if (int r = fft_launch<R>(s, Cp, Cp, 1, 0, +1, 1)) return r;
+    if (int r = fft_launch<R>(s, Cp, Cp, 1, 1, +1, 1)) return r;
+    if (int r = fft_launch<R>(s, Cp, G, 2, 2, +1, 1)) return r;
+    k_spme_adj_gather<R><<<(unsigned)(((long)sys->N * 32 + 255) / 256), 256, 0, st_>>>(
+        sys->N, (const typename V4<R>::T*)sys->pos, sys->id, n, K0, K1, K2, sys->st, G, d_q, d_r);
+    MD_CHECK_LAUNCH("spme adjoint gather");
+  }
+  double red[2];
+  MD_CUDA(cudaMemcpyAsync(red, sys->st->scratch, sizeof(red), cudaMemcpyDeviceToHost, st_));
+  if (dq) MD_CUDA(cudaMemcpyAsync(dq, d_q, sizeof(double) * nq, cudaMemcpyDeviceToHost, st_));
+  if (dr) MD_CUDA(cudaMemcpyAsync(dr, d_r, sizeof(double) * nr, cudaMemcpyDeviceToHost, st_));
+  if (dpsi) MD_CUDA(cudaMemcpyAsync(dpsi, d_p, sizeof(double) * np, cudaMemcpyDeviceToHost, st_));
+  if (d) MD_CUDA(cudaFreeAsync(d, st_));
+  MD_CUDA(cudaStreamSynchronize(st_));
+  if (energy) *energy = red[0];
+  if (dbeta) *dbeta = red[1];
   return MD_OK;
 }
 
@@ -521,7 +762,9 @@ extern "C" int md_spme_create(md_spme** out, md_system* sys, const int K[3], int
   bool ok = cudaMalloc(&s->Q, rs * s->nreal) == cudaSuccess &&
             cudaMalloc(&s->C, 2 * rs * s->nhalf * 4) == cudaSuccess &&
             cudaMalloc(&s->G, rs * s->nreal * 3) == cudaSuccess &&
-            cudaMalloc(&s->psi, rs * s->nhalf) == cudaSuccess;
+            cudaMalloc(&s->psi, rs * s->nhalf) == cudaSuccess &&
+            cudaMalloc(&s->d_box_tab, sizeof(double) * 3) == cudaSuccess &&
+            cudaMemset(s->d_box_tab, 0, sizeof(double) * 3) == cudaSuccess;
   if (!ok) {
     md_cuda_fail(cudaGetLastError(), "md_spme_create");
     md_spme_destroy(s);
@@ -533,7 +776,7 @@ extern "C" int md_spme_create(md_spme** out, md_system* sys, const int K[3], int
 
 extern "C" int md_spme_destroy(md_spme* s) {
   if (!s) return MD_OK;
-  void* p[] = {s->Q, s->C, s->G, s->psi};
+  void* p[] = {s->Q, s->C, s->G, s->psi, s->d_box_tab};
   for (void* q : p) if (q) cudaFree(q);
   delete s;
   return MD_OK;
@@ -542,6 +785,52 @@ extern "C" int md_spme_destroy(md_spme* s) {
 extern "C" int md_spme_apply(md_spme* s, md_system* sys, int with_stats) {
   if (!s || !sys || sys != s->sys) { md_set_error("md_spme_apply: bad arguments"); return MD_ERR_BADARG; }
   return sys->prec == MD_PREC_FP64 ? spme_run<double>(s, with_stats != 0) : spme_run<float>(s, with_stats != 0);
+}
+
+extern "C" int md_spme_energy_grad(md_spme* s, md_system* sys, double* energy, double* dE_dq, double* dE_dr,
+                                   double* dE_dbeta, double* dE_dpsi) {
+  if (!s || !sys || sys != s->sys) { md_set_error("md_spme_energy_grad: bad arguments"); return MD_ERR_BADARG; }
+  return sys->prec == MD_PREC_FP64 ? spme_energy_grad<double>(s, energy, dE_dq, dE_dr, dE_dbeta, dE_dpsi)
+                                   : spme_energy_grad<float>(s, energy, dE_dq, dE_dr, dE_dbeta, dE_dpsi);
+}
+
+__global__ void k_mesh_out(size_t n, const float* a, const double* b, double* out);
+
+extern "C" int md_spme_self_correction(md_spme* s, md_system* sys) {
+  if (!s || !sys || sys != s->sys) { md_set_error("md_spme_self_correction: bad arguments"); return MD_ERR_BADARG; }
+  const int Kmax = std::max(s->K[0], std::max(s->K[1], s->K[2]));
+  double* d = nullptr;
+  MD_CUDA(cudaMallocAsync((void**)&d, sizeof(double) * (3 * Kmax + 12), sys->stream));
+  k_selfcorr_weights<<<dim3(Kmax, 3), 256, 0, sys->stream>>>(s->K[0], s->K[1], s->K[2], s->beta, sys->st, d, Kmax);
+  MD_CHECK_LAUNCH("selfcorr weights");
+  k_selfcorr_coef<<<1, 9 * 32, 0, sys->stream>>>(s->K[0], s->K[1], s->K[2], s->order, sys->st, d, Kmax,
+                                                 d + 3 * Kmax);
+  MD_CHECK_LAUNCH("selfcorr coef");
+  const int nb = ceil_div(sys->N, 256);
+  if (sys->prec == MD_PREC_FP64)
+    k_selfcorr_apply<double><<<nb, 256, 0, sys->stream>>>(sys->N, (const double4a*)sys->pos, s->K[0], s->K[1],
+                                                           s->K[2], sys->st, d + 3 * Kmax, sys->force);
+  else
+    k_selfcorr_apply<float><<<nb, 256, 0, sys->stream>>>(sys->N, (const float4*)sys->pos, s->K[0], s->K[1],
+                                                         s->K[2], sys->st, d + 3 * Kmax, sys->force);
+  MD_CHECK_LAUNCH("selfcorr apply");
+  MD_CUDA(cudaFreeAsync(d, sys->stream));
+  return MD_OK;
+}
+
+extern "C" int md_spme_get_influence(md_spme* s, double* psi) {
+  if (!s || !psi) return MD_ERR_BADARG;
+  md_system* sys = s->sys;
+  double* d = nullptr;
+  MD_CUDA(cudaMallocAsync((void**)&d, sizeof(double) * s->nhalf, sys->stream));
+  const bool f = sys->prec != MD_PREC_FP64;
+  k_mesh_out<<<(unsigned)((s->nhalf + 255) / 256), 256, 0, sys->stream>>>(
+      s->nhalf, f ? (const float*)s->psi : nullptr, f ? nullptr : (const double*)s->psi, d);
+  MD_CHECK_LAUNCH("influence out");
+  MD_CUDA(cudaMemcpyAsync(psi, d, sizeof(double) * s->nhalf, cudaMemcpyDeviceToHost, sys->stream));
+  MD_CUDA(cudaFreeAsync(d, sys->stream));
+  MD_CUDA(cudaStreamSynchronize(sys->stream));
+  return MD_OK;
 }
 
 __global__ void k_mesh_out(size_t n, const float* a, const double* b, double* out) {

@@ -133,6 +133,15 @@ __global__ void k_set_vec(int N, int what, const double* in, const int* id,
   dst[k] = a;
 }
 
+// charges live in the w component of the position array
+template <class R>
+__global__ void k_charge_io(int N, int dir, typename V4<R>::T* p4, const int* id, double* host_order) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  if (dir == 0) p4[k].w = (R)host_order[id[k]];
+  else host_order[id[k]] = (double)p4[k].w;
+}
+
 __global__ void k_rcut_io(int N, int dir, float* rc, const int* id, float* host_order) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= N) return;
@@ -354,6 +363,37 @@ extern "C" int md_system_get_unwrapped_positions(md_system* s, double* pos) { re
 extern "C" int md_system_set_velocities(md_system* s, const double* v) { return upload_vec(s, 1, v); }
 extern "C" int md_system_get_velocities(md_system* s, double* v) { return download(s, 1, v); }
 extern "C" int md_system_get_forces(md_system* s, double* f) { return download(s, 2, f); }
+
+static int charge_io(md_system* s, int dir, double* q) {
+  if (int r = check_sys(s)) return r;
+  if (!q) return MD_ERR_BADARG;
+  if (dir == 0)
+    for (int i = 0; i < s->N; ++i)
+      if (!std::isfinite(q[i])) { md_set_error("non-finite charge at atom %d", i); return MD_ERR_BADARG; }
+  const size_t bytes = sizeof(double) * (size_t)s->N;
+  if (int r = ensure_stage(s, bytes)) return r;
+  MD_CUDA(cudaStreamSynchronize(s->stream));
+  double* d = nullptr;
+  MD_CUDA(cudaMallocAsync((void**)&d, bytes, s->stream));
+  if (dir == 0) {
+    memcpy(s->h_stage, q, bytes);
+    MD_CUDA(cudaMemcpyAsync(d, s->h_stage, bytes, cudaMemcpyHostToDevice, s->stream));
+  }
+  const int nb = ceil_div(s->N, 256);
+  if (s->prec == MD_PREC_FP64)
+    k_charge_io<double><<<nb, 256, 0, s->stream>>>(s->N, dir, (double4a*)s->pos, s->id, d);
+  else
+    k_charge_io<float><<<nb, 256, 0, s->stream>>>(s->N, dir, (float4*)s->pos, s->id, d);
+  MD_CHECK_LAUNCH("charge io");
+  if (dir == 1) MD_CUDA(cudaMemcpyAsync(s->h_stage, d, bytes, cudaMemcpyDeviceToHost, s->stream));
+  MD_CUDA(cudaFreeAsync(d, s->stream));
+  MD_CUDA(cudaStreamSynchronize(s->stream));
+  if (dir == 1) memcpy(q, s->h_stage, bytes);
+  return MD_OK;
+}
+
+extern "C" int md_system_set_charges(md_system* s, const double* q) { return charge_io(s, 0, const_cast<double*>(q)); }
+extern "C" int md_system_get_charges(md_system* s, double* q) { return charge_io(s, 1, q); }
 
 extern "C" int md_system_get_box(md_system* s, double box[3]) {
   if (int r = check_sys(s)) return r;

@@ -37,7 +37,8 @@ class SimParams(C.Structure):
     """md_sim_params"""
     _fields_ = [("lv", LangevinParams), ("skin", f64), ("cell_size", f64),
                 ("expansion", f64), ("nl_mode", i32), ("use_graph", i32),
-                ("stats_every", i32), ("max_rcut", f64)]
+                ("stats_every", i32), ("max_rcut", f64), ("integrator", i32), ("nhc_tau", f64),
+                ("remove_com", i32)]
 
 
 _SIGS = {
@@ -100,6 +101,11 @@ _SIGS = {
     "md_spme_destroy": (i32, [vp]),
     "md_spme_apply": (i32, [vp, vp, i32]),
     "md_spme_get_mesh": (i32, [vp, P(f64)]),
+    "md_spme_energy_grad": (i32, [vp, vp, P(f64), P(f64), P(f64), P(f64), P(f64)]),
+    "md_spme_get_influence": (i32, [vp, P(f64)]),
+    "md_spme_self_correction": (i32, [vp, vp]),
+    "md_system_set_charges": (i32, [vp, P(f64)]),
+    "md_system_get_charges": (i32, [vp, P(f64)]),
     "md_ewald_self_energy": (i32, [vp, f64, P(f64)]),
     "md_ewald_exact": (i32, [vp, P(i32), f64, P(f64), i32]),
     "md_error_estimate_pme": (i32, [vp, P(i32), f64, f64, P(f64), P(f64)]),
@@ -124,6 +130,27 @@ _SIGS = {
     "md_synth_slab": (i32, [i32, i32, P(f64), i32, f64, f64, f64, u64, P(f64)]),
     "md_synth_maxwell": (i32, [i32, P(f64), f64, u64, P(f64)]),
     "md_synth_charges": (i32, [i32, u64, P(f64)]),
+    "md_nhc_create": (i32, [P(vp), vp, f64, f64, i32]),
+    "md_nhc_destroy": (i32, [vp]),
+    "md_nhc_operator_L": (i32, [vp, vp, f64, i32]),
+    "md_nhc_step1": (i32, [vp, vp, vp, f64]),
+    "md_nhc_step2": (i32, [vp, vp, f64]),
+    "md_nhc_get_state": (i32, [vp, P(f64)]),
+    "md_sim_get_nhc_state": (i32, [vp, P(f64)]),
+    "md_nhc_npt_create": (i32, [P(vp), vp, f64, f64, f64, f64, f64]),
+    "md_nhc_npt_destroy": (i32, [vp]),
+    "md_nhc_npt_operator_L_CP": (i32, [vp, vp, f64]),
+    "md_nhc_npt_operator_L_v": (i32, [vp, vp, f64]),
+    "md_nhc_npt_operator_L_r": (i32, [vp, vp, f64]),
+    "md_nhc_npt_operator_L_box": (i32, [vp, vp, f64]),
+    "md_nhc_npt_get_state": (i32, [vp, P(f64)]),
+    "md_ikerr_create":(i32, [P(vp), P(i32), P(f64), f64, f64, i32, i32, i32, i32, f64, f64, i32]),
+    "md_ikerr_destroy": (i32, [vp]),
+    "md_ikerr_num_coeffs": (i32, [vp, P(i32)]),
+    "md_ikerr_evaluate": (i32, [vp, i32, P(f64), P(f64), P(f64)]),
+    "md_ikerr_evaluate_device": (i32, [vp, i32, vp, vp, vp, vp]),
+    "md_ikerr_get_hats": (i32, [vp, i32, P(f64), P(f64)]),
+    "md_ikerr_get_weights": (i32, [vp, i32, P(f64)]),
 }
 
 

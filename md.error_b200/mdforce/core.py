@@ -30,6 +30,8 @@ MD_ERR_TIMEOUT = 13
 
 PREC_MIXED = 0
 PREC_FP64 = 1
+INTEG_LANGEVIN = 0
+INTEG_NHC = 1
 NL_MINIMAGE = 0
 NL_CELLSHIFT = 1
 
@@ -166,6 +168,15 @@ class MDSystem:
     def set_velocities(self, vel):
         a = _f64(vel).reshape(self.n, 3)
         check(lib.md_system_set_velocities(self.h, _p(a)), "set_velocities")
+
+    def charges(self):
+        q = np.empty(self.n, np.float64)
+        check(lib.md_system_get_charges(self.h, _p(q)), "get_charges")
+        return q
+
+    def set_charges(self, q):
+        a = _f64(q).reshape(self.n)
+        check(lib.md_system_set_charges(self.h, _p(a)), "set_charges")
 
     def box(self):
         b = np.empty(3, np.float64)
@@ -335,6 +346,37 @@ class SPME:
         check(lib.md_spme_get_mesh(self.h, _p(Q)), "mesh")
         return Q
 
+    def self_correction(self, sys=None):
+        """SelfCorr::correction: add the analytic-differentiation self-force correction."""
+        check(lib.md_spme_self_correction(self.h, (sys or self.sys).h), "SPME::self_correction")
+
+    def influence(self):
+        """psi on the half spectrum [K0, K1, K2/2+1]."""
+        psi = np.empty((self.K[0], self.K[1], self.K[2] // 2 + 1), np.float64)
+        check(lib.md_spme_get_influence(self.h, _p(psi)), "influence")
+        return psi
+
+    def energy_grad(self, dq=True, dr=True, dpsi=False):
+        """Reciprocal energy and its exact gradient (md_spme_energy_grad):
+        dict with energy, dE_dbeta and, as asked, dE_dq [N], dE_dr [N, 3],
+        dE_dpsi [K0, K1, K2/2+1]."""
+        n = self.sys.n
+        e, db = C.c_double(), C.c_double()
+        gq = np.empty(n) if dq else None
+        gr = np.empty((n, 3)) if dr else None
+        gp = np.empty((self.K[0], self.K[1], self.K[2] // 2 + 1)) if dpsi else None
+        check(lib.md_spme_energy_grad(self.h, self.sys.h, C.byref(e), _p(gq) if dq else None,
+                                      _p(gr) if dr else None, C.byref(db), _p(gp) if dpsi else None),
+              "SPME::energy_grad")
+        out = {"energy": e.value, "dE_dbeta": db.value}
+        if dq:
+            out["dE_dq"] = gq
+        if dr:
+            out["dE_dr"] = gr
+        if dpsi:
+            out["dE_dpsi"] = gp
+        return out
+
 
 def ewald_self_energy(sys, beta):
     v = C.c_double()
@@ -493,11 +535,84 @@ class AdaptRCutEstimator:
         return out
 
 
+class NoseHoover_Chains2:
+    """NoseHoover_Chains2 (ENG/include/Thermostat.h:77-120): reinit(sys, refT, tauT),
+    operator_L(dt, sys), HamiltonianContribution(); step1/step2 give the
+    lj.nhc-xtc step (COM removal, operator_L(dt/2), VV step1 | forces | VV step2,
+    operator_L(dt/2))."""
+
+    def __init__(self, sys, ref_T, tau_T, remove_com=True):
+        h = C.c_void_p()
+        check(lib.md_nhc_create(C.byref(h), sys.h, float(ref_T), float(tau_T), 1 if remove_com else 0),
+              "NoseHoover_Chains2")
+        self.h = h
+        self.sys = sys
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.md_nhc_destroy(self.h)
+            self.h = None
+
+    def operator_L(self, dt, sys=None, with_stats=True):
+        check(lib.md_nhc_operator_L(self.h, (sys or self.sys).h, float(dt), 1 if with_stats else 0), "operator_L")
+
+    def step1(self, dt, nlist=None):
+        check(lib.md_nhc_step1(self.h, self.sys.h, nlist.h if nlist is not None else None, float(dt)), "step1")
+
+    def step2(self, dt):
+        check(lib.md_nhc_step2(self.h, self.sys.h, float(dt)), "step2")
+
+    def state(self):
+        out = np.zeros(5)
+        check(lib.md_nhc_get_state(self.h, _p(out)), "state")
+        return out
+
+    def HamiltonianContribution(self):
+        return float(self.state()[4])
+
+
+class NoseHoover_Chains2_Isobaric:
+    """NoseHoover_Chains2_Isobaric (ENG/include/Barostat.h:90-175): reinit(sys, refT,
+    tauT, refP, tauP, pressureCorr) and the operators L_CP, L_v, L_r, L_box."""
+
+    def __init__(self, sys, ref_T, tau_T, ref_P, tau_P, pressure_corr=0.0):
+        h = C.c_void_p()
+        check(lib.md_nhc_npt_create(C.byref(h), sys.h, float(ref_T), float(tau_T), float(ref_P), float(tau_P),
+                                    float(pressure_corr)), "NoseHoover_Chains2_Isobaric")
+        self.h = h
+        self.sys = sys
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.md_nhc_npt_destroy(self.h)
+            self.h = None
+
+    def operator_L_CP(self, dt):
+        check(lib.md_nhc_npt_operator_L_CP(self.h, self.sys.h, float(dt)), "operator_L_CP")
+
+    def operator_L_v(self, dt):
+        check(lib.md_nhc_npt_operator_L_v(self.h, self.sys.h, float(dt)), "operator_L_v")
+
+    def operator_L_r(self, dt):
+        check(lib.md_nhc_npt_operator_L_r(self.h, self.sys.h, float(dt)), "operator_L_r")
+
+    def operator_L_box(self, dt):
+        check(lib.md_nhc_npt_operator_L_box(self.h, self.sys.h, float(dt)), "operator_L_box")
+
+    def state(self):
+        out = np.zeros(5)
+        check(lib.md_nhc_npt_get_state(self.h, _p(out)), "state")
+        return out
+
+
 class Simulation:
     """Graph-captured Langevin MD driver (the hot loop of ENG/app/lj.nhc-xtc.cu)."""
 
     def __init__(self, sys, engine, skin, cell_size, lv, nl_mode=NL_MINIMAGE, expansion=1.5,
-                 use_graph=True, max_rcut=0.0):
+                 use_graph=True, max_rcut=0.0, integrator="langevin", nhc_tau=0.0, remove_com=True):
+        """integrator "langevin" (lv: BAOAB NVT/NPT) or "nhc" (the lj.nhc-xtc step:
+        2-chain Nose-Hoover at lv.temperature with period nhc_tau, velocity Verlet with
+        step lv.dt, COM velocity removed every step when remove_com)."""
         p = SimParams()
         p.lv = lv
         p.skin = skin
@@ -507,6 +622,9 @@ class Simulation:
         p.use_graph = 1 if use_graph else 0
         p.stats_every = 1
         p.max_rcut = max_rcut
+        p.integrator = {"langevin": INTEG_LANGEVIN, "nhc": INTEG_NHC}[integrator]
+        p.nhc_tau = nhc_tau
+        p.remove_com = 1 if remove_com else 0
         self.params = p
         h = C.c_void_p()
         check(lib.md_sim_create(C.byref(h), sys.h, engine.h, C.byref(p)), "Simulation")
@@ -531,6 +649,12 @@ class Simulation:
         v = C.c_int()
         check(lib.md_sim_uses_conditional_graph(self.h, C.byref(v)), "conditional")
         return bool(v.value)
+
+    def nhc_state(self):
+        """xi1, xi2, vxi1, vxi2, HamiltonianContribution of the driver's chain."""
+        out = np.zeros(5)
+        check(lib.md_sim_get_nhc_state(self.h, _p(out)), "nhc_state")
+        return out
 
     def attach_adapt_rcut(self, arc, sample_every=40, update_every=2000, prec=0.02, nrefine=0):
         """rcutAssignFeq / densityProfileSamplingFeq / rcutUpdateFeq of lj.nhc-xtc.cu."""

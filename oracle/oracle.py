@@ -45,6 +45,10 @@ _sigs = {
     "orc_normals4": (None, [u64, u64, u32, P(f64)]),
     "orc_md_langevin_run": (i32, [i32, P(f64), P(f64), P(f64), P(f32), P(f32), i32, i32, i32, P(f64),
                                   P(LvParams), P(f64), i32, i32, P(f64), P(i64)]),
+    "orc_md_nhc_run": (i32, [i32, P(f64), P(f64), P(f64), P(f32), P(f64), P(LvParams), i32, i32, i32, P(f64),
+                             P(f64), P(i64)]),
+    "orc_md_nhc_npt_run": (i32, [i32, P(f64), P(f64), P(f64), P(f32), P(f64), P(LvParams), f64, i32, i32,
+                                 P(f64), P(f64)]),
     "orc_num_threads": (i32, []),
     "orc_philox4x32_10": (None, [P(u32), P(u32), P(u32)]),
 }
@@ -197,6 +201,50 @@ def md_langevin_run(pos, vel, box, nsteps, *, dt, temperature, gamma_t, skin, rc
                                       nx, ny, nz, _p(b, f64), C.byref(prm), None if pc is None else _p(pc, f64),
                                       int(nsteps), int(cap), _p(stats, f64), _p(cnt, i64))
     return dict(pos=p, vel=v, box=b, stats=stats, rebuilds=int(cnt[0]), max_list=int(cnt[1]), status=status)
+
+
+def md_nhc_run(pos, vel, box, nsteps, *, dt, temperature, tau_t, skin, rcut, remove_com=True,
+               eps=1.0, sigma=1.0, shift=0.0, cap=1024, mass=None):
+    """CPU FP64 Nose-Hoover-chain velocity-Verlet MD (the lj.nhc-xtc step);
+    returns dict(pos, vel, stats, nhc, rebuilds, max_list, status)."""
+    p = np.ascontiguousarray(pos, np.float64).copy()
+    v = np.ascontiguousarray(vel, np.float64).copy()
+    n = p.shape[0]
+    b = np.ascontiguousarray(box, np.float64).copy()
+    prm = LvParams()
+    prm.dt, prm.temperature, prm.tau_p = dt, temperature, tau_t
+    prm.skin, prm.eps, prm.sigma, prm.shift = skin, eps, sigma, shift
+    rc = np.ascontiguousarray(rcut, np.float32)
+    m = None if mass is None else np.ascontiguousarray(mass, np.float64)
+    stats = np.zeros(7, np.float64)
+    nhc = np.zeros(5, np.float64)
+    cnt = np.zeros(2, np.int64)
+    status = _lib.orc_md_nhc_run(n, _p(p, f64), _p(v, f64), None if m is None else _p(m, f64), _p(rc, f32),
+                                 _p(b, f64), C.byref(prm), 1 if remove_com else 0, int(nsteps), int(cap),
+                                 _p(stats, f64), _p(nhc, f64), _p(cnt, i64))
+    return dict(pos=p, vel=v, stats=stats, nhc=nhc, rebuilds=int(cnt[0]), max_list=int(cnt[1]), status=status)
+
+
+def md_nhc_npt_run(pos, vel, box, nsteps, *, dt, temperature, tau_t, p_ref, tau_p, skin, rcut, pcorr=0.0,
+                   eps=1.0, sigma=1.0, shift=0.0, cap=1024, mass=None):
+    """CPU FP64 isobaric Nose-Hoover chain (MTK step of the reference operators);
+    returns dict(pos, vel, box, stats, state, status)."""
+    p = np.ascontiguousarray(pos, np.float64).copy()
+    v = np.ascontiguousarray(vel, np.float64).copy()
+    n = p.shape[0]
+    b = np.ascontiguousarray(box, np.float64).copy()
+    prm = LvParams()
+    prm.dt, prm.temperature, prm.gamma_t, prm.tau_p = dt, temperature, tau_t, tau_p
+    prm.p_ref[0] = p_ref
+    prm.skin, prm.eps, prm.sigma, prm.shift = skin, eps, sigma, shift
+    rc = np.ascontiguousarray(rcut, np.float32)
+    m = None if mass is None else np.ascontiguousarray(mass, np.float64)
+    stats = np.zeros(7, np.float64)
+    state = np.zeros(5, np.float64)
+    status = _lib.orc_md_nhc_npt_run(n, _p(p, f64), _p(v, f64), None if m is None else _p(m, f64), _p(rc, f32),
+                                     _p(b, f64), C.byref(prm), float(pcorr), int(nsteps), int(cap), _p(stats, f64),
+                                     _p(state, f64))
+    return dict(pos=p, vel=v, box=b, stats=stats, state=state, status=status)
 
 
 def num_threads():
@@ -357,6 +405,31 @@ def ref_spme(pos, q, box, beta, K, rcut, method, order):
     return dict(dir=df, rec=rf, energy=e.value, err_dir=ed.value, err_rec=er.value, err_interp=ei.value)
 
 
+def ref_selfcorr(pos, q, box, beta, K, order):
+    """The reference's own SelfCorr (oracle/_ref/libref_spme.so): the self-force
+    correction added to zero forces."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libref_spme.so"))
+    lib.ref_selfcorr.argtypes = [i32, P(f64), P(f64), P(f64), f64, P(i32), i32, P(f64)]
+    p = np.ascontiguousarray(pos, np.float64)
+    qq = np.ascontiguousarray(q, np.float64)
+    b = np.ascontiguousarray(box, np.float64)
+    KK = np.ascontiguousarray(K, np.int32)
+    F = np.zeros_like(p)
+    lib.ref_selfcorr(p.shape[0], _p(p, f64), _p(qq, f64), _p(b, f64), beta, _p(KK, i32), order, _p(F, f64))
+    return F
+
+
+def spme_selfcorr(pos, q, box, K, order, beta):
+    """Oracle restatement of SelfCorr: the correction added to zero forces."""
+    p = np.ascontiguousarray(pos, np.float64)
+    qq = np.ascontiguousarray(q, np.float64)
+    b = np.ascontiguousarray(box, np.float64)
+    KK = np.ascontiguousarray(K, np.int32)
+    F = np.zeros_like(p)
+    _lib.orc_spme_selfcorr(p.shape[0], _p(p, f64), _p(qq, f64), _p(b, f64), _p(KK, i32), order, beta, _p(F, f64))
+    return F
+
+
 # ---------------------------------------------------------------- SPME / Ewald
 _sigs3 = {
     "orc_bspline_weights": (None, [i32, f64, P(f64), P(f64)]),
@@ -367,6 +440,7 @@ _sigs3 = {
     "orc_ewald_rec_exact": (f64, [i32, P(f64), P(f64), P(f64), P(i32), f64, P(f64)]),
     "orc_ewald_dir": (f64, [i32, P(f64), P(f64), P(f64), f64, f64, P(f64)]),
     "orc_ewald_self": (f64, [i32, P(f64), f64]),
+    "orc_spme_selfcorr": (None, [i32, P(f64), P(f64), P(f64), P(i32), i32, f64, P(f64)]),
 }
 for _n, (_r, _a) in _sigs3.items():
     _f = getattr(_lib, _n)

@@ -317,6 +317,232 @@ int orc_md_langevin_run(int n, double* pos, double* vel, const double* mass, con
   return status;
 }
 
+/* ---------------------------------------------------------------- NHC NVT
+ * The step of ENG/app/lj.nhc-xtc.cu:159-200 restated literally in FP64:
+ * COM velocity removal (TranslationalFreedomRemover), NoseHoover_Chains2::
+ * operator_L(dt/2) (ENG/src/Thermostat.cu:255-275: the kinetic energy summed
+ * again after the velocity scaling), velocity Verlet step1, displacement test
+ * and rebuild, forces, step2, operator_L(dt/2). */
+typedef struct {
+  double xi1, xi2, vxi1, vxi2, Q1, Q2, LL, T;
+} orc_nhc;
+
+static double kinetic_sum(const orc_state* s, double K3[3]) {
+  double K[3] = {0, 0, 0};
+  for (int i = 0; i < s->n; ++i)
+    for (int d = 0; d < 3; ++d) K[d] += 0.5 / s->invm[i] * s->vel[3 * i + d] * s->vel[3 * i + d];
+  if (K3) for (int d = 0; d < 3; ++d) K3[d] = K[d];
+  return K[0] + K[1] + K[2];
+}
+
+static void nhc_L(orc_state* s, orc_nhc* c, double dt, double K3out[3]) {
+  c->vxi2 += (c->Q1 * c->vxi1 * c->vxi1 - c->T) / c->Q2 * (0.5 * dt);        /* G2 */
+  c->vxi1 *= exp(-c->vxi2 * 0.25 * dt);                                      /* vxi1 */
+  c->vxi1 += (2.0 * kinetic_sum(s, NULL) - c->LL * c->T) / c->Q1 * (0.5 * dt); /* G1 */
+  c->vxi1 *= exp(-c->vxi2 * 0.25 * dt);
+  const double a = exp(-c->vxi1 * dt);                                       /* Cv */
+  for (int k = 0; k < 3 * s->n; ++k) s->vel[k] *= a;
+  c->xi1 += c->vxi1 * dt;                                                    /* xi */
+  c->xi2 += c->vxi2 * dt;
+  c->vxi1 *= exp(-c->vxi2 * 0.25 * dt);
+  c->vxi1 += (2.0 * kinetic_sum(s, K3out) - c->LL * c->T) / c->Q1 * (0.5 * dt);
+  c->vxi1 *= exp(-c->vxi2 * 0.25 * dt);
+  c->vxi2 += (c->Q1 * c->vxi1 * c->vxi1 - c->T) / c->Q2 * (0.5 * dt);
+}
+
+static void remove_com(orc_state* s) {
+  double P[3] = {0, 0, 0}, M = 0;
+  for (int i = 0; i < s->n; ++i) {
+    const double m = 1.0 / s->invm[i];
+    M += m;
+    for (int d = 0; d < 3; ++d) P[d] += m * s->vel[3 * i + d];
+  }
+  for (int i = 0; i < s->n; ++i)
+    for (int d = 0; d < 3; ++d) s->vel[3 * i + d] -= P[d] / M;
+}
+
+/* p: dt, temperature (target T), gamma_t (unused), tau_p = tau_T of the chain,
+   skin, eps, sigma, shift.  stats_out (7): E, Wxx..Wzz, Kxx..Kzz after the last
+   step; nhc_out (5): xi1, xi2, vxi1, vxi2, HamiltonianContribution. */
+int orc_md_nhc_run(int n, double* pos, double* vel, const double* mass, const float* rcut, double box[3],
+                   const orc_lv_params* p, int remove_com_flag, int nsteps, int cap, double* stats_out,
+                   double* nhc_out, int64_t* counters_out) {
+  orc_state s;
+  memset(&s, 0, sizeof(s));
+  s.n = n;
+  s.cap = cap;
+  s.pos = pos;
+  s.vel = vel;
+  s.invm = (double*)malloc(sizeof(double) * n);
+  s.force = (double*)calloc(3 * (size_t)n, sizeof(double));
+  s.backup = (double*)malloc(sizeof(double) * 3 * n);
+  s.rcut = (float*)malloc(sizeof(float) * n);
+  s.image = (int*)calloc(3 * (size_t)n, sizeof(int));
+  s.nnb = (int*)calloc(n, sizeof(int));
+  s.list = (int*)malloc(sizeof(int) * (size_t)n * cap);
+  for (int i = 0; i < n; ++i) {
+    s.invm[i] = mass ? 1.0 / mass[i] : 1.0;
+    s.rcut[i] = rcut[i];
+  }
+  for (int d = 0; d < 3; ++d) s.L[d] = box[d];
+  orc_nhc c;
+  c.LL = 3.0 * n;
+  c.T = p->temperature;
+  c.Q1 = p->tau_p * p->tau_p * c.T / (4 * M_PI * M_PI) * c.LL;
+  c.Q2 = c.Q1 / c.LL;
+  c.xi1 = c.xi2 = 1.0;
+  c.vxi1 = c.vxi2 = 0.0;
+  const double h = 0.5 * p->dt, sh2 = 0.25 * p->skin * p->skin;
+  int status = 0, maxc;
+  wrap_and_rcut(&s);
+  maxc = build_list(&s, p->skin);
+  if (maxc > cap) status = 2;
+  forces(&s, p);
+  double K3[3] = {0, 0, 0};
+  for (int it = 0; it < nsteps; ++it) {
+    if (remove_com_flag) remove_com(&s);
+    nhc_L(&s, &c, h, NULL);
+    int far = 0;
+    double Li[3] = {1.0 / s.L[0], 1.0 / s.L[1], 1.0 / s.L[2]};
+    for (int i = 0; i < n; ++i) {
+      double d2 = 0;
+      for (int d = 0; d < 3; ++d) {
+        s.vel[3 * i + d] += h * s.force[3 * i + d] * s.invm[i];
+        s.pos[3 * i + d] += p->dt * s.vel[3 * i + d];
+        double dd = mi(s.pos[3 * i + d] - s.backup[3 * i + d], s.L[d], Li[d]);
+        d2 += dd * dd;
+      }
+      if (d2 > sh2) far = 1;
+    }
+    if (far) {
+      s.rebuilds++;
+      wrap_and_rcut(&s);
+      maxc = build_list(&s, p->skin);
+      if (maxc > cap) status = 2;
+    }
+    forces(&s, p);
+    for (int k = 0; k < 3 * n; ++k) s.vel[k] += h * s.force[k] * s.invm[k / 3];
+    nhc_L(&s, &c, h, K3);
+  }
+  for (int d = 0; d < 3; ++d) s.stats[4 + d] = K3[d];
+  if (stats_out) memcpy(stats_out, s.stats, sizeof(double) * 7);
+  if (nhc_out) {
+    nhc_out[0] = c.xi1; nhc_out[1] = c.xi2; nhc_out[2] = c.vxi1; nhc_out[3] = c.vxi2;
+    nhc_out[4] = 0.5 * c.Q1 * c.vxi1 * c.vxi1 + 0.5 * c.Q2 * c.vxi2 * c.vxi2 + c.LL * c.T * c.xi1 + c.T * c.xi2;
+  }
+  if (counters_out) { counters_out[0] = s.rebuilds; counters_out[1] = maxc; }
+  free(s.invm); free(s.force); free(s.backup); free(s.rcut); free(s.image); free(s.nnb); free(s.list);
+  return status;
+}
+
+/* ---------------------------------------------------------------- NHC NPT
+ * NoseHoover_Chains2_Isobaric operators (ENG/src/Barostat.cu:6-460) restated
+ * literally in FP64 (velocities scaled in place, K summed again), composed
+ * into the MTK step L_CP(dt/2) L_v(dt/2) L_r(dt) L_box(dt) | list + forces |
+ * L_v(dt/2) L_CP(dt/2); the list is rebuilt every step. */
+typedef struct {
+  double ep, vep, xi1, vxi1, Nf, Q1, W, T, Pref, pcorr;
+} orc_nhcp;
+
+static double nhcp_P(const orc_state* s, const orc_nhcp* c, const double K[3]) {
+  const double V = s->L[0] * s->L[1] * s->L[2];
+  double P = 0;
+  for (int d = 0; d < 3; ++d) P += 2.0 / V * (K[d] - 0.5 * s->stats[1 + d]);
+  return P / 3.0 + c->pcorr;
+}
+
+static void nhcp_L_CP(orc_state* s, orc_nhcp* c, double t) {
+  const double V = s->L[0] * s->L[1] * s->L[2];
+  double K3[3];
+  double K = kinetic_sum(s, K3);
+  c->vxi1 += (2.0 * K + c->W * c->vep * c->vep - (c->Nf + 1.0) * c->T) / c->Q1 * (0.5 * t); /* G1 */
+  c->vep *= exp(-c->vxi1 * 0.25 * t);                                                        /* vep */
+  c->vep += (6.0 / c->Nf * K + 3.0 * V * (nhcp_P(s, c, K3) - c->Pref)) / c->W * (0.5 * t);   /* Gep */
+  c->vep *= exp(-c->vxi1 * 0.25 * t);
+  const double a = exp(-(c->vxi1 + (1.0 + 3.0 / c->Nf) * c->vep) * t);                       /* Cv */
+  for (int k = 0; k < 3 * s->n; ++k) s->vel[k] *= a;
+  K = kinetic_sum(s, K3);
+  c->xi1 += c->vxi1 * t;                                                                     /* xi */
+  c->vep *= exp(-c->vxi1 * 0.25 * t);
+  c->vep += (6.0 / c->Nf * K + 3.0 * V * (nhcp_P(s, c, K3) - c->Pref)) / c->W * (0.5 * t);
+  c->vep *= exp(-c->vxi1 * 0.25 * t);
+  c->vxi1 += (2.0 * K + c->W * c->vep * c->vep - (c->Nf + 1.0) * c->T) / c->Q1 * (0.5 * t);
+  for (int d = 0; d < 3; ++d) s->stats[4 + d] = K3[d];
+}
+
+/* p: dt, temperature, gamma_t = tau_T, tau_p = tau_P, p_ref[0] = P_ref, skin, LJ;
+   pcorr: constant pressure correction.  state_out (5): ep, vep, xi1, vxi1, H. */
+int orc_md_nhc_npt_run(int n, double* pos, double* vel, const double* mass, const float* rcut, double box[3],
+                       const orc_lv_params* p, double pcorr, int nsteps, int cap, double* stats_out,
+                       double* state_out) {
+  orc_state s;
+  memset(&s, 0, sizeof(s));
+  s.n = n;
+  s.cap = cap;
+  s.pos = pos;
+  s.vel = vel;
+  s.invm = (double*)malloc(sizeof(double) * n);
+  s.force = (double*)calloc(3 * (size_t)n, sizeof(double));
+  s.backup = (double*)malloc(sizeof(double) * 3 * n);
+  s.rcut = (float*)malloc(sizeof(float) * n);
+  s.image = (int*)calloc(3 * (size_t)n, sizeof(int));
+  s.nnb = (int*)calloc(n, sizeof(int));
+  s.list = (int*)malloc(sizeof(int) * (size_t)n * cap);
+  for (int i = 0; i < n; ++i) {
+    s.invm[i] = mass ? 1.0 / mass[i] : 1.0;
+    s.rcut[i] = rcut[i];
+  }
+  for (int d = 0; d < 3; ++d) s.L[d] = box[d];
+  orc_nhcp c;
+  c.Nf = 3.0 * n - 3.0;
+  c.T = p->temperature;
+  c.Q1 = p->gamma_t * p->gamma_t * c.T * c.Nf;
+  c.W = p->tau_p * p->tau_p * c.T * c.Nf;
+  c.Pref = p->p_ref[0];
+  c.pcorr = pcorr;
+  c.ep = log(s.L[0] * s.L[1] * s.L[2]) / 3.0;
+  c.vep = 0.0;
+  c.xi1 = 1.0;
+  c.vxi1 = 0.0;
+  const double h = 0.5 * p->dt;
+  int status = 0;
+  wrap_and_rcut(&s);
+  if (build_list(&s, p->skin) > cap) status = 2;
+  forces(&s, p);
+  for (int it = 0; it < nsteps; ++it) {
+    nhcp_L_CP(&s, &c, h);
+    for (int k = 0; k < 3 * n; ++k) s.vel[k] += h * s.force[k] * s.invm[k / 3];      /* L_v */
+    {                                                                                 /* L_r */
+      const double xx = c.vep * p->dt * 0.5, s1 = exp(c.vep * p->dt);
+      const double x2 = xx * xx, x4 = x2 * x2, x6 = x4 * x2, x8 = x6 * x2, x10 = x8 * x2;
+      const double s2 = p->dt * exp(xx) *
+                        (1. + 1. / 6. * x2 + 1. / 120. * x4 + 1. / 5040. * x6 + 1. / 362880. * x8 +
+                         1. / 39916800. * x10);
+      for (int k = 0; k < 3 * n; ++k) s.pos[k] = s1 * s.pos[k] + s2 * s.vel[k];
+    }
+    {                                                                                 /* L_box */
+      const double sc = exp(c.vep * p->dt);
+      for (int d = 0; d < 3; ++d) s.L[d] *= sc;
+      c.ep += p->dt * c.vep;
+    }
+    wrap_and_rcut(&s);
+    if (build_list(&s, p->skin) > cap) status = 2;
+    forces(&s, p);
+    for (int k = 0; k < 3 * n; ++k) s.vel[k] += h * s.force[k] * s.invm[k / 3];
+    nhcp_L_CP(&s, &c, h);
+  }
+  for (int d = 0; d < 3; ++d) box[d] = s.L[d];
+  if (stats_out) memcpy(stats_out, s.stats, sizeof(double) * 7);
+  if (state_out) {
+    const double V = s.L[0] * s.L[1] * s.L[2];
+    state_out[0] = c.ep; state_out[1] = c.vep; state_out[2] = c.xi1; state_out[3] = c.vxi1;
+    state_out[4] = 0.5 * c.W * c.vep * c.vep + 0.5 * c.Q1 * c.vxi1 * c.vxi1 + (c.Nf + 1.0) * c.T * c.xi1 +
+                   c.Pref * V;
+  }
+  free(s.invm); free(s.force); free(s.backup); free(s.rcut); free(s.image); free(s.nnb); free(s.list);
+  return status;
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -243,3 +243,57 @@ double orc_ewald_self(int natom, const double* q, double beta) {
   for (int i = 0; i < natom; ++i) s += q[i] * q[i];
   return -beta / sqrt(M_PI) * s;
 }
+
+/* Self-force correction of analytic-differentiation SPME (SelfCorr::calKernel
+   and ::correction, RE/src/SelfCorr.cpp:99-220), rectangular box, |k| <= 3:
+     c_d(k) = sum_m (e^{-pi^2 m^2/beta^2}/m^2 / (2 pi V)) (-2) g_d(m_d, k) (-4 pi k K_d / L_d)
+     g_d(m, k) = (u + 2 pi k)^-n / sum_{l=-3..3} (u + 2 pi l)^-n,  u = 2 pi m / K_d
+   (0 at the Nyquist index of an even K_d), then for k = 1..3
+     F_id -= c_d(k) q_i^2 sin(2 pi k K_d x_id / L_d). */
+static double ipow_d(double x, int n) {
+  double r = 1;
+  for (int i = 0; i < n; ++i) r *= x;
+  return r;
+}
+
+static double alias_sum(double u, int n) {
+  double s = 1. / ipow_d(u, n), up = u, un = u;
+  for (int l = 0; l < 3; ++l) {
+    up += 2. * M_PI;
+    un -= 2. * M_PI;
+    s += 1. / ipow_d(up, n);
+    s += 1. / ipow_d(un, n);
+  }
+  return s;
+}
+
+void orc_spme_selfcorr(int natom, const double* pos, const double* q, const double box[3], const int K[3],
+                       int order, double beta, double* force) {
+  const double V = box[0] * box[1] * box[2];
+  const double scalor = 1. / (2. * M_PI * V);
+  double c[3][4] = {{0}};
+  for (int kk = 1; kk <= 3; ++kk) {
+    for (int i0 = 0; i0 < K[0]; ++i0)
+      for (int i1 = 0; i1 < K[1]; ++i1)
+        for (int i2 = 0; i2 < K[2]; ++i2) {
+          const int idx[3] = {i0, i1, i2};
+          int p[3];
+          for (int d = 0; d < 3; ++d) p[d] = idx[d] > (K[d] >> 1) ? idx[d] - K[d] : idx[d];
+          const double m[3] = {p[0] / box[0], p[1] / box[1], p[2] / box[2]};
+          const double m2 = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+          if (m2 == 0) continue;
+          const double t = M_PI / beta;
+          const double fm = exp(-t * t * m2) / m2 * scalor;
+          for (int d = 0; d < 3; ++d) {
+            if (idx[d] == (K[d] >> 1) && (K[d] % 2 == 0)) continue;
+            const double u = 2. * M_PI * p[d] / K[d];
+            const double g = 1. / ipow_d(u + 2. * M_PI * kk, order) / alias_sum(u, order);
+            c[d][kk] += (-2. * fm * g) * (-4.) * M_PI * kk * (double)K[d] / box[d];
+          }
+        }
+  }
+  for (int i = 0; i < natom; ++i)
+    for (int kk = 1; kk <= 3; ++kk)
+      for (int d = 0; d < 3; ++d)
+        force[3 * i + d] -= c[d][kk] * q[i] * q[i] * sin(2. * M_PI * kk * K[d] / box[d] * pos[3 * i + d]);
+}

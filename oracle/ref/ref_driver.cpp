@@ -53,6 +53,26 @@ extern "C" int ref_spme_forces(int n, const double* pos, const double* q, const 
   if (err_interp && method == 0) ele.errorEstimateInterpolRec(*err_interp);
   return 0;
 }
+
+// SelfCorr::reinit + correction (app/spme.cpp:266-270): adds the self-force
+// correction of analytic differentiation to force [n][3]
+#include "SelfCorr.h"
+extern "C" int ref_selfcorr(int n, const double* pos, const double* q, const double* box, double beta,
+                            const int* K, int order, double* force) {
+  std::vector<std::vector<double> > p(n, std::vector<double>(3)), f(n, std::vector<double>(3));
+  std::vector<double> qq(q, q + n);
+  for (int i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) { p[i][d] = pos[3 * i + d]; f[i][d] = force[3 * i + d]; }
+  std::ostringstream sink;  // reinit prints progress on stdout
+  std::streambuf* keep = std::cout.rdbuf(sink.rdbuf());
+  SelfCorr sc;
+  sc.reinit(beta, order, K[0], K[1], K[2], box[0], box[1], box[2]);
+  std::cout.rdbuf(keep);
+  sc.correction(p, qq, f);
+  for (int i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) force[3 * i + d] = f[i][d];
+  return 0;
+}
 #endif
 
 #ifdef REF_ARC

@@ -166,3 +166,16 @@ def test_error_estimates_on_device(mdf, orc, small, prec):
     beta = mdf.choose_beta(sys, 4.0, 1e-4)
     d, _ = mdf.errorEstimatePME(sys, (16, 16, 16), beta, 4.0)
     assert abs(d - 1e-4) < 1e-9
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_self_correction(mdf, orc, small, prec):
+    pos, q, box = small
+    for K, order in (((16, 16, 32), 6), ((32, 16, 16), 4)):
+        sys = make(mdf, pos, q, box, prec)
+        sp = mdf.SPME(sys, K, order, 1.3, "analytic")
+        eng = mdf.InteractionEngine(sys)
+        eng.clearInteraction()
+        sp.self_correction()
+        Fo = orc.spme_selfcorr(sys.positions(), q, box, K, order, 1.3)
+        assert np.abs(sys.forces() - Fo).max() < (1e-6 if prec == 0 else 1e-13) * np.abs(Fo).max()

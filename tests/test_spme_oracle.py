@@ -86,3 +86,14 @@ def test_error_estimates_match_reference_build(orc, charges, K, order):
     assert abs(d - ref["err_dir"]) <= 1e-14 * ref["err_dir"]
     assert abs(r - ref["err_rec"]) <= 1e-13 * ref["err_rec"]
     assert abs(e - ref["err_interp"]) <= 1e-13 * ref["err_interp"]
+
+
+@pytest.mark.parametrize("K,order", [((16, 16, 16), 6), ((16, 12, 15), 4), ((8, 16, 32), 8)])
+def test_selfcorr_oracle_matches_reference_build(orc, charges, K, order):
+    if not orc.ref_available("libref_spme.so"):
+        pytest.skip("reference SPME not built")
+    pos, q, box = charges
+    box = np.array([box[0], box[1], box[2] * 1.125])
+    a = orc.spme_selfcorr(pos, q, box, K, order, 1.5)
+    b = orc.ref_selfcorr(pos, q, box, 1.5, K, order)
+    assert np.abs(a - b).max() < 1e-12 * np.abs(b).max()
