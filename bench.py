@@ -55,6 +55,19 @@ def dist_env():
     return rank, world, local
 
 
+def replica_rate(torch, steps, t_local, world, device):
+    """Whole-job steps/s of `world` independent replicas: every rank ran
+    `steps` steps; the job's time is the slowest rank's (max over ranks,
+    all-reduced on `device` through the initialised process group)."""
+    t_max = t_local
+    if world > 1:
+        tt = torch.tensor([t_local], device=device, dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_max = float(tt.item())
+        torch.distributed.barrier()
+    return world * steps / t_max, t_max
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
@@ -337,13 +350,7 @@ def main():
         t_mixed = time_steps(torch, sim_m, stream, args.steps, flush, nvtx_range="timed")
     steps_done, rebuilds, flags = sim_m.counters()
     rebuilds_timed = rebuilds - rebuilds0
-    t_max = t_mixed
-    if world > 1:
-        tt = torch.tensor([t_mixed], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_max = float(tt.item())
-        torch.distributed.barrier()
-    value = world * args.steps / t_max
+    value, t_max = replica_rate(torch, args.steps, t_mixed, world, "cuda")
 
     # back-to-back (warm L2) throughput of the same loop, for reference
     torch.cuda.synchronize()

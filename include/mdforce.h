@@ -252,6 +252,24 @@ int md_error_estimate_spme_ik_noalloc(md_system* sys, const int K[3], int order,
 /* splitting beta whose real-space estimate equals target at cutoff rcut */
 int md_choose_beta(md_system* sys, double rcut, double target, double* beta);
 
+/* Inhomogeneous ik-SPME error map (ErrorEstimate_SPME_Ik::reinit / calError,
+ * longRange.hetero/profile.test/template/tools/analyze/src/ErrorEstimate_SPME_Ik.cpp:80-470,
+ * as driven by analyze/app/error.spme.ik.cpp): on the grid K (the SPME mesh, also the
+ * density-profile bins) of a rectangular box L, for B-spline order `order` and splitting
+ * beta.  The kernel is built at creation (FP64 3D transforms on the device).  Profiles:
+ * rho1 = density of charge signs (+1 / -1 per charge), rho2 = number density of charges,
+ * [K0][K1][K2]; set explicitly or averaged over deposited samples of a system. */
+typedef struct md_errmap md_errmap;
+int md_errmap_create(md_errmap** out, const int K[3], const double L[3], double beta, int order,
+                     int device);
+int md_errmap_destroy(md_errmap* h);
+int md_errmap_set_profile(md_errmap* h, const double* rho1, const double* rho2);
+int md_errmap_deposit(md_errmap* h, md_system* sys);
+int md_errmap_get_profile(md_errmap* h, double* rho1, double* rho2);
+/* error1, error2 [K0][K1][K2][2] (real, imaginary) for charge magnitude `charge`; the
+   RMS force error at a grid point is sqrt(error1[..][0] + error2[..][0]) (print_error) */
+int md_errmap_compute(md_errmap* h, double charge, double* error1, double* error2);
+
 /* ------------------------------------------------------- per-atom cutoff
  * Replaces AssignRCut::getRCut + assign (ENG/src/AssignRCut.cu:46-117):
  * rcut_i = lattice[iz + nz*(iy + ny*ix)], ix = int((x*nx)/Lx) etc. (binary32). */

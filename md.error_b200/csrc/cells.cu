@@ -139,22 +139,30 @@ __global__ void k_scatter(int N, const uint32_t* t_cell, const uint32_t* slot, c
 }
 
 // warp per cell: rank each member by its previous slot (ascending)
-__global__ void k_order(int ntot, const uint32_t* start, const uint32_t* members, uint32_t* perm,
-                        const DevState* st, int gate) {
+// Members of a cell are ranked by (cutoff, previous slot): atoms of equal
+// cutoff (hence similar list length) become neighbours in memory, so the
+// force kernel's warps, which take consecutive atoms, see rows of similar
+// length; the previous slot breaks ties, so the order is deterministic.
+__global__ void k_order(int ntot, const uint32_t* start, const uint32_t* members, const float* rcut,
+                        uint32_t* perm, const DevState* st, int gate) {
   if (gate && !(st->flags & FLAG_REBUILD)) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= ntot) return;
   const uint32_t s = start[warp], n = start[warp + 1] - s;
+  auto key = [&](uint32_t e) -> unsigned long long {
+    return ((unsigned long long)__float_as_uint(rcut[e]) << 32) | e;  // rcut >= 0 orders as its bits
+  };
   for (uint32_t b = 0; b < n; b += 32) {
-    uint32_t e = (b + lane < n) ? members[s + b + lane] : 0xffffffffu;
+    const uint32_t e = (b + lane < n) ? members[s + b + lane] : 0xffffffffu;
+    const unsigned long long ke = (b + lane < n) ? key(e) : ~0ull;
     uint32_t rank = 0;
     for (uint32_t b2 = 0; b2 < n; b2 += 32) {
-      uint32_t v = (b2 + lane < n) ? members[s + b2 + lane] : 0xffffffffu;
+      const unsigned long long v = (b2 + lane < n) ? key(members[s + b2 + lane]) : ~0ull;
 #pragma unroll 8
       for (int t = 0; t < 32; ++t) {
-        uint32_t vt = __shfl_sync(0xffffffffu, v, t);
-        rank += (vt < e) ? 1u : 0u;
+        const unsigned long long vt = __shfl_sync(0xffffffffu, v, t);
+        rank += (vt < ke) ? 1u : 0u;
       }
     }
     if (b + lane < n) perm[s + rank] = e;
@@ -241,7 +249,7 @@ static int rebuild_t(md_cell_list* cl, md_system* sys, Recorder* rec, bool gated
   }
   {
     int n = cl->ntot;
-    void* a[] = {&n, &cl->start, &cl->members, &cl->perm, &st, &gate};
+    void* a[] = {&n, &cl->start, &cl->members, &sys->rcut, &cl->perm, &st, &gate};
     if (int r = rec_launch(rec, (const void*)k_order, dim3(ceil_div((long long)n * 32, 256)), dim3(256), 0, a)) return r;
   }
   {

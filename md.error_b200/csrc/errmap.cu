@@ -1,0 +1,366 @@
+// Inhomogeneous ik-SPME error estimate on the mesh, FP64 on the GPU.
+// Reference: ErrorEstimate_SPME_Ik::reinit / calKernel / calError
+// (longRange.hetero/profile.test/template/tools/analyze/src/ErrorEstimate_SPME_Ik.cpp:80-470),
+// driven by analyze/app/error.spme.ik.cpp:82-85 with the density profile of
+// DensityProfile_PiecewiseConst (analyze/src/DensityProfile.cpp:7-90) on the
+// same grid as the mesh.  With N grid points, V the volume, rectangular box:
+//   g(m)       = -4 pi f(m) m*,  f = e^{-pi^2 |m*|^2/beta^2} / |m*|^2 / (2 pi V)
+//   a_d(m, k)  = (u + 2 pi k)^-n / sum_{l=-3..3} (u + 2 pi l)^-n,  u = 2 pi m_d / K_d
+//   k2b        = sum_{k = +-1..+-4} sum_dir V/N |IFFT(i g a_dir(k))|^2
+//   k1         = V i g 2 sum_{k, dir} a_dir(k)          (k space)
+//   k2a        = FFT(V/N |IFFT(k1 / V)|^2) + 2 FFT(k2b)
+//   e1_d = IFFT(k1_d FFT(rho1 V/N)) q/V,  e2 = IFFT(k2a FFT(rho2 V/N)) q^2/V
+//   error1 = sum_d e1_d^2 (real and imaginary parts apart), error2 = e2
+// (components of g zeroed at the Nyquist index of an even K_d).  The kernel
+// takes 25 batched 3D transforms at creation; an evaluation takes 2 + 4.
+// rho1 is the density of charge signs, rho2 the number density of charges
+// (profile1 / profile2 of the reference).
+#include <cmath>
+#include <vector>
+#include "device_common.cuh"
+
+int dft3_grid(double2* data, const int n[3], int sign, int batch, cudaStream_t stream);
+
+namespace {
+
+struct EmGrid {
+  int K[3];
+  long N;
+  double L[3];
+};
+
+__device__ __forceinline__ int em_c(int i, int K) { return i > (K >> 1) ? i - K : i; }
+__device__ __forceinline__ void em_idx(long t, const EmGrid& g, int ii[3]) {
+  ii[2] = (int)(t % g.K[2]);
+  ii[1] = (int)((t / g.K[2]) % g.K[1]);
+  ii[0] = (int)(t / ((long)g.K[2] * g.K[1]));
+}
+
+__device__ __forceinline__ double em_pow(double x, int n) {
+  double r = 1.0;
+  for (int i = 0; i < n; ++i) r *= x;
+  return r;
+}
+
+__device__ double em_alias(double u, int n) {
+  double s = 1.0 / em_pow(u, n), up = u, un = u;
+  for (int l = 0; l < 3; ++l) {
+    up += 2.0 * M_PI;
+    un -= 2.0 * M_PI;
+    s += 1.0 / em_pow(up, n);
+    s += 1.0 / em_pow(un, n);
+  }
+  return s;
+}
+
+__global__ void k_em_g(EmGrid g, double beta, double* gm /* [3][N] */) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= g.N) return;
+  int ii[3];
+  em_idx(t, g, ii);
+  const double m[3] = {em_c(ii[0], g.K[0]) / g.L[0], em_c(ii[1], g.K[1]) / g.L[1], em_c(ii[2], g.K[2]) / g.L[2]};
+  const double m2 = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+  const double V = g.L[0] * g.L[1] * g.L[2];
+  double fm = 0.0;
+  if (m2 != 0.0) {
+    const double tt = M_PI / beta;
+    fm = exp(-tt * tt * m2) / m2 / (2.0 * M_PI * V);
+  }
+  for (int d = 0; d < 3; ++d) gm[d * g.N + t] = -4.0 * M_PI * fm * m[d];
+}
+
+// w_d = i g_d a(k) for one (k, dir), or with k == 0 the final 2 sum_{k, dir} a;
+// k1 (nullable) receives V w
+__global__ void k_em_fill(EmGrid g, int order, const double* gm, int k, int dir, double2* w, double2* k1) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= g.N) return;
+  int ii[3];
+  em_idx(t, g, ii);
+  double a = 0.0;
+  if (t != 0) {
+    if (k != 0) {
+      const double u = 2.0 * M_PI * em_c(ii[dir], g.K[dir]) / g.K[dir];
+      a = 1.0 / em_pow(u + 2.0 * M_PI * k, order) * (1.0 / em_alias(u, order));
+    } else {
+      double u[3], fen[3];
+      for (int d = 0; d < 3; ++d) {
+        u[d] = 2.0 * M_PI * em_c(ii[d], g.K[d]) / g.K[d];
+        fen[d] = 1.0 / em_alias(u[d], order);
+      }
+      for (int kk = -4; kk <= 4; ++kk) {
+        if (kk == 0) continue;
+        for (int d = 0; d < 3; ++d) a += 1.0 / em_pow(u[d] + 2.0 * M_PI * kk, order) * fen[d];
+      }
+      a *= 2.0;
+    }
+  }
+  const double V = g.L[0] * g.L[1] * g.L[2];
+  for (int d = 0; d < 3; ++d) {
+    double v = gm[d * g.N + t] * a;
+    if (t == 0 || ((g.K[d] % 2 == 0) && ii[d] == (g.K[d] >> 1))) v = 0.0;
+    w[d * g.N + t] = make_double2(0.0, v);
+    if (k1) k1[d * g.N + t] = make_double2(0.0, v * V);
+  }
+}
+
+// out (+)= sum_d |w_d|^2 V / N as a real complex value
+__global__ void k_em_sq(EmGrid g, const double2* w, double2* out, int accumulate) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= g.N) return;
+  double s = 0.0;
+  for (int d = 0; d < 3; ++d) {
+    const double2 v = w[d * g.N + t];
+    s += v.x * v.x + v.y * v.y;
+  }
+  const double V = g.L[0] * g.L[1] * g.L[2];
+  s *= V / (double)g.N;
+  if (accumulate) out[t].x += s;
+  else out[t] = make_double2(s, 0.0);
+}
+
+__global__ void k_em_axpy2(long N, double2* a, const double2* b) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= N) return;
+  a[t].x += 2.0 * b[t].x;
+  a[t].y += 2.0 * b[t].y;
+}
+
+__global__ void k_em_load(EmGrid g, const double* rho1, const double* rho2, double2* r) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= g.N) return;
+  const double s = g.L[0] * g.L[1] * g.L[2] / (double)g.N;
+  r[t] = make_double2(rho1[t] * s, 0.0);
+  r[g.N + t] = make_double2(rho2[t] * s, 0.0);
+}
+
+__global__ void k_em_mult(EmGrid g, const double2* k1, const double2* k2a, const double2* r, double2* e) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= g.N) return;
+  const double2 r1 = r[t], r2 = r[g.N + t];
+  for (int d = 0; d < 3; ++d) {
+    const double2 a = k1[d * g.N + t];
+    e[d * g.N + t] = make_double2(r1.x * a.x - r1.y * a.y, r1.x * a.y + r1.y * a.x);
+  }
+  const double2 b = k2a[t];
+  e[3 * g.N + t] = make_double2(r2.x * b.x - r2.y * b.y, r2.x * b.y + r2.y * b.x);
+}
+
+__global__ void k_em_finish(EmGrid g, const double2* e, double charge, double* e1, double* e2) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= g.N) return;
+  const double V = g.L[0] * g.L[1] * g.L[2];
+  double s0 = 0.0, s1 = 0.0;
+  for (int d = 0; d < 3; ++d) {
+    const double re = e[d * g.N + t].x * charge / V, im = e[d * g.N + t].y;  // calError scales the real parts
+    s0 += re * re;
+    s1 += im * im;
+  }
+  e1[2 * t] = s0;
+  e1[2 * t + 1] = s1;
+  e2[2 * t] = e[3 * g.N + t].x * charge * charge / V;
+  e2[2 * t + 1] = e[3 * g.N + t].y;
+}
+
+// profile of charge signs and of charges, counts per grid bin
+// (DensityProfile_PiecewiseConst::reinit_conf binning)
+template <class R>
+__global__ void k_em_deposit(int N, const typename V4<R>::T* pos, EmGrid g, double* cnt1, double* cnt2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const typename V4<R>::T p = pos[i];
+  if (p.w == R(0)) return;
+  const double c[3] = {(double)p.x, (double)p.y, (double)p.z};
+  unsigned b[3];
+  for (int d = 0; d < 3; ++d) {
+    double x = c[d];
+    if (x >= g.L[d]) x -= g.L[d];
+    else if (x < 0) x += g.L[d];
+    const double q = x / (g.L[d] / g.K[d]);
+    b[d] = q > 0 ? (unsigned)q : 0u;
+    if (b[d] >= (unsigned)g.K[d]) b[d] = g.K[d] - 1;
+  }
+  const long idx = b[2] + (long)g.K[2] * (b[1] + (long)g.K[1] * b[0]);
+  atomicAdd(&cnt1[idx], p.w > R(0) ? 1.0 : -1.0);
+  atomicAdd(&cnt2[idx], 1.0);
+}
+
+__global__ void k_em_profile(long N, const double* cnt1, const double* cnt2, double inv, double* rho1, double* rho2) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= N) return;
+  rho1[t] = cnt1[t] * inv;
+  rho2[t] = cnt2[t] * inv;
+}
+
+}  // namespace
+
+struct md_errmap {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  EmGrid g;
+  double beta = 0;
+  int order = 0;
+  double2* k1 = nullptr;    // [3][N] k space
+  double2* k2a = nullptr;   // [N] k space
+  double2* work = nullptr;  // [4][N]
+  double2* work2 = nullptr; // [2][N]
+  double* rho = nullptr;    // [2][N] current profile (rho1, rho2)
+  double* cnt = nullptr;    // [2][N] deposited counts
+  int samples = 0;
+};
+
+static void em_free(md_errmap* h) {
+  void* p[] = {h->k1, h->k2a, h->work, h->work2, h->rho, h->cnt};
+  for (void* q : p) if (q) cudaFree(q);
+  if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+extern "C" int md_errmap_create(md_errmap** out, const int K[3], const double L[3], double beta, int order,
+                                int device) {
+  if (!out || !K || !L || !(beta > 0) || order < 2 || order > 14) {
+    md_set_error("md_errmap_create: bad arguments");
+    return MD_ERR_BADARG;
+  }
+  for (int d = 0; d < 3; ++d)
+    if (K[d] < 2 || K[d] > 1024 || !(L[d] > 0)) {
+      md_set_error("md_errmap_create: grid %d or box %g out of range on axis %d", K[d], L[d], d);
+      return MD_ERR_BADARG;
+    }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    md_set_error("md_errmap_create: no CUDA device %d", device);
+    return MD_ERR_CUDA;
+  }
+  MD_CUDA(cudaSetDevice(device));
+  md_errmap* h = new md_errmap();
+  h->device = device;
+  h->beta = beta;
+  h->order = order;
+  for (int d = 0; d < 3; ++d) { h->g.K[d] = K[d]; h->g.L[d] = L[d]; }
+  h->g.N = (long)K[0] * K[1] * K[2];
+  const long N = h->g.N;
+  double* gm = nullptr;
+  double2* k2b = nullptr;
+  bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaMalloc(&h->k1, sizeof(double2) * 3 * N) == cudaSuccess &&
+            cudaMalloc(&h->k2a, sizeof(double2) * N) == cudaSuccess &&
+            cudaMalloc(&h->work, sizeof(double2) * 4 * N) == cudaSuccess &&
+            cudaMalloc(&h->work2, sizeof(double2) * 2 * N) == cudaSuccess &&
+            cudaMalloc(&h->rho, sizeof(double) * 2 * N) == cudaSuccess &&
+            cudaMalloc(&h->cnt, sizeof(double) * 2 * N) == cudaSuccess &&
+            cudaMalloc(&gm, sizeof(double) * 3 * N) == cudaSuccess &&
+            cudaMalloc(&k2b, sizeof(double2) * N) == cudaSuccess;
+  auto fail = [&](int code) {
+    if (gm) cudaFree(gm);
+    if (k2b) cudaFree(k2b);
+    em_free(h);
+    delete h;
+    return code;
+  };
+  if (!ok) return fail(md_cuda_fail(cudaGetLastError(), "md_errmap_create allocation"));
+  cudaStream_t s = h->stream;
+  const unsigned nb = (unsigned)((N + 255) / 256);
+  MD_CUDA(cudaMemsetAsync(k2b, 0, sizeof(double2) * N, s));
+  MD_CUDA(cudaMemsetAsync(h->cnt, 0, sizeof(double) * 2 * N, s));
+  MD_CUDA(cudaMemsetAsync(h->rho, 0, sizeof(double) * 2 * N, s));
+  k_em_g<<<nb, 256, 0, s>>>(h->g, beta, gm);
+  for (int k = -4; k <= 4; ++k) {
+    if (k == 0) continue;
+    for (int dir = 0; dir < 3; ++dir) {
+      k_em_fill<<<nb, 256, 0, s>>>(h->g, order, gm, k, dir, h->work, nullptr);
+      if (int r = dft3_grid(h->work, h->g.K, +1, 3, s)) return fail(r);
+      k_em_sq<<<nb, 256, 0, s>>>(h->g, h->work, k2b, 1);
+    }
+  }
+  k_em_fill<<<nb, 256, 0, s>>>(h->g, order, gm, 0, 0, h->work, h->k1);
+  if (int r = dft3_grid(h->work, h->g.K, +1, 3, s)) return fail(r);
+  k_em_sq<<<nb, 256, 0, s>>>(h->g, h->work, h->k2a, 0);
+  if (int r = dft3_grid(h->k2a, h->g.K, -1, 1, s)) return fail(r);
+  if (int r = dft3_grid(k2b, h->g.K, -1, 1, s)) return fail(r);
+  k_em_axpy2<<<nb, 256, 0, s>>>(N, h->k2a, k2b);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(gm);
+  cudaFree(k2b);
+  gm = nullptr;
+  k2b = nullptr;
+  if (e != cudaSuccess) return fail(md_cuda_fail(e, "md_errmap_create kernel"));
+  *out = h;
+  return MD_OK;
+}
+
+extern "C" int md_errmap_destroy(md_errmap* h) {
+  if (!h) return MD_OK;
+  cudaSetDevice(h->device);
+  em_free(h);
+  delete h;
+  return MD_OK;
+}
+
+extern "C" int md_errmap_set_profile(md_errmap* h, const double* rho1, const double* rho2) {
+  if (!h || !rho1 || !rho2) return MD_ERR_BADARG;
+  MD_CUDA(cudaSetDevice(h->device));
+  const size_t b = sizeof(double) * h->g.N;
+  MD_CUDA(cudaMemcpyAsync(h->rho, rho1, b, cudaMemcpyHostToDevice, h->stream));
+  MD_CUDA(cudaMemcpyAsync(h->rho + h->g.N, rho2, b, cudaMemcpyHostToDevice, h->stream));
+  MD_CUDA(cudaStreamSynchronize(h->stream));
+  return MD_OK;
+}
+
+// one sample of the system's charges (sign and number per bin); the profile
+// becomes the average over the samples deposited so far
+extern "C" int md_errmap_deposit(md_errmap* h, md_system* sys) {
+  if (!h || !sys) return MD_ERR_BADARG;
+  DevState hs;
+  if (int r = sys->read_state(hs)) return r;
+  for (int d = 0; d < 3; ++d)
+    if (std::fabs(hs.L[d] - h->g.L[d]) > 1e-12 * h->g.L[d]) {
+      md_set_error("md_errmap_deposit: the system box differs from the error map's");
+      return MD_ERR_BADARG;
+    }
+  const int nb = ceil_div(sys->N, 256);
+  if (sys->prec == MD_PREC_FP64)
+    k_em_deposit<double><<<nb, 256, 0, sys->stream>>>(sys->N, (const double4a*)sys->pos, h->g, h->cnt,
+                                                      h->cnt + h->g.N);
+  else
+    k_em_deposit<float><<<nb, 256, 0, sys->stream>>>(sys->N, (const float4*)sys->pos, h->g, h->cnt, h->cnt + h->g.N);
+  MD_CHECK_LAUNCH("errmap deposit");
+  h->samples += 1;
+  const double dv = h->g.L[0] * h->g.L[1] * h->g.L[2] / (double)h->g.N;
+  k_em_profile<<<(unsigned)((h->g.N + 255) / 256), 256, 0, sys->stream>>>(h->g.N, h->cnt, h->cnt + h->g.N,
+                                                                         1.0 / (dv * h->samples), h->rho,
+                                                                         h->rho + h->g.N);
+  MD_CHECK_LAUNCH("errmap profile");
+  MD_CUDA(cudaStreamSynchronize(sys->stream));
+  return MD_OK;
+}
+
+// ErrorEstimate_SPME_Ik::calError: error1 [N][2], error2 [N][2] (real, imaginary);
+// the RMS force error of a grid point is sqrt(error1[i][0] + error2[i][0])
+extern "C" int md_errmap_compute(md_errmap* h, double charge, double* error1, double* error2) {
+  if (!h || !error1 || !error2) return MD_ERR_BADARG;
+  MD_CUDA(cudaSetDevice(h->device));
+  cudaStream_t s = h->stream;
+  const long N = h->g.N;
+  const unsigned nb = (unsigned)((N + 255) / 256);
+  k_em_load<<<nb, 256, 0, s>>>(h->g, h->rho, h->rho + N, h->work2);
+  if (int r = dft3_grid(h->work2, h->g.K, -1, 2, s)) return r;
+  k_em_mult<<<nb, 256, 0, s>>>(h->g, h->k1, h->k2a, h->work2, h->work);
+  if (int r = dft3_grid(h->work, h->g.K, +1, 4, s)) return r;
+  double* d = reinterpret_cast<double*>(h->work2);  // 4N doubles: error1, error2
+  k_em_finish<<<nb, 256, 0, s>>>(h->g, h->work, charge, d, d + 2 * N);
+  MD_CHECK_LAUNCH("errmap compute");
+  MD_CUDA(cudaMemcpyAsync(error1, d, sizeof(double) * 2 * N, cudaMemcpyDeviceToHost, s));
+  MD_CUDA(cudaMemcpyAsync(error2, d + 2 * N, sizeof(double) * 2 * N, cudaMemcpyDeviceToHost, s));
+  MD_CUDA(cudaStreamSynchronize(s));
+  return MD_OK;
+}
+
+extern "C" int md_errmap_get_profile(md_errmap* h, double* rho1, double* rho2) {
+  if (!h) return MD_ERR_BADARG;
+  MD_CUDA(cudaSetDevice(h->device));
+  MD_CUDA(cudaStreamSynchronize(h->stream));
+  if (rho1) MD_CUDA(cudaMemcpy(rho1, h->rho, sizeof(double) * h->g.N, cudaMemcpyDeviceToHost));
+  if (rho2) MD_CUDA(cudaMemcpy(rho2, h->rho + h->g.N, sizeof(double) * h->g.N, cudaMemcpyDeviceToHost));
+  return MD_OK;
+}

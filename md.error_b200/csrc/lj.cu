@@ -23,7 +23,23 @@ struct LJParams {
   double eps4, sig2, shift, beta, cb;  // cb = 2 beta / sqrt(pi)
 };
 
+// Build options of the mixed kernel (defaults are the measured best):
+//   MD_LJ_PREFETCH  1: load the next list line while the current one is processed
+//   MD_LJ_ACC       0: per-lane Kahan-compensated FP32 sums of the per-pass batch
+//                      sums; 1: the batch sums added in FP64
+#ifndef MD_LJ_PREFETCH
+#define MD_LJ_PREFETCH 0
+#endif
+#ifndef MD_LJ_ACC
+#define MD_LJ_ACC 1
+#endif
+
 struct Kahan {
+#if MD_LJ_ACC == 1
+  double s = 0.0;
+  __device__ __forceinline__ void add(float x) { s += (double)x; }
+  __device__ __forceinline__ double value() const { return s; }
+#else
   float s = 0.f, c = 0.f;
   __device__ __forceinline__ void add(float x) {
     float y = x - c;
@@ -32,6 +48,7 @@ struct Kahan {
     s = t;
   }
   __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+#endif
 };
 
 template <int G>
@@ -47,25 +64,24 @@ struct MixedAcc {
   float e = 0.f, vx = 0.f, vy = 0.f, vz = 0.f, ec = 0.f;
 };
 
-// One pass of a lane over U list entries k0, k0+G, ..., k0+(U-1)G of row i:
-// all index loads, then all position gathers, then the arithmetic, so that U
-// independent loads are in flight per lane. TAIL: entries at or past n are
-// skipped (only the last pass of a row can reach them).
+// One pass of a lane over the 4 list entries e4 of row i (one 16-byte load;
+// logical entries base + 8u): all position gathers, then the arithmetic, so
+// that 4 independent loads are in flight per lane. TAIL: entry u is inside
+// the row only when 8u < nvalid (only the last pass of a row).
 // The image shift k L of an entry is read from the 64-entry table `shift`
 // indexed by the entry's six image bits; the table holds the binary32
 // products k_d * L_d (exactly -L_d, +0 or L_d), so d - shift is the same
 // binary32 operation as shortestImage's x -= floorf(x/L + 0.5) L.
-template <int G, int U, bool TAIL, bool STATS, bool COUL>
-__device__ __forceinline__ void lj_pass_mixed(int k0, int n, const int* __restrict__ row,
-                                              const float4* __restrict__ pos, int i, const float4& pi,
-                                              float rc2, const float4* shift, const LJParams& p,
-                                              MixedAcc& a) {
-  int ee[U];
+template <int U, bool TAIL, bool STATS, bool COUL>
+__device__ __forceinline__ void lj_pass_mixed(const int4 e4, int nvalid, const float4* __restrict__ pos, int i,
+                                              const float4& pi, float rc2, const float4* shift,
+                                              const LJParams& p, MixedAcc& a) {
+  static_assert(U == 4, "one int4 of list entries per pass");
+  int ee[U] = {e4.x, e4.y, e4.z, e4.w};
   float4 pj[U];
+  if (TAIL) {
 #pragma unroll
-  for (int u = 0; u < U; ++u) {
-    const int kk = k0 + u * G;
-    ee[u] = (!TAIL || kk < n) ? __ldg(row + kk) : -1;
+    for (int u = 0; u < U; ++u) ee[u] = 8 * u < nvalid ? ee[u] : -1;
   }
 #pragma unroll
   // -1 marks "past the end" (a packed entry never has all six image bits set)
@@ -134,13 +150,34 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
     const float rc2 = __fmul_rn(rc, rc);
     int n = nnb[i];
     n = n < cap ? n : cap;
-    const int* row = list + (size_t)i * cap;
-    constexpr int U = 4;
-    int k0 = lane;
-    // passes whose U entries are all inside the row, then at most one ragged pass
-    for (; k0 + (U - 1) * G < n; k0 += U * G)
-      lj_pass_mixed<G, U, false, STATS, COUL>(k0, n, row, pos, i, pi, rc2, shift, p, a);
-    if (k0 < n) lj_pass_mixed<G, U, true, STATS, COUL>(k0, n, row, pos, i, pi, rc2, shift, p, a);
+    // row i as 16-byte vectors: pass q covers the 32-entry line q; with the
+    // transposed line layout (nl_slot) the vector of lane l holds logical
+    // entries 32q + l + 8u, u = 0..3, so for each u the 8 lanes gather 8
+    // consecutive neighbours.  Rows hold whole lines (cap is a multiple of
+    // 32), so every vector read stays inside the row.  The next pass's vector
+    // is loaded before the current one is processed.
+    static_assert(G * 4 == 32, "8 lanes x 4 entries per pass");
+    const int4* row4 = reinterpret_cast<const int4*>(list + (size_t)i * cap);
+    const int npass = (n + 31) >> 5;
+    if (npass > 0) {
+#if MD_LJ_PREFETCH
+      int4 cur = __ldg(row4 + lane);
+#endif
+      for (int q = 0; q < npass; ++q) {
+#if MD_LJ_PREFETCH
+        int4 nxt = cur;
+        if (q + 1 < npass) nxt = __ldg(row4 + (q + 1) * G + lane);
+#else
+        const int4 cur = __ldg(row4 + q * G + lane);
+#endif
+        const int rem = n - (32 * q + lane);  // entry u is inside the row when 8u < rem
+        if (rem > 24) lj_pass_mixed<4, false, STATS, COUL>(cur, rem, pos, i, pi, rc2, shift, p, a);
+        else if (rem > 0) lj_pass_mixed<4, true, STATS, COUL>(cur, rem, pos, i, pi, rc2, shift, p, a);
+#if MD_LJ_PREFETCH
+        cur = nxt;
+#endif
+      }
+    }
   }
   Kahan& fx = a.fx; Kahan& fy = a.fy; Kahan& fz = a.fz;
   const float e = a.e, vx = a.vx, vy = a.vy, vz = a.vz, ec = a.ec;
@@ -176,15 +213,20 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
     const double rc2 = rc * rc;
     int n = nnb[i];
     n = n < cap ? n : cap;
-    const int* row = list + (size_t)i * cap;
+    // transposed line layout (nl_slot): the 16-byte vector of lane l in line
+    // q holds logical entries 32q + l + 8u, u = 0..3
+    const int4* row4 = reinterpret_cast<const int4*>(list + (size_t)i * cap);
     constexpr int U = 4;
+    static_assert(G * U == 32, "8 lanes x 4 entries per line");
     for (int k0 = lane; k0 < n; k0 += U * G) {
       int jj[U];
       double4a pq[U];
+      const int4 e4 = __ldg(row4 + (k0 >> 5) * G + lane);
+      const int ev[U] = {e4.x, e4.y, e4.z, e4.w};
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int kk = k0 + u * G;
-        jj[u] = kk < n ? __ldg(row + kk) : -1;
+        jj[u] = kk < n ? ev[u] : -1;
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) pq[u] = pos[jj[u] != -1 ? (jj[u] & 0x03FFFFFF) : i];
@@ -260,6 +302,7 @@ int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats,
   const bool coul = eng->has_coul;
   int N = sys->N;
   int cap = nl->cap;
+  if (cap % 32 != 0) { md_set_error("neighbour-list capacity %d is not a multiple of 32", cap); return MD_ERR_BADARG; }
   int ow = overwrite ? 1 : 0;
   const int threads = 256;
   dim3 grid(ceil_div((long long)N * kLanes, threads));

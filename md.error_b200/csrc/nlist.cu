@@ -30,11 +30,18 @@ struct NlGeom {
 
 #define NL_TILE_CAP 2304
 #define NL_MAX_RUNS 160
+#define NL_RUN_MAXZ 7   // z cells of a run with per-atom z windows (longer runs are scanned whole)
 
-struct RunInfo {
-  int jb, cnt, off;     // global start, length, tile offset
-  int sx, sy, sz;       // cell-shift images (cell-shift criterion)
-  float b0[3], b1[3];   // run box (unwrapped frame of the home cell)
+// Runs of a home cell, one array per field (the 32 lanes of a warp read the
+// fields of 32 different runs at once, which a struct per run would turn
+// into 16-way shared-memory bank conflicts)
+struct RunTable {
+  int jb[NL_MAX_RUNS], cnt[NL_MAX_RUNS], off[NL_MAX_RUNS];  // global start, length, tile offset
+  int sx[NL_MAX_RUNS], sy[NL_MAX_RUNS], sz[NL_MAX_RUNS];    // periodic images of the run
+  float b0[3][NL_MAX_RUNS], b1[3][NL_MAX_RUNS];             // run box (unwrapped frame of the home cell)
+  int zc0[NL_MAX_RUNS], nz[NL_MAX_RUNS];  // first z cell (unwrapped); z cells with offsets in zoff (0 = none)
+  // zoff[k][r]: offset in run r of the first atom of its k-th z cell (k = nz: cnt)
+  unsigned short zoff[NL_RUN_MAXZ + 1][NL_MAX_RUNS];
 };
 
 __device__ __forceinline__ int img_code(int kx, int ky, int kz) {
@@ -42,7 +49,7 @@ __device__ __forceinline__ int img_code(int kx, int ky, int kz) {
 }
 
 template <class R, int MODE>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(256, 4)
 k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __restrict__ rcut,
            const uint32_t* __restrict__ start, NlGeom g, const DevState* __restrict__ st,
            double rlist_uniform, double skin, int cap, int* __restrict__ list, int* __restrict__ nnb,
@@ -50,7 +57,7 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
   typedef typename V4<R>::T T4;
   extern __shared__ __align__(16) unsigned char nl_smem[];
   T4* tile = reinterpret_cast<T4*>(nl_smem);
-  __shared__ RunInfo runs[NL_MAX_RUNS];
+  __shared__ RunTable rt;
   __shared__ int nruns, tile_n, use_global;
   __shared__ float rl_max_sh;
   if (gate && !(st->flags & FLAG_REBUILD)) return;
@@ -78,11 +85,13 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
   }
   __syncthreads();
 
-  // runs of candidate cells (thread 0; at most a few dozen)
-  if (threadIdx.x == 0) {
+  // runs of candidate cells: one thread per (x, y) column of the stencil
+  // computes its (at most 3) z segments; block-wide exclusive scans give
+  // each run its slot and tile offset in column order
+  int lo[3], hi[3];
+  bool full[3];
+  {
     const double rle = (double)rl_max_sh * (1.0 + 1e-6) + 2e-3;
-    int lo[3], hi[3];
-    bool full[3];
     for (int d = 0; d < 3; ++d) {
       if (!minimg) {
         const int reach = (h[d] >= rlist_uniform) ? 1 : (int)ceil(rlist_uniform / h[d]);
@@ -94,55 +103,110 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
         if (full[d]) { lo[d] = 0; hi[d] = g.nc[d] - 1; }
       }
     }
-    int nr = 0, off = 0;
-    bool overflow_runs = false;
-    for (int ix = lo[0]; ix <= hi[0]; ++ix) {
-      int cx = ix, sx = 0;
+  }
+  __shared__ int scan_r[32], scan_a[32];
+  __shared__ int base_r, base_a, overflow_runs;
+  if (threadIdx.x == 0) { base_r = 0; base_a = 0; overflow_runs = 0; }
+  __syncthreads();
+  const int ncy = hi[1] - lo[1] + 1;
+  const int ncols = (hi[0] - lo[0] + 1) * ncy;
+  for (int col0 = 0; col0 < ncols; col0 += blockDim.x) {
+    const int col = col0 + threadIdx.x;
+    int jb_s[3], cnt_s[3], rs[3], rz0[3], len_s[3], ra_s[3], nseg = 0;
+    int ix = 0, iy = 0, sx = 0, sy = 0, colbase = 0;
+    if (col < ncols) {
+      ix = lo[0] + col / ncy;
+      iy = lo[1] + col % ncy;
+      int cx = ix, cy = iy;
       if (cx < 0) { cx += g.nc[0]; sx = 1; } else if (cx >= g.nc[0]) { cx -= g.nc[0]; sx = -1; }
-      for (int iy = lo[1]; iy <= hi[1]; ++iy) {
-        int cy = iy, sy = 0;
-        if (cy < 0) { cy += g.nc[1]; sy = 1; } else if (cy >= g.nc[1]) { cy -= g.nc[1]; sy = -1; }
-        const int colbase = g.nc[2] * (cy + g.nc[1] * cx);
-        int ra[3], rb[3], rs[3], rz0[3], nseg = 0;
-        if (full[2]) { ra[0] = 0; rb[0] = g.nc[2] - 1; rs[0] = 0; rz0[0] = 0; nseg = 1; }
-        else {
-          const int zlo = lo[2], zhi = hi[2];
-          if (zlo < 0) { ra[nseg] = zlo + g.nc[2]; rb[nseg] = g.nc[2] - 1; rs[nseg] = 1; rz0[nseg] = zlo; ++nseg; }
-          const int a = max(zlo, 0), b = min(zhi, g.nc[2] - 1);
-          if (a <= b) { ra[nseg] = a; rb[nseg] = b; rs[nseg] = 0; rz0[nseg] = a; ++nseg; }
-          if (zhi >= g.nc[2]) { ra[nseg] = 0; rb[nseg] = zhi - g.nc[2]; rs[nseg] = -1; rz0[nseg] = g.nc[2]; ++nseg; }
-        }
-        for (int s = 0; s < nseg; ++s) {
-          const int jb = (int)start[colbase + ra[s]], je = (int)start[colbase + rb[s] + 1];
-          if (je == jb) continue;
-          if (nr == NL_MAX_RUNS) { overflow_runs = true; continue; }
-          RunInfo& R_ = runs[nr++];
-          R_.jb = jb; R_.cnt = je - jb; R_.off = off;
-          R_.sx = sx; R_.sy = sy; R_.sz = rs[s];
-          const int zc0 = rz0[s], zc1 = rz0[s] + (rb[s] - ra[s]);
-          R_.b0[0] = full[0] ? -1e30f : (float)(ix * h[0]); R_.b1[0] = full[0] ? 1e30f : (float)((ix + 1) * h[0]);
-          R_.b0[1] = full[1] ? -1e30f : (float)(iy * h[1]); R_.b1[1] = full[1] ? 1e30f : (float)((iy + 1) * h[1]);
-          R_.b0[2] = full[2] ? -1e30f : (float)(zc0 * h[2]); R_.b1[2] = full[2] ? 1e30f : (float)((zc1 + 1) * h[2]);
-          off += je - jb;
-        }
+      if (cy < 0) { cy += g.nc[1]; sy = 1; } else if (cy >= g.nc[1]) { cy -= g.nc[1]; sy = -1; }
+      colbase = g.nc[2] * (cy + g.nc[1] * cx);
+      int ra[3], rb[3], ns = 0;
+      if (full[2]) { ra[0] = 0; rb[0] = g.nc[2] - 1; rs[0] = 0; rz0[0] = 0; ns = 1; }
+      else {
+        const int zlo = lo[2], zhi = hi[2];
+        if (zlo < 0) { ra[ns] = zlo + g.nc[2]; rb[ns] = g.nc[2] - 1; rs[ns] = 1; rz0[ns] = zlo; ++ns; }
+        const int a = max(zlo, 0), b = min(zhi, g.nc[2] - 1);
+        if (a <= b) { ra[ns] = a; rb[ns] = b; rs[ns] = 0; rz0[ns] = a; ++ns; }
+        if (zhi >= g.nc[2]) { ra[ns] = 0; rb[ns] = zhi - g.nc[2]; rs[ns] = -1; rz0[ns] = g.nc[2]; ++ns; }
+      }
+      for (int s = 0; s < ns; ++s) {
+        const int jb = (int)start[colbase + ra[s]], je = (int)start[colbase + rb[s] + 1];
+        if (je == jb) continue;
+        jb_s[nseg] = jb; cnt_s[nseg] = je - jb; len_s[nseg] = rb[s] - ra[s];
+        rs[nseg] = rs[s]; rz0[nseg] = rz0[s]; ra_s[nseg] = ra[s];
+        ++nseg;
       }
     }
-    nruns = nr;
-    tile_n = off;
-    use_global = (off > NL_TILE_CAP) ? 1 : 0;
+    int atoms = 0;
+    for (int s = 0; s < nseg; ++s) atoms += cnt_s[s];
+    // inclusive warp scans of (runs, atoms), then across warps
+    int ir = nseg, ia = atoms;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int vr = __shfl_up_sync(0xffffffffu, ir, o), va = __shfl_up_sync(0xffffffffu, ia, o);
+      if (lane >= o) { ir += vr; ia += va; }
+    }
+    if (lane == 31) { scan_r[warp] = ir; scan_a[warp] = ia; }
+    __syncthreads();
+    int wr = base_r, wa = base_a;
+    for (int w = 0; w < warp; ++w) { wr += scan_r[w]; wa += scan_a[w]; }
+    int r_off = wr + ir - nseg, a_off = wa + ia - atoms;
+    for (int s = 0; s < nseg; ++s) {
+      if (r_off >= NL_MAX_RUNS) { overflow_runs = 1; break; }
+      const int q = r_off;
+      rt.jb[q] = jb_s[s]; rt.cnt[q] = cnt_s[s]; rt.off[q] = a_off;
+      rt.sx[q] = sx; rt.sy[q] = sy; rt.sz[q] = rs[s];
+      const int zc0 = rz0[s], zc1 = rz0[s] + len_s[s];
+      rt.b0[0][q] = full[0] ? -1e30f : (float)(ix * h[0]); rt.b1[0][q] = full[0] ? 1e30f : (float)((ix + 1) * h[0]);
+      rt.b0[1][q] = full[1] ? -1e30f : (float)(iy * h[1]); rt.b1[1][q] = full[1] ? 1e30f : (float)((iy + 1) * h[1]);
+      rt.b0[2][q] = full[2] ? -1e30f : (float)(zc0 * h[2]); rt.b1[2][q] = full[2] ? 1e30f : (float)((zc1 + 1) * h[2]);
+      // per-cell offsets for the per-atom z window (runs that do not wrap the
+      // whole z axis and have at most NL_RUN_MAXZ cells)
+      rt.zc0[q] = zc0;
+      const int nzq = (!full[2] && len_s[s] + 1 <= NL_RUN_MAXZ && cnt_s[s] <= 65535) ? len_s[s] + 1 : 0;
+      rt.nz[q] = nzq;
+      for (int k = 0; k < nzq; ++k)
+        rt.zoff[k][q] = (unsigned short)((int)start[colbase + ra_s[s] + k] - jb_s[s]);
+      if (nzq) rt.zoff[nzq][q] = (unsigned short)cnt_s[s];
+      ++r_off;
+      a_off += cnt_s[s];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 0; w < nwarp; ++w) { base_r += scan_r[w]; base_a += scan_a[w]; }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    nruns = min(base_r, NL_MAX_RUNS);
+    tile_n = base_a;
+    use_global = (base_a > NL_TILE_CAP) ? 1 : 0;
     if (overflow_runs) atomicOr(&stw->flags, FLAG_NL_OVERFLOW);
   }
   __syncthreads();
   const int nr = nruns;
-  if (!use_global) {
-    for (int r = 0; r < nr; ++r) {
-      const RunInfo& R_ = runs[r];
-      for (int t = threadIdx.x; t < R_.cnt; t += blockDim.x) tile[R_.off + t] = pos[R_.jb + t];
+  // stage the runs into the tile, one warp per run; a home cell with fewer
+  // than 4 atoms reads its candidates from L2 instead (staging would cost
+  // more than the few reads it saves)
+  const bool stage = !use_global && (i1 - i0) >= 4;
+  if (stage) {
+    for (int r = warp; r < nr; r += nwarp) {
+      const int c = rt.cnt[r], o = rt.off[r], jb = rt.jb[r];
+      for (int t = lane; t < c; t += 32) tile[o + t] = pos[jb + t];
     }
   }
   __syncthreads();
-  const bool glob = use_global;
+  const bool glob = !stage;
   const unsigned ltmask = (1u << lane) - 1u;
+  // When the stencil spans less than the box along every axis, each cell
+  // appears in exactly one run, at that run's periodic image k_run, and
+  // 2 rlist < L.  For any pair within rlist the reference's image
+  // floor((r_j - r_i)/L + 1/2) is then k_run (it can differ only where
+  // |d| is within rounding of L/2 > rlist, where both reject), so
+  // d = (r_j - r_i) - k_run L repeats the reference's binary32 operations and
+  // the image code is the run's.
+  const bool runshift = minimg && !full[0] && !full[1] && !full[2];
+  const float hz = (float)h[2];
 
   for (int i = i0 + warp; i < i1; i += nwarp) {
     const T4 pi = pos[i];
@@ -162,24 +226,76 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
     }
     const float rle_i = (float)rl * (1.0f + 1e-5f) + 2e-3f;
     int n = 0;
-    for (int r = 0; r < nr; ++r) {
-      const RunInfo& R_ = runs[r];
-      if (minimg) {
-        float dd = 0.f;
-        for (int d = 0; d < 3; ++d) {
-          const float e = fmaxf(0.f, fmaxf(R_.b0[d] - xe[d], xe[d] - R_.b1[d]));
-          dd += e * e;
+    int* rowp = list + (size_t)i * cap;
+    // the 32 lanes test 32 runs at a time against i's box distance and z
+    // window, then the surviving runs are walked in order
+    for (int rb = 0; rb < nr; rb += 32) {
+      bool keep = false;
+      int tbl = 0, tel = 0;
+      if (rb + lane < nr) {
+        const int r = rb + lane;
+        keep = true;
+        if (minimg) {
+          float dd = 0.f;
+          for (int d = 0; d < 3; ++d) {
+            const float e = fmaxf(0.f, fmaxf(rt.b0[d][r] - xe[d], xe[d] - rt.b1[d][r]));
+            dd += e * e;
+          }
+          keep = dd <= rle_i * rle_i;
         }
-        if (dd > rle_i * rle_i) continue;
+        // the cells of the run that meet i's z window [z - rl, z + rl]
+        tbl = 0;
+        tel = rt.cnt[r];
+        const int nzr = rt.nz[r];
+        if (keep && minimg && nzr) {
+          const int zc0 = rt.zc0[r];
+          const int k0 = max((int)floorf((xe[2] - rle_i) / hz) - zc0, 0);
+          const int k1 = min((int)floorf((xe[2] + rle_i) / hz) - zc0, nzr - 1);
+          keep = k0 <= k1;
+          if (keep) {
+            tbl = rt.zoff[k0][r];
+            tel = rt.zoff[k1 + 1][r];
+          }
+        }
       }
-      const R shx = mul_rn((R)R_.sx, L[0]), shy = mul_rn((R)R_.sy, L[1]), shz = mul_rn((R)R_.sz, L[2]);
-      for (int t0 = 0; t0 < R_.cnt; t0 += 32) {
+      unsigned km = __ballot_sync(0xffffffffu, keep);
+      while (km) {
+      const int src = __ffs(km) - 1;
+      km &= km - 1;
+      const int r = rb + src;
+      const int rjb = rt.jb[r], roff = rt.off[r], rsx = rt.sx[r], rsy = rt.sy[r], rsz = rt.sz[r];
+      const int tb = __shfl_sync(0xffffffffu, tbl, src), te = __shfl_sync(0xffffffffu, tel, src);
+      const R shx = mul_rn((R)rsx, L[0]), shy = mul_rn((R)rsy, L[1]), shz = mul_rn((R)rsz, L[2]);
+      if (runshift) {
+        const int rcode = img_code(rsx, rsy, rsz);
+        for (int t0 = tb; t0 < te; t0 += 32) {
+          const int t = t0 + lane;
+          bool ok = false;
+          const int j = rjb + t;
+          if (t < te) {
+            const T4 pj = glob ? pos[j] : tile[roff + t];
+            const R dx = sub_rn(sub_rn(pj.x, pi.x), shx);
+            const R dy = sub_rn(sub_rn(pj.y, pi.y), shy);
+            const R dz = sub_rn(sub_rn(pj.z, pi.z), shz);
+            const R d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
+            ok = (d2 < rl2) && (j != i);
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, ok);
+          if (ok) {
+            const int p = n + __popc(m & ltmask);
+            if (p < cap) rowp[nl_slot(p)] = j | rcode;
+          }
+          n += __popc(m);
+        }
+        continue;
+      }
+      for (int t0 = tb; t0 < te; t0 += 32) {
         const int t = t0 + lane;
         bool ok = false;
         int code = 0;
-        const int j = R_.jb + t;
-        if (t < R_.cnt) {
-          const T4 pj = glob ? pos[j] : tile[R_.off + t];
+        const int j = rjb + t;
+        if (t < te) {
+          const T4 pj = glob ? pos[j] : tile[roff + t];
           const R rx = sub_rn(pj.x, pi.x), ry = sub_rn(pj.y, pi.y), rz = sub_rn(pj.z, pi.z);
           const R kx = floor_r(add_rn(mul_rn(rx, Li[0]), R(0.5)));
           const R ky = floor_r(add_rn(mul_rn(ry, Li[1]), R(0.5)));
@@ -201,10 +317,11 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
         const unsigned m = __ballot_sync(0xffffffffu, ok);
         if (ok) {
           const int p = n + __popc(m & ltmask);
-          if (p < cap) list[(size_t)i * cap + p] = j | code;
+          if (p < cap) rowp[nl_slot(p)] = j | code;
         }
         n += __popc(m);
       }
+      }  // surviving runs of this group
     }
     if (lane == 0) {
       nnb[i] = n;
@@ -249,7 +366,7 @@ int nlist_build_impl(md_nlist* nl, md_system* sys, md_cell_list* cl, Recorder* r
   double rl = nl->rlist, skin = nl->skin;
   DevState* st = sys->st;
   int cap = nl->cap;
-  dim3 grid(cl->ntot), block(128);
+  dim3 grid(cl->ntot), block(256);
   void* a[] = {&N, &sys->pos, &sys->rcut, &cl->start, &g, &st, &rl, &skin, &cap, &nl->list,
                &nl->nnb, &nl->backup, &force_mi, &st, &gate};
   const void* f;
@@ -294,7 +411,9 @@ extern "C" int md_nlist_create(md_nlist** out, md_system* sys, double rlist, dou
   double expect = 4.0 / 3.0 * M_PI * rlist * rlist * rlist * rho;
   int cap = (int)(expect * expansion);
   if (cap < 30) cap = 30;
-  cap = (cap + 7) & ~7;
+  // rows are a whole number of 32-entry (128-byte) lines: the force kernels
+  // read a row in 16-byte vectors, 32 entries per pass, up to the line end
+  cap = (cap + 31) & ~31;
   nl->cap = cap;
   size_t r4 = sys->r4_size();
   if (alloc_lists(nl, sys) != MD_OK || cudaMalloc(&nl->nnb, sizeof(int) * sys->N) != cudaSuccess ||
@@ -343,7 +462,7 @@ extern "C" int md_nlist_fit(md_nlist* nl, md_system* sys, md_cell_list* cl) {
     if (r != MD_ERR_NLIST_OVERFLOW) return r;
     DevState hs;
     if (int q = sys->read_state(hs)) return q;
-    nl->cap = ((int)(hs.max_nnb * 1.2) + 32 + 7) & ~7;
+    nl->cap = ((int)(hs.max_nnb * 1.2) + 32 + 31) & ~31;
     if (int q = alloc_lists(nl, sys)) return q;
   }
   return MD_ERR_NLIST_OVERFLOW;
@@ -422,7 +541,7 @@ extern "C" int md_nlist_get(md_nlist* nl, md_system* sys, int32_t* counts, int32
     int c = nnb[k] < nl->cap ? nnb[k] : nl->cap;
     counts[o] = c;
     if (pairs)
-      for (int t = 0; t < c; ++t) pairs[off + t] = id[lst[(size_t)k * nl->cap + t] & 0x03FFFFFF];
+      for (int t = 0; t < c; ++t) pairs[off + t] = id[lst[(size_t)k * nl->cap + nl_slot(t)] & 0x03FFFFFF];
     off += c;
   }
   return MD_OK;

@@ -144,6 +144,12 @@ _SIGS = {
     "md_nhc_npt_operator_L_r": (i32, [vp, vp, f64]),
     "md_nhc_npt_operator_L_box": (i32, [vp, vp, f64]),
     "md_nhc_npt_get_state": (i32, [vp, P(f64)]),
+    "md_errmap_create": (i32, [P(vp), P(i32), P(f64), f64, i32, i32]),
+    "md_errmap_destroy": (i32, [vp]),
+    "md_errmap_set_profile": (i32, [vp, P(f64), P(f64)]),
+    "md_errmap_deposit": (i32, [vp, vp]),
+    "md_errmap_get_profile": (i32, [vp, P(f64), P(f64)]),
+    "md_errmap_compute": (i32, [vp, f64, P(f64), P(f64)]),
     "md_ikerr_create":(i32, [P(vp), P(i32), P(f64), f64, f64, i32, i32, i32, i32, f64, f64, i32]),
     "md_ikerr_destroy": (i32, [vp]),
     "md_ikerr_num_coeffs": (i32, [vp, P(i32)]),

@@ -408,6 +408,50 @@ def errorEstimateInterpolRec(sys, K, order, beta):
     return e.value
 
 
+class ErrorEstimate_SPME_Ik:
+    """ErrorEstimate_SPME_Ik (analyze tools): reinit(beta, order, dp) builds the
+    kernel on the grid K of box L; calError(charge) gives error1 and error2
+    ([K..., 2]); rms() the RMS force error per grid point."""
+
+    def __init__(self, K, L, beta, order, device=0):
+        h = C.c_void_p()
+        KK = (C.c_int * 3)(*[int(k) for k in K])
+        LL = (C.c_double * 3)(*[float(x) for x in L])
+        check(lib.md_errmap_create(C.byref(h), KK, LL, float(beta), int(order), int(device)),
+              "ErrorEstimate_SPME_Ik")
+        self.h = h
+        self.K = tuple(int(k) for k in K)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.md_errmap_destroy(self.h)
+            self.h = None
+
+    def set_profile(self, rho1, rho2):
+        a = _f64(rho1).reshape(-1)
+        b = _f64(rho2).reshape(-1)
+        check(lib.md_errmap_set_profile(self.h, _p(a), _p(b)), "set_profile")
+
+    def deposit(self, sys):
+        check(lib.md_errmap_deposit(self.h, sys.h), "deposit")
+
+    def profile(self):
+        a = np.empty(self.K)
+        b = np.empty(self.K)
+        check(lib.md_errmap_get_profile(self.h, _p(a), _p(b)), "profile")
+        return a, b
+
+    def calError(self, charge=1.0):
+        e1 = np.empty(self.K + (2,))
+        e2 = np.empty(self.K + (2,))
+        check(lib.md_errmap_compute(self.h, float(charge), _p(e1), _p(e2)), "calError")
+        return e1, e2
+
+    def rms(self, charge=1.0):
+        e1, e2 = self.calError(charge)
+        return np.sqrt(e1[..., 0] + e2[..., 0])
+
+
 def choose_beta(sys, rcut, target):
     b = C.c_double()
     check(lib.md_choose_beta(sys.h, float(rcut), float(target), C.byref(b)), "choose_beta")

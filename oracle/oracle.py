@@ -419,6 +419,46 @@ def ref_selfcorr(pos, q, box, beta, K, order):
     return F
 
 
+def spme_ik_errmap(K, box, beta, order, rho1, rho2, charge=1.0):
+    """Oracle restatement of ErrorEstimate_SPME_Ik::calError on the grid K:
+    returns (error1 [K..., 2], error2 [K..., 2]) -- real and imaginary parts."""
+    KK = np.ascontiguousarray(K, np.int32)
+    b = np.ascontiguousarray(box, np.float64)
+    r1 = np.ascontiguousarray(rho1, np.float64).reshape(-1)
+    r2 = np.ascontiguousarray(rho2, np.float64).reshape(-1)
+    n = int(np.prod(K))
+    e1 = np.zeros(2 * n)
+    e2 = np.zeros(2 * n)
+    _lib.orc_spme_ik_errmap(_p(KK, i32), _p(b, f64), float(beta), int(order), _p(r1, f64), _p(r2, f64),
+                            float(charge), _p(e1, f64), _p(e2, f64))
+    return e1.reshape(tuple(K) + (2,)), e2.reshape(tuple(K) + (2,))
+
+
+def ref_spme_ik_errmap(K, box, beta, order, rho1, rho2, charge=1.0):
+    """The reference's own ErrorEstimate_SPME_Ik (oracle/_ref/libref_errmap.so)."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libref_errmap.so"))
+    lib.ref_spme_ik_errmap.argtypes = [P(i32), P(f64), f64, i32, P(f64), P(f64), f64, P(f64), P(f64)]
+    KK = np.ascontiguousarray(K, np.int32)
+    b = np.ascontiguousarray(box, np.float64)
+    r1 = np.ascontiguousarray(rho1, np.float64).reshape(-1)
+    r2 = np.ascontiguousarray(rho2, np.float64).reshape(-1)
+    n = int(np.prod(K))
+    e1 = np.zeros(2 * n)
+    e2 = np.zeros(2 * n)
+    lib.ref_spme_ik_errmap(_p(KK, i32), _p(b, f64), float(beta), int(order), _p(r1, f64), _p(r2, f64),
+                           float(charge), _p(e1, f64), _p(e2, f64))
+    return e1.reshape(tuple(K) + (2,)), e2.reshape(tuple(K) + (2,))
+
+
+def dft3d(data, sign):
+    """The oracle's unnormalised 3D DFT (sign -1 forward, +1 backward)."""
+    a = np.ascontiguousarray(data, np.complex128)
+    n = np.ascontiguousarray(a.shape, np.int32)
+    buf = np.ascontiguousarray(np.stack([a.real, a.imag], -1), np.float64)
+    _lib.orc_dft3d(_p(n, i32), _p(buf, f64), int(sign))
+    return buf[..., 0] + 1j * buf[..., 1]
+
+
 def spme_selfcorr(pos, q, box, K, order, beta):
     """Oracle restatement of SelfCorr: the correction added to zero forces."""
     p = np.ascontiguousarray(pos, np.float64)
@@ -441,6 +481,8 @@ _sigs3 = {
     "orc_ewald_dir": (f64, [i32, P(f64), P(f64), P(f64), f64, f64, P(f64)]),
     "orc_ewald_self": (f64, [i32, P(f64), f64]),
     "orc_spme_selfcorr": (None, [i32, P(f64), P(f64), P(f64), P(i32), i32, f64, P(f64)]),
+    "orc_spme_ik_errmap": (None, [P(i32), P(f64), f64, i32, P(f64), P(f64), f64, P(f64), P(f64)]),
+    "orc_dft3d": (None, [P(i32), P(f64), i32]),
 }
 for _n, (_r, _a) in _sigs3.items():
     _f = getattr(_lib, _n)

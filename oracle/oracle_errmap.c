@@ -1,0 +1,161 @@
+/* ORACLE -- test infrastructure only.  CPU restatement of the inhomogeneous
+ * ik-SPME error estimate of ErrorEstimate_SPME_Ik (longRange.hetero/profile.test/
+ * template/tools/analyze/src/ErrorEstimate_SPME_Ik.cpp:119-470), rectangular box,
+ * on the grid of the density profile (the SPME mesh K):
+ *   g(m)   = -4 pi f(m) m*,  f = e^{-pi^2 |m*|^2/beta^2} / |m*|^2 / (2 pi V)
+ *   a_d(m, k) = (u_d + 2 pi k)^-n / sum_{l=-3..3} (u_d + 2 pi l)^-n,  u_d = 2 pi m_d / K_d
+ *   k2b = sum_{k = +-1..+-4} sum_dir V/N |IFFT(i g a_dir(k))|^2
+ *   k1  = i g 2 sum_{k, dir} a_dir(k)  (k-space kernel, times V)
+ *   k2a = FFT(V/N |IFFT(k1 / V)|^2) + 2 FFT(k2b)
+ *   e1_d = IFFT(k1_d FFT(rho1 V/N)) q/V,  e2 = IFFT(k2a FFT(rho2 V/N)) q^2/V
+ *   error1 = sum_d e1_d^2 (real and imaginary parts apart), error2 = e2
+ * with each component of g zeroed at the Nyquist index of an even K_d.
+ * Transforms are unnormalised, sign -1 forward / +1 backward. */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+void orc_dft3d(const int n[3], double* data, int sign);
+
+static double ipw(double x, int n) {
+  double r = 1;
+  for (int i = 0; i < n; ++i) r *= x;
+  return r;
+}
+
+static double alias(double u, int n) {
+  double s = 1. / ipw(u, n), up = u, un = u;
+  for (int l = 0; l < 3; ++l) {
+    up += 2. * M_PI;
+    un -= 2. * M_PI;
+    s += 1. / ipw(up, n);
+    s += 1. / ipw(un, n);
+  }
+  return s;
+}
+
+static int cidx(int i, int K) { return i > (K >> 1) ? i - K : i; }
+
+void orc_spme_ik_errmap(const int K[3], const double box[3], double beta, int order, const double* rho1,
+                        const double* rho2, double charge, double* e1, double* e2) {
+  const long N = (long)K[0] * K[1] * K[2];
+  const double V = box[0] * box[1] * box[2];
+  const double scal = 1. / (2. * M_PI * V);
+  double* g = (double*)calloc(3 * N, sizeof(double));
+  double* k1 = (double*)calloc(6 * N, sizeof(double));    /* 3 complex grids, kept k-space kernel */
+  double* w = (double*)calloc(6 * N, sizeof(double));     /* 3 complex work grids */
+  double* k2a = (double*)calloc(2 * N, sizeof(double));
+  double* k2b = (double*)calloc(2 * N, sizeof(double));
+  int even[3];
+  for (int d = 0; d < 3; ++d) even[d] = (K[d] % 2 == 0);
+  for (int i0 = 0; i0 < K[0]; ++i0)
+    for (int i1 = 0; i1 < K[1]; ++i1)
+      for (int i2 = 0; i2 < K[2]; ++i2) {
+        const long idx = i2 + (long)K[2] * (i1 + (long)K[1] * i0);
+        const double m[3] = {cidx(i0, K[0]) / box[0], cidx(i1, K[1]) / box[1], cidx(i2, K[2]) / box[2]};
+        const double m2 = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+        if (m2 == 0) continue;
+        const double t = M_PI / beta, fm = exp(-t * t * m2) / m2 * scal;
+        for (int d = 0; d < 3; ++d) g[d * N + idx] = -4. * M_PI * fm * m[d];
+      }
+  /* aliasing sums of the six k and three directions */
+  for (int k = -4; k <= 4; ++k) {
+    if (k == 0) continue;
+    for (int dir = 0; dir < 3; ++dir) {
+      memset(w, 0, sizeof(double) * 6 * N);
+      for (int i0 = 0; i0 < K[0]; ++i0)
+        for (int i1 = 0; i1 < K[1]; ++i1)
+          for (int i2 = 0; i2 < K[2]; ++i2) {
+            const long idx = i2 + (long)K[2] * (i1 + (long)K[1] * i0);
+            if (idx == 0) continue;
+            const int ii[3] = {i0, i1, i2};
+            const double u = 2. * M_PI * cidx(ii[dir], K[dir]) / K[dir];
+            const double a = 1. / ipw(u + 2. * M_PI * k, order) * (1. / alias(u, order));
+            for (int d = 0; d < 3; ++d) {
+              double v = g[d * N + idx] * a;
+              if (even[d] && ii[d] == (K[d] >> 1)) v = 0.;
+              w[2 * (d * N + idx) + 1] = v;
+            }
+          }
+      for (int d = 0; d < 3; ++d) orc_dft3d(K, w + 2 * d * N, +1);
+      for (long i = 0; i < N; ++i) {
+        double s = 0;
+        for (int d = 0; d < 3; ++d) {
+          const double re = w[2 * (d * N + i)], im = w[2 * (d * N + i) + 1];
+          s += re * re + im * im;
+        }
+        k2b[2 * i] += s * V / (double)N;
+      }
+    }
+  }
+  /* the summed kernel */
+  memset(w, 0, sizeof(double) * 6 * N);
+  for (int i0 = 0; i0 < K[0]; ++i0)
+    for (int i1 = 0; i1 < K[1]; ++i1)
+      for (int i2 = 0; i2 < K[2]; ++i2) {
+        const long idx = i2 + (long)K[2] * (i1 + (long)K[1] * i0);
+        if (idx == 0) continue;
+        const int ii[3] = {i0, i1, i2};
+        double u[3], fen[3];
+        for (int d = 0; d < 3; ++d) {
+          u[d] = 2. * M_PI * cidx(ii[d], K[d]) / K[d];
+          fen[d] = 1. / alias(u[d], order);
+        }
+        double sum = 0.;
+        for (int k = -4; k <= 4; ++k) {
+          if (k == 0) continue;
+          for (int d = 0; d < 3; ++d) sum += 1. / ipw(u[d] + 2. * M_PI * k, order) * fen[d];
+        }
+        for (int d = 0; d < 3; ++d) {
+          double v = g[d * N + idx] * sum * 2.;
+          if (even[d] && ii[d] == (K[d] >> 1)) v = 0.;
+          w[2 * (d * N + idx) + 1] = v;
+          k1[2 * (d * N + idx) + 1] = v * V;
+        }
+      }
+  for (int d = 0; d < 3; ++d) orc_dft3d(K, w + 2 * d * N, +1);
+  for (long i = 0; i < N; ++i) {
+    double s = 0;
+    for (int d = 0; d < 3; ++d) {
+      const double re = w[2 * (d * N + i)], im = w[2 * (d * N + i) + 1];
+      s += re * re + im * im;
+    }
+    k2a[2 * i] = s * V / (double)N;
+  }
+  orc_dft3d(K, k2a, -1);
+  orc_dft3d(K, k2b, -1);
+  for (long i = 0; i < 2 * N; ++i) k2a[i] += 2. * k2b[i];
+  /* the error of the profile */
+  double* r1 = (double*)calloc(2 * N, sizeof(double));
+  double* r2 = (double*)calloc(2 * N, sizeof(double));
+  for (long i = 0; i < N; ++i) {
+    r1[2 * i] = rho1[i] * V / (double)N;
+    r2[2 * i] = rho2[i] * V / (double)N;
+  }
+  orc_dft3d(K, r1, -1);
+  orc_dft3d(K, r2, -1);
+  double* ex = (double*)calloc(8 * N, sizeof(double)); /* e1x, e1y, e1z, e2 */
+  for (long i = 0; i < N; ++i) {
+    for (int d = 0; d < 3; ++d) {
+      const double ar = k1[2 * (d * N + i)], ai = k1[2 * (d * N + i) + 1];
+      ex[2 * (d * N + i)] = r1[2 * i] * ar - r1[2 * i + 1] * ai;
+      ex[2 * (d * N + i) + 1] = r1[2 * i] * ai + r1[2 * i + 1] * ar;
+    }
+    ex[2 * (3 * N + i)] = r2[2 * i] * k2a[2 * i] - r2[2 * i + 1] * k2a[2 * i + 1];
+    ex[2 * (3 * N + i) + 1] = r2[2 * i] * k2a[2 * i + 1] + r2[2 * i + 1] * k2a[2 * i];
+  }
+  for (int d = 0; d < 4; ++d) orc_dft3d(K, ex + 2 * d * N, +1);
+  for (long i = 0; i < N; ++i) {
+    double s0 = 0, s1 = 0;
+    for (int d = 0; d < 3; ++d) {
+      const double re = ex[2 * (d * N + i)] * charge / V, im = ex[2 * (d * N + i) + 1];
+      s0 += re * re;
+      s1 += im * im;
+    }
+    e1[2 * i] = s0;
+    e1[2 * i + 1] = s1;
+    e2[2 * i] = ex[2 * (3 * N + i)] * charge * charge / V;
+    e2[2 * i + 1] = ex[2 * (3 * N + i) + 1];
+  }
+  free(g); free(k1); free(w); free(k2a); free(k2b); free(r1); free(r2); free(ex);
+}

@@ -75,6 +75,43 @@ extern "C" int ref_selfcorr(int n, const double* pos, const double* q, const dou
 }
 #endif
 
+#ifdef REF_ERRMAP
+// ErrorEstimate_SPME_Ik::reinit + calError (analyze/app/error.spme.ik.cpp:82-85)
+// on a density profile given on the grid K (profile1: charge-sign density,
+// profile2: number density); error1 / error2 as [n][2] (real, imaginary).
+// the profile class keeps its data private and fills it only from trajectory
+// files: read its header with default-public members (same layout) so that
+// the driver can set the profile directly
+#include <cmath>
+#include <cstdlib>
+#include <string>
+#include <vector>
+#define class struct
+#include "DensityProfile.h"
+#undef class
+#include "ErrorEstimate_SPME_Ik.h"
+extern "C" int ref_spme_ik_errmap(const int* K, const double* box, double beta, int order, const double* rho1,
+                                  const double* rho2, double charge, double* e1, double* e2) {
+  DensityProfile_PiecewiseConst dp;
+  dp.boxsize.assign(box, box + 3);
+  dp.nx = K[0]; dp.ny = K[1]; dp.nz = K[2];
+  dp.nele = K[0] * K[1] * K[2];
+  dp.hx = box[0] / K[0]; dp.hy = box[1] / K[1]; dp.hz = box[2] / K[2];
+  dp.profile1.assign(rho1, rho1 + dp.nele);
+  dp.profile2.assign(rho2, rho2 + dp.nele);
+  dp.profileP.assign(dp.nele, 0.);
+  dp.profileN.assign(dp.nele, 0.);
+  ErrorEstimate_SPME_Ik est;
+  est.reinit(beta, order, dp);
+  est.calError(dp, charge);
+  for (unsigned i = 0; i < dp.nele; ++i) {
+    e1[2 * i] = est.error1[i][0]; e1[2 * i + 1] = est.error1[i][1];
+    e2[2 * i] = est.error2[i][0]; e2[2 * i + 1] = est.error2[i][1];
+  }
+  return 0;
+}
+#endif
+
 #ifdef REF_ARC
 #include "AdaptRCut.h"
 #include "PressureCorrection.h"

@@ -168,6 +168,51 @@ def test_error_estimates_on_device(mdf, orc, small, prec):
     assert abs(d - 1e-4) < 1e-9
 
 
+@pytest.mark.parametrize("K,box,beta,order", [((8, 8, 16), (3.0, 3.0, 6.0), 2.5, 4),
+                                              ((10, 12, 9), (3.1, 3.5, 2.9), 3.0, 6)])
+def test_error_map_matches_oracle(mdf, orc, K, box, beta, order):
+    rng = np.random.default_rng(2)
+    rho1 = rng.normal(0, 5, K)
+    rho2 = np.abs(rng.normal(30, 5, K))
+    em = mdf.ErrorEstimate_SPME_Ik(K, box, beta, order)
+    em.set_profile(rho1, rho2)
+    e1, e2 = em.calError(1.0)
+    o1, o2 = orc.spme_ik_errmap(K, box, beta, order, rho1, rho2, 1.0)
+    assert np.abs(e1 - o1).max() < 1e-11 * np.abs(o1).max()
+    assert np.abs(e2 - o2).max() < 1e-11 * np.abs(o2).max()
+
+
+def test_error_map_of_a_charged_slab(mdf, orc):
+    """Deposited profile of a charged slab (analyze/app/error.spme.ik.cpp on a
+    configuration): the profile and the error map against the oracle."""
+    s = mdf.systems.charged_slab(n=8192, box=(20.0, 20.0, 80.0), half=12.0)
+    K = (16, 16, 64)
+    sys = mdf.MDSystem(s.pos, s.box, charge=s.charge, precision=1)
+    em = mdf.ErrorEstimate_SPME_Ik(K, s.box, 1.0, 6)
+    em.deposit(sys)
+    rho1, rho2 = em.profile()
+    h = s.box / np.array(K)
+    idx = np.floor(np.mod(s.pos, s.box) / h).astype(int)
+    idx = np.minimum(idx, np.array(K) - 1)
+    c1 = np.zeros(K)
+    c2 = np.zeros(K)
+    np.add.at(c1, tuple(idx.T), np.sign(s.charge))
+    np.add.at(c2, tuple(idx.T), 1.0)
+    dv = np.prod(h)
+    assert np.allclose(rho1, c1 / dv, rtol=0, atol=1e-12)
+    assert np.allclose(rho2, c2 / dv, rtol=0, atol=1e-12)
+    e1, e2 = em.calError(1.0)
+    o1, o2 = orc.spme_ik_errmap(K, s.box, 1.0, 6, rho1, rho2, 1.0)
+    # real parts are the estimate; the imaginary parts are transform rounding
+    # (~1e-13) and are compared on the scale of the real parts
+    for a, b in ((e1, o1), (e2, o2)):
+        scale = np.abs(b[..., 0]).max()
+        assert np.abs(a[..., 0] - b[..., 0]).max() < 1e-11 * scale
+        assert np.abs(a[..., 1] - b[..., 1]).max() < 1e-9 * scale
+    rms = em.rms(1.0)
+    assert np.all(np.isfinite(rms)) and rms.max() > 0
+
+
 @pytest.mark.parametrize("prec", [0, 1])
 def test_self_correction(mdf, orc, small, prec):
     pos, q, box = small

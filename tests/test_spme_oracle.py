@@ -88,6 +88,27 @@ def test_error_estimates_match_reference_build(orc, charges, K, order):
     assert abs(e - ref["err_interp"]) <= 1e-13 * ref["err_interp"]
 
 
+@pytest.mark.parametrize("K,box,beta,order", [((8, 8, 16), (3.0, 3.0, 6.0), 2.5, 4),
+                                              ((10, 12, 9), (3.1, 3.5, 2.9), 3.0, 6)])
+def test_errmap_oracle_matches_reference_build(orc, K, box, beta, order):
+    if not orc.ref_available("libref_errmap.so"):
+        pytest.skip("reference error map not built")
+    rng = np.random.default_rng(2)
+    rho1 = rng.normal(0, 5, K)
+    rho2 = np.abs(rng.normal(30, 5, K))
+    a1, a2 = orc.spme_ik_errmap(K, box, beta, order, rho1, rho2, 1.0)
+    b1, b2 = orc.ref_spme_ik_errmap(K, box, beta, order, rho1, rho2, 1.0)
+    assert np.abs(a1 - b1).max() < 1e-12 * np.abs(b1).max()
+    assert np.abs(a2 - b2).max() < 1e-12 * np.abs(b2).max()
+
+
+def test_dft3d_matches_numpy(orc):
+    rng = np.random.default_rng(3)
+    a = rng.normal(size=(4, 6, 5)) + 1j * rng.normal(size=(4, 6, 5))
+    assert np.abs(orc.dft3d(a, -1) - np.fft.fftn(a)).max() < 1e-12
+    assert np.abs(orc.dft3d(a, +1) - np.fft.ifftn(a) * a.size).max() < 1e-12
+
+
 @pytest.mark.parametrize("K,order", [((16, 16, 16), 6), ((16, 12, 15), 4), ((8, 16, 32), 8)])
 def test_selfcorr_oracle_matches_reference_build(orc, charges, K, order):
     if not orc.ref_available("libref_spme.so"):
