@@ -41,6 +41,9 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--equil", type=int, default=4000,
                     help="untimed NVT relaxation steps of the random start")
+    ap.add_argument("--workload", default="lj_slab", choices=list(WORKLOADS),
+                    help="lj_slab: the 65536-atom slab of the headline metric (default); the others "
+                         "time the remaining named systems")
     ap.add_argument("--launch", default="graph", choices=["graph", "direct"],
                     help="direct: launch each step's kernels on the stream instead of one CUDA graph "
                          "(rebuild kernels gated on the device flag); for profilers that do not "
@@ -290,6 +293,94 @@ def cpu_baseline(s, lattice, nsteps):
     return (nsteps / el), orc.num_threads(), out
 
 
+WORKLOADS = ("lj_slab", "lj_fluid", "charged_fluid", "charged_slab")
+
+
+def run_workload(args):
+    """The other named systems, one JSON line each (rank 0): steps/s of the
+    mixed path and of plain FP64 through the graph-captured driver, force RMS
+    error of mixed against FP64 on the start configuration, per-step device
+    time.  lj_fluid: 4000-atom fcc LJ fluid, rc 2.5 shifted, Langevin NVT
+    gamma 0.1, dt 0.005.  charged_fluid: 20736 unit charges in a 30^3 box, LJ
+    rc 3.0 + real-space Ewald (beta 0.95, rc 3.0) + ik SPME 64^3 order 6,
+    Langevin NVT T 1, dt 0.002.  charged_slab: 1048576 unit charges, liquid
+    0.8 for |z - 200| < 64 in 100 x 100 x 400, vapour 0.01, SPME 128 x 128 x
+    512 order 6, beta for a real-space error of 1e-4 at rc 3.0 (uniform LJ
+    cutoff 3.0 in place of the adaptive one)."""
+    rank, world, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    import mdforce as mdf
+    w = args.workload
+    if w == "lj_fluid":
+        s = mdf.systems.lj_fluid_fcc()
+        rc, dt, T, gamma, coul = 2.5, 0.005, 1.0, 0.1, None
+        shift = -4.0 * (rc ** -12 - rc ** -6)
+    elif w == "charged_fluid":
+        s = mdf.systems.charged_fluid()
+        rc, dt, T, gamma, shift = 3.0, 0.002, 1.0, 1.0, 0.0
+        coul = dict(beta=0.95, K=(64, 64, 64), order=6)
+    else:
+        s = mdf.systems.charged_slab()
+        rc, dt, T, gamma, shift = 3.0, 0.002, 1.0, 1.0, 0.0
+        coul = dict(beta=None, K=(128, 128, 512), order=6)
+
+    def build(prec, pos, vel):
+        sys_ = mdf.MDSystem(pos, s.box, vel=vel, charge=s.charge, precision=prec)
+        sys_.set_rcut(np.full(s.n, rc, np.float32))
+        eng = mdf.InteractionEngine(sys_)
+        eng.registNonBondedInteraction(1.0, 1.0, shift)
+        sp = None
+        if coul is not None:
+            beta = coul["beta"] or mdf.choose_beta(sys_, rc, 1e-4)
+            coul["beta"] = beta
+            mdf.registCoulomb(eng, beta)
+            sp = mdf.SPME(sys_, coul["K"], coul["order"], beta, "ik")
+        lv = mdf.langevin_params(dt=dt, temperature=T, gamma_t=gamma, seed=1 + rank)
+        sim = mdf.Simulation(sys_, eng, skin=SKIN, cell_size=rc + SKIN, lv=lv, expansion=1.5, spme=sp,
+                             use_graph=args.launch == "graph")
+        return sys_, eng, sim
+
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    vel = s.vel if s.vel is not None else mdf.systems.maxwell(s.n, T, 11)
+    # relaxation of the start (random sequential addition / lattice), not timed
+    sys0, _, sim0 = build(0, s.pos, vel)
+    sim0.run(args.equil if args.equil != 4000 else 1000)
+    pos, vel = sys0.positions(), sys0.velocities()
+    del sim0, sys0
+    out = {}
+    for prec in (0, 1):
+        sys_, eng, sim = build(prec, pos, vel)
+        sys_.set_stream(stream.cuda_stream)
+        sim.run(args.warmup)
+        t = time_steps(torch, sim, stream, args.steps, flush)
+        out[prec] = (args.steps / t, sys_, sim)
+    # force RMS error of mixed against FP64 on the relaxed configuration
+    F = {}
+    for prec in (0, 1):
+        sys_, _, sim = build(prec, pos, vel)
+        F[prec] = sys_.forces()
+    d = F[0] - F[1]
+    err_abs = float(np.sqrt((d ** 2).sum(1).mean()))
+    err_rel = float(np.sqrt((d ** 2).sum() / (F[1] ** 2).sum()))
+    if rank == 0:
+        line = {"metric": "MD steps/s", "value": out[0][0], "unit": "steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / out[0][0],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 pair math / f64 accumulation", "data": "synthetic",
+                "config": {"workload": w, "n_atoms": s.n, "box": s.box.tolist(), "rc": rc, "skin": SKIN,
+                           "dt": dt, "T": T, "ensemble": "Langevin NVT",
+                           "electrostatics": None if coul is None else
+                           dict(beta=coul["beta"], mesh=list(coul["K"]), order=coul["order"], method="ik"),
+                           "l2": "flushed (256 MB write) between timed steps"},
+                "fp64_steps_per_s": out[1][0], "speedup_vs_fp64": out[0][0] / out[1][0],
+                "force_rms_err_vs_fp64": {"abs": err_abs, "rel": err_rel},
+                "tau_per_day": out[0][0] * dt * 86400}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -322,6 +413,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "lj_slab":
+        return run_workload(args)
     rank, world, local = dist_env()
     import torch
     if world > 1:

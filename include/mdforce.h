@@ -360,6 +360,9 @@ typedef struct md_sim_params {
   int integrator;       /* md_integrator: Langevin (lv) or Nose-Hoover chain + velocity Verlet */
   double nhc_tau;       /* NHC period tau_T (lv.temperature is the target, lv.dt the step) */
   int remove_com;       /* NHC: remove the centre-of-mass velocity every step */
+  md_spme* spme;        /* optional reciprocal SPME of the same system, added to the forces (and
+                           to energy / virial) every step; NULL = short range only.  The engine's
+                           real-space Ewald (md_engine_register_coulomb) completes the split */
 } md_sim_params;
 enum md_integrator {
   MD_INTEG_LANGEVIN = 0,

@@ -184,4 +184,6 @@ int nhc_vv1_impl(md_nhc* h, md_nlist* nl, double dt, Recorder* rec, cudaGraphCon
                  int use_cond);
 int nhc_vv2_impl(md_nhc* h, double dt, Recorder* rec, int kick, int end, int start, int account);
 int nhc_settle_impl(md_nhc* h);
+int spme_apply_impl(md_spme* s, bool with_stats, Recorder* rec);
+bool spme_belongs_to(const md_spme* s, const md_system* sys);
 int set_flag_impl(md_system* sys, unsigned bits, Recorder* rec);

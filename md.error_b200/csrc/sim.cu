@@ -78,6 +78,8 @@ static int record_step(md_sim* s, Recorder* rec, bool use_graph) {
   }
   s->conditional = cond;
   if (int r = lj_apply_impl(s->eng, sys, s->nl, true, true, rec)) return r;
+  if (s->p.spme)
+    if (int r = spme_apply_impl(s->p.spme, true, rec)) return r;
   if (nhc) {
     // closing kick + operator_L(dt/2), then this step's successor's COM
     // removal and operator_L(dt/2), as a pending velocity map
@@ -118,6 +120,10 @@ extern "C" int md_sim_create(md_sim** out, md_system* sys, md_engine* eng, const
     return MD_ERR_BADARG;
   }
   if (!eng->has_lj) { md_set_error("md_sim_create: register a non-bonded interaction first"); return MD_ERR_BADARG; }
+  if (p->spme && !spme_belongs_to(p->spme, sys)) {
+    md_set_error("md_sim_create: the SPME object belongs to another system");
+    return MD_ERR_BADARG;
+  }
   md_sim* s = new md_sim();
   s->sys = sys;
   s->eng = eng;
@@ -160,6 +166,7 @@ extern "C" int md_sim_create(md_sim** out, md_system* sys, md_engine* eng, const
   Recorder rec;
   rec.stream = sys->stream;
   if ((r = lj_apply_impl(eng, sys, s->nl, true, true, &rec))) return fail(r);
+  if (p->spme && (r = spme_apply_impl(p->spme, true, &rec))) return fail(r);
   if (p->integrator == MD_INTEG_NHC) {
     if (!(p->nhc_tau > 0)) { md_set_error("md_sim_create: the Nose-Hoover chain needs nhc_tau > 0"); return fail(MD_ERR_BADARG); }
     if ((r = md_nhc_create(&s->nhc, sys, p->lv.temperature, p->nhc_tau, p->remove_com))) return fail(r);

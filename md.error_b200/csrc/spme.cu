@@ -611,7 +611,8 @@ __global__ void k_ewald_force(int N, const double4a* __restrict__ pos, const flo
 
 // ---------------------------------------------------------------- host
 template <class R>
-static int fft_launch(md_spme* s, const void* in, void* out, int mode, int axis, int sign, int batch) {
+static int fft_launch(md_spme* s, Recorder* rec, const void* in, void* out, int mode, int axis, int sign,
+                      int batch) {
   const int K0 = s->K[0], K1 = s->K[1], K2 = s->K[2], K2h = s->K2h;
   int n;
   long nlines, stride = 1, inner = 1, outer = 0, in_as = 0, out_as = 0;
@@ -632,65 +633,101 @@ static int fft_launch(md_spme* s, const void* in, void* out, int mode, int axis,
   const int threads = lpb * n / 2 < 32 ? 32 : lpb * n / 2;
   const size_t smem = sizeof(typename C2<R>::T) * (n / 2 + 2 * (size_t)lpb * n);
   dim3 grid((unsigned)((nlines + lpb - 1) / lpb), batch);
-  k_fft<R><<<grid, threads, smem, s->sys->stream>>>(in, out, mode, n, lpb, nlines, stride, inner, outer, in_as,
-                                                     out_as, sign);
-  MD_CHECK_LAUNCH("spme fft");
-  return MD_OK;
+  void* a[] = {&in, &out, &mode, &n, &lpb, &nlines, &stride, &inner, &outer, &in_as, &out_as, &sign};
+  return rec_launch(rec, (const void*)k_fft<R>, grid, dim3(threads), smem, a);
+}
+
+template <class R>
+__global__ void k_zero_mesh(size_t n, R* Q) {
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t < n) Q[t] = R(0);
 }
 
 // influence refresh (only when the box changed), spread and the forward
-// transform: C[0] = Q^ on the half spectrum
+// transform: C[0] = Q^ on the half spectrum.  Every launch goes through the
+// recorder, so the chain is either run on the stream or recorded into the
+// step graph of the simulation driver.
 template <class R>
-static int spme_forward_mesh(md_spme* s) {
+static int spme_forward_mesh(md_spme* s, Recorder* rec) {
   typedef typename C2<R>::T T2;
   md_system* sys = s->sys;
-  cudaStream_t st_ = sys->stream;
-  const int K0 = s->K[0], K1 = s->K[1], K2 = s->K[2], n = s->order;
+  int K0 = s->K[0], K1 = s->K[1], K2 = s->K[2], n = s->order, N = sys->N;
   R* Q = (R*)s->Q;
   T2* C = (T2*)s->C;
-  k_spme_influence<R><<<(unsigned)((s->nhalf + 255) / 256), 256, 0, st_>>>(K0, K1, K2, n, s->beta, sys->st,
-                                                                           (R*)s->psi, s->d_box_tab);
-  MD_CHECK_LAUNCH("spme influence");
-  k_spme_box_tab<<<1, 1, 0, st_>>>(sys->st, s->d_box_tab);
-  MD_CHECK_LAUNCH("spme box tab");
-  MD_CUDA(cudaMemsetAsync(Q, 0, sizeof(R) * s->nreal, st_));
-  const long nt = (long)sys->N * n * n;
-  k_spme_spread<R><<<(unsigned)((nt + 255) / 256), 256, 0, st_>>>(sys->N, (const typename V4<R>::T*)sys->pos, n, K0,
-                                                                   K1, K2, sys->st, Q);
-  MD_CHECK_LAUNCH("spme spread");
-  if (int r = fft_launch<R>(s, Q, C, 0, 2, -1, 1)) return r;
-  if (int r = fft_launch<R>(s, C, C, 1, 1, -1, 1)) return r;
-  if (int r = fft_launch<R>(s, C, C, 1, 0, -1, 1)) return r;
+  R* psi = (R*)s->psi;
+  DevState* st = sys->st;
+  double beta = s->beta;
+  size_t nreal = s->nreal;
+  {
+    void* a[] = {&K0, &K1, &K2, &n, &beta, &st, &psi, &s->d_box_tab};
+    if (int r = rec_launch(rec, (const void*)k_spme_influence<R>, dim3((unsigned)((s->nhalf + 255) / 256)),
+                           dim3(256), 0, a)) return r;
+  }
+  {
+    void* a[] = {&st, &s->d_box_tab};
+    if (int r = rec_launch(rec, (const void*)k_spme_box_tab, dim3(1), dim3(1), 0, a)) return r;
+  }
+  {
+    void* a[] = {&nreal, &Q};
+    if (int r = rec_launch(rec, (const void*)k_zero_mesh<R>, dim3((unsigned)((nreal + 255) / 256)), dim3(256), 0, a))
+      return r;
+  }
+  {
+    const long nt = (long)N * n * n;
+    const void* pos = sys->pos;
+    void* a[] = {&N, &pos, &n, &K0, &K1, &K2, &st, &Q};
+    if (int r = rec_launch(rec, (const void*)k_spme_spread<R>, dim3((unsigned)((nt + 255) / 256)), dim3(256), 0, a))
+      return r;
+  }
+  if (int r = fft_launch<R>(s, rec, Q, C, 0, 2, -1, 1)) return r;
+  if (int r = fft_launch<R>(s, rec, C, C, 1, 1, -1, 1)) return r;
+  if (int r = fft_launch<R>(s, rec, C, C, 1, 0, -1, 1)) return r;
   return MD_OK;
 }
 
 template <class R>
-static int spme_run(md_spme* s, bool with_stats) {
+static int spme_run(md_spme* s, bool with_stats, Recorder* rec) {
   typedef typename C2<R>::T T2;
   md_system* sys = s->sys;
-  cudaStream_t st_ = sys->stream;
-  const int K0 = s->K[0], K1 = s->K[1], K2 = s->K[2], n = s->order;
+  int K0 = s->K[0], K1 = s->K[1], K2 = s->K[2], n = s->order, N = sys->N, method = s->method;
   T2* C = (T2*)s->C;
   R* G = (R*)s->G;
-  if (int r = spme_forward_mesh<R>(s)) return r;
+  DevState* st = sys->st;
+  if (int r = spme_forward_mesh<R>(s, rec)) return r;
   const int nb = (int)((s->nhalf + 255) / 256);
   if (with_stats && nb > sys->max_partial_blocks) { md_set_error("partials buffer too small for the mesh"); return MD_ERR_BADARG; }
-  k_spme_kspace<R><<<nb, 256, 0, st_>>>(K0, K1, K2, s->method, s->beta, (const R*)s->psi, C, s->nhalf, sys->st,
-                                         sys->partials, with_stats ? 1 : 0);
-  MD_CHECK_LAUNCH("spme kspace");
-  if (with_stats) {
-    k_spme_stats_merge<<<1, 1, 0, st_>>>(sys->st);
-    MD_CHECK_LAUNCH("spme merge");
+  {
+    double beta = s->beta;
+    const R* psi = (const R*)s->psi;
+    size_t nhalf = s->nhalf;
+    int ws = with_stats ? 1 : 0;
+    void* a[] = {&K0, &K1, &K2, &method, &beta, &psi, &C, &nhalf, &st, &sys->partials, &ws};
+    if (int r = rec_launch(rec, (const void*)k_spme_kspace<R>, dim3(nb), dim3(256), 0, a)) return r;
   }
-  const int nconv = s->method == 0 ? 3 : 1;
+  if (with_stats) {
+    void* a[] = {&st};
+    if (int r = rec_launch(rec, (const void*)k_spme_stats_merge, dim3(1), dim3(1), 0, a)) return r;
+  }
+  const int nconv = method == 0 ? 3 : 1;
   T2* Cp = C + s->nhalf;
-  if (int r = fft_launch<R>(s, Cp, Cp, 1, 0, +1, nconv)) return r;
-  if (int r = fft_launch<R>(s, Cp, Cp, 1, 1, +1, nconv)) return r;
-  if (int r = fft_launch<R>(s, Cp, G, 2, 2, +1, nconv)) return r;
-  k_spme_gather<R><<<(unsigned)(((long)sys->N * 32 + 255) / 256), 256, 0, st_>>>(
-      sys->N, (const typename V4<R>::T*)sys->pos, n, K0, K1, K2, s->method, sys->st, G, s->nreal, sys->force);
-  MD_CHECK_LAUNCH("spme gather");
+  if (int r = fft_launch<R>(s, rec, Cp, Cp, 1, 0, +1, nconv)) return r;
+  if (int r = fft_launch<R>(s, rec, Cp, Cp, 1, 1, +1, nconv)) return r;
+  if (int r = fft_launch<R>(s, rec, Cp, G, 2, 2, +1, nconv)) return r;
+  {
+    const void* pos = sys->pos;
+    size_t nreal = s->nreal;
+    void* a[] = {&N, &pos, &n, &K0, &K1, &K2, &method, &st, &G, &nreal, &sys->force};
+    if (int r = rec_launch(rec, (const void*)k_spme_gather<R>, dim3((unsigned)(((long)N * 32 + 255) / 256)),
+                           dim3(256), 0, a)) return r;
+  }
   return MD_OK;
+}
+
+bool spme_belongs_to(const md_spme* s, const md_system* sys) { return s && s->sys == sys; }
+
+// the chain of one SPME force evaluation, recorded (driver) or launched
+int spme_apply_impl(md_spme* s, bool with_stats, Recorder* rec) {
+  return s->sys->prec == MD_PREC_FP64 ? spme_run<double>(s, with_stats, rec) : spme_run<float>(s, with_stats, rec);
 }
 
 // energy and gradient: recompute the mesh and its transform, influence
@@ -712,15 +749,17 @@ static int spme_energy_grad(md_spme* s, double* energy, double* dq, double* dr, 
   double* d_q = dq ? d : nullptr;
   double* d_r = dr ? d + nq : nullptr;
   double* d_p = dpsi ? d + nq + nr : nullptr;
-  if (int r = spme_forward_mesh<R>(s)) return r;
+  Recorder rec;
+  rec.stream = st_;
+  if (int r = spme_forward_mesh<R>(s, &rec)) return r;
   k_spme_adj_kspace<R><<<nb, 256, 0, st_>>>(K0, K1, K2, s->beta, (const R*)s->psi, C, s->nhalf, sys->st,
                                              sys->partials, d_p);
   MD_CHECK_LAUNCH("spme adjoint kspace");
   if (dq || dr) {
     T2* Cp = C + s->nhalf;
-    if (int r = fft_launch<R>(s, Cp, Cp, 1, 0, +1, 1)) return r;
-    if (int r = fft_launch<R>(s, Cp, Cp, 1, 1, +1, 1)) return r;
-    if (int r = fft_launch<R>(s, Cp, G, 2, 2, +1, 1)) return r;
+    if (int r = fft_launch<R>(s, &rec, Cp, Cp, 1, 0, +1, 1)) return r;
+    if (int r = fft_launch<R>(s, &rec, Cp, Cp, 1, 1, +1, 1)) return r;
+    if (int r = fft_launch<R>(s, &rec, Cp, G, 2, 2, +1, 1)) return r;
     k_spme_adj_gather<R><<<(unsigned)(((long)sys->N * 32 + 255) / 256), 256, 0, st_>>>(
         sys->N, (const typename V4<R>::T*)sys->pos, sys->id, n, K0, K1, K2, sys->st, G, d_q, d_r);
     MD_CHECK_LAUNCH("spme adjoint gather");
@@ -784,7 +823,9 @@ extern "C" int md_spme_destroy(md_spme* s) {
 
 extern "C" int md_spme_apply(md_spme* s, md_system* sys, int with_stats) {
   if (!s || !sys || sys != s->sys) { md_set_error("md_spme_apply: bad arguments"); return MD_ERR_BADARG; }
-  return sys->prec == MD_PREC_FP64 ? spme_run<double>(s, with_stats != 0) : spme_run<float>(s, with_stats != 0);
+  Recorder rec;
+  rec.stream = sys->stream;
+  return spme_apply_impl(s, with_stats != 0, &rec);
 }
 
 extern "C" int md_spme_energy_grad(md_spme* s, md_system* sys, double* energy, double* dE_dq, double* dE_dr,

@@ -38,7 +38,7 @@ class SimParams(C.Structure):
     _fields_ = [("lv", LangevinParams), ("skin", f64), ("cell_size", f64),
                 ("expansion", f64), ("nl_mode", i32), ("use_graph", i32),
                 ("stats_every", i32), ("max_rcut", f64), ("integrator", i32), ("nhc_tau", f64),
-                ("remove_com", i32)]
+                ("remove_com", i32), ("spme", C.c_void_p)]
 
 
 _SIGS = {

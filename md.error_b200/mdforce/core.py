@@ -653,10 +653,13 @@ class Simulation:
     """Graph-captured Langevin MD driver (the hot loop of ENG/app/lj.nhc-xtc.cu)."""
 
     def __init__(self, sys, engine, skin, cell_size, lv, nl_mode=NL_MINIMAGE, expansion=1.5,
-                 use_graph=True, max_rcut=0.0, integrator="langevin", nhc_tau=0.0, remove_com=True):
+                 use_graph=True, max_rcut=0.0, integrator="langevin", nhc_tau=0.0, remove_com=True,
+                 spme=None):
         """integrator "langevin" (lv: BAOAB NVT/NPT) or "nhc" (the lj.nhc-xtc step:
         2-chain Nose-Hoover at lv.temperature with period nhc_tau, velocity Verlet with
-        step lv.dt, COM velocity removed every step when remove_com)."""
+        step lv.dt, COM velocity removed every step when remove_com).  spme: an SPME
+        of the same system whose reciprocal forces are added every step (with the
+        engine's real-space Ewald, registCoulomb, this is the full Ewald split)."""
         p = SimParams()
         p.lv = lv
         p.skin = skin
@@ -669,6 +672,8 @@ class Simulation:
         p.integrator = {"langevin": INTEG_LANGEVIN, "nhc": INTEG_NHC}[integrator]
         p.nhc_tau = nhc_tau
         p.remove_com = 1 if remove_com else 0
+        p.spme = spme.h if spme is not None else None
+        self._spme = spme  # keep the SPME alive as long as the driver
         self.params = p
         h = C.c_void_p()
         check(lib.md_sim_create(C.byref(h), sys.h, engine.h, C.byref(p)), "Simulation")
