@@ -354,7 +354,7 @@ def run_workload(args):
         sys_, eng, sim = build(prec, pos, vel)
         sys_.set_stream(stream.cuda_stream)
         sim.run(args.warmup)
-        t = time_steps(torch, sim, stream, args.steps, flush)
+        t = time_steps(torch, sim, stream, args.steps, flush, nvtx_range="timed" if prec == 0 else None)
         out[prec] = (args.steps / t, sys_, sim)
     # force RMS error of mixed against FP64 on the relaxed configuration
     F = {}
