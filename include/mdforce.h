@@ -204,7 +204,8 @@ typedef struct md_spme md_spme;
 int md_spme_create(md_spme** out, md_system* sys, const int K[3], int order, double beta, int method);
 int md_spme_destroy(md_spme* spme);
 int md_spme_apply(md_spme* spme, md_system* sys, int with_stats);
-/* the charge mesh Q of the last apply (calQ), [K0][K1][K2] */
+/* the charge mesh Q (calQ) of the system's current positions, [K0][K1][K2] (spread on
+ * demand; the force chain consumes its mesh in the first transform pass) */
 int md_spme_get_mesh(md_spme* spme, double* Q);
 /* Adjoint of the reciprocal SPME energy E = 1/2 sum_m psi(m) |Q^(m)|^2 (the energy of
  * ElectrostaticInteraction_rec_BSpline, RE/src/EleRecBSpline.cpp:393-536; no gradient

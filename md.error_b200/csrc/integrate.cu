@@ -164,13 +164,21 @@ __device__ __forceinline__ void lv_particle_step1(int k, typename V4<R>::T* __re
 // (with_box) and, with advance, runs box_advance for the next step.
 template <class R>
 __global__ void __launch_bounds__(256)
-k_lv_step2(int N, typename V4<R>::T* __restrict__ vel, const double4a* __restrict__ force,
-           DevState* st, LvDev p, double* partials, int with_box, int kick, int advance) {
+k_lv_step2(int N, typename V4<R>::T* __restrict__ vel, double4a* __restrict__ force,
+           DevState* st, LvDev p, double* partials, int with_box, int kick, int advance,
+           const double4a* __restrict__ fadd, int merge_rec) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   double kin[3] = {0, 0, 0};
   if (k < N) {
     typename V4<R>::T v = vel[k];
-    const double4a f = force[k];
+    double4a f = force[k];
+    if (fadd) {
+      const double4a g = fadd[k];
+      f.x += g.x;
+      f.y += g.y;
+      f.z += g.z;
+      force[k] = f;
+    }
     const double im = (double)v.w;
     const double h = kick ? 0.5 * p.dt : 0.0;
     double vx = v.x + h * f.x * im, vy = v.y + h * f.y * im, vz = v.z + h * f.z * im;
@@ -183,6 +191,11 @@ k_lv_step2(int N, typename V4<R>::T* __restrict__ vel, const double4a* __restric
   }
   const bool last = block_reduce_finish<3>(kin, partials, &st->red_counter[RED_KIN],
                                            &st->stats[MD_STAT_KINETIC_XX], true);
+  if (last && merge_rec) {
+    // reciprocal energy into its slot, its diagonal virial added to the virial slots
+    st->stats[MD_STAT_ELEC_REC] = st->scratch[0];
+    for (int d = 0; d < 3; ++d) st->stats[MD_STAT_VIRIAL_XX + d] += st->scratch[1 + d];
+  }
   if (last && with_box) {
     // P_dd = 2/V (K_dd - W_dd/2) + tail correction (MDStatistic::pressureXX)
     const double V = st->L[0] * st->L[1] * st->L[2];
@@ -232,12 +245,12 @@ int langevin_step1_impl(md_system* sys, md_nlist* nl, Recorder* rec, bool with_b
   return rec_launch(rec, f, dim3(ceil_div(N, 256)), dim3(256), 0, a);
 }
 
-int langevin_step2_impl(md_system* sys, Recorder* rec, int kick, int advance) {
+int langevin_step2_impl(md_system* sys, Recorder* rec, int kick, int advance, const double4a* fadd, int merge_rec) {
   LvDev p = make_lv(sys, nullptr);
   DevState* st = sys->st;
   int N = sys->N;
   int with_box = 1;
-  void* a[] = {&N, &sys->vel, &sys->force, &st, &p, &sys->partials, &with_box, &kick, &advance};
+  void* a[] = {&N, &sys->vel, &sys->force, &st, &p, &sys->partials, &with_box, &kick, &advance, &fadd, &merge_rec};
   const void* f = sys->prec == MD_PREC_FP64 ? (const void*)k_lv_step2<double> : (const void*)k_lv_step2<float>;
   return rec_launch(rec, f, dim3(ceil_div(N, 256)), dim3(256), 0, a);
 }
@@ -277,9 +290,11 @@ extern "C" int md_vv_step2(md_system* sys, double dt, int with_stats) {
   int nb = ceil_div(N, 256);
   (void)with_stats;
   if (sys->prec == MD_PREC_FP64)
-    k_lv_step2<double><<<nb, 256, 0, sys->stream>>>(N, (double4a*)sys->vel, sys->force, st, p, sys->partials, 0, 1, 0);
+    k_lv_step2<double><<<nb, 256, 0, sys->stream>>>(N, (double4a*)sys->vel, sys->force, st, p, sys->partials, 0, 1, 0,
+                                                     nullptr, 0);
   else
-    k_lv_step2<float><<<nb, 256, 0, sys->stream>>>(N, (float4*)sys->vel, sys->force, st, p, sys->partials, 0, 1, 0);
+    k_lv_step2<float><<<nb, 256, 0, sys->stream>>>(N, (float4*)sys->vel, sys->force, st, p, sys->partials, 0, 1, 0,
+                                                    nullptr, 0);
   MD_CHECK_LAUNCH("vv step2");
   return MD_OK;
 }

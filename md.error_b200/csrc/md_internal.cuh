@@ -168,6 +168,7 @@ struct Recorder {
   cudaGraph_t graph = nullptr;   // when non-null, launches become kernel nodes
   cudaGraphNode_t last = nullptr;
   bool has_last = false;
+  cudaGraphNode_t join = nullptr;  // second dependency of the next node (a branch joining back)
   cudaStream_t stream = nullptr;
 };
 int rec_launch(Recorder* r, const void* func, dim3 grid, dim3 block, size_t smem, void** args);
@@ -178,12 +179,20 @@ int nlist_build_impl(md_nlist* nl, md_system* sys, md_cell_list* cl, Recorder* r
 int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats, bool overwrite, Recorder* rec);
 int langevin_step1_impl(md_system* sys, md_nlist* nl, Recorder* rec, bool with_box_kernel,
                         cudaGraphConditionalHandle cond, int use_cond);
-int langevin_step2_impl(md_system* sys, Recorder* rec, int kick, int advance);
+// fadd: per-atom force of a concurrent branch (SPME), added into the force
+// array by the closing kick; merge_rec: the branch's reciprocal energy and
+// virial (DevState::scratch) are merged into the statistics by its last block
+int langevin_step2_impl(md_system* sys, Recorder* rec, int kick, int advance, const double4a* fadd = nullptr,
+                        int merge_rec = 0);
 int clear_stats_impl(md_system* sys, Recorder* rec, int first, int count);
 int nhc_vv1_impl(md_nhc* h, md_nlist* nl, double dt, Recorder* rec, cudaGraphConditionalHandle cond,
                  int use_cond);
 int nhc_vv2_impl(md_nhc* h, double dt, Recorder* rec, int kick, int end, int start, int account);
 int nhc_settle_impl(md_nhc* h);
-int spme_apply_impl(md_spme* s, bool with_stats, Recorder* rec);
+// concurrent: the chain may run beside the real-space kernel; it then stores
+// its forces in spme_force_buffer() and leaves its energy and virial in
+// DevState::scratch for the closing kick to merge
+int spme_apply_impl(md_spme* s, bool with_stats, Recorder* rec, bool concurrent = false);
+const double4a* spme_force_buffer(const md_spme* s);
 bool spme_belongs_to(const md_spme* s, const md_system* sys);
 int set_flag_impl(md_system* sys, unsigned bits, Recorder* rec);

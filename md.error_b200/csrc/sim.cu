@@ -6,8 +6,11 @@
 //                the rebuild decision into a graph conditional
 //   IF(rebuild)  bin, scan, scatter, order, gather, copy back, list build
 //   LJ           forces (overwrite) + FP64 energy / virial (store)
-//   k_lv_step2   closing B, kinetic tensor, pressure, box momentum half kick,
-//                and the box B A O A of the next step
+//   SPME         (when attached) the reciprocal chain; with the Langevin
+//                integrator a second branch beside LJ, joined by k_lv_step2
+//   k_lv_step2   closing B (adding the SPME forces, energy and virial),
+//                kinetic tensor, pressure, box momentum half kick, and the
+//                box B A O A of the next step
 // Where the driver cannot create conditional nodes the rebuild kernels are
 // recorded unconditionally and return at once unless the device flag is set.
 // Density sampling and the adaptive-cutoff update run between graph launches
@@ -77,15 +80,30 @@ static int record_step(md_sim* s, Recorder* rec, bool use_graph) {
     if (int r = nlist_build_impl(s->nl, sys, s->cl, rec, true)) return r;
   }
   s->conditional = cond;
+  // Langevin with SPME: the reciprocal chain is a second branch beside the
+  // real-space kernel (both depend on the rebuild); it stores its forces in
+  // its own buffer and leaves its energy and virial for the closing kick,
+  // which adds both in
+  const bool branch = s->p.spme && !nhc;
+  const cudaGraphNode_t fork = rec->last;
+  const bool fork_has = rec->has_last;
   if (int r = lj_apply_impl(s->eng, sys, s->nl, true, true, rec)) return r;
-  if (s->p.spme)
-    if (int r = spme_apply_impl(s->p.spme, true, rec)) return r;
+  if (s->p.spme) {
+    const cudaGraphNode_t lj = rec->last;
+    if (branch && rec->graph) {
+      rec->last = fork;
+      rec->has_last = fork_has;
+    }
+    if (int r = spme_apply_impl(s->p.spme, true, rec, branch)) return r;
+    if (branch && rec->graph) rec->join = lj;
+  }
   if (nhc) {
     // closing kick + operator_L(dt/2), then this step's successor's COM
     // removal and operator_L(dt/2), as a pending velocity map
     if (int r = nhc_vv2_impl(s->nhc, s->p.lv.dt, rec, 1, 1, 1, 1)) return r;
   } else {
-    if (int r = langevin_step2_impl(sys, rec, 1, 1)) return r;
+    if (int r = langevin_step2_impl(sys, rec, 1, 1, branch ? spme_force_buffer(s->p.spme) : nullptr, branch ? 1 : 0))
+      return r;
   }
   return MD_OK;
 }

@@ -6,19 +6,29 @@
 //   analytic differentiation         RE/src/EleRecFBSpline.cpp:771-907, 1146-1195
 //   exact reciprocal sum (ES)        RE/src/EleRecES.cpp:49-144
 //
-// Chain per call: spread (one thread per atom x (k0,k1) column, atomic adds
-// along k2) -> R2C along z -> C2C along y, x (forward) -> k-space pass (energy
-// and virial in FP64, influence multiply; ik writes the three products
-// i(-2 pi m_d) psi Q^, analytic writes psi Q^) -> C2C x, y (inverse) -> C2R
-// along z with the Hermitian completion of an r2c half spectrum (the FFTW c2r
-// convention the reference relies on) -> gather (one warp per atom).
-// The FFT is a radix-2 Stockham transform of whole lines in shared memory;
-// a block holds several lines that are adjacent in memory so that strided
+// Chain of one force evaluation (each step one kernel):
+//   spread      charges into a shared-memory tile per block of 64 charges,
+//               the tile added to the mesh with 4-wide atomics
+//   z pass      R2C along z (real lines -> half-complex lines)
+//   y pass      forward C2C along y
+//   x pass      forward C2C along x, k-space step (energy and virial in FP64,
+//               influence multiply; ik: the three products i(-2 pi m_d) psi Q^,
+//               analytic: psi Q^ / 2) and the inverse C2C along x, fused
+//   y pass      inverse C2C along y (all products)
+//   z pass      C2R along z with the Hermitian completion of an r2c half
+//               spectrum (the FFTW c2r convention the reference relies on);
+//               for ik the three meshes are written interleaved, one Real4
+//               per mesh point
+//   gather      order-templated, LPA lanes per atom
+// The FFT passes are radix-8 Stockham transforms of whole lines in shared
+// memory; a block holds several lines adjacent in memory so that strided
 // axes load coalesced.  Mixed precision: mesh, FFT and gather in FP32,
 // energy/virial and force accumulation in FP64.  Power-of-two mesh sizes.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 #include "device_common.cuh"
 
@@ -36,8 +46,13 @@ struct md_spme {
   size_t nreal = 0, nhalf = 0;
   void* Q = nullptr;      // real mesh
   void* C = nullptr;      // complex half meshes: [0] Q^, [1..3] products
-  void* G = nullptr;      // real convolution meshes (3 for ik, 1 analytic)
+  void* G = nullptr;      // convolved real mesh(es): ik Real4 (x, y, z, 0) per point; analytic and adjoint one Real
   void* psi = nullptr;    // influence function on the half spectrum (ik normalisation)
+  void* tw[3] = {nullptr, nullptr, nullptr};  // per-axis forward twiddles exp(-2 pi i m / K_d)
+  double* bm = nullptr;   // per-axis |b(m)|^2 (k_spme_bmod)
+  double4a* frec = nullptr;   // reciprocal forces of a concurrent evaluation (stored, not added)
+  double* partials = nullptr; // block partials of the x pass (its own: it may run beside other reductions)
+  int max_blocks = 0;
   double* d_box_tab = nullptr;  // box psi was computed for (device; 0 = never)
 };
 
@@ -74,36 +89,163 @@ __device__ __forceinline__ void grid_coord(R x, R Linv, int K, int& base, R& fra
   if (base >= K) { base -= K; }
 }
 
-__device__ __forceinline__ int wrapk(int k, int K) { return k < 0 ? k + K : k; }
+// The same recursion with the order a compile-time constant, so that the
+// weight arrays stay in registers (a runtime order spills them to local
+// memory).  D: also the derivatives dM_n/du.
+template <class R, int NO, bool D>
+__device__ __forceinline__ void bsp_t(R f, R (&w)[NO], R (&dw)[NO]) {
+  w[0] = f;
+  w[1] = R(1) - f;
+#pragma unroll
+  for (int j = 2; j < NO; ++j) w[j] = R(0);
+#pragma unroll
+  for (int k = 3; k <= NO; ++k) {
+    if (D && k == NO) {
+#pragma unroll
+      for (int j = 0; j < NO; ++j) dw[j] = (j < NO - 1 ? w[j] : R(0)) - (j > 0 ? w[j - 1] : R(0));
+    }
+    const R inv = R(1) / R(k - 1);
+#pragma unroll
+    for (int j = k - 1; j >= 0; --j) {
+      const R u = f + R(j);
+      const R a = (j < k - 1) ? w[j] : R(0);
+      const R b = (j > 0) ? w[j - 1] : R(0);
+      w[j] = (u * a + (R(k) - u) * b) * inv;
+    }
+  }
+  if (D && NO == 2) { dw[0] = R(1); dw[1] = R(-1); }
+}
+
+// Orders with a compiled spread / gather (md_spme_create accepts 2..14).
+#define SPME_ORDERS(X) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14)
 
 // ---------------------------------------------------------------- spread
+// A block takes SPREAD_ATOMS consecutive charges (cell order, hence compact
+// in space) and spreads them into a shared-memory tile that covers their
+// stencils, with shared-memory atomics; the tile is then added to the mesh
+// with one 4-wide atomic per 4 z points (binary32) or scalar atomics
+// (binary64), skipping empty groups.  Each charge's stencil base is taken in
+// the periodic image closest to the block's first charge, so that a block
+// next to a periodic face still has a compact tile.  The tile's z origin and
+// extent are multiples of 4 (K2 is a power of two >= 4, so a group never
+// wraps); rows are padded by one element against bank conflicts.  A block
+// whose tile does not fit adds every stencil point with a global atomic.
+constexpr int SPREAD_ATOMS = 64;
+constexpr int SPREAD_THREADS = 256;
+constexpr int SPREAD_TILE_BYTES = 64 * 1024;
+
 template <class R>
-__global__ void k_spme_spread(int N, const typename V4<R>::T* __restrict__ pos, int n, int K0, int K1, int K2,
-                              const DevState* __restrict__ st, R* __restrict__ Q) {
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const int nn = n * n;
-  const long i = t / nn;
-  if (i >= N) return;
-  const int ab = (int)(t - i * nn), a = ab / n, b = ab % n;
-  const typename V4<R>::T p = pos[i];
-  if (p.w == R(0)) return;
-  int b0, b1, b2;
-  R f0, f1, f2;
-  grid_coord<R>(p.x, (R)st->Li[0], K0, b0, f0);
-  grid_coord<R>(p.y, (R)st->Li[1], K1, b1, f1);
-  grid_coord<R>(p.z, (R)st->Li[2], K2, b2, f2);
-  R w0[16], w1[16], w2[16];
-  bspline_w<R>(n, f0, w0, nullptr);
-  bspline_w<R>(n, f1, w1, nullptr);
-  bspline_w<R>(n, f2, w2, nullptr);
-  const R qab = p.w * w0[a] * w1[b];
-  const long row = ((long)wrapk(b0 - a, K0) * K1 + wrapk(b1 - b, K1)) * K2;
-  for (int c = 0; c < n; ++c) atomicAdd(&Q[row + wrapk(b2 - c, K2)], qab * w2[c]);
+__device__ __forceinline__ void mesh_add4(R* dst, R a, R b, R c, R d);
+template <>
+__device__ __forceinline__ void mesh_add4<float>(float* dst, float a, float b, float c, float d) {
+  atomicAdd(reinterpret_cast<float4*>(dst), make_float4(a, b, c, d));
+}
+template <>
+__device__ __forceinline__ void mesh_add4<double>(double* dst, double a, double b, double c, double d) {
+  if (a != 0.0) atomicAdd(dst, a);
+  if (b != 0.0) atomicAdd(dst + 1, b);
+  if (c != 0.0) atomicAdd(dst + 2, c);
+  if (d != 0.0) atomicAdd(dst + 3, d);
+}
+
+template <class R, int NO>
+__global__ void __launch_bounds__(SPREAD_THREADS)
+k_spme_spread_t(int N, const typename V4<R>::T* __restrict__ pos, int K0, int K1, int K2,
+                const DevState* __restrict__ st, R* __restrict__ Q, int tile_cap) {
+  extern __shared__ __align__(16) unsigned char sp_smem[];
+  R* tile = reinterpret_cast<R*>(sp_smem);
+  __shared__ R sw[3][NO][SPREAD_ATOMS];
+  __shared__ R sq[SPREAD_ATOMS];
+  __shared__ int sb[3][SPREAD_ATOMS];
+  __shared__ int sbox[6];
+  const int i0 = blockIdx.x * SPREAD_ATOMS;
+  const int na = min(SPREAD_ATOMS, N - i0);
+  const int K[3] = {K0, K1, K2};
+  if (threadIdx.x < 6) sbox[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
+  __syncthreads();
+  if ((int)threadIdx.x < na) {
+    const typename V4<R>::T p = pos[i0 + threadIdx.x], p0 = pos[i0];
+    const R x[3] = {p.x, p.y, p.z}, x0[3] = {p0.x, p0.y, p0.z};
+    const R q = p.w;
+    sq[threadIdx.x] = q;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      int b, r;
+      R f, fr;
+      grid_coord<R>(x[d], (R)st->Li[d], K[d], b, f);
+      grid_coord<R>(x0[d], (R)st->Li[d], K[d], r, fr);
+      const int dv = b - r;
+      if (2 * dv > K[d]) b -= K[d];
+      else if (2 * dv < -K[d]) b += K[d];
+      sb[d][threadIdx.x] = b;
+      R w[NO], dw[NO];
+      bsp_t<R, NO, false>(f, w, dw);
+#pragma unroll
+      for (int j = 0; j < NO; ++j) sw[d][j][threadIdx.x] = w[j];
+      if (q != R(0)) {
+        atomicMin(&sbox[d], b);
+        atomicMax(&sbox[3 + d], b);
+      }
+    }
+  }
+  __syncthreads();
+  if (sbox[0] > sbox[3]) return;  // no charge in this block
+  const int o0 = sbox[0] - (NO - 1), o1 = sbox[1] - (NO - 1);
+  const int o2 = (sbox[2] - (NO - 1)) & ~3;
+  const long e0 = sbox[3] - o0 + 1, e1 = sbox[4] - o1 + 1;
+  const long e2 = (sbox[5] - o2 + 4) & ~3;
+  const long rs = e2 + 1;
+  const int nab = na * NO * NO;
+  if (e0 * e1 * rs <= tile_cap) {
+    const int tsz = (int)(e0 * e1 * rs), ie1 = (int)e1, irs = (int)rs;
+    for (int e = threadIdx.x; e < tsz; e += SPREAD_THREADS) tile[e] = R(0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < nab; e += SPREAD_THREADS) {
+      const int at = e / (NO * NO), ab = e - at * (NO * NO), a = ab / NO, b = ab - a * NO;
+      const R q = sq[at];
+      if (q == R(0)) continue;
+      const R qab = q * sw[0][a][at] * sw[1][b][at];
+      R* row = tile + ((sb[0][at] - a - o0) * ie1 + (sb[1][at] - b - o1)) * irs + (sb[2][at] - o2);
+#pragma unroll
+      for (int c = 0; c < NO; ++c) atomicAdd(row - c, qab * sw[2][c][at]);
+    }
+    __syncthreads();
+    const int g2 = (int)(e2 >> 2), ng = (int)(e0 * e1) * g2;
+    for (int g = threadIdx.x; g < ng; g += SPREAD_THREADS) {
+      const int z4 = g % g2, xy = g / g2, y = xy % ie1, x = xy / ie1;
+      const R* s = tile + (x * ie1 + y) * irs + 4 * z4;
+      const R v0 = s[0], v1 = s[1], v2 = s[2], v3 = s[3];
+      if (v0 == R(0) && v1 == R(0) && v2 == R(0) && v3 == R(0)) continue;
+      const int gx = (o0 + x) & (K0 - 1), gy = (o1 + y) & (K1 - 1), gz = (o2 + 4 * z4) & (K2 - 1);
+      mesh_add4<R>(Q + ((size_t)gx * K1 + gy) * K2 + gz, v0, v1, v2, v3);
+    }
+  } else {
+    for (int e = threadIdx.x; e < nab; e += SPREAD_THREADS) {
+      const int at = e / (NO * NO), ab = e - at * (NO * NO), a = ab / NO, b = ab - a * NO;
+      const R q = sq[at];
+      if (q == R(0)) continue;
+      const R qab = q * sw[0][a][at] * sw[1][b][at];
+      const size_t row = ((size_t)((sb[0][at] - a) & (K0 - 1)) * K1 + ((sb[1][at] - b) & (K1 - 1))) * K2;
+#pragma unroll
+      for (int c = 0; c < NO; ++c) atomicAdd(Q + row + ((sb[2][at] - c) & (K2 - 1)), qab * sw[2][c][at]);
+    }
+  }
 }
 
 // ---------------------------------------------------------------- FFT
-// Stockham radix-2 of one length-n line held in shared memory (two buffers);
-// the `lpb` lines of the block are processed together, n/2 threads per line.
+// Stockham transform of whole lines in shared memory, in the formulation of
+// Govindaraju et al. (SC'08): with Ns the length already transformed, stage
+// (radix R) takes butterfly j < n/R, reads its R inputs at stride n/R,
+// multiplies input r by W_n^{r k n/(Ns R)} (k = j mod Ns), applies an R-point
+// DFT in registers and writes output r to (j / Ns) Ns R + k + r Ns.  Stages
+// of radix 8, then one of radix 4 or 2, cover n = 2^LOGN and leave the line
+// in natural order.  One stage reads all its inputs, synchronises and then
+// writes, so a single buffer per line suffices.  A block of FFT_THREADS
+// threads holds FFT_THREADS / TPL lines (TPL = n/8 threads per line), each
+// padded by one element; twiddles come from a per-axis table computed once
+// in FP64 (conjugated for the inverse transform).
+constexpr int FFT_THREADS = 128;
+
 template <class T2>
 __device__ __forceinline__ T2 cmul(T2 a, T2 b) {
   T2 r;
@@ -111,99 +253,385 @@ __device__ __forceinline__ T2 cmul(T2 a, T2 b) {
   r.y = a.x * b.y + a.y * b.x;
   return r;
 }
-
-template <class R>
-__device__ void line_fft(typename C2<R>::T* x, typename C2<R>::T* y, const typename C2<R>::T* tw, int n,
-                         int lpb, typename C2<R>::T** out) {
-  typedef typename C2<R>::T T2;
-  const int half = n >> 1;
-  const int l = threadIdx.x / half, p = threadIdx.x % half;
-  for (int m = 1; m < n; m <<= 1) {
-    if (l < lpb) {
-      const int k = p % m, j = p / m;
-      const T2 w = tw[k * (half / m)];
-      const T2 c0 = x[l * n + p], c1 = cmul(w, x[l * n + p + half]);
-      T2 s, d;
-      s.x = c0.x + c1.x; s.y = c0.y + c1.y;
-      d.x = c0.x - c1.x; d.y = c0.y - c1.y;
-      y[l * n + j * 2 * m + k] = s;
-      y[l * n + j * 2 * m + k + m] = d;
-    }
-    __syncthreads();
-    T2* t = x; x = y; y = t;
-  }
-  *out = x;
+template <class T2>
+__device__ __forceinline__ T2 c_add(T2 a, T2 b) {
+  T2 r;
+  r.x = a.x + b.x;
+  r.y = a.y + b.y;
+  return r;
+}
+template <class T2>
+__device__ __forceinline__ T2 c_sub(T2 a, T2 b) {
+  T2 r;
+  r.x = a.x - b.x;
+  r.y = a.y - b.y;
+  return r;
+}
+// a * (SIGN i)
+template <int SIGN, class T2>
+__device__ __forceinline__ T2 c_mul_si(T2 a) {
+  T2 r;
+  r.x = SIGN > 0 ? -a.y : a.y;
+  r.y = SIGN > 0 ? a.x : -a.x;
+  return r;
 }
 
-template <class R>
-__device__ void load_twiddles(typename C2<R>::T* tw, int n, int sign) {
-  for (int t = threadIdx.x; t < n / 2; t += blockDim.x) {
-    double s, c;
-    sincospi(2.0 * t / n, &s, &c);
-    tw[t].x = (R)c;
-    tw[t].y = (R)(sign * s);
+// X_s = sum_r v_r exp(SIGN 2 pi i r s / 4)
+template <int SIGN, class T2>
+__device__ __forceinline__ void dft4(T2& v0, T2& v1, T2& v2, T2& v3) {
+  const T2 s0 = c_add(v0, v2), d0 = c_sub(v0, v2), s1 = c_add(v1, v3), d1 = c_mul_si<SIGN>(c_sub(v1, v3));
+  v0 = c_add(s0, s1);
+  v2 = c_sub(s0, s1);
+  v1 = c_add(d0, d1);
+  v3 = c_sub(d0, d1);
+}
+
+template <class R, int RR, int SIGN>
+__device__ __forceinline__ void dft_reg(typename C2<R>::T (&v)[RR]) {
+  typedef typename C2<R>::T T2;
+  if constexpr (RR == 2) {
+    const T2 a = v[0];
+    v[0] = c_add(a, v[1]);
+    v[1] = c_sub(a, v[1]);
+  } else if constexpr (RR == 4) {
+    dft4<SIGN>(v[0], v[1], v[2], v[3]);
+  } else {
+    // radix 8 = two radix-4 DFTs of the even and odd inputs, odd ones
+    // multiplied by W^k, W = exp(SIGN 2 pi i / 8)
+    T2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6], o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4<SIGN>(e0, e1, e2, e3);
+    dft4<SIGN>(o0, o1, o2, o3);
+    const R h = R(0.70710678118654752440);  // 1/sqrt(2)
+    T2 t;
+    t.x = (SIGN > 0 ? o1.x - o1.y : o1.x + o1.y) * h;
+    t.y = (SIGN > 0 ? o1.y + o1.x : o1.y - o1.x) * h;
+    o1 = t;
+    o2 = c_mul_si<SIGN>(o2);
+    t.x = (SIGN > 0 ? -o3.x - o3.y : -o3.x + o3.y) * h;
+    t.y = (SIGN > 0 ? -o3.y + o3.x : -o3.y - o3.x) * h;
+    o3 = t;
+    v[0] = c_add(e0, o0);
+    v[4] = c_sub(e0, o0);
+    v[1] = c_add(e1, o1);
+    v[5] = c_sub(e1, o1);
+    v[2] = c_add(e2, o2);
+    v[6] = c_sub(e2, o2);
+    v[3] = c_add(e3, o3);
+    v[7] = c_sub(e3, o3);
   }
 }
 
-// mode 0: real input lines (z, contiguous) -> half-complex output
-// mode 1: complex lines along axis x or y of the half-complex array
-// mode 2: half-complex z lines -> real output (Hermitian completion)
-template <class R>
-__global__ void k_fft(const void* in, void* out, int mode, int n, int lpb, long nlines, long stride,
-                      long lines_inner, long outer_stride, long in_astride, long out_astride, int sign) {
+template <int LOGN>
+struct FftGeom {
+  static constexpr int n = 1 << LOGN;
+  static constexpr int TPL = n >= 8 ? n / 8 : 1;  // threads per line
+  static constexpr int LPB = FFT_THREADS / TPL;   // lines per block
+  static constexpr int LS = n + 1;                // padded line stride
+  static constexpr int EPT = LPB * n / FFT_THREADS;  // elements per thread
+};
+
+// the stages from Ns = 2^LOGNS on, for the line x of this thread (lane tl of
+// the line's TPL threads); every thread of the block takes part
+template <class R, int LOGN, int LOGNS, int SIGN>
+__device__ __forceinline__ void fft_stages(typename C2<R>::T* x, const typename C2<R>::T* tw, int tl) {
   typedef typename C2<R>::T T2;
-  extern __shared__ __align__(16) unsigned char fft_smem[];
-  T2* tw = reinterpret_cast<T2*>(fft_smem);
-  T2* x = tw + n / 2;
-  T2* y = x + lpb * n;
-  load_twiddles<R>(tw, n, sign);
-  const long line0 = (long)blockIdx.x * lpb;
-  const int batch = blockIdx.y;
-  const int nh = n / 2 + 1;
-  // load
-  for (int e = threadIdx.x; e < lpb * n; e += blockDim.x) {
-    int l, k;
-    if (mode == 1) { l = e % lpb; k = e / lpb; }  // lines adjacent in memory: coalesce across l
-    else { l = e / n; k = e % n; }
-    const long L = line0 + l;
-    T2 v;
-    v.x = R(0); v.y = R(0);
-    if (L < nlines) {
-      if (mode == 0) {
-        const R* src = reinterpret_cast<const R*>(in) + batch * in_astride + L * n;
-        v.x = src[k];
-      } else if (mode == 1) {
-        const T2* src = reinterpret_cast<const T2*>(in) + batch * in_astride;
-        const long o = (L / lines_inner) * outer_stride + (L % lines_inner);
-        v = src[o + k * stride];
-      } else {
-        const T2* src = reinterpret_cast<const T2*>(in) + batch * in_astride + L * nh;
-        if (k < nh) v = src[k];
-        else { const T2 u = src[n - k]; v.x = u.x; v.y = -u.y; }
-      }
+  constexpr int n = 1 << LOGN, TPL = FftGeom<LOGN>::TPL;
+  constexpr int LR = (LOGN - LOGNS) >= 3 ? 3 : (LOGN - LOGNS);
+  constexpr int RR = 1 << LR, NS = 1 << LOGNS, NBF = n / RR, BPT = NBF / TPL;
+  static_assert(BPT >= 1, "at least one butterfly per thread");
+  T2 v[BPT][RR];
+#pragma unroll
+  for (int q = 0; q < BPT; ++q) {
+    const int j = tl + q * TPL;
+#pragma unroll
+    for (int r = 0; r < RR; ++r) v[q][r] = x[j + r * NBF];
+    if constexpr (LOGNS > 0) {
+      const int k = j & (NS - 1);
+#pragma unroll
+      for (int r = 1; r < RR; ++r) v[q][r] = cmul(v[q][r], tw[(r * k) << (LOGN - LOGNS - LR)]);
     }
-    x[l * n + k] = v;
+    dft_reg<R, RR, SIGN>(v[q]);
   }
   __syncthreads();
-  T2* res;
-  line_fft<R>(x, y, tw, n, lpb, &res);
-  // store
-  for (int e = threadIdx.x; e < lpb * n; e += blockDim.x) {
-    int l, k;
-    if (mode == 1) { l = e % lpb; k = e / lpb; }
-    else { l = e / n; k = e % n; }
-    const long L = line0 + l;
-    if (L >= nlines) continue;
-    const T2 v = res[l * n + k];
-    if (mode == 0) {
-      if (k < nh) reinterpret_cast<T2*>(out)[batch * out_astride + L * nh + k] = v;
-    } else if (mode == 1) {
-      const long o = (L / lines_inner) * outer_stride + (L % lines_inner);
-      reinterpret_cast<T2*>(out)[batch * out_astride + o + k * stride] = v;
-    } else {
-      reinterpret_cast<R*>(out)[batch * out_astride + L * n + k] = v.x;
+#pragma unroll
+  for (int q = 0; q < BPT; ++q) {
+    const int j = tl + q * TPL;
+    const int d = ((j >> LOGNS) << (LOGNS + LR)) + (j & (NS - 1));
+#pragma unroll
+    for (int r = 0; r < RR; ++r) x[d + r * NS] = v[q][r];
+  }
+  __syncthreads();
+  if constexpr (LOGNS + LR < LOGN) fft_stages<R, LOGN, LOGNS + LR, SIGN>(x, tw, tl);
+}
+
+template <class R, int SIGN>
+__device__ __forceinline__ void load_tw(typename C2<R>::T* tw, const typename C2<R>::T* __restrict__ twg, int n) {
+  for (int m = threadIdx.x; m < n; m += blockDim.x) {
+    typename C2<R>::T w = twg[m];
+    if (SIGN > 0) w.y = -w.y;
+    tw[m] = w;
+  }
+}
+
+// One transform pass over lines of one axis.
+//   MODE 0: real lines along z (contiguous) -> half-complex lines (n/2+1);
+//           the input lines are cleared after they are read
+//   MODE 1: complex lines of the half spectrum; line L starts at
+//           (L / inner) * outer + L % inner, elements `stride` apart; lines
+//           adjacent in memory share a block, so loads coalesce across lines
+//   MODE 2: half-complex z lines -> real lines (Hermitian completion, the
+//           FFTW c2r convention the reference relies on)
+// blockIdx.y selects the batch (in_bs / out_bs apart).  OUT4 (MODE 2): the
+// three batches of a line are transformed side by side in one block, by
+// three groups of FFT_THREADS threads, and written interleaved, one Real4
+// (x, y, z, 0) per mesh point.
+template <class R, int LOGN, int MODE, int SIGN, int OUT4>
+__global__ void __launch_bounds__(FFT_THREADS * (OUT4 ? 3 : 1))
+k_fftp(const void* in, void* out, const typename C2<R>::T* __restrict__ twg, long nlines, long stride, long inner,
+       long outer, long in_bs, long out_bs) {
+  typedef typename C2<R>::T T2;
+  typedef FftGeom<LOGN> G;
+  constexpr int n = G::n, LPB = G::LPB, LS = G::LS, NG = OUT4 ? 3 : 1, nh = n / 2 + 1;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  T2* tw = reinterpret_cast<T2*>(fft_smem);
+  T2* X = tw + n;
+  long* lo = reinterpret_cast<long*>(X + NG * LPB * LS);
+  load_tw<R, SIGN>(tw, twg, n);
+  const long line0 = (long)blockIdx.x * LPB;
+  if (threadIdx.x < LPB) {
+    const long L = line0 + threadIdx.x;
+    lo[threadIdx.x] = MODE == 1 ? (L / inner) * outer + L % inner : L;
+  }
+  __syncthreads();
+  const int grp = NG > 1 ? (int)threadIdx.x / FFT_THREADS : 0;
+  const int gt = NG > 1 ? (int)threadIdx.x % FFT_THREADS : (int)threadIdx.x;
+  const long batch = OUT4 ? grp : blockIdx.y;
+  T2* Xb = X + grp * LPB * LS;
+  {
+    // all loads of a thread are issued before any shared-memory store (and,
+    // in MODE 0, before the mesh is cleared), so they are in flight together
+    T2 vv[G::EPT];
+#pragma unroll
+    for (int s = 0; s < G::EPT; ++s) {
+      const int e = gt + s * FFT_THREADS;
+      int l, k;
+      if (MODE == 1) { l = e % LPB; k = e / LPB; }
+      else { l = e >> LOGN; k = e & (n - 1); }
+      const long L = line0 + l;
+      T2 v;
+      v.x = R(0);
+      v.y = R(0);
+      if (L < nlines) {
+        if (MODE == 0) {
+          v.x = reinterpret_cast<const R*>(in)[batch * in_bs + L * n + k];
+        } else if (MODE == 1) {
+          v = reinterpret_cast<const T2*>(in)[batch * in_bs + lo[l] + k * stride];
+        } else {
+          const T2* src = reinterpret_cast<const T2*>(in) + batch * in_bs + L * nh;
+          if (k < nh) v = src[k];
+          else { const T2 u = src[n - k]; v.x = u.x; v.y = -u.y; }
+        }
+      }
+      vv[s] = v;
+    }
+#pragma unroll
+    for (int s = 0; s < G::EPT; ++s) {
+      const int e = gt + s * FFT_THREADS;
+      int l, k;
+      if (MODE == 1) { l = e % LPB; k = e / LPB; }
+      else { l = e >> LOGN; k = e & (n - 1); }
+      if (MODE == 0) {
+        // the real mesh is consumed: cleared for the next spread
+        const long L = line0 + l;
+        if (L < nlines) reinterpret_cast<R*>(const_cast<void*>(in))[batch * in_bs + L * n + k] = R(0);
+      }
+      Xb[l * LS + k] = vv[s];
     }
   }
+  __syncthreads();
+  fft_stages<R, LOGN, 0, SIGN>(Xb + (gt / G::TPL) * LS, tw, gt % G::TPL);
+  if (OUT4) {
+    typedef typename V4<R>::T R4;
+    for (int e = threadIdx.x; e < LPB * n; e += NG * FFT_THREADS) {
+      const int l2 = e >> LOGN, k = e & (n - 1);
+      const long L = line0 + l2;
+      if (L >= nlines) continue;
+      R4 o;
+      o.x = X[l2 * LS + k].x;
+      o.y = X[LPB * LS + l2 * LS + k].x;
+      o.z = X[2 * LPB * LS + l2 * LS + k].x;
+      o.w = R(0);
+      reinterpret_cast<R4*>(out)[L * n + k] = o;
+    }
+    return;
+  }
+  for (int e = threadIdx.x; e < LPB * n; e += FFT_THREADS) {
+    int l2, k;
+    if (MODE == 1) { l2 = e % LPB; k = e / LPB; }
+    else { l2 = e >> LOGN; k = e & (n - 1); }
+    const long L = line0 + l2;
+    if (L >= nlines) continue;
+    const T2 v = X[l2 * LS + k];
+    if (MODE == 0) {
+      if (k < nh) reinterpret_cast<T2*>(out)[batch * out_bs + L * nh + k] = v;
+    } else if (MODE == 1) {
+      reinterpret_cast<T2*>(out)[batch * out_bs + lo[l2] + k * stride] = v;
+    } else {
+      reinterpret_cast<R*>(out)[batch * out_bs + L * n + k] = v.x;
+    }
+  }
+}
+
+template <class R>
+static size_t fftp_smem(int logn, int nbuf) {
+  const int n = 1 << logn, tpl = n >= 8 ? n / 8 : 1, lpb = FFT_THREADS / tpl;
+  return sizeof(typename C2<R>::T) * ((size_t)n + (size_t)nbuf * lpb * (n + 1)) + sizeof(long) * lpb;
+}
+
+// Forward transform along x, the k-space step and the inverse transform(s)
+// along x, in one pass over the x lines (y, kz fixed) of the half spectrum:
+//   psi(m) = exp(-pi^2 m^2 / beta^2) / m^2 |b0(i)|^2 |b1(j)|^2 |b2(k)|^2 / (pi V)
+//     (calB / calPsiFPhiF), evaluated in FP64 from the per-axis |b|^2
+//     tables for the current box, so an NPT box change needs no extra pass,
+//   E = 1/2 sum_m psi |Q^|^2 and the diagonal virial (FP64, with_stats),
+//   ik (METHOD 0): the three products phi_d = i (-2 pi m_d) psi Q^,
+//   (merge = 0: the sums stay in DevState::scratch for a later merge)
+//   analytic (METHOD 1): psi Q^ / 2 (FBSpline normalisation),
+// each transformed back along x and written to C[1 + d].  One group of
+// FFT_THREADS threads per product: group 0 runs the forward transform and
+// the k-space step (the other groups run the same stages on their own
+// buffers, keeping the barriers uniform), then every group forms and
+// inverts its product.  The last block merges the energy and the virial
+// into the statistics slots.
+template <class R, int LOGN, int METHOD>
+__global__ void __launch_bounds__(FFT_THREADS * (METHOD == 0 ? 3 : 1))
+k_fft_x_kspace(typename C2<R>::T* C, const typename C2<R>::T* __restrict__ twg, const double* __restrict__ bm, int K1,
+               int K2, double beta, DevState* st, double* partials, int with_stats, int merge) {
+  typedef typename C2<R>::T T2;
+  typedef FftGeom<LOGN> G;
+  constexpr int n = G::n, LPB = G::LPB, LS = G::LS, EPT = G::EPT, NG = METHOD == 0 ? 3 : 1;
+  const int K2h = K2 / 2 + 1;
+  const long nlines = (long)K1 * K2h, stride = nlines;
+  const size_t nhalf = (size_t)n * nlines;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  T2* twf = reinterpret_cast<T2*>(fft_smem);
+  T2* twi = twf + n;
+  T2* X = twi + n;
+  T2* Y = X + LPB * LS;  // NG buffers
+  R* PS = reinterpret_cast<R*>(Y + NG * LPB * LS);
+  int* lj = reinterpret_cast<int*>(PS + LPB * LS);
+  int* lk = lj + LPB;
+  load_tw<R, -1>(twf, twg, n);
+  load_tw<R, 1>(twi, twg, n);
+  const long line0 = (long)blockIdx.x * LPB;
+  if (threadIdx.x < LPB) {
+    const long L = line0 + threadIdx.x;
+    lj[threadIdx.x] = (int)(L / K2h);
+    lk[threadIdx.x] = (int)(L % K2h);
+  }
+  const int grp = NG > 1 ? (int)threadIdx.x / FFT_THREADS : 0;
+  const int gt = NG > 1 ? (int)threadIdx.x % FFT_THREADS : (int)threadIdx.x;
+  if (grp == 0) {
+    T2 vv[EPT];
+#pragma unroll
+    for (int s = 0; s < EPT; ++s) {
+      const int e = gt + s * FFT_THREADS, l = e % LPB, i = e / LPB;
+      const long L = line0 + l;
+      vv[s].x = R(0);
+      vv[s].y = R(0);
+      if (L < nlines) vv[s] = C[L + i * stride];
+    }
+#pragma unroll
+    for (int s = 0; s < EPT; ++s) {
+      const int e = gt + s * FFT_THREADS;
+      X[(e % LPB) * LS + e / LPB] = vv[s];
+    }
+  }
+  __syncthreads();
+  const int l = gt / G::TPL, tl = gt % G::TPL;
+  fft_stages<R, LOGN, 0, -1>((grp == 0 ? X : Y + grp * LPB * LS) + l * LS, twf, tl);
+  double v[4] = {0, 0, 0, 0};
+  if (grp == 0) {
+    const double V = st->L[0] * st->L[1] * st->L[2];
+    const double sc = M_PI * M_PI / (beta * beta), pv = 1.0 / (M_PI * V);
+    const double* bm1 = bm + n;
+    const double* bm2 = bm1 + K1;
+#pragma unroll
+    for (int s = 0; s < EPT; ++s) {
+      const int e = gt + s * FFT_THREADS, le = e % LPB, i = e / LPB;
+      const long L = line0 + le;
+      const int j = lj[le], k = lk[le];
+      const int ip = i <= n / 2 ? i : i - n, jp = j <= K1 / 2 ? j : j - K1, kp = k;
+      const double m[3] = {ip * st->Li[0], jp * st->Li[1], kp * st->Li[2]};
+      const double mm = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+      const bool live = L < nlines && (ip || jp || kp);
+      const R ps = live ? (R)(exp(-sc * mm) / mm * (bm[i] * bm1[j] * bm2[k]) * pv) : R(0);
+      PS[le * LS + i] = ps;
+      if (with_stats && live) {
+        // E = 1/2 sum_m |Q^|^2 psi over the full spectrum: interior z planes count twice
+        const T2 q = X[le * LS + i];
+        const double wgt = (k == 0 || (2 * k == K2)) ? 1.0 : 2.0;
+        const double e2 = 0.5 * wgt * ((double)q.x * q.x + (double)q.y * q.y) * (double)ps;
+        const double f = 2.0 * (1.0 + M_PI * M_PI * mm / (beta * beta)) / mm;
+        v[0] += e2;
+        // pressure tensor V P_aa = sum_m E_m (1 - f m_a^2); the virial slots hold W_aa = -V P_aa
+#pragma unroll
+        for (int d = 0; d < 3; ++d) v[1 + d] += -e2 * (1.0 - f * m[d] * m[d]);
+      }
+    }
+  }
+  __syncthreads();
+  T2* Yg = Y + grp * LPB * LS;
+#pragma unroll
+  for (int s = 0; s < EPT; ++s) {
+    const int e = gt + s * FFT_THREADS, le = e % LPB, i = e / LPB;
+    const T2 q = X[le * LS + i];
+    const R ps = PS[le * LS + i];
+    T2 g;
+    if (METHOD == 0) {
+      // phi_d = i (-2 pi m_d) psi Q^, d = grp, m = (i', j', k) / L (signed indices)
+      const int ix = grp == 0 ? (i <= n / 2 ? i : i - n)
+                              : grp == 1 ? (lj[le] <= K1 / 2 ? lj[le] : lj[le] - K1) : lk[le];
+      const R c = (R)(-2.0 * M_PI * (ix * st->Li[grp])) * ps;
+      g.x = -q.y * c;
+      g.y = q.x * c;
+    } else {
+      g.x = q.x * (R(0.5) * ps);
+      g.y = q.y * (R(0.5) * ps);
+    }
+    Yg[le * LS + i] = g;
+  }
+  __syncthreads();
+  fft_stages<R, LOGN, 0, 1>(Yg + l * LS, twi, tl);
+  T2* out = C + (1 + grp) * nhalf;
+  for (int e = gt; e < LPB * n; e += FFT_THREADS) {
+    const int le = e % LPB, i = e / LPB;
+    const long L = line0 + le;
+    if (L < nlines) out[L + i * stride] = Yg[le * LS + i];
+  }
+  if (with_stats && block_reduce_finish<4>(v, partials, &st->red_counter[RED_SPME], st->scratch, true) && merge) {
+    // reciprocal energy into its slot, its diagonal virial added to the virial slots
+    st->stats[MD_STAT_ELEC_REC] = st->scratch[0];
+    for (int d = 0; d < 3; ++d) st->stats[MD_STAT_VIRIAL_XX + d] += st->scratch[1 + d];
+  }
+}
+
+template <class R>
+static size_t fftx_smem(int logn, int method) {
+  const int n = 1 << logn, tpl = n >= 8 ? n / 8 : 1, lpb = FFT_THREADS / tpl, ng = method == 0 ? 3 : 1;
+  return sizeof(typename C2<R>::T) * (2 * (size_t)n + (1 + (size_t)ng) * lpb * (n + 1)) +
+         sizeof(R) * (size_t)lpb * (n + 1) + 2 * sizeof(int) * lpb;
+}
+
+// per-axis forward twiddle table exp(-2 pi i m / n), m < n, from FP64
+template <class R>
+__global__ void k_fft_twiddles(int n, typename C2<R>::T* tw) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  double s, c;
+  sincospi(2.0 * m / n, &s, &c);
+  tw[m].x = (R)c;
+  tw[m].y = (R)(-s);
 }
 
 // ---------------------------------------------------------------- influence
@@ -223,7 +651,9 @@ __device__ __forceinline__ double bmod_d(int n, int K, int m) {
 
 // psi is recomputed only when the box differs from `tab`, the box it was last
 // computed for (NPT); the comparison is made on the device so that no host
-// round trip is needed, and `tab` is updated by k_spme_box_tab afterwards
+// round trip is needed, and `tab` is updated by k_spme_box_tab afterwards.
+// The force chain evaluates psi inside its x pass; this stored copy serves
+// the adjoint and md_spme_get_influence.
 template <class R>
 __global__ void k_spme_influence(int K0, int K1, int K2, int n, double beta, const DevState* st, R* psi,
                                  const double* tab) {
@@ -246,109 +676,200 @@ __global__ void k_spme_box_tab(const DevState* st, double* tab) {
   for (int d = 0; d < 3; ++d) tab[d] = st->L[d];
 }
 
-// energy + diagonal virial and the products written into C[1..]
-template <class R>
-__global__ void __launch_bounds__(256)
-k_spme_kspace(int K0, int K1, int K2, int method, double beta, const R* __restrict__ psi,
-              typename C2<R>::T* __restrict__ C, size_t nhalf, DevState* st, double* partials, int with_stats) {
-  typedef typename C2<R>::T T2;
-  const int K2h = K2 / 2 + 1;
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  double v[4] = {0, 0, 0, 0};
-  if (t < (long)nhalf) {
-    const int k = (int)(t % K2h), j = (int)((t / K2h) % K1), i = (int)(t / ((long)K2h * K1));
-    const int ip = i <= K0 / 2 ? i : i - K0, jp = j <= K1 / 2 ? j : j - K1, kp = k;
-    const T2 q = C[t];
-    const R ps = psi[t];
-    const double m[3] = {ip * st->Li[0], jp * st->Li[1], kp * st->Li[2]};
-    if (method == 0) {
-      for (int d = 0; d < 3; ++d) {
-        const R c = (R)(-2.0 * M_PI * m[d]) * ps;  // phi_d = i (-2 pi m_d) psi
-        T2 g;
-        g.x = -q.y * c;
-        g.y = q.x * c;
-        C[(1 + d) * nhalf + t] = g;
-      }
-    } else {
-      T2 g;
-      g.x = q.x * (R(0.5) * ps);  // analytic: psi / 2 (FBSpline normalisation)
-      g.y = q.y * (R(0.5) * ps);
-      C[nhalf + t] = g;
-    }
-    if (with_stats && (ip || jp || kp)) {
-      // E = 1/2 sum_m |Q^|^2 psi over the full spectrum: interior z planes count twice
-      const double wgt = (k == 0 || (2 * k == K2)) ? 1.0 : 2.0;
-      const double e = 0.5 * wgt * ((double)q.x * q.x + (double)q.y * q.y) * (double)ps;
-      const double mm = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
-      const double f = 2.0 * (1.0 + M_PI * M_PI * mm / (beta * beta)) / mm;
-      v[0] = e;
-      // pressure tensor V P_aa = sum_m E_m (1 - f m_a^2); the virial slots hold W_aa = -V P_aa
-      for (int d = 0; d < 3; ++d) v[1 + d] = -e * (1.0 - f * m[d] * m[d]);
-    }
-  }
-  if (with_stats) block_reduce_finish<4>(v, partials, &st->red_counter[RED_SPME], st->scratch, true);
-}
-
-__global__ void k_spme_stats_merge(DevState* st) {
-  // reciprocal energy into its slot, its diagonal virial added to the virial slots
-  st->stats[MD_STAT_ELEC_REC] = st->scratch[0];
-  for (int d = 0; d < 3; ++d) st->stats[MD_STAT_VIRIAL_XX + d] += st->scratch[1 + d];
+// per-axis |b_d(m)|^2 tables, concatenated: [0, K0) | [0, K1) | [0, K2/2+1)
+__global__ void k_spme_bmod(int K0, int K1, int K2, int n, double* bm) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < K0) bm[t] = bmod_d(n, K0, t);
+  else if (t < K0 + K1) bm[t] = bmod_d(n, K1, t - K0);
+  else if (t < K0 + K1 + K2 / 2 + 1) bm[t] = bmod_d(n, K2, t - K0 - K1);
 }
 
 // ---------------------------------------------------------------- gather
-template <class R>
-__global__ void __launch_bounds__(256)
-k_spme_gather(int N, const typename V4<R>::T* __restrict__ pos, int n, int K0, int K1, int K2, int method,
-              const DevState* __restrict__ st, const R* __restrict__ G, size_t nreal, double4a* __restrict__ force) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= N) return;
-  const typename V4<R>::T p = pos[warp];
-  int b0, b1, b2;
-  R f0, f1, f2;
-  grid_coord<R>(p.x, (R)st->Li[0], K0, b0, f0);
-  grid_coord<R>(p.y, (R)st->Li[1], K1, b1, f1);
-  grid_coord<R>(p.z, (R)st->Li[2], K2, b2, f2);
-  R w0[16], w1[16], w2[16], d0[16], d1[16], d2[16];
-  bspline_w<R>(n, f0, w0, d0);
-  bspline_w<R>(n, f1, w1, d1);
-  bspline_w<R>(n, f2, w2, d2);
-  R fx = 0, fy = 0, fz = 0;
-  for (int ab = lane; ab < n * n; ab += 32) {
-    const int a = ab / n, b = ab % n;
-    const long row = ((long)wrapk(b0 - a, K0) * K1 + wrapk(b1 - b, K1)) * K2;
-    for (int c = 0; c < n; ++c) {
-      const long idx = row + wrapk(b2 - c, K2);
-      if (method == 0) {
-        const R w = w0[a] * w1[b] * w2[c];
-        fx += G[idx] * w;
-        fy += G[nreal + idx] * w;
-        fz += G[2 * nreal + idx] * w;
-      } else {
-        const R g = G[idx];
-        fx -= g * d0[a] * w1[b] * w2[c];
-        fy -= g * w0[a] * d1[b] * w2[c];
-        fz -= g * w0[a] * w1[b] * d2[c];
-      }
+// A block takes GATHER_ATOMS consecutive atoms (cell order) with LPA lanes
+// each (the power of two >= order, at least 4); lane a takes the stencil
+// plane b0 - a and runs over its order^2 points, and the lanes' sums are
+// combined by shuffles.  The block first stages the mesh region covering its
+// charges' stencils (image-adjusted as in the spread) into shared memory
+// with coalesced, independent row loads, then gathers from there; a block
+// whose region does not fit reads the mesh directly.
+//   MODE 0: ik, the three convolved meshes interleaved, one Real4 per point
+//   MODE 1: analytic differentiation of the single convolved mesh
+//   MODE 2: adjoint gather of Phi: potential dE/dq_i and exact position
+//           gradient dE/dx_i, written in the caller's atom order
+// store (MODES 0, 1): force is a separate buffer that receives every atom's
+// reciprocal force (zero for neutral atoms) instead of accumulating it.
+// MD_SPME_GATHER_TILE_KB: shared-memory budget of the staged region (0: read
+// the mesh directly)
+#ifndef MD_SPME_GATHER_TILE_KB
+#define MD_SPME_GATHER_TILE_KB 64
+#endif
+constexpr int GATHER_ATOMS = 32;
+constexpr int GATHER_TILE_BYTES = MD_SPME_GATHER_TILE_KB * 1024;
+
+__host__ __device__ constexpr int gather_lanes(int order) { return order <= 4 ? 4 : (order <= 8 ? 8 : 16); }
+
+template <class R, int NO, int MODE>
+__global__ void __launch_bounds__(GATHER_ATOMS * gather_lanes(NO))
+k_spme_gather_t(int N, const typename V4<R>::T* __restrict__ pos, const int* __restrict__ id, int K0, int K1,
+                int K2, const DevState* __restrict__ st, const void* __restrict__ Gv, double4a* __restrict__ force,
+                double* __restrict__ dq, double* __restrict__ dr, int tile_cap, int store) {
+  typedef typename V4<R>::T R4;
+  typedef typename std::conditional<MODE == 0, R4, R>::type GT;  // mesh element
+  constexpr int LPA = gather_lanes(NO), NT = GATHER_ATOMS * LPA;
+  extern __shared__ __align__(32) unsigned char g_smem[];
+  GT* tile = reinterpret_cast<GT*>(g_smem);
+  __shared__ int sbox[6];
+  const int i0 = blockIdx.x * GATHER_ATOMS;
+  const int i = i0 + (int)threadIdx.x / LPA, a = threadIdx.x & (LPA - 1);
+  const bool act = i < N;
+  const int K[3] = {K0, K1, K2};
+  if (threadIdx.x < 6) sbox[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
+  R4 p;
+  if (act) p = pos[i];
+  else { p.x = R(0); p.y = R(0); p.z = R(0); p.w = R(0); }
+  const R4 p0 = pos[i0];
+  const R x[3] = {p.x, p.y, p.z}, x0[3] = {p0.x, p0.y, p0.z};
+  int bb[3];
+  R ff[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    int r;
+    R fr;
+    grid_coord<R>(x[d], (R)st->Li[d], K[d], bb[d], ff[d]);
+    grid_coord<R>(x0[d], (R)st->Li[d], K[d], r, fr);
+    const int dv = bb[d] - r;
+    if (2 * dv > K[d]) bb[d] -= K[d];
+    else if (2 * dv < -K[d]) bb[d] += K[d];
+  }
+  // a neutral atom feels no force, but its potential is the adjoint's dE/dq
+  const bool live = act && (MODE == 2 || p.w != R(0));
+  __syncthreads();
+  if (live && a == 0) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      atomicMin(&sbox[d], bb[d]);
+      atomicMax(&sbox[3 + d], bb[d]);
     }
   }
-  double Fx = fx, Fy = fy, Fz = fz;
-  for (int o = 16; o > 0; o >>= 1) {
-    Fx += __shfl_xor_sync(0xffffffffu, Fx, o);
-    Fy += __shfl_xor_sync(0xffffffffu, Fy, o);
-    Fz += __shfl_xor_sync(0xffffffffu, Fz, o);
+  R w0[NO], w1[NO], w2[NO], d0[NO], d1[NO], d2[NO];
+  bsp_t<R, NO, MODE != 0>(ff[0], w0, d0);
+  bsp_t<R, NO, MODE != 0>(ff[1], w1, d1);
+  bsp_t<R, NO, MODE != 0>(ff[2], w2, d2);
+  R wa = R(0), da = R(0);
+#pragma unroll
+  for (int j = 0; j < NO; ++j)
+    if (j == a) { wa = w0[j]; da = d0[j]; }
+  __syncthreads();
+  if (sbox[0] > sbox[3]) {  // no charge in this block
+    if (MODE != 2 && store && act && a == 0) force[i] = double4a{0.0, 0.0, 0.0, 0.0};
+    return;
   }
-  if (lane == 0) {
-    const double q = (double)p.w;
-    double4a f = force[warp];
-    if (method == 0) {
-      f.x += q * Fx; f.y += q * Fy; f.z += q * Fz;
+  const int o0 = sbox[0] - (NO - 1), o1 = sbox[1] - (NO - 1), o2 = sbox[2] - (NO - 1);
+  const long e0 = sbox[3] - o0 + 1, e1 = sbox[4] - o1 + 1, e2 = sbox[5] - o2 + 1;
+  // odd plane stride: the lanes of an atom (one x plane each) then fall on
+  // different shared-memory banks
+  const long ps = (e1 * e2) | 1;
+  const bool staged = e0 * ps <= tile_cap;
+  const GT* Gm = reinterpret_cast<const GT*>(Gv);
+  if (staged) {
+    // one mesh row (e2 points along z) per warp pass, lanes along z
+    const int nrow = (int)(e0 * e1), ie1 = (int)e1, ie2 = (int)e2, ips = (int)ps;
+    for (int row = threadIdx.x >> 5; row < nrow; row += NT >> 5) {
+      const int y = row % ie1, xx = row / ie1;
+      const size_t g = ((size_t)((o0 + xx) & (K0 - 1)) * K1 + ((o1 + y) & (K1 - 1))) * K2;
+      GT* t = tile + xx * ips + y * ie2;
+      for (int z = threadIdx.x & 31; z < ie2; z += 32) t[z] = Gm[g + ((o2 + z) & (K2 - 1))];
+    }
+    __syncthreads();
+  }
+  // each stencil row (order points along z) is summed in the working
+  // precision, the rows in FP64
+  double F0 = 0.0, F1 = 0.0, F2 = 0.0, F3 = 0.0;
+  if (live && a < NO) {
+    int kz[NO];
+    size_t xrow;
+    if (staged) {
+#pragma unroll
+      for (int c = 0; c < NO; ++c) kz[c] = bb[2] - c - o2;
+      xrow = (size_t)(bb[0] - a - o0) * ps;
     } else {
-      f.x += 2.0 * q * Fx * K0 * st->Li[0];
-      f.y += 2.0 * q * Fy * K1 * st->Li[1];
-      f.z += 2.0 * q * Fz * K2 * st->Li[2];
+#pragma unroll
+      for (int c = 0; c < NO; ++c) kz[c] = (bb[2] - c) & (K2 - 1);
+      xrow = (size_t)((bb[0] - a) & (K0 - 1)) * K1;
     }
-    force[warp] = f;
+#pragma unroll
+    for (int b = 0; b < NO; ++b) {
+      const GT* G = staged ? tile + xrow + (bb[1] - b - o1) * e2
+                           : Gm + (xrow + ((bb[1] - b) & (K1 - 1))) * K2;
+      const R wab = wa * w1[b];
+      R s0 = R(0), s1 = R(0), s2 = R(0), s3 = R(0);
+      if constexpr (MODE == 0) {
+#pragma unroll
+        for (int c = 0; c < NO; ++c) {
+          const R4 g = G[kz[c]];
+          const R w = wab * w2[c];
+          s0 += g.x * w;
+          s1 += g.y * w;
+          s2 += g.z * w;
+        }
+      } else {
+        const R dab = da * w1[b], wdb = wa * d1[b];
+#pragma unroll
+        for (int c = 0; c < NO; ++c) {
+          const R g = G[kz[c]];
+          if (MODE == 1) {
+            s0 -= g * dab * w2[c];
+            s1 -= g * wdb * w2[c];
+            s2 -= g * wab * d2[c];
+          } else {
+            s0 += g * wab * w2[c];
+            s1 += g * dab * w2[c];
+            s2 += g * wdb * w2[c];
+            s3 += g * wab * d2[c];
+          }
+        }
+      }
+      F0 += (double)s0;
+      F1 += (double)s1;
+      F2 += (double)s2;
+      if (MODE == 2) F3 += (double)s3;
+    }
   }
+#pragma unroll
+  for (int o = LPA / 2; o > 0; o >>= 1) {
+    F0 += __shfl_xor_sync(0xffffffffu, F0, o);
+    F1 += __shfl_xor_sync(0xffffffffu, F1, o);
+    F2 += __shfl_xor_sync(0xffffffffu, F2, o);
+    if (MODE == 2) F3 += __shfl_xor_sync(0xffffffffu, F3, o);
+  }
+  if (!act || a != 0) return;
+  const double q = (double)p.w;
+  if (MODE == 2) {
+    const int o = id[i];  // results in the caller's atom order
+    if (dq) dq[o] = F0;
+    if (dr) {
+      dr[3 * o] = q * F1 * K0 * st->Li[0];
+      dr[3 * o + 1] = q * F2 * K1 * st->Li[1];
+      dr[3 * o + 2] = q * F3 * K2 * st->Li[2];
+    }
+    return;
+  }
+  double4a f = {0.0, 0.0, 0.0, 0.0};
+  if (!live) {
+    if (store) force[i] = f;
+    return;
+  }
+  if (!store) f = force[i];
+  if (MODE == 0) {
+    f.x += q * F0;
+    f.y += q * F1;
+    f.z += q * F2;
+  } else {
+    f.x += 2.0 * q * F0 * K0 * st->Li[0];
+    f.y += 2.0 * q * F1 * K1 * st->Li[1];
+    f.z += 2.0 * q * F2 * K2 * st->Li[2];
+  }
+  force[i] = f;
 }
 
 // ---------------------------------------------------------------- adjoint
@@ -392,53 +913,6 @@ k_spme_adj_kspace(int K0, int K1, int K2, double beta, const R* __restrict__ psi
     }
   }
   block_reduce_finish<2>(v, partials, &st->red_counter[RED_SPME], st->scratch, true);
-}
-
-template <class R>
-__global__ void __launch_bounds__(256)
-k_spme_adj_gather(int N, const typename V4<R>::T* __restrict__ pos, const int* __restrict__ id, int n, int K0,
-                  int K1, int K2, const DevState* __restrict__ st, const R* __restrict__ Phi,
-                  double* __restrict__ dq, double* __restrict__ dr) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= N) return;
-  const typename V4<R>::T p = pos[warp];
-  int b0, b1, b2;
-  R f0, f1, f2;
-  grid_coord<R>(p.x, (R)st->Li[0], K0, b0, f0);
-  grid_coord<R>(p.y, (R)st->Li[1], K1, b1, f1);
-  grid_coord<R>(p.z, (R)st->Li[2], K2, b2, f2);
-  R w0[16], w1[16], w2[16], d0[16], d1[16], d2[16];
-  bspline_w<R>(n, f0, w0, d0);
-  bspline_w<R>(n, f1, w1, d1);
-  bspline_w<R>(n, f2, w2, d2);
-  double pot = 0, gx = 0, gy = 0, gz = 0;
-  for (int ab = lane; ab < n * n; ab += 32) {
-    const int a = ab / n, b = ab % n;
-    const long row = ((long)wrapk(b0 - a, K0) * K1 + wrapk(b1 - b, K1)) * K2;
-    for (int c = 0; c < n; ++c) {
-      const R g = Phi[row + wrapk(b2 - c, K2)];
-      pot += (double)(g * w0[a] * w1[b] * w2[c]);
-      gx += (double)(g * d0[a] * w1[b] * w2[c]);
-      gy += (double)(g * w0[a] * d1[b] * w2[c]);
-      gz += (double)(g * w0[a] * w1[b] * d2[c]);
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    pot += __shfl_xor_sync(0xffffffffu, pot, o);
-    gx += __shfl_xor_sync(0xffffffffu, gx, o);
-    gy += __shfl_xor_sync(0xffffffffu, gy, o);
-    gz += __shfl_xor_sync(0xffffffffu, gz, o);
-  }
-  if (lane == 0) {
-    const double q = (double)p.w;
-    const int o = id[warp];  // results in the caller's atom order
-    if (dq) dq[o] = pot;
-    if (dr) {
-      dr[3 * o] = q * gx * K0 * st->Li[0];
-      dr[3 * o + 1] = q * gy * K1 * st->Li[1];
-      dr[3 * o + 2] = q * gz * K2 * st->Li[2];
-    }
-  }
 }
 
 // ---------------------------------------------------------------- self-force correction
@@ -610,125 +1084,233 @@ __global__ void k_ewald_force(int N, const double4a* __restrict__ pos, const flo
 }
 
 // ---------------------------------------------------------------- host
+template <class R, int LOGN>
+static const void* fftp_fn_n(int mode, int sign, int out4) {
+  if (mode == 0) return (const void*)k_fftp<R, LOGN, 0, -1, 0>;
+  if (mode == 1) return sign < 0 ? (const void*)k_fftp<R, LOGN, 1, -1, 0> : (const void*)k_fftp<R, LOGN, 1, 1, 0>;
+  return out4 ? (const void*)k_fftp<R, LOGN, 2, 1, 1> : (const void*)k_fftp<R, LOGN, 2, 1, 0>;
+}
+
+// line lengths 4 .. 1024
+#define FFT_LOGNS(X) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
+
 template <class R>
-static int fft_launch(md_spme* s, Recorder* rec, const void* in, void* out, int mode, int axis, int sign,
-                      int batch) {
+static const void* fftp_fn(int logn, int mode, int sign, int out4) {
+  switch (logn) {
+#define FFT_CASE(L) case L: return fftp_fn_n<R, L>(mode, sign, out4);
+    FFT_LOGNS(FFT_CASE)
+#undef FFT_CASE
+  }
+  return nullptr;
+}
+
+template <class R>
+static const void* fftx_fn(int logn, int method) {
+  switch (logn) {
+#define FFT_CASE(L) \
+  case L: return method == 0 ? (const void*)k_fft_x_kspace<R, L, 0> : (const void*)k_fft_x_kspace<R, L, 1>;
+    FFT_LOGNS(FFT_CASE)
+#undef FFT_CASE
+  }
+  return nullptr;
+}
+
+template <class R>
+static const void* spread_fn(int order) {
+  switch (order) {
+#define ORDER_CASE(NO) case NO: return (const void*)k_spme_spread_t<R, NO>;
+    SPME_ORDERS(ORDER_CASE)
+#undef ORDER_CASE
+  }
+  return nullptr;
+}
+
+template <class R>
+static const void* gather_fn(int order, int mode) {
+  switch (order) {
+#define ORDER_CASE(NO)                                                                          \
+  case NO:                                                                                      \
+    return mode == 0 ? (const void*)k_spme_gather_t<R, NO, 0>                                   \
+                     : (mode == 1 ? (const void*)k_spme_gather_t<R, NO, 1> : (const void*)k_spme_gather_t<R, NO, 2>);
+    SPME_ORDERS(ORDER_CASE)
+#undef ORDER_CASE
+  }
+  return nullptr;
+}
+
+static int ilog2i(int k) {
+  int l = 0;
+  while ((1 << l) < k) ++l;
+  return l;
+}
+static int fft_lpb(int n) { return FFT_THREADS / (n >= 8 ? n / 8 : 1); }
+
+// one transform pass: mode 0 R2C z, 1 C2C along `axis` (0 x, 1 y), 2 C2R z
+// (out4: the three batches interleaved into Real4)
+template <class R>
+static int fft_launch(md_spme* s, Recorder* rec, const void* in, void* out, int mode, int axis, int sign, int batch,
+                      int out4) {
   const int K0 = s->K[0], K1 = s->K[1], K2 = s->K[2], K2h = s->K2h;
   int n;
-  long nlines, stride = 1, inner = 1, outer = 0, in_as = 0, out_as = 0;
-  if (mode == 0) {
+  long nlines, stride = 1, inner = 1, outer = 0, in_bs = 0, out_bs = 0;
+  if (mode == 0 || mode == 2) {
+    axis = 2;
     n = K2; nlines = (long)K0 * K1;
-  } else if (mode == 2) {
-    n = K2; nlines = (long)K0 * K1;
-    in_as = (long)s->nhalf; out_as = (long)s->nreal;
+    in_bs = (long)s->nhalf; out_bs = (long)s->nreal;
   } else if (axis == 1) {
     n = K1; nlines = (long)K0 * K2h; stride = K2h; inner = K2h; outer = (long)K1 * K2h;
-    in_as = out_as = (long)s->nhalf;
+    in_bs = out_bs = (long)s->nhalf;
   } else {
     n = K0; nlines = (long)K1 * K2h; stride = (long)K1 * K2h; inner = (long)K1 * K2h; outer = 0;
-    in_as = out_as = (long)s->nhalf;
+    in_bs = out_bs = (long)s->nhalf;
   }
-  int lpb = 512 / n;
-  if (lpb < 1) lpb = 1;
-  const int threads = lpb * n / 2 < 32 ? 32 : lpb * n / 2;
-  const size_t smem = sizeof(typename C2<R>::T) * (n / 2 + 2 * (size_t)lpb * n);
-  dim3 grid((unsigned)((nlines + lpb - 1) / lpb), batch);
-  void* a[] = {&in, &out, &mode, &n, &lpb, &nlines, &stride, &inner, &outer, &in_as, &out_as, &sign};
-  return rec_launch(rec, (const void*)k_fft<R>, grid, dim3(threads), smem, a);
+  const int logn = ilog2i(n), lpb = fft_lpb(n);
+  const size_t smem = fftp_smem<R>(logn, out4 ? 3 : 1);
+  dim3 grid((unsigned)((nlines + lpb - 1) / lpb), out4 ? 1 : batch);
+  const void* twg = s->tw[axis];
+  void* a[] = {&in, &out, &twg, &nlines, &stride, &inner, &outer, &in_bs, &out_bs};
+  return rec_launch(rec, fftp_fn<R>(logn, mode, sign, out4), grid, dim3(FFT_THREADS * (out4 ? 3 : 1)), smem, a);
+}
+
+// dynamic shared memory above the default 48 KB needs the opt-in attribute
+static int smem_optin(const void* fn, size_t bytes) {
+  if (bytes > 48 * 1024) MD_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return MD_OK;
 }
 
 template <class R>
-__global__ void k_zero_mesh(size_t n, R* Q) {
-  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (t < n) Q[t] = R(0);
-}
-
-// influence refresh (only when the box changed), spread and the forward
-// transform: C[0] = Q^ on the half spectrum.  Every launch goes through the
-// recorder, so the chain is either run on the stream or recorded into the
-// step graph of the simulation driver.
-template <class R>
-static int spme_forward_mesh(md_spme* s, Recorder* rec) {
+static int spme_prepare(md_spme* s) {
   typedef typename C2<R>::T T2;
-  md_system* sys = s->sys;
-  int K0 = s->K[0], K1 = s->K[1], K2 = s->K[2], n = s->order, N = sys->N;
-  R* Q = (R*)s->Q;
-  T2* C = (T2*)s->C;
+  cudaStream_t str = s->sys->stream;
+  // the real mesh starts cleared; every z pass clears it again after reading
+  MD_CUDA(cudaMemsetAsync(s->Q, 0, sizeof(R) * s->nreal, str));
+  MD_CUDA(cudaMalloc(&s->frec, sizeof(double4a) * s->sys->N));
+  s->max_blocks = ceil_div((long)s->K[1] * s->K2h, fft_lpb(s->K[0]));
+  MD_CUDA(cudaMalloc(&s->partials, sizeof(double) * 4 * s->max_blocks));
+  const int nbm = s->K[0] + s->K[1] + s->K2h;
+  MD_CUDA(cudaMalloc(&s->bm, sizeof(double) * nbm));
+  k_spme_bmod<<<ceil_div(nbm, 256), 256, 0, str>>>(s->K[0], s->K[1], s->K[2], s->order, s->bm);
+  MD_CHECK_LAUNCH("spme bmod");
+  for (int d = 0; d < 3; ++d) {
+    MD_CUDA(cudaMalloc(&s->tw[d], sizeof(T2) * s->K[d]));
+    k_fft_twiddles<R><<<ceil_div(s->K[d], 256), 256, 0, str>>>(s->K[d], (T2*)s->tw[d]);
+    MD_CHECK_LAUNCH("fft twiddles");
+  }
+  const int l0 = ilog2i(s->K[0]), l1 = ilog2i(s->K[1]), l2 = ilog2i(s->K[2]);
+  if (int r = smem_optin(spread_fn<R>(s->order), SPREAD_TILE_BYTES)) return r;
+  if (int r = smem_optin(fftp_fn<R>(l2, 0, -1, 0), fftp_smem<R>(l2, 1))) return r;
+  if (int r = smem_optin(fftp_fn<R>(l2, 2, 1, 0), fftp_smem<R>(l2, 1))) return r;
+  if (int r = smem_optin(fftp_fn<R>(l2, 2, 1, 1), fftp_smem<R>(l2, 3))) return r;
+  for (int sg = -1; sg <= 1; sg += 2) {
+    if (int r = smem_optin(fftp_fn<R>(l1, 1, sg, 0), fftp_smem<R>(l1, 1))) return r;
+    if (int r = smem_optin(fftp_fn<R>(l0, 1, sg, 0), fftp_smem<R>(l0, 1))) return r;
+  }
+  if (int r = smem_optin(fftx_fn<R>(l0, s->method), fftx_smem<R>(l0, s->method))) return r;
+  for (int m = 0; m < 3; ++m)
+    if (int r = smem_optin(gather_fn<R>(s->order, m), GATHER_TILE_BYTES)) return r;
+  return MD_OK;
+}
+
+// stored influence function psi, refreshed only when the box changed
+// (adjoint and md_spme_get_influence; the force chain evaluates psi in its
+// x pass)
+template <class R>
+static int influence_launch(md_spme* s, Recorder* rec) {
+  int K0 = s->K[0], K1 = s->K[1], K2 = s->K[2], n = s->order;
   R* psi = (R*)s->psi;
-  DevState* st = sys->st;
+  DevState* st = s->sys->st;
   double beta = s->beta;
-  size_t nreal = s->nreal;
   {
     void* a[] = {&K0, &K1, &K2, &n, &beta, &st, &psi, &s->d_box_tab};
     if (int r = rec_launch(rec, (const void*)k_spme_influence<R>, dim3((unsigned)((s->nhalf + 255) / 256)),
                            dim3(256), 0, a)) return r;
   }
-  {
-    void* a[] = {&st, &s->d_box_tab};
-    if (int r = rec_launch(rec, (const void*)k_spme_box_tab, dim3(1), dim3(1), 0, a)) return r;
-  }
-  {
-    void* a[] = {&nreal, &Q};
-    if (int r = rec_launch(rec, (const void*)k_zero_mesh<R>, dim3((unsigned)((nreal + 255) / 256)), dim3(256), 0, a))
-      return r;
-  }
-  {
-    const long nt = (long)N * n * n;
-    const void* pos = sys->pos;
-    void* a[] = {&N, &pos, &n, &K0, &K1, &K2, &st, &Q};
-    if (int r = rec_launch(rec, (const void*)k_spme_spread<R>, dim3((unsigned)((nt + 255) / 256)), dim3(256), 0, a))
-      return r;
-  }
-  if (int r = fft_launch<R>(s, rec, Q, C, 0, 2, -1, 1)) return r;
-  if (int r = fft_launch<R>(s, rec, C, C, 1, 1, -1, 1)) return r;
-  if (int r = fft_launch<R>(s, rec, C, C, 1, 0, -1, 1)) return r;
+  void* a[] = {&st, &s->d_box_tab};
+  return rec_launch(rec, (const void*)k_spme_box_tab, dim3(1), dim3(1), 0, a);
+}
+
+// charges onto the (cleared) real mesh
+template <class R>
+static int spread_launch(md_spme* s, Recorder* rec) {
+  md_system* sys = s->sys;
+  int K0 = s->K[0], K1 = s->K[1], K2 = s->K[2], N = sys->N;
+  R* Q = (R*)s->Q;
+  DevState* st = sys->st;
+  const void* pos = sys->pos;
+  int cap = SPREAD_TILE_BYTES / (int)sizeof(R);
+  void* a[] = {&N, &pos, &K0, &K1, &K2, &st, &Q, &cap};
+  return rec_launch(rec, spread_fn<R>(s->order), dim3(ceil_div(N, SPREAD_ATOMS)), dim3(SPREAD_THREADS),
+                    SPREAD_TILE_BYTES, a);
+}
+
+// spread and the forward transform along z (which clears the real mesh for
+// the next spread), y and (with_x) x: C[0] = Q^ on the half spectrum.  Every
+// launch goes through the recorder, so the chain is either run on the stream
+// or recorded into the step graph of the simulation driver.
+template <class R>
+static int spme_forward_mesh(md_spme* s, Recorder* rec, bool with_x) {
+  typedef typename C2<R>::T T2;
+  R* Q = (R*)s->Q;
+  T2* C = (T2*)s->C;
+  if (int r = spread_launch<R>(s, rec)) return r;
+  if (int r = fft_launch<R>(s, rec, Q, C, 0, 2, -1, 1, 0)) return r;
+  if (int r = fft_launch<R>(s, rec, C, C, 1, 1, -1, 1, 0)) return r;
+  if (with_x)
+    if (int r = fft_launch<R>(s, rec, C, C, 1, 0, -1, 1, 0)) return r;
   return MD_OK;
 }
 
 template <class R>
-static int spme_run(md_spme* s, bool with_stats, Recorder* rec) {
+static int gather_launch(md_spme* s, Recorder* rec, int mode, double* dq, double* dr, bool store) {
+  md_system* sys = s->sys;
+  int N = sys->N, K0 = s->K[0], K1 = s->K[1], K2 = s->K[2];
+  const void* pos = sys->pos;
+  const void* G = s->G;
+  DevState* st = sys->st;
+  const size_t el = mode == 0 ? sizeof(typename V4<R>::T) : sizeof(R);
+  int cap = (int)(GATHER_TILE_BYTES / el);
+  double4a* force = store ? s->frec : sys->force;
+  int st_ = store ? 1 : 0;
+  void* a[] = {&N, &pos, &sys->id, &K0, &K1, &K2, &st, &G, &force, &dq, &dr, &cap, &st_};
+  return rec_launch(rec, gather_fn<R>(s->order, mode), dim3(ceil_div(N, GATHER_ATOMS)),
+                    dim3(GATHER_ATOMS * gather_lanes(s->order)), GATHER_TILE_BYTES, a);
+}
+
+template <class R>
+static int spme_run(md_spme* s, bool with_stats, Recorder* rec, bool concurrent) {
   typedef typename C2<R>::T T2;
   md_system* sys = s->sys;
-  int K0 = s->K[0], K1 = s->K[1], K2 = s->K[2], n = s->order, N = sys->N, method = s->method;
+  int K1 = s->K[1], K2 = s->K[2], method = s->method;
   T2* C = (T2*)s->C;
-  R* G = (R*)s->G;
   DevState* st = sys->st;
-  if (int r = spme_forward_mesh<R>(s, rec)) return r;
-  const int nb = (int)((s->nhalf + 255) / 256);
-  if (with_stats && nb > sys->max_partial_blocks) { md_set_error("partials buffer too small for the mesh"); return MD_ERR_BADARG; }
+  if (int r = spme_forward_mesh<R>(s, rec, false)) return r;
+  const int l0 = ilog2i(s->K[0]);
+  const int nb = ceil_div((long)K1 * s->K2h, fft_lpb(s->K[0]));
+  if (with_stats && nb > s->max_blocks) { md_set_error("partials buffer too small for the mesh"); return MD_ERR_BADARG; }
   {
     double beta = s->beta;
-    const R* psi = (const R*)s->psi;
-    size_t nhalf = s->nhalf;
-    int ws = with_stats ? 1 : 0;
-    void* a[] = {&K0, &K1, &K2, &method, &beta, &psi, &C, &nhalf, &st, &sys->partials, &ws};
-    if (int r = rec_launch(rec, (const void*)k_spme_kspace<R>, dim3(nb), dim3(256), 0, a)) return r;
-  }
-  if (with_stats) {
-    void* a[] = {&st};
-    if (int r = rec_launch(rec, (const void*)k_spme_stats_merge, dim3(1), dim3(1), 0, a)) return r;
+    const void* twg = s->tw[0];
+    int ws = with_stats ? 1 : 0, merge = concurrent ? 0 : 1;
+    void* a[] = {&C, &twg, &s->bm, &K1, &K2, &beta, &st, &s->partials, &ws, &merge};
+    if (int r = rec_launch(rec, fftx_fn<R>(l0, method), dim3(nb), dim3(FFT_THREADS * (method == 0 ? 3 : 1)),
+                           fftx_smem<R>(l0, method), a)) return r;
   }
   const int nconv = method == 0 ? 3 : 1;
   T2* Cp = C + s->nhalf;
-  if (int r = fft_launch<R>(s, rec, Cp, Cp, 1, 0, +1, nconv)) return r;
-  if (int r = fft_launch<R>(s, rec, Cp, Cp, 1, 1, +1, nconv)) return r;
-  if (int r = fft_launch<R>(s, rec, Cp, G, 2, 2, +1, nconv)) return r;
-  {
-    const void* pos = sys->pos;
-    size_t nreal = s->nreal;
-    void* a[] = {&N, &pos, &n, &K0, &K1, &K2, &method, &st, &G, &nreal, &sys->force};
-    if (int r = rec_launch(rec, (const void*)k_spme_gather<R>, dim3((unsigned)(((long)N * 32 + 255) / 256)),
-                           dim3(256), 0, a)) return r;
-  }
-  return MD_OK;
+  if (int r = fft_launch<R>(s, rec, Cp, Cp, 1, 1, +1, nconv, 0)) return r;
+  if (int r = fft_launch<R>(s, rec, Cp, s->G, 2, 2, +1, nconv, method == 0 ? 1 : 0)) return r;
+  return gather_launch<R>(s, rec, method, nullptr, nullptr, concurrent);
 }
 
 bool spme_belongs_to(const md_spme* s, const md_system* sys) { return s && s->sys == sys; }
 
 // the chain of one SPME force evaluation, recorded (driver) or launched
-int spme_apply_impl(md_spme* s, bool with_stats, Recorder* rec) {
-  return s->sys->prec == MD_PREC_FP64 ? spme_run<double>(s, with_stats, rec) : spme_run<float>(s, with_stats, rec);
+int spme_apply_impl(md_spme* s, bool with_stats, Recorder* rec, bool concurrent) {
+  return s->sys->prec == MD_PREC_FP64 ? spme_run<double>(s, with_stats, rec, concurrent)
+                                      : spme_run<float>(s, with_stats, rec, concurrent);
 }
+
+const double4a* spme_force_buffer(const md_spme* s) { return s->frec; }
 
 // energy and gradient: recompute the mesh and its transform, influence
 // multiply (energy, dE/dbeta, dE/dpsi), one inverse transform to Phi, gather
@@ -737,9 +1319,8 @@ static int spme_energy_grad(md_spme* s, double* energy, double* dq, double* dr, 
   typedef typename C2<R>::T T2;
   md_system* sys = s->sys;
   cudaStream_t st_ = sys->stream;
-  const int K0 = s->K[0], K1 = s->K[1], K2 = s->K[2], n = s->order;
+  const int K0 = s->K[0], K1 = s->K[1], K2 = s->K[2];
   T2* C = (T2*)s->C;
-  R* G = (R*)s->G;
   const int nb = (int)((s->nhalf + 255) / 256);
   if (nb > sys->max_partial_blocks) { md_set_error("partials buffer too small for the mesh"); return MD_ERR_BADARG; }
   // device outputs: dq [N], dr [N][3], dpsi [nhalf] (FP64, caller's atom order)
@@ -751,18 +1332,17 @@ static int spme_energy_grad(md_spme* s, double* energy, double* dq, double* dr, 
   double* d_p = dpsi ? d + nq + nr : nullptr;
   Recorder rec;
   rec.stream = st_;
-  if (int r = spme_forward_mesh<R>(s, &rec)) return r;
+  if (int r = influence_launch<R>(s, &rec)) return r;
+  if (int r = spme_forward_mesh<R>(s, &rec, true)) return r;
   k_spme_adj_kspace<R><<<nb, 256, 0, st_>>>(K0, K1, K2, s->beta, (const R*)s->psi, C, s->nhalf, sys->st,
                                              sys->partials, d_p);
   MD_CHECK_LAUNCH("spme adjoint kspace");
   if (dq || dr) {
     T2* Cp = C + s->nhalf;
-    if (int r = fft_launch<R>(s, &rec, Cp, Cp, 1, 0, +1, 1)) return r;
-    if (int r = fft_launch<R>(s, &rec, Cp, Cp, 1, 1, +1, 1)) return r;
-    if (int r = fft_launch<R>(s, &rec, Cp, G, 2, 2, +1, 1)) return r;
-    k_spme_adj_gather<R><<<(unsigned)(((long)sys->N * 32 + 255) / 256), 256, 0, st_>>>(
-        sys->N, (const typename V4<R>::T*)sys->pos, sys->id, n, K0, K1, K2, sys->st, G, d_q, d_r);
-    MD_CHECK_LAUNCH("spme adjoint gather");
+    if (int r = fft_launch<R>(s, &rec, Cp, Cp, 1, 0, +1, 1, 0)) return r;
+    if (int r = fft_launch<R>(s, &rec, Cp, Cp, 1, 1, +1, 1, 0)) return r;
+    if (int r = fft_launch<R>(s, &rec, Cp, s->G, 2, 2, +1, 1, 0)) return r;
+    if (int r = gather_launch<R>(s, &rec, 2, d_q, d_r, false)) return r;
   }
   double red[2];
   MD_CUDA(cudaMemcpyAsync(red, sys->st->scratch, sizeof(red), cudaMemcpyDeviceToHost, st_));
@@ -798,9 +1378,10 @@ extern "C" int md_spme_create(md_spme** out, md_system* sys, const int K[3], int
   s->nreal = (size_t)K[0] * K[1] * K[2];
   s->nhalf = (size_t)K[0] * K[1] * s->K2h;
   const size_t rs = sys->real_size();
+  // G: ik Real4 per mesh point (the adjoint's single mesh fits as well)
   bool ok = cudaMalloc(&s->Q, rs * s->nreal) == cudaSuccess &&
             cudaMalloc(&s->C, 2 * rs * s->nhalf * 4) == cudaSuccess &&
-            cudaMalloc(&s->G, rs * s->nreal * 3) == cudaSuccess &&
+            cudaMalloc(&s->G, sys->r4_size() * s->nreal) == cudaSuccess &&
             cudaMalloc(&s->psi, rs * s->nhalf) == cudaSuccess &&
             cudaMalloc(&s->d_box_tab, sizeof(double) * 3) == cudaSuccess &&
             cudaMemset(s->d_box_tab, 0, sizeof(double) * 3) == cudaSuccess;
@@ -809,13 +1390,17 @@ extern "C" int md_spme_create(md_spme** out, md_system* sys, const int K[3], int
     md_spme_destroy(s);
     return MD_ERR_CUDA;
   }
+  if (int r = sys->prec == MD_PREC_FP64 ? spme_prepare<double>(s) : spme_prepare<float>(s)) {
+    md_spme_destroy(s);
+    return r;
+  }
   *out = s;
   return MD_OK;
 }
 
 extern "C" int md_spme_destroy(md_spme* s) {
   if (!s) return MD_OK;
-  void* p[] = {s->Q, s->C, s->G, s->psi, s->d_box_tab};
+  void* p[] = {s->Q, s->C, s->G, s->psi, s->d_box_tab, s->tw[0], s->tw[1], s->tw[2], s->bm, s->frec, s->partials};
   for (void* q : p) if (q) cudaFree(q);
   delete s;
   return MD_OK;
@@ -862,6 +1447,10 @@ extern "C" int md_spme_self_correction(md_spme* s, md_system* sys) {
 extern "C" int md_spme_get_influence(md_spme* s, double* psi) {
   if (!s || !psi) return MD_ERR_BADARG;
   md_system* sys = s->sys;
+  Recorder rec;
+  rec.stream = sys->stream;
+  if (int r = sys->prec == MD_PREC_FP64 ? influence_launch<double>(s, &rec) : influence_launch<float>(s, &rec))
+    return r;
   double* d = nullptr;
   MD_CUDA(cudaMallocAsync((void**)&d, sizeof(double) * s->nhalf, sys->stream));
   const bool f = sys->prec != MD_PREC_FP64;
@@ -879,15 +1468,21 @@ __global__ void k_mesh_out(size_t n, const float* a, const double* b, double* ou
   if (t < n) out[t] = a ? (double)a[t] : b[t];
 }
 
+// the charge mesh of the current positions: spread onto the cleared mesh,
+// copied out, and cleared again for the next force evaluation
 extern "C" int md_spme_get_mesh(md_spme* s, double* Q) {
   if (!s || !Q) return MD_ERR_BADARG;
   md_system* sys = s->sys;
+  Recorder rec;
+  rec.stream = sys->stream;
+  const bool f = sys->prec != MD_PREC_FP64;
+  if (int r = f ? spread_launch<float>(s, &rec) : spread_launch<double>(s, &rec)) return r;
   double* d = nullptr;
   MD_CUDA(cudaMallocAsync((void**)&d, sizeof(double) * s->nreal, sys->stream));
-  const bool f = sys->prec != MD_PREC_FP64;
   k_mesh_out<<<(unsigned)((s->nreal + 255) / 256), 256, 0, sys->stream>>>(
       s->nreal, f ? (const float*)s->Q : nullptr, f ? nullptr : (const double*)s->Q, d);
   MD_CHECK_LAUNCH("mesh out");
+  MD_CUDA(cudaMemsetAsync(s->Q, 0, sys->real_size() * s->nreal, sys->stream));
   MD_CUDA(cudaMemcpyAsync(Q, d, sizeof(double) * s->nreal, cudaMemcpyDeviceToHost, sys->stream));
   MD_CUDA(cudaFreeAsync(d, sys->stream));
   MD_CUDA(cudaStreamSynchronize(sys->stream));

@@ -55,11 +55,14 @@ int rec_launch(Recorder* r, const void* func, dim3 grid, dim3 block, size_t smem
     p.sharedMemBytes = (unsigned)smem;
     p.kernelParams = args;
     p.extra = nullptr;
-    cudaGraphNode_t node;
-    MD_CUDA(cudaGraphAddKernelNode(&node, r->graph, r->has_last ? &r->last : nullptr,
-                                   r->has_last ? 1 : 0, &p));
+    cudaGraphNode_t node, deps[2];
+    size_t nd = 0;
+    if (r->has_last) deps[nd++] = r->last;
+    if (r->join) deps[nd++] = r->join;
+    MD_CUDA(cudaGraphAddKernelNode(&node, r->graph, nd ? deps : nullptr, nd, &p));
     r->last = node;
     r->has_last = true;
+    r->join = nullptr;
     return MD_OK;
   }
   cudaStream_t s = r ? r->stream : nullptr;
