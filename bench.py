@@ -310,8 +310,12 @@ def run_workload(args):
     rc 3.0 + real-space Ewald (beta 0.95, rc 3.0) + ik SPME 64^3 order 6,
     Langevin NVT T 1, dt 0.002.  charged_slab: 1048576 unit charges, liquid
     0.8 for |z - 200| < 64 in 100 x 100 x 400, vapour 0.01, SPME 128 x 128 x
-    512 order 6, beta for a real-space error of 1e-4 at rc 3.0 (uniform LJ
-    cutoff 3.0 in place of the adaptive one)."""
+    512 order 6, beta for a real-space error of 1e-4 at rc 3.0; adaptive
+    per-atom cutoff 3.0..5.0 (AdaptRCut on 2-sigma bins of the density
+    sampled during the relaxation, re-estimated on the reference's schedule).
+    Charged systems also report the a-priori RMS force errors of the real
+    space (errorEstimatePME at rc 3.0) and of the ik-SPME interpolation
+    (errorEstimateInterpolRec) beside the measured mixed-vs-FP64 error."""
     rank, world, local = dist_env()
     import torch
     torch.cuda.set_device(local)
@@ -329,10 +333,16 @@ def run_workload(args):
         s = mdf.systems.charged_slab()
         rc, dt, T, gamma, shift = 3.0, 0.002, 1.0, 1.0, 0.0
         coul = dict(beta=None, K=(128, 128, 512), order=6)
+    adaptive = w == "charged_slab"
+    arc_kw = dict(refh=2.0, rcmin=3.0, rcmax=5.0, rcstep=0.5)
+    lattice = [None]
 
-    def build(prec, pos, vel):
+    def build(prec, pos, vel, attach=True):
         sys_ = mdf.MDSystem(pos, s.box, vel=vel, charge=s.charge, precision=prec)
-        sys_.set_rcut(np.full(s.n, rc, np.float32))
+        if lattice[0] is None:
+            sys_.set_rcut(np.full(s.n, rc, np.float32))
+        else:
+            mdf.AssignRCut(lattice[0]).assign(sys_)
         eng = mdf.InteractionEngine(sys_)
         eng.registNonBondedInteraction(1.0, 1.0, shift)
         sp = None
@@ -343,7 +353,10 @@ def run_workload(args):
             sp = mdf.SPME(sys_, coul["K"], coul["order"], beta, "ik")
         lv = mdf.langevin_params(dt=dt, temperature=T, gamma_t=gamma, seed=1 + rank)
         sim = mdf.Simulation(sys_, eng, skin=SKIN_SPEC, cell_size=rc + SKIN_SPEC, lv=lv, expansion=1.5, spme=sp,
-                             use_graph=args.launch == "graph")
+                             use_graph=args.launch == "graph", max_rcut=arc_kw["rcmax"] if adaptive else 0.0)
+        if adaptive and attach and lattice[0] is not None:
+            arc = mdf.AdaptRCutEstimator(sys_, **arc_kw)
+            sim.attach_adapt_rcut(arc, sample_every=SAMPLE_EVERY, update_every=UPDATE_EVERY, prec=TARGET_PREC)
         return sys_, eng, sim
 
     stream = torch.cuda.Stream()
@@ -351,7 +364,25 @@ def run_workload(args):
     vel = s.vel if s.vel is not None else mdf.systems.maxwell(s.n, T, 11)
     # relaxation of the start (random sequential addition / lattice), not timed
     sys0, _, sim0 = build(0, s.pos, vel)
-    sim0.run(args.equil if args.equil != 4000 else 1000)
+    n_equil = args.equil if args.equil != 4000 else 1000
+    if adaptive:
+        # density sampled over the second half of the relaxation -> cutoff lattice
+        arc0 = mdf.AdaptRCutEstimator(sys0, **arc_kw)
+        done = 0
+        while done < max(n_equil, SAMPLE_EVERY):
+            sim0.run(SAMPLE_EVERY)
+            done += SAMPLE_EVERY
+            if done > n_equil // 2:
+                arc0.deposite()
+        arc0.update(TARGET_PREC)
+        rcl, _, _ = arc0.rcut()
+        lattice[0] = rcl.astype(np.float32)
+        rc_info = (f"adaptive per-bin lattice {arc0.n} from AdaptRCut at target {TARGET_PREC}, rc 3.0..5.0 step "
+                   f"0.5 (2-sigma bins); bins per rc {({float(v): int((rcl == v).sum()) for v in np.unique(rcl)})}")
+        del arc0
+    else:
+        sim0.run(n_equil)
+        rc_info = rc
     pos, vel = sys0.positions(), sys0.velocities()
     del sim0, sys0
     out = {}
@@ -363,9 +394,14 @@ def run_workload(args):
         out[prec] = (args.steps / t, sys_, sim)
     # force RMS error of mixed against FP64 on the relaxed configuration
     F = {}
+    apriori = None
     for prec in (0, 1):
-        sys_, _, sim = build(prec, pos, vel)
+        sys_, _, sim = build(prec, pos, vel, attach=False)
         F[prec] = sys_.forces()
+        if coul is not None and prec == 1:
+            e_dir, _ = mdf.errorEstimatePME(sys_, coul["K"], coul["beta"], rc)
+            e_rec = mdf.errorEstimateInterpolRec(sys_, coul["K"], coul["order"], coul["beta"])
+            apriori = {"real_space_rc3": e_dir, "spme_ik_interpolation": e_rec}
     d = F[0] - F[1]
     err_abs = float(np.sqrt((d ** 2).sum(1).mean()))
     err_rel = float(np.sqrt((d ** 2).sum() / (F[1] ** 2).sum()))
@@ -374,7 +410,7 @@ def run_workload(args):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / out[0][0],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32 pair math / f64 accumulation", "data": "synthetic",
-                "config": {"workload": w, "n_atoms": s.n, "box": s.box.tolist(), "rc": rc, "skin": SKIN_SPEC,
+                "config": {"workload": w, "n_atoms": s.n, "box": s.box.tolist(), "rc": rc_info, "skin": SKIN_SPEC,
                            "dt": dt, "T": T, "ensemble": "Langevin NVT",
                            "electrostatics": None if coul is None else
                            dict(beta=coul["beta"], mesh=list(coul["K"]), order=coul["order"], method="ik"),
@@ -382,6 +418,8 @@ def run_workload(args):
                 "fp64_steps_per_s": out[1][0], "speedup_vs_fp64": out[0][0] / out[1][0],
                 "force_rms_err_vs_fp64": {"abs": err_abs, "rel": err_rel},
                 "tau_per_day": out[0][0] * dt * 86400}
+        if apriori is not None:
+            line["apriori_force_rms_error"] = apriori
         print(json.dumps(line), flush=True)
     return 0
 

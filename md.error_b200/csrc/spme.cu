@@ -708,6 +708,72 @@ constexpr int GATHER_TILE_BYTES = MD_SPME_GATHER_TILE_KB * 1024;
 
 __host__ __device__ constexpr int gather_lanes(int order) { return order <= 4 ? 4 : (order <= 8 ? 8 : 16); }
 
+// one stencil row of order points: point c at G[-c] (the staged region) or
+// at G[kz[c]] (the mesh, wrapped indices)
+template <class R, int NO, int MODE, class GT, class A>
+__device__ __forceinline__ void gather_row(const GT* G, R wa, R da, R w1b, R d1b, const R (&w2)[NO],
+                                           const R (&d2)[NO], A& s0, A& s1, A& s2, A& s3) {
+  const R wab = wa * w1b;
+  if constexpr (MODE == 0) {
+#pragma unroll
+    for (int c = 0; c < NO; ++c) {
+      const GT g = G[-c];
+      const R w = wab * w2[c];
+      s0 += g.x * w;
+      s1 += g.y * w;
+      s2 += g.z * w;
+    }
+  } else {
+    const R dab = da * w1b, wdb = wa * d1b;
+#pragma unroll
+    for (int c = 0; c < NO; ++c) {
+      const R g = G[-c];
+      if (MODE == 1) {
+        s0 -= g * dab * w2[c];
+        s1 -= g * wdb * w2[c];
+        s2 -= g * wab * d2[c];
+      } else {
+        s0 += (double)(g * wab * w2[c]);
+        s1 += (double)(g * dab * w2[c]);
+        s2 += (double)(g * wdb * w2[c]);
+        s3 += (double)(g * wab * d2[c]);
+      }
+    }
+  }
+}
+
+template <class R, int NO, int MODE, class GT, class A>
+__device__ __forceinline__ void gather_row_idx(const GT* G, const int (&kz)[NO], R wa, R da, R w1b, R d1b,
+                                               const R (&w2)[NO], const R (&d2)[NO], A& s0, A& s1, A& s2, A& s3) {
+  const R wab = wa * w1b;
+  if constexpr (MODE == 0) {
+#pragma unroll
+    for (int c = 0; c < NO; ++c) {
+      const GT g = G[kz[c]];
+      const R w = wab * w2[c];
+      s0 += g.x * w;
+      s1 += g.y * w;
+      s2 += g.z * w;
+    }
+  } else {
+    const R dab = da * w1b, wdb = wa * d1b;
+#pragma unroll
+    for (int c = 0; c < NO; ++c) {
+      const R g = G[kz[c]];
+      if (MODE == 1) {
+        s0 -= g * dab * w2[c];
+        s1 -= g * wdb * w2[c];
+        s2 -= g * wab * d2[c];
+      } else {
+        s0 += (double)(g * wab * w2[c]);
+        s1 += (double)(g * dab * w2[c]);
+        s2 += (double)(g * wdb * w2[c]);
+        s3 += (double)(g * wab * d2[c]);
+      }
+    }
+  }
+}
+
 template <class R, int NO, int MODE>
 __global__ void __launch_bounds__(GATHER_ATOMS * gather_lanes(NO))
 k_spme_gather_t(int N, const typename V4<R>::T* __restrict__ pos, const int* __restrict__ id, int K0, int K1,
@@ -773,68 +839,44 @@ k_spme_gather_t(int N, const typename V4<R>::T* __restrict__ pos, const int* __r
   const GT* Gm = reinterpret_cast<const GT*>(Gv);
   if (staged) {
     // one mesh row (e2 points along z) per warp pass, lanes along z
+    // row (xx, y) = warp + k * (NT / 32), stepped without divisions
     const int nrow = (int)(e0 * e1), ie1 = (int)e1, ie2 = (int)e2, ips = (int)ps;
-    for (int row = threadIdx.x >> 5; row < nrow; row += NT >> 5) {
-      const int y = row % ie1, xx = row / ie1;
+    constexpr int NWARP = NT >> 5;
+    const int w0 = threadIdx.x >> 5;
+    int y = w0 % ie1, xx = w0 / ie1;
+    for (int row = w0; row < nrow; row += NWARP) {
       const size_t g = ((size_t)((o0 + xx) & (K0 - 1)) * K1 + ((o1 + y) & (K1 - 1))) * K2;
       GT* t = tile + xx * ips + y * ie2;
       for (int z = threadIdx.x & 31; z < ie2; z += 32) t[z] = Gm[g + ((o2 + z) & (K2 - 1))];
+      y += NWARP;
+      while (y >= ie1) { y -= ie1; ++xx; }
     }
     __syncthreads();
   }
-  // each stencil row (order points along z) is summed in the working
-  // precision, the rows in FP64
-  double F0 = 0.0, F1 = 0.0, F2 = 0.0, F3 = 0.0;
+  // the lane's order^2 points are summed in the working precision (FP64 for
+  // the adjoint), the lanes in FP64
+  typedef typename std::conditional<MODE == 2, double, R>::type A;
+  A s0 = A(0), s1 = A(0), s2 = A(0), s3 = A(0);
   if (live && a < NO) {
-    int kz[NO];
-    size_t xrow;
     if (staged) {
+      // row b of plane a starts at tp - b e2; point c of the row at -c
+      const int ie2 = (int)e2;
+      const GT* tp = tile + (bb[0] - a - o0) * (int)ps + (bb[1] - o1) * ie2 + (bb[2] - o2);
 #pragma unroll
-      for (int c = 0; c < NO; ++c) kz[c] = bb[2] - c - o2;
-      xrow = (size_t)(bb[0] - a - o0) * ps;
+      for (int b = 0; b < NO; ++b)
+        gather_row<R, NO, MODE>(tp - b * ie2, wa, da, w1[b], d1[b], w2, d2, s0, s1, s2, s3);
     } else {
+      int kz[NO];
 #pragma unroll
       for (int c = 0; c < NO; ++c) kz[c] = (bb[2] - c) & (K2 - 1);
-      xrow = (size_t)((bb[0] - a) & (K0 - 1)) * K1;
-    }
+      const size_t xrow = (size_t)((bb[0] - a) & (K0 - 1)) * K1;
 #pragma unroll
-    for (int b = 0; b < NO; ++b) {
-      const GT* G = staged ? tile + xrow + (bb[1] - b - o1) * e2
-                           : Gm + (xrow + ((bb[1] - b) & (K1 - 1))) * K2;
-      const R wab = wa * w1[b];
-      R s0 = R(0), s1 = R(0), s2 = R(0), s3 = R(0);
-      if constexpr (MODE == 0) {
-#pragma unroll
-        for (int c = 0; c < NO; ++c) {
-          const R4 g = G[kz[c]];
-          const R w = wab * w2[c];
-          s0 += g.x * w;
-          s1 += g.y * w;
-          s2 += g.z * w;
-        }
-      } else {
-        const R dab = da * w1[b], wdb = wa * d1[b];
-#pragma unroll
-        for (int c = 0; c < NO; ++c) {
-          const R g = G[kz[c]];
-          if (MODE == 1) {
-            s0 -= g * dab * w2[c];
-            s1 -= g * wdb * w2[c];
-            s2 -= g * wab * d2[c];
-          } else {
-            s0 += g * wab * w2[c];
-            s1 += g * dab * w2[c];
-            s2 += g * wdb * w2[c];
-            s3 += g * wab * d2[c];
-          }
-        }
-      }
-      F0 += (double)s0;
-      F1 += (double)s1;
-      F2 += (double)s2;
-      if (MODE == 2) F3 += (double)s3;
+      for (int b = 0; b < NO; ++b)
+        gather_row_idx<R, NO, MODE>(Gm + (xrow + ((bb[1] - b) & (K1 - 1))) * K2, kz, wa, da, w1[b], d1[b], w2, d2,
+                                    s0, s1, s2, s3);
     }
   }
+  double F0 = s0, F1 = s1, F2 = s2, F3 = s3;
 #pragma unroll
   for (int o = LPA / 2; o > 0; o >>= 1) {
     F0 += __shfl_xor_sync(0xffffffffu, F0, o);
