@@ -33,6 +33,25 @@ struct LJParams {
 #ifndef MD_LJ_ACC
 #define MD_LJ_ACC 1
 #endif
+//   MD_LJ_LISTLD    list loads: 0 read-only path, 1 streaming (ld.cs),
+//                   2 no L1 allocation, so L1 keeps the position gathers
+//                   (each list line is read once per step)
+#ifndef MD_LJ_LISTLD
+#define MD_LJ_LISTLD 2
+#endif
+
+__device__ __forceinline__ int4 load_list4(const int4* p) {
+#if MD_LJ_LISTLD == 1
+  return __ldcs(p);
+#elif MD_LJ_LISTLD == 2
+  int4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+  return v;
+#else
+  return __ldg(p);
+#endif
+}
 
 struct Kahan {
 #if MD_LJ_ACC == 1
@@ -161,14 +180,14 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
     const int npass = (n + 31) >> 5;
     if (npass > 0) {
 #if MD_LJ_PREFETCH
-      int4 cur = __ldg(row4 + lane);
+      int4 cur = load_list4(row4 + lane);
 #endif
       for (int q = 0; q < npass; ++q) {
 #if MD_LJ_PREFETCH
         int4 nxt = cur;
-        if (q + 1 < npass) nxt = __ldg(row4 + (q + 1) * G + lane);
+        if (q + 1 < npass) nxt = load_list4(row4 + (q + 1) * G + lane);
 #else
-        const int4 cur = __ldg(row4 + q * G + lane);
+        const int4 cur = load_list4(row4 + q * G + lane);
 #endif
         const int rem = n - (32 * q + lane);  // entry u is inside the row when 8u < rem
         if (rem > 24) lj_pass_mixed<4, false, STATS, COUL>(cur, rem, pos, i, pi, rc2, shift, p, a);
