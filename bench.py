@@ -298,7 +298,7 @@ def cpu_baseline(s, lattice, nsteps):
     return (nsteps / el), orc.num_threads(), out
 
 
-WORKLOADS = ("lj_slab", "lj_fluid", "charged_fluid", "charged_slab")
+WORKLOADS = ("lj_slab", "lj_fluid", "charged_fluid", "charged_slab", "lj_slab_lfc")
 
 
 def run_workload(args):
@@ -313,6 +313,11 @@ def run_workload(args):
     512 order 6, beta for a real-space error of 1e-4 at rc 3.0; adaptive
     per-atom cutoff 3.0..5.0 (AdaptRCut on 2-sigma bins of the density
     sampled during the relaxation, re-estimated on the reference's schedule).
+    lj_slab_lfc: the 65536-atom slab at a uniform cutoff 3.5 with the
+    long-range force correction (ForceCorr on 1-sigma bins: field from the
+    density sampled during the relaxation, then assigned every 40 steps,
+    sampled every 40 and re-estimated every 2000, the fcorr app's schedule),
+    Langevin NVT T 0.85, dt 0.005.
     Charged systems also report the a-priori RMS force errors of the real
     space (errorEstimatePME at rc 3.0) and of the ik-SPME interpolation
     (errorEstimateInterpolRec) beside the measured mixed-vs-FP64 error."""
@@ -321,10 +326,14 @@ def run_workload(args):
     torch.cuda.set_device(local)
     import mdforce as mdf
     w = args.workload
+    lfc = w == "lj_slab_lfc"
     if w == "lj_fluid":
         s = mdf.systems.lj_fluid_fcc()
         rc, dt, T, gamma, coul = 2.5, 0.005, 1.0, 0.1, None
         shift = -4.0 * (rc ** -12 - rc ** -6)
+    elif lfc:
+        s = build_slab(mdf)
+        rc, dt, T, gamma, shift, coul = 3.5, DT, TEMP, 1.0, 0.0, None
     elif w == "charged_fluid":
         s = mdf.systems.charged_fluid()
         rc, dt, T, gamma, shift = 3.0, 0.002, 1.0, 1.0, 0.0
@@ -336,6 +345,8 @@ def run_workload(args):
     adaptive = w == "charged_slab"
     arc_kw = dict(refh=2.0, rcmin=3.0, rcmax=5.0, rcstep=0.5)
     lattice = [None]
+    lfc_profile = [None]
+    keep = []
 
     def build(prec, pos, vel, attach=True):
         sys_ = mdf.MDSystem(pos, s.box, vel=vel, charge=s.charge, precision=prec)
@@ -357,6 +368,16 @@ def run_workload(args):
         if adaptive and attach and lattice[0] is not None:
             arc = mdf.AdaptRCutEstimator(sys_, **arc_kw)
             sim.attach_adapt_rcut(arc, sample_every=SAMPLE_EVERY, update_every=UPDATE_EVERY, prec=TARGET_PREC)
+        if lfc and lfc_profile[0] is not None:
+            fc = mdf.ForceCorr(sys_, rc, refh=1.0)
+            fc.set_profile(lfc_profile[0])
+            fc.update()
+            fc.assign()
+            if attach:
+                sim.attach_force_corr(fc, assign_every=40, sample_every=SAMPLE_EVERY, update_every=UPDATE_EVERY)
+            else:
+                eng.setForceCorrection(fc)
+            keep.append(fc)
         return sys_, eng, sim
 
     stream = torch.cuda.Stream()
@@ -380,6 +401,18 @@ def run_workload(args):
         rc_info = (f"adaptive per-bin lattice {arc0.n} from AdaptRCut at target {TARGET_PREC}, rc 3.0..5.0 step "
                    f"0.5 (2-sigma bins); bins per rc {({float(v): int((rcl == v).sum()) for v in np.unique(rcl)})}")
         del arc0
+    elif lfc:
+        fc0 = mdf.ForceCorr(sys0, rc, refh=1.0)
+        done = 0
+        while done < max(n_equil, SAMPLE_EVERY):
+            sim0.run(SAMPLE_EVERY)
+            done += SAMPLE_EVERY
+            if done > n_equil // 2:
+                fc0.deposite()
+        fc0.update()
+        lfc_profile[0] = fc0.profile()
+        rc_info = f"uniform {rc} with the long-range force correction (bins {fc0.n})"
+        del fc0
     else:
         sim0.run(n_equil)
         rc_info = rc

@@ -415,6 +415,42 @@ int md_arc_pressure_correction(md_adapt_rcut* arc, md_system* sys, double out[3]
 int md_sim_attach_adapt_rcut(md_sim* sim, md_adapt_rcut* arc, int sample_every, int update_every,
                              double prec, int nrefine);
 
+/* ------------------------------------------------- long-range force correction
+ * LFC of the fcorr simulation tools (FCR = shortRange.inhomo/template/tools/simulation.fcorr):
+ * ForceCorr::reinit(rc, dp) (FCR/src/ForceCorr.cu:112-148, makeS2k :193-262) on the density
+ * bins of DensityProfile_PiecewiseConst(box, refh) (odd counts); calError (:150-179) turns
+ * the averaged profile into a per-bin correction force field, FFT-convolved in FP64 on the
+ * device; AssignForceCorr::getForceCorr / zero / assign (FCR/src/AssignForceCorr.cu:55-178)
+ * give every atom the field value of its bin, which the non-bonded kernel adds to the
+ * atom's force (FCR/src/InteractionEngine_interface.cu:1118) once the correction is set on
+ * the engine.  The field starts at zero (the app's afc.zero()). */
+typedef struct md_fcorr md_fcorr;
+int md_fcorr_create(md_fcorr** out, md_system* sys, double rc, double refh);
+int md_fcorr_destroy(md_fcorr* fc);
+int md_fcorr_get_dims(md_fcorr* fc, int n[3]);
+/* DensityProfile_PiecewiseConst::deposite / clearData, or an explicit profile [nx][ny][nz] */
+int md_fcorr_deposit(md_fcorr* fc, md_system* sys);
+int md_fcorr_clear_profile(md_fcorr* fc);
+int md_fcorr_set_profile(md_fcorr* fc, const double* rho);
+/* the profile of the last update (or the one set) */
+int md_fcorr_get_profile(md_fcorr* fc, double* rho);
+/* DensityProfile::calculate + ForceCorr::calError + AssignForceCorr::getForceCorr */
+int md_fcorr_update(md_fcorr* fc);
+/* AssignForceCorr::zero: the per-bin field set to zero */
+int md_fcorr_zero(md_fcorr* fc);
+/* the field error2r{x,y,z}: real parts re[3][nele], imaginary parts im[3][nele] */
+int md_fcorr_get_field(md_fcorr* fc, double* re, double* im);
+/* AssignForceCorr::assign: each atom's value from the current field; and the
+   per-atom values [N][3] in the caller's atom order */
+int md_fcorr_assign(md_fcorr* fc, md_system* sys);
+int md_fcorr_get_values(md_fcorr* fc, double* values);
+/* the non-bonded kernel adds the per-atom values to the forces (NULL: none) */
+int md_engine_set_force_correction(md_engine* eng, md_fcorr* fc);
+/* the driver on the fcorr app's schedule (FCR/app/lj.nhc-xtc.cu:172-227): after step i,
+   assign when i % assign_every == 0; deposit when (i+1) % sample_every == 0; update
+   and clear the samples when (i+1) % update_every == 0.  Also sets it on the engine. */
+int md_sim_attach_force_corr(md_sim* sim, md_fcorr* fc, int assign_every, int sample_every, int update_every);
+
 /* ------------------------------------------------------------ synthetic inputs
  * Seeded generators of the benchmark systems (host only, no GPU needed).  The
  * reference builds inputs with gen.conf* tools

@@ -491,29 +491,37 @@ extern "C" int md_arc_get_profile(md_adapt_rcut* a, double* rho) {
   return MD_OK;
 }
 
-extern "C" int md_arc_update(md_adapt_rcut* a, double prec, int nrefine) {
-  if (!a || !(prec > 0) || nrefine < 0) { md_set_error("md_arc_update: bad arguments"); return MD_ERR_BADARG; }
-  md_system* sys = a->sys;
-  DevState hs;
-  if (int r = sys->read_state(hs)) return r;
+// Kernel tables for the current box (rebuilt when the box changed),
+// DensityProfile::calculate (counts / (dv * ndata), or the explicit profile)
+// and the forward transform of the profile into rhok.
+static int arc_profile_transform(md_adapt_rcut* a, DevState& hs, const char* who) {
+  if (int r = a->sys->read_state(hs)) return r;
   bool box_changed = false;
   for (int d = 0; d < 3; ++d) box_changed |= fabs(hs.L[d] - a->box_tab[d]) > 1e-9 * a->box_tab[d];
   if (box_changed)
     if (int r = build_tables(a)) return r;
   const long ne = a->nele;
   const int nb = (int)((ne + 255) / 256);
-  // DensityProfile::calculate: counts / (dv * ndata), or the explicit profile
   if (a->ndata > 0) {
     double dv = (hs.L[0] / a->n[0]) * (hs.L[1] / a->n[1]) * (hs.L[2] / a->n[2]);
     k_arc_profile<<<nb, 256, 0, a->sys->stream>>>(ne, a->counts, 1.0 / (dv * a->ndata), a->rho, a->rhok);
   } else if (a->ndata < 0) {
     k_arc_profile<<<nb, 256, 0, a->sys->stream>>>(ne, nullptr, 0.0, a->rho, a->rhok);
   } else {
-    md_set_error("md_arc_update: no density samples deposited");
+    md_set_error("%s: no density samples deposited", who);
     return MD_ERR_BADARG;
   }
   MD_CHECK_LAUNCH("arc profile");
-  if (int r = dft3(a, a->rhok, -1, 1)) return r;
+  return dft3(a, a->rhok, -1, 1);
+}
+
+extern "C" int md_arc_update(md_adapt_rcut* a, double prec, int nrefine) {
+  if (!a || !(prec > 0) || nrefine < 0) { md_set_error("md_arc_update: bad arguments"); return MD_ERR_BADARG; }
+  md_system* sys = a->sys;
+  DevState hs;
+  if (int r = arc_profile_transform(a, hs, "md_arc_update")) return r;
+  const long ne = a->nele;
+  const int nb = (int)((ne + 255) / 256);
   const double V = hs.L[0] * hs.L[1] * hs.L[2];
   k_arc_multiply<<<nb, 256, 0, a->sys->stream>>>(ne, a->nrc, a->rhok, V / ne, a->s1k, a->s2k, a->work);
   MD_CHECK_LAUNCH("arc multiply");
@@ -594,5 +602,189 @@ extern "C" int md_arc_pressure_correction(md_adapt_rcut* a, md_system* sys, doub
     MD_CUDA(cudaMemcpyAsync(out, a->pcorr, sizeof(double) * 3, cudaMemcpyDeviceToHost, a->sys->stream));
     MD_CUDA(cudaStreamSynchronize(a->sys->stream));
   }
+  return MD_OK;
+}
+
+// ------------------------------------------------------------ LFC
+// Long-range force correction (FCR = shortRange.inhomo/template/tools/
+// simulation.fcorr):
+//   ForceCorr::makeS2k        FCR/src/ForceCorr.cu:193-262: the AdaptRCut
+//                             kernel i k_d T(k) of the single cutoff rc (the
+//                             x^-5 quadrature over [rc, 30] and the boundary
+//                             term), so the tables of an md_adapt_rcut with
+//                             rcmin = rcmax = rc are reused
+//   ForceCorr::calError       FCR/src/ForceCorr.cu:150-179:
+//                             field_d = IFFT(s2k_d FFT(rho) V / nele) / V
+//   AssignForceCorr::getForceCorr / zero / assign
+//                             FCR/src/AssignForceCorr.cu:55-178: the per-bin
+//                             field (working precision) and, at assign, each
+//                             atom's value at its bin (binary32 binning)
+//   InteractionEngine (LFC)   FCR/src/InteractionEngine_interface.cu:1118:
+//                             the force kernel adds the atom's value
+// The per-atom values are stored by original atom id, so the cell sort
+// never has to carry them.
+struct md_fcorr {
+  md_adapt_rcut* arc = nullptr;  // bins, density samples and the kernel table
+  double* field = nullptr;       // [3][nele] real parts, [3][nele] imaginary parts
+  double4a* corr = nullptr;      // per-atom value by atom id
+  int N = 0;
+};
+
+__global__ void k_fc_multiply(long nele, const double2* rhok, double scale, const double* s2k, double2* work) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= nele) return;
+  const double2 r = make_double2(rhok[i].x * scale, rhok[i].y * scale);
+  for (int d = 0; d < 3; ++d) {
+    const double b = s2k[(long)d * nele + i];  // one cutoff: s2k[d][0][i]
+    work[(long)d * nele + i] = make_double2(-r.y * b, r.x * b);
+  }
+}
+
+__global__ void k_fc_extract(long nele, const double2* work, double Vi, double* field) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= nele) return;
+  for (int d = 0; d < 3; ++d) {
+    const double2 w = work[(long)d * nele + i];
+    field[(long)d * nele + i] = w.x * Vi;
+    field[(long)(3 + d) * nele + i] = w.y * Vi;
+  }
+}
+
+// AssignForceCorr::assign: bin of the (wrapped) binary32 coordinate,
+// ix = int((x nx) / Lx); the value in the working precision R
+template <class R>
+__global__ void k_fc_assign(int N, const typename V4<R>::T* __restrict__ pos, const int* __restrict__ id,
+                            const DevState* st, int nx, int ny, int nz, const double* __restrict__ field,
+                            long nele, double4a* __restrict__ corr) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  const typename V4<R>::T p = pos[k];
+  float x = (float)p.x, y = (float)p.y, z = (float)p.z;
+  const float Lx = st->Lf[0], Ly = st->Lf[1], Lz = st->Lf[2];
+  if (x < 0) x = __fadd_rn(x, Lx); else if (x >= Lx) x = __fsub_rn(x, Lx);
+  if (y < 0) y = __fadd_rn(y, Ly); else if (y >= Ly) y = __fsub_rn(y, Ly);
+  if (z < 0) z = __fadd_rn(z, Lz); else if (z >= Lz) z = __fsub_rn(z, Lz);
+  int ix = __float2int_rz(__fdiv_rn(__fmul_rn(x, (float)nx), Lx));
+  int iy = __float2int_rz(__fdiv_rn(__fmul_rn(y, (float)ny), Ly));
+  int iz = __float2int_rz(__fdiv_rn(__fmul_rn(z, (float)nz), Lz));
+  ix = min(max(ix, 0), nx - 1); iy = min(max(iy, 0), ny - 1); iz = min(max(iz, 0), nz - 1);
+  const long b = iz + (long)nz * (iy + (long)ny * ix);
+  corr[id[k]] = double4a{(double)(R)field[b], (double)(R)field[nele + b], (double)(R)field[2 * nele + b], 0.0};
+}
+
+const double4a* fcorr_values(const md_fcorr* f) { return f ? f->corr : nullptr; }
+
+extern "C" int md_fcorr_create(md_fcorr** out, md_system* sys, double rc, double refh) {
+  if (!out || !sys || !(rc > 0) || !(rc < 30.0) || !(refh > 0)) {
+    md_set_error("md_fcorr_create: bad arguments (0 < rc < 30, refh > 0)");
+    return MD_ERR_BADARG;
+  }
+  md_fcorr* f = new md_fcorr();
+  f->N = sys->N;
+  if (int r = md_arc_create(&f->arc, sys, refh, rc, rc, 1.0)) { delete f; return r; }
+  const long ne = f->arc->nele;
+  bool ok = cudaMalloc(&f->field, sizeof(double) * 6 * ne) == cudaSuccess &&
+            cudaMalloc(&f->corr, sizeof(double4a) * sys->N) == cudaSuccess &&
+            cudaMemsetAsync(f->field, 0, sizeof(double) * 6 * ne, sys->stream) == cudaSuccess &&
+            cudaMemsetAsync(f->corr, 0, sizeof(double4a) * sys->N, sys->stream) == cudaSuccess;
+  if (!ok) {
+    md_cuda_fail(cudaGetLastError(), "md_fcorr_create");
+    md_fcorr_destroy(f);
+    return MD_ERR_CUDA;
+  }
+  *out = f;
+  return MD_OK;
+}
+
+extern "C" int md_fcorr_destroy(md_fcorr* f) {
+  if (!f) return MD_OK;
+  md_arc_destroy(f->arc);
+  if (f->field) cudaFree(f->field);
+  if (f->corr) cudaFree(f->corr);
+  delete f;
+  return MD_OK;
+}
+
+extern "C" int md_fcorr_get_dims(md_fcorr* f, int n[3]) {
+  if (!f || !n) return MD_ERR_BADARG;
+  return md_arc_get_dims(f->arc, n, nullptr);
+}
+
+extern "C" int md_fcorr_deposit(md_fcorr* f, md_system* sys) {
+  if (!f || !sys || sys->N != f->N) return MD_ERR_BADARG;
+  return md_arc_deposit(f->arc, sys);
+}
+
+extern "C" int md_fcorr_clear_profile(md_fcorr* f) {
+  if (!f) return MD_ERR_BADARG;
+  return md_arc_clear_profile(f->arc);
+}
+
+extern "C" int md_fcorr_set_profile(md_fcorr* f, const double* rho) {
+  if (!f || !rho) return MD_ERR_BADARG;
+  return md_arc_set_profile(f->arc, rho);
+}
+
+extern "C" int md_fcorr_get_profile(md_fcorr* f, double* rho) {
+  if (!f || !rho) return MD_ERR_BADARG;
+  return md_arc_get_profile(f->arc, rho);
+}
+
+extern "C" int md_fcorr_update(md_fcorr* f) {
+  if (!f) return MD_ERR_BADARG;
+  md_adapt_rcut* a = f->arc;
+  DevState hs;
+  if (int r = arc_profile_transform(a, hs, "md_fcorr_update")) return r;
+  const long ne = a->nele;
+  const int nb = (int)((ne + 255) / 256);
+  const double V = hs.L[0] * hs.L[1] * hs.L[2];
+  k_fc_multiply<<<nb, 256, 0, a->sys->stream>>>(ne, a->rhok, V / ne, a->s2k, a->work);
+  MD_CHECK_LAUNCH("fcorr multiply");
+  if (int r = dft3(a, a->work, +1, 3)) return r;
+  k_fc_extract<<<nb, 256, 0, a->sys->stream>>>(ne, a->work, 1.0 / V, f->field);
+  MD_CHECK_LAUNCH("fcorr extract");
+  return MD_OK;
+}
+
+extern "C" int md_fcorr_zero(md_fcorr* f) {
+  if (!f) return MD_ERR_BADARG;
+  MD_CUDA(cudaMemsetAsync(f->field, 0, sizeof(double) * 6 * f->arc->nele, f->arc->sys->stream));
+  return MD_OK;
+}
+
+extern "C" int md_fcorr_get_field(md_fcorr* f, double* re, double* im) {
+  if (!f) return MD_ERR_BADARG;
+  const long ne = f->arc->nele;
+  cudaStream_t s = f->arc->sys->stream;
+  if (re) MD_CUDA(cudaMemcpyAsync(re, f->field, sizeof(double) * 3 * ne, cudaMemcpyDeviceToHost, s));
+  if (im) MD_CUDA(cudaMemcpyAsync(im, f->field + 3 * ne, sizeof(double) * 3 * ne, cudaMemcpyDeviceToHost, s));
+  MD_CUDA(cudaStreamSynchronize(s));
+  DevState hs;
+  if (int r = f->arc->sys->read_state(hs)) return r;
+  if (hs.flags & FLAG_QUADRATURE) { md_set_error("adaptive quadrature reached its depth bound"); return MD_ERR_BADARG; }
+  return MD_OK;
+}
+
+extern "C" int md_fcorr_assign(md_fcorr* f, md_system* sys) {
+  if (!f || !sys || sys->N != f->N) { md_set_error("md_fcorr_assign: bad arguments"); return MD_ERR_BADARG; }
+  md_adapt_rcut* a = f->arc;
+  const int nb = ceil_div(sys->N, 256);
+  if (sys->prec == MD_PREC_FP64)
+    k_fc_assign<double><<<nb, 256, 0, sys->stream>>>(sys->N, (const double4a*)sys->pos, sys->id, sys->st, a->n[0],
+                                                       a->n[1], a->n[2], f->field, a->nele, f->corr);
+  else
+    k_fc_assign<float><<<nb, 256, 0, sys->stream>>>(sys->N, (const float4*)sys->pos, sys->id, sys->st, a->n[0],
+                                                      a->n[1], a->n[2], f->field, a->nele, f->corr);
+  MD_CHECK_LAUNCH("fcorr assign");
+  return MD_OK;
+}
+
+extern "C" int md_fcorr_get_values(md_fcorr* f, double* v) {
+  if (!f || !v) return MD_ERR_BADARG;
+  std::vector<double4a> h(f->N);
+  cudaStream_t s = f->arc->sys->stream;
+  MD_CUDA(cudaMemcpyAsync(h.data(), f->corr, sizeof(double4a) * f->N, cudaMemcpyDeviceToHost, s));
+  MD_CUDA(cudaStreamSynchronize(s));
+  for (int i = 0; i < f->N; ++i) { v[3 * i] = h[i].x; v[3 * i + 1] = h[i].y; v[3 * i + 2] = h[i].z; }
   return MD_OK;
 }

@@ -77,6 +77,14 @@ __device__ __forceinline__ double group_sum(double v) {
   return v;
 }
 
+// long-range force correction of the atom (LFC: forcx[ii] += fsumx + fcx[ii],
+// FCR/src/InteractionEngine_interface.cu:1118), added to the FP64 sum
+__device__ __forceinline__ void add_correction(double4a& f, const double4a& c) {
+  f.x += c.x;
+  f.y += c.y;
+  f.z += c.z;
+}
+
 // ---------------------------------------------------------------- mixed
 struct MixedAcc {
   Kahan fx, fy, fz;
@@ -149,7 +157,8 @@ __global__ void __launch_bounds__(256, COUL ? 4 : 5)
 k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut,
            const int* __restrict__ list, const int* __restrict__ nnb, int cap,
            const DevState* __restrict__ st, LJParams p, double4a* __restrict__ force, int overwrite,
-           double* partials, unsigned* counter, double* stats) {
+           double* partials, unsigned* counter, double* stats, const double4a* __restrict__ corr,
+           const int* __restrict__ id) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = t / G;
   const int lane = t & (G - 1);
@@ -204,6 +213,7 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
   if (i < N && lane == 0) {
     double4a f = overwrite ? double4a{0, 0, 0, 0} : force[i];
     f.x += Fx; f.y += Fy; f.z += Fz;
+    if (corr) add_correction(f, corr[id[i]]);
     force[i] = f;
   }
   if (STATS) {
@@ -220,7 +230,8 @@ __global__ void __launch_bounds__(256)
 k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcut,
           const int* __restrict__ list, const int* __restrict__ nnb, int cap,
           const DevState* __restrict__ st, LJParams p, double4a* __restrict__ force, int overwrite,
-          double* partials, unsigned* counter, double* stats) {
+          double* partials, unsigned* counter, double* stats, const double4a* __restrict__ corr,
+          const int* __restrict__ id) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = t / G;
   const int lane = t & (G - 1);
@@ -288,6 +299,7 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
   if (i < N && lane == 0) {
     double4a f = overwrite ? double4a{0, 0, 0, 0} : force[i];
     f.x += Fx; f.y += Fy; f.z += Fz;
+    if (corr) add_correction(f, corr[id[i]]);
     force[i] = f;
   }
   if (STATS) {
@@ -329,8 +341,9 @@ int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats,
   DevState* st = sys->st;
   unsigned* counter = &st->red_counter[RED_LJ];
   double* stats = &st->stats[MD_STAT_NB_ENERGY];
+  const double4a* corr = fcorr_values(eng->fcorr);
   void* a[] = {&N, &sys->pos, &sys->rcut, &nl->list, &nl->nnb, &cap, &st, &p, &sys->force, &ow,
-               &sys->partials, &counter, &stats};
+               &sys->partials, &counter, &stats, &corr, &sys->id};
   const void* f;
   if (sys->prec == MD_PREC_FP64) {
     if (coul) f = with_stats ? (const void*)k_lj_fp64<kLanes, true, true> : (const void*)k_lj_fp64<kLanes, false, true>;
@@ -371,6 +384,12 @@ extern "C" int md_engine_register_lj(md_engine* e, double eps, double sigma, dou
   e->eps = eps;
   e->sigma = sigma;
   e->shift = shift;
+  return MD_OK;
+}
+
+extern "C" int md_engine_set_force_correction(md_engine* e, md_fcorr* fc) {
+  if (!e) return MD_ERR_BADARG;
+  e->fcorr = fc;
   return MD_OK;
 }
 

@@ -161,7 +161,10 @@ struct md_engine {
   bool has_coul = false;
   double beta = 0;
   int n_bonds = 0;
+  md_fcorr* fcorr = nullptr;  // long-range force correction added by the non-bonded kernel
 };
+// per-atom correction values (by atom id) of an md_fcorr
+const double4a* fcorr_values(const md_fcorr* f);
 
 // launch helper: direct launch or kernel-node recording ---------------------
 struct Recorder {

@@ -40,6 +40,9 @@ struct md_sim {
   int64_t steps = 0;
   md_nhc* nhc = nullptr;  // MD_INTEG_NHC
   bool nhc_settled = false;  // velocities / chain brought to the end of the last step
+  // long-range force correction schedule
+  md_fcorr* fcorr = nullptr;
+  int fc_assign_every = 0, fc_sample_every = 0, fc_update_every = 0;
   // adaptive cutoff schedule
   md_adapt_rcut* arc = nullptr;
   int sample_every = 0, update_every = 0, nrefine = 0;
@@ -203,6 +206,23 @@ extern "C" int md_sim_create(md_sim** out, md_system* sys, md_engine* eng, const
   return MD_OK;
 }
 
+extern "C" int md_sim_attach_force_corr(md_sim* s, md_fcorr* fc, int assign_every, int sample_every,
+                                        int update_every) {
+  if (!s || !fc || assign_every < 1 || sample_every < 1 || update_every < 1) {
+    md_set_error("md_sim_attach_force_corr: bad arguments");
+    return MD_ERR_BADARG;
+  }
+  s->fcorr = fc;
+  s->fc_assign_every = assign_every;
+  s->fc_sample_every = sample_every;
+  s->fc_update_every = update_every;
+  if (int r = md_engine_set_force_correction(s->eng, fc)) return r;
+  // the recorded non-bonded kernel must see the correction values
+  if (s->exec)
+    if (int r = build_graph(s)) return r;
+  return MD_OK;
+}
+
 extern "C" int md_sim_attach_adapt_rcut(md_sim* s, md_adapt_rcut* arc, int sample_every, int update_every,
                                         double prec, int nrefine) {
   if (!s || !arc || sample_every < 1 || update_every < 1 || !(prec > 0) || nrefine < 0) {
@@ -236,6 +256,19 @@ extern "C" int md_sim_run(md_sim* s, int nsteps) {
       Recorder rec;
       rec.stream = sys->stream;
       if (int r = record_step(s, &rec, false)) return r;
+    }
+    if (s->fcorr) {
+      // FCR/app/lj.nhc-xtc.cu:172-227, step i = s->steps: assign after the
+      // force of step i, then the samples and the update after step i + 1
+      const int64_t i0 = s->steps;
+      if (i0 % s->fc_assign_every == 0)
+        if (int r = md_fcorr_assign(s->fcorr, sys)) return r;
+      if ((i0 + 1) % s->fc_sample_every == 0)
+        if (int r = md_fcorr_deposit(s->fcorr, sys)) return r;
+      if ((i0 + 1) % s->fc_update_every == 0) {
+        if (int r = md_fcorr_update(s->fcorr)) return r;
+        if (int r = md_fcorr_clear_profile(s->fcorr)) return r;
+      }
     }
     s->steps += 1;
     if (s->arc) {

@@ -157,6 +157,20 @@ _SIGS = {
     "md_ikerr_evaluate_device": (i32, [vp, i32, vp, vp, vp, vp]),
     "md_ikerr_get_hats": (i32, [vp, i32, P(f64), P(f64)]),
     "md_ikerr_get_weights": (i32, [vp, i32, P(f64)]),
+    "md_fcorr_create": (i32, [P(vp), vp, f64, f64]),
+    "md_fcorr_destroy": (i32, [vp]),
+    "md_fcorr_get_dims": (i32, [vp, P(i32)]),
+    "md_fcorr_deposit": (i32, [vp, vp]),
+    "md_fcorr_clear_profile": (i32, [vp]),
+    "md_fcorr_set_profile": (i32, [vp, P(f64)]),
+    "md_fcorr_get_profile": (i32, [vp, P(f64)]),
+    "md_fcorr_update": (i32, [vp]),
+    "md_fcorr_zero": (i32, [vp]),
+    "md_fcorr_get_field": (i32, [vp, P(f64), P(f64)]),
+    "md_fcorr_assign": (i32, [vp, vp]),
+    "md_fcorr_get_values": (i32, [vp, P(f64)]),
+    "md_engine_set_force_correction": (i32, [vp, vp]),
+    "md_sim_attach_force_corr": (i32, [vp, vp, i32, i32, i32]),
 }
 
 

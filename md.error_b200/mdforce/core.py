@@ -300,6 +300,11 @@ class InteractionEngine:
     def registNonBondedInteraction(self, epsilon=1.0, sigma=1.0, shift=0.0):
         check(lib.md_engine_register_lj(self.h, epsilon, sigma, shift), "registNonBondedInteraction")
 
+    def setForceCorrection(self, fc):
+        """the non-bonded kernel adds the per-atom LFC values (None: off)"""
+        check(lib.md_engine_set_force_correction(self.h, fc.h if fc is not None else None), "setForceCorrection")
+        self.fcorr = fc
+
     def registBondedInteraction(self, n_bonds=0):
         check(lib.md_engine_register_bonded(self.h, int(n_bonds)), "registBondedInteraction")
 
@@ -579,6 +584,68 @@ class AdaptRCutEstimator:
         return out
 
 
+class ForceCorr:
+    """Long-range LJ force correction (LFC) of the fcorr tools: ForceCorr
+    (FCR/src/ForceCorr.cu) on a DensityProfile_PiecewiseConst(box, refh) and
+    AssignForceCorr (FCR/src/AssignForceCorr.cu), on the GPU.  reinit(rc, dp) is
+    the constructor; update() is dp.calculate + calError + getForceCorr; assign()
+    gives every atom its bin's value, which the engine adds to the forces once
+    set with InteractionEngine.setForceCorrection."""
+
+    def __init__(self, sys, rc, refh=1.0):
+        h = C.c_void_p()
+        check(lib.md_fcorr_create(C.byref(h), sys.h, float(rc), float(refh)), "ForceCorr")
+        self.h = h
+        self.sys = sys
+        self.rc = float(rc)
+        n = (C.c_int * 3)()
+        check(lib.md_fcorr_get_dims(h, n), "dims")
+        self.n = tuple(n)
+        self.nele = self.n[0] * self.n[1] * self.n[2]
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.md_fcorr_destroy(self.h)
+            self.h = None
+
+    def deposite(self, sys=None):
+        check(lib.md_fcorr_deposit(self.h, (sys or self.sys).h), "deposite")
+
+    def clearData(self):
+        check(lib.md_fcorr_clear_profile(self.h), "clearData")
+
+    def set_profile(self, rho):
+        a = _f64(rho).reshape(self.n)
+        check(lib.md_fcorr_set_profile(self.h, _p(a)), "set_profile")
+
+    def profile(self):
+        a = np.empty(self.n, np.float64)
+        check(lib.md_fcorr_get_profile(self.h, _p(a)), "profile")
+        return a
+
+    def update(self):
+        check(lib.md_fcorr_update(self.h), "ForceCorr::calError")
+
+    def zero(self):
+        check(lib.md_fcorr_zero(self.h), "AssignForceCorr::zero")
+
+    def field(self):
+        """(re, im): error2r{x,y,z} on the bins, each (3, nx, ny, nz)"""
+        re = np.empty((3,) + self.n)
+        im = np.empty((3,) + self.n)
+        check(lib.md_fcorr_get_field(self.h, _p(re), _p(im)), "field")
+        return re, im
+
+    def assign(self, sys=None):
+        check(lib.md_fcorr_assign(self.h, (sys or self.sys).h), "AssignForceCorr::assign")
+
+    def values(self):
+        """per-atom correction [N][3], original atom order"""
+        v = np.empty((self.sys.n, 3))
+        check(lib.md_fcorr_get_values(self.h, _p(v)), "values")
+        return v
+
+
 class NoseHoover_Chains2:
     """NoseHoover_Chains2 (ENG/include/Thermostat.h:77-120): reinit(sys, refT, tauT),
     operator_L(dt, sys), HamiltonianContribution(); step1/step2 give the
@@ -704,6 +771,13 @@ class Simulation:
         out = np.zeros(5)
         check(lib.md_sim_get_nhc_state(self.h, _p(out)), "nhc_state")
         return out
+
+    def attach_force_corr(self, fc, assign_every=40, sample_every=40, update_every=2000):
+        """assignForceCorrFeq / densityProfileSamplingFeq / updateForceCorrFeq of the
+        fcorr app (FCR/app/lj.nhc-xtc.cu:50-51, 172-227); sets it on the engine."""
+        check(lib.md_sim_attach_force_corr(self.h, fc.h, int(assign_every), int(sample_every), int(update_every)),
+              "attach_force_corr")
+        self.fcorr = fc
 
     def attach_adapt_rcut(self, arc, sample_every=40, update_every=2000, prec=0.02, nrefine=0):
         """rcutAssignFeq / densityProfileSamplingFeq / rcutUpdateFeq of lj.nhc-xtc.cu."""

@@ -363,6 +363,40 @@ def adapt_rcut(box, n, rc, rho, prec, nrefine=0, with_pc=True):
     return out
 
 
+def fcorr_field(box, n, rc, rho):
+    """ForceCorr::makeS2k + calError (FCR/src/ForceCorr.cu:150-262): the s2k kernel
+    is AdaptRCut's for the single cutoff rc; field_d = IFFT(s2k_d FFT(rho) V/nele)/V.
+    Returns the complex field (3, nx, ny, nz)."""
+    n = tuple(int(v) for v in n)
+    V = float(np.prod(box))
+    nele = int(np.prod(n))
+    _, s2 = arc_kernels(box, n, [rc])
+    rk = dft3d(np.asarray(rho, np.float64).reshape(n).astype(np.complex128), -1) * (V / nele)
+    out = np.empty((3,) + n, np.complex128)
+    for d in range(3):
+        out[d] = dft3d(rk * (1j * s2[d, 0]), +1) / V
+    return out
+
+
+def fcorr_assign(pos, box, n, field_re, prec_f32=True):
+    """AssignForceCorr::assign (FCR/src/AssignForceCorr.cu:131-163): wrap the
+    binary32 coordinate once, bin ix = int((x nx) / Lx) in binary32, take the
+    bin's value (rounded to binary32 for the mixed path)."""
+    p = np.asarray(pos, np.float32)
+    L = np.asarray(box, np.float32)
+    nn = np.asarray(n, np.int64)
+    idx = []
+    for d in range(3):
+        x = p[:, d].copy()
+        x = np.where(x < 0, (x + L[d]).astype(np.float32), np.where(x >= L[d], (x - L[d]).astype(np.float32), x))
+        q = ((x * np.float32(nn[d])).astype(np.float32) / L[d]).astype(np.float32)
+        i = np.clip(np.trunc(q).astype(np.int64), 0, nn[d] - 1)
+        idx.append(i)
+    b = idx[2] + nn[2] * (idx[1] + nn[1] * idx[0])
+    v = np.stack([field_re[d].reshape(-1)[b] for d in range(3)], 1)
+    return v.astype(np.float32).astype(np.float64) if prec_f32 else v
+
+
 # ---------------------------------------------------------------- reference (compiled from its sources)
 REF_DIR = os.path.join(HERE, "_ref")
 
@@ -385,6 +419,19 @@ def ref_adapt_rcut(box, n, rcmin, rcmax, rcstep, rho, prec, nrefine=0):
     lib.ref_arc_run(_p(b, f64), _p(nn, i32), rcmin, rcmax, rcstep, _p(r, f64), prec, nrefine, _p(err, f64),
                     _p(rcut, f64), _p(idx, i32), _p(rerr, f64), _p(pc, f64))
     return dict(error=err, rcut=rcut, index=idx, result_error=rerr, pcorr=pc)
+
+
+def ref_fcorr(box, n, rc, rho):
+    """The reference's own ForceCorr (oracle/_ref/libref_fcorr.so): reinit(rc, dp) +
+    calError(dp); the complex field error2r{x,y,z} (3, nx, ny, nz)."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libref_fcorr.so"))
+    lib.ref_fcorr_run.argtypes = [P(f64), P(i32), f64, P(f64), P(f64), P(f64)]
+    b = np.ascontiguousarray(box, np.float64)
+    nn = np.ascontiguousarray(n, np.int32)
+    r = np.ascontiguousarray(rho, np.float64).reshape(tuple(n))
+    re = np.zeros((3,) + tuple(n)); im = np.zeros((3,) + tuple(n))
+    lib.ref_fcorr_run(_p(b, f64), _p(nn, i32), float(rc), _p(r, f64), _p(re, f64), _p(im, f64))
+    return re + 1j * im
 
 
 def ref_spme(pos, q, box, beta, K, rcut, method, order):

@@ -152,3 +152,26 @@ extern "C" int ref_arc_run(const double* box, const int* nbin, double rcmin, dou
   return 0;
 }
 #endif
+
+#ifdef REF_FCORR
+#include "ForceCorr.h"
+
+// ForceCorr::reinit(rc, dp) + calError(dp) on a given profile: the complex
+// field error2r{x,y,z}, real parts re[3][nele], imaginary parts im[3][nele]
+extern "C" int ref_fcorr_run(const double* box, const int* nbin, double rc, const double* profile, double* re,
+                             double* im) {
+  DensityProfile_PiecewiseConst dp;
+  dp.set(box, nbin, profile);
+  ForceCorr fc;
+  fc.reinit(rc, dp);
+  fc.calError(dp);
+  const int nele = nbin[0] * nbin[1] * nbin[2];
+  const fftw_complex* f[3] = {fc.getForceCorrX(), fc.getForceCorrY(), fc.getForceCorrZ()};
+  for (int d = 0; d < 3; ++d)
+    for (int i = 0; i < nele; ++i) {
+      re[(size_t)d * nele + i] = f[d][i][0];
+      im[(size_t)d * nele + i] = f[d][i][1];
+    }
+  return 0;
+}
+#endif
