@@ -270,6 +270,14 @@ int md_errmap_get_profile(md_errmap* h, double* rho1, double* rho2);
 /* error1, error2 [K0][K1][K2][2] (real, imaginary) for charge magnitude `charge`; the
    RMS force error at a grid point is sqrt(error1[..][0] + error2[..][0]) (print_error) */
 int md_errmap_compute(md_errmap* h, double charge, double* error1, double* error2);
+/* Real-space map of the same form (ErrorEstimate_dir::reinit / calError,
+ * analyze/src/ErrorEstimate_dir.cpp:70-331, driven by analyze/app/error.dir.cpp): kernels
+ * s2k (vector) and s1k (scalar) of the erfc force beyond rcut, from the analyze tools'
+ * adaptive Gauss-4 quadrature (tolerance 1e-20).  The quadrature needs erfc(beta rcut)
+ * small; when it does not converge the call fails with MD_ERR_BADARG.  The handle takes
+ * md_errmap_set_profile / deposit / compute like the ik map. */
+int md_errmap_create_dir(md_errmap** out, const int K[3], const double L[3], double beta, double rcut,
+                         int device);
 
 /* ------------------------------------------------------- per-atom cutoff
  * Replaces AssignRCut::getRCut + assign (ENG/src/AssignRCut.cu:46-117):

@@ -1,4 +1,4 @@
-// Inhomogeneous ik-SPME error estimate on the mesh, FP64 on the GPU.
+// Inhomogeneous ik-SPME and real-space error estimates on a grid, FP64 on the GPU.
 // Reference: ErrorEstimate_SPME_Ik::reinit / calKernel / calError
 // (longRange.hetero/profile.test/template/tools/analyze/src/ErrorEstimate_SPME_Ik.cpp:80-470),
 // driven by analyze/app/error.spme.ik.cpp:82-85 with the density profile of
@@ -191,6 +191,117 @@ __global__ void k_em_profile(long N, const double* cnt1, const double* cnt2, dou
   rho2[t] = cnt2[t] * inv;
 }
 
+// ---- real-space map (ErrorEstimate_dir, analyze/src/ErrorEstimate_dir.cpp:124-331)
+// Integrands: 0: r f(r)^2 sin(2 pi k r), 1: r^2 f(r)^2, 2: -2 erfc(beta r) sin(2 pi k r),
+// f(r) = (2 beta/sqrt(pi) e^{-beta^2 r^2} + erfc(beta r)/r) / r.
+__device__ double dir_f(int kind, double k, double beta, double r) {
+  if (kind == 2) return -2. * erfc(beta * r) * sin(2. * M_PI * k * r);
+  const double betar = beta * r, ri = 1. / r;
+  const double fr = (2. * beta / sqrt(M_PI) * exp(-betar * betar) + erfc(betar) * ri) * ri;
+  if (kind == 0) return r * fr * fr * sin(2. * M_PI * k * r);
+  return r * r * fr * fr;
+}
+
+// Gauss-4 box of the analyze tools' Integral1D (src/Integral1D.cpp:60-85)
+__device__ double dir_coarse(int kind, double k, double beta, double xlo, double xup) {
+  const double hx = xup - xlo;
+  const double v0 = sqrt((3 - 2 * sqrt(1.2)) / 7.), v1 = sqrt((3 + 2 * sqrt(1.2)) / 7.);
+  const double x0 = 0.5 * (xup - xlo) * (-v1) + 0.5 * (xup + xlo);
+  const double x1 = 0.5 * (xup - xlo) * (-v0) + 0.5 * (xup + xlo);
+  const double x2 = 0.5 * (xup - xlo) * (+v0) + 0.5 * (xup + xlo);
+  const double x3 = 0.5 * (xup - xlo) * (+v1) + 0.5 * (xup + xlo);
+  const double w0 = (18 + sqrt(30.)) / 36., w1 = (18 - sqrt(30.)) / 36.;
+  return 0.5 * hx * (w1 * (dir_f(kind, k, beta, x0) + dir_f(kind, k, beta, x3)) +
+                     w0 * (dir_f(kind, k, beta, x1) + dir_f(kind, k, beta, x2)));
+}
+
+// Integral1D::cal_int(Gauss4, f, xlo, xup, tol, init_nx): init_nx boxes of
+// tol/init_nx; a box is bisected while |coarse - (left + right)| >= 255 tol
+// (children tol/2) and while its width is at least 1e-13 of the initial box.
+// Depth first with an explicit stack; a stack deeper than DIR_MAXD or more
+// than DIR_BUDGET boxes (the reference would not finish either) sets the
+// quadrature flag and keeps the best value so far.
+constexpr int DIR_MAXD = 56;
+constexpr long DIR_BUDGET = 1L << 20;
+
+__device__ double dir_int(int kind, double k, double beta, double xlo, double xup, double tol, int init_nx,
+                          unsigned* flag) {
+  double sa[DIR_MAXD], sb[DIR_MAXD], st[DIR_MAXD], sc[DIR_MAXD];
+  const double hx = (xup - xlo) / (double)init_nx, nxi = 1. / (double)init_nx;
+  double total = 0.0;
+  long boxes = 0;
+  for (int i = 0; i < init_nx; i++) {
+    const double x = xlo + i * hx;
+    int top = 1;
+    sa[0] = x; sb[0] = x + hx; st[0] = tol * nxi; sc[0] = dir_coarse(kind, k, beta, x, x + hx);
+    double part = 0.0;
+    while (top > 0) {
+      --top;
+      const double a = sa[top], b = sb[top], t = st[top], coarse = sc[top];
+      const double hh = 0.5 * (b - a);
+      const double c0 = dir_coarse(kind, k, beta, a, a + hh), c1 = dir_coarse(kind, k, beta, a + hh, b);
+      const double v = c0 + c1;
+      ++boxes;
+      if (fabs(coarse - v) < t * 255 || hh * 2 < 1e-13 * hx) { part += v; continue; }
+      if (top + 2 > DIR_MAXD || boxes > DIR_BUDGET) { atomicOr(flag, 1u); part += v; continue; }
+      sa[top] = a + hh; sb[top] = b; st[top] = t * 0.5; sc[top] = c1; ++top;  // right, popped later
+      sa[top] = a; sb[top] = a + hh; st[top] = t * 0.5; sc[top] = c0; ++top;  // left first
+    }
+    total += part;
+  }
+  return total;
+}
+
+// one thread per octant point (ax, ay, az) >= 0; every sign image inside
+// [-K/2, K - K/2) gets the values (the tables are exactly even in |k| and
+// odd in k_d, so the images agree with a per-point evaluation)
+__global__ void k_em_dir_tables(EmGrid g, double beta, double rcut, double2* k1, double2* k2a, unsigned* flag) {
+  const int hx = g.K[0] / 2 + 1, hy = g.K[1] / 2 + 1, hz = g.K[2] / 2 + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= hx * hy * hz) return;
+  const int az = t % hz, ay = (t / hz) % hy, ax = t / (hz * hy);
+  const double* L = g.L;
+  // makeS1k (|k| from the integer indices)
+  const double k1m = sqrt(ax * ax / (L[0] * L[0]) + ay * ay / (L[1] * L[1]) + az * az / (L[2] * L[2]));
+  double s1;
+  if (k1m != 0) s1 = 2. / k1m * dir_int(0, k1m, beta, rcut, 30, 1e-20, 10, flag);
+  else s1 = 4. * M_PI * dir_int(1, k1m, beta, rcut, 30, 1e-20, 10, flag);
+  // makeS2k (|k| from the wave vector)
+  const double kx0 = ax / L[0], ky0 = ay / L[1], kz0 = az / L[2];
+  const double k = sqrt(kx0 * kx0 + ky0 * ky0 + kz0 * kz0);
+  double an = 0.0, size = 0.0;
+  if (k != 0) {
+    an = dir_int(2, k, beta, rcut, 30, 1e-20, 10, flag) / k;
+    const double e = 2. * M_PI * k * rcut;
+    size = 2. * M_PI * rcut * erfc(beta * rcut) * (2. * cos(e) / e - 2. * sin(e) / (e * e));
+    size /= k;
+  }
+  for (int sx = 0; sx < 2; ++sx) {
+    const int ix = sx ? -ax : ax;
+    if ((sx && ax == 0) || ix < -(g.K[0] / 2) || ix >= g.K[0] - g.K[0] / 2) continue;
+    for (int sy = 0; sy < 2; ++sy) {
+      const int iy = sy ? -ay : ay;
+      if ((sy && ay == 0) || iy < -(g.K[1] / 2) || iy >= g.K[1] - g.K[1] / 2) continue;
+      for (int sz = 0; sz < 2; ++sz) {
+        const int iz = sz ? -az : az;
+        if ((sz && az == 0) || iz < -(g.K[2] / 2) || iz >= g.K[2] - g.K[2] / 2) continue;
+        const int lx = ix < 0 ? ix + g.K[0] : ix, ly = iy < 0 ? iy + g.K[1] : iy, lz = iz < 0 ? iz + g.K[2] : iz;
+        const long p = lz + (long)g.K[2] * (ly + (long)g.K[1] * lx);
+        k2a[p] = make_double2(s1, 0.0);
+        const double kk[3] = {ix / L[0], iy / L[1], iz / L[2]};
+        for (int d = 0; d < 3; ++d) {
+          double v = 0.0;
+          if (k != 0) {
+            v = 2 * M_PI * kk[d] * an;
+            v += size * kk[d];
+          }
+          k1[d * g.N + p] = make_double2(0.0, v);
+        }
+      }
+    }
+  }
+}
+
 }  // namespace
 
 struct md_errmap {
@@ -285,6 +396,72 @@ extern "C" int md_errmap_create(md_errmap** out, const int K[3], const double L[
   gm = nullptr;
   k2b = nullptr;
   if (e != cudaSuccess) return fail(md_cuda_fail(e, "md_errmap_create kernel"));
+  *out = h;
+  return MD_OK;
+}
+
+// ErrorEstimate_dir::reinit (analyze/src/ErrorEstimate_dir.cpp:70-122): the
+// same object as the ik map with k1 = s2k and k2a = s1k, so set_profile,
+// deposit and compute (calError) are shared
+extern "C" int md_errmap_create_dir(md_errmap** out, const int K[3], const double L[3], double beta, double rcut,
+                                    int device) {
+  if (!out || !K || !L || !(beta > 0) || !(rcut > 0) || !(rcut < 30.0)) {
+    md_set_error("md_errmap_create_dir: bad arguments (beta > 0, 0 < rcut < 30)");
+    return MD_ERR_BADARG;
+  }
+  for (int d = 0; d < 3; ++d)
+    if (K[d] < 2 || K[d] > 1024 || !(L[d] > 0)) {
+      md_set_error("md_errmap_create_dir: grid %d or box %g out of range on axis %d", K[d], L[d], d);
+      return MD_ERR_BADARG;
+    }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    md_set_error("md_errmap_create_dir: no CUDA device %d", device);
+    return MD_ERR_CUDA;
+  }
+  MD_CUDA(cudaSetDevice(device));
+  md_errmap* h = new md_errmap();
+  h->device = device;
+  h->beta = beta;
+  h->order = 0;
+  for (int d = 0; d < 3; ++d) { h->g.K[d] = K[d]; h->g.L[d] = L[d]; }
+  h->g.N = (long)K[0] * K[1] * K[2];
+  const long N = h->g.N;
+  unsigned* flag = nullptr;
+  bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaMalloc(&h->k1, sizeof(double2) * 3 * N) == cudaSuccess &&
+            cudaMalloc(&h->k2a, sizeof(double2) * N) == cudaSuccess &&
+            cudaMalloc(&h->work, sizeof(double2) * 4 * N) == cudaSuccess &&
+            cudaMalloc(&h->work2, sizeof(double2) * 2 * N) == cudaSuccess &&
+            cudaMalloc(&h->rho, sizeof(double) * 2 * N) == cudaSuccess &&
+            cudaMalloc(&h->cnt, sizeof(double) * 2 * N) == cudaSuccess &&
+            cudaMalloc(&flag, sizeof(unsigned)) == cudaSuccess;
+  auto fail = [&](int code) {
+    if (flag) cudaFree(flag);
+    em_free(h);
+    delete h;
+    return code;
+  };
+  if (!ok) return fail(md_cuda_fail(cudaGetLastError(), "md_errmap_create_dir allocation"));
+  cudaStream_t s = h->stream;
+  MD_CUDA(cudaMemsetAsync(h->cnt, 0, sizeof(double) * 2 * N, s));
+  MD_CUDA(cudaMemsetAsync(h->rho, 0, sizeof(double) * 2 * N, s));
+  MD_CUDA(cudaMemsetAsync(flag, 0, sizeof(unsigned), s));
+  const int oct = (K[0] / 2 + 1) * (K[1] / 2 + 1) * (K[2] / 2 + 1);
+  k_em_dir_tables<<<ceil_div(oct, 64), 64, 0, s>>>(h->g, beta, rcut, h->k1, h->k2a, flag);
+  unsigned hf = 0;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hf, flag, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail(md_cuda_fail(e, "md_errmap_create_dir kernel"));
+  if (hf) {
+    md_set_error("md_errmap_create_dir: the adaptive quadrature did not converge (erfc(beta rcut) too large "
+                 "for the reference's tolerance)");
+    return fail(MD_ERR_BADARG);
+  }
+  cudaFree(flag);
+  flag = nullptr;
   *out = h;
   return MD_OK;
 }

@@ -146,6 +146,7 @@ _SIGS = {
     "md_nhc_npt_get_state": (i32, [vp, P(f64)]),
     "md_errmap_create": (i32, [P(vp), P(i32), P(f64), f64, i32, i32]),
     "md_errmap_destroy": (i32, [vp]),
+    "md_errmap_create_dir": (i32, [P(vp), P(i32), P(f64), f64, f64, i32]),
     "md_errmap_set_profile": (i32, [vp, P(f64), P(f64)]),
     "md_errmap_deposit": (i32, [vp, vp]),
     "md_errmap_get_profile": (i32, [vp, P(f64), P(f64)]),

@@ -457,6 +457,20 @@ class ErrorEstimate_SPME_Ik:
         return np.sqrt(e1[..., 0] + e2[..., 0])
 
 
+class ErrorEstimate_dir(ErrorEstimate_SPME_Ik):
+    """ErrorEstimate_dir (analyze tools): reinit(beta, rcut, dp) builds the
+    real-space kernels on the grid K of box L; calError / rms as for the ik map."""
+
+    def __init__(self, K, L, beta, rcut, device=0):
+        h = C.c_void_p()
+        KK = (C.c_int * 3)(*[int(k) for k in K])
+        LL = (C.c_double * 3)(*[float(x) for x in L])
+        check(lib.md_errmap_create_dir(C.byref(h), KK, LL, float(beta), float(rcut), int(device)),
+              "ErrorEstimate_dir")
+        self.h = h
+        self.K = tuple(int(k) for k in K)
+
+
 def choose_beta(sys, rcut, target):
     b = C.c_double()
     check(lib.md_choose_beta(sys.h, float(rcut), float(target), C.byref(b)), "choose_beta")

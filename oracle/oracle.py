@@ -481,6 +481,33 @@ def spme_ik_errmap(K, box, beta, order, rho1, rho2, charge=1.0):
     return e1.reshape(tuple(K) + (2,)), e2.reshape(tuple(K) + (2,))
 
 
+def dir_errmap(K, box, beta, rcut, rho1, rho2, charge=1.0):
+    """ErrorEstimate_dir::reinit + calError restated (oracle_errmap.c): error1, error2 as
+    (K0, K1, K2, 2) arrays (real, imaginary)."""
+    KK = np.ascontiguousarray(K, np.int32)
+    b = np.ascontiguousarray(box, np.float64)
+    r1 = np.ascontiguousarray(rho1, np.float64).reshape(tuple(K))
+    r2 = np.ascontiguousarray(rho2, np.float64).reshape(tuple(K))
+    e1 = np.zeros(tuple(K) + (2,)); e2 = np.zeros(tuple(K) + (2,))
+    _lib.orc_dir_errmap(_p(KK, i32), _p(b, f64), float(beta), float(rcut), _p(r1, f64), _p(r2, f64),
+                        float(charge), _p(e1, f64), _p(e2, f64))
+    return e1, e2
+
+
+def ref_dir_errmap(K, box, beta, rcut, rho1, rho2, charge=1.0):
+    """The reference's own ErrorEstimate_dir (oracle/_ref/libref_errdir.so)."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libref_errdir.so"))
+    lib.ref_dir_errmap.argtypes = [P(i32), P(f64), f64, f64, P(f64), P(f64), f64, P(f64), P(f64)]
+    KK = np.ascontiguousarray(K, np.int32)
+    b = np.ascontiguousarray(box, np.float64)
+    r1 = np.ascontiguousarray(rho1, np.float64).reshape(tuple(K))
+    r2 = np.ascontiguousarray(rho2, np.float64).reshape(tuple(K))
+    e1 = np.zeros(tuple(K) + (2,)); e2 = np.zeros(tuple(K) + (2,))
+    lib.ref_dir_errmap(_p(KK, i32), _p(b, f64), float(beta), float(rcut), _p(r1, f64), _p(r2, f64),
+                       float(charge), _p(e1, f64), _p(e2, f64))
+    return e1, e2
+
+
 def ref_spme_ik_errmap(K, box, beta, order, rho1, rho2, charge=1.0):
     """The reference's own ErrorEstimate_SPME_Ik (oracle/_ref/libref_errmap.so)."""
     lib = C.CDLL(os.path.join(REF_DIR, "libref_errmap.so"))
@@ -529,6 +556,7 @@ _sigs3 = {
     "orc_ewald_self": (f64, [i32, P(f64), f64]),
     "orc_spme_selfcorr": (None, [i32, P(f64), P(f64), P(f64), P(i32), i32, f64, P(f64)]),
     "orc_spme_ik_errmap": (None, [P(i32), P(f64), f64, i32, P(f64), P(f64), f64, P(f64), P(f64)]),
+    "orc_dir_errmap": (None, [P(i32), P(f64), f64, f64, P(f64), P(f64), f64, P(f64), P(f64)]),
     "orc_dft3d": (None, [P(i32), P(f64), i32]),
 }
 for _n, (_r, _a) in _sigs3.items():

@@ -36,6 +36,47 @@ static double alias(double u, int n) {
 
 static int cidx(int i, int K) { return i > (K >> 1) ? i - K : i; }
 
+/* calError of both maps: e1_d = IFFT(k1_d FFT(rho1 V/N)) q/V, e2 = IFFT(k2a FFT(rho2 V/N)) q^2/V
+ * (real parts scaled), error1 = sum_d e1_d^2 with real and imaginary parts apart; k1 [3][N]
+ * and k2a [N] complex, interleaved */
+static void errmap_apply(const int K[3], const double box[3], const double* k1, const double* k2a,
+                         const double* rho1, const double* rho2, double charge, double* e1, double* e2) {
+  const long N = (long)K[0] * K[1] * K[2];
+  const double V = box[0] * box[1] * box[2];
+  double* r1 = (double*)calloc(2 * N, sizeof(double));
+  double* r2 = (double*)calloc(2 * N, sizeof(double));
+  for (long i = 0; i < N; ++i) {
+    r1[2 * i] = rho1[i] * V / (double)N;
+    r2[2 * i] = rho2[i] * V / (double)N;
+  }
+  orc_dft3d(K, r1, -1);
+  orc_dft3d(K, r2, -1);
+  double* ex = (double*)calloc(8 * N, sizeof(double)); /* e1x, e1y, e1z, e2 */
+  for (long i = 0; i < N; ++i) {
+    for (int d = 0; d < 3; ++d) {
+      const double ar = k1[2 * (d * N + i)], ai = k1[2 * (d * N + i) + 1];
+      ex[2 * (d * N + i)] = r1[2 * i] * ar - r1[2 * i + 1] * ai;
+      ex[2 * (d * N + i) + 1] = r1[2 * i] * ai + r1[2 * i + 1] * ar;
+    }
+    ex[2 * (3 * N + i)] = r2[2 * i] * k2a[2 * i] - r2[2 * i + 1] * k2a[2 * i + 1];
+    ex[2 * (3 * N + i) + 1] = r2[2 * i] * k2a[2 * i + 1] + r2[2 * i + 1] * k2a[2 * i];
+  }
+  for (int d = 0; d < 4; ++d) orc_dft3d(K, ex + 2 * d * N, +1);
+  for (long i = 0; i < N; ++i) {
+    double s0 = 0, s1 = 0;
+    for (int d = 0; d < 3; ++d) {
+      const double re = ex[2 * (d * N + i)] * charge / V, im = ex[2 * (d * N + i) + 1];
+      s0 += re * re;
+      s1 += im * im;
+    }
+    e1[2 * i] = s0;
+    e1[2 * i + 1] = s1;
+    e2[2 * i] = ex[2 * (3 * N + i)] * charge * charge / V;
+    e2[2 * i + 1] = ex[2 * (3 * N + i) + 1];
+  }
+  free(r1); free(r2); free(ex);
+}
+
 void orc_spme_ik_errmap(const int K[3], const double box[3], double beta, int order, const double* rho1,
                         const double* rho2, double charge, double* e1, double* e2) {
   const long N = (long)K[0] * K[1] * K[2];
@@ -125,37 +166,103 @@ void orc_spme_ik_errmap(const int K[3], const double box[3], double beta, int or
   orc_dft3d(K, k2a, -1);
   orc_dft3d(K, k2b, -1);
   for (long i = 0; i < 2 * N; ++i) k2a[i] += 2. * k2b[i];
-  /* the error of the profile */
-  double* r1 = (double*)calloc(2 * N, sizeof(double));
-  double* r2 = (double*)calloc(2 * N, sizeof(double));
-  for (long i = 0; i < N; ++i) {
-    r1[2 * i] = rho1[i] * V / (double)N;
-    r2[2 * i] = rho2[i] * V / (double)N;
+  errmap_apply(K, box, k1, k2a, rho1, rho2, charge, e1, e2);
+  free(g); free(k1); free(w); free(k2a); free(k2b);
+}
+
+
+/* ------------------------------------------------------------ real space
+ * ErrorEstimate_dir::makeS1k / makeS2k / calError (analyze/src/ErrorEstimate_dir.cpp:
+ * 124-331), rectangular box:
+ *   s1k(k) = 2/k int_rc^30 r f(r)^2 sin(2 pi k r) dr  (k != 0),  4 pi int_rc^30 r^2 f^2 dr (k = 0),
+ *     f(r) = (2 beta/sqrt(pi) e^{-beta^2 r^2} + erfc(beta r)/r) / r
+ *   s2k_d(k) = i k_d [2 pi / k int_rc^30 -2 erfc(beta r) sin(2 pi k r) dr
+ *              + 2 pi rc erfc(beta rc) (2 cos(e)/e - 2 sin(e)/e^2) / k],  e = 2 pi k rc
+ * with the integrals of the analyze tools' Integral1D (src/Integral1D.cpp:60-232):
+ * Gauss-4 boxes (nodes sqrt((3 -+ 2 sqrt(1.2))/7), weights (18 +- sqrt 30)/36),
+ * the range split into 10 boxes of tol/10, a box bisected while
+ * |coarse - (left + right)| >= 255 tol (children tol/2) and while its width is at
+ * least 1e-13 of the initial box; tol = 1e-20.  Then the calError above with
+ * k1 = s2k, k2a = s1k. */
+typedef struct { int kind; double k, beta; } DirFn;
+
+static double dir_f(const DirFn* f, double r) {
+  if (f->kind == 2) return -2. * erfc(f->beta * r) * sin(2. * M_PI * f->k * r);
+  const double betar = f->beta * r, ri = 1. / r;
+  const double fr = (2. * f->beta / sqrt(M_PI) * exp(-betar * betar) + erfc(betar) * ri) * ri;
+  if (f->kind == 0) return r * fr * fr * sin(2. * M_PI * f->k * r);
+  return r * r * fr * fr;
+}
+
+static double dir_coarse(const DirFn* f, double xlo, double xup) {
+  const double hx = xup - xlo;
+  const double v0 = sqrt((3 - 2 * sqrt(1.2)) / 7.), v1 = sqrt((3 + 2 * sqrt(1.2)) / 7.);
+  const double x0 = 0.5 * (xup - xlo) * (-v1) + 0.5 * (xup + xlo);
+  const double x1 = 0.5 * (xup - xlo) * (-v0) + 0.5 * (xup + xlo);
+  const double x2 = 0.5 * (xup - xlo) * (+v0) + 0.5 * (xup + xlo);
+  const double x3 = 0.5 * (xup - xlo) * (+v1) + 0.5 * (xup + xlo);
+  const double w0 = (18 + sqrt(30.)) / 36., w1 = (18 - sqrt(30.)) / 36.;
+  return 0.5 * hx * (w1 * (dir_f(f, x0) + dir_f(f, x3)) + w0 * (dir_f(f, x1) + dir_f(f, x2)));
+}
+
+static double dir_box(const DirFn* f, double xlo, double xup, double tol, double coarse, double ghx) {
+  const double hhx = 0.5 * (xup - xlo);
+  const double c0 = dir_coarse(f, xlo, xlo + hhx), c1 = dir_coarse(f, xlo + hhx, xup);
+  double value = c0 + c1;
+  if (fabs(coarse - value) < tol * 255) return value;
+  if (hhx * 2 < 1e-13 * ghx) return value;
+  value = 0;
+  value += dir_box(f, xlo, xlo + hhx, tol * 0.5, c0, ghx);
+  value += dir_box(f, xlo + hhx, xup, tol * 0.5, c1, ghx);
+  return value;
+}
+
+static double dir_int(int kind, double k, double beta, double xlo, double xup, double tol, int init_nx) {
+  DirFn f = {kind, k, beta};
+  const double hx = (xup - xlo) / (double)init_nx, nxi = 1. / (double)init_nx;
+  double value = 0;
+  for (int i = 0; i < init_nx; i++) {
+    const double x = xlo + i * hx;
+    value += dir_box(&f, x, x + hx, tol * nxi, dir_coarse(&f, x, x + hx), hx);
   }
-  orc_dft3d(K, r1, -1);
-  orc_dft3d(K, r2, -1);
-  double* ex = (double*)calloc(8 * N, sizeof(double)); /* e1x, e1y, e1z, e2 */
-  for (long i = 0; i < N; ++i) {
-    for (int d = 0; d < 3; ++d) {
-      const double ar = k1[2 * (d * N + i)], ai = k1[2 * (d * N + i) + 1];
-      ex[2 * (d * N + i)] = r1[2 * i] * ar - r1[2 * i + 1] * ai;
-      ex[2 * (d * N + i) + 1] = r1[2 * i] * ai + r1[2 * i + 1] * ar;
+  return value;
+}
+
+void orc_dir_errmap(const int K[3], const double box[3], double beta, double rcut, const double* rho1,
+                    const double* rho2, double charge, double* e1, double* e2) {
+  const long N = (long)K[0] * K[1] * K[2];
+  double* k1 = (double*)calloc(6 * N, sizeof(double));
+  double* k2a = (double*)calloc(2 * N, sizeof(double));
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int ix = -K[0] / 2; ix < K[0] - K[0] / 2; ++ix) {
+    const int lx = ix < 0 ? ix + K[0] : ix;
+    for (int iy = -K[1] / 2; iy < K[1] - K[1] / 2; ++iy) {
+      const int ly = iy < 0 ? iy + K[1] : iy;
+      for (int iz = -K[2] / 2; iz < K[2] - K[2] / 2; ++iz) {
+        const int lz = iz < 0 ? iz + K[2] : iz;
+        const long p = lz + (long)K[2] * (ly + (long)K[1] * lx);
+        /* makeS1k */
+        const double k1m = sqrt(ix * ix / (box[0] * box[0]) + iy * iy / (box[1] * box[1]) + iz * iz / (box[2] * box[2]));
+        if (k1m != 0) k2a[2 * p] = 2. / k1m * dir_int(0, k1m, beta, rcut, 30, 1e-20, 10);
+        else k2a[2 * p] = 4. * M_PI * dir_int(1, k1m, beta, rcut, 30, 1e-20, 10);
+        /* makeS2k */
+        const double kx = ix / box[0], ky = iy / box[1], kz = iz / box[2];
+        const double k = sqrt(kx * kx + ky * ky + kz * kz);
+        if (k != 0) {
+          const double an = dir_int(2, k, beta, rcut, 30, 1e-20, 10) / k;
+          const double e = 2. * M_PI * k * rcut;
+          double size = 2. * M_PI * rcut * erfc(beta * rcut) * (2. * cos(e) / e - 2. * sin(e) / (e * e));
+          size /= k;
+          const double kk[3] = {kx, ky, kz};
+          for (int d = 0; d < 3; ++d) {
+            double v = 2 * M_PI * kk[d] * an;
+            v += size * kk[d];
+            k1[2 * (d * N + p) + 1] = v;
+          }
+        }
+      }
     }
-    ex[2 * (3 * N + i)] = r2[2 * i] * k2a[2 * i] - r2[2 * i + 1] * k2a[2 * i + 1];
-    ex[2 * (3 * N + i) + 1] = r2[2 * i] * k2a[2 * i + 1] + r2[2 * i + 1] * k2a[2 * i];
   }
-  for (int d = 0; d < 4; ++d) orc_dft3d(K, ex + 2 * d * N, +1);
-  for (long i = 0; i < N; ++i) {
-    double s0 = 0, s1 = 0;
-    for (int d = 0; d < 3; ++d) {
-      const double re = ex[2 * (d * N + i)] * charge / V, im = ex[2 * (d * N + i) + 1];
-      s0 += re * re;
-      s1 += im * im;
-    }
-    e1[2 * i] = s0;
-    e1[2 * i + 1] = s1;
-    e2[2 * i] = ex[2 * (3 * N + i)] * charge * charge / V;
-    e2[2 * i + 1] = ex[2 * (3 * N + i) + 1];
-  }
-  free(g); free(k1); free(w); free(k2a); free(k2b); free(r1); free(r2); free(ex);
+  errmap_apply(K, box, k1, k2a, rho1, rho2, charge, e1, e2);
+  free(k1); free(k2a);
 }

@@ -175,3 +175,37 @@ extern "C" int ref_fcorr_run(const double* box, const int* nbin, double rc, cons
   return 0;
 }
 #endif
+
+#ifdef REF_ERRDIR
+// ErrorEstimate_dir::reinit + calError (analyze/app/error.dir.cpp) on a density
+// profile given on the grid K; error1 / error2 as [n][2] (real, imaginary).
+// The profile header is read with default-public members, as for the ik map.
+#include <cmath>
+#include <cstdlib>
+#include <string>
+#include <vector>
+#define class struct
+#include "DensityProfile.h"
+#undef class
+#include "ErrorEstimate_dir.h"
+extern "C" int ref_dir_errmap(const int* K, const double* box, double beta, double rcut, const double* rho1,
+                              const double* rho2, double charge, double* e1, double* e2) {
+  DensityProfile_PiecewiseConst dp;
+  dp.boxsize.assign(box, box + 3);
+  dp.nx = K[0]; dp.ny = K[1]; dp.nz = K[2];
+  dp.nele = K[0] * K[1] * K[2];
+  dp.hx = box[0] / K[0]; dp.hy = box[1] / K[1]; dp.hz = box[2] / K[2];
+  dp.profile1.assign(rho1, rho1 + dp.nele);
+  dp.profile2.assign(rho2, rho2 + dp.nele);
+  dp.profileP.assign(dp.nele, 0.);
+  dp.profileN.assign(dp.nele, 0.);
+  ErrorEstimate_dir est;
+  est.reinit(beta, rcut, dp);
+  est.calError(dp, charge);
+  for (unsigned i = 0; i < dp.nele; ++i) {
+    e1[2 * i] = est.error1[i][0]; e1[2 * i + 1] = est.error1[i][1];
+    e2[2 * i] = est.error2[i][0]; e2[2 * i + 1] = est.error2[i][1];
+  }
+  return 0;
+}
+#endif

@@ -182,6 +182,30 @@ def test_error_map_matches_oracle(mdf, orc, K, box, beta, order):
     assert np.abs(e2 - o2).max() < 1e-11 * np.abs(o2).max()
 
 
+@pytest.mark.parametrize("K,box,beta,rc", [((8, 8, 24), (6.0, 6.0, 18.0), 2.5, 1.35),
+                                           ((6, 5, 16), (5.0, 4.5, 14.0), 3.0, 1.2)])
+def test_dir_error_map_matches_oracle(mdf, orc, K, box, beta, rc):
+    """Real-space map (ErrorEstimate_dir) against the oracle, which matches the
+    reference's own build to 1e-12; even and odd grid sizes."""
+    rng = np.random.default_rng(3)
+    rho1 = rng.normal(0, 5, K)
+    rho2 = np.abs(rng.normal(30, 5, K))
+    em = mdf.ErrorEstimate_dir(K, box, beta, rc)
+    em.set_profile(rho1, rho2)
+    e1, e2 = em.calError(1.0)
+    o1, o2 = orc.dir_errmap(K, box, beta, rc, rho1, rho2, 1.0)
+    assert np.abs(e1[..., 0] - o1[..., 0]).max() < 1e-10 * np.abs(o1[..., 0]).max()
+    assert np.abs(e2[..., 0] - o2[..., 0]).max() < 1e-10 * np.abs(o2[..., 0]).max()
+    assert np.all(np.isfinite(em.rms()))
+
+
+def test_dir_error_map_rejects_unconverged_quadrature(mdf):
+    """erfc(beta rcut) = 4e-4: the reference's 1e-20 quadrature would not finish;
+    the map reports that instead of running on."""
+    with pytest.raises(mdf.MDException):
+        mdf.ErrorEstimate_dir((4, 4, 8), (6.0, 6.0, 18.0), 2.5, 1.0)
+
+
 def test_error_map_of_a_charged_slab(mdf, orc):
     """Deposited profile of a charged slab (analyze/app/error.spme.ik.cpp on a
     configuration): the profile and the error map against the oracle."""

@@ -118,3 +118,21 @@ def test_selfcorr_oracle_matches_reference_build(orc, charges, K, order):
     a = orc.spme_selfcorr(pos, q, box, K, order, 1.5)
     b = orc.ref_selfcorr(pos, q, box, 1.5, K, order)
     assert np.abs(a - b).max() < 1e-12 * np.abs(b).max()
+
+
+@pytest.mark.parametrize("K,box,beta,rc", [((8, 8, 24), (6.0, 6.0, 18.0), 2.5, 1.35),
+                                           ((5, 6, 15), (5.0, 6.0, 15.0), 3.0, 1.2)])
+def test_dir_errmap_oracle_matches_reference_build(orc, K, box, beta, rc):
+    """ErrorEstimate_dir restated (oracle_errmap.c) against the reference's own
+    analyze/src/ErrorEstimate_dir.cpp built in oracle/_ref."""
+    if not orc.ref_available("libref_errdir.so"):
+        pytest.skip("reference ErrorEstimate_dir not built (needs the reference tree at build time)")
+    rng = np.random.default_rng(1)
+    z = (np.arange(K[2]) + 0.5) * box[2] / K[2]
+    rho2 = np.ascontiguousarray(np.broadcast_to(np.where(np.abs(z - box[2] / 2) < 4, 30.0, 1.0), K), np.float64)
+    rho2 = rho2 * (1 + 0.1 * rng.random(K))
+    rho1 = np.ascontiguousarray(rho2 * 0.1 * (rng.random(K) - 0.5))
+    a1, a2 = orc.dir_errmap(K, box, beta, rc, rho1, rho2, 1.0)
+    b1, b2 = orc.ref_dir_errmap(K, box, beta, rc, rho1, rho2, 1.0)
+    assert np.abs(a1 - b1).max() < 1e-12 * np.abs(b1).max()
+    assert np.abs(a2[..., 0] - b2[..., 0]).max() < 1e-12 * np.abs(b2[..., 0]).max()
