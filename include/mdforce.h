@@ -126,6 +126,10 @@ int md_system_get_rcut(md_system* sys, float* rcut);
 int md_system_normalize(md_system* sys);
 /* FP64 statistic slots (MDStatistic::updateHost); out has MD_STAT_COUNT entries. */
 int md_system_read_stats(md_system* sys, double* out);
+/* The same slots copied to out in stream order without waiting (out should be
+   page-locked); out is valid after md_system_synchronize.  A per-step read of
+   the statistics that does not stall the launch queue. */
+int md_system_read_stats_async(md_system* sys, double* out);
 int md_system_clear_stats(md_system* sys);
 
 /* ------------------------------------------------------------- cell list
@@ -278,6 +282,19 @@ int md_errmap_compute(md_errmap* h, double charge, double* error1, double* error
  * md_errmap_set_profile / deposit / compute like the ik map. */
 int md_errmap_create_dir(md_errmap** out, const int K[3], const double L[3], double beta, double rcut,
                          int device);
+/* Analytic-differentiation SPME map (ErrorEstimate_SPME_Ana::reinit / calKernel / calError,
+ * analyze/src/ErrorEstimate_SPME_Ana.cpp:140-745, driven by analyze/app/error.spme.ana.cpp):
+ * alias images 0 < |k| <= 2, the derivative-of-B-spline term in the second moment and a
+ * homogeneous self-force error.  Takes md_errmap_set_profile / deposit / compute like the
+ * ik map; the RMS force error at a grid point is
+ * sqrt(error1[..][0] + error2[..][0] + self_error * charge^4) (print_error). */
+int md_errmap_create_ana(md_errmap** out, const int K[3], const double L[3], double beta, int order,
+                         int device);
+/* self_error of the analytic map (0 for the other maps); multiply by charge^4 */
+int md_errmap_self_error(md_errmap* h, double* out);
+/* FConvRho1_{x,y,z} of the analytic map for alias index k (0 < |k| <= 2) and the current
+   profile: IFFT(FFT(rho1 V/N) V F_d(k)) / V, out [3][K0][K1][K2][2] (print_error columns) */
+int md_errmap_ana_fconv(md_errmap* h, int k, double* out);
 
 /* ------------------------------------------------------- per-atom cutoff
  * Replaces AssignRCut::getRCut + assign (ENG/src/AssignRCut.cu:46-117):

@@ -53,7 +53,7 @@ __device__ double em_alias(double u, int n) {
   return s;
 }
 
-__global__ void k_em_g(EmGrid g, double beta, double* gm /* [3][N] */) {
+__global__ void k_em_g(EmGrid g, double beta, double* gm /* [3][N] */, double* fmo /* [N] or null */) {
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (t >= g.N) return;
   int ii[3];
@@ -67,11 +67,13 @@ __global__ void k_em_g(EmGrid g, double beta, double* gm /* [3][N] */) {
     fm = exp(-tt * tt * m2) / m2 / (2.0 * M_PI * V);
   }
   for (int d = 0; d < 3; ++d) gm[d * g.N + t] = -4.0 * M_PI * fm * m[d];
+  if (fmo) fmo[t] = fm;
 }
 
-// w_d = i g_d a(k) for one (k, dir), or with k == 0 the final 2 sum_{k, dir} a;
-// k1 (nullable) receives V w
-__global__ void k_em_fill(EmGrid g, int order, const double* gm, int k, int dir, double2* w, double2* k1) {
+// w_d = i g_d a(k) for one (k, dir), or with k == 0 the final 2 sum_{k, dir} a
+// over 0 < |k| <= kcut; k1 (nullable) receives V w
+__global__ void k_em_fill(EmGrid g, int order, int kcut, const double* gm, int k, int dir, double2* w,
+                          double2* k1) {
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (t >= g.N) return;
   int ii[3];
@@ -87,7 +89,7 @@ __global__ void k_em_fill(EmGrid g, int order, const double* gm, int k, int dir,
         u[d] = 2.0 * M_PI * em_c(ii[d], g.K[d]) / g.K[d];
         fen[d] = 1.0 / em_alias(u[d], order);
       }
-      for (int kk = -4; kk <= 4; ++kk) {
+      for (int kk = -kcut; kk <= kcut; ++kk) {
         if (kk == 0) continue;
         for (int d = 0; d < 3; ++d) a += 1.0 / em_pow(u[d] + 2.0 * M_PI * kk, order) * fen[d];
       }
@@ -118,11 +120,107 @@ __global__ void k_em_sq(EmGrid g, const double2* w, double2* out, int accumulate
   else out[t] = make_double2(s, 0.0);
 }
 
-__global__ void k_em_axpy2(long N, double2* a, const double2* b) {
+__global__ void k_em_axpy(long N, double2* a, const double2* b, double c) {
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (t >= N) return;
-  a[t].x += 2.0 * b[t].x;
-  a[t].y += 2.0 * b[t].y;
+  a[t].x += c * b[t].x;
+  a[t].y += c * b[t].y;
+}
+
+// ---- analytic-differentiation map (ErrorEstimate_SPME_Ana, analyze/src/
+// ErrorEstimate_SPME_Ana.cpp:220-667).  F_d(m, k) = -2 f(m) a_d(m, k) is the
+// alias-k force kernel of the differentiated B-spline (zero at the Nyquist
+// index of an even K_d); A*_dd = L_e L_f / V is the reciprocal box diagonal.
+__device__ __forceinline__ double ema_fm(const EmGrid& g, int order, double fm, const int ii[3], int d, int k) {
+  if ((g.K[d] % 2 == 0) && ii[d] == (g.K[d] >> 1)) return 0.0;
+  const double u = 2.0 * M_PI * em_c(ii[d], g.K[d]) / g.K[d];
+  double fen = 1.0 / em_pow(u + 2.0 * M_PI * k, order);
+  fen /= em_alias(u, order);
+  return -2.0 * fm * fen;
+}
+
+__host__ __device__ __forceinline__ double ema_astar(const double L[3], int d) {
+  const double V = L[0] * (L[1] * L[2]);
+  const int e = (d + 1) % 3, f = (d + 2) % 3;
+  return (L[e < f ? e : f] * L[e < f ? f : e]) * (1.0 / V);
+}
+
+// component dir of w (k space) set to i (g_dir a_dir(k) + 2 pi k K_dir A*_dd F_dir(k));
+// the other components of w are left as they are
+__global__ void k_ema_fill_diff(EmGrid g, int order, const double* gm, const double* fm, int k, int dir,
+                                double2* w) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= g.N) return;
+  int ii[3];
+  em_idx(t, g, ii);
+  double v = 0.0;
+  if (t != 0) {
+    const double u = 2.0 * M_PI * em_c(ii[dir], g.K[dir]) / g.K[dir];
+    const double a = 1.0 / em_pow(u + 2.0 * M_PI * k, order) * (1.0 / em_alias(u, order));
+    v = gm[dir * g.N + t] * a;
+    if ((g.K[dir] % 2 == 0) && ii[dir] == (g.K[dir] >> 1)) v = 0.0;
+  }
+  v += 2.0 * M_PI * (double)k * g.K[dir] * ema_astar(g.L, dir) * ema_fm(g, order, fm[t], ii, dir, k);
+  w[dir * g.N + t] = make_double2(0.0, v);
+}
+
+// sum over the grid of F_d(m, k), one block of 256 per (k, d): out[ki * 3 + d],
+// ki = 0..2 kcut - 1 for k = -kcut..-1, 1..kcut
+__global__ void k_ema_selfsum(EmGrid g, int order, int kcut, const double* fm, double* out) {
+  const int b = blockIdx.x, d = b % 3, ki = b / 3;
+  const int k = ki < kcut ? ki - kcut : ki - kcut + 1;
+  double s = 0.0;
+  for (long t = threadIdx.x; t < g.N; t += blockDim.x) {
+    int ii[3];
+    em_idx(t, g, ii);
+    s += ema_fm(g, order, fm[t], ii, d, k);
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int h = blockDim.x >> 1; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[b] = red[0];
+}
+
+// f(m) alone (the scalar factor of g)
+__global__ void k_ema_fm(EmGrid g, double beta, double* fmo) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= g.N) return;
+  int ii[3];
+  em_idx(t, g, ii);
+  const double m[3] = {em_c(ii[0], g.K[0]) / g.L[0], em_c(ii[1], g.K[1]) / g.L[1], em_c(ii[2], g.K[2]) / g.L[2]};
+  const double m2 = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+  const double V = g.L[0] * g.L[1] * g.L[2];
+  double fm = 0.0;
+  if (m2 != 0.0) {
+    const double tt = M_PI / beta;
+    fm = exp(-tt * tt * m2) / m2 / (2.0 * M_PI * V);
+  }
+  fmo[t] = fm;
+}
+
+// e_d = FFT(rho1 V/N) * V F_d(k) for the three d (FConvRho1 before its backward transform)
+__global__ void k_ema_fconv(EmGrid g, int order, const double* fm, int k, const double2* r1, double2* e) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= g.N) return;
+  int ii[3];
+  em_idx(t, g, ii);
+  const double V = g.L[0] * (g.L[1] * g.L[2]);
+  const double2 c = r1[t];
+  for (int d = 0; d < 3; ++d) {
+    const double b = ema_fm(g, order, fm[t], ii, d, k) * V;
+    e[d * g.N + t] = make_double2(c.x * b, c.y * b);
+  }
+}
+
+__global__ void k_ema_div(long n, double2* a, double s) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  a[t].x /= s;
+  a[t].y /= s;
 }
 
 __global__ void k_em_load(EmGrid g, const double* rho1, const double* rho2, double2* r) {
@@ -304,8 +402,17 @@ __global__ void k_em_dir_tables(EmGrid g, double beta, double rcut, double2* k1,
 
 }  // namespace
 
+// alias images summed by the reciprocal maps (global_half_N_k_sum of
+// ErrorEstimate_SPME_Ik.cpp:5 and ErrorEstimate_SPME_Ana.cpp:5)
+constexpr int EM_KCUT_IK = 4;
+constexpr int EM_KCUT_ANA = 2;
+
+enum { EM_KIND_IK = 0, EM_KIND_DIR = 1, EM_KIND_ANA = 2 };
+
 struct md_errmap {
   int device = 0;
+  int kind = EM_KIND_IK;
+  double self_error = 0;    // analytic map: self-force error of a unit charge (times q^4)
   cudaStream_t stream = nullptr;
   EmGrid g;
   double beta = 0;
@@ -374,21 +481,21 @@ extern "C" int md_errmap_create(md_errmap** out, const int K[3], const double L[
   MD_CUDA(cudaMemsetAsync(k2b, 0, sizeof(double2) * N, s));
   MD_CUDA(cudaMemsetAsync(h->cnt, 0, sizeof(double) * 2 * N, s));
   MD_CUDA(cudaMemsetAsync(h->rho, 0, sizeof(double) * 2 * N, s));
-  k_em_g<<<nb, 256, 0, s>>>(h->g, beta, gm);
-  for (int k = -4; k <= 4; ++k) {
+  k_em_g<<<nb, 256, 0, s>>>(h->g, beta, gm, nullptr);
+  for (int k = -EM_KCUT_IK; k <= EM_KCUT_IK; ++k) {
     if (k == 0) continue;
     for (int dir = 0; dir < 3; ++dir) {
-      k_em_fill<<<nb, 256, 0, s>>>(h->g, order, gm, k, dir, h->work, nullptr);
+      k_em_fill<<<nb, 256, 0, s>>>(h->g, order, EM_KCUT_IK, gm, k, dir, h->work, nullptr);
       if (int r = dft3_grid(h->work, h->g.K, +1, 3, s)) return fail(r);
       k_em_sq<<<nb, 256, 0, s>>>(h->g, h->work, k2b, 1);
     }
   }
-  k_em_fill<<<nb, 256, 0, s>>>(h->g, order, gm, 0, 0, h->work, h->k1);
+  k_em_fill<<<nb, 256, 0, s>>>(h->g, order, EM_KCUT_IK, gm, 0, 0, h->work, h->k1);
   if (int r = dft3_grid(h->work, h->g.K, +1, 3, s)) return fail(r);
   k_em_sq<<<nb, 256, 0, s>>>(h->g, h->work, h->k2a, 0);
   if (int r = dft3_grid(h->k2a, h->g.K, -1, 1, s)) return fail(r);
   if (int r = dft3_grid(k2b, h->g.K, -1, 1, s)) return fail(r);
-  k_em_axpy2<<<nb, 256, 0, s>>>(N, h->k2a, k2b);
+  k_em_axpy<<<nb, 256, 0, s>>>(N, h->k2a, k2b, 2.0);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   cudaFree(gm);
@@ -425,6 +532,7 @@ extern "C" int md_errmap_create_dir(md_errmap** out, const int K[3], const doubl
   h->device = device;
   h->beta = beta;
   h->order = 0;
+  h->kind = EM_KIND_DIR;
   for (int d = 0; d < 3; ++d) { h->g.K[d] = K[d]; h->g.L[d] = L[d]; }
   h->g.N = (long)K[0] * K[1] * K[2];
   const long N = h->g.N;
@@ -463,6 +571,142 @@ extern "C" int md_errmap_create_dir(md_errmap** out, const int K[3], const doubl
   cudaFree(flag);
   flag = nullptr;
   *out = h;
+  return MD_OK;
+}
+
+// ErrorEstimate_SPME_Ana::reinit / calKernel (analyze/src/ErrorEstimate_SPME_Ana.cpp:140-667):
+//   self  = sum_{0<|k|<=2} sum_d (2 pi k K_d A*_dd)^2 (sum_m F_d(m, k))^2
+//   k2b   = sum_{0<|k|<=2} sum_dir V/N (|IFFT(i g a_dir(k))|^2
+//            + |IFFT(i g a_dir(k) + i 2 pi k K_dir A*_dd F_dir(k) e_dir)|^2)
+//   k1    = V i g 2 sum_{k, dir} a_dir(k),  k2a = FFT(V/N |IFFT(k1 / V)|^2) + FFT(k2b)
+// The second square of each (k, dir) changes component dir only; the other two
+// keep the backward transforms of the first.
+extern "C" int md_errmap_create_ana(md_errmap** out, const int K[3], const double L[3], double beta, int order,
+                                    int device) {
+  if (!out || !K || !L || !(beta > 0) || order < 2 || order > 14) {
+    md_set_error("md_errmap_create_ana: bad arguments");
+    return MD_ERR_BADARG;
+  }
+  for (int d = 0; d < 3; ++d)
+    if (K[d] < 2 || K[d] > 1024 || !(L[d] > 0)) {
+      md_set_error("md_errmap_create_ana: grid %d or box %g out of range on axis %d", K[d], L[d], d);
+      return MD_ERR_BADARG;
+    }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    md_set_error("md_errmap_create_ana: no CUDA device %d", device);
+    return MD_ERR_CUDA;
+  }
+  MD_CUDA(cudaSetDevice(device));
+  md_errmap* h = new md_errmap();
+  h->device = device;
+  h->beta = beta;
+  h->order = order;
+  h->kind = EM_KIND_ANA;
+  for (int d = 0; d < 3; ++d) { h->g.K[d] = K[d]; h->g.L[d] = L[d]; }
+  h->g.N = (long)K[0] * K[1] * K[2];
+  const long N = h->g.N;
+  constexpr int NSELF = 2 * EM_KCUT_ANA * 3;
+  double *gm = nullptr, *fm = nullptr, *selfs = nullptr;
+  double2* k2b = nullptr;
+  bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaMalloc(&h->k1, sizeof(double2) * 3 * N) == cudaSuccess &&
+            cudaMalloc(&h->k2a, sizeof(double2) * N) == cudaSuccess &&
+            cudaMalloc(&h->work, sizeof(double2) * 4 * N) == cudaSuccess &&
+            cudaMalloc(&h->work2, sizeof(double2) * 2 * N) == cudaSuccess &&
+            cudaMalloc(&h->rho, sizeof(double) * 2 * N) == cudaSuccess &&
+            cudaMalloc(&h->cnt, sizeof(double) * 2 * N) == cudaSuccess &&
+            cudaMalloc(&gm, sizeof(double) * 3 * N) == cudaSuccess &&
+            cudaMalloc(&fm, sizeof(double) * N) == cudaSuccess &&
+            cudaMalloc(&selfs, sizeof(double) * NSELF) == cudaSuccess &&
+            cudaMalloc(&k2b, sizeof(double2) * N) == cudaSuccess;
+  auto fail = [&](int code) {
+    void* p[] = {gm, fm, selfs, k2b};
+    for (void* q : p) if (q) cudaFree(q);
+    em_free(h);
+    delete h;
+    return code;
+  };
+  if (!ok) return fail(md_cuda_fail(cudaGetLastError(), "md_errmap_create_ana allocation"));
+  cudaStream_t s = h->stream;
+  const unsigned nb = (unsigned)((N + 255) / 256);
+  MD_CUDA(cudaMemsetAsync(k2b, 0, sizeof(double2) * N, s));
+  MD_CUDA(cudaMemsetAsync(h->cnt, 0, sizeof(double) * 2 * N, s));
+  MD_CUDA(cudaMemsetAsync(h->rho, 0, sizeof(double) * 2 * N, s));
+  k_em_g<<<nb, 256, 0, s>>>(h->g, beta, gm, fm);
+  k_ema_selfsum<<<NSELF, 256, 0, s>>>(h->g, order, EM_KCUT_ANA, fm, selfs);
+  for (int k = -EM_KCUT_ANA; k <= EM_KCUT_ANA; ++k) {
+    if (k == 0) continue;
+    for (int dir = 0; dir < 3; ++dir) {
+      k_em_fill<<<nb, 256, 0, s>>>(h->g, order, EM_KCUT_ANA, gm, k, dir, h->work, nullptr);
+      if (int r = dft3_grid(h->work, h->g.K, +1, 3, s)) return fail(r);
+      k_em_sq<<<nb, 256, 0, s>>>(h->g, h->work, k2b, 1);
+      k_ema_fill_diff<<<nb, 256, 0, s>>>(h->g, order, gm, fm, k, dir, h->work);
+      if (int r = dft3_grid(h->work + dir * N, h->g.K, +1, 1, s)) return fail(r);
+      k_em_sq<<<nb, 256, 0, s>>>(h->g, h->work, k2b, 1);
+    }
+  }
+  k_em_fill<<<nb, 256, 0, s>>>(h->g, order, EM_KCUT_ANA, gm, 0, 0, h->work, h->k1);
+  if (int r = dft3_grid(h->work, h->g.K, +1, 3, s)) return fail(r);
+  k_em_sq<<<nb, 256, 0, s>>>(h->g, h->work, h->k2a, 0);
+  if (int r = dft3_grid(h->k2a, h->g.K, -1, 1, s)) return fail(r);
+  if (int r = dft3_grid(k2b, h->g.K, -1, 1, s)) return fail(r);
+  k_em_axpy<<<nb, 256, 0, s>>>(N, h->k2a, k2b, 1.0);
+  double hs[NSELF];
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hs, selfs, sizeof(hs), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail(md_cuda_fail(e, "md_errmap_create_ana kernel"));
+  double self = 0.0;
+  for (int ki = 0; ki < 2 * EM_KCUT_ANA; ++ki) {
+    const int k = ki < EM_KCUT_ANA ? ki - EM_KCUT_ANA : ki - EM_KCUT_ANA + 1;
+    for (int d = 0; d < 3; ++d) {
+      const double astar = ema_astar(L, d), sd = hs[ki * 3 + d];
+      self += 4. * M_PI * M_PI * k * k * K[d] * K[d] * astar * astar * sd * sd;
+    }
+  }
+  h->self_error = self;
+  cudaFree(gm); cudaFree(fm); cudaFree(selfs); cudaFree(k2b);
+  gm = fm = selfs = nullptr;
+  k2b = nullptr;
+  *out = h;
+  return MD_OK;
+}
+
+extern "C" int md_errmap_self_error(md_errmap* h, double* out) {
+  if (!h || !out) return MD_ERR_BADARG;
+  *out = h->self_error;
+  return MD_OK;
+}
+
+// FConvRho1_d(k) of ErrorEstimate_SPME_Ana::calError: IFFT(FFT(rho1 V/N) V F_d(k)) / V
+// for the three d, out [3][N][2]
+extern "C" int md_errmap_ana_fconv(md_errmap* h, int k, double* out) {
+  if (!h || !out) return MD_ERR_BADARG;
+  if (h->kind != EM_KIND_ANA) {
+    md_set_error("md_errmap_ana_fconv: the map is not the analytic-differentiation map");
+    return MD_ERR_BADARG;
+  }
+  if (k == 0 || k < -EM_KCUT_ANA || k > EM_KCUT_ANA) {
+    md_set_error("md_errmap_ana_fconv: alias index %d outside 0 < |k| <= %d", k, EM_KCUT_ANA);
+    return MD_ERR_BADARG;
+  }
+  MD_CUDA(cudaSetDevice(h->device));
+  cudaStream_t s = h->stream;
+  const long N = h->g.N;
+  const unsigned nb = (unsigned)((N + 255) / 256);
+  double* fm = reinterpret_cast<double*>(h->work + 3 * N);  // last N complex of work: f(m)
+  k_em_load<<<nb, 256, 0, s>>>(h->g, h->rho, h->rho + N, h->work2);
+  if (int r = dft3_grid(h->work2, h->g.K, -1, 1, s)) return r;
+  k_ema_fm<<<nb, 256, 0, s>>>(h->g, h->beta, fm);
+  k_ema_fconv<<<nb, 256, 0, s>>>(h->g, h->order, fm, k, h->work2, h->work);
+  if (int r = dft3_grid(h->work, h->g.K, +1, 3, s)) return r;
+  const double V = h->g.L[0] * (h->g.L[1] * h->g.L[2]);
+  k_ema_div<<<(unsigned)((3 * N + 255) / 256), 256, 0, s>>>(3 * N, h->work, V);
+  MD_CHECK_LAUNCH("errmap fconv");
+  MD_CUDA(cudaMemcpyAsync(out, h->work, sizeof(double2) * 3 * N, cudaMemcpyDeviceToHost, s));
+  MD_CUDA(cudaStreamSynchronize(s));
   return MD_OK;
 }
 

@@ -455,6 +455,14 @@ extern "C" int md_system_read_stats(md_system* s, double* out) {
   return MD_OK;
 }
 
+extern "C" int md_system_read_stats_async(md_system* s, double* out) {
+  if (int r = check_sys(s)) return r;
+  if (!out) return MD_ERR_BADARG;
+  MD_CUDA(cudaMemcpyAsync(out, s->st->stats, sizeof(double) * MD_STAT_COUNT, cudaMemcpyDeviceToHost,
+                          s->stream));
+  return MD_OK;
+}
+
 extern "C" int md_system_clear_stats(md_system* s) {
   if (int r = check_sys(s)) return r;
   Recorder rec;

@@ -62,6 +62,7 @@ _SIGS = {
     "md_system_get_rcut": (i32, [vp, P(f32)]),
     "md_system_normalize": (i32, [vp]),
     "md_system_read_stats": (i32, [vp, P(f64)]),
+    "md_system_read_stats_async": (i32, [vp, P(f64)]),
     "md_system_clear_stats": (i32, [vp]),
     "md_cell_list_create": (i32, [P(vp), vp, f64, i32, i32]),
     "md_cell_list_destroy": (i32, [vp]),
@@ -147,6 +148,9 @@ _SIGS = {
     "md_errmap_create": (i32, [P(vp), P(i32), P(f64), f64, i32, i32]),
     "md_errmap_destroy": (i32, [vp]),
     "md_errmap_create_dir": (i32, [P(vp), P(i32), P(f64), f64, f64, i32]),
+    "md_errmap_create_ana": (i32, [P(vp), P(i32), P(f64), f64, i32, i32]),
+    "md_errmap_self_error": (i32, [vp, P(f64)]),
+    "md_errmap_ana_fconv": (i32, [vp, i32, P(f64)]),
     "md_errmap_set_profile": (i32, [vp, P(f64), P(f64)]),
     "md_errmap_deposit": (i32, [vp, vp]),
     "md_errmap_get_profile": (i32, [vp, P(f64), P(f64)]),

@@ -204,6 +204,14 @@ class MDSystem:
         check(lib.md_system_read_stats(self.h, _p(out)), "read_stats")
         return out
 
+    def stats_async(self, out):
+        """Queue a copy of the statistic slots into out (float64, MD_STAT_COUNT,
+        page-locked for a copy that does not wait); out is valid after
+        synchronize()."""
+        if out.dtype != np.float64 or out.size < STAT_COUNT or not out.flags.c_contiguous:
+            raise ValueError("stats_async: out must be a contiguous float64 array of STAT_COUNT entries")
+        check(lib.md_system_read_stats_async(self.h, _p(out)), "read_stats_async")
+
     def clear_stats(self):
         check(lib.md_system_clear_stats(self.h), "clear_stats")
 
@@ -469,6 +477,60 @@ class ErrorEstimate_dir(ErrorEstimate_SPME_Ik):
               "ErrorEstimate_dir")
         self.h = h
         self.K = tuple(int(k) for k in K)
+
+
+class ErrorEstimate_SPME_Ana(ErrorEstimate_SPME_Ik):
+    """ErrorEstimate_SPME_Ana (analyze tools): reinit(beta, order, dp) builds the
+    analytic-differentiation kernel on the grid K of box L; calError(charge)
+    gives error1 and error2 ([K..., 2]); the RMS force error adds the self term
+    self_error * charge^4."""
+
+    def __init__(self, K, L, beta, order, device=0):
+        h = C.c_void_p()
+        KK = (C.c_int * 3)(*[int(k) for k in K])
+        LL = (C.c_double * 3)(*[float(x) for x in L])
+        check(lib.md_errmap_create_ana(C.byref(h), KK, LL, float(beta), int(order), int(device)),
+              "ErrorEstimate_SPME_Ana")
+        self.h = h
+        self.K = tuple(int(k) for k in K)
+        self.L = tuple(float(x) for x in L)
+
+    def self_error(self):
+        v = C.c_double()
+        check(lib.md_errmap_self_error(self.h, C.byref(v)), "self_error")
+        return v.value
+
+    def qself_error(self, charge=1.0):
+        return self.self_error() * charge ** 4
+
+    def rms(self, charge=1.0):
+        e1, e2 = self.calError(charge)
+        return np.sqrt(e1[..., 0] + e2[..., 0] + self.qself_error(charge))
+
+    def fconv(self, k):
+        """FConvRho1_{x,y,z} for alias index k (0 < |k| <= 2): [3, K..., 2]."""
+        out = np.empty((3,) + self.K + (2,))
+        check(lib.md_errmap_ana_fconv(self.h, int(k), _p(out)), "fconv")
+        return out
+
+    def print_error(self, path, charge=1.0):
+        """The columns of ErrorEstimate_SPME_Ana::print_error along x at y = z = 0:
+        x, RMS, error1 (re, im), error2 (re, im), self error, and the k = 1
+        x-kernel terms of FConvRho1 (taken, as the reference does, at the
+        grid's linear index i)."""
+        e1, e2 = self.calError(charge)
+        q = self.qself_error(charge)
+        fc = self.fconv(1)[0].reshape(-1, 2)
+        Kx, Lx = self.K[0], self.L[0]
+        c = 4.0 * np.pi ** 2 * Kx * Kx * (1.0 / Lx) ** 2
+        with open(path, "w") as f:
+            f.write("# 1      2         3-4       5-6      7\n")
+            f.write("# x  RMS-E  E_inhomo^2  E_homo^2  selfE^2\n")
+            for i in range(Kx):
+                a, b = e1[i, 0, 0], e2[i, 0, 0]
+                f.write("%f %e   %e %e %e %e   %e %e %e\n" % (
+                    (i + 0.5) * Lx / Kx, np.sqrt(a[0] + b[0] + q), a[0], a[1], b[0], b[1], q,
+                    np.sqrt(c * fc[i, 0] ** 2), np.sqrt(c * fc[i, 1] ** 2)))
 
 
 def choose_beta(sys, rcut, target):

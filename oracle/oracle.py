@@ -296,6 +296,42 @@ def dp_deposit(coord, box, n, profile=None):
     return prof
 
 
+def spme_ana_errmap(K, box, beta, order, rho1, rho2, charge=1.0, with_fconv=False):
+    """ErrorEstimate_SPME_Ana::reinit + calError restated (oracle_errmap.c): error1,
+    error2 as (K0, K1, K2, 2) arrays, the uncharged self error, and with with_fconv
+    FConvRho1 as (4, 3, K0, K1, K2, 2) for k = -2, -1, 1, 2 (else None)."""
+    KK = np.ascontiguousarray(K, np.int32)
+    b = np.ascontiguousarray(box, np.float64)
+    r1 = np.ascontiguousarray(rho1, np.float64).reshape(-1)
+    r2 = np.ascontiguousarray(rho2, np.float64).reshape(-1)
+    e1 = np.zeros(tuple(K) + (2,)); e2 = np.zeros(tuple(K) + (2,))
+    self_ = C.c_double()
+    fc = np.zeros((4, 3) + tuple(K) + (2,)) if with_fconv else None
+    _lib.orc_spme_ana_errmap(_p(KK, i32), _p(b, f64), float(beta), int(order), _p(r1, f64), _p(r2, f64),
+                             float(charge), _p(e1, f64), _p(e2, f64), C.byref(self_),
+                             _p(fc, f64) if with_fconv else None)
+    return e1, e2, self_.value, fc
+
+
+def ref_spme_ana_errmap(K, box, beta, order, rho1, rho2, charge=1.0, with_fconv=False):
+    """The reference's own ErrorEstimate_SPME_Ana (oracle/_ref/libref_errana.so), same
+    returns as spme_ana_errmap."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libref_errana.so"))
+    lib.ref_spme_ana_errmap.argtypes = [P(i32), P(f64), f64, i32, P(f64), P(f64), f64, P(f64), P(f64),
+                                        P(f64), P(f64)]
+    KK = np.ascontiguousarray(K, np.int32)
+    b = np.ascontiguousarray(box, np.float64)
+    r1 = np.ascontiguousarray(rho1, np.float64).reshape(-1)
+    r2 = np.ascontiguousarray(rho2, np.float64).reshape(-1)
+    e1 = np.zeros(tuple(K) + (2,)); e2 = np.zeros(tuple(K) + (2,))
+    self_ = np.zeros(1)
+    fc = np.zeros((4, 3) + tuple(K) + (2,)) if with_fconv else None
+    lib.ref_spme_ana_errmap(_p(KK, i32), _p(b, f64), float(beta), int(order), _p(r1, f64), _p(r2, f64),
+                            float(charge), _p(e1, f64), _p(e2, f64), _p(self_, f64),
+                            _p(fc, f64) if with_fconv else None)
+    return e1, e2, float(self_[0]), fc
+
+
 def dft3d(data, sign):
     """in-place unnormalised 3D DFT of a complex128 array"""
     d = np.ascontiguousarray(data, np.complex128).copy()
@@ -557,6 +593,8 @@ _sigs3 = {
     "orc_spme_selfcorr": (None, [i32, P(f64), P(f64), P(f64), P(i32), i32, f64, P(f64)]),
     "orc_spme_ik_errmap": (None, [P(i32), P(f64), f64, i32, P(f64), P(f64), f64, P(f64), P(f64)]),
     "orc_dir_errmap": (None, [P(i32), P(f64), f64, f64, P(f64), P(f64), f64, P(f64), P(f64)]),
+    "orc_spme_ana_errmap": (None, [P(i32), P(f64), f64, i32, P(f64), P(f64), f64, P(f64), P(f64),
+                                   P(f64), P(f64)]),
     "orc_dft3d": (None, [P(i32), P(f64), i32]),
 }
 for _n, (_r, _a) in _sigs3.items():

@@ -266,3 +266,164 @@ void orc_dir_errmap(const int K[3], const double box[3], double beta, double rcu
   errmap_apply(K, box, k1, k2a, rho1, rho2, charge, e1, e2);
   free(k1); free(k2a);
 }
+
+
+/* ------------------------------------------------- analytic differentiation
+ * ErrorEstimate_SPME_Ana::reinit / calKernel / calError (analyze/src/
+ * ErrorEstimate_SPME_Ana.cpp:140-745), rectangular box, alias images
+ * 0 < |k| <= 2 (global_half_N_k_sum = 2):
+ *   F_d(m, k) = -2 f(m) a_d(m, k)   (0 at the Nyquist index of an even K_d)
+ *   A*_dd     = L_e L_f / V,  c_d(k) = 2 pi k K_d A*_dd
+ *   self      = sum_{k, d} c_d(k)^2 (sum_m F_d(m, k))^2
+ *   k2b       = sum_{k, dir} V/N (|IFFT(w)|^2 + |IFFT(w + i c_dir(k) F_dir(k) e_dir)|^2),
+ *               w = i g a_dir(k)
+ *   k1        = V i g 2 sum_{k, dir} a_dir(k),  k2a = FFT(V/N |IFFT(k1 / V)|^2) + FFT(k2b)
+ * then calError as for the ik map.  fconv (nullable) receives
+ * FConvRho1_d(k) = IFFT(FFT(rho1 V/N) V F_d(k)) / V as [4 (k = -2,-1,1,2)][3][N][2]. */
+static double ana_astar(const double box[3], int d) {
+  const double V = box[0] * (box[1] * box[2]);
+  if (d == 0) return (box[1] * box[2]) * (1. / V);
+  if (d == 1) return (box[0] * box[2]) * (1. / V);
+  return (box[0] * box[1]) * (1. / V);
+}
+
+static double ana_F(const int K[3], int order, double fm, const int ii[3], int d, int k) {
+  if (K[d] % 2 == 0 && ii[d] == (K[d] >> 1)) return 0.;
+  const double u = 2. * M_PI * cidx(ii[d], K[d]) / K[d];
+  double fen = 1. / ipw(u + 2. * M_PI * k, order);
+  fen /= alias(u, order);
+  return -2. * fm * fen;
+}
+
+void orc_spme_ana_errmap(const int K[3], const double box[3], double beta, int order, const double* rho1,
+                         const double* rho2, double charge, double* e1, double* e2, double* self_out,
+                         double* fconv) {
+  const int KC = 2;
+  const long N = (long)K[0] * K[1] * K[2];
+  const double V = box[0] * box[1] * box[2];
+  const double scal = 1. / (2. * M_PI * V);
+  double* g = (double*)calloc(3 * N, sizeof(double));
+  double* f = (double*)calloc(N, sizeof(double));
+  double* k1 = (double*)calloc(6 * N, sizeof(double));
+  double* w = (double*)calloc(6 * N, sizeof(double));
+  double* k2a = (double*)calloc(2 * N, sizeof(double));
+  double* k2b = (double*)calloc(2 * N, sizeof(double));
+  int even[3];
+  for (int d = 0; d < 3; ++d) even[d] = (K[d] % 2 == 0);
+  for (long idx = 0; idx < N; ++idx) {
+    const int ii[3] = {(int)(idx / ((long)K[1] * K[2])), (int)((idx / K[2]) % K[1]), (int)(idx % K[2])};
+    const double m[3] = {cidx(ii[0], K[0]) / box[0], cidx(ii[1], K[1]) / box[1], cidx(ii[2], K[2]) / box[2]};
+    const double m2 = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+    if (m2 == 0) continue;
+    const double t = M_PI / beta;
+    f[idx] = exp(-t * t * m2) / m2 * scal;
+    for (int d = 0; d < 3; ++d) g[d * N + idx] = -4. * M_PI * f[idx] * m[d];
+  }
+  /* self-force error: sequential sums over the grid, as calKernel takes them */
+  double self = 0.;
+  for (int k = -KC; k <= KC; ++k) {
+    if (k == 0) continue;
+    for (int d = 0; d < 3; ++d) {
+      double s = 0.;
+      for (long idx = 0; idx < N; ++idx) {
+        const int ii[3] = {(int)(idx / ((long)K[1] * K[2])), (int)((idx / K[2]) % K[1]), (int)(idx % K[2])};
+        s += ana_F(K, order, f[idx], ii, d, k);
+      }
+      const double a = ana_astar(box, d);
+      self += 4. * M_PI * M_PI * k * k * K[d] * K[d] * a * a * s * s;
+    }
+  }
+  *self_out = self;
+  /* second moment of the aliased force kernels */
+  for (int k = -KC; k <= KC; ++k) {
+    if (k == 0) continue;
+    for (int dir = 0; dir < 3; ++dir) {
+      memset(w, 0, sizeof(double) * 6 * N);
+      double* wd = (double*)calloc(2 * N, sizeof(double)); /* component dir with the derivative term */
+      for (long idx = 1; idx < N; ++idx) {
+        const int ii[3] = {(int)(idx / ((long)K[1] * K[2])), (int)((idx / K[2]) % K[1]), (int)(idx % K[2])};
+        const double u = 2. * M_PI * cidx(ii[dir], K[dir]) / K[dir];
+        const double a = 1. / ipw(u + 2. * M_PI * k, order) * (1. / alias(u, order));
+        for (int d = 0; d < 3; ++d) {
+          double v = g[d * N + idx] * a;
+          if (even[d] && ii[d] == (K[d] >> 1)) v = 0.;
+          w[2 * (d * N + idx) + 1] = v;
+        }
+      }
+      for (long idx = 0; idx < N; ++idx) {
+        const int ii[3] = {(int)(idx / ((long)K[1] * K[2])), (int)((idx / K[2]) % K[1]), (int)(idx % K[2])};
+        wd[2 * idx + 1] = w[2 * (dir * N + idx) + 1] +
+                          2. * M_PI * (double)k * K[dir] * ana_astar(box, dir) * ana_F(K, order, f[idx], ii, dir, k);
+      }
+      for (int d = 0; d < 3; ++d) orc_dft3d(K, w + 2 * d * N, +1);
+      orc_dft3d(K, wd, +1);
+      for (int pass = 0; pass < 2; ++pass)
+        for (long i = 0; i < N; ++i) {
+          double s = 0;
+          for (int d = 0; d < 3; ++d) {
+            const double* src = (pass == 1 && d == dir) ? wd + 2 * i : w + 2 * (d * N + i);
+            s += src[0] * src[0] + src[1] * src[1];
+          }
+          k2b[2 * i] += s * V / (double)N;
+        }
+      free(wd);
+    }
+  }
+  /* the summed kernel */
+  memset(w, 0, sizeof(double) * 6 * N);
+  for (long idx = 1; idx < N; ++idx) {
+    const int ii[3] = {(int)(idx / ((long)K[1] * K[2])), (int)((idx / K[2]) % K[1]), (int)(idx % K[2])};
+    double u[3], fen[3];
+    for (int d = 0; d < 3; ++d) {
+      u[d] = 2. * M_PI * cidx(ii[d], K[d]) / K[d];
+      fen[d] = 1. / alias(u[d], order);
+    }
+    double sum = 0.;
+    for (int k = -KC; k <= KC; ++k) {
+      if (k == 0) continue;
+      for (int d = 0; d < 3; ++d) sum += 1. / ipw(u[d] + 2. * M_PI * k, order) * fen[d];
+    }
+    for (int d = 0; d < 3; ++d) {
+      double v = g[d * N + idx] * sum * 2.;
+      if (even[d] && ii[d] == (K[d] >> 1)) v = 0.;
+      w[2 * (d * N + idx) + 1] = v;
+      k1[2 * (d * N + idx) + 1] = v * V;
+    }
+  }
+  for (int d = 0; d < 3; ++d) orc_dft3d(K, w + 2 * d * N, +1);
+  for (long i = 0; i < N; ++i) {
+    double s = 0;
+    for (int d = 0; d < 3; ++d) {
+      const double re = w[2 * (d * N + i)], im = w[2 * (d * N + i) + 1];
+      s += re * re + im * im;
+    }
+    k2a[2 * i] = s * V / (double)N;
+  }
+  orc_dft3d(K, k2a, -1);
+  orc_dft3d(K, k2b, -1);
+  for (long i = 0; i < 2 * N; ++i) k2a[i] += k2b[i];
+  errmap_apply(K, box, k1, k2a, rho1, rho2, charge, e1, e2);
+  if (fconv) {
+    double* r1 = (double*)calloc(2 * N, sizeof(double));
+    for (long i = 0; i < N; ++i) r1[2 * i] = rho1[i] * V / (double)N;
+    orc_dft3d(K, r1, -1);
+    int slot = 0;
+    for (int k = -KC; k <= KC; ++k) {
+      if (k == 0) continue;
+      for (int d = 0; d < 3; ++d) {
+        double* o = fconv + 2 * N * (3 * slot + d);
+        for (long idx = 0; idx < N; ++idx) {
+          const int ii[3] = {(int)(idx / ((long)K[1] * K[2])), (int)((idx / K[2]) % K[1]), (int)(idx % K[2])};
+          const double b = ana_F(K, order, f[idx], ii, d, k) * V;
+          o[2 * idx] = r1[2 * idx] * b;
+          o[2 * idx + 1] = r1[2 * idx + 1] * b;
+        }
+        orc_dft3d(K, o, +1);
+        for (long i = 0; i < 2 * N; ++i) o[i] /= V;
+      }
+      ++slot;
+    }
+    free(r1);
+  }
+  free(g); free(f); free(k1); free(w); free(k2a); free(k2b);
+}

@@ -209,3 +209,57 @@ extern "C" int ref_dir_errmap(const int* K, const double* box, double beta, doub
   return 0;
 }
 #endif
+
+#ifdef REF_ERRANA
+// ErrorEstimate_SPME_Ana::reinit + calError (analyze/app/error.spme.ana.cpp) on a
+// density profile given on the grid K; error1 / error2 as [n][2] (real, imaginary),
+// the uncharged self error, and (when fconv is not null) FConvRho1 of the four
+// alias indices k = -2, -1, 1, 2 as [4][3][n][2].  The profile header is read with
+// default-public members, as for the ik map.
+#include <cmath>
+#include <cstdlib>
+#include <string>
+#include <vector>
+#define class struct
+#include "DensityProfile.h"
+#undef class
+#include "ErrorEstimate_SPME_Ana.h"
+extern "C" int ref_spme_ana_errmap(const int* K, const double* box, double beta, int order, const double* rho1,
+                                   const double* rho2, double charge, double* e1, double* e2, double* self_out,
+                                   double* fconv) {
+  DensityProfile_PiecewiseConst dp;
+  dp.boxsize.assign(box, box + 3);
+  dp.nx = K[0]; dp.ny = K[1]; dp.nz = K[2];
+  dp.nele = K[0] * K[1] * K[2];
+  dp.hx = box[0] / K[0]; dp.hy = box[1] / K[1]; dp.hz = box[2] / K[2];
+  dp.profile1.assign(rho1, rho1 + dp.nele);
+  dp.profile2.assign(rho2, rho2 + dp.nele);
+  dp.profileP.assign(dp.nele, 0.);
+  dp.profileN.assign(dp.nele, 0.);
+  ErrorEstimate_SPME_Ana est;
+  est.reinit(beta, order, dp);
+  est.calError(dp, charge);
+  const unsigned n = dp.nele;
+  for (unsigned i = 0; i < n; ++i) {
+    e1[2 * i] = est.error1[i][0]; e1[2 * i + 1] = est.error1[i][1];
+    e2[2 * i] = est.error2[i][0]; e2[2 * i + 1] = est.error2[i][1];
+  }
+  *self_out = est.self_error;
+  if (fconv) {
+    // kcut (a default-private member) is global_half_N_k_sum = 2 of the source file
+    const int kc = 2;
+    int slot = 0;
+    for (int k = -kc; k <= kc; ++k) {
+      if (k == 0) continue;
+      fftw_complex* src[3] = {est.FConvRho1x[k + kc], est.FConvRho1y[k + kc], est.FConvRho1z[k + kc]};
+      for (int d = 0; d < 3; ++d)
+        for (unsigned i = 0; i < n; ++i) {
+          fconv[2 * (n * (3 * slot + d) + i)] = src[d][i][0];
+          fconv[2 * (n * (3 * slot + d) + i) + 1] = src[d][i][1];
+        }
+      ++slot;
+    }
+  }
+  return 0;
+}
+#endif

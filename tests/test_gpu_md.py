@@ -233,3 +233,22 @@ def test_langevin_temperature(mdf, fluid):
     T = np.mean(Ts)
     # BAOAB kinetic temperature is exact for harmonic forces and O(dt^2) here
     assert abs(T - 1.0) < 0.02, T
+
+
+def test_stream_ordered_stats_rows_match_blocking_reads(mdf, fluid):
+    # one row per step queued without a wait equals the blocking read taken
+    # after the same step on an identical run (to the order of the FP64
+    # block-sum reduction)
+    import torch
+    a, sa, _ = _run_gpu(mdf, fluid, 0, 0)
+    b, sb, _ = _run_gpu(mdf, fluid, 0, 0)
+    rows = torch.zeros((5, mdf.STAT_COUNT), dtype=torch.float64).pin_memory().numpy()
+    for k in range(5):
+        sa.run(1)
+        a.stats_async(rows[k])
+    a.synchronize()
+    for k in range(5):
+        sb.run(1)
+        assert np.allclose(rows[k], b.stats(), rtol=1e-12, atol=1e-12)
+    with pytest.raises(ValueError):
+        a.stats_async(np.zeros(3))

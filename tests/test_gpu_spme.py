@@ -206,6 +206,59 @@ def test_dir_error_map_rejects_unconverged_quadrature(mdf):
         mdf.ErrorEstimate_dir((4, 4, 8), (6.0, 6.0, 18.0), 2.5, 1.0)
 
 
+@pytest.mark.parametrize("K,box,beta,order", [((8, 8, 16), (3.0, 3.0, 6.0), 2.5, 4),
+                                              ((7, 6, 5), (5.0, 4.0, 3.5), 1.8, 5),
+                                              ((10, 12, 9), (3.1, 3.5, 2.9), 3.0, 6)])
+def test_ana_error_map_matches_oracle(mdf, orc, K, box, beta, order):
+    """Analytic-differentiation map (ErrorEstimate_SPME_Ana) against the oracle,
+    which matches the reference's own build to 1e-12: error1, error2, the self
+    error and FConvRho1 of every alias index; even and odd grids and orders."""
+    rng = np.random.default_rng(4)
+    rho1 = rng.normal(0, 5, K)
+    rho2 = np.abs(rng.normal(30, 5, K))
+    em = mdf.ErrorEstimate_SPME_Ana(K, box, beta, order)
+    em.set_profile(rho1, rho2)
+    e1, e2 = em.calError(1.3)
+    o1, o2, oself, ofc = orc.spme_ana_errmap(K, box, beta, order, rho1, rho2, 1.3, with_fconv=True)
+    for a, b in ((e1, o1), (e2, o2)):
+        scale = np.abs(b[..., 0]).max()
+        assert np.abs(a[..., 0] - b[..., 0]).max() < 1e-11 * scale
+        assert np.abs(a[..., 1] - b[..., 1]).max() < 1e-9 * scale
+    assert abs(em.self_error() - oself) <= 1e-11 * abs(oself)
+    for slot, k in enumerate((-2, -1, 1, 2)):
+        fc = em.fconv(k)
+        assert np.abs(fc - ofc[slot]).max() < 1e-11 * np.abs(ofc[slot]).max()
+    rms = em.rms(1.3)
+    assert np.allclose(rms, np.sqrt(o1[..., 0] + o2[..., 0] + oself * 1.3 ** 4), rtol=1e-10, atol=0)
+
+
+def test_ana_error_map_print_error_and_arguments(mdf, orc, tmp_path):
+    K, box = (8, 8, 16), (3.0, 3.0, 6.0)
+    rng = np.random.default_rng(5)
+    rho1 = rng.normal(0, 5, K)
+    rho2 = np.abs(rng.normal(30, 5, K))
+    em = mdf.ErrorEstimate_SPME_Ana(K, box, 2.5, 4)
+    em.set_profile(rho1, rho2)
+    path = tmp_path / "error.out"
+    em.print_error(str(path))
+    rows = np.loadtxt(path)
+    assert rows.shape == (K[0], 9)
+    o1, o2, oself, _ = orc.spme_ana_errmap(K, box, 2.5, 4, rho1, rho2, 1.0)
+    assert np.allclose(rows[:, 0], (np.arange(K[0]) + 0.5) * box[0] / K[0], atol=1e-6)
+    assert np.allclose(rows[:, 1], np.sqrt(o1[:, 0, 0, 0] + o2[:, 0, 0, 0] + oself), rtol=1e-5)
+    assert np.allclose(rows[:, 6], oself, rtol=1e-5)
+    for k in (0, 3, -3):
+        with pytest.raises(mdf.MDException):
+            em.fconv(k)
+    # the other maps have no self term and no FConvRho1
+    import ctypes as C
+    ik = mdf.ErrorEstimate_SPME_Ik(K, box, 2.5, 4)
+    v = C.c_double(-1.0)
+    assert mdf.lib.md_errmap_self_error(ik.h, C.byref(v)) == 0 and v.value == 0.0
+    out = np.zeros((3,) + K + (2,))
+    assert mdf.lib.md_errmap_ana_fconv(ik.h, 1, out.ctypes.data_as(C.POINTER(C.c_double))) == 11
+
+
 def test_error_map_of_a_charged_slab(mdf, orc):
     """Deposited profile of a charged slab (analyze/app/error.spme.ik.cpp on a
     configuration): the profile and the error map against the oracle."""

@@ -136,3 +136,27 @@ def test_dir_errmap_oracle_matches_reference_build(orc, K, box, beta, rc):
     b1, b2 = orc.ref_dir_errmap(K, box, beta, rc, rho1, rho2, 1.0)
     assert np.abs(a1 - b1).max() < 1e-12 * np.abs(b1).max()
     assert np.abs(a2[..., 0] - b2[..., 0]).max() < 1e-12 * np.abs(b2[..., 0]).max()
+
+
+@pytest.mark.parametrize("K,box,beta,order", [((8, 8, 16), (3.0, 3.0, 6.0), 2.5, 4),
+                                              ((7, 6, 5), (5.0, 4.0, 3.5), 1.8, 5),
+                                              ((10, 12, 9), (3.1, 3.5, 2.9), 3.0, 6)])
+def test_ana_errmap_oracle_matches_reference_build(orc, K, box, beta, order):
+    """ErrorEstimate_SPME_Ana restated (oracle_errmap.c) against the reference's own
+    analyze/src/ErrorEstimate_SPME_Ana.cpp built in oracle/_ref: error1, error2, the
+    self error and FConvRho1; even and odd grids, even and odd orders."""
+    if not orc.ref_available("libref_errana.so"):
+        pytest.skip("reference ErrorEstimate_SPME_Ana not built (needs the reference tree at build time)")
+    rng = np.random.default_rng(4)
+    rho1 = rng.normal(0, 5, K)
+    rho2 = np.abs(rng.normal(30, 5, K))
+    a1, a2, aself, afc = orc.spme_ana_errmap(K, box, beta, order, rho1, rho2, 1.3, with_fconv=True)
+    b1, b2, bself, bfc = orc.ref_spme_ana_errmap(K, box, beta, order, rho1, rho2, 1.3, with_fconv=True)
+    # real parts are the estimate; the imaginary parts are transform rounding and
+    # are compared on the scale of the real parts
+    for a, b in ((a1, b1), (a2, b2)):
+        scale = np.abs(b[..., 0]).max()
+        assert np.abs(a[..., 0] - b[..., 0]).max() < 1e-12 * scale
+        assert np.abs(a[..., 1] - b[..., 1]).max() < 1e-12 * scale
+    assert abs(aself - bself) <= 1e-12 * abs(bself)
+    assert np.abs(afc - bfc).max() < 1e-12 * np.abs(bfc).max()
