@@ -42,7 +42,9 @@ enum md_status {
   MD_ERR_BADARG = 11,         /* invalid argument / NaN input                 */
   MD_ERR_UNSUPPORTED = 12,    /* feature absent (e.g. bonded terms present)   */
   MD_ERR_TIMEOUT = 13,        /* a bounded device wait gave up                */
-  MD_ERR_NOMEM = 14
+  MD_ERR_NOMEM = 14,
+  MD_ERR_IO = 15              /* a file could not be opened, read or written (MDExcptCannotOpenFile,
+                                 MDExcptWrongFileFormat) */
 };
 
 /* arithmetic of the force path */
@@ -131,6 +133,24 @@ int md_system_read_stats(md_system* sys, double* out);
    the statistics that does not stall the launch queue. */
 int md_system_read_stats_async(md_system* sys, double* out);
 int md_system_clear_stats(md_system* sys);
+
+/* ------------------------------------------------------- configuration files
+ * .gro files as the reference engine reads and writes them (GromacsFileManager::readGroFile /
+ * writeGroFile, ENG/src/GromacsFileManager.cpp:7-124; MDSystem::initConfig and
+ * writeHostDataGro, ENG/src/MDSystem_interface.cu:39-215).  Names are 8-byte slots
+ * ([N][8], NUL padded; StringSize of the reference); pos / vel are [N][3].  Values pass
+ * through binary32 both ways (the reference's ScalorType), so reading gives the reference's
+ * values and writing gives its bytes.  An atom line without a velocity reads as zero
+ * velocity.  Any of resd_index, resd_name, atom_name, atom_index, vel may be NULL (on
+ * writing: indices 1..N, empty names, zero velocity).  File errors return MD_ERR_IO. */
+int md_gro_count(const char* path, int* n_atoms);
+int md_gro_read(const char* path, int n_atoms, int* resd_index, char* resd_name, char* atom_name,
+                int* atom_index, double* pos, double* vel, double box[3]);
+/* title is the first line without its newline (writeHostDataGro writes
+   "# at time = %f, step = %d"); NULL writes an empty title */
+int md_gro_write(const char* path, const char* title, int n_atoms, const int* resd_index,
+                 const char* resd_name, const char* atom_name, const int* atom_index, const double* pos,
+                 const double* vel, const double box[3]);
 
 /* ------------------------------------------------------------- cell list
  * Replaces CellList(sys, cellSize, NThreadCell, NThreadAtom, bdir, divide) and

@@ -128,6 +128,10 @@ _SIGS = {
     "md_arc_assign": (i32, [vp, vp]),
     "md_arc_pressure_correction": (i32, [vp, vp, P(f64)]),
     "md_synth_fcc": (i32, [i32, i32, i32, P(f64), f64, u64, P(f64)]),
+    "md_gro_count": (i32, [C.c_char_p, P(i32)]),
+    "md_gro_read": (i32, [C.c_char_p, i32, P(i32), P(C.c_char), P(C.c_char), P(i32), P(f64), P(f64), P(f64)]),
+    "md_gro_write": (i32, [C.c_char_p, C.c_char_p, i32, P(i32), P(C.c_char), P(C.c_char), P(i32), P(f64),
+                           P(f64), P(f64)]),
     "md_synth_slab": (i32, [i32, i32, P(f64), i32, f64, f64, f64, u64, P(f64)]),
     "md_synth_maxwell": (i32, [i32, P(f64), f64, u64, P(f64)]),
     "md_synth_charges": (i32, [i32, u64, P(f64)]),

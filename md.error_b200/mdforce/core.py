@@ -27,6 +27,8 @@ MD_ERR_CUDA = 10
 MD_ERR_BADARG = 11
 MD_ERR_UNSUPPORTED = 12
 MD_ERR_TIMEOUT = 13
+MD_ERR_NOMEM = 14
+MD_ERR_IO = 15
 
 PREC_MIXED = 0
 PREC_FP64 = 1
@@ -75,9 +77,14 @@ class MDExcptTimeout(MDException):
     code = MD_ERR_TIMEOUT
 
 
+class MDExcptIO(MDException, OSError):
+    """MDExcptCannotOpenFile / MDExcptWrongFileFormat of the reference."""
+    code = MD_ERR_IO
+
+
 _BY_CODE = {c.code: c for c in (MDExcptCuda, MDExcptShortCellList, MDExcptShortNeighborList,
                                  MDExcptCellIndexOverflow, MDExcptBadArgument,
-                                 MDExcptUnsupported, MDExcptTimeout)}
+                                 MDExcptUnsupported, MDExcptTimeout, MDExcptIO)}
 
 
 def check(status, what=""):
@@ -531,6 +538,83 @@ class ErrorEstimate_SPME_Ana(ErrorEstimate_SPME_Ik):
                 f.write("%f %e   %e %e %e %e   %e %e %e\n" % (
                     (i + 0.5) * Lx / Kx, np.sqrt(a[0] + b[0] + q), a[0], a[1], b[0], b[1], q,
                     np.sqrt(c * fc[i, 0] ** 2), np.sqrt(c * fc[i, 1] ** 2)))
+
+
+class GroConf:
+    """A .gro configuration (GromacsFileManager::readGroFile): residue and atom
+    indices, names (str), positions and velocities [N, 3] and the box edges."""
+
+    def __init__(self, pos, box, vel=None, resd_index=None, resd_name=None, atom_name=None,
+                 atom_index=None, title=""):
+        self.pos = _f64(pos).reshape(-1, 3)
+        n = self.pos.shape[0]
+        self.box = _f64(box, (3,))
+        self.vel = np.zeros((n, 3)) if vel is None else _f64(vel).reshape(-1, 3)
+        self.resd_index = np.arange(1, n + 1, dtype=np.int32) if resd_index is None else \
+            np.ascontiguousarray(resd_index, np.int32)
+        self.atom_index = np.arange(1, n + 1, dtype=np.int32) if atom_index is None else \
+            np.ascontiguousarray(atom_index, np.int32)
+        self.resd_name = [""] * n if resd_name is None else list(resd_name)
+        self.atom_name = [""] * n if atom_name is None else list(atom_name)
+        self.title = title
+
+    @property
+    def n(self):
+        return self.pos.shape[0]
+
+
+def _names_to_slots(names):
+    out = np.zeros((len(names), 8), np.uint8)
+    for i, s in enumerate(names):
+        b = s.encode()[:7]
+        out[i, :len(b)] = np.frombuffer(b, np.uint8)
+    return out
+
+
+def read_gro(path):
+    """GromacsFileManager::readGroFile (values pass through binary32 as in the reference)."""
+    n = C.c_int()
+    check(lib.md_gro_count(str(path).encode(), C.byref(n)), "read_gro")
+    n = n.value
+    ri = np.zeros(n, np.int32)
+    ai = np.zeros(n, np.int32)
+    rn = np.zeros((n, 8), np.uint8)
+    an = np.zeros((n, 8), np.uint8)
+    pos = np.zeros((n, 3))
+    vel = np.zeros((n, 3))
+    box = np.zeros(3)
+    check(lib.md_gro_read(str(path).encode(), n, _p(ri, C.c_int), _p(rn, C.c_char), _p(an, C.c_char),
+                          _p(ai, C.c_int), _p(pos), _p(vel), _p(box)), "read_gro")
+    with open(path, "rb") as f:
+        title = f.readline().decode(errors="replace").rstrip("\n")
+    dec = lambda row: bytes(row).split(b"\0", 1)[0].decode()
+    return GroConf(pos, box, vel, ri, [dec(r) for r in rn], [dec(r) for r in an], ai, title)
+
+
+def write_gro(path, conf, title=None):
+    """GromacsFileManager::writeGroFile with the given first line."""
+    rn = _names_to_slots(conf.resd_name)
+    an = _names_to_slots(conf.atom_name)
+    t = conf.title if title is None else title
+    check(lib.md_gro_write(str(path).encode(), t.encode(), conf.n, _p(conf.resd_index, C.c_int),
+                           _p(rn, C.c_char), _p(an, C.c_char), _p(conf.atom_index, C.c_int),
+                           _p(_f64(conf.pos)), _p(_f64(conf.vel)), _p(_f64(conf.box))), "write_gro")
+
+
+def system_from_gro(path, charge=None, mass=None, precision=PREC_MIXED, device=0):
+    """MDSystem::initConfig(configfile) + initDeviceData: the system and the
+    configuration it was read from (names and indices for writing it back)."""
+    conf = read_gro(path)
+    return MDSystem(conf.pos, conf.box, vel=conf.vel, charge=charge, mass=mass, precision=precision,
+                    device=device), conf
+
+
+def write_system_gro(path, sys, conf, step=0, time=0.0):
+    """MDSystem::writeHostDataGro: the system's current positions (wrapped, original
+    order), velocities and box with the names of conf, titled as the reference does."""
+    out = GroConf(sys.positions(), sys.box(), sys.velocities(), conf.resd_index, conf.resd_name,
+                  conf.atom_name, conf.atom_index)
+    write_gro(path, out, "# at time = %f, step = %d" % (time, step))
 
 
 def choose_beta(sys, rcut, target):

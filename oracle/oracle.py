@@ -674,3 +674,36 @@ def error_estimate_pme(box, K, beta, rcut, c2, natom):
 def error_estimate_spme_ik(box, K, order, beta, c2, natom):
     b = np.ascontiguousarray(box, np.float64); KK = np.ascontiguousarray(K, np.int32)
     return _lib.orc_error_estimate_spme_ik(_p(b, f64), _p(KK, i32), order, beta, c2, natom)
+
+
+def ref_gro_read(path, n):
+    """The reference engine's own GromacsFileManager::readGroFile
+    (oracle/_ref/libref_gro.so): binary32 values; None when it threw."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libref_gro.so"))
+    lib.ref_gro_read.argtypes = [C.c_char_p, i32, P(i32), P(C.c_char), P(C.c_char), P(i32), P(C.c_float),
+                                 P(C.c_float), P(C.c_float)]
+    ri = np.zeros(n, np.int32); ai = np.zeros(n, np.int32)
+    rn = np.zeros((n, 8), np.uint8); an = np.zeros((n, 8), np.uint8)
+    pos = np.zeros((n, 3), np.float32); vel = np.zeros((n, 3), np.float32); box = np.zeros(3, np.float32)
+    r = lib.ref_gro_read(str(path).encode(), n, _p(ri, i32), _p(rn, C.c_char), _p(an, C.c_char), _p(ai, i32),
+                         _p(pos, C.c_float), _p(vel, C.c_float), _p(box, C.c_float))
+    if r:
+        return None
+    dec = lambda row: bytes(row).split(b"\0", 1)[0].decode()
+    return dict(resd_index=ri, atom_index=ai, resd_name=[dec(x) for x in rn], atom_name=[dec(x) for x in an],
+                pos=pos, vel=vel, box=box)
+
+
+def ref_gro_write(path, title, resd_index, resd_name, atom_name, atom_index, pos, vel, box):
+    """The reference engine's GromacsFileManager::writeGroFile after `title`, from binary32 arrays."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libref_gro.so"))
+    lib.ref_gro_write.argtypes = [C.c_char_p, C.c_char_p, i32, P(i32), P(C.c_char), P(C.c_char), P(i32),
+                                  P(C.c_float), P(C.c_float), P(C.c_float)]
+    n = len(resd_index)
+    slots = lambda names: np.array([list(s.encode()[:7].ljust(8, b"\0")) for s in names], np.uint8).reshape(n, 8)
+    rn, an = slots(resd_name), slots(atom_name)
+    ri = np.ascontiguousarray(resd_index, np.int32); ai = np.ascontiguousarray(atom_index, np.int32)
+    p = np.ascontiguousarray(pos, np.float32); v = np.ascontiguousarray(vel, np.float32)
+    b = np.ascontiguousarray(box, np.float32)
+    return lib.ref_gro_write(str(path).encode(), title.encode(), n, _p(ri, i32), _p(rn, C.c_char), _p(an, C.c_char),
+                             _p(ai, i32), _p(p, C.c_float), _p(v, C.c_float), _p(b, C.c_float))

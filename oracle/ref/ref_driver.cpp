@@ -263,3 +263,44 @@ extern "C" int ref_spme_ana_errmap(const int* K, const double* box, double beta,
   return 0;
 }
 #endif
+
+#ifdef REF_GRO
+// GromacsFileManager::readGroFile / writeGroFile (ENG/src/GromacsFileManager.cpp)
+// with the engine's ScalorType (float) arrays; names in StringSize (8) slots.
+// Reading returns 0, or 1 when the reader threw (cannot open / wrong format).
+#include "GromacsFileManager.h"
+extern "C" int ref_gro_read(const char* path, int n, int* resd_index, char* resd_name, char* atom_name,
+                            int* atom_index, float* pos, float* vel, float* box) {
+  std::vector<IndexType> ri(n), ai(n);
+  std::vector<ScalorType> x(n), y(n), z(n), u(n), v(n), w(n);
+  try {
+    GromacsFileManager::readGroFile(path, ri.data(), resd_name, atom_name, ai.data(), x.data(), y.data(), z.data(),
+                                    u.data(), v.data(), w.data(), &box[0], &box[1], &box[2]);
+  } catch (...) {
+    return 1;
+  }
+  for (int i = 0; i < n; ++i) {
+    resd_index[i] = (int)ri[i]; atom_index[i] = (int)ai[i];
+    pos[3 * i] = x[i]; pos[3 * i + 1] = y[i]; pos[3 * i + 2] = z[i];
+    vel[3 * i] = u[i]; vel[3 * i + 1] = v[i]; vel[3 * i + 2] = w[i];
+  }
+  return 0;
+}
+extern "C" int ref_gro_write(const char* path, const char* title, int n, const int* resd_index,
+                             const char* resd_name, const char* atom_name, const int* atom_index, const float* pos,
+                             const float* vel, const float* box) {
+  FILE* fp = fopen(path, "w");
+  if (!fp) return 1;
+  fputs(title, fp);
+  std::vector<IndexType> ri(resd_index, resd_index + n), ai(atom_index, atom_index + n);
+  std::vector<ScalorType> x(n), y(n), z(n), u(n), v(n), w(n);
+  for (int i = 0; i < n; ++i) {
+    x[i] = pos[3 * i]; y[i] = pos[3 * i + 1]; z[i] = pos[3 * i + 2];
+    u[i] = vel[3 * i]; v[i] = vel[3 * i + 1]; w[i] = vel[3 * i + 2];
+  }
+  GromacsFileManager::writeGroFile(fp, n, ri.data(), resd_name, atom_name, ai.data(), x.data(), y.data(), z.data(),
+                                   u.data(), v.data(), w.data(), box[0], box[1], box[2]);
+  fclose(fp);
+  return 0;
+}
+#endif

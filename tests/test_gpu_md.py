@@ -252,3 +252,25 @@ def test_stream_ordered_stats_rows_match_blocking_reads(mdf, fluid):
         assert np.allclose(rows[k], b.stats(), rtol=1e-12, atol=1e-12)
     with pytest.raises(ValueError):
         a.stats_async(np.zeros(3))
+
+
+def test_system_from_gro_and_back(mdf, fluid, tmp_path):
+    # MDSystem::initConfig from a .gro file, a short run, writeHostDataGro
+    src = tmp_path / "start.gro"
+    mdf.write_gro(src, mdf.GroConf(fluid.pos, fluid.box, fluid.vel, atom_name=["lj"] * fluid.n,
+                                   resd_name=["lj"] * fluid.n), "start")
+    sys, conf = mdf.system_from_gro(src, precision=1)
+    assert np.array_equal(sys.positions(), conf.pos)
+    sys.set_rcut(np.full(sys.n, 2.5, np.float32))
+    eng = mdf.InteractionEngine(sys)
+    eng.registNonBondedInteraction(1.0, 1.0, 0.0)
+    lv = mdf.langevin_params(dt=0.005, temperature=1.0, gamma_t=0.5, seed=3)
+    sim = mdf.Simulation(sys, eng, skin=0.3, cell_size=2.8, lv=lv)
+    sim.run(20)
+    out = tmp_path / "confout.gro"
+    mdf.write_system_gro(out, sys, conf, step=20, time=0.1)
+    back = mdf.read_gro(out)
+    assert back.title == "# at time = 0.100000, step = 20"
+    assert back.atom_name == conf.atom_name
+    assert np.abs(back.pos - sys.positions()).max() < 5e-4 + 1e-4
+    assert np.abs(back.vel - sys.velocities()).max() < 5e-5 + 1e-5
