@@ -79,6 +79,7 @@ enum md_stat_slot {
   MD_STAT_PRESSURE_CORR_ZZ = 10,
   MD_STAT_ELEC_REC = 11,   /* reciprocal (SPME) energy       */
   MD_STAT_ELEC_SELF = 12,  /* -beta/sqrt(pi) sum q^2         */
+  MD_STAT_BOND_ENERGY = 13, /* mdStatisticBondedPotential: bonds and angles */
   MD_STAT_COUNT = 16
 };
 
@@ -204,13 +205,43 @@ int md_nlist_get(md_nlist* nl, md_system* sys, int32_t* counts, int32_t* pairs);
 int md_engine_create(md_engine** out, md_system* sys);
 int md_engine_destroy(md_engine* eng);
 int md_engine_register_lj(md_engine* eng, double epsilon, double sigma, double shift);
-/* registBondedInteraction: bonds, angles and exclusions are not part of this path;
-   returns MD_OK for n_bonds == 0 and MD_ERR_UNSUPPORTED otherwise. */
+/* Bonded terms (SystemBondedInteraction::reinit + BondedInteractionList,
+ * ENG/src/SystemBondedInteraction.cu:100-230; force functions ENG/include/BondInteraction.h:217-372,
+ * ENG/include/AngleInteraction.h:365-1216; kernels calBondInteraction / calAngleInteraction,
+ * ENG/src/InteractionEngine_interface.cu:1399-1775).  Atom indices are the original
+ * (md_system_create) order.  Parameters are [n][3] as the *Parameter classes take them:
+ *   MD_BOND_HARMONIC (k, r0):      F = k (1 - r0/r) d,     E = k/2 (r - r0)^2
+ *   MD_BOND_FENE (k, rinf):        F = k rinf^2/(rinf^2 - r^2) d,  E = -k/2 rinf^2 ln(1 - r^2/rinf^2)
+ *   MD_BOND_FENE2 (k, rs, r0):     the FENE form in r - r0 with range rs
+ *   MD_ANGLE_HARMONIC (k, theta0): E = k (theta - theta0)^2 (atoms edge0, centre, edge1)
+ *   MD_ANGLE_COS0 (k):             E = k (1 - cos(pi - theta))
+ * with d = r_partner - r_self under the minimum image.  Each atom gathers its own
+ * terms; the bonded energy goes to MD_STAT_BOND_ENERGY and the virial is added to the
+ * non-bonded one.  A later call replaces the earlier set of that kind. */
+enum md_bonded_type {
+  MD_BOND_HARMONIC = 10000,   /* mdForceHarmonicSpring */
+  MD_BOND_FENE = 10001,       /* mdForceFENE           */
+  MD_BOND_FENE2 = 10002,      /* mdForceFENE2          */
+  MD_ANGLE_HARMONIC = 20000,  /* mdForceAngleHarmonic  */
+  MD_ANGLE_COS0 = 20001       /* mdForceCosAngle0      */
+};
+int md_engine_set_bonds(md_engine* eng, int n, const int* atoms /* [n][2] */, const int* type,
+                        const double* param /* [n][3] */);
+int md_engine_set_angles(md_engine* eng, int n, const int* atoms /* [n][3] edge0, centre, edge1 */,
+                         const int* type, const double* param /* [n][3] */);
+/* Exclusions (ExclusionList, ENG/include/ExclusionList.h): excluded pairs take no
+   non-bonded force.  They are removed from the neighbour list after each build. */
+int md_engine_set_exclusions(md_engine* eng, int n, const int* pairs /* [n][2] */);
+/* the exclusion pass alone, for a list built before the exclusions were given */
+int md_nlist_apply_exclusions(md_nlist* nl, md_system* sys);
+/* registBondedInteraction: checks that n_bonds bonds were given to md_engine_set_bonds. */
 int md_engine_register_bonded(md_engine* eng, int n_bonds);
 int md_engine_clear_forces(md_engine* eng, md_system* sys);
 /* with_stats != 0 accumulates energy and diagonal virial into the FP64 slots. */
 int md_engine_apply_nonbonded(md_engine* eng, md_system* sys, md_nlist* nl, int with_stats);
-/* applyBondedInteraction: MD_OK with nothing to do when no bonds are registered. */
+/* applyBondedInteraction with statistics: adds the bonded forces to the system's forces
+   (after md_engine_apply_nonbonded), stores MD_STAT_BOND_ENERGY and adds the virial;
+   nothing to do without bonds or angles. */
 int md_engine_apply_bonded(md_engine* eng, md_system* sys);
 /* Real-space Ewald (ElectrostaticInteraction_dir, RE/src/EleDir.cpp:43-61) fused into
    the non-bonded kernel: E = 1/2 sum q_i q_j erfc(beta r)/r over the same list and

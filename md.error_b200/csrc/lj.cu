@@ -395,17 +395,12 @@ extern "C" int md_engine_set_force_correction(md_engine* e, md_fcorr* fc) {
 
 extern "C" int md_engine_register_bonded(md_engine* e, int n_bonds) {
   if (!e || n_bonds < 0) return MD_ERR_BADARG;
-  if (n_bonds > 0) {
-    md_set_error("bonded interactions are not part of this force path (%d bonds given)", n_bonds);
-    return MD_ERR_UNSUPPORTED;
+  if (n_bonds != e->n_bonds) {
+    md_set_error("registBondedInteraction: %d bonds expected, %d given to md_engine_set_bonds", n_bonds,
+                 e->n_bonds);
+    return MD_ERR_BADARG;
   }
-  e->n_bonds = 0;
   return MD_OK;
-}
-
-extern "C" int md_engine_apply_bonded(md_engine* e, md_system* sys) {
-  if (!e || !sys) return MD_ERR_BADARG;
-  return MD_OK;  // no bonded terms registered: nothing to add
 }
 
 extern "C" int md_engine_clear_forces(md_engine* e, md_system* sys) {

@@ -37,7 +37,7 @@ enum : unsigned {
 };
 
 // reduction counters (one per kind of last-block reduction)
-enum { RED_LJ = 0, RED_KIN = 1, RED_DISP = 2, RED_SPME = 3, RED_MISC = 4, RED_COUNT = 8 };
+enum { RED_LJ = 0, RED_KIN = 1, RED_DISP = 2, RED_SPME = 3, RED_MISC = 4, RED_BOND = 5 /* and 6 */, RED_COUNT = 8 };
 
 struct DevState {
   double L[3];       // box edge, FP64 master copy
@@ -82,6 +82,8 @@ inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 // box update on the host side copy
 void box_fill(DevState& s, const double L[3]);
 
+struct md_topo;  // bonded terms and exclusions by atom id (bonded.cu)
+
 struct md_system {
   int N = 0;
   int prec = MD_PREC_MIXED;
@@ -107,6 +109,9 @@ struct md_system {
   // pinned host staging
   void* h_stage = nullptr;
   size_t h_stage_bytes = 0;
+  // bonded topology (null when none); the version counts its changes
+  md_topo* topo = nullptr;
+  int topo_version = 0;
   // rc lattice (AssignRCut)
   float* d_lattice = nullptr;
   int lat_n[3] = {0, 0, 0};
@@ -180,6 +185,13 @@ int rec_launch(Recorder* r, const void* func, dim3 grid, dim3 block, size_t smem
 int cells_rebuild_impl(md_cell_list* cl, md_system* sys, Recorder* rec, bool conditional);
 int nlist_build_impl(md_nlist* nl, md_system* sys, md_cell_list* cl, Recorder* rec, bool conditional);
 int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats, bool overwrite, Recorder* rec);
+// bonded terms (bonded.cu): slot map refresh after a cell sort, exclusion pass
+// after a list build, the bonded force kernel; each a no-op without topology
+void topo_destroy(md_topo* t);
+bool topo_has_terms(const md_topo* t);
+int topo_slot_launch(md_system* sys, Recorder* rec, bool gated);
+int topo_exclude_launch(md_system* sys, md_nlist* nl, Recorder* rec, bool gated);
+int bonded_apply_impl(md_system* sys, Recorder* rec, int with_stats);
 int langevin_step1_impl(md_system* sys, md_nlist* nl, Recorder* rec, bool with_box_kernel,
                         cudaGraphConditionalHandle cond, int use_cond);
 // fadd: per-atom force of a concurrent branch (SPME), added into the force

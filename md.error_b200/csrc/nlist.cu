@@ -379,6 +379,7 @@ int nlist_build_impl(md_nlist* nl, md_system* sys, md_cell_list* cl, Recorder* r
     smem = NL_TILE_CAP * sizeof(float4);
   }
   if (int r = rec_launch(rec, f, grid, block, smem, a)) return r;
+  if (int r = topo_exclude_launch(sys, nl, rec, gated)) return r;
   nl->built = true;
   return MD_OK;
 }

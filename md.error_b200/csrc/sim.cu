@@ -37,6 +37,7 @@ struct md_sim {
   cudaGraphExec_t exec = nullptr;
   bool conditional = false;
   float* lattice_in_graph = nullptr;
+  int topo_in_graph = -1;
   int64_t steps = 0;
   md_nhc* nhc = nullptr;  // MD_INTEG_NHC
   bool nhc_settled = false;  // velocities / chain brought to the end of the last step
@@ -91,6 +92,7 @@ static int record_step(md_sim* s, Recorder* rec, bool use_graph) {
   const cudaGraphNode_t fork = rec->last;
   const bool fork_has = rec->has_last;
   if (int r = lj_apply_impl(s->eng, sys, s->nl, true, true, rec)) return r;
+  if (int r = bonded_apply_impl(sys, rec, 1)) return r;
   if (s->p.spme) {
     const cudaGraphNode_t lj = rec->last;
     if (branch && rec->graph) {
@@ -121,6 +123,7 @@ static int build_graph(md_sim* s) {
   if (int r = record_step(s, &g, true)) return r;
   MD_CUDA(cudaGraphInstantiate(&s->exec, s->graph, 0));
   s->lattice_in_graph = s->sys->d_lattice;
+  s->topo_in_graph = s->sys->topo_version;
   return MD_OK;
 }
 
@@ -240,7 +243,7 @@ extern "C" int md_sim_attach_adapt_rcut(md_sim* s, md_adapt_rcut* arc, int sampl
 extern "C" int md_sim_run(md_sim* s, int nsteps) {
   if (!s || nsteps < 0) return MD_ERR_BADARG;
   md_system* sys = s->sys;
-  if (s->exec && sys->d_lattice != s->lattice_in_graph)
+  if (s->exec && (sys->d_lattice != s->lattice_in_graph || sys->topo_version != s->topo_in_graph))
     if (int r = build_graph(s)) return r;
   if (s->nhc && s->nhc_settled && nsteps > 0) {
     // re-open the step the last run closed: COM removal + operator_L(dt/2)

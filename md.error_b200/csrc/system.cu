@@ -281,6 +281,7 @@ extern "C" int md_system_destroy(md_system* s) {
   void* ptrs[] = {s->pos, s->vel, s->force, s->image, s->id, s->rcut, s->t_pos, s->t_vel,
                   s->t_force, s->t_image, s->t_id, s->t_rcut, s->st, s->partials, s->d_lattice};
   for (void* p : ptrs) if (p) cudaFree(p);
+  topo_destroy(s->topo);
   if (s->h_stage) cudaFreeHost(s->h_stage);
   if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
   delete s;

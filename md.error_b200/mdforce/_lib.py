@@ -84,6 +84,10 @@ _SIGS = {
     "md_engine_clear_forces": (i32, [vp, vp]),
     "md_engine_apply_nonbonded": (i32, [vp, vp, vp, i32]),
     "md_engine_apply_bonded": (i32, [vp, vp]),
+    "md_engine_set_bonds": (i32, [vp, i32, P(i32), P(i32), P(f64)]),
+    "md_engine_set_angles": (i32, [vp, i32, P(i32), P(i32), P(f64)]),
+    "md_engine_set_exclusions": (i32, [vp, i32, P(i32)]),
+    "md_nlist_apply_exclusions": (i32, [vp, vp]),
     "md_assign_rcut": (i32, [vp, P(f32), i32, i32, i32]),
     "md_set_rcut_uniform": (i32, [vp, f32]),
     "md_vv_step1": (i32, [vp, f64]),

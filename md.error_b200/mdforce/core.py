@@ -42,6 +42,9 @@ STAT_ELEC_DIR = 4
 STAT_KINETIC_XX, STAT_KINETIC_YY, STAT_KINETIC_ZZ = 5, 6, 7
 STAT_PRESSURE_CORR_XX = 8
 STAT_ELEC_REC, STAT_ELEC_SELF = 11, 12
+STAT_BOND_ENERGY = 13
+BOND_HARMONIC, BOND_FENE, BOND_FENE2 = 10000, 10001, 10002
+ANGLE_HARMONIC, ANGLE_COS0 = 20000, 20001
 STAT_COUNT = 16
 
 
@@ -322,6 +325,38 @@ class InteractionEngine:
 
     def registBondedInteraction(self, n_bonds=0):
         check(lib.md_engine_register_bonded(self.h, int(n_bonds)), "registBondedInteraction")
+
+    @staticmethod
+    def _terms(atoms, types, params, width):
+        a = np.ascontiguousarray(atoms, np.int32).reshape(-1, width)
+        n = a.shape[0]
+        t = np.ascontiguousarray(np.broadcast_to(np.asarray(types, np.int32), (n,)))
+        p = np.zeros((n, 3))
+        if n:
+            q = np.asarray(params, np.float64)
+            q = np.broadcast_to(q, (n,) + q.shape[-1:]) if q.ndim == 1 else q.reshape(n, -1)
+            p[:, :q.shape[1]] = q
+        return a, t, p
+
+    def setBonds(self, atoms, types, params):
+        """Bonds [n, 2] (original atom order), types BOND_* and parameters as the
+        reference's HarmonicSpringParameter(k, r0) / FENEParameter(k, rinf) /
+        FENE2Parameter(k, rs, r0) take them ([n, <=3] or one row for all)."""
+        a, t, p = self._terms(atoms, types, params, 2)
+        check(lib.md_engine_set_bonds(self.h, a.shape[0], _p(a, C.c_int), _p(t, C.c_int), _p(p)), "setBonds")
+        self._bonds = (a, t, p)
+
+    def setAngles(self, atoms, types, params):
+        """Angles [n, 3] (edge0, centre, edge1), types ANGLE_* and parameters
+        AngleHarmonicParameter(k, theta0) / CosAngle0Parameter(k)."""
+        a, t, p = self._terms(atoms, types, params, 3)
+        check(lib.md_engine_set_angles(self.h, a.shape[0], _p(a, C.c_int), _p(t, C.c_int), _p(p)), "setAngles")
+        self._angles = (a, t, p)
+
+    def setExclusions(self, pairs):
+        """Pairs [n, 2] that take no non-bonded force (ExclusionList)."""
+        a = np.ascontiguousarray(pairs, np.int32).reshape(-1, 2)
+        check(lib.md_engine_set_exclusions(self.h, a.shape[0], _p(a, C.c_int)), "setExclusions")
 
     def clearInteraction(self, sys=None):
         check(lib.md_engine_clear_forces(self.h, (sys or self.sys).h), "clearInteraction")

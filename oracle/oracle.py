@@ -593,6 +593,10 @@ _sigs3 = {
     "orc_spme_selfcorr": (None, [i32, P(f64), P(f64), P(f64), P(i32), i32, f64, P(f64)]),
     "orc_spme_ik_errmap": (None, [P(i32), P(f64), f64, i32, P(f64), P(f64), f64, P(f64), P(f64)]),
     "orc_dir_errmap": (None, [P(i32), P(f64), f64, f64, P(f64), P(f64), f64, P(f64), P(f64)]),
+    "orc_bond_term": (None, [i32, P(f64), i32, P(f64), P(f64), P(f64)]),
+    "orc_angle_term": (None, [i32, P(f64), i32, P(f64), P(f64), P(f64), P(f64), P(f64)]),
+    "orc_bonded_apply": (None, [i32, P(f64), P(f64), i32, i32, P(i32), P(i32), P(f64), i32, P(i32), P(i32),
+                                P(f64), P(f64), P(f64)]),
     "orc_spme_ana_errmap": (None, [P(i32), P(f64), f64, i32, P(f64), P(f64), f64, P(f64), P(f64),
                                    P(f64), P(f64)]),
     "orc_dft3d": (None, [P(i32), P(f64), i32]),
@@ -707,3 +711,49 @@ def ref_gro_write(path, title, resd_index, resd_name, atom_name, atom_index, pos
     b = np.ascontiguousarray(box, np.float32)
     return lib.ref_gro_write(str(path).encode(), title.encode(), n, _p(ri, i32), _p(rn, C.c_char), _p(an, C.c_char),
                              _p(ai, i32), _p(p, C.c_float), _p(v, C.c_float), _p(b, C.c_float))
+
+
+def bond_term(btype, uparam, prec, d):
+    """Force on the reference atom and energy of one bond term (oracle_bonded.c)."""
+    u = np.zeros(3); u[:len(uparam)] = uparam
+    dd = np.ascontiguousarray(d, np.float64); f = np.zeros(3); e = C.c_double()
+    _lib.orc_bond_term(int(btype), _p(u, f64), int(prec), _p(dd, f64), _p(f, f64), C.byref(e))
+    return f, e.value
+
+
+def angle_term(atype, uparam, prec, d0, d1):
+    """forcePoten01 of one angle term (oracle_bonded.c): f0, f1, energy."""
+    u = np.zeros(3); u[:len(uparam)] = uparam
+    a = np.ascontiguousarray(d0, np.float64); b = np.ascontiguousarray(d1, np.float64)
+    f0 = np.zeros(3); f1 = np.zeros(3); e = C.c_double()
+    _lib.orc_angle_term(int(atype), _p(u, f64), int(prec), _p(a, f64), _p(b, f64), _p(f0, f64), _p(f1, f64),
+                        C.byref(e))
+    return f0, f1, e.value
+
+
+def bonded_apply(pos, box, prec, bonds, btype, bparam, angles, atype, aparam):
+    """The engine's per-atom bonded gather (oracle_bonded.c): forces [n, 3] in
+    original order and (energy, virial xx, yy, zz)."""
+    p = np.ascontiguousarray(pos, np.float64); b = np.ascontiguousarray(box, np.float64)
+    n = p.shape[0]
+    bo = np.ascontiguousarray(bonds, np.int32).reshape(-1, 2); bt = np.ascontiguousarray(btype, np.int32)
+    bp = np.zeros((len(bo), 3)); bp[:, :np.shape(bparam)[1] if len(bo) else 0] = bparam if len(bo) else 0
+    an = np.ascontiguousarray(angles, np.int32).reshape(-1, 3); at = np.ascontiguousarray(atype, np.int32)
+    ap = np.zeros((len(an), 3)); ap[:, :np.shape(aparam)[1] if len(an) else 0] = aparam if len(an) else 0
+    f = np.zeros((n, 3)); st = np.zeros(4)
+    _lib.orc_bonded_apply(n, _p(p, f64), _p(b, f64), int(prec), len(bo), _p(bo, i32), _p(bt, i32), _p(bp, f64),
+                          len(an), _p(an, i32), _p(at, i32), _p(ap, f64), _p(f, f64), _p(st, f64))
+    return f, st
+
+
+def ref_bonded_term(ftype, uparam, d0, d1=None):
+    """The reference's own bond / angle force functions (oracle/_ref/libref_bonded.so,
+    binary32): bond -> (f, e); angle (forcePoten01) -> (f0, f1, e)."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libref_bonded.so"))
+    lib.ref_bonded_term.argtypes = [i32, P(f64), P(f64), P(f64), P(f64), P(f64), P(f64)]
+    u = np.zeros(3); u[:len(uparam)] = uparam
+    a = np.ascontiguousarray(d0, np.float64)
+    b = np.zeros(3) if d1 is None else np.ascontiguousarray(d1, np.float64)
+    f0 = np.zeros(3); f1 = np.zeros(3); e = np.zeros(1)
+    lib.ref_bonded_term(int(ftype), _p(u, f64), _p(a, f64), _p(b, f64), _p(f0, f64), _p(f1, f64), _p(e, f64))
+    return (f0, float(e[0])) if d1 is None else (f0, f1, float(e[0]))

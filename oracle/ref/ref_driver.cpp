@@ -304,3 +304,36 @@ extern "C" int ref_gro_write(const char* path, const char* title, int n, const i
   return 0;
 }
 #endif
+
+#ifdef REF_BONDED
+// The engine's bond and angle force functions (include/BondInteraction.h,
+// include/AngleInteraction.h) evaluated on the host in binary32: one term for
+// the given parameters (as the *Parameter classes take them) and difference
+// vectors.  Bonds give the force on the reference atom; angles forcePoten01.
+#include "BondInteraction.h"
+#include "AngleInteraction.h"
+extern "C" int ref_bonded_term(int ftype, const double* u, const double* d0, const double* d1, double* f0,
+                               double* f1, double* e) {
+  ScalorType p[3] = {0, 0, 0};
+  ScalorType a0 = (ScalorType)d0[0], a1 = (ScalorType)d0[1], a2 = (ScalorType)d0[2];
+  ScalorType b0 = (ScalorType)d1[0], b1 = (ScalorType)d1[1], b2 = (ScalorType)d1[2];
+  ScalorType g0[3] = {0, 0, 0}, g1[3] = {0, 0, 0}, dp = 0;
+  switch (ftype) {
+    case mdForceHarmonicSpring: HarmonicSpring::initParameter(p, (ScalorType)u[0], (ScalorType)u[1]); break;
+    case mdForceFENE: FENE::initParameter(p, (ScalorType)u[0], (ScalorType)u[1]); break;
+    case mdForceFENE2: FENE2::initParameter(p, (ScalorType)u[0], (ScalorType)u[1], (ScalorType)u[2]); break;
+    case mdForceAngleHarmonic: AngleHarmonic::initParameter(p, (ScalorType)u[0], (ScalorType)u[1]); break;
+    case mdForceCosAngle0: CosAngle0::initParameter(p, (ScalorType)u[0]); break;
+    default: return 1;
+  }
+  if (ftype < mdForceAngleHarmonic) {
+    bondForcePoten((InteractionType)ftype, p, a0, a1, a2, &g0[0], &g0[1], &g0[2], &dp);
+  } else {
+    angleForcePoten(false, (InteractionType)ftype, p, a0, a1, a2, b0, b1, b2, &g0[0], &g0[1], &g0[2], &g1[0],
+                    &g1[1], &g1[2], &dp);
+  }
+  for (int k = 0; k < 3; ++k) { f0[k] = g0[k]; f1[k] = g1[k]; }
+  *e = dp;
+  return 0;
+}
+#endif
