@@ -127,6 +127,9 @@ int md_system_get_rcut(md_system* sys, float* rcut);
 /* Wrap every atom into [0,L) and update its image counters
    (normalizeSystem, ENG/src/BoxGeometry.cu:6-50). */
 int md_system_normalize(md_system* sys);
+/* atom types [N] in original order, 0 <= type < 16 (MDSystem hdata.type); 0 unless given */
+int md_system_set_types(md_system* sys, const int* type);
+int md_system_get_types(md_system* sys, int* type);
 /* FP64 statistic slots (MDStatistic::updateHost); out has MD_STAT_COUNT entries. */
 int md_system_read_stats(md_system* sys, double* out);
 /* The same slots copied to out in stream order without waiting (out should be
@@ -205,6 +208,14 @@ int md_nlist_get(md_nlist* nl, md_system* sys, int32_t* counts, int32_t* pairs);
 int md_engine_create(md_engine** out, md_system* sys);
 int md_engine_destroy(md_engine* eng);
 int md_engine_register_lj(md_engine* eng, double epsilon, double sigma, double shift);
+/* Several atom types (SystemNonBondedInteraction::add(t0, t1, LennardJones6_12Parameter)
+ * with AtomNBForceTable::calForceIndex, ENG/include/NonBondedInteraction.h:673-683, and the
+ * nbForce dispatch of ENG/include/NonBondedInteraction.h:469-495): LJ parameters for the
+ * unordered pair (t0, t1), 0 <= t < 16.  Once a pair is given the non-bonded kernels look up
+ * every pair's parameters by the two atoms' types, and pairs never given take no force and
+ * no energy (mdForceNULL); md_engine_register_lj is then ignored.  The cutoff stays the
+ * per-atom rcut_i.  Atom types come from md_system_create or md_system_set_types. */
+int md_engine_register_lj_pair(md_engine* eng, int t0, int t1, double epsilon, double sigma, double shift);
 /* Bonded terms (SystemBondedInteraction::reinit + BondedInteractionList,
  * ENG/src/SystemBondedInteraction.cu:100-230; force functions ENG/include/BondInteraction.h:217-372,
  * ENG/include/AngleInteraction.h:365-1216; kernels calBondInteraction / calAngleInteraction,

@@ -272,6 +272,7 @@ int cells_rebuild_impl(md_cell_list* cl, md_system* sys, Recorder* rec, bool gat
   int r = (sys->prec == MD_PREC_FP64) ? rebuild_t<double>(cl, sys, rec, gated)
                                       : rebuild_t<float>(cl, sys, rec, gated);
   if (r == MD_OK) r = topo_slot_launch(sys, rec, gated);  // ids moved: refresh the slot map
+  if (r == MD_OK) r = types_slot_launch(sys, rec, gated);  // and the per-slot types
   if (r == MD_OK) cl->built = true;
   return r;
 }

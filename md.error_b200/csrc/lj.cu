@@ -13,6 +13,7 @@
 // virial (1/2 sum over the full list, as the reference's per-atom buffers)
 // are block-reduced in FP64 and finished by the last block in a fixed order.
 #include <cmath>
+#include <vector>
 #include "device_common.cuh"
 
 // LJ 6-12 parameters and the real-space Ewald splitting (EleDir::
@@ -99,10 +100,11 @@ struct MixedAcc {
 // indexed by the entry's six image bits; the table holds the binary32
 // products k_d * L_d (exactly -L_d, +0 or L_d), so d - shift is the same
 // binary32 operation as shortestImage's x -= floorf(x/L + 0.5) L.
-template <int U, bool TAIL, bool STATS, bool COUL>
+template <int U, bool TAIL, bool STATS, bool COUL, bool TYPES>
 __device__ __forceinline__ void lj_pass_mixed(const int4 e4, int nvalid, const float4* __restrict__ pos, int i,
                                               const float4& pi, float rc2, const float4* shift,
-                                              const LJParams& p, MixedAcc& a) {
+                                              const LJParams& p, MixedAcc& a, const uint8_t* __restrict__ type,
+                                              const float4* tab) {
   static_assert(U == 4, "one int4 of list entries per pass");
   int ee[U] = {e4.x, e4.y, e4.z, e4.w};
   float4 pj[U];
@@ -113,6 +115,13 @@ __device__ __forceinline__ void lj_pass_mixed(const int4 e4, int nvalid, const f
 #pragma unroll
   // -1 marks "past the end" (a packed entry never has all six image bits set)
   for (int u = 0; u < U; ++u) pj[u] = __ldg(pos + ((!TAIL || ee[u] != -1) ? (ee[u] & 0x03FFFFFF) : i));
+  // typed: the pair's (4 eps, sigma^2, shift) from the block's table row of
+  // type i (tab points at that row); the j types gathered beside the positions
+  int tj[U];
+  if (TYPES) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) tj[u] = __ldg(type + ((!TAIL || ee[u] != -1) ? (ee[u] & 0x03FFFFFF) : i));
+  }
   // the U pair forces of this pass are summed in FP32, the pass sum is added
   // to the lane's Kahan-compensated accumulator
   float bx = 0.f, by = 0.f, bz = 0.f;
@@ -124,11 +133,12 @@ __device__ __forceinline__ void lj_pass_mixed(const int4 e4, int nvalid, const f
     const float dz = __fsub_rn(__fsub_rn(pj[u].z, pi.z), sh.z);
     const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
     if ((!TAIL || ee[u] != -1) && r2 < rc2) {
+      const float4 pp = TYPES ? tab[tj[u]] : make_float4(p.eps4f, p.sig2f, p.shiftf, 0.f);
       const float ri2 = __fdividef(1.0f, r2);
-      const float s2 = p.sig2f * ri2;
+      const float s2 = pp.y * ri2;
       const float s6 = s2 * s2 * s2;
       // 4 eps (6 s^6 - 12 s^12) / r^2 = (4 eps / r^2) s^6 (6 - 12 s^6)
-      float fs = (p.eps4f * ri2) * s6 * fmaf(-12.f, s6, 6.f);
+      float fs = (pp.x * ri2) * s6 * fmaf(-12.f, s6, 6.f);
       if (COUL) {
         const float qq = pi.w * pj[u].w;
         const float rinv = rsqrtf(r2);
@@ -140,7 +150,7 @@ __device__ __forceinline__ void lj_pass_mixed(const int4 e4, int nvalid, const f
       by += fs * dy;
       bz += fs * dz;
       if (STATS) {
-        a.e += fmaf(p.eps4f, fmaf(s6, s6, -s6), p.shiftf);
+        a.e += fmaf(pp.x, fmaf(s6, s6, -s6), pp.z);
         a.vx += fs * dx * dx;
         a.vy += fs * dy * dy;
         a.vz += fs * dz * dz;
@@ -152,13 +162,13 @@ __device__ __forceinline__ void lj_pass_mixed(const int4 e4, int nvalid, const f
   a.fz.add(bz);
 }
 
-template <int G, bool STATS, bool COUL>
-__global__ void __launch_bounds__(256, COUL ? 4 : 5)
+template <int G, bool STATS, bool COUL, bool TYPES>
+__global__ void __launch_bounds__(256, (COUL || TYPES) ? 4 : 5)
 k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut,
            const int* __restrict__ list, const int* __restrict__ nnb, int cap,
            const DevState* __restrict__ st, LJParams p, double4a* __restrict__ force, int overwrite,
            double* partials, unsigned* counter, double* stats, const double4a* __restrict__ corr,
-           const int* __restrict__ id) {
+           const int* __restrict__ id, const uint8_t* __restrict__ type, const void* __restrict__ ptab, int nt) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = t / G;
   const int lane = t & (G - 1);
@@ -170,10 +180,14 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
                            __fmul_rn((float)((int)((c >> 2) & 3u) - 1), st->Lf[1]),
                            __fmul_rn((float)((int)(c >> 4) - 1), st->Lf[2]), 0.f);
   }
+  __shared__ float4 tab[TYPES ? MD_MAX_TYPES * MD_MAX_TYPES : 1];
+  if (TYPES)
+    for (int c = threadIdx.x; c < nt * nt; c += blockDim.x) tab[c] = reinterpret_cast<const float4*>(ptab)[c];
   __syncthreads();
   MixedAcc a;
   if (i < N) {
     const float4 pi = pos[i];
+    const float4* trow = TYPES ? tab + nt * (int)type[i] : tab;
     const float rc = rcut[i];
     const float rc2 = __fmul_rn(rc, rc);
     int n = nnb[i];
@@ -199,8 +213,8 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
         const int4 cur = load_list4(row4 + q * G + lane);
 #endif
         const int rem = n - (32 * q + lane);  // entry u is inside the row when 8u < rem
-        if (rem > 24) lj_pass_mixed<4, false, STATS, COUL>(cur, rem, pos, i, pi, rc2, shift, p, a);
-        else if (rem > 0) lj_pass_mixed<4, true, STATS, COUL>(cur, rem, pos, i, pi, rc2, shift, p, a);
+        if (rem > 24) lj_pass_mixed<4, false, STATS, COUL, TYPES>(cur, rem, pos, i, pi, rc2, shift, p, a, type, trow);
+        else if (rem > 0) lj_pass_mixed<4, true, STATS, COUL, TYPES>(cur, rem, pos, i, pi, rc2, shift, p, a, type, trow);
 #if MD_LJ_PREFETCH
         cur = nxt;
 #endif
@@ -225,13 +239,20 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
 }
 
 // ---------------------------------------------------------------- FP64
-template <int G, bool STATS, bool COUL>
+template <int G, bool STATS, bool COUL, bool TYPES>
 __global__ void __launch_bounds__(256)
 k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcut,
           const int* __restrict__ list, const int* __restrict__ nnb, int cap,
           const DevState* __restrict__ st, LJParams p, double4a* __restrict__ force, int overwrite,
           double* partials, unsigned* counter, double* stats, const double4a* __restrict__ corr,
-          const int* __restrict__ id) {
+          const int* __restrict__ id, const uint8_t* __restrict__ type, const void* __restrict__ ptab, int nt) {
+  __shared__ double4a tab[TYPES ? MD_MAX_TYPES * MD_MAX_TYPES : 1];
+  if (TYPES) {
+    const double4a* src = reinterpret_cast<const double4a*>(reinterpret_cast<const float4*>(ptab) +
+                                                            MD_MAX_TYPES * MD_MAX_TYPES);
+    for (int c = threadIdx.x; c < nt * nt; c += blockDim.x) tab[c] = src[c];
+    __syncthreads();
+  }
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = t / G;
   const int lane = t & (G - 1);
@@ -271,10 +292,12 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
       const double dz = __dsub_rn(__dsub_rn(pj.z, pi.z), __dmul_rn(kz, L2));
       const double r2 = dx * dx + dy * dy + dz * dz;
       if (jj[u] != -1 && r2 < rc2) {
+        const double4a pp = TYPES ? tab[nt * (int)type[i] + (int)type[jj[u] & 0x03FFFFFF]]
+                                  : double4a{p.eps4, p.sig2, p.shift, 0.0};
         const double ri2 = 1.0 / r2;
-        const double s2 = p.sig2 * ri2;
+        const double s2 = pp.y * ri2;
         const double s6 = s2 * s2 * s2;
-        double fs = p.eps4 * (6.0 * s6 - 12.0 * s6 * s6) * ri2;
+        double fs = pp.x * (6.0 * s6 - 12.0 * s6 * s6) * ri2;
         if (COUL) {
           const double qq = pi.w * pj.w;
           const double r = sqrt(r2);
@@ -286,7 +309,7 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
         fy += fs * dy;
         fz += fs * dz;
         if (STATS) {
-          e += p.eps4 * (s6 * s6 - s6) + p.shift;
+          e += pp.x * (s6 * s6 - s6) + pp.z;
           vx += fs * dx * dx;
           vy += fs * dy * dy;
           vz += fs * dz * dz;
@@ -342,16 +365,44 @@ int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats,
   unsigned* counter = &st->red_counter[RED_LJ];
   double* stats = &st->stats[MD_STAT_NB_ENERGY];
   const double4a* corr = fcorr_values(eng->fcorr);
-  void* a[] = {&N, &sys->pos, &sys->rcut, &nl->list, &nl->nnb, &cap, &st, &p, &sys->force, &ow,
-               &sys->partials, &counter, &stats, &corr, &sys->id};
-  const void* f;
-  if (sys->prec == MD_PREC_FP64) {
-    if (coul) f = with_stats ? (const void*)k_lj_fp64<kLanes, true, true> : (const void*)k_lj_fp64<kLanes, false, true>;
-    else f = with_stats ? (const void*)k_lj_fp64<kLanes, true, false> : (const void*)k_lj_fp64<kLanes, false, false>;
-  } else {
-    if (coul) f = with_stats ? (const void*)k_lj_mixed<kLanes, true, true> : (const void*)k_lj_mixed<kLanes, false, true>;
-    else f = with_stats ? (const void*)k_lj_mixed<kLanes, true, false> : (const void*)k_lj_mixed<kLanes, false, false>;
+  // typed pairs: the (4 eps, sigma^2, shift) table, binary32 then binary64 rows
+  const bool typed = eng->nt > 0;
+  int nt = eng->nt;
+  if (typed) {
+    if (sys->ntypes > nt) {
+      md_set_error("the system has atom types up to %d, the interaction table covers %d", sys->ntypes - 1, nt);
+      return MD_ERR_BADARG;
+    }
+    if (eng->tab_dirty || !eng->d_tab) {
+      const size_t nf = MD_MAX_TYPES * MD_MAX_TYPES;
+      if (!eng->d_tab) MD_CUDA(cudaMalloc(&eng->d_tab, nf * (sizeof(float4) + sizeof(double4a))));
+      std::vector<float4> tf(nf);
+      std::vector<double4a> td(nf);
+      for (int a0 = 0; a0 < nt; ++a0)
+        for (int a1 = 0; a1 < nt; ++a1) {
+          const double* q = eng->lj_pair[a0][a1];
+          const double e4 = eng->lj_pair_set[a0][a1] ? 4.0 * q[0] : 0.0, s2 = q[1] * q[1];
+          const double sh = eng->lj_pair_set[a0][a1] ? q[2] : 0.0;
+          tf[a0 * nt + a1] = make_float4((float)e4, (float)s2, (float)sh, 0.f);
+          td[a0 * nt + a1] = double4a{e4, s2, sh, 0.0};
+        }
+      MD_CUDA(cudaMemcpy(eng->d_tab, tf.data(), nf * sizeof(float4), cudaMemcpyHostToDevice));
+      MD_CUDA(cudaMemcpy(reinterpret_cast<char*>(eng->d_tab) + nf * sizeof(float4), td.data(),
+                         nf * sizeof(double4a), cudaMemcpyHostToDevice));
+      eng->tab_dirty = false;
+    }
   }
+  const uint8_t* type = sys->type;
+  const void* ptab = eng->d_tab;
+  void* a[] = {&N, &sys->pos, &sys->rcut, &nl->list, &nl->nnb, &cap, &st, &p, &sys->force, &ow,
+               &sys->partials, &counter, &stats, &corr, &sys->id, &type, &ptab, &nt};
+  const void* f;
+#define LJ_PICK(K, T)                                                                       \
+  (coul ? (with_stats ? (const void*)K<kLanes, true, true, T> : (const void*)K<kLanes, false, true, T>) \
+        : (with_stats ? (const void*)K<kLanes, true, false, T> : (const void*)K<kLanes, false, false, T>))
+  if (sys->prec == MD_PREC_FP64) f = typed ? LJ_PICK(k_lj_fp64, true) : LJ_PICK(k_lj_fp64, false);
+  else f = typed ? LJ_PICK(k_lj_mixed, true) : LJ_PICK(k_lj_mixed, false);
+#undef LJ_PICK
   return rec_launch(rec, f, grid, dim3(threads), 0, a);
 }
 
@@ -374,7 +425,33 @@ extern "C" int md_engine_create(md_engine** out, md_system* sys) {
 }
 
 extern "C" int md_engine_destroy(md_engine* e) {
+  if (e && e->d_tab) cudaFree(e->d_tab);
   delete e;
+  return MD_OK;
+}
+
+// SystemNonBondedInteraction::add(type0, type1, LennardJones6_12Parameter(eps, sigma, shift, rc))
+// with AtomNBForceTable::calForceIndex (ENG/include/NonBondedInteraction.h:673-683): one
+// parameter set per unordered type pair; pairs never given interact with nothing
+// (mdForceNULL).  The cutoff stays the per-atom rcut_i.
+extern "C" int md_engine_register_lj_pair(md_engine* e, int t0, int t1, double eps, double sigma, double shift) {
+  if (!e || t0 < 0 || t1 < 0 || t0 >= MD_MAX_TYPES || t1 >= MD_MAX_TYPES || !(eps >= 0) || !(sigma > 0) ||
+      !std::isfinite(shift)) {
+    md_set_error("md_engine_register_lj_pair: bad arguments (types 0..%d, eps >= 0, sigma > 0)", MD_MAX_TYPES - 1);
+    return MD_ERR_BADARG;
+  }
+  for (int k = 0; k < 2; ++k) {
+    const int a = k ? t1 : t0, b = k ? t0 : t1;
+    e->lj_pair[a][b][0] = eps;
+    e->lj_pair[a][b][1] = sigma;
+    e->lj_pair[a][b][2] = shift;
+    e->lj_pair_set[a][b] = true;
+  }
+  const int need = (t0 > t1 ? t0 : t1) + 1;
+  if (need > e->nt) e->nt = need;
+  e->has_lj = true;
+  e->tab_dirty = true;
+  if (e->sys) e->sys->topo_version += 1;  // a recorded step graph picks the typed kernel up
   return MD_OK;
 }
 

@@ -109,6 +109,11 @@ struct md_system {
   // pinned host staging
   void* h_stage = nullptr;
   size_t h_stage_bytes = 0;
+  // atom types (TypeType of the reference): by original id and by current
+  // slot (refreshed by every cell sort); 0 for every atom unless given
+  uint8_t* type_by_id = nullptr;
+  uint8_t* type = nullptr;
+  int ntypes = 1;
   // bonded topology (null when none); the version counts its changes
   md_topo* topo = nullptr;
   int topo_version = 0;
@@ -163,6 +168,13 @@ struct md_engine {
   md_system* sys = nullptr;
   bool has_lj = false;
   double eps = 1, sigma = 1, shift = 0;
+  // per type pair LJ (SystemNonBondedInteraction::add / AtomNBForceTable):
+  // nt > 0 selects the typed kernels; pairs not given take no force
+  int nt = 0;
+  double lj_pair[16][16][3] = {};  // eps, sigma, shift (symmetric)
+  bool lj_pair_set[16][16] = {};
+  void* d_tab = nullptr;           // float4 [nt*nt] then double4a [nt*nt] (eps4, sig2, shift)
+  bool tab_dirty = false;
   bool has_coul = false;
   double beta = 0;
   int n_bonds = 0;
@@ -190,6 +202,9 @@ int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats,
 void topo_destroy(md_topo* t);
 bool topo_has_terms(const md_topo* t);
 int topo_slot_launch(md_system* sys, Recorder* rec, bool gated);
+// per-slot atom types from the per-id ones after a sort (system.cu)
+int types_slot_launch(md_system* sys, Recorder* rec, bool gated);
+constexpr int MD_MAX_TYPES = 16;
 int topo_exclude_launch(md_system* sys, md_nlist* nl, Recorder* rec, bool gated);
 int bonded_apply_impl(md_system* sys, Recorder* rec, int with_stats);
 int langevin_step1_impl(md_system* sys, md_nlist* nl, Recorder* rec, bool with_box_kernel,

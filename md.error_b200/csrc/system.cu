@@ -5,6 +5,7 @@
 #include <cstdarg>
 #include <cmath>
 #include <cstring>
+#include <vector>
 #include "device_common.cuh"
 
 static thread_local char g_err[1024] = "no error";
@@ -203,11 +204,60 @@ static int ensure_stage(md_system* s, size_t bytes) {
   return MD_OK;
 }
 
+__global__ void k_type_slot(int N, const int* __restrict__ id, const uint8_t* __restrict__ by_id,
+                            uint8_t* __restrict__ by_slot, const DevState* st, int gate) {
+  if (gate && !(st->flags & FLAG_REBUILD)) return;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < N) by_slot[k] = by_id[id[k]];
+}
+
+int types_slot_launch(md_system* sys, Recorder* rec, bool gated) {
+  if (sys->ntypes <= 1) return MD_OK;  // every slot holds type 0
+  int N = sys->N, gate = gated ? 1 : 0;
+  void* a[] = {&N, &sys->id, &sys->type_by_id, &sys->type, &sys->st, &gate};
+  return rec_launch(rec, (const void*)k_type_slot, dim3(ceil_div(N, 256)), dim3(256), 0, a);
+}
+
+extern "C" int md_system_set_types(md_system* s, const int* type) {
+  if (!s || !type) return MD_ERR_BADARG;
+  int nt = 1;
+  for (int i = 0; i < s->N; ++i) {
+    if (type[i] < 0 || type[i] >= MD_MAX_TYPES) {
+      md_set_error("md_system_set_types: atom %d has type %d (0 <= type < %d)", i, type[i], MD_MAX_TYPES);
+      return MD_ERR_BADARG;
+    }
+    if (type[i] + 1 > nt) nt = type[i] + 1;
+  }
+  std::vector<uint8_t> t8(type, type + s->N);
+  MD_CUDA(cudaSetDevice(s->device));
+  MD_CUDA(cudaMemcpyAsync(s->type_by_id, t8.data(), s->N, cudaMemcpyHostToDevice, s->stream));
+  s->ntypes = nt;
+  k_type_slot<<<ceil_div(s->N, 256), 256, 0, s->stream>>>(s->N, s->id, s->type_by_id, s->type, s->st, 0);
+  MD_CHECK_LAUNCH("types");
+  MD_CUDA(cudaStreamSynchronize(s->stream));
+  s->topo_version += 1;
+  return MD_OK;
+}
+
+extern "C" int md_system_get_types(md_system* s, int* type) {
+  if (!s || !type) return MD_ERR_BADARG;
+  std::vector<uint8_t> t8(s->N);
+  MD_CUDA(cudaMemcpyAsync(t8.data(), s->type_by_id, s->N, cudaMemcpyDeviceToHost, s->stream));
+  MD_CUDA(cudaStreamSynchronize(s->stream));
+  for (int i = 0; i < s->N; ++i) type[i] = t8[i];
+  return MD_OK;
+}
+
 extern "C" int md_system_create(md_system** out, int n, const double box[3], const double* pos,
                                 const double* vel, const int* type, const double* charge,
                                 const double* mass, int precision, int device) {
-  (void)type;
   if (!out || n <= 0 || !box || !pos) { md_set_error("md_system_create: bad arguments"); return MD_ERR_BADARG; }
+  if (type)
+    for (int i = 0; i < n; ++i)
+      if (type[i] < 0 || type[i] >= MD_MAX_TYPES) {
+        md_set_error("md_system_create: atom %d has type %d (0 <= type < %d)", i, type[i], MD_MAX_TYPES);
+        return MD_ERR_BADARG;
+      }
   if (precision != MD_PREC_MIXED && precision != MD_PREC_FP64) { md_set_error("bad precision %d", precision); return MD_ERR_BADARG; }
   for (int d = 0; d < 3; ++d)
     if (!(box[d] > 0) || !std::isfinite(box[d])) { md_set_error("md_system_create: bad box"); return MD_ERR_BADARG; }
@@ -240,6 +290,7 @@ extern "C" int md_system_create(md_system** out, int n, const double box[3], con
   ALLOC(s->st, sizeof(DevState));
   s->max_partial_blocks = ceil_div((long long)n * 32, 128) + 1024;
   ALLOC(s->partials, sizeof(double) * 8 * (size_t)s->max_partial_blocks);
+  ALLOC(s->type_by_id, (size_t)n); ALLOC(s->type, (size_t)n);
 #undef ALLOC
   DevState hs;
   memset(&hs, 0, sizeof(hs));
@@ -266,9 +317,14 @@ extern "C" int md_system_create(md_system** out, int n, const double box[3], con
     k_upload<double><<<nb, 256, 0, s->stream>>>(n, dpos, pv, pq, pm, (double4a*)s->pos, (double4a*)s->vel, s->id, s->image, s->force, s->rcut);
   else
     k_upload<float><<<nb, 256, 0, s->stream>>>(n, dpos, pv, pq, pm, (float4*)s->pos, (float4*)s->vel, s->id, s->image, s->force, s->rcut);
+  cudaMemsetAsync(s->type_by_id, 0, (size_t)n, s->stream);
+  cudaMemsetAsync(s->type, 0, (size_t)n, s->stream);
   cudaError_t e = cudaStreamSynchronize(s->stream);
   cudaFree(dbuf);
   if (e != cudaSuccess) return fail(md_cuda_fail(e, "upload"));
+  if (type)
+    if (int r = md_system_set_types(s, type)) return fail(r);
+  s->topo_version = 0;
   rc = MD_OK;
   *out = s;
   return rc;
@@ -279,7 +335,8 @@ extern "C" int md_system_destroy(md_system* s) {
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   void* ptrs[] = {s->pos, s->vel, s->force, s->image, s->id, s->rcut, s->t_pos, s->t_vel,
-                  s->t_force, s->t_image, s->t_id, s->t_rcut, s->st, s->partials, s->d_lattice};
+                  s->t_force, s->t_image, s->t_id, s->t_rcut, s->st, s->partials, s->d_lattice,
+                  s->type_by_id, s->type};
   for (void* p : ptrs) if (p) cudaFree(p);
   topo_destroy(s->topo);
   if (s->h_stage) cudaFreeHost(s->h_stage);

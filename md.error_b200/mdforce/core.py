@@ -116,7 +116,7 @@ def device_count():
 class MDSystem:
     """Per-atom SoA on the device (MDSystem / DeviceMDData)."""
 
-    def __init__(self, pos, box, vel=None, charge=None, mass=None, precision=PREC_MIXED, device=0):
+    def __init__(self, pos, box, vel=None, charge=None, mass=None, precision=PREC_MIXED, device=0, type=None):
         pos = _f64(pos).reshape(-1, 3)
         self.n = pos.shape[0]
         box = _f64(box, (3,))
@@ -131,7 +131,12 @@ class MDSystem:
                 a = _f64(arr).reshape(shape)
                 keep.append(a)
                 args.append(_p(a))
-        args.append(None)  # type
+        if type is None:
+            args.append(None)
+        else:
+            t = np.ascontiguousarray(type, np.int32).reshape(-1)
+            keep.append(t)
+            args.append(_p(t, C.c_int))
         for arr in (charge, mass):
             if arr is None:
                 args.append(None)
@@ -153,6 +158,16 @@ class MDSystem:
 
     def synchronize(self):
         check(lib.md_system_synchronize(self.h), "synchronize")
+
+    def set_types(self, type):
+        """Atom types 0..15 in original order (MDSystem hdata.type)."""
+        t = np.ascontiguousarray(type, np.int32).reshape(-1)
+        check(lib.md_system_set_types(self.h, _p(t, C.c_int)), "set_types")
+
+    def types(self):
+        out = np.empty(self.n, np.int32)
+        check(lib.md_system_get_types(self.h, _p(out, C.c_int)), "types")
+        return out
 
     def _get3(self, fn):
         out = np.empty((self.n, 3), np.float64)
@@ -317,6 +332,12 @@ class InteractionEngine:
 
     def registNonBondedInteraction(self, epsilon=1.0, sigma=1.0, shift=0.0):
         check(lib.md_engine_register_lj(self.h, epsilon, sigma, shift), "registNonBondedInteraction")
+
+    def registNonBondedInteractionPair(self, type0, type1, epsilon=1.0, sigma=1.0, shift=0.0):
+        """SystemNonBondedInteraction::add(type0, type1, LennardJones6_12Parameter):
+        LJ for one pair of atom types; pairs never given take no force."""
+        check(lib.md_engine_register_lj_pair(self.h, int(type0), int(type1), float(epsilon), float(sigma),
+                                             float(shift)), "registNonBondedInteractionPair")
 
     def setForceCorrection(self, fc):
         """the non-bonded kernel adds the per-atom LFC values (None: off)"""

@@ -160,6 +160,28 @@ def lj_allpair_f64(pos, rcut, box, eps=1.0, sigma=1.0, shift=0.0, pos32=None, bo
     return F, st
 
 
+def lj_allpair_typed(pos, rcut, box, types, pairs, pos32=None, box32=None):
+    """All-pairs LJ with atom types; pairs = {(t0, t1): (eps, sigma, shift)} (symmetric),
+    other pairs take no force.  Returns (force[N,3], stats[E, Wxx, Wyy, Wzz])."""
+    p = np.ascontiguousarray(pos, np.float64)
+    n = p.shape[0]
+    t = np.ascontiguousarray(types, np.int32)
+    nt = int(max(max(max(k) for k in pairs) + 1, t.max() + 1))
+    tab = np.zeros((nt, nt, 3)); on = np.zeros((nt, nt), np.int32)
+    for (a, b), v in pairs.items():
+        tab[a, b] = tab[b, a] = v
+        on[a, b] = on[b, a] = 1
+    rc = np.ascontiguousarray(rcut, np.float64)
+    b = np.ascontiguousarray(box, np.float64)
+    F = np.empty((n, 3)); st = np.empty(4)
+    p32 = None if pos32 is None else np.ascontiguousarray(pos32, np.float32)
+    b32 = None if box32 is None else np.ascontiguousarray(box32, np.float32)
+    _lib.orc_lj_allpair_typed(n, _p(p, f64), _p(rc, f64), _p(t, i32), nt, _p(tab, f64), _p(on, i32), _p(b, f64),
+                              None if p32 is None else _p(p32, f32), None if b32 is None else _p(b32, f32),
+                              _p(F, f64), _p(st, f64))
+    return F, st
+
+
 def assign_rcut_f32(pos, box, lattice):
     p = np.ascontiguousarray(pos, np.float32)
     b = np.ascontiguousarray(box, np.float32)
@@ -593,6 +615,8 @@ _sigs3 = {
     "orc_spme_selfcorr": (None, [i32, P(f64), P(f64), P(f64), P(i32), i32, f64, P(f64)]),
     "orc_spme_ik_errmap": (None, [P(i32), P(f64), f64, i32, P(f64), P(f64), f64, P(f64), P(f64)]),
     "orc_dir_errmap": (None, [P(i32), P(f64), f64, f64, P(f64), P(f64), f64, P(f64), P(f64)]),
+    "orc_lj_allpair_typed": (None, [i32, P(f64), P(f64), P(i32), i32, P(f64), P(i32), P(f64), P(f32), P(f32),
+                                    P(f64), P(f64)]),
     "orc_bond_term": (None, [i32, P(f64), i32, P(f64), P(f64), P(f64)]),
     "orc_angle_term": (None, [i32, P(f64), i32, P(f64), P(f64), P(f64), P(f64), P(f64)]),
     "orc_bonded_apply": (None, [i32, P(f64), P(f64), i32, i32, P(i32), P(i32), P(f64), i32, P(i32), P(i32),

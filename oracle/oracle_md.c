@@ -274,6 +274,65 @@ void orc_lj_allpair_f64(int n, const double* pos, const double* rcut, double eps
   }
 }
 
+/* The same with atom types (AtomNBForceTable::calForceIndex, ENG/include/
+   NonBondedInteraction.h:673-683): the pair (type_i, type_j) takes tab[type_i][type_j] =
+   {eps, sigma, shift}, or no force and no energy where set[type_i][type_j] == 0
+   (mdForceNULL).  tab is [nt][nt][3], set [nt][nt]. */
+void orc_lj_allpair_typed(int n, const double* pos, const double* rcut, const int* type, int nt,
+                          const double* tab, const int* set, const double box[3], const float* pos32,
+                          const float* box32, double* force, double* stats) {
+  double inv[3];
+  for (int d = 0; d < 3; ++d) inv[d] = 1.0 / box[d];
+  float inv32[3] = {0, 0, 0};
+  if (pos32) orc_box_inverse_f32(box32, inv32);
+  double E = 0, Wx = 0, Wy = 0, Wz = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : E, Wx, Wy, Wz)
+  for (int i = 0; i < n; ++i) {
+    double fx = 0, fy = 0, fz = 0;
+    const double rc2 = rcut[i] * rcut[i];
+    const float rc32 = (float)rcut[i];
+    const float rc232 = rc32 * rc32;
+    for (int j = 0; j < n; ++j) {
+      if (j == i) continue;
+      const int pr = type[i] * nt + type[j];
+      if (!set[pr]) continue;
+      double dx = mi_f64(pos[3 * j] - pos[3 * i], box[0], inv[0]);
+      double dy = mi_f64(pos[3 * j + 1] - pos[3 * i + 1], box[1], inv[1]);
+      double dz = mi_f64(pos[3 * j + 2] - pos[3 * i + 2], box[2], inv[2]);
+      double r2 = dx * dx + dy * dy + dz * dz;
+      int in;
+      if (pos32) {
+        float ex = mi_f32(pos32[3 * j] - pos32[3 * i], box32[0], inv32[0]);
+        float ey = mi_f32(pos32[3 * j + 1] - pos32[3 * i + 1], box32[1], inv32[1]);
+        float ez = mi_f32(pos32[3 * j + 2] - pos32[3 * i + 2], box32[2], inv32[2]);
+        in = (ex * ex + ey * ey + ez * ez) < rc232;
+      } else {
+        in = r2 < rc2;
+      }
+      if (!in) continue;
+      const double e4 = 4.0 * tab[3 * pr], s2 = tab[3 * pr + 1] * tab[3 * pr + 1], sh = tab[3 * pr + 2];
+      double ri2 = 1.0 / r2;
+      double sr2 = s2 * ri2;
+      double sr6 = sr2 * sr2 * sr2;
+      double fs = e4 * (6.0 * sr6 - 12.0 * sr6 * sr6) * ri2;
+      fx += fs * dx;
+      fy += fs * dy;
+      fz += fs * dz;
+      E += 0.5 * (e4 * (sr6 * sr6 - sr6) + sh);
+      Wx += 0.5 * fs * dx * dx;
+      Wy += 0.5 * fs * dy * dy;
+      Wz += 0.5 * fs * dz * dz;
+    }
+    force[3 * i] = fx;
+    force[3 * i + 1] = fy;
+    force[3 * i + 2] = fz;
+  }
+  stats[0] = E;
+  stats[1] = Wx;
+  stats[2] = Wy;
+  stats[3] = Wz;
+}
+
 /* AssignRCut::assign index (ENG/src/AssignRCut.cu:93-112) in binary32 */
 float orc_lattice_rcut_f32(float x, float y, float z, const float box[3], const float* lat,
                            int nx, int ny, int nz) {

@@ -274,3 +274,74 @@ def test_system_from_gro_and_back(mdf, fluid, tmp_path):
     assert back.atom_name == conf.atom_name
     assert np.abs(back.pos - sys.positions()).max() < 5e-4 + 1e-4
     assert np.abs(back.vel - sys.velocities()).max() < 5e-5 + 1e-5
+
+
+TYPED_PAIRS = {(0, 0): (1.0, 1.0, 0.0), (0, 1): (1.5, 0.8, 0.01), (1, 1): (0.5, 0.88, 0.0),
+               (0, 2): (0.7, 1.1, -0.02)}  # (1, 2) and (2, 2) never given: no interaction
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_typed_lj_forces_vs_oracle(mdf, orc, small_slab, prec):
+    """Several atom types (SystemNonBondedInteraction::add per type pair,
+    AtomNBForceTable lookup), adaptive per-atom cutoff, after a cell sort."""
+    s = small_slab
+    rc = adaptive_rcut(s.n, seed=4)
+    types = np.random.default_rng(9).integers(0, 3, s.n)
+    sys = mdf.MDSystem(s.pos, s.box, precision=prec, type=types)
+    assert np.array_equal(sys.types(), types)
+    sys.set_rcut(rc)
+    cl = mdf.CellList(sys, 2.8)
+    cl.rebuild()
+    nl = mdf.NeighborList(sys, 5.3, 0.3, expansion=3.0)
+    nl.fit(sys, cl)
+    eng = mdf.InteractionEngine(sys)
+    for (a, b), v in TYPED_PAIRS.items():
+        eng.registNonBondedInteractionPair(a, b, *v)
+    eng.clearInteraction()
+    sys.clear_stats()
+    eng.applyNonBondedInteraction(sys, nl, with_stats=True)
+    F, st, gp = sys.forces(), sys.stats(), sys.positions()
+    if prec == 0:
+        Fo, so = orc.lj_allpair_typed(gp, rc.astype(np.float64), s.box, types, TYPED_PAIRS,
+                                      pos32=gp.astype(np.float32), box32=s.box.astype(np.float32))
+        tol = TOL_MIXED
+    else:
+        Fo, so = orc.lj_allpair_typed(gp, rc.astype(np.float64), s.box, types, TYPED_PAIRS)
+        tol = TOL_FP64
+    assert rel_rms(F, Fo) < tol
+    assert np.allclose(st[:4], so, rtol=tol * 10, atol=0), (st[:4], so)
+
+
+def test_typed_driver_and_arguments(mdf, fluid):
+    types = np.arange(fluid.n) % 2
+    out = []
+    for use_graph in (True, False):
+        sys = mdf.MDSystem(fluid.pos, fluid.box, vel=fluid.vel, precision=0, type=types)
+        sys.set_rcut(np.full(sys.n, 2.5, np.float32))
+        eng = mdf.InteractionEngine(sys)
+        eng.registNonBondedInteractionPair(0, 0, 1.0, 1.0)
+        eng.registNonBondedInteractionPair(0, 1, 1.2, 0.9)
+        eng.registNonBondedInteractionPair(1, 1, 0.8, 1.05)
+        lv = mdf.langevin_params(dt=0.005, temperature=1.0, gamma_t=0.5, seed=2)
+        sim = mdf.Simulation(sys, eng, skin=0.3, cell_size=2.8, lv=lv, use_graph=use_graph)
+        sim.run(50)
+        out.append(sys.positions())
+        assert np.all(np.isfinite(out[-1]))
+        # the types follow their atoms through the sorts
+        assert np.array_equal(sys.types(), types)
+    assert np.array_equal(out[0], out[1])
+    with pytest.raises(mdf.MDExcptBadArgument):
+        mdf.MDSystem(fluid.pos, fluid.box, type=np.full(fluid.n, 16))
+    with pytest.raises(mdf.MDExcptBadArgument):
+        eng.registNonBondedInteractionPair(0, 16, 1.0, 1.0)
+    # a system type beyond the interaction table is refused at the force call
+    sys = mdf.MDSystem(fluid.pos, fluid.box, precision=0, type=np.arange(fluid.n) % 3)
+    sys.set_rcut(np.full(sys.n, 2.5, np.float32))
+    eng = mdf.InteractionEngine(sys)
+    eng.registNonBondedInteractionPair(0, 1, 1.0, 1.0)
+    cl = mdf.CellList(sys, 2.8)
+    cl.rebuild()
+    nl = mdf.NeighborList(sys, 2.5, 0.3)
+    nl.fit(sys, cl)
+    with pytest.raises(mdf.MDExcptBadArgument):
+        eng.applyNonBondedInteraction(sys, nl)
