@@ -86,6 +86,51 @@ __device__ __forceinline__ void add_correction(double4a& f, const double4a& c) {
   f.z += c.z;
 }
 
+// Typed pairs: the nbForcePoten dispatch of ENG/include/NonBondedInteraction.h:556-600
+// over the pair's kind, two 4-vectors per type pair (A, B):
+//   LJ 6-12   (1): A = (1, 4 eps, sigma^2, shift)
+//                  F = 4 eps (6 s^6 - 12 s^12)/r^2 d,  E = 4 eps (s^12 - s^6) + shift
+//   LJ 6-12 B (5): A = (5, eps, sigma^2, shift), B.x = rcut^2 (LennardJones6_12B::forcePoten, :1010-1031)
+//                  F = -eps (12 s^12 - 12 s^6)/r^2 d,  E = eps (s^12 - 2 s^6 + shift), 0 beyond rcut
+//   CosTail   (3): A = (3, eps, b, rc), B = (rcut, 1/wc, [wc == 0], 0) (CosTail::forcePoten, :1400-1440)
+//                  r <= rc: the WCA-shaped core in b; rc < r < rcut: -eps cos^2(pi/2 (r - rc)/wc)
+//   none      (0): no force, no energy (mdForceNULL)
+// with d = r_j - r_i; the caller has already applied the per-atom cutoff.
+template <class R, class V>
+__device__ __forceinline__ R typed_pair(const V& A, const V& B, R r2, R& e) {
+  const int kind = (int)A.x;
+  if (kind == 1) {
+    const R ri2 = R(1) / r2, s2 = A.z * ri2, s6 = s2 * s2 * s2;
+    e = A.y * (s6 * s6 - s6) + A.w;
+    return A.y * (R(6) * s6 - R(12) * s6 * s6) * ri2;
+  }
+  if (kind == 5) {
+    if (r2 > B.x) { e = R(0); return R(0); }
+    const R ri2 = R(1) / r2, s2 = A.z * ri2, s6 = s2 * s2 * s2;
+    e = A.y * (s6 * s6 - s6 * R(2) + A.w);
+    return -A.y * (R(12) * s6 * s6 - R(12) * s6) * ri2;
+  }
+  if (kind == 3) {
+    const R ri = R(1) / sqrt(r2);
+    if (r2 <= A.w * A.w) {
+      const R sri = A.z * ri, sri2 = sri * sri, sri6 = sri2 * sri2 * sri2;
+      e = R(4) * A.y * (sri6 * sri6 - sri6) + (B.z != R(0) ? A.y : R(0));
+      return -R(24) * A.y * (R(2) * sri6 * sri6 - sri6) * ri * ri;
+    }
+    if (r2 < B.x * B.x) {
+      const R pi_ = sizeof(R) == 4 ? R(3.14159265f) : R(M_PI);
+      const R term = R(0.5) * pi_ * (r2 * ri - A.w) * B.y;
+      const R c = cos(term);
+      e = -A.y * c * c;
+      return A.y * pi_ * B.y * c * sin(term) * ri;
+    }
+    e = R(0);
+    return R(0);
+  }
+  e = R(0);
+  return R(0);
+}
+
 // ---------------------------------------------------------------- mixed
 struct MixedAcc {
   Kahan fx, fy, fz;
@@ -133,27 +178,47 @@ __device__ __forceinline__ void lj_pass_mixed(const int4 e4, int nvalid, const f
     const float dz = __fsub_rn(__fsub_rn(pj[u].z, pi.z), sh.z);
     const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
     if ((!TAIL || ee[u] != -1) && r2 < rc2) {
-      const float4 pp = TYPES ? tab[tj[u]] : make_float4(p.eps4f, p.sig2f, p.shiftf, 0.f);
       const float ri2 = __fdividef(1.0f, r2);
-      const float s2 = pp.y * ri2;
-      const float s6 = s2 * s2 * s2;
-      // 4 eps (6 s^6 - 12 s^12) / r^2 = (4 eps / r^2) s^6 (6 - 12 s^6)
-      float fs = (pp.x * ri2) * s6 * fmaf(-12.f, s6, 6.f);
-      if (COUL) {
-        const float qq = pi.w * pj[u].w;
-        const float rinv = rsqrtf(r2);
-        const float er = erfcf(p.betaf * r2 * rinv);
-        fs -= qq * (er * rinv + p.cbf * __expf(-p.betaf * p.betaf * r2)) * ri2;
-        if (STATS) a.ec += qq * er * rinv;
-      }
-      bx += fs * dx;
-      by += fs * dy;
-      bz += fs * dz;
-      if (STATS) {
-        a.e += fmaf(pp.x, fmaf(s6, s6, -s6), pp.z);
-        a.vx += fs * dx * dx;
-        a.vy += fs * dy * dy;
-        a.vz += fs * dz * dz;
+      if (TYPES) {
+        float ep = 0.f;
+        float fs = typed_pair<float>(tab[2 * tj[u]], tab[2 * tj[u] + 1], r2, ep);
+        if (COUL) {
+          const float qq = pi.w * pj[u].w;
+          const float rinv = rsqrtf(r2);
+          const float er = erfcf(p.betaf * r2 * rinv);
+          fs -= qq * (er * rinv + p.cbf * __expf(-p.betaf * p.betaf * r2)) * ri2;
+          if (STATS) a.ec += qq * er * rinv;
+        }
+        bx += fs * dx;
+        by += fs * dy;
+        bz += fs * dz;
+        if (STATS) {
+          a.e += ep;
+          a.vx += fs * dx * dx;
+          a.vy += fs * dy * dy;
+          a.vz += fs * dz * dz;
+        }
+      } else {
+        const float s2 = p.sig2f * ri2;
+        const float s6 = s2 * s2 * s2;
+        // 4 eps (6 s^6 - 12 s^12) / r^2 = (4 eps / r^2) s^6 (6 - 12 s^6)
+        float fs = (p.eps4f * ri2) * s6 * fmaf(-12.f, s6, 6.f);
+        if (COUL) {
+          const float qq = pi.w * pj[u].w;
+          const float rinv = rsqrtf(r2);
+          const float er = erfcf(p.betaf * r2 * rinv);
+          fs -= qq * (er * rinv + p.cbf * __expf(-p.betaf * p.betaf * r2)) * ri2;
+          if (STATS) a.ec += qq * er * rinv;
+        }
+        bx += fs * dx;
+        by += fs * dy;
+        bz += fs * dz;
+        if (STATS) {
+          a.e += fmaf(p.eps4f, fmaf(s6, s6, -s6), p.shiftf);
+          a.vx += fs * dx * dx;
+          a.vy += fs * dy * dy;
+          a.vz += fs * dz * dz;
+        }
       }
     }
   }
@@ -180,14 +245,14 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
                            __fmul_rn((float)((int)((c >> 2) & 3u) - 1), st->Lf[1]),
                            __fmul_rn((float)((int)(c >> 4) - 1), st->Lf[2]), 0.f);
   }
-  __shared__ float4 tab[TYPES ? MD_MAX_TYPES * MD_MAX_TYPES : 1];
+  __shared__ float4 tab[TYPES ? 2 * MD_MAX_TYPES * MD_MAX_TYPES : 1];
   if (TYPES)
-    for (int c = threadIdx.x; c < nt * nt; c += blockDim.x) tab[c] = reinterpret_cast<const float4*>(ptab)[c];
+    for (int c = threadIdx.x; c < 2 * nt * nt; c += blockDim.x) tab[c] = reinterpret_cast<const float4*>(ptab)[c];
   __syncthreads();
   MixedAcc a;
   if (i < N) {
     const float4 pi = pos[i];
-    const float4* trow = TYPES ? tab + nt * (int)type[i] : tab;
+    const float4* trow = TYPES ? tab + 2 * nt * (int)type[i] : tab;
     const float rc = rcut[i];
     const float rc2 = __fmul_rn(rc, rc);
     int n = nnb[i];
@@ -246,11 +311,11 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
           const DevState* __restrict__ st, LJParams p, double4a* __restrict__ force, int overwrite,
           double* partials, unsigned* counter, double* stats, const double4a* __restrict__ corr,
           const int* __restrict__ id, const uint8_t* __restrict__ type, const void* __restrict__ ptab, int nt) {
-  __shared__ double4a tab[TYPES ? MD_MAX_TYPES * MD_MAX_TYPES : 1];
+  __shared__ double4a tab[TYPES ? 2 * MD_MAX_TYPES * MD_MAX_TYPES : 1];
   if (TYPES) {
     const double4a* src = reinterpret_cast<const double4a*>(reinterpret_cast<const float4*>(ptab) +
-                                                            MD_MAX_TYPES * MD_MAX_TYPES);
-    for (int c = threadIdx.x; c < nt * nt; c += blockDim.x) tab[c] = src[c];
+                                                            2 * MD_MAX_TYPES * MD_MAX_TYPES);
+    for (int c = threadIdx.x; c < 2 * nt * nt; c += blockDim.x) tab[c] = src[c];
     __syncthreads();
   }
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -292,12 +357,17 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
       const double dz = __dsub_rn(__dsub_rn(pj.z, pi.z), __dmul_rn(kz, L2));
       const double r2 = dx * dx + dy * dy + dz * dz;
       if (jj[u] != -1 && r2 < rc2) {
-        const double4a pp = TYPES ? tab[nt * (int)type[i] + (int)type[jj[u] & 0x03FFFFFF]]
-                                  : double4a{p.eps4, p.sig2, p.shift, 0.0};
         const double ri2 = 1.0 / r2;
-        const double s2 = pp.y * ri2;
-        const double s6 = s2 * s2 * s2;
-        double fs = pp.x * (6.0 * s6 - 12.0 * s6 * s6) * ri2;
+        double fs, ep = 0.0;
+        if (TYPES) {
+          const int c = 2 * (nt * (int)type[i] + (int)type[jj[u] & 0x03FFFFFF]);
+          fs = typed_pair<double>(tab[c], tab[c + 1], r2, ep);
+        } else {
+          const double s2 = p.sig2 * ri2;
+          const double s6 = s2 * s2 * s2;
+          fs = p.eps4 * (6.0 * s6 - 12.0 * s6 * s6) * ri2;
+          ep = p.eps4 * (s6 * s6 - s6) + p.shift;
+        }
         if (COUL) {
           const double qq = pi.w * pj.w;
           const double r = sqrt(r2);
@@ -309,7 +379,7 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
         fy += fs * dy;
         fz += fs * dz;
         if (STATS) {
-          e += pp.x * (s6 * s6 - s6) + pp.z;
+          e += ep;
           vx += fs * dx * dx;
           vy += fs * dy * dy;
           vz += fs * dz * dz;
@@ -374,17 +444,43 @@ int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats,
       return MD_ERR_BADARG;
     }
     if (eng->tab_dirty || !eng->d_tab) {
-      const size_t nf = MD_MAX_TYPES * MD_MAX_TYPES;
+      const size_t nf = 2 * MD_MAX_TYPES * MD_MAX_TYPES;
       if (!eng->d_tab) MD_CUDA(cudaMalloc(&eng->d_tab, nf * (sizeof(float4) + sizeof(double4a))));
-      std::vector<float4> tf(nf);
-      std::vector<double4a> td(nf);
+      std::vector<float4> tf(nf, make_float4(0.f, 0.f, 0.f, 0.f));
+      std::vector<double4a> td(nf, double4a{0, 0, 0, 0});
       for (int a0 = 0; a0 < nt; ++a0)
         for (int a1 = 0; a1 < nt; ++a1) {
-          const double* q = eng->lj_pair[a0][a1];
-          const double e4 = eng->lj_pair_set[a0][a1] ? 4.0 * q[0] : 0.0, s2 = q[1] * q[1];
-          const double sh = eng->lj_pair_set[a0][a1] ? q[2] : 0.0;
-          tf[a0 * nt + a1] = make_float4((float)e4, (float)s2, (float)sh, 0.f);
-          td[a0 * nt + a1] = double4a{e4, s2, sh, 0.0};
+          const double* q = eng->nb_param[a0][a1];
+          const size_t c = 2 * (size_t)(a0 * nt + a1);
+          // derived parameters as the *Parameter::reinit of each kind forms them,
+          // in binary32 for the mixed table and binary64 for the FP64 one
+          switch (eng->nb_kind[a0][a1]) {
+            case MD_NB_LJ6_12: {
+              const float sf = (float)q[1];
+              tf[c] = make_float4(1.f, 4.f * (float)q[0], sf * sf, (float)q[2]);
+              td[c] = double4a{1.0, 4.0 * q[0], q[1] * q[1], q[2]};
+              break;
+            }
+            case MD_NB_LJ6_12B: {
+              const float sf = (float)q[1], rf = (float)q[3];
+              tf[c] = make_float4(5.f, (float)q[0], sf * sf, (float)q[2]);
+              tf[c + 1] = make_float4(rf * rf, 0.f, 0.f, 0.f);
+              td[c] = double4a{5.0, q[0], q[1] * q[1], q[2]};
+              td[c + 1] = double4a{q[3] * q[3], 0, 0, 0};
+              break;
+            }
+            case MD_NB_COSTAIL: {
+              const float ef = (float)q[0], bf = (float)q[1], wf = (float)q[2];
+              const float rcf = bf * powf(2.f, 1.f / 6.f);
+              tf[c] = make_float4(3.f, ef, bf, rcf);
+              tf[c + 1] = make_float4(rcf + wf, wf != 0.f ? 1.f / wf : 0.f, wf == 0.f ? 1.f : 0.f, 0.f);
+              const double rcd = q[1] * pow(2.0, 1.0 / 6.0);
+              td[c] = double4a{3.0, q[0], q[1], rcd};
+              td[c + 1] = double4a{rcd + q[2], q[2] != 0 ? 1.0 / q[2] : 0.0, q[2] == 0 ? 1.0 : 0.0, 0};
+              break;
+            }
+            default: break;  // kind 0: no interaction
+          }
         }
       MD_CUDA(cudaMemcpy(eng->d_tab, tf.data(), nf * sizeof(float4), cudaMemcpyHostToDevice));
       MD_CUDA(cudaMemcpy(reinterpret_cast<char*>(eng->d_tab) + nf * sizeof(float4), td.data(),
@@ -434,18 +530,25 @@ extern "C" int md_engine_destroy(md_engine* e) {
 // with AtomNBForceTable::calForceIndex (ENG/include/NonBondedInteraction.h:673-683): one
 // parameter set per unordered type pair; pairs never given interact with nothing
 // (mdForceNULL).  The cutoff stays the per-atom rcut_i.
-extern "C" int md_engine_register_lj_pair(md_engine* e, int t0, int t1, double eps, double sigma, double shift) {
-  if (!e || t0 < 0 || t1 < 0 || t0 >= MD_MAX_TYPES || t1 >= MD_MAX_TYPES || !(eps >= 0) || !(sigma > 0) ||
-      !std::isfinite(shift)) {
-    md_set_error("md_engine_register_lj_pair: bad arguments (types 0..%d, eps >= 0, sigma > 0)", MD_MAX_TYPES - 1);
+extern "C" int md_engine_register_nb_pair(md_engine* e, int t0, int t1, int kind, const double* param) {
+  if (!e || !param || t0 < 0 || t1 < 0 || t0 >= MD_MAX_TYPES || t1 >= MD_MAX_TYPES) {
+    md_set_error("md_engine_register_nb_pair: bad arguments (types 0..%d)", MD_MAX_TYPES - 1);
+    return MD_ERR_BADARG;
+  }
+  bool ok = std::isfinite(param[0]) && std::isfinite(param[1]) && std::isfinite(param[2]) &&
+            std::isfinite(param[3]) && param[0] >= 0;
+  if (kind == MD_NB_LJ6_12) ok = ok && param[1] > 0;
+  else if (kind == MD_NB_LJ6_12B) ok = ok && param[1] > 0 && param[3] > 0;
+  else if (kind == MD_NB_COSTAIL) ok = ok && param[1] > 0 && param[2] >= 0;
+  else if (kind != MD_NB_NULL) ok = false;
+  if (!ok) {
+    md_set_error("md_engine_register_nb_pair: kind %d or its parameters out of range", kind);
     return MD_ERR_BADARG;
   }
   for (int k = 0; k < 2; ++k) {
     const int a = k ? t1 : t0, b = k ? t0 : t1;
-    e->lj_pair[a][b][0] = eps;
-    e->lj_pair[a][b][1] = sigma;
-    e->lj_pair[a][b][2] = shift;
-    e->lj_pair_set[a][b] = true;
+    for (int c = 0; c < 4; ++c) e->nb_param[a][b][c] = param[c];
+    e->nb_kind[a][b] = kind;
   }
   const int need = (t0 > t1 ? t0 : t1) + 1;
   if (need > e->nt) e->nt = need;
@@ -453,6 +556,11 @@ extern "C" int md_engine_register_lj_pair(md_engine* e, int t0, int t1, double e
   e->tab_dirty = true;
   if (e->sys) e->sys->topo_version += 1;  // a recorded step graph picks the typed kernel up
   return MD_OK;
+}
+
+extern "C" int md_engine_register_lj_pair(md_engine* e, int t0, int t1, double eps, double sigma, double shift) {
+  const double q[4] = {eps, sigma, shift, 0.0};
+  return md_engine_register_nb_pair(e, t0, t1, MD_NB_LJ6_12, q);
 }
 
 extern "C" int md_engine_register_lj(md_engine* e, double eps, double sigma, double shift) {

@@ -171,9 +171,9 @@ struct md_engine {
   // per type pair LJ (SystemNonBondedInteraction::add / AtomNBForceTable):
   // nt > 0 selects the typed kernels; pairs not given take no force
   int nt = 0;
-  double lj_pair[16][16][3] = {};  // eps, sigma, shift (symmetric)
-  bool lj_pair_set[16][16] = {};
-  void* d_tab = nullptr;           // float4 [nt*nt] then double4a [nt*nt] (eps4, sig2, shift)
+  int nb_kind[16][16] = {};        // md_nb_kind per type pair (symmetric), 0: none
+  double nb_param[16][16][4] = {};  // the kind's user parameters
+  void* d_tab = nullptr;            // float4 [2*16*16] then double4a [2*16*16]
   bool tab_dirty = false;
   bool has_coul = false;
   double beta = 0;

@@ -86,6 +86,7 @@ _SIGS = {
     "md_engine_apply_bonded": (i32, [vp, vp]),
     "md_engine_set_bonds": (i32, [vp, i32, P(i32), P(i32), P(f64)]),
     "md_engine_register_lj_pair": (i32, [vp, i32, i32, f64, f64, f64]),
+    "md_engine_register_nb_pair": (i32, [vp, i32, i32, i32, P(f64)]),
     "md_system_set_types": (i32, [vp, P(i32)]),
     "md_system_get_types": (i32, [vp, P(i32)]),
     "md_engine_set_angles": (i32, [vp, i32, P(i32), P(i32), P(f64)]),

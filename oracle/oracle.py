@@ -161,16 +161,20 @@ def lj_allpair_f64(pos, rcut, box, eps=1.0, sigma=1.0, shift=0.0, pos32=None, bo
 
 
 def lj_allpair_typed(pos, rcut, box, types, pairs, pos32=None, box32=None):
-    """All-pairs LJ with atom types; pairs = {(t0, t1): (eps, sigma, shift)} (symmetric),
-    other pairs take no force.  Returns (force[N,3], stats[E, Wxx, Wyy, Wzz])."""
+    """All-pairs non-bonded forces with atom types; pairs = {(t0, t1): params} (symmetric)
+    with params (eps, sigma, shift) for LJ 6-12 or (kind, (p0, p1, p2, p3)) for the other
+    kinds (1 LJ 6-12, 5 LJ 6-12 B, 3 CosTail); other pairs take no force.
+    Returns (force[N,3], stats[E, Wxx, Wyy, Wzz])."""
     p = np.ascontiguousarray(pos, np.float64)
     n = p.shape[0]
     t = np.ascontiguousarray(types, np.int32)
     nt = int(max(max(max(k) for k in pairs) + 1, t.max() + 1))
-    tab = np.zeros((nt, nt, 3)); on = np.zeros((nt, nt), np.int32)
+    tab = np.zeros((nt, nt, 4)); on = np.zeros((nt, nt), np.int32)
     for (a, b), v in pairs.items():
-        tab[a, b] = tab[b, a] = v
-        on[a, b] = on[b, a] = 1
+        kind, q = (1, tuple(v) + (0.0,)) if not isinstance(v[0], int) or len(v) != 2 else v
+        q = np.zeros(4) + np.pad(np.asarray(q, float), (0, 4 - len(q)))
+        tab[a, b] = tab[b, a] = q
+        on[a, b] = on[b, a] = kind
     rc = np.ascontiguousarray(rcut, np.float64)
     b = np.ascontiguousarray(box, np.float64)
     F = np.empty((n, 3)); st = np.empty(4)
@@ -617,6 +621,7 @@ _sigs3 = {
     "orc_dir_errmap": (None, [P(i32), P(f64), f64, f64, P(f64), P(f64), f64, P(f64), P(f64)]),
     "orc_lj_allpair_typed": (None, [i32, P(f64), P(f64), P(i32), i32, P(f64), P(i32), P(f64), P(f32), P(f32),
                                     P(f64), P(f64)]),
+    "orc_nb_pair": (None, [i32, P(f64), i32, P(f64), P(f64), P(f64)]),
     "orc_bond_term": (None, [i32, P(f64), i32, P(f64), P(f64), P(f64)]),
     "orc_angle_term": (None, [i32, P(f64), i32, P(f64), P(f64), P(f64), P(f64), P(f64)]),
     "orc_bonded_apply": (None, [i32, P(f64), P(f64), i32, i32, P(i32), P(i32), P(f64), i32, P(i32), P(i32),
@@ -781,3 +786,21 @@ def ref_bonded_term(ftype, uparam, d0, d1=None):
     f0 = np.zeros(3); f1 = np.zeros(3); e = np.zeros(1)
     lib.ref_bonded_term(int(ftype), _p(u, f64), _p(a, f64), _p(b, f64), _p(f0, f64), _p(f1, f64), _p(e, f64))
     return (f0, float(e[0])) if d1 is None else (f0, f1, float(e[0]))
+
+
+def nb_pair(kind, uparam, prec, d):
+    """One non-bonded pair of a kind (oracle_md.c): force on i, energy."""
+    u = np.zeros(4); u[:len(uparam)] = uparam
+    dd = np.ascontiguousarray(d, np.float64); f = np.zeros(3); e = C.c_double()
+    _lib.orc_nb_pair(int(kind), _p(u, f64), int(prec), _p(dd, f64), _p(f, f64), C.byref(e))
+    return f, e.value
+
+
+def ref_nb_pair(kind, uparam, d):
+    """The reference's own pair functions (oracle/_ref/libref_nb.so), binary32."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libref_nb.so"))
+    lib.ref_nb_pair.argtypes = [i32, P(f64), P(f64), P(f64), P(f64)]
+    u = np.zeros(4); u[:len(uparam)] = uparam
+    dd = np.ascontiguousarray(d, np.float64); f = np.zeros(3); e = np.zeros(1)
+    lib.ref_nb_pair(int(kind), _p(u, f64), _p(dd, f64), _p(f, f64), _p(e, f64))
+    return f, float(e[0])

@@ -275,11 +275,97 @@ void orc_lj_allpair_f64(int n, const double* pos, const double* rcut, double eps
 }
 
 /* The same with atom types (AtomNBForceTable::calForceIndex, ENG/include/
-   NonBondedInteraction.h:673-683): the pair (type_i, type_j) takes tab[type_i][type_j] =
-   {eps, sigma, shift}, or no force and no energy where set[type_i][type_j] == 0
-   (mdForceNULL).  tab is [nt][nt][3], set [nt][nt]. */
+   NonBondedInteraction.h:673-683): the pair (type_i, type_j) takes the pair kind
+   kind[type_i][type_j] with parameters tab[type_i][type_j][4] (nb_pair_d), or no force
+   and no energy where the kind is 0 (mdForceNULL). */
+/* One non-bonded pair of a kind of the nbForcePoten dispatch (ENG/include/
+   NonBondedInteraction.h:556-600) for d = r_j - r_i: the force on i and the
+   energy, the parameters as the *Parameter classes take them.
+     kind 1 LennardJones6_12 (eps, sigma, shift)        :867-886
+     kind 5 LennardJones6_12B (eps, sigma, shift, rcut) :1010-1031
+     kind 3 CosTail (eps, b, wc)                        :1379-1440
+   prec 0 follows the binary32 operations of those functions, prec 1 the same
+   formulas in binary64 (the accurate cos and sin for the fast intrinsics). */
+static float nb_pair_f(int kind, const double* u, float dx, float dy, float dz, float* f) {
+  const float dr2 = dx * dx + dy * dy + dz * dz;
+  float sc = 0.f, e = 0.f;
+  if (kind == 1) {
+    const float eps = (float)u[0], sig = (float)u[1], sh = (float)u[2];
+    const float ri2 = 1.f / dr2, sri2 = sig * sig * ri2, sri6 = sri2 * sri2 * sri2;
+    sc = -4.f * eps * (12.f * sri6 * sri6 - 6.f * sri6) * ri2;
+    e = 4.f * (eps * (sri6 * sri6 - sri6) + sh * 0.25f);
+  } else if (kind == 5) {
+    const float eps = (float)u[0], sig = (float)u[1], sh = (float)u[2], rc = (float)u[3];
+    const float b = dr2 > rc * rc ? 0.f : 1.f;
+    const float ri2 = 1.f / dr2, sri2 = sig * sig * ri2, sri6 = sri2 * sri2 * sri2;
+    sc = -b * eps * (12.f * sri6 * sri6 - 12.f * sri6) * ri2;
+    e = b * (eps * (sri6 * sri6 - sri6 * 2.f + sh));
+  } else if (kind == 3) {
+    const float eps = (float)u[0], bv = (float)u[1], wc = (float)u[2];
+    const float wci = wc != 0.f ? 1.f / wc : 0.f;
+    const float rc = bv * powf(2.f, 1.f / 6.f), rcut = rc + wc;
+    const float ri = 1.f / sqrtf(dr2);
+    if (dr2 <= rc * rc) {
+      const float sri = bv * ri, sri2 = sri * sri, sri6 = sri2 * sri2 * sri2;
+      sc = -24.f * eps * (2.f * sri6 * sri6 - sri6) * ri * ri;
+      e = 4.f * eps * (sri6 * sri6 - sri6);
+      if (wc == 0.f) e += eps;
+    } else if (dr2 < rcut * rcut) {
+      const float term = 0.5f * 3.14159265f * (dr2 * ri - rc) * wci;
+      const float cost = cosf(term);
+      sc = eps * 3.14159265f * wci * cost * sinf(term) * ri;
+      e = -eps * cost * cost;
+    }
+  }
+  f[0] = dx * sc; f[1] = dy * sc; f[2] = dz * sc;
+  return e;
+}
+
+static double nb_pair_d(int kind, const double* u, double dx, double dy, double dz, double* f) {
+  const double dr2 = dx * dx + dy * dy + dz * dz;
+  double sc = 0., e = 0.;
+  if (kind == 1) {
+    const double ri2 = 1. / dr2, sri2 = u[1] * u[1] * ri2, sri6 = sri2 * sri2 * sri2;
+    sc = -4. * u[0] * (12. * sri6 * sri6 - 6. * sri6) * ri2;
+    e = 4. * (u[0] * (sri6 * sri6 - sri6) + u[2] * 0.25);
+  } else if (kind == 5) {
+    const double b = dr2 > u[3] * u[3] ? 0. : 1.;
+    const double ri2 = 1. / dr2, sri2 = u[1] * u[1] * ri2, sri6 = sri2 * sri2 * sri2;
+    sc = -b * u[0] * (12. * sri6 * sri6 - 12. * sri6) * ri2;
+    e = b * (u[0] * (sri6 * sri6 - sri6 * 2. + u[2]));
+  } else if (kind == 3) {
+    const double eps = u[0], bv = u[1], wc = u[2];
+    const double wci = wc != 0. ? 1. / wc : 0.;
+    const double rc = bv * pow(2., 1. / 6.), rcut = rc + wc;
+    const double ri = 1. / sqrt(dr2);
+    if (dr2 <= rc * rc) {
+      const double sri = bv * ri, sri2 = sri * sri, sri6 = sri2 * sri2 * sri2;
+      sc = -24. * eps * (2. * sri6 * sri6 - sri6) * ri * ri;
+      e = 4. * eps * (sri6 * sri6 - sri6);
+      if (wc == 0.) e += eps;
+    } else if (dr2 < rcut * rcut) {
+      const double term = 0.5 * M_PI * (dr2 * ri - rc) * wci;
+      const double cost = cos(term);
+      sc = eps * M_PI * wci * cost * sin(term) * ri;
+      e = -eps * cost * cost;
+    }
+  }
+  f[0] = dx * sc; f[1] = dy * sc; f[2] = dz * sc;
+  return e;
+}
+
+void orc_nb_pair(int kind, const double* u, int prec, const double* d, double* f, double* e) {
+  if (prec == 0) {
+    float ff[3];
+    *e = nb_pair_f(kind, u, (float)d[0], (float)d[1], (float)d[2], ff);
+    for (int k = 0; k < 3; ++k) f[k] = ff[k];
+  } else {
+    *e = nb_pair_d(kind, u, d[0], d[1], d[2], f);
+  }
+}
+
 void orc_lj_allpair_typed(int n, const double* pos, const double* rcut, const int* type, int nt,
-                          const double* tab, const int* set, const double box[3], const float* pos32,
+                          const double* tab, const int* kind, const double box[3], const float* pos32,
                           const float* box32, double* force, double* stats) {
   double inv[3];
   for (int d = 0; d < 3; ++d) inv[d] = 1.0 / box[d];
@@ -295,7 +381,7 @@ void orc_lj_allpair_typed(int n, const double* pos, const double* rcut, const in
     for (int j = 0; j < n; ++j) {
       if (j == i) continue;
       const int pr = type[i] * nt + type[j];
-      if (!set[pr]) continue;
+      if (!kind[pr]) continue;
       double dx = mi_f64(pos[3 * j] - pos[3 * i], box[0], inv[0]);
       double dy = mi_f64(pos[3 * j + 1] - pos[3 * i + 1], box[1], inv[1]);
       double dz = mi_f64(pos[3 * j + 2] - pos[3 * i + 2], box[2], inv[2]);
@@ -310,18 +396,15 @@ void orc_lj_allpair_typed(int n, const double* pos, const double* rcut, const in
         in = r2 < rc2;
       }
       if (!in) continue;
-      const double e4 = 4.0 * tab[3 * pr], s2 = tab[3 * pr + 1] * tab[3 * pr + 1], sh = tab[3 * pr + 2];
-      double ri2 = 1.0 / r2;
-      double sr2 = s2 * ri2;
-      double sr6 = sr2 * sr2 * sr2;
-      double fs = e4 * (6.0 * sr6 - 12.0 * sr6 * sr6) * ri2;
-      fx += fs * dx;
-      fy += fs * dy;
-      fz += fs * dz;
-      E += 0.5 * (e4 * (sr6 * sr6 - sr6) + sh);
-      Wx += 0.5 * fs * dx * dx;
-      Wy += 0.5 * fs * dy * dy;
-      Wz += 0.5 * fs * dz * dz;
+      double f[3];
+      const double e = nb_pair_d(kind[pr], tab + 4 * pr, dx, dy, dz, f);
+      fx += f[0];
+      fy += f[1];
+      fz += f[2];
+      E += 0.5 * e;
+      Wx += 0.5 * f[0] * dx;
+      Wy += 0.5 * f[1] * dy;
+      Wz += 0.5 * f[2] * dz;
     }
     force[3 * i] = fx;
     force[3 * i + 1] = fy;

@@ -337,3 +337,31 @@ extern "C" int ref_bonded_term(int ftype, const double* u, const double* d0, con
   return 0;
 }
 #endif
+
+#ifdef REF_NB
+// The engine's non-bonded pair functions (include/NonBondedInteraction.h,
+// nbForcePoten dispatch) evaluated on the host in binary32 for one pair:
+// kind 1 LennardJones6_12 (eps, sigma, shift, rcut), 5 LennardJones6_12B
+// (eps, sigma, shift, rcut), 3 CosTail (eps, b, wc).
+#include "NonBondedInteraction.h"
+extern "C" int ref_nb_pair(int kind, const double* u, const double* d, double* f, double* e) {
+  ScalorType p[16] = {0};
+  switch (kind) {
+    case mdForceLennardJones6_12:
+      LennardJones6_12::initParameter(p, (ScalorType)u[0], (ScalorType)u[1], (ScalorType)u[2], (ScalorType)u[3]);
+      break;
+    case mdForceLennardJones6_12B:
+      LennardJones6_12B::initParameter(p, (ScalorType)u[0], (ScalorType)u[1], (ScalorType)u[2], (ScalorType)u[3]);
+      break;
+    case mdForceCosTail:
+      CosTail::initParameter(p, (ScalorType)u[0], (ScalorType)u[1], (ScalorType)u[2]);
+      break;
+    default: return 1;
+  }
+  ScalorType fx = 0, fy = 0, fz = 0, dp = 0;
+  nbForcePoten((InteractionType)kind, p, (ScalorType)d[0], (ScalorType)d[1], (ScalorType)d[2], &fx, &fy, &fz, &dp);
+  f[0] = fx; f[1] = fy; f[2] = fz;
+  *e = dp;
+  return 0;
+}
+#endif

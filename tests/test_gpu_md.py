@@ -345,3 +345,39 @@ def test_typed_driver_and_arguments(mdf, fluid):
     nl.fit(sys, cl)
     with pytest.raises(mdf.MDExcptBadArgument):
         eng.applyNonBondedInteraction(sys, nl)
+
+
+KIND_PAIRS = {(0, 0): (1.0, 1.0, 0.0), (0, 1): (5, (1.1, 0.95, 0.1, 2.2)), (1, 1): (3, (1.0, 0.95, 1.6)),
+              (0, 2): (3, (0.8, 1.0, 0.0)), (2, 2): (1, (0.6, 1.05, -0.01))}  # (1, 2): none
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_pair_kinds_vs_oracle(mdf, orc, small_slab, prec):
+    """LJ 6-12, LJ 6-12 B, CosTail (with and without its tail) and a missing pair
+    in one typed system (the nbForcePoten dispatch)."""
+    s = small_slab
+    rc = adaptive_rcut(s.n, seed=5)
+    types = np.random.default_rng(10).integers(0, 3, s.n)
+    sys = mdf.MDSystem(s.pos, s.box, precision=prec, type=types)
+    sys.set_rcut(rc)
+    cl = mdf.CellList(sys, 2.8)
+    cl.rebuild()
+    nl = mdf.NeighborList(sys, 5.3, 0.3, expansion=3.0)
+    nl.fit(sys, cl)
+    eng = mdf.InteractionEngine(sys)
+    for (a, b), v in KIND_PAIRS.items():
+        if len(v) == 3:
+            eng.registNonBondedInteractionPair(a, b, *v)
+        else:
+            eng.registNonBondedPair(a, b, v[0], v[1])
+    eng.clearInteraction()
+    sys.clear_stats()
+    eng.applyNonBondedInteraction(sys, nl, with_stats=True)
+    F, st, gp = sys.forces(), sys.stats(), sys.positions()
+    kw = dict(pos32=gp.astype(np.float32), box32=s.box.astype(np.float32)) if prec == 0 else {}
+    Fo, so = orc.lj_allpair_typed(gp, rc.astype(np.float64), s.box, types, KIND_PAIRS, **kw)
+    tol = TOL_MIXED if prec == 0 else TOL_FP64
+    assert rel_rms(F, Fo) < tol
+    assert np.allclose(st[:4], so, rtol=tol * 10, atol=0), (st[:4], so)
+    with pytest.raises(mdf.MDExcptBadArgument):
+        eng.registNonBondedPair(0, 0, 7, (1.0, 1.0))
