@@ -216,13 +216,22 @@ int md_engine_register_lj(md_engine* eng, double epsilon, double sigma, double s
  * no energy (mdForceNULL); md_engine_register_lj is then ignored.  The cutoff stays the
  * per-atom rcut_i.  Atom types come from md_system_create or md_system_set_types. */
 int md_engine_register_lj_pair(md_engine* eng, int t0, int t1, double epsilon, double sigma, double shift);
-/* The other pair kinds of the nbForce dispatch, for a type pair; param[4] as the reference's
-   *Parameter classes take them (the values of md_nb_kind are InteractionType's):
-     MD_NB_LJ6_12   (eps, sigma, shift, -)      LennardJones6_12
-     MD_NB_LJ6_12B  (eps, sigma, shift, rcut)   LennardJones6_12B: E = eps (s^12 - 2 s^6 + shift), 0 beyond rcut
-     MD_NB_COSTAIL  (eps, b, wc, -)             CosTail: WCA core of size b, -eps cos^2 tail of width wc
-     MD_NB_NULL     no interaction */
-enum md_nb_kind { MD_NB_NULL = 0, MD_NB_LJ6_12 = 1, MD_NB_COSTAIL = 3, MD_NB_LJ6_12B = 5 };
+/* The pair kinds of the nbForce dispatch, for a type pair; param[6] as the reference's
+   *Parameter classes take them, unused entries 0 (the values of md_nb_kind are InteractionType's):
+     MD_NB_LJ6_12       (eps, sigma, shift)             LennardJones6_12
+     MD_NB_LJ6_12B      (eps, sigma, shift, rcut)       LennardJones6_12B: E = eps (s^12 - 2 s^6 + shift),
+                                                        0 beyond rcut
+     MD_NB_LJ6_12_CAP   (eps, sigma, shift, rcut, cap)  LennardJones6_12 with the force magnitude held at
+                                                        cap inside the radius where it reaches cap
+     MD_NB_LJ6_12B_CAP  (eps, sigma, shift, rcut, cap)  the same for the B form
+     MD_NB_COSTAIL      (eps, b, wc)                    CosTail: WCA core of size b, -eps cos^2 tail of width wc
+     MD_NB_COSTAIL_CAP  (eps, b, wc, cap)               CosTail with the capped core
+     MD_NB_NULL         no interaction
+   The cap radius is found as the reference finds it (0.95 steps, then bisection to 1e-4).
+   A coincident pair (r = 0) takes no force from the capped kinds (the reference gives
+   (-cap, 0, 0) there). */
+enum md_nb_kind { MD_NB_NULL = 0, MD_NB_LJ6_12 = 1, MD_NB_LJ6_12_CAP = 2, MD_NB_COSTAIL = 3,
+                  MD_NB_COSTAIL_CAP = 4, MD_NB_LJ6_12B = 5, MD_NB_LJ6_12B_CAP = 6 };
 int md_engine_register_nb_pair(md_engine* eng, int t0, int t1, int kind, const double* param);
 /* Bonded terms (SystemBondedInteraction::reinit + BondedInteractionList,
  * ENG/src/SystemBondedInteraction.cu:100-230; force functions ENG/include/BondInteraction.h:217-372,

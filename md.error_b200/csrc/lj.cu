@@ -97,8 +97,50 @@ __device__ __forceinline__ void add_correction(double4a& f, const double4a& c) {
 //   none      (0): no force, no energy (mdForceNULL)
 // with d = r_j - r_i; the caller has already applied the per-atom cutoff.
 template <class R, class V>
-__device__ __forceinline__ R typed_pair(const V& A, const V& B, R r2, R& e) {
+__device__ __forceinline__ R typed_pair(const V& A, const V& B, const V& C, R r2, R& e) {
   const int kind = (int)A.x;
+  if (kind == 2 || kind == 6) {
+    // LennardJones6_12_cap / _12B_cap (:1094-1135, :1271-1312): B = (rcut, cap, capR, pcapR);
+    // constant force cap inside capR (a coincident pair takes none here)
+    if (kind == 2 ? r2 >= B.x * B.x : r2 > B.x * B.x) { e = R(0); return R(0); }
+    if (r2 == R(0)) { e = R(0); return R(0); }
+    if (r2 < B.z * B.z) {
+      const R s = R(1) / sqrt(r2);
+      e = -B.y * (sqrt(r2) - B.z) + B.w;
+      return -s * B.y;
+    }
+    const R ri2 = R(1) / r2, s2 = A.z * ri2, s6 = s2 * s2 * s2;
+    if (kind == 2) {
+      e = R(4) * A.y * (s6 * s6 - s6) + A.w;
+      return -(R(4) * A.y * (R(12) * s6 * s6 - R(6) * s6) * ri2);
+    }
+    e = A.y * (s6 * s6 - R(2) * s6 + A.w);
+    return -(A.y * (R(12) * s6 * s6 - R(12) * s6) * ri2);
+  }
+  if (kind == 4) {
+    // CosTail_cap (:1532-1570): A = (4, eps, b, rc), B = (rcut, 1/wc, [wc == 0], 0),
+    // C = (cap, capR, pcapR, 0)
+    if (r2 == R(0)) { e = R(0); return R(0); }
+    const R ri = R(1) / sqrt(r2);
+    if (r2 < C.y * C.y) {
+      e = -C.x * (sqrt(r2) - C.y) + C.z;
+      return -ri * C.x;
+    }
+    if (r2 <= A.w * A.w) {
+      const R sri = A.z * ri, sri2 = sri * sri, sri6 = sri2 * sri2 * sri2;
+      e = R(4) * A.y * (sri6 * sri6 - sri6) + (B.z != R(0) ? A.y : R(0));
+      return -R(24) * A.y * (R(2) * sri6 * sri6 - sri6) * ri * ri;
+    }
+    if (r2 < B.x * B.x) {
+      const R pi_ = sizeof(R) == 4 ? R(3.14159265f) : R(M_PI);
+      const R term = R(0.5) * pi_ * (r2 * ri - A.w) * B.y;
+      const R c = cos(term);
+      e = -A.y * c * c;
+      return A.y * pi_ * B.y * c * sin(term) * ri;
+    }
+    e = R(0);
+    return R(0);
+  }
   if (kind == 1) {
     const R ri2 = R(1) / r2, s2 = A.z * ri2, s6 = s2 * s2 * s2;
     e = A.y * (s6 * s6 - s6) + A.w;
@@ -181,7 +223,7 @@ __device__ __forceinline__ void lj_pass_mixed(const int4 e4, int nvalid, const f
       const float ri2 = __fdividef(1.0f, r2);
       if (TYPES) {
         float ep = 0.f;
-        float fs = typed_pair<float>(tab[2 * tj[u]], tab[2 * tj[u] + 1], r2, ep);
+        float fs = typed_pair<float>(tab[3 * tj[u]], tab[3 * tj[u] + 1], tab[3 * tj[u] + 2], r2, ep);
         if (COUL) {
           const float qq = pi.w * pj[u].w;
           const float rinv = rsqrtf(r2);
@@ -245,14 +287,14 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
                            __fmul_rn((float)((int)((c >> 2) & 3u) - 1), st->Lf[1]),
                            __fmul_rn((float)((int)(c >> 4) - 1), st->Lf[2]), 0.f);
   }
-  __shared__ float4 tab[TYPES ? 2 * MD_MAX_TYPES * MD_MAX_TYPES : 1];
+  __shared__ float4 tab[TYPES ? 3 * MD_MAX_TYPES * MD_MAX_TYPES : 1];
   if (TYPES)
-    for (int c = threadIdx.x; c < 2 * nt * nt; c += blockDim.x) tab[c] = reinterpret_cast<const float4*>(ptab)[c];
+    for (int c = threadIdx.x; c < 3 * nt * nt; c += blockDim.x) tab[c] = reinterpret_cast<const float4*>(ptab)[c];
   __syncthreads();
   MixedAcc a;
   if (i < N) {
     const float4 pi = pos[i];
-    const float4* trow = TYPES ? tab + 2 * nt * (int)type[i] : tab;
+    const float4* trow = TYPES ? tab + 3 * nt * (int)type[i] : tab;
     const float rc = rcut[i];
     const float rc2 = __fmul_rn(rc, rc);
     int n = nnb[i];
@@ -311,11 +353,11 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
           const DevState* __restrict__ st, LJParams p, double4a* __restrict__ force, int overwrite,
           double* partials, unsigned* counter, double* stats, const double4a* __restrict__ corr,
           const int* __restrict__ id, const uint8_t* __restrict__ type, const void* __restrict__ ptab, int nt) {
-  __shared__ double4a tab[TYPES ? 2 * MD_MAX_TYPES * MD_MAX_TYPES : 1];
+  __shared__ double4a tab[TYPES ? 3 * MD_MAX_TYPES * MD_MAX_TYPES : 1];
   if (TYPES) {
     const double4a* src = reinterpret_cast<const double4a*>(reinterpret_cast<const float4*>(ptab) +
-                                                            2 * MD_MAX_TYPES * MD_MAX_TYPES);
-    for (int c = threadIdx.x; c < 2 * nt * nt; c += blockDim.x) tab[c] = src[c];
+                                                            3 * MD_MAX_TYPES * MD_MAX_TYPES);
+    for (int c = threadIdx.x; c < 3 * nt * nt; c += blockDim.x) tab[c] = src[c];
     __syncthreads();
   }
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -360,8 +402,8 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
         const double ri2 = 1.0 / r2;
         double fs, ep = 0.0;
         if (TYPES) {
-          const int c = 2 * (nt * (int)type[i] + (int)type[jj[u] & 0x03FFFFFF]);
-          fs = typed_pair<double>(tab[c], tab[c + 1], r2, ep);
+          const int c = 3 * (nt * (int)type[i] + (int)type[jj[u] & 0x03FFFFFF]);
+          fs = typed_pair<double>(tab[c], tab[c + 1], tab[c + 2], r2, ep);
         } else {
           const double s2 = p.sig2 * ri2;
           const double s6 = s2 * s2 * s2;
@@ -409,6 +451,35 @@ __global__ void k_clear_force(int N, double4a* f) {
 
 static const int kLanes = 8;
 
+// lj6_12_findCapR / lj6_12B_findCapR and the potential there (ENG/include/
+// NonBondedInteraction.h:1027-1073, :1204-1250): step the radius down by 0.95
+// from 0.95 rcut until the unbounded force reaches the cap, then bisect to
+// 1e-4; in the table's precision T
+template <class T>
+static T cap_force(bool bform, T eps, T sig, T rcut, T r) {
+  const T dr2 = r * r;
+  if (bform ? dr2 > rcut * rcut : dr2 >= rcut * rcut) return T(0);
+  const T ri = T(1) / r, ri2 = ri * ri, sri2 = sig * sig * ri2, sri6 = sri2 * sri2 * sri2;
+  return bform ? eps * (T(12) * sri6 * sri6 - T(12) * sri6) * ri : T(4) * eps * (T(12) * sri6 * sri6 - T(6) * sri6) * ri;
+}
+
+template <class T>
+static void cap_radius(bool bform, T eps, T sig, T shift, T rcut, T cap, T& capR, T& pcapR) {
+  T point = T(0.95) * rcut;
+  for (int it = 0; it < 4096 && cap_force<T>(bform, eps, sig, rcut, point) < cap; ++it) point *= T(0.95);
+  T lower = point, upper = rcut;
+  for (int it = 0; it < 200 && std::fabs(upper - lower) > 1e-4; ++it) {
+    const T mid = T(0.5) * (upper + lower);
+    if (cap_force<T>(bform, eps, sig, rcut, mid) > cap) lower = mid;
+    else upper = mid;
+  }
+  capR = T(0.5) * (upper + lower);
+  const T dr2 = capR * capR;
+  if (bform ? dr2 > rcut * rcut : dr2 >= rcut * rcut) { pcapR = T(0); return; }
+  const T ri = T(1) / capR, ri2 = ri * ri, sri2 = sig * sig * ri2, sri6 = sri2 * sri2 * sri2;
+  pcapR = bform ? eps * (sri6 * sri6 - T(2) * sri6 + shift) : T(4) * eps * (sri6 * sri6 - sri6) + shift;
+}
+
 int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats, bool overwrite,
                   Recorder* rec) {
   if (!eng->has_lj) { md_set_error("no non-bonded interaction registered"); return MD_ERR_BADARG; }
@@ -444,14 +515,14 @@ int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats,
       return MD_ERR_BADARG;
     }
     if (eng->tab_dirty || !eng->d_tab) {
-      const size_t nf = 2 * MD_MAX_TYPES * MD_MAX_TYPES;
+      const size_t nf = 3 * MD_MAX_TYPES * MD_MAX_TYPES;
       if (!eng->d_tab) MD_CUDA(cudaMalloc(&eng->d_tab, nf * (sizeof(float4) + sizeof(double4a))));
       std::vector<float4> tf(nf, make_float4(0.f, 0.f, 0.f, 0.f));
       std::vector<double4a> td(nf, double4a{0, 0, 0, 0});
       for (int a0 = 0; a0 < nt; ++a0)
         for (int a1 = 0; a1 < nt; ++a1) {
           const double* q = eng->nb_param[a0][a1];
-          const size_t c = 2 * (size_t)(a0 * nt + a1);
+          const size_t c = 3 * (size_t)(a0 * nt + a1);
           // derived parameters as the *Parameter::reinit of each kind forms them,
           // in binary32 for the mixed table and binary64 for the FP64 one
           switch (eng->nb_kind[a0][a1]) {
@@ -477,6 +548,39 @@ int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats,
               const double rcd = q[1] * pow(2.0, 1.0 / 6.0);
               td[c] = double4a{3.0, q[0], q[1], rcd};
               td[c + 1] = double4a{rcd + q[2], q[2] != 0 ? 1.0 / q[2] : 0.0, q[2] == 0 ? 1.0 : 0.0, 0};
+              break;
+            }
+            case MD_NB_LJ6_12_CAP:
+            case MD_NB_LJ6_12B_CAP: {
+              const bool bform = eng->nb_kind[a0][a1] == MD_NB_LJ6_12B_CAP;
+              const float kf = bform ? 6.f : 2.f;
+              const float sf = (float)q[1], rcf = (float)q[3], capf = (float)q[4];
+              float Rf, Pf;
+              cap_radius<float>(bform, (float)q[0], sf, (float)q[2], rcf, capf, Rf, Pf);
+              tf[c] = make_float4(kf, (float)q[0], sf * sf, (float)q[2]);
+              tf[c + 1] = make_float4(rcf, capf, Rf, Pf);
+              double Rd, Pd;
+              cap_radius<double>(bform, q[0], q[1], q[2], q[3], q[4], Rd, Pd);
+              td[c] = double4a{(double)kf, q[0], q[1] * q[1], q[2]};
+              td[c + 1] = double4a{q[3], q[4], Rd, Pd};
+              break;
+            }
+            case MD_NB_COSTAIL_CAP: {
+              // CosTail_cap::initParameter: the cap radius of LJ 6-12 (eps, b, shift 0,
+              // rcut rc) with the same cap
+              const float ef = (float)q[0], bf = (float)q[1], wf = (float)q[2], capf = (float)q[3];
+              const float rcf = bf * powf(2.f, 1.f / 6.f);
+              float Rf, Pf;
+              cap_radius<float>(false, ef, bf, 0.f, rcf, capf, Rf, Pf);
+              tf[c] = make_float4(4.f, ef, bf, rcf);
+              tf[c + 1] = make_float4(rcf + wf, wf != 0.f ? 1.f / wf : 0.f, wf == 0.f ? 1.f : 0.f, 0.f);
+              tf[c + 2] = make_float4(capf, Rf, Pf, 0.f);
+              const double rcd = q[1] * pow(2.0, 1.0 / 6.0);
+              double Rd, Pd;
+              cap_radius<double>(false, q[0], q[1], 0.0, rcd, q[3], Rd, Pd);
+              td[c] = double4a{4.0, q[0], q[1], rcd};
+              td[c + 1] = double4a{rcd + q[2], q[2] != 0 ? 1.0 / q[2] : 0.0, q[2] == 0 ? 1.0 : 0.0, 0};
+              td[c + 2] = double4a{q[3], Rd, Pd, 0};
               break;
             }
             default: break;  // kind 0: no interaction
@@ -535,11 +639,14 @@ extern "C" int md_engine_register_nb_pair(md_engine* e, int t0, int t1, int kind
     md_set_error("md_engine_register_nb_pair: bad arguments (types 0..%d)", MD_MAX_TYPES - 1);
     return MD_ERR_BADARG;
   }
-  bool ok = std::isfinite(param[0]) && std::isfinite(param[1]) && std::isfinite(param[2]) &&
-            std::isfinite(param[3]) && param[0] >= 0;
+  bool ok = param[0] >= 0;
+  for (int c = 0; c < 6; ++c) ok = ok && std::isfinite(param[c]);
   if (kind == MD_NB_LJ6_12) ok = ok && param[1] > 0;
   else if (kind == MD_NB_LJ6_12B) ok = ok && param[1] > 0 && param[3] > 0;
   else if (kind == MD_NB_COSTAIL) ok = ok && param[1] > 0 && param[2] >= 0;
+  else if (kind == MD_NB_LJ6_12_CAP || kind == MD_NB_LJ6_12B_CAP)
+    ok = ok && param[0] > 0 && param[1] > 0 && param[3] > 0 && param[4] > 0;
+  else if (kind == MD_NB_COSTAIL_CAP) ok = ok && param[0] > 0 && param[1] > 0 && param[2] >= 0 && param[3] > 0;
   else if (kind != MD_NB_NULL) ok = false;
   if (!ok) {
     md_set_error("md_engine_register_nb_pair: kind %d or its parameters out of range", kind);
@@ -547,7 +654,7 @@ extern "C" int md_engine_register_nb_pair(md_engine* e, int t0, int t1, int kind
   }
   for (int k = 0; k < 2; ++k) {
     const int a = k ? t1 : t0, b = k ? t0 : t1;
-    for (int c = 0; c < 4; ++c) e->nb_param[a][b][c] = param[c];
+    for (int c = 0; c < 6; ++c) e->nb_param[a][b][c] = param[c];
     e->nb_kind[a][b] = kind;
   }
   const int need = (t0 > t1 ? t0 : t1) + 1;
@@ -559,7 +666,7 @@ extern "C" int md_engine_register_nb_pair(md_engine* e, int t0, int t1, int kind
 }
 
 extern "C" int md_engine_register_lj_pair(md_engine* e, int t0, int t1, double eps, double sigma, double shift) {
-  const double q[4] = {eps, sigma, shift, 0.0};
+  const double q[6] = {eps, sigma, shift, 0.0, 0.0, 0.0};
   return md_engine_register_nb_pair(e, t0, t1, MD_NB_LJ6_12, q);
 }
 

@@ -172,8 +172,8 @@ struct md_engine {
   // nt > 0 selects the typed kernels; pairs not given take no force
   int nt = 0;
   int nb_kind[16][16] = {};        // md_nb_kind per type pair (symmetric), 0: none
-  double nb_param[16][16][4] = {};  // the kind's user parameters
-  void* d_tab = nullptr;            // float4 [2*16*16] then double4a [2*16*16]
+  double nb_param[16][16][6] = {};  // the kind's user parameters
+  void* d_tab = nullptr;            // float4 [3*16*16] then double4a [3*16*16]
   bool tab_dirty = false;
   bool has_coul = false;
   double beta = 0;

@@ -44,7 +44,7 @@ STAT_PRESSURE_CORR_XX = 8
 STAT_ELEC_REC, STAT_ELEC_SELF = 11, 12
 STAT_BOND_ENERGY = 13
 BOND_HARMONIC, BOND_FENE, BOND_FENE2 = 10000, 10001, 10002
-NB_NULL, NB_LJ6_12, NB_COSTAIL, NB_LJ6_12B = 0, 1, 3, 5
+NB_NULL, NB_LJ6_12, NB_LJ6_12_CAP, NB_COSTAIL, NB_COSTAIL_CAP, NB_LJ6_12B, NB_LJ6_12B_CAP = 0, 1, 2, 3, 4, 5, 6
 ANGLE_HARMONIC, ANGLE_COS0 = 20000, 20001
 STAT_COUNT = 16
 
@@ -342,8 +342,10 @@ class InteractionEngine:
 
     def registNonBondedPair(self, type0, type1, kind, params):
         """A pair kind of the nbForce dispatch for a type pair: NB_LJ6_12 (eps, sigma,
-        shift), NB_LJ6_12B (eps, sigma, shift, rcut), NB_COSTAIL (eps, b, wc), NB_NULL."""
-        q = np.zeros(4)
+        shift), NB_LJ6_12B (eps, sigma, shift, rcut), NB_LJ6_12_CAP / NB_LJ6_12B_CAP
+        (eps, sigma, shift, rcut, cap), NB_COSTAIL (eps, b, wc), NB_COSTAIL_CAP
+        (eps, b, wc, cap), NB_NULL."""
+        q = np.zeros(6)
         q[:len(params)] = params
         check(lib.md_engine_register_nb_pair(self.h, int(type0), int(type1), int(kind), _p(q)),
               "registNonBondedPair")

@@ -169,10 +169,10 @@ def lj_allpair_typed(pos, rcut, box, types, pairs, pos32=None, box32=None):
     n = p.shape[0]
     t = np.ascontiguousarray(types, np.int32)
     nt = int(max(max(max(k) for k in pairs) + 1, t.max() + 1))
-    tab = np.zeros((nt, nt, 4)); on = np.zeros((nt, nt), np.int32)
+    tab = np.zeros((nt, nt, 6)); on = np.zeros((nt, nt), np.int32)
     for (a, b), v in pairs.items():
-        kind, q = (1, tuple(v) + (0.0,)) if not isinstance(v[0], int) or len(v) != 2 else v
-        q = np.zeros(4) + np.pad(np.asarray(q, float), (0, 4 - len(q)))
+        kind, q = (1, tuple(v)) if not isinstance(v[0], int) or len(v) != 2 else v
+        q = np.pad(np.asarray(q, float), (0, 6 - len(q)))
         tab[a, b] = tab[b, a] = q
         on[a, b] = on[b, a] = kind
     rc = np.ascontiguousarray(rcut, np.float64)
@@ -790,7 +790,7 @@ def ref_bonded_term(ftype, uparam, d0, d1=None):
 
 def nb_pair(kind, uparam, prec, d):
     """One non-bonded pair of a kind (oracle_md.c): force on i, energy."""
-    u = np.zeros(4); u[:len(uparam)] = uparam
+    u = np.zeros(6); u[:len(uparam)] = uparam
     dd = np.ascontiguousarray(d, np.float64); f = np.zeros(3); e = C.c_double()
     _lib.orc_nb_pair(int(kind), _p(u, f64), int(prec), _p(dd, f64), _p(f, f64), C.byref(e))
     return f, e.value
@@ -800,7 +800,7 @@ def ref_nb_pair(kind, uparam, d):
     """The reference's own pair functions (oracle/_ref/libref_nb.so), binary32."""
     lib = C.CDLL(os.path.join(REF_DIR, "libref_nb.so"))
     lib.ref_nb_pair.argtypes = [i32, P(f64), P(f64), P(f64), P(f64)]
-    u = np.zeros(4); u[:len(uparam)] = uparam
+    u = np.zeros(6); u[:len(uparam)] = uparam
     dd = np.ascontiguousarray(d, np.float64); f = np.zeros(3); e = np.zeros(1)
     lib.ref_nb_pair(int(kind), _p(u, f64), _p(dd, f64), _p(f, f64), _p(e, f64))
     return f, float(e[0])

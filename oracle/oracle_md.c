@@ -276,7 +276,7 @@ void orc_lj_allpair_f64(int n, const double* pos, const double* rcut, double eps
 
 /* The same with atom types (AtomNBForceTable::calForceIndex, ENG/include/
    NonBondedInteraction.h:673-683): the pair (type_i, type_j) takes the pair kind
-   kind[type_i][type_j] with parameters tab[type_i][type_j][4] (nb_pair_d), or no force
+   kind[type_i][type_j] with parameters tab[type_i][type_j][6] (nb_pair_d), or no force
    and no energy where the kind is 0 (mdForceNULL). */
 /* One non-bonded pair of a kind of the nbForcePoten dispatch (ENG/include/
    NonBondedInteraction.h:556-600) for d = r_j - r_i: the force on i and the
@@ -286,6 +286,49 @@ void orc_lj_allpair_f64(int n, const double* pos, const double* rcut, double eps
      kind 3 CosTail (eps, b, wc)                        :1379-1440
    prec 0 follows the binary32 operations of those functions, prec 1 the same
    formulas in binary64 (the accurate cos and sin for the fast intrinsics). */
+/* lj6_12_findCapR / lj6_12B_findCapR with the potential at the cap radius
+   (NonBondedInteraction.h:1027-1073, :1204-1250), binary32 and binary64 */
+static float capf_force(int bform, float eps, float sig, float rcut, float r) {
+  const float dr2 = r * r;
+  if (bform ? dr2 > rcut * rcut : dr2 >= rcut * rcut) return 0.f;
+  const float ri = 1.f / r, ri2 = ri * ri, sri2 = sig * sig * ri2, sri6 = sri2 * sri2 * sri2;
+  return bform ? eps * (12.f * sri6 * sri6 - 12.f * sri6) * ri : 4.f * eps * (12.f * sri6 * sri6 - 6.f * sri6) * ri;
+}
+static void capf_radius(int bform, float eps, float sig, float sh, float rcut, float cap, float* R, float* P) {
+  float point = 0.95f * rcut;
+  while (capf_force(bform, eps, sig, rcut, point) < cap) point *= 0.95f;
+  float lower = point, upper = rcut;
+  while (fabsf(upper - lower) > 1e-4) {
+    const float mid = 0.5f * (upper + lower);
+    if (capf_force(bform, eps, sig, rcut, mid) > cap) lower = mid; else upper = mid;
+  }
+  *R = 0.5f * (upper + lower);
+  const float dr2 = *R * *R;
+  if (bform ? dr2 > rcut * rcut : dr2 >= rcut * rcut) { *P = 0.f; return; }
+  const float ri = 1.f / *R, ri2 = ri * ri, sri2 = sig * sig * ri2, sri6 = sri2 * sri2 * sri2;
+  *P = bform ? eps * (sri6 * sri6 - 2.f * sri6 + sh) : 4.f * eps * (sri6 * sri6 - sri6) + sh;
+}
+static double capd_force(int bform, double eps, double sig, double rcut, double r) {
+  const double dr2 = r * r;
+  if (bform ? dr2 > rcut * rcut : dr2 >= rcut * rcut) return 0.;
+  const double ri = 1. / r, ri2 = ri * ri, sri2 = sig * sig * ri2, sri6 = sri2 * sri2 * sri2;
+  return bform ? eps * (12. * sri6 * sri6 - 12. * sri6) * ri : 4. * eps * (12. * sri6 * sri6 - 6. * sri6) * ri;
+}
+static void capd_radius(int bform, double eps, double sig, double sh, double rcut, double cap, double* R, double* P) {
+  double point = 0.95 * rcut;
+  while (capd_force(bform, eps, sig, rcut, point) < cap) point *= 0.95;
+  double lower = point, upper = rcut;
+  while (fabs(upper - lower) > 1e-4) {
+    const double mid = 0.5 * (upper + lower);
+    if (capd_force(bform, eps, sig, rcut, mid) > cap) lower = mid; else upper = mid;
+  }
+  *R = 0.5 * (upper + lower);
+  const double dr2 = *R * *R;
+  if (bform ? dr2 > rcut * rcut : dr2 >= rcut * rcut) { *P = 0.; return; }
+  const double ri = 1. / *R, ri2 = ri * ri, sri2 = sig * sig * ri2, sri6 = sri2 * sri2 * sri2;
+  *P = bform ? eps * (sri6 * sri6 - 2. * sri6 + sh) : 4. * eps * (sri6 * sri6 - sri6) + sh;
+}
+
 static float nb_pair_f(int kind, const double* u, float dx, float dy, float dz, float* f) {
   const float dr2 = dx * dx + dy * dy + dz * dz;
   float sc = 0.f, e = 0.f;
@@ -300,12 +343,33 @@ static float nb_pair_f(int kind, const double* u, float dx, float dy, float dz, 
     const float ri2 = 1.f / dr2, sri2 = sig * sig * ri2, sri6 = sri2 * sri2 * sri2;
     sc = -b * eps * (12.f * sri6 * sri6 - 12.f * sri6) * ri2;
     e = b * (eps * (sri6 * sri6 - sri6 * 2.f + sh));
-  } else if (kind == 3) {
+  } else if (kind == 2 || kind == 6) {
+    const int bform = kind == 6;
+    const float eps = (float)u[0], sig = (float)u[1], sh = (float)u[2], rc = (float)u[3], cap = (float)u[4];
+    float R, P;
+    capf_radius(bform, eps, sig, sh, rc, cap, &R, &P);
+    if (bform ? dr2 > rc * rc : dr2 >= rc * rc) {
+    } else if (dr2 < R * R) {
+      const float s = 1.f / sqrtf(dx * dx + dy * dy + dz * dz);
+      sc = -s * cap;
+      e = -cap * (sqrtf(dr2) - R) + P;
+    } else {
+      const float ri2 = 1.f / dr2, sri2 = sig * sig * ri2, sri6 = sri2 * sri2 * sri2;
+      sc = -(bform ? eps * (12.f * sri6 * sri6 - 12.f * sri6) * ri2 : 4.f * eps * (12.f * sri6 * sri6 - 6.f * sri6) * ri2);
+      e = bform ? eps * (sri6 * sri6 - 2.f * sri6 + sh) : 4.f * eps * (sri6 * sri6 - sri6) + sh;
+    }
+  } else if (kind == 3 || kind == 4) {
     const float eps = (float)u[0], bv = (float)u[1], wc = (float)u[2];
     const float wci = wc != 0.f ? 1.f / wc : 0.f;
     const float rc = bv * powf(2.f, 1.f / 6.f), rcut = rc + wc;
     const float ri = 1.f / sqrtf(dr2);
-    if (dr2 <= rc * rc) {
+    float R = 0.f, P = 0.f;
+    if (kind == 4) capf_radius(0, eps, bv, 0.f, rc, (float)u[3], &R, &P);
+    if (kind == 4 && dr2 < R * R) {
+      const float s = 1.f / sqrtf(dx * dx + dy * dy + dz * dz);
+      sc = -s * (float)u[3];
+      e = -(float)u[3] * (sqrtf(dr2) - R) + P;
+    } else if (dr2 <= rc * rc) {
       const float sri = bv * ri, sri2 = sri * sri, sri6 = sri2 * sri2 * sri2;
       sc = -24.f * eps * (2.f * sri6 * sri6 - sri6) * ri * ri;
       e = 4.f * eps * (sri6 * sri6 - sri6);
@@ -333,12 +397,31 @@ static double nb_pair_d(int kind, const double* u, double dx, double dy, double 
     const double ri2 = 1. / dr2, sri2 = u[1] * u[1] * ri2, sri6 = sri2 * sri2 * sri2;
     sc = -b * u[0] * (12. * sri6 * sri6 - 12. * sri6) * ri2;
     e = b * (u[0] * (sri6 * sri6 - sri6 * 2. + u[2]));
-  } else if (kind == 3) {
+  } else if (kind == 2 || kind == 6) {
+    const int bform = kind == 6;
+    double R, P;
+    capd_radius(bform, u[0], u[1], u[2], u[3], u[4], &R, &P);
+    if (bform ? dr2 > u[3] * u[3] : dr2 >= u[3] * u[3]) {
+    } else if (dr2 < R * R) {
+      const double s = 1. / sqrt(dr2);
+      sc = -s * u[4];
+      e = -u[4] * (sqrt(dr2) - R) + P;
+    } else {
+      const double ri2 = 1. / dr2, sri2 = u[1] * u[1] * ri2, sri6 = sri2 * sri2 * sri2;
+      sc = -(bform ? u[0] * (12. * sri6 * sri6 - 12. * sri6) * ri2 : 4. * u[0] * (12. * sri6 * sri6 - 6. * sri6) * ri2);
+      e = bform ? u[0] * (sri6 * sri6 - 2. * sri6 + u[2]) : 4. * u[0] * (sri6 * sri6 - sri6) + u[2];
+    }
+  } else if (kind == 3 || kind == 4) {
     const double eps = u[0], bv = u[1], wc = u[2];
     const double wci = wc != 0. ? 1. / wc : 0.;
     const double rc = bv * pow(2., 1. / 6.), rcut = rc + wc;
     const double ri = 1. / sqrt(dr2);
-    if (dr2 <= rc * rc) {
+    double R = 0., P = 0.;
+    if (kind == 4) capd_radius(0, eps, bv, 0., rc, u[3], &R, &P);
+    if (kind == 4 && dr2 < R * R) {
+      sc = -ri * u[3];
+      e = -u[3] * (sqrt(dr2) - R) + P;
+    } else if (dr2 <= rc * rc) {
       const double sri = bv * ri, sri2 = sri * sri, sri6 = sri2 * sri2 * sri2;
       sc = -24. * eps * (2. * sri6 * sri6 - sri6) * ri * ri;
       e = 4. * eps * (sri6 * sri6 - sri6);
@@ -397,7 +480,7 @@ void orc_lj_allpair_typed(int n, const double* pos, const double* rcut, const in
       }
       if (!in) continue;
       double f[3];
-      const double e = nb_pair_d(kind[pr], tab + 4 * pr, dx, dy, dz, f);
+      const double e = nb_pair_d(kind[pr], tab + 6 * pr, dx, dy, dz, f);
       fx += f[0];
       fy += f[1];
       fz += f[2];

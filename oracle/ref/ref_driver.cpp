@@ -342,7 +342,8 @@ extern "C" int ref_bonded_term(int ftype, const double* u, const double* d0, con
 // The engine's non-bonded pair functions (include/NonBondedInteraction.h,
 // nbForcePoten dispatch) evaluated on the host in binary32 for one pair:
 // kind 1 LennardJones6_12 (eps, sigma, shift, rcut), 5 LennardJones6_12B
-// (eps, sigma, shift, rcut), 3 CosTail (eps, b, wc).
+// (eps, sigma, shift, rcut), 3 CosTail (eps, b, wc), 2 / 6 the capped LJ forms
+// (eps, sigma, shift, rcut, cap), 4 CosTail_cap (eps, b, wc, cap).
 #include "NonBondedInteraction.h"
 extern "C" int ref_nb_pair(int kind, const double* u, const double* d, double* f, double* e) {
   ScalorType p[16] = {0};
@@ -355,6 +356,17 @@ extern "C" int ref_nb_pair(int kind, const double* u, const double* d, double* f
       break;
     case mdForceCosTail:
       CosTail::initParameter(p, (ScalorType)u[0], (ScalorType)u[1], (ScalorType)u[2]);
+      break;
+    case mdForceLennardJones6_12_cap:
+      LennardJones6_12_cap::initParameter(p, (ScalorType)u[0], (ScalorType)u[1], (ScalorType)u[2],
+                                          (ScalorType)u[3], (ScalorType)u[4]);
+      break;
+    case mdForceLennardJones6_12B_cap:
+      LennardJones6_12B_cap::initParameter(p, (ScalorType)u[0], (ScalorType)u[1], (ScalorType)u[2],
+                                           (ScalorType)u[3], (ScalorType)u[4]);
+      break;
+    case mdForceCosTail_cap:
+      CosTail_cap::initParameter(p, (ScalorType)u[0], (ScalorType)u[1], (ScalorType)u[2], (ScalorType)u[3]);
       break;
     default: return 1;
   }

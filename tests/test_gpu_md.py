@@ -348,16 +348,20 @@ def test_typed_driver_and_arguments(mdf, fluid):
 
 
 KIND_PAIRS = {(0, 0): (1.0, 1.0, 0.0), (0, 1): (5, (1.1, 0.95, 0.1, 2.2)), (1, 1): (3, (1.0, 0.95, 1.6)),
-              (0, 2): (3, (0.8, 1.0, 0.0)), (2, 2): (1, (0.6, 1.05, -0.01))}  # (1, 2): none
+              (0, 2): (3, (0.8, 1.0, 0.0)), (2, 2): (1, (0.6, 1.05, -0.01)),
+              # capped forms with caps low enough that close pairs of the liquid reach them
+              (0, 3): (2, (1.0, 1.0, 0.0, 2.5, 5.0)), (3, 3): (6, (1.0, 1.0, 0.0, 2.2, 4.0)),
+              (1, 3): (4, (1.0, 0.95, 1.5, 5.0))}  # (1, 2), (2, 3): none
 
 
 @pytest.mark.parametrize("prec", [0, 1])
 def test_pair_kinds_vs_oracle(mdf, orc, small_slab, prec):
-    """LJ 6-12, LJ 6-12 B, CosTail (with and without its tail) and a missing pair
-    in one typed system (the nbForcePoten dispatch)."""
+    """Every pair kind of the nbForcePoten dispatch in one typed system: LJ 6-12,
+    LJ 6-12 B, CosTail with and without its tail, the three capped forms and
+    missing pairs."""
     s = small_slab
     rc = adaptive_rcut(s.n, seed=5)
-    types = np.random.default_rng(10).integers(0, 3, s.n)
+    types = np.random.default_rng(10).integers(0, 4, s.n)
     sys = mdf.MDSystem(s.pos, s.box, precision=prec, type=types)
     sys.set_rcut(rc)
     cl = mdf.CellList(sys, 2.8)

@@ -4,7 +4,8 @@ dispatch) compiled as host code in oracle/_ref: bit-equal in binary32."""
 import numpy as np
 import pytest
 
-KINDS = [(1, (1.2, 0.9, 0.05, 3.0)), (5, (1.1, 1.0, 0.1, 2.2)), (3, (1.0, 0.95, 1.6)), (3, (1.0, 0.95, 0.0))]
+KINDS = [(1, (1.2, 0.9, 0.05, 3.0)), (5, (1.1, 1.0, 0.1, 2.2)), (3, (1.0, 0.95, 1.6)), (3, (1.0, 0.95, 0.0)),
+         (2, (1.2, 0.9, 0.05, 2.5, 50.0)), (6, (1.1, 1.0, 0.1, 2.2, 40.0)), (4, (1.0, 0.95, 1.6, 30.0))]
 
 
 @pytest.mark.parametrize("kind,u", KINDS)
@@ -14,7 +15,7 @@ def test_pairs_equal_the_reference_header(orc, kind, u):
     rng = np.random.default_rng(kind)
     for _ in range(1000):
         d = rng.normal(size=3)
-        d *= rng.uniform(0.85, 3.0) / np.linalg.norm(d)
+        d *= rng.uniform(0.6, 3.0) / np.linalg.norm(d)  # the capped kinds' cores included
         f, e = orc.nb_pair(kind, u, 0, d)
         rf, re = orc.ref_nb_pair(kind, u, d)
         assert np.array_equal(f, rf) and e == re
