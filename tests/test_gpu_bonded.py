@@ -205,3 +205,33 @@ def test_bad_topologies_are_rejected(mdf, poly):
         eng.setExclusions([[3, 3]])
     with pytest.raises(mdf.MDExcptBadArgument):
         eng.registBondedInteraction(3)
+
+
+def test_topology_path_equals_direct_lists(mdf, poly):
+    """Molecules and copy numbers (Topology::System) give the same bonded forces
+    as the expanded lists handed over directly."""
+    s = poly
+    t = mdf.topology
+    length = 12
+    chain = t.Molecule("chain")
+    for _ in range(length):
+        chain.pushAtom(t.Atom("B", 0, 1.0, 0.0))
+    for k in range(length - 1):
+        chain.addBond(t.Bond(k, k + 1, mdf.BOND_FENE, (30.0, 1.5)))
+    for k in range(length - 2):
+        chain.addAngle(t.Angle(k, k + 1, k + 2, mdf.ANGLE_COS0, (3.0,)))
+    top = t.System()
+    top.addMolecules(chain, s["n"] // length)
+    a = mdf.MDSystem(s["pos"], s["box"], precision=1)
+    ea = mdf.InteractionEngine(a)
+    e = t.registBondedInteraction(ea, top)
+    t.initTopology(a, top)
+    ea.clearInteraction()
+    ea.applyBondedInteraction(a)
+    b = mdf.MDSystem(s["pos"], s["box"], precision=1)
+    eb = mdf.InteractionEngine(b)
+    eb.setBonds(e["bonds"], mdf.BOND_FENE, (30.0, 1.5))
+    eb.setAngles(e["angles"], mdf.ANGLE_COS0, (3.0,))
+    eb.clearInteraction()
+    eb.applyBondedInteraction(b)
+    assert np.array_equal(a.forces(), b.forces())
