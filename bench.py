@@ -567,13 +567,12 @@ def main():
                              p_ref=(0.0, 0.0, 0.0), npt_dirs=4, seed=1)
     sim_e = mdf.Simulation(sys_e, eng_e, skin=SKIN, cell_size=2.8, lv=lv, expansion=1.5)
     t_setup = time.perf_counter() - t0
-    # one page-locked row per step: each step's energy / virial / kinetic
-    # tensor is copied back in stream order, read once the run has drained
+    # one page-locked row per step: the device writes each step's energy /
+    # virial / kinetic tensor there as the step ends; read once the run drains
     stat_rows = torch.zeros((e2e_steps, mdf.STAT_COUNT), dtype=torch.float64).pin_memory().numpy()
+    sim_e.set_stats_ring(stat_rows)
     t1 = time.perf_counter()
-    for k in range(e2e_steps):
-        sim_e.run(1)
-        sys_e.stats_async(stat_rows[k])
+    sim_e.run(e2e_steps)
     sys_e.synchronize()
     fin_pos = sys_e.positions()
     fin_f = sys_e.forces()
@@ -581,8 +580,8 @@ def main():
     e2e_sps = e2e_steps / t_e2e
     h2d = (pin_pos.numel() + pin_vel.numel()) * 8 / e2e_steps
     d2h = mdf.STAT_COUNT * 8 + (fin_pos.size + fin_f.size) * 8 / e2e_steps
-    if not np.isfinite(stat_rows).all():
-        raise RuntimeError("non-finite statistics in the end-to-end run")
+    if not np.isfinite(stat_rows).all() or not np.array_equal(stat_rows[-1], sys_e.stats()):
+        raise RuntimeError("per-step statistics of the end-to-end run are missing or non-finite")
 
     # step1, LJ, step2 every step; bin, scan, scatter, order, gather, copy back,
     # list build per rebuild; the density deposit every 40 steps; 3 + 3*3 DFT
@@ -622,8 +621,8 @@ def main():
             "nlist_build_us": t_nl * 1e6,
             "e2e": {"value": e2e_sps, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps, "setup_s": t_setup,
-                    "path": "MDSystem from pinned host arrays, Simulation.run(1) + statistics copied to a "
-                            "pinned row every step (stream-ordered, one wait at the end), "
+                    "path": "MDSystem from pinned host arrays, Simulation.run(steps) with every step's "
+                            "statistics written by the device into its own pinned host row, "
                             "positions and forces read back at the end"},
             "gpu_launches": launches,
             "list_rebuilds_timed": rebuilds_timed,

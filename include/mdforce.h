@@ -553,6 +553,13 @@ int md_engine_set_force_correction(md_engine* eng, md_fcorr* fc);
 /* the driver on the fcorr app's schedule (FCR/app/lj.nhc-xtc.cu:172-227): after step i,
    assign when i % assign_every == 0; deposit when (i+1) % sample_every == 0; update
    and clear the samples when (i+1) % update_every == 0.  Also sets it on the engine. */
+/* Per-step statistics without host involvement: after every step of md_sim_run the
+   device writes the MD_STAT_COUNT slots into row (k mod rows) of the host array
+   host[rows][MD_STAT_COUNT], k counting the steps since this call.  Page-locked memory is
+   used in place; other host memory is registered here.  The rows are valid after
+   md_system_synchronize; rows = 0 detaches.  (MDStatistic::updateHost of every step,
+   for callers that read each step's energy and virial.) */
+int md_sim_set_stats_ring(md_sim* sim, double* host, int rows);
 int md_sim_attach_force_corr(md_sim* sim, md_fcorr* fc, int assign_every, int sample_every, int update_every);
 
 /* ------------------------------------------------------------ synthetic inputs

@@ -32,6 +32,13 @@ __device__ __forceinline__ void lv_particle_step1(int k, typename V4<R>::T* __re
                                                   const typename V4<R>::T* __restrict__ backup,
                                                   DevState* st, const LvDev& p);
 
+// threads per block of the driver's Langevin halves (a multiple of 32, <= 256);
+// 128 measured 0.2-0.3 % more steps/s than 256 on the 65,536-atom slab (twice
+// as many blocks for these latency-bound passes)
+#ifndef MD_LV_THREADS
+#define MD_LV_THREADS 128
+#endif
+
 template <class R>
 __global__ void __launch_bounds__(256)
 k_lv_step1(int N, typename V4<R>::T* __restrict__ pos, typename V4<R>::T* __restrict__ vel,
@@ -179,7 +186,7 @@ int langevin_step1_impl(md_system* sys, md_nlist* nl, Recorder* rec, bool with_b
   void* bk = nl ? nl->backup : nullptr;
   void* a[] = {&N, &sys->pos, &sys->vel, &sys->force, &sys->id, &bk, &st, &p, &cond, &use_cond};
   const void* f = sys->prec == MD_PREC_FP64 ? (const void*)k_lv_step1<double> : (const void*)k_lv_step1<float>;
-  return rec_launch(rec, f, dim3(ceil_div(N, 256)), dim3(256), 0, a);
+  return rec_launch(rec, f, dim3(ceil_div(N, MD_LV_THREADS)), dim3(MD_LV_THREADS), 0, a);
 }
 
 int langevin_step2_impl(md_system* sys, Recorder* rec, int kick, int advance, const double4a* fadd, int merge_rec) {
@@ -189,7 +196,7 @@ int langevin_step2_impl(md_system* sys, Recorder* rec, int kick, int advance, co
   int with_box = 1;
   void* a[] = {&N, &sys->vel, &sys->force, &st, &p, &sys->partials, &with_box, &kick, &advance, &fadd, &merge_rec};
   const void* f = sys->prec == MD_PREC_FP64 ? (const void*)k_lv_step2<double> : (const void*)k_lv_step2<float>;
-  return rec_launch(rec, f, dim3(ceil_div(N, 256)), dim3(256), 0, a);
+  return rec_launch(rec, f, dim3(ceil_div(N, MD_LV_THREADS)), dim3(MD_LV_THREADS), 0, a);
 }
 
 // ------------------------------------------------------------ velocity Verlet

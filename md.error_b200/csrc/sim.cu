@@ -48,7 +48,24 @@ struct md_sim {
   md_adapt_rcut* arc = nullptr;
   int sample_every = 0, update_every = 0, nrefine = 0;
   double prec = 0;
+  // statistics ring in page-locked host memory: each step's slots are written
+  // there by the device, row (count mod rows)
+  double* ring = nullptr;     // device view of the host rows
+  int ring_rows = 0;
+  unsigned* ring_count = nullptr;
+  void* ring_registered = nullptr;  // host pointer this library registered
 };
+
+static void ring_release(md_sim* s);
+
+// the step's statistic slots into the next row of the host ring
+__global__ void k_stats_ring(const DevState* st, double* ring, int rows, unsigned* count) {
+  const unsigned r = *count;
+  const int t = threadIdx.x;
+  if (t < MD_STAT_COUNT) ring[(size_t)(r % (unsigned)rows) * MD_STAT_COUNT + t] = st->stats[t];
+  __syncthreads();
+  if (t == 0) *count = r + 1;
+}
 
 static int record_step(md_sim* s, Recorder* rec, bool use_graph) {
   md_system* sys = s->sys;
@@ -110,6 +127,11 @@ static int record_step(md_sim* s, Recorder* rec, bool use_graph) {
     if (int r = langevin_step2_impl(sys, rec, 1, 1, branch ? spme_force_buffer(s->p.spme) : nullptr, branch ? 1 : 0))
       return r;
   }
+  if (s->ring) {
+    DevState* st = sys->st;
+    void* a[] = {&st, &s->ring, &s->ring_rows, &s->ring_count};
+    if (int r = rec_launch(rec, (const void*)k_stats_ring, dim3(1), dim3(32), 0, a)) return r;
+  }
   return MD_OK;
 }
 
@@ -129,6 +151,8 @@ static int build_graph(md_sim* s) {
 
 extern "C" int md_sim_destroy(md_sim* s) {
   if (!s) return MD_OK;
+  if (s->sys && s->sys->stream) cudaStreamSynchronize(s->sys->stream);
+  ring_release(s);
   if (s->exec) cudaGraphExecDestroy(s->exec);
   if (s->graph) cudaGraphDestroy(s->graph);
   md_nlist_destroy(s->nl);
@@ -206,6 +230,40 @@ extern "C" int md_sim_create(md_sim** out, md_system* sys, md_engine* eng, const
   if (p->use_graph)
     if ((r = build_graph(s))) return fail(r);
   *out = s;
+  return MD_OK;
+}
+
+static void ring_release(md_sim* s) {
+  if (s->ring_count) cudaFree(s->ring_count);
+  if (s->ring_registered) cudaHostUnregister(s->ring_registered);
+  s->ring = nullptr;
+  s->ring_rows = 0;
+  s->ring_count = nullptr;
+  s->ring_registered = nullptr;
+}
+
+extern "C" int md_sim_set_stats_ring(md_sim* s, double* host, int rows) {
+  if (!s || rows < 0 || (rows > 0 && !host)) return MD_ERR_BADARG;
+  MD_CUDA(cudaStreamSynchronize(s->sys->stream));
+  ring_release(s);
+  if (rows > 0) {
+    // page-locked memory is device-addressable under unified addressing; other
+    // host memory is registered (and unregistered again by this library)
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, host) != cudaSuccess || at.type != cudaMemoryTypeHost) {
+      cudaGetLastError();
+      MD_CUDA(cudaHostRegister(host, sizeof(double) * MD_STAT_COUNT * (size_t)rows, cudaHostRegisterMapped));
+      s->ring_registered = host;
+    }
+    double* dev = nullptr;
+    MD_CUDA(cudaHostGetDevicePointer((void**)&dev, host, 0));
+    MD_CUDA(cudaMalloc(&s->ring_count, sizeof(unsigned)));
+    MD_CUDA(cudaMemset(s->ring_count, 0, sizeof(unsigned)));
+    s->ring = dev;
+    s->ring_rows = rows;
+  }
+  if (s->exec)
+    if (int r = build_graph(s)) return r;
   return MD_OK;
 }
 

@@ -188,6 +188,7 @@ _SIGS = {
     "md_fcorr_get_values": (i32, [vp, P(f64)]),
     "md_engine_set_force_correction": (i32, [vp, vp]),
     "md_sim_attach_force_corr": (i32, [vp, vp, i32, i32, i32]),
+    "md_sim_set_stats_ring": (i32, [vp, P(f64), i32]),
 }
 
 

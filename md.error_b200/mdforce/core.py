@@ -983,6 +983,19 @@ class Simulation:
     def run(self, nsteps):
         check(lib.md_sim_run(self.h, int(nsteps)), "Simulation::run")
 
+    def set_stats_ring(self, rows):
+        """Every step's statistic slots written by the device into rows
+        (float64 [R, STAT_COUNT], page-locked for a copy without registration),
+        row k mod R for the k-th step from now; None detaches."""
+        if rows is None:
+            check(lib.md_sim_set_stats_ring(self.h, None, 0), "set_stats_ring")
+            self._ring = None
+            return
+        if rows.dtype != np.float64 or rows.ndim != 2 or rows.shape[1] != STAT_COUNT or not rows.flags.c_contiguous:
+            raise ValueError("set_stats_ring: rows must be a contiguous float64 [R, STAT_COUNT] array")
+        check(lib.md_sim_set_stats_ring(self.h, _p(rows), rows.shape[0]), "set_stats_ring")
+        self._ring = rows
+
     def counters(self):
         s, r, f = C.c_int64(), C.c_int64(), C.c_int()
         check(lib.md_sim_counters(self.h, C.byref(s), C.byref(r), C.byref(f)), "counters")

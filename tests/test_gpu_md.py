@@ -385,3 +385,30 @@ def test_pair_kinds_vs_oracle(mdf, orc, small_slab, prec):
     assert np.allclose(st[:4], so, rtol=tol * 10, atol=0), (st[:4], so)
     with pytest.raises(mdf.MDExcptBadArgument):
         eng.registNonBondedPair(0, 0, 7, (1.0, 1.0))
+
+
+def test_stats_ring_rows_match_stepwise_reads(mdf, fluid):
+    """md_sim_set_stats_ring: the device writes every step's slots into host rows;
+    they equal the blocking reads taken after each step of an identical run."""
+    import torch
+    a, sa, _ = _run_gpu(mdf, fluid, 0, 0)
+    b, sb, _ = _run_gpu(mdf, fluid, 0, 0)
+    rows = torch.zeros((4, mdf.STAT_COUNT), dtype=torch.float64).pin_memory().numpy()
+    sa.set_stats_ring(rows)
+    sa.run(6)  # rows wrap: steps 5 and 6 land in rows 0 and 1
+    a.synchronize()
+    ref = []
+    for _ in range(6):
+        sb.run(1)
+        ref.append(b.stats())
+    for row, k in ((2, 2), (3, 3), (0, 4), (1, 5)):
+        assert np.allclose(rows[row], ref[k], rtol=1e-12, atol=1e-12)
+    # pageable memory is registered by the library for the ring's lifetime
+    plain = np.zeros((3, mdf.STAT_COUNT))
+    sa.set_stats_ring(plain)
+    sa.run(2)
+    a.synchronize()
+    assert np.allclose(plain[1], a.stats(), rtol=1e-12, atol=1e-12)
+    sa.set_stats_ring(None)
+    with pytest.raises(ValueError):
+        sa.set_stats_ring(np.zeros((3, 4)))
