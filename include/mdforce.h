@@ -374,6 +374,9 @@ int md_errmap_self_error(md_errmap* h, double* out);
 /* FConvRho1_{x,y,z} of the analytic map for alias index k (0 < |k| <= 2) and the current
    profile: IFFT(FFT(rho1 V/N) V F_d(k)) / V, out [3][K0][K1][K2][2] (print_error columns) */
 int md_errmap_ana_fconv(md_errmap* h, int k, double* out);
+/* print_meanf of the maps: the signed mean force error field
+   e1_d = Re IFFT(k1_d FFT(rho1 V/N)) charge / V of the current profile, out [3][K0][K1][K2] */
+int md_errmap_mean_force(md_errmap* h, double charge, double* out);
 
 /* ------------------------------------------------------- per-atom cutoff
  * Replaces AssignRCut::getRCut + assign (ENG/src/AssignRCut.cu:46-117):

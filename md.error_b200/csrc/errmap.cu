@@ -758,8 +758,9 @@ extern "C" int md_errmap_deposit(md_errmap* h, md_system* sys) {
 
 // ErrorEstimate_SPME_Ik::calError: error1 [N][2], error2 [N][2] (real, imaginary);
 // the RMS force error of a grid point is sqrt(error1[i][0] + error2[i][0])
-extern "C" int md_errmap_compute(md_errmap* h, double charge, double* error1, double* error2) {
-  if (!h || !error1 || !error2) return MD_ERR_BADARG;
+// the convolutions of calError: work[0..3) = IFFT(k1_d FFT(rho1 V/N)),
+// work[3] = IFFT(k2a FFT(rho2 V/N)), unscaled
+static int em_convolve(md_errmap* h) {
   MD_CUDA(cudaSetDevice(h->device));
   cudaStream_t s = h->stream;
   const long N = h->g.N;
@@ -767,7 +768,36 @@ extern "C" int md_errmap_compute(md_errmap* h, double charge, double* error1, do
   k_em_load<<<nb, 256, 0, s>>>(h->g, h->rho, h->rho + N, h->work2);
   if (int r = dft3_grid(h->work2, h->g.K, -1, 2, s)) return r;
   k_em_mult<<<nb, 256, 0, s>>>(h->g, h->k1, h->k2a, h->work2, h->work);
-  if (int r = dft3_grid(h->work, h->g.K, +1, 4, s)) return r;
+  return dft3_grid(h->work, h->g.K, +1, 4, s);
+}
+
+__global__ void k_em_meanf(long N, const double2* e, double scale, double* out) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= 3 * N) return;
+  out[t] = e[t].x * scale;
+}
+
+// print_meanf of the maps (ErrorEstimate_SPME_Ana.cpp:806-842): the mean force error
+// field e1_d = Re IFFT(k1_d FFT(rho1 V/N)) q / V, out [3][K0][K1][K2]
+extern "C" int md_errmap_mean_force(md_errmap* h, double charge, double* out) {
+  if (!h || !out) return MD_ERR_BADARG;
+  if (int r = em_convolve(h)) return r;
+  const long N = h->g.N;
+  const double V = h->g.L[0] * h->g.L[1] * h->g.L[2];
+  double* d = reinterpret_cast<double*>(h->work2);  // 2N complex = 4N doubles >= 3N
+  k_em_meanf<<<(unsigned)((3 * N + 255) / 256), 256, 0, h->stream>>>(N, h->work, charge / V, d);
+  MD_CHECK_LAUNCH("errmap mean force");
+  MD_CUDA(cudaMemcpyAsync(out, d, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, h->stream));
+  MD_CUDA(cudaStreamSynchronize(h->stream));
+  return MD_OK;
+}
+
+extern "C" int md_errmap_compute(md_errmap* h, double charge, double* error1, double* error2) {
+  if (!h || !error1 || !error2) return MD_ERR_BADARG;
+  if (int r = em_convolve(h)) return r;
+  cudaStream_t s = h->stream;
+  const long N = h->g.N;
+  const unsigned nb = (unsigned)((N + 255) / 256);
   double* d = reinterpret_cast<double*>(h->work2);  // 4N doubles: error1, error2
   k_em_finish<<<nb, 256, 0, s>>>(h->g, h->work, charge, d, d + 2 * N);
   MD_CHECK_LAUNCH("errmap compute");

@@ -163,6 +163,7 @@ _SIGS = {
     "md_errmap_create_ana": (i32, [P(vp), P(i32), P(f64), f64, i32, i32]),
     "md_errmap_self_error": (i32, [vp, P(f64)]),
     "md_errmap_ana_fconv": (i32, [vp, i32, P(f64)]),
+    "md_errmap_mean_force": (i32, [vp, f64, P(f64)]),
     "md_errmap_set_profile": (i32, [vp, P(f64), P(f64)]),
     "md_errmap_deposit": (i32, [vp, vp]),
     "md_errmap_get_profile": (i32, [vp, P(f64), P(f64)]),

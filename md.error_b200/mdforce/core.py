@@ -538,6 +538,12 @@ class ErrorEstimate_SPME_Ik:
         e1, e2 = self.calError(charge)
         return np.sqrt(e1[..., 0] + e2[..., 0])
 
+    def mean_force(self, charge=1.0):
+        """The signed mean force error field e1_d (print_meanf): [3, K...]."""
+        out = np.empty((3,) + self.K)
+        check(lib.md_errmap_mean_force(self.h, float(charge), _p(out)), "mean_force")
+        return out
+
 
 class ErrorEstimate_dir(ErrorEstimate_SPME_Ik):
     """ErrorEstimate_dir (analyze tools): reinit(beta, rcut, dp) builds the

@@ -301,3 +301,18 @@ def test_self_correction(mdf, orc, small, prec):
         sp.self_correction()
         Fo = orc.spme_selfcorr(sys.positions(), q, box, K, order, 1.3)
         assert np.abs(sys.forces() - Fo).max() < (1e-6 if prec == 0 else 1e-13) * np.abs(Fo).max()
+
+
+def test_mean_force_field_matches_the_error1_components(mdf, orc):
+    """print_meanf: the signed mean force error field; its squares summed over
+    the three components are error1's real part."""
+    K, box = (8, 8, 16), (3.0, 3.0, 6.0)
+    rng = np.random.default_rng(6)
+    rho1 = rng.normal(0, 5, K)
+    rho2 = np.abs(rng.normal(30, 5, K))
+    for em in (mdf.ErrorEstimate_SPME_Ik(K, box, 2.5, 4), mdf.ErrorEstimate_SPME_Ana(K, box, 2.5, 4)):
+        em.set_profile(rho1, rho2)
+        mf = em.mean_force(1.3)
+        e1, _ = em.calError(1.3)
+        assert mf.shape == (3,) + K
+        assert np.allclose((mf ** 2).sum(axis=0), e1[..., 0], rtol=1e-12, atol=1e-14 * np.abs(e1[..., 0]).max())
