@@ -119,6 +119,11 @@ int md_system_get_forces(md_system* sys, double* force);
 /* per-atom charges [N] in original order (MDSystem ddata.charge) */
 int md_system_set_charges(md_system* sys, const double* charge);
 int md_system_get_charges(md_system* sys, double* charge);
+/* per-atom masses [N] in original order (MDSystem hdata.mass / massi, copied by
+   MDSystem::initTopology, shortRange.inhomo/template/tools.collision/cal.real.error/src/
+   MDSystem_interface.cu:125-127); every mass must be positive */
+int md_system_set_masses(md_system* sys, const double* mass);
+int md_system_get_masses(md_system* sys, double* mass);
 int md_system_get_box(md_system* sys, double box[3]);
 int md_system_set_box(md_system* sys, const double box[3]);
 /* per-atom cutoff rcut_i in original order (MDSystem ddata.rcut) */
@@ -329,9 +334,10 @@ int md_error_estimate_spme_ik(md_system* sys, const int K[3], int order, double 
  * callers that reserve all device memory in their own pool or must keep the stream
  * allocator from growing between steps. No counterpart in the reference. Its scratch
  * is one fixed 180 KiB array per device: meshes up to K0*K1*K2 = 4,194,304 points
- * (larger ones give MD_ERR_BADARG); the first call on a device looks the array up
- * and should come before any stream capture; calls that overlap in time on one
- * device race on the shared scratch. */
+ * (larger ones give MD_ERR_BADARG). Each call looks the array's device address up,
+ * waits for the system's stream and copies its tables from pageable host memory, so
+ * it must not be called while that stream is being captured. Calls that overlap in
+ * time on one device race on the shared scratch. */
 int md_error_estimate_spme_ik_noalloc(md_system* sys, const int K[3], int order, double beta, double* err);
 /* splitting beta whose real-space estimate equals target at cutoff rcut */
 int md_choose_beta(md_system* sys, double rcut, double target, double* beta);
@@ -556,6 +562,7 @@ int md_engine_set_force_correction(md_engine* eng, md_fcorr* fc);
 /* the driver on the fcorr app's schedule (FCR/app/lj.nhc-xtc.cu:172-227): after step i,
    assign when i % assign_every == 0; deposit when (i+1) % sample_every == 0; update
    and clear the samples when (i+1) % update_every == 0.  Also sets it on the engine. */
+int md_sim_attach_force_corr(md_sim* sim, md_fcorr* fc, int assign_every, int sample_every, int update_every);
 /* Per-step statistics without host involvement: after every step of md_sim_run the
    device writes the MD_STAT_COUNT slots into row (k mod rows) of the host array
    host[rows][MD_STAT_COUNT], k counting the steps since this call.  Page-locked memory is
@@ -563,7 +570,6 @@ int md_engine_set_force_correction(md_engine* eng, md_fcorr* fc);
    md_system_synchronize; rows = 0 detaches.  (MDStatistic::updateHost of every step,
    for callers that read each step's energy and virial.) */
 int md_sim_set_stats_ring(md_sim* sim, double* host, int rows);
-int md_sim_attach_force_corr(md_sim* sim, md_fcorr* fc, int assign_every, int sample_every, int update_every);
 
 /* ------------------------------------------------------------ synthetic inputs
  * Seeded generators of the benchmark systems (host only, no GPU needed).  The

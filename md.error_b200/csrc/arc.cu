@@ -350,7 +350,15 @@ __global__ void k_pc_multiply(long nele, int nrc, const double2* rhok, double sc
   }
 }
 
-// p_aa = sum_i 0.5 conv_aa[idx_i](i) rho_i dv / V^2 (PressureCorrection::correction)
+// PressureCorrection::correction (ENG/src/PressureCorrection.cu:175-211) adds the
+// new sum to the members pxx, pyy, pzz, which it never resets, and then divides
+// them by V: p_new = (p_old + S / V) / V with S = sum_i 0.5 conv_aa[idx_i](i)
+// rho_i dv.  The old value's share is scaled here; k_pc_reduce then adds S / V^2.
+__global__ void k_pc_carry(double* p, double inv_volume) {
+  if (threadIdx.x < 3) p[threadIdx.x] *= inv_volume;
+}
+
+// p_aa += sum_i 0.5 conv_aa[idx_i](i) rho_i dv / V^2
 __global__ void k_pc_reduce(long nele, int nrc, const double2* work, const int* idx, const double* rho,
                             double fac, double* partials, unsigned* counter, double* out) {
   long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -359,7 +367,7 @@ __global__ void k_pc_reduce(long nele, int nrc, const double2* work, const int* 
     const int c = idx[i];
     for (int d = 0; d < 3; ++d) v[d] = 0.5 * work[((long)d * nrc + c) * nele + i].x * rho[i] * fac;
   }
-  block_reduce_finish<3>(v, partials, counter, out, true);
+  block_reduce_finish<3>(v, partials, counter, out, false);
 }
 
 __global__ void k_store_pcorr(const double* p, DevState* st) {
@@ -434,6 +442,7 @@ extern "C" int md_arc_create(md_adapt_rcut** out, md_system* sys, double refh, d
   cudaMemcpyAsync(a->d_rc, a->rc.data(), sizeof(double) * nrc, cudaMemcpyHostToDevice, a->sys->stream);
   cudaMemsetAsync(a->counts, 0, sizeof(double) * ne, a->sys->stream);
   cudaMemsetAsync(a->rho, 0, sizeof(double) * ne, a->sys->stream);
+  cudaMemsetAsync(a->pcorr, 0, sizeof(double) * 3, a->sys->stream);  // pxx = pyy = pzz = 0 (:82)
   if (int r = build_tables(a)) { md_arc_destroy(a); return r; }
   *out = a;
   return MD_OK;
@@ -542,6 +551,8 @@ extern "C" int md_arc_update(md_adapt_rcut* a, double prec, int nrefine) {
   if (int r = dft3(a, a->work, +1, 3 * a->nrc)) return r;
   const double dv = (hs.L[0] / a->n[0]) * (hs.L[1] / a->n[1]) * (hs.L[2] / a->n[2]);
   if (nb > sys->max_partial_blocks) { md_set_error("partials buffer too small"); return MD_ERR_BADARG; }
+  k_pc_carry<<<1, 32, 0, a->sys->stream>>>(a->pcorr, 1.0 / V);
+  MD_CHECK_LAUNCH("pc carry");
   k_pc_reduce<<<nb, 256, 0, a->sys->stream>>>(ne, a->nrc, a->work, a->rcidx, a->rho, dv / (V * V), sys->partials,
                                          &sys->st->red_counter[RED_MISC], a->pcorr);
   MD_CHECK_LAUNCH("pc reduce");

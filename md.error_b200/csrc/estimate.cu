@@ -5,7 +5,6 @@
 //   ElectrostaticInteraction_rec_BSpline::errorEstimate    RE/src/EleRecBSpline.cpp:154-206
 //   EleEcalculator (produce4Item)                          RE/src/EleEcalculator.cpp:100-220
 #include <cmath>
-#include <mutex>
 #include <vector>
 #include "device_common.cuh"
 
@@ -165,34 +164,31 @@ extern "C" int md_error_estimate_spme_ik(md_system* sys, const int K[3], int ord
 // (160^3 fits; 256^3 does not) and larger ones are rejected with
 // MD_ERR_BADARG. All calls on one device share the scratch: two calls that
 // overlap in time (different streams or host threads on one device) race and
-// return wrong estimates; calls issued one after the other are safe.
+// return wrong estimates; calls issued one after the other are safe. The call
+// waits for the system's stream (it reads the charges and the result back)
+// and copies its tables from pageable host memory, so it must not be issued
+// while that stream is being captured into a CUDA graph.
 constexpr int EST_TAB = 3 * 1025;
 constexpr int EST_NOALLOC_MAX_BLOCKS = 16384;
 constexpr int EST_NOALLOC_MAX_DEVICES = 64;
 static __device__ __align__(256) double g_est_scratch[2 * EST_TAB + EST_NOALLOC_MAX_BLOCKS];  // 180 KiB
 
-// Device address of g_est_scratch on `device`, looked up once per device with
-// that device current (the first call on a device does this setup, so it
-// should come before any stream capture that includes the entry point).
+// Device address of g_est_scratch on `device`, looked up with that device
+// current on every call (the lookup is cheap once the module is loaded, and a
+// fresh lookup stays valid after a cudaDeviceReset has reloaded the module).
 static int est_scratch(int device, double** out) {
-  static std::mutex mu;
-  static double* addr[EST_NOALLOC_MAX_DEVICES] = {};
   if (device < 0 || device >= EST_NOALLOC_MAX_DEVICES) {
     md_set_error("device %d outside the %d devices the estimate scratch supports", device, EST_NOALLOC_MAX_DEVICES);
     return MD_ERR_BADARG;
   }
-  std::lock_guard<std::mutex> lock(mu);
-  if (!addr[device]) {
-    int prev = 0;
-    MD_CUDA(cudaGetDevice(&prev));
-    MD_CUDA(cudaSetDevice(device));
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_est_scratch);
-    cudaSetDevice(prev);
-    if (e != cudaSuccess) return md_cuda_fail(e, "cudaGetSymbolAddress(g_est_scratch)");
-    addr[device] = (double*)p;
-  }
-  *out = addr[device];
+  int prev = 0;
+  MD_CUDA(cudaGetDevice(&prev));
+  if (prev != device) MD_CUDA(cudaSetDevice(device));
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_est_scratch);
+  if (prev != device) cudaSetDevice(prev);
+  if (e != cudaSuccess) return md_cuda_fail(e, "cudaGetSymbolAddress(g_est_scratch)");
+  *out = (double*)p;
   return MD_OK;
 }
 

@@ -258,7 +258,8 @@ extern "C" int md_sim_set_stats_ring(md_sim* s, double* host, int rows) {
     double* dev = nullptr;
     MD_CUDA(cudaHostGetDevicePointer((void**)&dev, host, 0));
     MD_CUDA(cudaMalloc(&s->ring_count, sizeof(unsigned)));
-    MD_CUDA(cudaMemset(s->ring_count, 0, sizeof(unsigned)));
+    // ordered with the step graphs, which run on the system's (non-blocking) stream
+    MD_CUDA(cudaMemsetAsync(s->ring_count, 0, sizeof(unsigned), s->sys->stream));
     s->ring = dev;
     s->ring_rows = rows;
   }

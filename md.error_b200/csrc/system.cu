@@ -146,6 +146,16 @@ __global__ void k_charge_io(int N, int dir, typename V4<R>::T* p4, const int* id
   else host_order[id[k]] = (double)p4[k].w;
 }
 
+// masses live in vel.w as 1/m (MDSystem hdata.massi); m given and returned in
+// original atom order
+template <class R>
+__global__ void k_mass_io(int N, int dir, typename V4<R>::T* v4, const int* id, double* host_order) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  if (dir == 0) v4[k].w = (R)(1.0 / host_order[id[k]]);
+  else host_order[id[k]] = 1.0 / (double)v4[k].w;
+}
+
 __global__ void k_rcut_io(int N, int dir, float* rc, const int* id, float* host_order) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= N) return;
@@ -425,12 +435,15 @@ extern "C" int md_system_set_velocities(md_system* s, const double* v) { return 
 extern "C" int md_system_get_velocities(md_system* s, double* v) { return download(s, 1, v); }
 extern "C" int md_system_get_forces(md_system* s, double* f) { return download(s, 2, f); }
 
-static int charge_io(md_system* s, int dir, double* q) {
+// per-atom scalar kept in a w component: what 0 charge (pos.w), 1 mass (vel.w = 1/m)
+static int charge_io(md_system* s, int dir, double* q, int what = 0) {
   if (int r = check_sys(s)) return r;
   if (!q) return MD_ERR_BADARG;
   if (dir == 0)
-    for (int i = 0; i < s->N; ++i)
-      if (!std::isfinite(q[i])) { md_set_error("non-finite charge at atom %d", i); return MD_ERR_BADARG; }
+    for (int i = 0; i < s->N; ++i) {
+      if (!std::isfinite(q[i])) { md_set_error("non-finite %s at atom %d", what ? "mass" : "charge", i); return MD_ERR_BADARG; }
+      if (what == 1 && !(q[i] > 0)) { md_set_error("mass %g of atom %d is not positive", q[i], i); return MD_ERR_BADARG; }
+    }
   const size_t bytes = sizeof(double) * (size_t)s->N;
   if (int r = ensure_stage(s, bytes)) return r;
   MD_CUDA(cudaStreamSynchronize(s->stream));
@@ -441,11 +454,17 @@ static int charge_io(md_system* s, int dir, double* q) {
     MD_CUDA(cudaMemcpyAsync(d, s->h_stage, bytes, cudaMemcpyHostToDevice, s->stream));
   }
   const int nb = ceil_div(s->N, 256);
-  if (s->prec == MD_PREC_FP64)
+  if (what == 1) {
+    if (s->prec == MD_PREC_FP64)
+      k_mass_io<double><<<nb, 256, 0, s->stream>>>(s->N, dir, (double4a*)s->vel, s->id, d);
+    else
+      k_mass_io<float><<<nb, 256, 0, s->stream>>>(s->N, dir, (float4*)s->vel, s->id, d);
+  } else if (s->prec == MD_PREC_FP64) {
     k_charge_io<double><<<nb, 256, 0, s->stream>>>(s->N, dir, (double4a*)s->pos, s->id, d);
-  else
+  } else {
     k_charge_io<float><<<nb, 256, 0, s->stream>>>(s->N, dir, (float4*)s->pos, s->id, d);
-  MD_CHECK_LAUNCH("charge io");
+  }
+  MD_CHECK_LAUNCH("charge / mass io");
   if (dir == 1) MD_CUDA(cudaMemcpyAsync(s->h_stage, d, bytes, cudaMemcpyDeviceToHost, s->stream));
   MD_CUDA(cudaFreeAsync(d, s->stream));
   MD_CUDA(cudaStreamSynchronize(s->stream));
@@ -455,6 +474,8 @@ static int charge_io(md_system* s, int dir, double* q) {
 
 extern "C" int md_system_set_charges(md_system* s, const double* q) { return charge_io(s, 0, const_cast<double*>(q)); }
 extern "C" int md_system_get_charges(md_system* s, double* q) { return charge_io(s, 1, q); }
+extern "C" int md_system_set_masses(md_system* s, const double* m) { return charge_io(s, 0, const_cast<double*>(m), 1); }
+extern "C" int md_system_get_masses(md_system* s, double* m) { return charge_io(s, 1, m, 1); }
 
 extern "C" int md_system_get_box(md_system* s, double box[3]) {
   if (int r = check_sys(s)) return r;

@@ -115,6 +115,8 @@ _SIGS = {
     "md_spme_self_correction": (i32, [vp, vp]),
     "md_system_set_charges": (i32, [vp, P(f64)]),
     "md_system_get_charges": (i32, [vp, P(f64)]),
+    "md_system_set_masses": (i32, [vp, P(f64)]),
+    "md_system_get_masses": (i32, [vp, P(f64)]),
     "md_ewald_self_energy": (i32, [vp, f64, P(f64)]),
     "md_ewald_exact": (i32, [vp, P(i32), f64, P(f64), i32]),
     "md_error_estimate_pme": (i32, [vp, P(i32), f64, f64, P(f64), P(f64)]),

@@ -204,6 +204,16 @@ class MDSystem:
         a = _f64(q).reshape(self.n)
         check(lib.md_system_set_charges(self.h, _p(a)), "set_charges")
 
+    def set_masses(self, m):
+        """Per-atom masses in original order (MDSystem hdata.mass)."""
+        a = _f64(m).reshape(self.n)
+        check(lib.md_system_set_masses(self.h, _p(a)), "set_masses")
+
+    def masses(self):
+        out = np.empty(self.n, np.float64)
+        check(lib.md_system_get_masses(self.h, _p(out)), "masses")
+        return out
+
     def box(self):
         b = np.empty(3, np.float64)
         check(lib.md_system_get_box(self.h, _p(b)), "get_box")

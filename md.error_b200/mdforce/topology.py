@@ -133,12 +133,14 @@ class System:
 
 
 def initTopology(sys, top):
-    """MDSystem::initTopology: the system's types and charges from the topology
-    (masses are given to MDSystem at creation, e.g. mass=top.expand()['mass'])."""
+    """MDSystem::initTopology (shortRange.inhomo/template/tools.collision/cal.real.error/
+    src/MDSystem_interface.cu:116-133): the system's types, masses and charges from the
+    topology."""
     e = top.expand()
     if e["type"].shape[0] != sys.n:
         raise ValueError(f"topology has {e['type'].shape[0]} atoms, the system {sys.n}")
     sys.set_types(e["type"])
+    sys.set_masses(e["mass"])
     sys.set_charges(e["charge"])
     return e
 

@@ -2,12 +2,17 @@
 adaptive-cutoff profiles of the 16000-atom slab at T* = 0.85, target 0.0045
 (shortRange.inhomo/alltext/writeDown/fig/t0.85-n16000-adapt-e0.0045/
 a.density.x.out, a.rcut.x.out, a.error.x.out).  Run in a tree where the
-reference is mounted; the JSON it writes is committed."""
+reference is present (MDERROR_REFERENCE); the JSON it writes is committed."""
 import json
 import os
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+from oracle.refpath import reference_root  # noqa: E402
+
+REF = sys.argv[1] if len(sys.argv) > 1 else reference_root()
+if not REF:
+    sys.exit("reference tree not found: set MDERROR_REFERENCE or pass its path")
 D = os.path.join(REF, "shortRange.inhomo/alltext/writeDown/fig/t0.85-n16000-adapt-e0.0045")
 
 

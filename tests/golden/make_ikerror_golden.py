@@ -27,7 +27,11 @@ def water_like(L):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+    from oracle.refpath import reference_root
+    ref = sys.argv[1] if len(sys.argv) > 1 else reference_root()
+    if not ref:
+        sys.exit("reference tree not found: set MDERROR_REFERENCE or pass its path")
     sys.path.insert(0, os.path.join(ref, "optiBasis"))
     from Region import Region
     from Bspline import Bspline

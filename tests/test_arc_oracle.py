@@ -91,3 +91,27 @@ def test_adapt_rcut_golden_profile(orc):
     ref_err = np.interp(xb, np.array(g["error_x"]), np.array(g["error"]))
     ratio = err[ok] / ref_err[ok]
     assert np.median(ratio) > 0.5 and np.median(ratio) < 2.0
+
+
+@pytest.mark.slow
+def test_adapt_rcut_oracle_matches_reference_on_benchmark_bins(orc):
+    """The slab benchmark's own estimate: 41 x 41 x 161 bins of the committed
+    start's deposited density, target 0.02, rc 2.5..5.0 step 0.5, oracle
+    against the reference's AdaptRCut built from its sources (about a minute)."""
+    if not orc.ref_available("libref_arc.so"):
+        pytest.skip("reference AdaptRCut not built (needs the reference tree at build time)")
+    z = np.load(os.path.join(HERE, "golden", "slab65536_start.npz"))
+    box = z["box"]
+    n = orc.dp_bins(box, 1.0)
+    assert n == (41, 41, 161)
+    rho = orc.dp_deposit(z["pos"], box, n) / np.prod(box / np.array(n))
+    a = orc.adapt_rcut(box, n, np.arange(2.5, 5.01, 0.5), rho, 0.02)
+    b = orc.ref_adapt_rcut(box, n, 2.5, 5.0, 0.5, rho, 0.02)
+    # a one-sample profile leaves vapour bins empty; there the convolved error
+    # square can come out negative and both give NaN in the same bins (a NaN
+    # error never meets the target, so the bin takes rcmax in both)
+    assert np.array_equal(np.isnan(a["error"]), np.isnan(b["error"]))
+    assert np.allclose(a["error"], b["error"], rtol=1e-12, atol=0, equal_nan=True)
+    assert np.array_equal(a["index"], b["index"])
+    assert np.array_equal(a["rcut"], b["rcut"])
+    assert np.allclose(a["result_error"], b["result_error"], rtol=1e-12, atol=0, equal_nan=True)

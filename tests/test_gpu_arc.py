@@ -80,3 +80,25 @@ def test_sim_with_adaptive_cutoff(mdf):
     p = sys.stats()
     assert p[mdf.STAT_PRESSURE_CORR_XX] != 0.0
     assert sim.uses_conditional_graph()
+
+
+def test_pressure_correction_carries_previous_value(mdf, orc, small):
+    """PressureCorrection::correction (ENG/src/PressureCorrection.cu:175-211) adds
+    each new sum to pxx, pyy, pzz without resetting them and then divides by V,
+    so a second update gives p1 / V + (the second profile's own correction)."""
+    sys, box = small
+    arc = mdf.AdaptRCutEstimator(sys, refh=4.0, rcmin=2.5, rcmax=5.0, rcstep=0.5)
+    n = arc.n
+    rho1, rho2 = slab_profile(n, seed=0), slab_profile(n, seed=1)
+    arc.set_profile(rho1)
+    arc.update(4e-3)
+    p1 = arc.pressure_correction()
+    arc.set_profile(rho2)
+    arc.update(4e-3)
+    p2 = arc.pressure_correction()
+    o1 = orc.adapt_rcut(box, n, arc.rc_list, rho1, 4e-3)["pcorr"]
+    o2 = orc.adapt_rcut(box, n, arc.rc_list, rho2, 4e-3)["pcorr"]
+    V = float(np.prod(box))
+    assert np.allclose(p1, o1, rtol=1e-6)
+    assert np.allclose(p2, o1 / V + o2, rtol=1e-6)
+    assert not np.allclose(p2, o2, rtol=1e-12, atol=0)  # the carried share is there

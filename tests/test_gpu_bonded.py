@@ -235,3 +235,24 @@ def test_topology_path_equals_direct_lists(mdf, poly):
     eb.clearInteraction()
     eb.applyBondedInteraction(b)
     assert np.array_equal(a.forces(), b.forces())
+
+
+def test_init_topology_sets_masses(mdf, poly):
+    """initTopology copies each atom's mass, charge and type from the topology,
+    as MDSystem::initTopology does; masses reach the integrator as 1/m."""
+    s = poly
+    t = mdf.topology
+    mol = t.Molecule("pair")
+    mol.pushAtom(t.Atom("A", 0, 2.0, 0.5))
+    mol.pushAtom(t.Atom("B", 1, 0.5, -0.5))
+    top = t.System()
+    top.addMolecules(mol, s["n"] // 2)
+    for prec in (0, 1):
+        a = mdf.MDSystem(s["pos"][: 2 * (s["n"] // 2)], s["box"], precision=prec)
+        t.initTopology(a, top)
+        want = np.tile([2.0, 0.5], s["n"] // 2)
+        assert np.allclose(a.masses(), want, rtol=1e-7)
+        assert np.array_equal(a.types(), np.tile([0, 1], s["n"] // 2))
+        assert np.allclose(a.charges(), np.tile([0.5, -0.5], s["n"] // 2))
+        with pytest.raises(mdf.MDExcptBadArgument):
+            a.set_masses(np.zeros(a.n))

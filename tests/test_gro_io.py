@@ -6,9 +6,13 @@ import os
 import numpy as np
 import pytest
 
+from oracle.refpath import reference_root
+
+_REF = reference_root()
+# the reference's own start configurations (read only when the tree is present)
 REF_CONFS = [
-    "/root/reference/shortRange.inhomo/template/confs/N00010000-T0.7-100x020x020.gro",
-    "/root/reference/shortRange.inhomo/template/confs/conf.16000.gro",
+    os.path.join(_REF or "", "shortRange.inhomo/template/confs/N00010000-T0.7-100x020x020.gro"),
+    os.path.join(_REF or "", "shortRange.inhomo/template/confs/conf.16000.gro"),
 ]
 
 
