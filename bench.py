@@ -3,11 +3,14 @@
 
 Workload (one step = one Langevin NPT MD step of the whole slab through the
 graph-captured driver): 40 x 40 x 160 sigma box, liquid rho* 0.78 for
-|z - 80| < 24.84, vapour 0.02, adaptive per-slab LJ cutoff in [2.5, 5.0],
-skin 0.3, Langevin NPT with P_zz = 0 (x, y fixed), dt 0.005, T* 0.85.
+|z - 80| < 24.84, vapour 0.02, adaptive per-bin LJ cutoff in [2.5, 5.0]
+(AdaptRCut at target 0.02, re-estimated every 2000 steps), skin 0.6,
+Langevin NPT with P_zz = 0 (x, y fixed), dt 0.005, T* 0.85, from the
+committed start tests/golden/slab65536_start.npz.
 `value` is the mixed-precision path (FP32 pair math, FP64 accumulation);
-the plain FP64 path runs the same steps and is reported beside it together
-with the force RMS error of mixed against FP64 on the same configuration.
+the plain FP64 path runs the same steps and is reported beside it, with the
+force RMS error of mixed against FP64 and of both against long-cutoff FP64
+forces, beside the AdaptRCut a-priori estimate.
 
 python bench.py --gpus N --steps K --warmup W [--impl reference]
 """
@@ -18,6 +21,7 @@ import subprocess
 import sys
 import threading
 import time
+from types import SimpleNamespace
 
 import numpy as np
 
@@ -45,7 +49,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--equil", type=int, default=4000,
-                    help="untimed NVT relaxation steps of the random start")
+                    help="untimed relaxation steps of the other workloads' starts (the slab's start is "
+                         "committed)")
     ap.add_argument("--workload", default="lj_slab", choices=list(WORKLOADS),
                     help="lj_slab: the 65536-atom slab of the headline metric (default); the others "
                          "time the remaining named systems")
@@ -151,60 +156,56 @@ def profiled_traffic(kernel):
     return None
 
 
-def build_slab(mdf):
-    s = mdf.systems.lj_slab()
-    return s
+START = os.path.join(ROOT, "tests", "golden", "slab65536_start.npz")
+
+
+def load_slab_start():
+    """The committed start of the 65,536-atom slab (tests/golden/make_slab_start.py):
+    random sequential addition + 4000 Langevin NVT steps, and the adaptive cutoff
+    lattice of the reference's AdaptRCut at target 0.02.  Plain numpy: both arms
+    read it, neither generates or relaxes it."""
+    z = np.load(START)
+    return SimpleNamespace(name="lj_slab", pos=z["pos"].astype(np.float64), vel=z["vel"].astype(np.float64),
+                           box=np.asarray(z["box"], np.float64), lattice=np.asarray(z["lattice"], np.float32),
+                           n=int(z["pos"].shape[0]), relax=int(z["relax_steps"]))
 
 
 RC_MIN, RC_MAX, RC_STEP = 2.5, 5.0, 0.5
 TARGET_PREC = 0.02      # targetPrec of ENG/app/lj.nhc-xtc.cu:57
 SAMPLE_EVERY, UPDATE_EVERY = 40, 2000  # densityProfileSamplingFeq, rcutUpdateFeq (:49-51)
+GAMMA_T, TAU_P, KAPPA_T = 1.0, 2.0, 0.1
+RC_LONG = 10.0          # cutoff of the long-range FP64 reference forces (+ LFC)
 
 
-def make_sim(mdf, s, prec, lattice, seed=1, npt=True, gamma=1.0, adaptive=True, use_graph=True):
+def slab_config(s, world):
+    """The workload as both arms state it (identical dicts)."""
+    counts = {float(v): int((s.lattice == v).sum()) for v in np.unique(s.lattice)}
+    return {"workload": "lj_slab_65536_npt", "n_atoms": s.n, "box": s.box.tolist(),
+            "rc": f"adaptive per-bin lattice {tuple(s.lattice.shape)} from the reference AdaptRCut at target "
+                  f"{TARGET_PREC}, rc {RC_MIN}..{RC_MAX} step {RC_STEP}, bins per rc {counts}; re-estimated every "
+                  f"{UPDATE_EVERY} steps from samples every {SAMPLE_EVERY}",
+            "skin": SKIN, "dt": DT, "T": TEMP,
+            "ensemble": f"Langevin NPT Pzz=0 (gamma {GAMMA_T}, tau_P {TAU_P}, kappa_T {KAPPA_T})",
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": "GPU arm: flushed (256 MB write) between timed steps; CPU arm: no flush",
+            "start": f"tests/golden/slab65536_start.npz: random sequential addition (0.8 sigma) + {s.relax} "
+                     f"Langevin NVT steps on the CPU oracle"}
+
+
+def make_sim(mdf, s, prec, lattice, seed=1, use_graph=True, attach_arc=True):
     sys_ = mdf.MDSystem(s.pos, s.box, vel=s.vel, precision=prec)
-    if lattice is None:
-        sys_.set_rcut(np.full(s.n, RC_MIN, np.float32))
-    else:
-        mdf.AssignRCut(lattice).assign(sys_)
+    mdf.AssignRCut(lattice).assign(sys_)
     eng = mdf.InteractionEngine(sys_)
     eng.registNonBondedInteraction(1.0, 1.0, 0.0)
-    lv = mdf.langevin_params(dt=DT, temperature=TEMP, gamma_t=gamma, tau_p=2.0 if npt else 0.0,
-                             kappa_t=0.1 if npt else 0.0, p_ref=(0.0, 0.0, 0.0),
-                             npt_dirs=4 if npt else 0, seed=seed)
+    lv = mdf.langevin_params(dt=DT, temperature=TEMP, gamma_t=GAMMA_T, tau_p=TAU_P, kappa_t=KAPPA_T,
+                             p_ref=(0.0, 0.0, 0.0), npt_dirs=4, seed=seed)
     sim = mdf.Simulation(sys_, eng, skin=SKIN, cell_size=2.8, lv=lv, expansion=1.5, use_graph=use_graph,
                          max_rcut=RC_MAX)
-    if adaptive:
+    arc = None
+    if attach_arc:
         arc = mdf.AdaptRCutEstimator(sys_, refh=1.0, rcmin=RC_MIN, rcmax=RC_MAX, rcstep=RC_STEP)
         sim.attach_adapt_rcut(arc, sample_every=SAMPLE_EVERY, update_every=UPDATE_EVERY, prec=TARGET_PREC)
-    return sys_, eng, sim
-
-
-def equilibrate(mdf, s, nsteps):
-    """Relax the random-sequential-addition start (0.8 sigma contacts) by
-    Langevin NVT at T*, sampling the density profile every 40 steps; at the end
-    the adaptive-cutoff estimate (AdaptRCut, target 0.02, rc 2.5..5.0) of the
-    sampled profile gives the per-bin cutoff lattice.  Not timed."""
-    sys_, eng, sim = make_sim(mdf, s, 0, None, seed=12345, npt=False, gamma=2.0, adaptive=False)
-    arc = mdf.AdaptRCutEstimator(sys_, refh=1.0, rcmin=RC_MIN, rcmax=RC_MAX, rcstep=RC_STEP)
-    done = 0
-    while done < max(nsteps, SAMPLE_EVERY):
-        sim.run(SAMPLE_EVERY)
-        done += SAMPLE_EVERY
-        if done > nsteps // 2:
-            arc.deposite()
-    arc.update(TARGET_PREC)
-    rc, idx, err = arc.rcut()
-    lattice = rc.astype(np.float32)
-    sys_.synchronize()
-    out = mdf.systems.SyntheticSystem(s.name, sys_.positions(), sys_.box(), sys_.velocities(),
-                                      s.charge, dict(s.meta, equilibrated_steps=done))
-    counts = {float(v): int((rc == v).sum()) for v in np.unique(rc)}
-    info = (f"adaptive per-bin lattice {arc.n} from AdaptRCut at target {TARGET_PREC}, "
-            f"rc {RC_MIN}..{RC_MAX} step {RC_STEP}; bins per rc {counts}; "
-            f"re-estimated every {UPDATE_EVERY} steps from samples every {SAMPLE_EVERY}")
-    del sim, eng, sys_, arc
-    return out, lattice, info
+    return sys_, eng, sim, arc
 
 
 def time_steps(torch, sim, stream, steps, flush, nvtx_range=None):
@@ -227,14 +228,20 @@ def time_steps(torch, sim, stream, steps, flush, nvtx_range=None):
     return sum(a.elapsed_time(b) for a, b in ev) / 1e3
 
 
-def time_lj_kernel(torch, mdf, sys_, eng, sim, stream, reps=50):
-    """Average duration of the dominant kernel (LJ forces) on the bench state."""
-    # the simulation owns its list; time the kernel on a list built the same way
-    cl = mdf.CellList(sys_, 2.8)
+def fitted_list(mdf, sys_, skin=SKIN, cell=2.8):
+    cl = mdf.CellList(sys_, cell)
     cl.rebuild()
     rc = sys_.rcut()
-    nl = mdf.NeighborList(sys_, float(rc.max()) + SKIN, SKIN, expansion=1.5)
+    nl = mdf.NeighborList(sys_, float(rc.max()) + skin, skin, expansion=1.5)
     nl.fit(sys_, cl)
+    return cl, nl
+
+
+def time_kernels(torch, mdf, sys_, eng, stream, reps=50):
+    """Average CUDA-event duration of the LJ force kernel on the bench state (a
+    list built the way the driver builds it), of one list build, and the list's
+    entry count P."""
+    cl, nl = fitted_list(mdf, sys_)
     counts, _ = nl.lists()
     P = int(counts.sum())
     torch.cuda.synchronize()
@@ -261,41 +268,109 @@ def time_lj_kernel(torch, mdf, sys_, eng, sim, stream, reps=50):
     return t_lj, P, t_nl
 
 
-def force_error(mdf, s, lattice):
-    """RMS force error of mixed against FP64 on the same configuration."""
-    out = {}
-    for prec in (0, 1):
-        sys_ = mdf.MDSystem(s.pos, s.box, precision=prec)
-        if lattice is None:
-            sys_.set_rcut(np.full(s.n, 2.5, np.float32))
-        else:
-            mdf.AssignRCut(lattice).assign(sys_)
-        cl = mdf.CellList(sys_, 2.8)
-        cl.rebuild()
-        nl = mdf.NeighborList(sys_, float(sys_.rcut().max()) + SKIN, SKIN, expansion=1.5)
-        nl.fit(sys_, cl)
-        eng = mdf.InteractionEngine(sys_)
-        eng.registNonBondedInteraction(1.0, 1.0, 0.0)
-        eng.clearInteraction()
-        eng.applyNonBondedInteraction(sys_, nl, with_stats=True)
-        out[prec] = sys_.forces()
-    d = out[0] - out[1]
-    rms_abs = float(np.sqrt((d ** 2).sum(1).mean()))
-    rms_rel = float(np.sqrt((d ** 2).sum() / (out[1] ** 2).sum()))
-    return rms_abs, rms_rel
+def start_forces(mdf, s, prec):
+    """Forces of the adaptive-cutoff LJ on the start configuration."""
+    sys_ = mdf.MDSystem(s.pos, s.box, precision=prec)
+    mdf.AssignRCut(s.lattice).assign(sys_)
+    _, nl = fitted_list(mdf, sys_)
+    eng = mdf.InteractionEngine(sys_)
+    eng.registNonBondedInteraction(1.0, 1.0, 0.0)
+    eng.clearInteraction()
+    eng.applyNonBondedInteraction(sys_, nl, with_stats=True)
+    return sys_, sys_.forces()
 
 
-def cpu_baseline(s, lattice, nsteps):
+def long_cutoff_forces(mdf, s):
+    """FP64 forces at a uniform cutoff of 10 sigma plus the long-range force
+    correction (ForceCorr on 1-sigma bins of this configuration's density, averaged
+    over x and y): the
+    near-exact LJ forces the adaptive cutoff approximates.  The FP64 kernel that
+    computes them is the one the tests pin to the all-pairs oracle."""
+    sys_ = mdf.MDSystem(s.pos, s.box, precision=1)
+    sys_.set_rcut(np.full(s.n, RC_LONG, np.float32))
+    fc = mdf.ForceCorr(sys_, RC_LONG, refh=1.0)
+    fc.deposite()
+    fc.update()         # DensityProfile::calculate of the one sample
+    rho = fc.profile()  # averaged over the slab's homogeneous x and y
+    fc.set_profile(np.broadcast_to(rho.mean(axis=(0, 1), keepdims=True), rho.shape))
+    fc.update()
+    fc.assign()
+    _, nl = fitted_list(mdf, sys_, skin=0.0, cell=5.0)
+    eng = mdf.InteractionEngine(sys_)
+    eng.registNonBondedInteraction(1.0, 1.0, 0.0)
+    eng.setForceCorrection(fc)
+    eng.clearInteraction()
+    eng.applyNonBondedInteraction(sys_, nl, with_stats=True)
+    return sys_.forces()
+
+
+def apriori_error(mdf, sys_, s):
+    """RMS over atoms of the AdaptRCut error estimate (ENG/src/AdaptRCut.cu calError)
+    of each atom's bin at the cutoff the lattice gives it, for this configuration's
+    density: one deposit, averaged over x and y (the slab is homogeneous there;
+    a single sample leaves most vapour bins empty)."""
+    arc = mdf.AdaptRCutEstimator(sys_, refh=1.0, rcmin=RC_MIN, rcmax=RC_MAX, rcstep=RC_STEP)
+    arc.clearData()
+    arc.deposite()
+    arc.update(TARGET_PREC)  # DensityProfile::calculate of the one sample
+    rho = arc.profile()
+    arc.set_profile(np.broadcast_to(rho.mean(axis=(0, 1), keepdims=True), rho.shape))
+    arc.update(TARGET_PREC)
+    err = arc.error()  # (nrc, nx, ny, nz)
+    idx = np.rint((s.lattice - RC_MIN) / RC_STEP).astype(np.int64)
+    per_bin = np.take_along_axis(err, idx[None], 0)[0]
+    n = np.array(arc.n)
+    b = np.clip(np.floor(s.pos / s.box * n).astype(np.int64), 0, n - 1)
+    e_atom = per_bin[b[:, 0], b[:, 1], b[:, 2]]
+    return float(np.sqrt((e_atom ** 2).mean())), float(per_bin.max())
+
+
+def cpu_port(s, nsteps):
+    """The oracle's CPU FP64 Langevin NPT MD (cell + Verlet list, OpenMP) on the
+    start, at the GPU arm's skin and lattice."""
     from oracle import oracle as orc
-    rc = None if lattice is not None else np.full(s.n, 2.5, np.float32)
-    kw = dict(dt=DT, temperature=TEMP, gamma_t=1.0, skin=SKIN_SPEC, rcut=rc, lattice=lattice, tau_p=2.0,
-              kappa_t=0.1, p_ref=(0, 0, 0), npt_dirs=4, seed=1, cap=1024)
+    kw = dict(dt=DT, temperature=TEMP, gamma_t=GAMMA_T, skin=SKIN, lattice=s.lattice, tau_p=TAU_P,
+              kappa_t=KAPPA_T, p_ref=(0, 0, 0), npt_dirs=4, seed=1, cap=1024)
     orc.md_langevin_run(s.pos, s.vel, s.box, 1, **kw)  # warm (page in, list build)
     t = time.perf_counter()
     out = orc.md_langevin_run(s.pos, s.vel, s.box, nsteps, **kw)
     el = time.perf_counter() - t
-    # the run includes one initial list build + force evaluation; count it as a step
-    return (nsteps / el), orc.num_threads(), out
+    if out["status"] != 0:
+        raise RuntimeError(f"CPU port failed: status {out['status']}")
+    return nsteps / el, orc.num_threads()
+
+
+def reference_loop(pairs_per_step):
+    """The reference's own CPU LJ loop (force.kernel/test.kernels/app/explicit.cpp,
+    built as shipped into oracle/_ref/ref_explicit_lj): its fixed sample of
+    10,000 atoms x 39,999 list entries (4.0e8 pair forces with Newton's third
+    law), one copy per host core at once.  Returns the aggregate pair rate and
+    the slab steps/s it projects for the force loop alone (pairs_per_step =
+    half the list entries of one slab step)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_explicit_lj")
+    if not os.access(exe, os.X_OK):
+        return None
+    cores = os.cpu_count() or 1
+    t = time.perf_counter()
+    procs = [subprocess.Popen([exe], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+             for _ in range(cores)]
+    reals = []
+    for p in procs:
+        out, _ = p.communicate(timeout=600)
+        for ln in out.splitlines():
+            if ln.startswith("system:"):
+                reals.append(float(ln.split("real:")[1]))
+    wall = time.perf_counter() - t
+    if len(reals) != cores:
+        return None
+    pairs = 10000 * 39999
+    rate = pairs * cores / max(reals)
+    return {"pairs_per_s": rate, "pairs_per_s_per_core": pairs / float(np.median(reals)), "cores": cores,
+            "wall_s": wall, "slab_pairs_per_step": pairs_per_step,
+            "projected_force_loop_steps_per_s": rate / pairs_per_step,
+            "sample": "force.kernel/test.kernels/app/explicit.cpp as shipped (g++ -O3 -msse -msse2): FP32 LJ "
+                      "over its own random list of 10,000 x 39,999 entries, Newton's third law, no cutoff "
+                      "test or periodic images; one copy per core"}
 
 
 WORKLOADS = ("lj_slab", "lj_fluid", "charged_fluid", "charged_slab", "lj_slab_lfc")
@@ -332,7 +407,7 @@ def run_workload(args):
         rc, dt, T, gamma, coul = 2.5, 0.005, 1.0, 0.1, None
         shift = -4.0 * (rc ** -12 - rc ** -6)
     elif lfc:
-        s = build_slab(mdf)
+        s = mdf.systems.lj_slab()
         rc, dt, T, gamma, shift, coul = 3.5, DT, TEMP, 1.0, 0.0, None
     elif w == "charged_fluid":
         s = mdf.systems.charged_fluid()
@@ -418,6 +493,22 @@ def run_workload(args):
         rc_info = rc
     pos, vel = sys0.positions(), sys0.velocities()
     del sim0, sys0
+    chosen = None
+    if w == "charged_slab":
+        # beta and the mesh from the error estimates of the relaxed charge profile
+        # (md_choose_spme_params) at a total target of 1e-4: the configuration's
+        # 128 x 128 x 512 mesh cannot meet it with the beta the real space needs
+        sysc = mdf.MDSystem(pos, s.box, charge=s.charge, precision=1)
+        config_mesh = coul["K"]
+        beta, K, e_dir, e_rec = mdf.choose_spme_params(sysc, rc, coul["order"], 1e-4, kmax=1024)
+        e_cfg = mdf.ErrorEstimate_SPME_Ik(config_mesh, s.box, beta, coul["order"])
+        e_cfg.deposit(sysc)
+        cfg_max = float(np.nanmax(e_cfg.rms(1.0)))
+        del e_cfg, sysc
+        coul["beta"], coul["K"] = beta, K
+        chosen = {"target": 1e-4, "beta": beta, "mesh": list(K), "real_space_max_bin": e_dir,
+                  "spme_ik_max_bin": e_rec, "total_max_bin": float(np.hypot(e_dir, e_rec)),
+                  "config_mesh": list(config_mesh), "config_mesh_spme_ik_max_bin": cfg_max}
     out = {}
     for prec in (0, 1):
         sys_, eng, sim = build(prec, pos, vel)
@@ -438,6 +529,9 @@ def run_workload(args):
     d = F[0] - F[1]
     err_abs = float(np.sqrt((d ** 2).sum(1).mean()))
     err_rel = float(np.sqrt((d ** 2).sum() / (F[1] ** 2).sum()))
+    sampled = None
+    if chosen is not None:
+        sampled = sampled_electrostatics_error(mdf, s, pos, lattice[0], arc_kw, coul)
     if rank == 0:
         line = {"metric": "MD steps/s", "value": out[0][0], "unit": "steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / out[0][0],
@@ -453,32 +547,91 @@ def run_workload(args):
                 "tau_per_day": out[0][0] * dt * 86400}
         if apriori is not None:
             line["apriori_force_rms_error"] = apriori
+        if chosen is not None:
+            line["electrostatics_choice"] = chosen
+            line["force_rms_err_vs_converged"] = sampled
         print(json.dumps(line), flush=True)
     return 0
 
 
+def sampled_electrostatics_error(mdf, s, pos, lattice, arc_kw, coul, nsample=4096, seed=3):
+    """Electrostatic forces of the run's parameters (real-space Ewald at the
+    per-atom adaptive cutoffs >= 3.0, ik SPME at the chosen beta, mesh, order 6)
+    in both precisions against a converged FP64 Ewald sum, on nsample atoms
+    drawn without replacement: real space at a uniform 7.0 (erfc(7 beta) below
+    1e-20) and SPME on twice the mesh per axis (at most 1024) with B-spline
+    order 12 (its homogeneous a-priori estimate is reported).  Only the
+    electrostatics enter (LJ switched off)."""
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(s.n, size=min(nsample, s.n), replace=False))
+    beta = coul["beta"]
+
+    def forces(prec, rc_uniform, K, order):
+        sys_ = mdf.MDSystem(pos, s.box, charge=s.charge, precision=prec)
+        if rc_uniform is None:
+            mdf.AssignRCut(lattice).assign(sys_)
+        else:
+            sys_.set_rcut(np.full(s.n, rc_uniform, np.float32))
+        rmax = float(sys_.rcut().max())
+        eng = mdf.InteractionEngine(sys_)
+        eng.registNonBondedInteraction(0.0, 1.0, 0.0)
+        mdf.registCoulomb(eng, beta)
+        cl = mdf.CellList(sys_, max(3.3, rmax / 2))
+        cl.rebuild()
+        nl = mdf.NeighborList(sys_, rmax + 0.3, 0.3, expansion=1.3)
+        nl.fit(sys_, cl)
+        eng.clearInteraction()
+        eng.applyNonBondedInteraction(sys_, nl)
+        mdf.SPME(sys_, K, order, beta, "ik").apply()
+        est = mdf.errorEstimateInterpolRec(sys_, K, order, beta) if prec == 1 else None
+        return sys_.forces()[idx], est
+
+    fine = tuple(min(1024, 2 * k) for k in coul["K"])
+    Fref, est_ref = forces(1, 7.0, fine, 12)
+    out = {"sample": f"{len(idx)} atoms", "reference": {"real_space_rc": 7.0, "mesh": list(fine), "order": 12,
+                                                          "spme_ik_apriori": est_ref}}
+    for prec, name in ((0, "mixed"), (1, "fp64")):
+        F, _ = forces(prec, None, coul["K"], coul["order"])
+        d = F - Fref
+        out[name] = float(np.sqrt((d ** 2).sum(1).mean()))
+    return out
+
+
 def run_reference(args):
+    """The reference arm: the same workload, config, metric and unit on the host
+    cores, without the GPU engine (libmdforce is never loaded).  The reference's
+    MD engine is CUDA that does not build with nvcc 12.9, so the full step is
+    timed on the oracle's CPU port (FP64 Langevin NPT with cell and Verlet lists,
+    OpenMP on all host threads) from the committed start, at the GPU arm's skin
+    and cutoff lattice; beside it, the reference's own CPU LJ loop
+    (explicit.cpp, built as shipped)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    import mdforce as mdf
-    # the same seeded start, relaxation and cutoff lattice as the GPU arm; the
-    # preparation is not timed (it runs on the device when one is present)
-    s, lattice, rcinfo = equilibrate(mdf, build_slab(mdf), args.equil)
-    from oracle import oracle as orc
-    # bounded sample: estimate one step, cap the whole run at ~150 s
-    sps0, cores, _ = cpu_baseline(s, lattice, 3)
-    budget_steps = max(3, min(args.steps, int(150 * sps0)))
-    sps, cores, out = cpu_baseline(s, lattice, budget_steps)
+    s = load_slab_start()
+    # bounded sample: the warm-up steps untimed, then --steps steps (at most ~60 s)
+    sps0, cores = cpu_port(s, max(2, min(args.warmup, 5)))
+    nsteps = max(2, min(args.steps, int(60 * sps0)))
+    sps, cores = cpu_port(s, nsteps)
+    half_pairs = None
+    try:
+        from oracle import oracle as orc
+        # list entries of the slab's start at rc_i + skin (the force loop's workload)
+        rc = orc.assign_rcut_f32(s.pos, s.box, s.lattice)
+        cnt, _ = orc.nlist_allpair_f32(s.pos.astype(np.float32), rc, SKIN, s.box.astype(np.float32))
+        half_pairs = int(cnt.sum()) // 2
+    except Exception:  # the projection is optional context
+        half_pairs = None
+    loop = reference_loop(half_pairs) if half_pairs else None
     line = {
         "impl": "reference", "metric": METRIC, "value": sps, "unit": "steps/s", "n_gpus": args.gpus,
-        "steps": budget_steps, "warmup": args.warmup, "ms_per_step": 1e3 / sps, "higher_is_better": True,
+        "steps": nsteps, "warmup": args.warmup, "ms_per_step": 1e3 / sps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "lj_slab_65536_npt", "n_atoms": s.n, "box": s.box.tolist(),
-                   "rc": rcinfo, "skin": SKIN_SPEC, "dt": DT, "parallelism": "replicas"},
+        "config": slab_config(s, world),
         "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": cores, "kind": "port",
-                         "sample": f"{budget_steps} Langevin NPT steps of the full 65536-atom slab "
-                                   f"(oracle CPU FP64 cell+Verlet list LJ, OpenMP, skin {SKIN_SPEC})"},
+                         "sample": f"{nsteps} Langevin NPT steps of the full 65536-atom slab from the committed "
+                                   f"start (oracle CPU FP64 cell + Verlet list LJ, OpenMP, skin {SKIN})"},
+        "reference_loop": loop,
         "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -501,133 +654,192 @@ def main():
     torch.cuda.set_device(local)
     import mdforce as mdf
 
-    s, lattice, rcinfo = equilibrate(mdf, build_slab(mdf), args.equil)
+    s = load_slab_start()
+    lattice = s.lattice
+    N = s.n
     stream = torch.cuda.Stream()
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
     # ---- mixed precision path (the headline value)
     use_graph = args.launch == "graph"
-    sys_m, eng_m, sim_m = make_sim(mdf, s, 0, lattice, seed=1 + rank, use_graph=use_graph)
+    sys_m, eng_m, sim_m, arc_m = make_sim(mdf, s, 0, lattice, seed=1 + rank, use_graph=use_graph)
     sys_m.set_stream(stream.cuda_stream)
     sim_m.run(args.warmup)
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    _, rebuilds0, _ = sim_m.counters()
+    steps0, rebuilds0, _ = sim_m.counters()
     with Clocks(local) as clk:
         t_mixed = time_steps(torch, sim_m, stream, args.steps, flush, nvtx_range="timed")
     steps_done, rebuilds, flags = sim_m.counters()
     rebuilds_timed = rebuilds - rebuilds0
     value, t_max = replica_rate(torch, args.steps, t_mixed, world, "cuda")
 
-    # back-to-back (warm L2) throughput of the same loop, for reference
+    # ---- the reference's whole schedule (lj.nhc-xtc.cu:226-254): one 2000-step
+    # period with 50 density deposits and one AdaptRCut update + assign + tail
+    # pressure correction (host-scheduled between graph launches), warm L2
     torch.cuda.synchronize()
+    period = UPDATE_EVERY - (steps_done % UPDATE_EVERY)  # up to and including the next update
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
     with torch.cuda.stream(stream):
         a.record(stream)
-        sim_m.run(args.steps)
+        sim_m.run(period)
         b.record(stream)
     torch.cuda.synchronize()
-    warm_sps = args.steps / (a.elapsed_time(b) / 1e3)
+    t_period = time.perf_counter() - t0
+    period_dev = a.elapsed_time(b) / 1e3
+    # the density deposit alone, then one update cycle (estimate + assign +
+    # pressure correction) on the run's state (the period's update cleared the
+    # samples, so the deposits come first)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(10):
+        arc_m.deposite()
+    sys_m.synchronize()
+    deposit_s = (time.perf_counter() - t0) / 10
+    t0 = time.perf_counter()
+    arc_m.update(TARGET_PREC)
+    arc_m.assign()
+    arc_m.pressure_correction()
+    sys_m.synchronize()
+    arc_update_s = time.perf_counter() - t0
 
     # ---- FP64 path, same steps
     fp64_sps = None
+    t_lj64 = None
     if not args.no_fp64:
-        sys_d, eng_d, sim_d = make_sim(mdf, s, 1, lattice, seed=1 + rank, use_graph=use_graph)
+        sys_d, eng_d, sim_d, _ = make_sim(mdf, s, 1, lattice, seed=1 + rank, use_graph=use_graph)
         sys_d.set_stream(stream.cuda_stream)
         sim_d.run(args.warmup)
         t64 = time_steps(torch, sim_d, stream, args.steps, flush)
         fp64_sps = args.steps / t64
+        t_lj64, _, t_nl64 = time_kernels(torch, mdf, sys_d, eng_d, stream)
         del sim_d, eng_d, sys_d
 
     # ---- dominant kernel: LJ forces, algorithmic bytes / CUDA-event duration
-    t_lj, P, t_nl = time_lj_kernel(torch, mdf, sys_m, eng_m, sim_m, stream)
-    N = s.n
+    t_lj, P, t_nl = time_kernels(torch, mdf, sys_m, eng_m, stream)
     alg_bytes = N * 16 + N * 4 + P * 4 + N * 24  # positions, rcut, list indices, FP64 forces
     peak, peak_kind = measured_peak_hbm()
     achieved = alg_bytes / t_lj / 1e9
-    rms_abs, rms_rel = force_error(mdf, s, lattice)
 
-    # ---- end to end through the C ABI with host buffers
-    e2e_steps = args.steps
+    # ---- accuracy on the start configuration
+    sm, Fm = start_forces(mdf, s, 0)
+    _, Fd = start_forces(mdf, s, 1)
+    d = Fm - Fd
+    rms_abs = float(np.sqrt((d ** 2).sum(1).mean()))
+    rms_rel = float(np.sqrt((d ** 2).sum() / (Fd ** 2).sum()))
+    Fl = long_cutoff_forces(mdf, s)
+    d = Fm - Fl
+    err_long = float(np.sqrt((d ** 2).sum(1).mean()))
+    d = Fd - Fl
+    err_long64 = float(np.sqrt((d ** 2).sum(1).mean()))
+    est_rms, est_max = apriori_error(mdf, sm, s)
+    del sm
+
+    # ---- end to end through the C ABI with host buffers: one full AdaptRCut
+    # period from pinned host arrays, every step's statistics written by the
+    # device into its own pinned host row, positions and forces read back
+    e2e_steps = max(args.steps, UPDATE_EVERY)
     pin_pos = torch.from_numpy(np.ascontiguousarray(s.pos)).pin_memory()
     pin_vel = torch.from_numpy(np.ascontiguousarray(s.vel)).pin_memory()
+    stat_rows = torch.zeros((e2e_steps, mdf.STAT_COUNT), dtype=torch.float64).pin_memory().numpy()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    sys_e, eng_e, sim_e = None, None, None
     sys_e = mdf.MDSystem(pin_pos.numpy(), s.box, vel=pin_vel.numpy(), precision=0)
-    if lattice is None:
-        sys_e.set_rcut(np.full(N, 2.5, np.float32))
-    else:
-        mdf.AssignRCut(lattice).assign(sys_e)
+    mdf.AssignRCut(lattice).assign(sys_e)
     eng_e = mdf.InteractionEngine(sys_e)
     eng_e.registNonBondedInteraction(1.0, 1.0, 0.0)
-    lv = mdf.langevin_params(dt=DT, temperature=TEMP, gamma_t=1.0, tau_p=2.0, kappa_t=0.1,
+    lv = mdf.langevin_params(dt=DT, temperature=TEMP, gamma_t=GAMMA_T, tau_p=TAU_P, kappa_t=KAPPA_T,
                              p_ref=(0.0, 0.0, 0.0), npt_dirs=4, seed=1)
-    sim_e = mdf.Simulation(sys_e, eng_e, skin=SKIN, cell_size=2.8, lv=lv, expansion=1.5)
-    t_setup = time.perf_counter() - t0
-    # one page-locked row per step: the device writes each step's energy /
-    # virial / kinetic tensor there as the step ends; read once the run drains
-    stat_rows = torch.zeros((e2e_steps, mdf.STAT_COUNT), dtype=torch.float64).pin_memory().numpy()
+    sim_e = mdf.Simulation(sys_e, eng_e, skin=SKIN, cell_size=2.8, lv=lv, expansion=1.5, max_rcut=RC_MAX)
+    arc_e = mdf.AdaptRCutEstimator(sys_e, refh=1.0, rcmin=RC_MIN, rcmax=RC_MAX, rcstep=RC_STEP)
+    sim_e.attach_adapt_rcut(arc_e, sample_every=SAMPLE_EVERY, update_every=UPDATE_EVERY, prec=TARGET_PREC)
     sim_e.set_stats_ring(stat_rows)
+    t_setup = time.perf_counter() - t0
     t1 = time.perf_counter()
     sim_e.run(e2e_steps)
     sys_e.synchronize()
     fin_pos = sys_e.positions()
     fin_f = sys_e.forces()
-    t_e2e = time.perf_counter() - t1 + t_setup
-    e2e_sps = e2e_steps / t_e2e
+    t_run = time.perf_counter() - t1
+    e2e_sps = e2e_steps / (t_setup + t_run)
     h2d = (pin_pos.numel() + pin_vel.numel()) * 8 / e2e_steps
     d2h = mdf.STAT_COUNT * 8 + (fin_pos.size + fin_f.size) * 8 / e2e_steps
-    if not np.isfinite(stat_rows).all() or not np.array_equal(stat_rows[-1], sys_e.stats()):
+    # the last row is the last step's statistics; the AdaptRCut update after that
+    # step has since replaced the tail pressure correction slots
+    keep = [k for k in range(mdf.STAT_COUNT)
+            if k not in (mdf.STAT_PRESSURE_CORR_XX, mdf.STAT_PRESSURE_CORR_XX + 1, mdf.STAT_PRESSURE_CORR_XX + 2)]
+    if not np.isfinite(stat_rows).all() or not np.array_equal(stat_rows[-1][keep], sys_e.stats()[keep]):
         raise RuntimeError("per-step statistics of the end-to-end run are missing or non-finite")
+    del sim_e, arc_e, eng_e, sys_e
 
     # step1, LJ, step2 every step; bin, scan, scatter, order, gather, copy back,
-    # list build per rebuild; the density deposit every 40 steps; 3 + 3*3 DFT
-    # passes + 7 element-wise kernels per cutoff update (every 2000 steps)
-    n_updates = (args.warmup + args.steps) // UPDATE_EVERY - args.warmup // UPDATE_EVERY
-    # (direct launch: the 7 rebuild kernels are launched every step and return
-    # early unless the device flag asks for a rebuild)
+    # list build per rebuild; the density deposit every 40 steps and 3 + 3*3 DFT
+    # passes + 7 element-wise kernels per cutoff update (every 2000 steps) --
+    # neither falls in a timed range shorter than 40 steps after the warm-up
+    first, last = steps0, steps0 + args.steps
+    n_updates = last // UPDATE_EVERY - first // UPDATE_EVERY
+    n_deposits = last // SAMPLE_EVERY - first // SAMPLE_EVERY
     rebuild_launches = 7 * (rebuilds_timed if use_graph else args.steps)
-    launches = (3 * args.steps + rebuild_launches + args.steps // SAMPLE_EVERY + 22 * n_updates)
-    cpu = None
+    launches = 3 * args.steps + rebuild_launches + n_deposits + 22 * n_updates
+    cpu = loop = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         n_cpu = 30
-        sps_cpu, cores, _ = cpu_baseline(s, lattice, n_cpu)
+        sps_cpu, cores = cpu_port(s, n_cpu)
         cpu = {"value": sps_cpu, "unit": "steps/s", "cores": cores, "kind": "port",
-               "sample": f"{n_cpu} Langevin NPT steps of the full 65536-atom slab "
-                         f"(oracle CPU FP64 cell+Verlet list LJ, OpenMP, skin {SKIN_SPEC})"}
+               "sample": f"{n_cpu} Langevin NPT steps of the full 65536-atom slab from the committed start "
+                         f"(oracle CPU FP64 cell + Verlet list LJ, OpenMP, skin {SKIN})"}
+        loop = reference_loop(P // 2)
     if rank == 0:
+        per_step = 1.0 / (value / world)
+        amortised = 1.0 / (per_step + (arc_update_s + (UPDATE_EVERY // SAMPLE_EVERY) * deposit_s) / UPDATE_EVERY)
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair math / f64 accumulation",
             "data": "synthetic",
-            "config": {"workload": "lj_slab_65536_npt", "n_atoms": N, "box": s.box.tolist(),
-                       "rc": rcinfo, "skin": SKIN, "dt": DT, "T": TEMP, "ensemble": "Langevin NPT Pzz=0",
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "flushed (256 MB write) between timed steps",
-                       "start": f"random sequential addition, {args.equil} NVT relaxation steps"},
+            "config": slab_config(s, world),
             "fp64_steps_per_s": fp64_sps,
             "speedup_vs_fp64": (value / world / fp64_sps) if fp64_sps else None,
-            "warm_l2_steps_per_s": warm_sps,
-            "force_rms_err_vs_fp64": {"abs": rms_abs, "rel": rms_rel},
+            "force_rms_err_vs_fp64": {"abs": rms_abs, "rel": rms_rel,
+                                      "what": "mixed against the FP64 path, same cutoffs, on the start"},
+            "force_rms_err_vs_long_cutoff": {
+                "mixed": err_long, "fp64": err_long64,
+                "apriori_estimate_rms": est_rms, "apriori_estimate_max_bin": est_max,
+                "target": TARGET_PREC,
+                "what": f"RMS over atoms of |F - F_ref| (eps/sigma) on the start, F_ref = FP64 forces at a "
+                        f"uniform cutoff {RC_LONG} plus the long-range force correction; the estimate is the "
+                        f"AdaptRCut error of each atom's bin at its assigned cutoff"},
             "list_rebuilds": rebuilds, "tau_per_day": value / world * DT * 86400,
+            "schedule": {"period_steps": period, "period_device_s": period_dev, "period_wall_s": t_period,
+                         "period_steps_per_s": period / t_period,
+                         "arc_update_ms": 1e3 * arc_update_s, "deposit_ms": 1e3 * deposit_s,
+                         "steps_per_s_with_arc": amortised,
+                         "what": "one AdaptRCut period of the reference app (50 deposits, 1 update + assign + "
+                                 "pressure correction per 2000 steps); period_* measured warm-L2 through "
+                                 "Simulation.run, steps_per_s_with_arc = flushed value with the measured "
+                                 "update and deposit costs amortised"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profiled_traffic("k_lj_mixed"),
                          "kernel": "k_lj_mixed",
-                         "kernel_us": t_lj * 1e6, "alg_bytes": alg_bytes, "peak_kind": peak_kind},
-            "nlist_build_us": t_nl * 1e6,
+                         "kernel_us": t_lj * 1e6, "alg_bytes": alg_bytes, "list_entries": P,
+                         "peak_kind": peak_kind},
+            "kernel_us": {"lj_mixed": t_lj * 1e6, "lj_fp64": None if t_lj64 is None else t_lj64 * 1e6,
+                          "nlist_build_mixed": t_nl * 1e6,
+                          "nlist_build_fp64": None if t_lj64 is None else t_nl64 * 1e6},
             "e2e": {"value": e2e_sps, "unit": "steps/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "steps": e2e_steps, "setup_s": t_setup,
-                    "path": "MDSystem from pinned host arrays, Simulation.run(steps) with every step's "
-                            "statistics written by the device into its own pinned host row, "
-                            "positions and forces read back at the end"},
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps, "setup_s": t_setup, "run_s": t_run,
+                    "steady_steps_per_s": e2e_steps / t_run,
+                    "path": "MDSystem from pinned host arrays, AdaptRCut attached on the reference schedule, "
+                            "Simulation.run(steps) with every step's statistics written by the device into its "
+                            "own pinned host row, positions and forces read back at the end"},
             "gpu_launches": launches,
             "list_rebuilds_timed": rebuilds_timed,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "reference_loop": loop,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -341,6 +341,20 @@ int md_error_estimate_spme_ik(md_system* sys, const int K[3], int order, double 
 int md_error_estimate_spme_ik_noalloc(md_system* sys, const int K[3], int order, double beta, double* err);
 /* splitting beta whose real-space estimate equals target at cutoff rcut */
 int md_choose_beta(md_system* sys, double rcut, double target, double* beta);
+/* Splitting beta and power-of-two mesh K (at most kmax per axis) for an inhomogeneous
+ * system so that the largest per-bin RMS force error estimate is within target / sqrt(2)
+ * in real space and in reciprocal space (ik, B-spline order `order`).  No counterpart
+ * function in the reference: it drives the reference's estimates the way their users pick
+ * the parameters.  beta: errorEstimatePME's real-space term
+ * (RE/src/ElectrostaticInteraction.cpp:349-401) at the largest local sum of q^2 per volume
+ * over cubes of edge ~2 rcut.  K: grown from the homogeneous estimate
+ * (RE/src/EleRecBSpline.cpp:154-206), then decided by the inhomogeneous ik-SPME map
+ * (ErrorEstimate_SPME_Ik, as md_errmap_create) of the system's current charge profile on
+ * each candidate mesh, coarsest axis doubled until within budget, finest axis halved
+ * while within budget.  err_dir, err_rec (nullable): the two largest per-bin estimates.
+ * MD_ERR_BADARG when no mesh up to kmax meets the budget. */
+int md_choose_spme_params(md_system* sys, double rcut, int order, double target, int kmax, double* beta,
+                          int K[3], double* err_dir, double* err_rec);
 
 /* Inhomogeneous ik-SPME error map (ErrorEstimate_SPME_Ik::reinit / calError,
  * longRange.hetero/profile.test/template/tools/analyze/src/ErrorEstimate_SPME_Ik.cpp:80-470,

@@ -230,16 +230,75 @@ __global__ void k_dft_axis(double2* data, ArcDims g, int axis, int sign, int bat
   }
 }
 
+// Power-of-two lines: radix-2 Stockham FFT of one line per block in shared
+// memory (autosorting, natural order in and out; Govindaraju et al., SC'08),
+// same convention and result as k_dft_axis.  Stage Ns (1, 2, 4, ...): for
+// butterfly j < n/2, k = j mod Ns, v1 = x[j + n/2] exp(sign i pi k / Ns);
+// y[2 Ns floor(j/Ns) + k] = x[j] + v1, y[... + Ns] = x[j] - v1.  Twiddles
+// exp(sign 2 pi i t / n), t < n/2, from FP64 sincospi once per block.
+__global__ void k_fft2_axis(double2* data, ArcDims g, int axis, int sign, int batch, int logn) {
+  extern __shared__ double2 sm[];
+  const int n = 1 << logn, h = n >> 1;
+  double2* x = sm;
+  double2* y = sm + n;
+  double2* tw = sm + 2 * n;
+  const int a1 = (axis + 1) % 3, a2 = (axis + 2) % 3;
+  const long lines = (long)g.n[a1] * g.n[a2];
+  const long lid = blockIdx.x;
+  if (lid >= lines * batch) return;
+  const long nele = (long)g.n[0] * g.n[1] * g.n[2];
+  const int b = (int)(lid / lines);
+  const long r = lid % lines;
+  const int i1 = (int)(r / g.n[a2]), i2 = (int)(r % g.n[a2]);
+  const long stride[3] = {(long)g.n[1] * g.n[2], (long)g.n[2], 1};
+  double2* base = data + (long)b * nele + i1 * stride[a1] + i2 * stride[a2];
+  const long st = stride[axis];
+  for (int j = threadIdx.x; j < n; j += blockDim.x) x[j] = base[j * st];
+  for (int t = threadIdx.x; t < h; t += blockDim.x) {
+    double sn, cs;
+    sincospi(2.0 * t / n, &sn, &cs);
+    tw[t] = make_double2(cs, sign * sn);
+  }
+  __syncthreads();
+  for (int ls = 0; ls < logn; ++ls) {
+    const int Ns = 1 << ls;
+    for (int j = threadIdx.x; j < h; j += blockDim.x) {
+      const int k = j & (Ns - 1);
+      const double2 w = tw[k << (logn - 1 - ls)];  // exp(sign i pi k / Ns)
+      const double2 v0 = x[j], u = x[j + h];
+      const double2 v1 = make_double2(u.x * w.x - u.y * w.y, u.x * w.y + u.y * w.x);
+      const int d = ((j >> ls) << (ls + 1)) + k;
+      y[d] = make_double2(v0.x + v1.x, v0.y + v1.y);
+      y[d + Ns] = make_double2(v0.x - v1.x, v0.y - v1.y);
+    }
+    __syncthreads();
+    double2* t = x;
+    x = y;
+    y = t;
+  }
+  for (int j = threadIdx.x; j < n; j += blockDim.x) base[j * st] = x[j];
+}
+
 // unnormalised 3D DFT (sign -1 forward, +1 backward) of `batch` consecutive
-// complex grids [n0][n1][n2], in place, any sizes up to 1024 per axis
+// complex grids [n0][n1][n2], in place, any sizes up to 1024 per axis;
+// power-of-two axes by the FFT above, others by the direct sum
 int dft3_grid(double2* data, const int n[3], int sign, int batch, cudaStream_t stream) {
   ArcDims g;
   for (int d = 0; d < 3; ++d) g.n[d] = n[d];
   for (int axis = 2; axis >= 0; --axis) {
+    const int na = g.n[axis];
     long lines = (long)g.n[(axis + 1) % 3] * g.n[(axis + 2) % 3] * batch;
-    size_t smem = sizeof(double2) * 2 * g.n[axis];
-    k_dft_axis<<<(unsigned)lines, 128, smem, stream>>>(data, g, axis, sign, batch);
-    MD_CHECK_LAUNCH("dft axis");
+    if (na >= 2 && (na & (na - 1)) == 0) {
+      int logn = 0;
+      while ((1 << logn) < na) ++logn;
+      const size_t smem = sizeof(double2) * (2 * na + na / 2);
+      k_fft2_axis<<<(unsigned)lines, 128, smem, stream>>>(data, g, axis, sign, batch, logn);
+      MD_CHECK_LAUNCH("fft axis");
+    } else {
+      size_t smem = sizeof(double2) * 2 * na;
+      k_dft_axis<<<(unsigned)lines, 128, smem, stream>>>(data, g, axis, sign, batch);
+      MD_CHECK_LAUNCH("dft axis");
+    }
   }
   return MD_OK;
 }

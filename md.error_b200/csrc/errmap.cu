@@ -15,7 +15,9 @@
 // takes 25 batched 3D transforms at creation; an evaluation takes 2 + 4.
 // rho1 is the density of charge signs, rho2 the number density of charges
 // (profile1 / profile2 of the reference).
+#include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 #include "device_common.cuh"
 
@@ -813,5 +815,175 @@ extern "C" int md_errmap_get_profile(md_errmap* h, double* rho1, double* rho2) {
   MD_CUDA(cudaStreamSynchronize(h->stream));
   if (rho1) MD_CUDA(cudaMemcpy(rho1, h->rho, sizeof(double) * h->g.N, cudaMemcpyDeviceToHost));
   if (rho2) MD_CUDA(cudaMemcpy(rho2, h->rho + h->g.N, sizeof(double) * h->g.N, cudaMemcpyDeviceToHost));
+  return MD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Choice of the splitting parameter and the mesh for an inhomogeneous system
+// (no counterpart function in the reference; it applies the reference's error
+// estimates the way their users pick beta and K).  The budget is split evenly:
+// target / sqrt(2) for the real space and for the reciprocal space.
+//  - beta: the real-space estimate of errorEstimatePME
+//    (RE/src/ElectrostaticInteraction.cpp:349-401), 2 q_rms sqrt(c2 / (N rcut V))
+//    exp(-beta^2 rcut^2), taken with c2 / V replaced by the largest local sum
+//    of q^2 per volume, averaged over cubes of edge about 2 rcut around each
+//    bin of a rcut/2 grid: the short-range limit of the inhomogeneous real-space
+//    map.  (The map itself, ErrorEstimate_dir, is built by a quadrature that
+//    does not converge at the beta rcut of about 3 that such targets need.)
+//  - K: powers of two per axis.  Starting from the homogeneous ik estimate
+//    (EleRecBSpline.cpp:154-206), the axis with the coarsest spacing is
+//    doubled until the largest per-bin RMS error of the inhomogeneous ik-SPME
+//    map (ErrorEstimate_SPME_Ik) of the system's charge profile on that mesh
+//    is within budget, then the axis with the finest spacing is halved while
+//    it stays within budget.
+__global__ void k_em_rms_max(long n, const double* e1, const double* e2, unsigned long long* out) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (t < n) {
+    const double s = e1[2 * t] + e2[2 * t];
+    v = s > 0.0 ? sqrt(s) : 0.0;  // a negative sum is rounding in an empty bin
+  }
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0 && v > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
+}
+
+// largest per-bin RMS force error of the ik map on mesh K for the system's profile
+static int em_ik_max(md_system* sys, const int K[3], const double L[3], double beta, int order, double charge,
+                     double* out) {
+  md_errmap* h = nullptr;
+  if (int r = md_errmap_create(&h, K, L, beta, order, sys->device)) return r;
+  int r = md_errmap_deposit(h, sys);
+  unsigned long long* dmax = nullptr;
+  if (!r && cudaMallocAsync((void**)&dmax, sizeof(unsigned long long), h->stream) != cudaSuccess)
+    r = md_cuda_fail(cudaGetLastError(), "error map maximum");
+  if (!r) r = em_convolve(h);
+  if (!r) {
+    const long N = h->g.N;
+    const unsigned nb = (unsigned)((N + 255) / 256);
+    double* d = reinterpret_cast<double*>(h->work2);
+    cudaMemsetAsync(dmax, 0, sizeof(unsigned long long), h->stream);
+    k_em_finish<<<nb, 256, 0, h->stream>>>(h->g, h->work, charge, d, d + 2 * N);
+    k_em_rms_max<<<nb, 256, 0, h->stream>>>(N, d, d + 2 * N, dmax);
+    unsigned long long bits = 0;
+    if (cudaMemcpyAsync(&bits, dmax, sizeof(bits), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess)
+      r = md_cuda_fail(cudaGetLastError(), "error map maximum");
+    double v;
+    memcpy(&v, &bits, sizeof(v));
+    *out = v;
+  }
+  if (dmax) cudaFreeAsync(dmax, h->stream);
+  md_errmap_destroy(h);
+  return r;
+}
+
+extern "C" int md_choose_spme_params(md_system* sys, double rcut, int order, double target, int kmax,
+                                     double* beta, int K[3], double* err_dir, double* err_rec) {
+  if (!sys || !(rcut > 0) || order < 2 || order > 14 || !(target > 0) || !beta || !K || kmax < 2 * order) {
+    md_set_error("md_choose_spme_params: bad arguments");
+    return MD_ERR_BADARG;
+  }
+  if (kmax > 1024) kmax = 1024;
+  DevState hs;
+  if (int r = sys->read_state(hs)) return r;
+  const int N = sys->N;
+  std::vector<double> pos(3 * (size_t)N), q(N);
+  if (int r = md_system_get_positions(sys, pos.data())) return r;
+  if (int r = md_system_get_charges(sys, q.data())) return r;
+  double c2 = 0.0;
+  for (double v : q) c2 += v * v;
+  if (!(c2 > 0)) { md_set_error("md_choose_spme_params: the system has no charges"); return MD_ERR_BADARG; }
+  const double qrms = sqrt(c2 / N);
+  // local q^2 density: bins of at most rcut/2, box average over +-m bins (periodic)
+  int nb[3], m[3];
+  double hb[3];
+  for (int d = 0; d < 3; ++d) {
+    nb[d] = std::max(1, (int)floor(hs.L[d] / (0.5 * rcut)));
+    hb[d] = hs.L[d] / nb[d];
+    m[d] = std::min((int)ceil(rcut / hb[d]), (nb[d] - 1) / 2);
+  }
+  const size_t nbt = (size_t)nb[0] * nb[1] * nb[2];
+  std::vector<double> w(nbt, 0.0), t1(nbt), t2(nbt);
+  for (int i = 0; i < N; ++i) {
+    int b[3];
+    for (int d = 0; d < 3; ++d) {
+      double x = pos[3 * (size_t)i + d] - floor(pos[3 * (size_t)i + d] / hs.L[d]) * hs.L[d];
+      b[d] = std::min(nb[d] - 1, std::max(0, (int)(x / hb[d])));
+    }
+    w[b[2] + (size_t)nb[2] * (b[1] + (size_t)nb[1] * b[0])] += q[i] * q[i];
+  }
+  // separable periodic box filter along z, y, x
+  auto filt = [&](const std::vector<double>& in, std::vector<double>& out, int axis) {
+    for (int i0 = 0; i0 < nb[0]; ++i0)
+      for (int i1 = 0; i1 < nb[1]; ++i1)
+        for (int i2 = 0; i2 < nb[2]; ++i2) {
+          double s = 0.0;
+          for (int k = -m[axis]; k <= m[axis]; ++k) {
+            int c[3] = {i0, i1, i2};
+            c[axis] = ((c[axis] + k) % nb[axis] + nb[axis]) % nb[axis];
+            s += in[c[2] + (size_t)nb[2] * (c[1] + (size_t)nb[1] * c[0])];
+          }
+          out[i2 + (size_t)nb[2] * (i1 + (size_t)nb[1] * i0)] = s;
+        }
+  };
+  filt(w, t1, 2);
+  filt(t1, t2, 1);
+  filt(t2, t1, 0);
+  double vol = 1.0;
+  for (int d = 0; d < 3; ++d) vol *= (2 * m[d] + 1) * hb[d];
+  double rho_max = 0.0;
+  for (double v : t1) rho_max = std::max(rho_max, v / vol);
+  const double tb = target / sqrt(2.0);
+  const double pre = 2.0 * qrms * sqrt(rho_max / rcut);
+  const double b = sqrt(std::max(log(pre / tb), 1.0)) / rcut;
+  *beta = b;
+  if (err_dir) *err_dir = pre * exp(-b * b * rcut * rcut);
+  // mesh: homogeneous estimate first, then the inhomogeneous map
+  int k[3];
+  for (int d = 0; d < 3; ++d) {
+    k[d] = 1;
+    while (k[d] <= order) k[d] <<= 1;
+  }
+  auto coarsest = [&](int lim) {
+    int a = -1;
+    for (int d = 0; d < 3; ++d)
+      if (2 * k[d] <= lim && (a < 0 || hs.L[d] / k[d] > hs.L[a] / k[a])) a = d;
+    return a;
+  };
+  for (int it = 0; it < 40; ++it) {
+    double e = 0.0;
+    if (int r = md_error_estimate_spme_ik(sys, k, order, b, &e)) return r;
+    if (e <= tb) break;
+    const int a = coarsest(kmax);
+    if (a < 0) break;
+    k[a] *= 2;
+  }
+  double e = 0.0;
+  for (int it = 0; it < 40; ++it) {
+    if (int r = em_ik_max(sys, k, hs.L, b, order, qrms, &e)) return r;
+    if (e <= tb) break;
+    const int a = coarsest(kmax);
+    if (a < 0) {
+      md_set_error("md_choose_spme_params: meshes up to %d per axis give %g > %g in reciprocal space", kmax, e, tb);
+      return MD_ERR_BADARG;
+    }
+    k[a] *= 2;
+  }
+  for (int it = 0; it < 40; ++it) {
+    int a = -1;
+    for (int d = 0; d < 3; ++d)
+      if (k[d] / 2 > order && (a < 0 || hs.L[d] / k[d] < hs.L[a] / k[a])) a = d;
+    if (a < 0) break;
+    k[a] /= 2;
+    double e2 = 0.0;
+    if (int r = em_ik_max(sys, k, hs.L, b, order, qrms, &e2)) return r;
+    if (e2 > tb) {
+      k[a] *= 2;
+      break;
+    }
+    e = e2;
+  }
+  for (int d = 0; d < 3; ++d) K[d] = k[d];
+  if (err_rec) *err_rec = e;
   return MD_OK;
 }

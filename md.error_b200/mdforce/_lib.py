@@ -123,6 +123,7 @@ _SIGS = {
     "md_error_estimate_spme_ik": (i32, [vp, P(i32), i32, f64, P(f64)]),
     "md_error_estimate_spme_ik_noalloc": (i32, [vp, P(i32), i32, f64, P(f64)]),
     "md_choose_beta": (i32, [vp, f64, f64, P(f64)]),
+    "md_choose_spme_params": (i32, [vp, f64, i32, f64, i32, P(f64), P(i32), P(f64), P(f64)]),
     "md_sim_attach_adapt_rcut": (i32, [vp, vp, i32, i32, f64, i32]),
     "md_arc_create": (i32, [P(vp), vp, f64, f64, f64, f64]),
     "md_arc_destroy": (i32, [vp]),

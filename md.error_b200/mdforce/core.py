@@ -706,6 +706,18 @@ def choose_beta(sys, rcut, target):
     return b.value
 
 
+def choose_spme_params(sys, rcut, order, target, kmax=1024):
+    """(beta, K, err_dir, err_rec): splitting parameter and power-of-two mesh whose
+    largest per-bin error estimates (real space at the densest region; ik-SPME map
+    ErrorEstimate_SPME_Ik of the system's charge profile) are within target/sqrt(2)
+    each (md_choose_spme_params)."""
+    b, ed, er = C.c_double(), C.c_double(), C.c_double()
+    K = (C.c_int * 3)()
+    check(lib.md_choose_spme_params(sys.h, float(rcut), int(order), float(target), int(kmax), C.byref(b), K,
+                                    C.byref(ed), C.byref(er)), "choose_spme_params")
+    return b.value, tuple(K), ed.value, er.value
+
+
 class AssignRCut:
     """Per-atom cutoff from an rc lattice (AssignRCut::getRCut + assign)."""
 

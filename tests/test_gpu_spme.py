@@ -316,3 +316,53 @@ def test_mean_force_field_matches_the_error1_components(mdf, orc):
         e1, _ = em.calError(1.3)
         assert mf.shape == (3,) + K
         assert np.allclose((mf ** 2).sum(axis=0), e1[..., 0], rtol=1e-12, atol=1e-14 * np.abs(e1[..., 0]).max())
+
+
+def test_choose_spme_params_meets_target(mdf):
+    """md_choose_spme_params on a charged liquid-vapour slab (4000 +-1 charges,
+    16 x 16 x 48, liquid rho 0.8 for |z - 24| < 7.5, vapour elsewhere): both
+    largest per-bin estimates within target / sqrt(2); each mesh axis needed
+    (halving it breaks the reciprocal budget, by the ik map); and the FP64
+    forces with the chosen beta and K (real space at rc 3 + ik SPME, order 6)
+    within the target RMS of the converged Ewald sum (real space at rc 7.9,
+    exact reciprocal sum to 1e-12)."""
+    box = np.array([16.0, 16.0, 48.0])
+    n = 4000
+    thick, n_in = mdf.systems.slab_counts(n, box, 2, 0.8, 0.02)
+    pos = mdf.systems.slab(n, n_in, box, 2, 24.0, 0.5 * thick, 0.8, 5)
+    q = mdf.systems.charges(n, 6)
+    target, rc, order = 2e-3, 3.0, 6
+    sys = mdf.MDSystem(pos, box, charge=q, precision=1)
+    beta, K, e_dir, e_rec = mdf.choose_spme_params(sys, rc, order, target, kmax=256)
+    tb = target / np.sqrt(2)
+    assert e_dir <= tb * (1 + 1e-9) and e_rec <= tb
+    assert all(k & (k - 1) == 0 for k in K)
+    for d in range(3):
+        if K[d] // 2 <= order:
+            continue
+        Kh = list(K)
+        Kh[d] //= 2
+        em = mdf.ErrorEstimate_SPME_Ik(Kh, box, beta, order)
+        em.deposit(sys)
+        assert np.nanmax(em.rms(1.0)) > tb, (K, d)
+    out = {}
+    for which, rcut in (("chosen", rc), ("reference", 7.9)):
+        s = mdf.MDSystem(pos, box, charge=q, precision=1)
+        s.set_rcut(np.full(n, rcut, np.float32))
+        eng = mdf.InteractionEngine(s)
+        eng.registNonBondedInteraction(0.0, 1.0, 0.0)
+        mdf.registCoulomb(eng, beta)
+        cl = mdf.CellList(s, 3.3)
+        cl.rebuild()
+        nl = mdf.NeighborList(s, rcut + 0.3, 0.3, expansion=1.5)
+        nl.fit(s, cl)
+        eng.clearInteraction()
+        eng.applyNonBondedInteraction(s, nl)
+        if which == "chosen":
+            mdf.SPME(s, K, order, beta, "ik").apply()
+        else:
+            mmax = [2 * int(np.ceil(1.67 * beta * L)) + 1 for L in box]
+            mdf.ewald_exact(s, mmax, beta)
+        out[which] = s.forces()
+    err = float(np.sqrt(((out["chosen"] - out["reference"]) ** 2).sum(1).mean()))
+    assert err < target, (err, beta, K, e_dir, e_rec)
