@@ -118,6 +118,15 @@ int md_system_get_velocities(md_system* sys, double* vel);
 int md_system_get_forces(md_system* sys, double* force);
 /* per-atom charges [N] in original order (MDSystem ddata.charge) */
 int md_system_set_charges(md_system* sys, const double* charge);
+/* Zero-copy input from device memory (e.g. torch tensors): raw device pointers in the
+   caller's atom order; NULL members leave that quantity unchanged.  Asynchronous on the
+   system's stream, which must be the producer's stream (md_system_set_stream) or ordered
+   after it.  (The md_device_view of the survey's drop-in boundary: a DeviceMDData view.) */
+typedef struct md_device_view {
+  const double* pos;     /* [N][3] positions */
+  const double* charge;  /* [N] charges */
+} md_device_view;
+int md_system_set_device_view(md_system* sys, const md_device_view* v);
 int md_system_get_charges(md_system* sys, double* charge);
 /* per-atom masses [N] in original order (MDSystem hdata.mass / massi, copied by
    MDSystem::initTopology, shortRange.inhomo/template/tools.collision/cal.real.error/src/
@@ -308,6 +317,11 @@ int md_spme_get_mesh(md_spme* spme, double* Q);
  * Every output is nullable; host arrays in original atom order; synchronises. */
 int md_spme_energy_grad(md_spme* spme, md_system* sys, double* energy, double* dE_dq,
                         double* dE_dr, double* dE_dbeta, double* dE_dpsi);
+/* md_spme_energy_grad with DEVICE outputs (energy, dE_dbeta: one double each; dE_dq [N],
+   dE_dr [N][3] in the caller's atom order; each nullable), asynchronous on the system's
+   stream: with md_system_set_device_view a differentiable SPME energy without host copies */
+int md_spme_energy_grad_device(md_spme* spme, md_system* sys, double* energy, double* dE_dq, double* dE_dr,
+                               double* dE_dbeta);
 /* influence function psi on the half spectrum [K0][K1][K2/2+1] (calPsiFPhiF, ik scaling) */
 int md_spme_get_influence(md_spme* spme, double* psi);
 /* Self-force correction of analytic differentiation (SelfCorr::reinit + correction,
@@ -352,7 +366,7 @@ int md_choose_beta(md_system* sys, double rcut, double target, double* beta);
  * (ErrorEstimate_SPME_Ik, as md_errmap_create) of the system's current charge profile on
  * each candidate mesh, coarsest axis doubled until within budget, finest axis halved
  * while within budget.  err_dir, err_rec (nullable): the two largest per-bin estimates.
- * MD_ERR_BADARG when no mesh up to kmax meets the budget. */
+ * Meshes stay within kmax per axis and 2^27 points; MD_ERR_BADARG when none meets the budget. */
 int md_choose_spme_params(md_system* sys, double rcut, int order, double target, int kmax, double* beta,
                           int K[3], double* err_dir, double* err_rec);
 
@@ -600,6 +614,34 @@ int md_synth_slab(int n, int n_in, const double box[3], int axis, double center,
 int md_synth_maxwell(int n, const double* mass, double temperature, uint64_t seed, double* vel);
 /* n/2 charges +1 and n/2 charges -1 in seeded random order */
 int md_synth_charges(int n, uint64_t seed, double* q);
+
+/* ------------------------------------------------------------ SPME with a Hermite basis
+ * ik-SPME whose interpolation basis is optiBasis's symmetric piecewise cubic Hermite basis
+ * (optiBasis/Hermite.py:6-130, optiBasis/HatComput.py:155-300: value 1 and slope 0 at 0,
+ * coefficients [v_1..v_n, d_1..d_n] at the knots j CC/nbin, n = nbin or nbin - 1 when
+ * bound0), in place of the B-spline of ElectrostaticInteraction_rec_BSpline
+ * (RE/src/EleRecBSpline.cpp:393-536, the interpolation factor of calB :729-796 taken from
+ * the basis' integer samples), with hand-written adjoints for the optiBasis gradient loop
+ * (optiBasis/compute_basis.py:38-111).  FP64.  Every array argument is DEVICE memory in the
+ * caller's atom order (raw pointers, e.g. torch tensors' data_ptr()), every call is
+ * asynchronous on `stream` (NULL: the default stream); coeffs [C][ncoef] is a batch of
+ * candidate bases.  For one system of natoms charges on mesh K in box L, splitting beta. */
+typedef struct md_hspme md_hspme;
+int md_hspme_create(md_hspme** out, int natoms, const int K[3], const double L[3], double beta, double CC,
+                    int nbin, int bound0, int device);
+int md_hspme_destroy(md_hspme* h);
+int md_hspme_num_coeffs(md_hspme* h, int* out);
+/* reciprocal energy[C] of charges q [N] at positions r [N][3] for each candidate, and when
+   non-NULL: ik forces [C][N][3], dE/dq [C][N], dE/dr [C][N][3] (the exact gradient), dE/dc
+   [C][ncoef] */
+int md_hspme_energy(md_hspme* h, const double* q, const double* r, const double* coeffs, int C,
+                    double* energy, double* forces, double* dE_dq, double* dE_dr, double* dE_dc, void* stream);
+/* force-error functional loss[C] = 1/N sum_i |F_i - fref_i|^2 of the ik forces against given
+   reference forces fref [N][3] (e.g. md_ewald_exact), and when non-NULL its gradients dL/dq
+   [C][N], dL/dr [C][N][3], dL/dc [C][ncoef] (second adjoint of the SPME chain) */
+int md_hspme_force_error(md_hspme* h, const double* q, const double* r, const double* coeffs, int C,
+                         const double* fref, double* loss, double* dL_dq, double* dL_dr, double* dL_dc,
+                         void* stream);
 
 /* ------------------------------------------------------------ optiBasis error functional
  * Replaces HermiteLossFunc / HermiteLossFunc_Bound0 .value / .deriv

@@ -169,6 +169,37 @@ __global__ void k_order(int ntot, const uint32_t* start, const uint32_t* members
   }
 }
 
+// warp per cell, after the gather: the cell's slots ranked by (z, slot), so
+// that each cell's z order is at zord[start[c] ..] (slot order itself stays by
+// cutoff for the force kernel)
+template <class R>
+__global__ void k_zorder(int ntot, const uint32_t* start, const typename V4<R>::T* pos, uint32_t* zord,
+                         const DevState* st, int gate) {
+  if (gate && !(st->flags & FLAG_REBUILD)) return;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= ntot) return;
+  const uint32_t s = start[warp], n = start[warp + 1] - s;
+  for (uint32_t b = 0; b < n; b += 32) {
+    const bool on = b + lane < n;
+    const uint32_t e = on ? s + b + lane : 0u;
+    const R ze = on ? pos[e].z : R(0);
+    uint32_t rank = 0;
+    for (uint32_t b2 = 0; b2 < n; b2 += 32) {
+      const bool on2 = b2 + lane < n;
+      const uint32_t e2 = on2 ? s + b2 + lane : 0xffffffffu;
+      const R z2 = on2 ? pos[e2].z : R(0);
+#pragma unroll 8
+      for (int t = 0; t < 32; ++t) {
+        const R zt = __shfl_sync(0xffffffffu, z2, t);
+        const uint32_t et = __shfl_sync(0xffffffffu, e2, t);
+        rank += (et != 0xffffffffu && (zt < ze || (zt == ze && et < e))) ? 1u : 0u;
+      }
+    }
+    if (on) zord[s + rank] = e;
+  }
+}
+
 // AssignRCut::assign index (ENG/src/AssignRCut.cu:93-112) in binary32
 __device__ __forceinline__ float lattice_rcut(float x, float y, float z, const DevState* st,
                                               const float* lat, int nx, int ny, int nz) {
@@ -265,6 +296,12 @@ static int rebuild_t(md_cell_list* cl, md_system* sys, Recorder* rec, bool gated
                  &pos, &vel, &sys->force, &sys->image, &sys->id, &sys->rcut, &st, &gate};
     if (int r = rec_launch(rec, (const void*)k_copyback<R>, dim3(nb), dim3(256), 0, a)) return r;
   }
+  {
+    int n = cl->ntot;
+    void* a[] = {&n, &cl->start, &pos, &cl->zord, &st, &gate};
+    if (int r = rec_launch(rec, (const void*)k_zorder<R>, dim3(ceil_div((long long)n * 32, 256)), dim3(256), 0, a))
+      return r;
+  }
   return MD_OK;
 }
 
@@ -305,6 +342,7 @@ extern "C" int md_cell_list_create(md_cell_list** out, md_system* sys, double ce
             cudaMalloc(&cl->start, sizeof(uint32_t) * (cl->ntot + 1)) == cudaSuccess &&
             cudaMalloc(&cl->members, sizeof(uint32_t) * N) == cudaSuccess &&
             cudaMalloc(&cl->perm, sizeof(uint32_t) * N) == cudaSuccess &&
+            cudaMalloc(&cl->zord, sizeof(uint32_t) * N) == cudaSuccess &&
             cudaMemset(cl->count, 0, sizeof(uint32_t) * cl->ntot) == cudaSuccess;
   if (!ok) {
     md_cuda_fail(cudaGetLastError(), "md_cell_list_create");
@@ -317,7 +355,7 @@ extern "C" int md_cell_list_create(md_cell_list** out, md_system* sys, double ce
 
 extern "C" int md_cell_list_destroy(md_cell_list* cl) {
   if (!cl) return MD_OK;
-  void* p[] = {cl->cell_of, cl->t_cell, cl->slot, cl->count, cl->start, cl->members, cl->perm};
+  void* p[] = {cl->cell_of, cl->t_cell, cl->slot, cl->count, cl->start, cl->members, cl->perm, cl->zord};
   for (void* q : p) if (q) cudaFree(q);
   delete cl;
   return MD_OK;

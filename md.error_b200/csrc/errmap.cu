@@ -944,10 +944,14 @@ extern "C" int md_choose_spme_params(md_system* sys, double rcut, int order, dou
     k[d] = 1;
     while (k[d] <= order) k[d] <<= 1;
   }
+  // meshes are kept to at most 2^27 points (an ik map of that size holds
+  // about 30 GB of FP64 kernels and profiles)
+  const long long max_points = 1ll << 27;
   auto coarsest = [&](int lim) {
     int a = -1;
+    const long long pts = (long long)k[0] * k[1] * k[2];
     for (int d = 0; d < 3; ++d)
-      if (2 * k[d] <= lim && (a < 0 || hs.L[d] / k[d] > hs.L[a] / k[a])) a = d;
+      if (2 * k[d] <= lim && 2 * pts <= max_points && (a < 0 || hs.L[d] / k[d] > hs.L[a] / k[a])) a = d;
     return a;
   };
   for (int it = 0; it < 40; ++it) {
@@ -964,7 +968,8 @@ extern "C" int md_choose_spme_params(md_system* sys, double rcut, int order, dou
     if (e <= tb) break;
     const int a = coarsest(kmax);
     if (a < 0) {
-      md_set_error("md_choose_spme_params: meshes up to %d per axis give %g > %g in reciprocal space", kmax, e, tb);
+      md_set_error("md_choose_spme_params: meshes up to %d per axis and 2^27 points give %g > %g in reciprocal "
+                   "space", kmax, e, tb);
       return MD_ERR_BADARG;
     }
     k[a] *= 2;

@@ -140,6 +140,9 @@ struct md_cell_list {
   uint32_t* start = nullptr;       // exclusive scan, ntot+1
   uint32_t* members = nullptr;     // cell member lists (current index)
   uint32_t* perm = nullptr;        // perm[new] = old
+  // the slots of each cell ordered by z: zord[start[c] .. start[c+1]) (the list
+  // build reads runs of cells in this order to cut each atom's z window exactly)
+  uint32_t* zord = nullptr;
   bool built = false;
 };
 

@@ -48,15 +48,24 @@ __device__ __forceinline__ int img_code(int kx, int ky, int kz) {
   return ((kx + 1) << 26) | ((ky + 1) << 28) | ((kz + 1) << 30);
 }
 
+// the slot index carried in the w component of a staged position (bit copy)
+template <class R> __device__ __forceinline__ R slot_as_w(int j);
+template <> __device__ __forceinline__ float slot_as_w<float>(int j) { return __int_as_float(j); }
+template <> __device__ __forceinline__ double slot_as_w<double>(int j) { return __longlong_as_double((long long)j); }
+template <class R> __device__ __forceinline__ int slot_of_w(R w);
+template <> __device__ __forceinline__ int slot_of_w<float>(float w) { return __float_as_int(w); }
+template <> __device__ __forceinline__ int slot_of_w<double>(double w) { return (int)__double_as_longlong(w); }
+
 template <class R, int MODE>
 __global__ void __launch_bounds__(256, 4)
 k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __restrict__ rcut,
-           const uint32_t* __restrict__ start, NlGeom g, const DevState* __restrict__ st,
-           double rlist_uniform, double skin, int cap, int* __restrict__ list, int* __restrict__ nnb,
-           typename V4<R>::T* __restrict__ backup, int force_minimage, DevState* stw, int gate) {
+           const uint32_t* __restrict__ start, const uint32_t* __restrict__ zord, NlGeom g,
+           const DevState* __restrict__ st, double rlist_uniform, double skin, int cap, int* __restrict__ list,
+           int* __restrict__ nnb, typename V4<R>::T* __restrict__ backup, int force_minimage, DevState* stw,
+           int gate) {
   typedef typename V4<R>::T T4;
   extern __shared__ __align__(16) unsigned char nl_smem[];
-  T4* tile = reinterpret_cast<T4*>(nl_smem);
+  T4* tile = reinterpret_cast<T4*>(nl_smem);  // w carries the atom's slot (charges are not needed here)
   __shared__ RunTable rt;
   __shared__ int nruns, tile_n, use_global;
   __shared__ float rl_max_sh;
@@ -189,10 +198,17 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
   // than 4 atoms reads its candidates from L2 instead (staging would cost
   // more than the few reads it saves)
   const bool stage = !use_global && (i1 - i0) >= 4;
+  // a run's cells are staged in their z order (zord), so each cell of the run
+  // is a z-sorted slice of the tile
   if (stage) {
     for (int r = warp; r < nr; r += nwarp) {
       const int c = rt.cnt[r], o = rt.off[r], jb = rt.jb[r];
-      for (int t = lane; t < c; t += 32) tile[o + t] = pos[jb + t];
+      for (int t = lane; t < c; t += 32) {
+        const int j = (int)zord[jb + t];
+        T4 v = pos[j];
+        v.w = slot_as_w<R>(j);
+        tile[o + t] = v;
+      }
     }
   }
   __syncthreads();
@@ -207,6 +223,11 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
   // the image code is the run's.
   const bool runshift = minimg && !full[0] && !full[1] && !full[2];
   const float hz = (float)h[2];
+  const float Lzf = (float)st->L[2];
+  // z of entry t of a run (z order) in the stored, wrapped frame
+  auto zat = [&](int roff, int rjb, int t) -> float {
+    return glob ? (float)pos[zord[rjb + t]].z : (float)tile[roff + t].z;
+  };
 
   for (int i = i0 + warp; i < i1; i += nwarp) {
     const T4 pi = pos[i];
@@ -235,84 +256,112 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
       if (rb + lane < nr) {
         const int r = rb + lane;
         keep = true;
+        float wz = rle_i;  // z half-window of i in this run's (x, y) column
         if (minimg) {
-          float dd = 0.f;
-          for (int d = 0; d < 3; ++d) {
+          float dxy = 0.f;
+          for (int d = 0; d < 2; ++d) {
             const float e = fmaxf(0.f, fmaxf(rt.b0[d][r] - xe[d], xe[d] - rt.b1[d][r]));
-            dd += e * e;
+            dxy += e * e;
           }
-          keep = dd <= rle_i * rle_i;
+          const float ez = fmaxf(0.f, fmaxf(rt.b0[2][r] - xe[2], xe[2] - rt.b1[2][r]));
+          keep = dxy + ez * ez <= rle_i * rle_i;
+          wz = sqrtf(fmaxf(rle_i * rle_i - dxy, 0.f));
         }
-        // the cells of the run that meet i's z window [z - rl, z + rl]
+        // the cells of the run that meet i's z window [z - wz, z + wz]; the
+        // first and last of them are cut to the window by binary search in
+        // their z order (the middle ones lie inside it whole)
         tbl = 0;
         tel = rt.cnt[r];
         const int nzr = rt.nz[r];
         if (keep && minimg && nzr) {
           const int zc0 = rt.zc0[r];
-          const int k0 = max((int)floorf((xe[2] - rle_i) / hz) - zc0, 0);
-          const int k1 = min((int)floorf((xe[2] + rle_i) / hz) - zc0, nzr - 1);
+          const int k0 = max((int)floorf((xe[2] - wz) / hz) - zc0, 0);
+          const int k1 = min((int)floorf((xe[2] + wz) / hz) - zc0, nzr - 1);
           keep = k0 <= k1;
           if (keep) {
-            tbl = rt.zoff[k0][r];
-            tel = rt.zoff[k1 + 1][r];
+            const int roff = rt.off[r], rjb = rt.jb[r];
+            // window in the stored frame: z_stored = z_run + sz L_z
+            const float shift = (float)rt.sz[r] * Lzf;
+            const float zlo = xe[2] - wz - 1e-3f + shift, zhi = xe[2] + wz + 1e-3f + shift;
+            int lo = rt.zoff[k0][r], hi = rt.zoff[k0 + 1][r];  // first index with z >= zlo
+            while (lo < hi) {
+              const int mid = (lo + hi) >> 1;
+              if (zat(roff, rjb, mid) < zlo) lo = mid + 1; else hi = mid;
+            }
+            tbl = lo;
+            lo = rt.zoff[k1][r];  // first index with z > zhi
+            hi = rt.zoff[k1 + 1][r];
+            while (lo < hi) {
+              const int mid = (lo + hi) >> 1;
+              if (zat(roff, rjb, mid) <= zhi) lo = mid + 1; else hi = mid;
+            }
+            tel = lo;
+            keep = tbl < tel;
           }
         }
       }
-      unsigned km = __ballot_sync(0xffffffffu, keep);
-      while (km) {
-      const int src = __ffs(km) - 1;
-      km &= km - 1;
-      const int r = rb + src;
-      const int rjb = rt.jb[r], roff = rt.off[r], rsx = rt.sx[r], rsy = rt.sy[r], rsz = rt.sz[r];
-      const int tb = __shfl_sync(0xffffffffu, tbl, src), te = __shfl_sync(0xffffffffu, tel, src);
-      const R shx = mul_rn((R)rsx, L[0]), shy = mul_rn((R)rsy, L[1]), shz = mul_rn((R)rsz, L[2]);
-      if (runshift) {
-        const int rcode = img_code(rsx, rsy, rsz);
-        for (int t0 = tb; t0 < te; t0 += 32) {
-          const int t = t0 + lane;
-          bool ok = false;
-          const int j = rjb + t;
-          if (t < te) {
-            const T4 pj = glob ? pos[j] : tile[roff + t];
-            const R dx = sub_rn(sub_rn(pj.x, pi.x), shx);
-            const R dy = sub_rn(sub_rn(pj.y, pi.y), shy);
-            const R dz = sub_rn(sub_rn(pj.z, pi.z), shz);
-            const R d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
-            ok = (d2 < rl2) && (j != i);
-          }
-          const unsigned m = __ballot_sync(0xffffffffu, ok);
-          if (ok) {
-            const int p = n + __popc(m & ltmask);
-            if (p < cap) rowp[nl_slot(p)] = j | rcode;
-          }
-          n += __popc(m);
-        }
-        continue;
+      // the candidate ranges of the surviving runs, packed end to end into
+      // 32-lane chunks: lane l of a chunk takes candidate c = t0 + l, owned by
+      // the last run whose range starts at or before c (found by a 5-step
+      // search over the warp's exclusive prefix sums; an empty range never
+      // owns a candidate)
+      const int len = keep ? tel - tbl : 0;
+      int incl = len;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
       }
-      for (int t0 = tb; t0 < te; t0 += 32) {
-        const int t = t0 + lane;
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      const int excl = incl - len;
+      for (int t0 = 0; t0 < total; t0 += 32) {
+        const int cidx = t0 + lane;
+        int own = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const int e = __shfl_sync(0xffffffffu, excl, own + step < 32 ? own + step : 31);
+          if (own + step < 32 && e <= cidx) own += step;
+        }
+        const int oexcl = __shfl_sync(0xffffffffu, excl, own);
+        const int otb = __shfl_sync(0xffffffffu, tbl, own);
         bool ok = false;
-        int code = 0;
-        const int j = rjb + t;
-        if (t < te) {
-          const T4 pj = glob ? pos[j] : tile[roff + t];
-          const R rx = sub_rn(pj.x, pi.x), ry = sub_rn(pj.y, pi.y), rz = sub_rn(pj.z, pi.z);
-          const R kx = floor_r(add_rn(mul_rn(rx, Li[0]), R(0.5)));
-          const R ky = floor_r(add_rn(mul_rn(ry, Li[1]), R(0.5)));
-          const R kz = floor_r(add_rn(mul_rn(rz, Li[2]), R(0.5)));
-          R dx, dy, dz;
-          if (minimg) {
-            dx = sub_rn(rx, mul_rn(kx, L[0]));
-            dy = sub_rn(ry, mul_rn(ky, L[1]));
-            dz = sub_rn(rz, mul_rn(kz, L[2]));
+        int j = 0, code = 0;
+        if (cidx < total) {
+          const int r = rb + own;
+          const int rjb = rt.jb[r], roff = rt.off[r], rsx = rt.sx[r], rsy = rt.sy[r], rsz = rt.sz[r];
+          const int t = otb + (cidx - oexcl);
+          T4 pj;
+          if (glob) {
+            j = (int)zord[rjb + t];
+            pj = pos[j];
           } else {
-            dx = sub_rn(sub_rn(pj.x, shx), pi.x);
-            dy = sub_rn(sub_rn(pj.y, shy), pi.y);
-            dz = sub_rn(sub_rn(pj.z, shz), pi.z);
+            pj = tile[roff + t];
+            j = slot_of_w<R>(pj.w);
+          }
+          R dx, dy, dz;
+          if (runshift) {
+            dx = sub_rn(sub_rn(pj.x, pi.x), mul_rn((R)rsx, L[0]));
+            dy = sub_rn(sub_rn(pj.y, pi.y), mul_rn((R)rsy, L[1]));
+            dz = sub_rn(sub_rn(pj.z, pi.z), mul_rn((R)rsz, L[2]));
+            code = img_code(rsx, rsy, rsz);
+          } else {
+            const R rx = sub_rn(pj.x, pi.x), ry = sub_rn(pj.y, pi.y), rz = sub_rn(pj.z, pi.z);
+            const R kx = floor_r(add_rn(mul_rn(rx, Li[0]), R(0.5)));
+            const R ky = floor_r(add_rn(mul_rn(ry, Li[1]), R(0.5)));
+            const R kz = floor_r(add_rn(mul_rn(rz, Li[2]), R(0.5)));
+            if (minimg) {
+              dx = sub_rn(rx, mul_rn(kx, L[0]));
+              dy = sub_rn(ry, mul_rn(ky, L[1]));
+              dz = sub_rn(rz, mul_rn(kz, L[2]));
+            } else {
+              dx = sub_rn(sub_rn(pj.x, mul_rn((R)rsx, L[0])), pi.x);
+              dy = sub_rn(sub_rn(pj.y, mul_rn((R)rsy, L[1])), pi.y);
+              dz = sub_rn(sub_rn(pj.z, mul_rn((R)rsz, L[2])), pi.z);
+            }
+            code = img_code((int)kx, (int)ky, (int)kz);
           }
           const R d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
           ok = (d2 < rl2) && (j != i);
-          code = img_code((int)kx, (int)ky, (int)kz);
         }
         const unsigned m = __ballot_sync(0xffffffffu, ok);
         if (ok) {
@@ -321,7 +370,6 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
         }
         n += __popc(m);
       }
-      }  // surviving runs of this group
     }
     if (lane == 0) {
       nnb[i] = n;
@@ -367,7 +415,7 @@ int nlist_build_impl(md_nlist* nl, md_system* sys, md_cell_list* cl, Recorder* r
   DevState* st = sys->st;
   int cap = nl->cap;
   dim3 grid(cl->ntot), block(256);
-  void* a[] = {&N, &sys->pos, &sys->rcut, &cl->start, &g, &st, &rl, &skin, &cap, &nl->list,
+  void* a[] = {&N, &sys->pos, &sys->rcut, &cl->start, &cl->zord, &g, &st, &rl, &skin, &cap, &nl->list,
                &nl->nnb, &nl->backup, &force_mi, &st, &gate};
   const void* f;
   size_t smem;

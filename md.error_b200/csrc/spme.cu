@@ -1356,8 +1356,16 @@ const double4a* spme_force_buffer(const md_spme* s) { return s->frec; }
 
 // energy and gradient: recompute the mesh and its transform, influence
 // multiply (energy, dE/dbeta, dE/dpsi), one inverse transform to Phi, gather
+__global__ void k_adj_out(const DevState* st, double* energy, double* dbeta) {
+  if (energy) *energy = st->scratch[0];
+  if (dbeta) *dbeta = st->scratch[1];
+}
+
+// dev = true: energy, dq, dr, dbeta are device pointers the results are left
+// in (no host copy, no wait); dpsi must then be NULL
 template <class R>
-static int spme_energy_grad(md_spme* s, double* energy, double* dq, double* dr, double* dbeta, double* dpsi) {
+static int spme_energy_grad(md_spme* s, double* energy, double* dq, double* dr, double* dbeta, double* dpsi,
+                            bool dev = false) {
   typedef typename C2<R>::T T2;
   md_system* sys = s->sys;
   cudaStream_t st_ = sys->stream;
@@ -1368,10 +1376,10 @@ static int spme_energy_grad(md_spme* s, double* energy, double* dq, double* dr, 
   // device outputs: dq [N], dr [N][3], dpsi [nhalf] (FP64, caller's atom order)
   const size_t nq = dq ? (size_t)sys->N : 0, nr = dr ? 3 * (size_t)sys->N : 0, np = dpsi ? s->nhalf : 0;
   double* d = nullptr;
-  if (nq + nr + np) MD_CUDA(cudaMallocAsync((void**)&d, sizeof(double) * (nq + nr + np), st_));
-  double* d_q = dq ? d : nullptr;
-  double* d_r = dr ? d + nq : nullptr;
-  double* d_p = dpsi ? d + nq + nr : nullptr;
+  if (!dev && nq + nr + np) MD_CUDA(cudaMallocAsync((void**)&d, sizeof(double) * (nq + nr + np), st_));
+  double* d_q = dev ? dq : (dq ? d : nullptr);
+  double* d_r = dev ? dr : (dr ? d + nq : nullptr);
+  double* d_p = dev ? nullptr : (dpsi ? d + nq + nr : nullptr);
   Recorder rec;
   rec.stream = st_;
   if (int r = influence_launch<R>(s, &rec)) return r;
@@ -1385,6 +1393,11 @@ static int spme_energy_grad(md_spme* s, double* energy, double* dq, double* dr, 
     if (int r = fft_launch<R>(s, &rec, Cp, Cp, 1, 1, +1, 1, 0)) return r;
     if (int r = fft_launch<R>(s, &rec, Cp, s->G, 2, 2, +1, 1, 0)) return r;
     if (int r = gather_launch<R>(s, &rec, 2, d_q, d_r, false)) return r;
+  }
+  if (dev) {
+    k_adj_out<<<1, 1, 0, st_>>>(sys->st, energy, dbeta);
+    MD_CHECK_LAUNCH("spme adjoint out");
+    return MD_OK;
   }
   double red[2];
   MD_CUDA(cudaMemcpyAsync(red, sys->st->scratch, sizeof(red), cudaMemcpyDeviceToHost, st_));
@@ -1453,6 +1466,15 @@ extern "C" int md_spme_apply(md_spme* s, md_system* sys, int with_stats) {
   Recorder rec;
   rec.stream = sys->stream;
   return spme_apply_impl(s, with_stats != 0, &rec);
+}
+
+// the same with DEVICE outputs (energy and dE_dbeta one double each, dE_dq [N],
+// dE_dr [N][3], caller's atom order), asynchronous on the system's stream
+extern "C" int md_spme_energy_grad_device(md_spme* s, md_system* sys, double* energy, double* dE_dq, double* dE_dr,
+                                          double* dE_dbeta) {
+  if (!s || !sys || sys != s->sys) { md_set_error("md_spme_energy_grad_device: bad arguments"); return MD_ERR_BADARG; }
+  return sys->prec == MD_PREC_FP64 ? spme_energy_grad<double>(s, energy, dE_dq, dE_dr, dE_dbeta, nullptr, true)
+                                   : spme_energy_grad<float>(s, energy, dE_dq, dE_dr, dE_dbeta, nullptr, true);
 }
 
 extern "C" int md_spme_energy_grad(md_spme* s, md_system* sys, double* energy, double* dE_dq, double* dE_dr,

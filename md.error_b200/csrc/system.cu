@@ -137,6 +137,20 @@ __global__ void k_set_vec(int N, int what, const double* in, const int* id,
   dst[k] = a;
 }
 
+// md_system_set_device_view: positions [N][3] and / or charges [N] from device
+// memory in the caller's atom order into the cell-ordered arrays
+template <class R>
+__global__ void k_set_view(int N, const double* __restrict__ pos, const double* __restrict__ q, const int* id,
+                           typename V4<R>::T* p4) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  const int o = id[k];
+  typename V4<R>::T a = p4[k];
+  if (pos) { a.x = (R)pos[3 * o]; a.y = (R)pos[3 * o + 1]; a.z = (R)pos[3 * o + 2]; }
+  if (q) a.w = (R)q[o];
+  p4[k] = a;
+}
+
 // charges live in the w component of the position array
 template <class R>
 __global__ void k_charge_io(int N, int dir, typename V4<R>::T* p4, const int* id, double* host_order) {
@@ -469,6 +483,21 @@ static int charge_io(md_system* s, int dir, double* q, int what = 0) {
   MD_CUDA(cudaFreeAsync(d, s->stream));
   MD_CUDA(cudaStreamSynchronize(s->stream));
   if (dir == 1) memcpy(q, s->h_stage, bytes);
+  return MD_OK;
+}
+
+// Zero-copy input from device tensors: no host copy, no wait; the caller's
+// stream must be the system's (md_system_set_stream) or be ordered with it.
+extern "C" int md_system_set_device_view(md_system* s, const md_device_view* v) {
+  if (int r = check_sys(s)) return r;
+  if (!v) return MD_ERR_BADARG;
+  if (!v->pos && !v->charge) return MD_OK;
+  const int nb = ceil_div(s->N, 256);
+  if (s->prec == MD_PREC_FP64)
+    k_set_view<double><<<nb, 256, 0, s->stream>>>(s->N, v->pos, v->charge, s->id, (double4a*)s->pos);
+  else
+    k_set_view<float><<<nb, 256, 0, s->stream>>>(s->N, v->pos, v->charge, s->id, (float4*)s->pos);
+  MD_CHECK_LAUNCH("device view");
   return MD_OK;
 }
 

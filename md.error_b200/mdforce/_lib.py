@@ -26,6 +26,11 @@ f64 = C.c_double
 P = C.POINTER
 
 
+class DeviceView(C.Structure):
+    """md_device_view: raw device pointers (caller's atom order)"""
+    _fields_ = [("pos", C.c_void_p), ("charge", C.c_void_p)]
+
+
 class LangevinParams(C.Structure):
     """md_langevin_params"""
     _fields_ = [("dt", f64), ("temperature", f64), ("gamma_t", f64),
@@ -111,6 +116,13 @@ _SIGS = {
     "md_spme_apply": (i32, [vp, vp, i32]),
     "md_spme_get_mesh": (i32, [vp, P(f64)]),
     "md_spme_energy_grad": (i32, [vp, vp, P(f64), P(f64), P(f64), P(f64), P(f64)]),
+    "md_spme_energy_grad_device": (i32, [vp, vp, vp, vp, vp, vp]),
+    "md_system_set_device_view": (i32, [vp, P(DeviceView)]),
+    "md_hspme_create": (i32, [P(vp), i32, P(i32), P(f64), f64, f64, i32, i32, i32]),
+    "md_hspme_destroy": (i32, [vp]),
+    "md_hspme_num_coeffs": (i32, [vp, P(i32)]),
+    "md_hspme_energy": (i32, [vp, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp]),
+    "md_hspme_force_error": (i32, [vp, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp]),
     "md_spme_get_influence": (i32, [vp, P(f64)]),
     "md_spme_self_correction": (i32, [vp, vp]),
     "md_system_set_charges": (i32, [vp, P(f64)]),

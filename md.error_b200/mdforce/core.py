@@ -204,6 +204,14 @@ class MDSystem:
         a = _f64(q).reshape(self.n)
         check(lib.md_system_set_charges(self.h, _p(a)), "set_charges")
 
+    def set_device_view(self, pos_ptr=None, charge_ptr=None):
+        """Positions [N,3] and/or charges [N] from device memory (raw pointers, e.g.
+        torch tensors' data_ptr(), caller's atom order), without a host copy
+        (md_system_set_device_view).  Asynchronous on the system's stream."""
+        from ._lib import DeviceView
+        v = DeviceView(pos_ptr or None, charge_ptr or None)
+        check(lib.md_system_set_device_view(self.h, C.byref(v)), "set_device_view")
+
     def set_masses(self, m):
         """Per-atom masses in original order (MDSystem hdata.mass)."""
         a = _f64(m).reshape(self.n)
@@ -452,6 +460,12 @@ class SPME:
         psi = np.empty((self.K[0], self.K[1], self.K[2] // 2 + 1), np.float64)
         check(lib.md_spme_get_influence(self.h, _p(psi)), "influence")
         return psi
+
+    def energy_grad_device(self, energy_ptr, dq_ptr=None, dr_ptr=None, dbeta_ptr=None):
+        """md_spme_energy_grad with outputs in device memory (raw pointers; energy and
+        dE/dbeta one double each, dE/dq [N], dE/dr [N,3]); no host copy, no wait."""
+        check(lib.md_spme_energy_grad_device(self.h, self.sys.h, energy_ptr, dq_ptr, dr_ptr, dbeta_ptr),
+              "SPME::energy_grad_device")
 
     def energy_grad(self, dq=True, dr=True, dpsi=False):
         """Reciprocal energy and its exact gradient (md_spme_energy_grad):

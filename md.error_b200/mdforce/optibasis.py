@@ -151,42 +151,169 @@ def ik_error_loss(coeffs, functional):
 def spme_energy(q, r, spme, recompute=False):
     """Reciprocal SPME energy of charges q [N] at positions r [N, 3] (float64
     tensors), differentiable in both through the hand-written adjoint
-    (md_spme_energy_grad).  The system of `spme` takes q and r on every call.
-    With recompute=True the forward keeps nothing but the inputs and the
-    backward recomputes spread, transforms and gather (memory-lean); by
-    default the gradient comes with the forward pass and is kept for the
-    backward."""
+    (md_spme_energy_grad).  The system of `spme` takes q and r on every call:
+    CUDA tensors are handed over as raw device pointers on torch's current
+    stream (md_system_set_device_view, md_spme_energy_grad_device: no host
+    copy, no wait); CPU tensors go through host arrays.  With recompute=True
+    the forward keeps nothing but the inputs and the backward recomputes
+    spread, transforms and gather (memory-lean); by default the gradient comes
+    with the forward pass and is kept for the backward."""
     torch = _torch()
     sys_ = spme.sys
 
     def run(qq, rr, grads):
-        sys_.set_charges(qq.detach().cpu().numpy())
-        sys_.set_positions(rr.detach().cpu().numpy())
-        return spme.energy_grad(dq=grads, dr=grads)
+        if qq.is_cuda:
+            qd = qq.detach().to(torch.float64).contiguous()
+            rd = rr.detach().to(torch.float64).contiguous()
+            sys_.set_stream(torch.cuda.current_stream(qd.device).cuda_stream)
+            sys_.set_device_view(rd.data_ptr(), qd.data_ptr())
+            e = torch.empty(2, dtype=torch.float64, device=qd.device)
+            gq = torch.empty_like(qd) if grads else None
+            gr = torch.empty_like(rd) if grads else None
+            spme.energy_grad_device(e.data_ptr(), gq.data_ptr() if grads else None,
+                                    gr.data_ptr() if grads else None, e[1:].data_ptr())
+            return e[0], gq, gr
+        sys_.set_charges(qq.detach().numpy())
+        sys_.set_positions(rr.detach().numpy())
+        out = spme.energy_grad(dq=grads, dr=grads)
+        e = torch.tensor(out["energy"], dtype=torch.float64)
+        if not grads:
+            return e, None, None
+        return e, torch.from_numpy(out["dE_dq"]), torch.from_numpy(out["dE_dr"])
 
     class _SPMEEnergy(torch.autograd.Function):
         @staticmethod
         def forward(ctx, qq, rr):
-            out = run(qq, rr, not recompute)
+            e, gq, gr = run(qq, rr, not recompute)
             if recompute:
                 ctx.save_for_backward(qq, rr)
             else:
-                ctx.save_for_backward(torch.from_numpy(out["dE_dq"]), torch.from_numpy(out["dE_dr"]))
-            ctx.dev = qq.device
-            return torch.tensor(out["energy"], dtype=torch.float64, device=qq.device)
+                ctx.save_for_backward(gq, gr)
+            return e
 
         @staticmethod
         def backward(ctx, g):
             a, b = ctx.saved_tensors
             if recompute:
-                out = run(a, b, True)
-                gq, gr = torch.from_numpy(out["dE_dq"]), torch.from_numpy(out["dE_dr"])
+                _, gq, gr = run(a, b, True)
             else:
                 gq, gr = a, b
-            gc = g.detach().to("cpu", torch.float64)
-            return (gc * gq).to(ctx.dev), (gc * gr).to(ctx.dev)
+            return (g * gq).to(gq.dtype), (g * gr).to(gr.dtype)
 
     return _SPMEEnergy.apply(q, r)
+
+
+class HermiteSPME:
+    """ik-SPME whose interpolation basis is the piecewise cubic Hermite basis of
+    optiBasis (coefficients [v_1..v_n, d_1..d_n] as HermiteLossFunc(_Bound0)),
+    for natoms charges on mesh K in box L with splitting beta, on the GPU in
+    FP64 (md_hspme_*).  Inputs and outputs are CUDA float64 tensors handed over
+    as raw device pointers on torch's current stream."""
+
+    def __init__(self, natoms, K, L, beta, CC, nbin, bound0=False, device=0):
+        K = [int(k) for k in (K if np.ndim(K) else [K] * 3)]
+        L = _box_of(L)
+        h = C.c_void_p()
+        check(lib.md_hspme_create(C.byref(h), int(natoms), (C.c_int * 3)(*K), (C.c_double * 3)(*L), float(beta),
+                                  float(CC), int(nbin), 1 if bound0 else 0, int(device)), "md_hspme_create")
+        self.h = h
+        self.natoms, self.K, self.L = int(natoms), K, L
+        n = C.c_int()
+        check(lib.md_hspme_num_coeffs(self.h, C.byref(n)), "md_hspme_num_coeffs")
+        self.ncoef = n.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.md_hspme_destroy(self.h)
+            self.h = None
+
+    @staticmethod
+    def _ptr(t):
+        return None if t is None else t.data_ptr()
+
+    def energy(self, q, r, coeffs, forces=False, grads=False):
+        """energy [C] (coeffs [C, ncoef] or [ncoef]) and, as asked, ik forces
+        [C, N, 3] and the gradients dE/dq [C, N], dE/dr [C, N, 3], dE/dc [C, ncoef]."""
+        torch = _torch()
+        c = coeffs.detach().reshape(-1, self.ncoef).to(torch.float64).contiguous()
+        q = q.detach().to(torch.float64).contiguous()
+        r = r.detach().to(torch.float64).contiguous()
+        nc, n, dev = c.shape[0], self.natoms, c.device
+        e = torch.empty(nc, dtype=torch.float64, device=dev)
+        F = torch.empty(nc, n, 3, dtype=torch.float64, device=dev) if forces else None
+        gq = torch.empty(nc, n, dtype=torch.float64, device=dev) if grads else None
+        gr = torch.empty(nc, n, 3, dtype=torch.float64, device=dev) if grads else None
+        gc = torch.empty(nc, self.ncoef, dtype=torch.float64, device=dev) if grads else None
+        P = self._ptr
+        check(lib.md_hspme_energy(self.h, P(q), P(r), P(c), nc, P(e), P(F), P(gq), P(gr), P(gc),
+                                  torch.cuda.current_stream(dev).cuda_stream), "md_hspme_energy")
+        return {"energy": e, "forces": F, "dE_dq": gq, "dE_dr": gr, "dE_dc": gc}
+
+    def force_error(self, q, r, coeffs, fref, grads=True):
+        """L [C] = 1/N sum_i |F_i - fref_i|^2 of the ik forces against fref [N, 3] and,
+        with grads, dL/dq [C, N], dL/dr [C, N, 3], dL/dc [C, ncoef]."""
+        torch = _torch()
+        c = coeffs.detach().reshape(-1, self.ncoef).to(torch.float64).contiguous()
+        q = q.detach().to(torch.float64).contiguous()
+        r = r.detach().to(torch.float64).contiguous()
+        f = fref.detach().to(torch.float64).contiguous()
+        nc, n, dev = c.shape[0], self.natoms, c.device
+        loss = torch.empty(nc, dtype=torch.float64, device=dev)
+        gq = torch.empty(nc, n, dtype=torch.float64, device=dev) if grads else None
+        gr = torch.empty(nc, n, 3, dtype=torch.float64, device=dev) if grads else None
+        gc = torch.empty(nc, self.ncoef, dtype=torch.float64, device=dev) if grads else None
+        P = self._ptr
+        check(lib.md_hspme_force_error(self.h, P(q), P(r), P(c), nc, P(f), P(loss), P(gq), P(gr), P(gc),
+                                       torch.cuda.current_stream(dev).cuda_stream), "md_hspme_force_error")
+        return {"loss": loss, "dL_dq": gq, "dL_dr": gr, "dL_dc": gc}
+
+
+def hermite_spme_energy(q, r, coeffs, hspme):
+    """Reciprocal energies [C] of the candidate bases coeffs [C, ncoef], as a
+    torch.autograd.Function differentiable in q [N], r [N, 3] and coeffs (the
+    gradients come from the hand-written adjoint in the same pass)."""
+    torch = _torch()
+
+    class _E(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, qq, rr, cc):
+            out = hspme.energy(qq, rr, cc, grads=True)
+            ctx.save_for_backward(out["dE_dq"], out["dE_dr"], out["dE_dc"])
+            ctx.cshape = cc.shape
+            return out["energy"]
+
+        @staticmethod
+        def backward(ctx, g):
+            gq, gr, gc = ctx.saved_tensors
+            g = g.reshape(-1)
+            return ((g[:, None] * gq).sum(0), (g[:, None, None] * gr).sum(0),
+                    (g[:, None] * gc).reshape(ctx.cshape))
+
+    return _E.apply(q, r, coeffs)
+
+
+def hermite_spme_force_error(q, r, coeffs, fref, hspme):
+    """Force-error functional [C] (1/N sum |F_ik - fref|^2 per candidate) as a
+    torch.autograd.Function differentiable in q, r and coeffs (second adjoint of
+    the SPME chain, md_hspme_force_error); fref is a constant."""
+    torch = _torch()
+
+    class _L(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, qq, rr, cc):
+            out = hspme.force_error(qq, rr, cc, fref, grads=True)
+            ctx.save_for_backward(out["dL_dq"], out["dL_dr"], out["dL_dc"])
+            ctx.cshape = cc.shape
+            return out["loss"]
+
+        @staticmethod
+        def backward(ctx, g):
+            gq, gr, gc = ctx.saved_tensors
+            g = g.reshape(-1)
+            return ((g[:, None] * gq).sum(0), (g[:, None, None] * gr).sum(0),
+                    (g[:, None] * gc).reshape(ctx.cshape))
+
+    return _L.apply(q, r, coeffs)
 
 
 def bspline_initial_basis(CC, nbin, order, bound0=False):

@@ -113,6 +113,31 @@ def test_autograd_function(mdf, small):
         assert rel(rt.grad.numpy(), 3.0 * ref["dE_dr"]) < 1e-13
 
 
+def test_autograd_function_device_tensors(mdf, small):
+    """CUDA tensors go to the system as raw device pointers and the gradients
+    come back in device memory (md_system_set_device_view,
+    md_spme_energy_grad_device): the same values as the host path."""
+    import torch
+    from mdforce.optibasis import spme_energy
+    pos, q, box = small
+    sys, sp = make(mdf, pos, q, box)
+    ref = sp.energy_grad()
+    for recompute in (False, True):
+        qt = torch.tensor(q, dtype=torch.float64, device="cuda", requires_grad=True)
+        rt = torch.tensor(pos, dtype=torch.float64, device="cuda", requires_grad=True)
+        E = spme_energy(qt, rt, sp, recompute=recompute)
+        assert E.is_cuda
+        (3.0 * E).backward()
+        assert abs(E.item() - ref["energy"]) < 1e-13 * abs(ref["energy"])
+        assert rel(qt.grad.cpu().numpy(), 3.0 * ref["dE_dq"]) < 1e-13
+        assert rel(rt.grad.cpu().numpy(), 3.0 * ref["dE_dr"]) < 1e-13
+    # moved positions reach the system through the view
+    rt = torch.tensor(pos + 0.01, dtype=torch.float64, device="cuda")
+    E2 = spme_energy(torch.tensor(q, dtype=torch.float64, device="cuda"), rt, sp)
+    sys.set_positions(pos + 0.01)
+    assert abs(E2.item() - sp.energy_grad(dq=False, dr=False)["energy"]) < 1e-13 * abs(E2.item())
+
+
 def test_autograd_gradcheck(mdf):
     import torch
     from mdforce.optibasis import spme_energy
