@@ -265,7 +265,11 @@ def time_kernels(torch, mdf, sys_, eng, stream, reps=50):
             y.record(stream)
     torch.cuda.synchronize()
     t_nl = sum(x.elapsed_time(y) for x, y in ev) / 1e3 / len(ev)
-    return t_lj, P, t_nl
+    del nl, cl
+    # entries within rc_i (the pairs that interact): a list with zero skin
+    cl0, nl0 = fitted_list(mdf, sys_, skin=0.0)
+    c0, _ = nl0.lists()
+    return t_lj, P, t_nl, int(c0.sum())
 
 
 def start_forces(mdf, s, prec):
@@ -724,12 +728,13 @@ def main():
         sim_d.run(args.warmup)
         t64 = time_steps(torch, sim_d, stream, args.steps, flush)
         fp64_sps = args.steps / t64
-        t_lj64, _, t_nl64 = time_kernels(torch, mdf, sys_d, eng_d, stream)
+        t_lj64, _, t_nl64, _ = time_kernels(torch, mdf, sys_d, eng_d, stream)
         del sim_d, eng_d, sys_d
 
     # ---- dominant kernel: LJ forces, algorithmic bytes / CUDA-event duration
-    t_lj, P, t_nl = time_kernels(torch, mdf, sys_m, eng_m, stream)
+    t_lj, P, t_nl, P_rc = time_kernels(torch, mdf, sys_m, eng_m, stream)
     alg_bytes = N * 16 + N * 4 + P * 4 + N * 24  # positions, rcut, list indices, FP64 forces
+    alg_bytes_rc = N * 16 + N * 4 + P_rc * 4 + N * 24  # the same with the interacting pairs only
     peak, peak_kind = measured_peak_hbm()
     achieved = alg_bytes / t_lj / 1e9
 
@@ -785,13 +790,13 @@ def main():
     del sim_e, arc_e, eng_e, sys_e
 
     # step1, LJ, step2 every step; bin, scan, scatter, order, gather, copy back,
-    # list build per rebuild; the density deposit every 40 steps and 3 + 3*3 DFT
-    # passes + 7 element-wise kernels per cutoff update (every 2000 steps) --
-    # neither falls in a timed range shorter than 40 steps after the warm-up
+    # z order, list build per rebuild; the density deposit every 40 steps and
+    # 3 + 3*3 DFT passes + 7 element-wise kernels per cutoff update (every 2000
+    # steps)
     first, last = steps0, steps0 + args.steps
     n_updates = last // UPDATE_EVERY - first // UPDATE_EVERY
     n_deposits = last // SAMPLE_EVERY - first // SAMPLE_EVERY
-    rebuild_launches = 7 * (rebuilds_timed if use_graph else args.steps)
+    rebuild_launches = 8 * (rebuilds_timed if use_graph else args.steps)
     launches = 3 * args.steps + rebuild_launches + n_deposits + 22 * n_updates
     cpu = loop = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -834,6 +839,8 @@ def main():
                          "frac": achieved / peak, "traffic": profiled_traffic("k_lj_mixed"),
                          "kernel": "k_lj_mixed",
                          "kernel_us": t_lj * 1e6, "alg_bytes": alg_bytes, "list_entries": P,
+                         "pairs_within_rc": P_rc, "alg_bytes_within_rc": alg_bytes_rc,
+                         "frac_within_rc": alg_bytes_rc / t_lj / 1e9 / peak,
                          "peak_kind": peak_kind},
             "kernel_us": {"lj_mixed": t_lj * 1e6, "lj_fp64": None if t_lj64 is None else t_lj64 * 1e6,
                           "nlist_build_mixed": t_nl * 1e6,
