@@ -91,43 +91,50 @@ __global__ void k_bin(int N, typename V4<R>::T* pos, int4* image, DevState* st, 
 // zeroes count for the next rebuild
 __global__ void __launch_bounds__(1024) k_scan(int n, uint32_t* count, uint32_t* start, DevState* st, int gate) {
   if (gate && !(st->flags & FLAG_REBUILD)) return;
+  // exclusive scan of the cell counts (and their reset) in tiles of 4T cells:
+  // thread t of a tile holds cells 4t..4t+3, so each warp reads and writes
+  // 512 contiguous bytes; the running total carries from tile to tile
   __shared__ uint32_t wsum[32];
   const int T = blockDim.x;
-  const int chunk = (n + T - 1) / T;
-  const int b = threadIdx.x * chunk;
-  const int e = min(n, b + chunk);
-  uint32_t tot = 0;
-  for (int i = b; i < e; ++i) tot += count[i];
-  // exclusive block scan of the per-thread totals
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  uint32_t x = tot;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = T >> 5;
+  uint32_t carry = 0;
+  for (int base = 0; base < n; base += 4 * T) {
+    const int i0 = base + 4 * threadIdx.x;
+    uint32_t v[4];
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) wsum[wid] = x;
-  __syncthreads();
-  if (wid == 0) {
-    uint32_t w = (lane < (T >> 5)) ? wsum[lane] : 0u;
+    for (int k = 0; k < 4; ++k) v[k] = (i0 + k < n) ? count[i0 + k] : 0u;
+    const uint32_t tot = v[0] + v[1] + v[2] + v[3];
+    uint32_t x = tot;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += y;
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
     }
-    wsum[lane] = w;
+    if (lane == 31) wsum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      uint32_t w = lane < nw ? wsum[lane] : 0u;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      wsum[lane] = w;
+    }
+    __syncthreads();
+    uint32_t run = carry + (wid > 0 ? wsum[wid - 1] : 0u) + x - tot;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (i0 + k < n) {
+        start[i0 + k] = run;
+        count[i0 + k] = 0u;
+      }
+      run += v[k];
+    }
+    carry += wsum[nw - 1];
+    __syncthreads();  // wsum is rewritten by the next tile
   }
-  __syncthreads();
-  uint32_t run = (wid > 0 ? wsum[wid - 1] : 0u) + x - tot;
-  for (int i = b; i < e; ++i) {
-    const uint32_t v = count[i];
-    start[i] = run;
-    count[i] = 0u;
-    run += v;
-  }
-  if (threadIdx.x == T - 1) start[n] = run;
-  // the thread owning the last chunk may be before T-1 when n < T*chunk
-  if (e == n && b < e) start[n] = run;
+  if (threadIdx.x == 0) start[n] = carry;
 }
 
 __global__ void k_scatter(int N, const uint32_t* t_cell, const uint32_t* slot, const uint32_t* start,

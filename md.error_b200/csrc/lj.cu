@@ -12,7 +12,11 @@
 // shuffles, the atom force is accumulated in FP64.  Energy and the diagonal
 // virial (1/2 sum over the full list, as the reference's per-atom buffers)
 // are block-reduced in FP64 and finished by the last block in a fixed order.
+// The plain LJ case (one type, no charges) runs its pair arithmetic branch
+// free, two entries per packed binary32 (f32x2) instruction, with the same
+// binary32 criterion.
 #include <cmath>
+#include <type_traits>
 #include <vector>
 #include "device_common.cuh"
 
@@ -25,11 +29,12 @@ struct LJParams {
 };
 
 // Build options of the mixed kernel (defaults are the measured best):
-//   MD_LJ_PREFETCH  1: load the next list line while the current one is processed
+//   MD_LJ_PREFETCH  1: the plain LJ pass loads the next list line while the
+//                   current one is processed
 //   MD_LJ_ACC       0: per-lane Kahan-compensated FP32 sums of the per-pass batch
 //                      sums; 1: the batch sums added in FP64
 #ifndef MD_LJ_PREFETCH
-#define MD_LJ_PREFETCH 0
+#define MD_LJ_PREFETCH 1
 #endif
 #ifndef MD_LJ_ACC
 #define MD_LJ_ACC 1
@@ -39,6 +44,11 @@ struct LJParams {
 //                   (each list line is read once per step)
 #ifndef MD_LJ_LISTLD
 #define MD_LJ_LISTLD 2
+#endif
+//   MD_LJ_PACKED    1: plain LJ (no charges, one type) through the branch-free
+//                   pass with packed binary32 pair arithmetic
+#ifndef MD_LJ_PACKED
+#define MD_LJ_PACKED 1
 #endif
 
 __device__ __forceinline__ int4 load_list4(const int4* p) {
@@ -269,8 +279,139 @@ __device__ __forceinline__ void lj_pass_mixed(const int4 e4, int nvalid, const f
   a.fz.add(bz);
 }
 
+// Packed binary32 pairs (sm_100 f32x2): one instruction applies the same
+// round-to-nearest binary32 operation to both halves, so every half equals
+// the scalar .rn result.
+struct F2 {
+  unsigned long long v;
+};
+__device__ __forceinline__ F2 f2(float lo, float hi) {
+  F2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2_split(F2 a, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a.v));
+}
+__device__ __forceinline__ F2 f2_sub(F2 a, F2 b) {
+  F2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 f2_mul(F2 a, F2 b) {
+  F2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 f2_fma(F2 a, F2 b, F2 c) {
+  F2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return r;
+}
+
+// Accumulators of the packed pass: energy as (pair, pair) halves without the
+// shift, which is added once per interacting pair at the end (cnt); virial
+// (xx, yy) packed and zz.
+struct PackedAcc {
+  Kahan fx, fy, fz;
+  F2 e2 = {0ull}, vxy = {0ull};
+  float vz = 0.f;
+  int cnt = 0;
+};
+
+__device__ __forceinline__ void acc_stats(const MixedAcc& a, const LJParams&, float& e, float& vx, float& vy,
+                                          float& vz, float& ec) {
+  e = a.e; vx = a.vx; vy = a.vy; vz = a.vz; ec = a.ec;
+}
+__device__ __forceinline__ void acc_stats(const PackedAcc& a, const LJParams& p, float& e, float& vx, float& vy,
+                                          float& vz, float& ec) {
+  float e0, e1;
+  f2_split(a.e2, e0, e1);
+  e = fmaf((float)a.cnt, p.shiftf, e0 + e1);
+  f2_split(a.vxy, vx, vy);
+  vz = a.vz;
+  ec = 0.f;
+}
+
+// Plain LJ 6-12 (no charges, one type) over the 4 entries of a pass, branch
+// free: the criterion is the binary32 |d|^2 < rc_i^2 of lj_pass_mixed
+// ((x_j - x_i) - k L per axis, (dx^2 + dy^2) + dz^2), computed with x and y
+// packed; entries beyond rc_i (and past the row's end) continue with
+// r^2 = 1e30, where s^6 = (sigma^2/r^2)^3 underflows to 0 and the pair adds
+// exactly zero force, virial and energy.  The pair arithmetic of entries
+// (0, 1) and (2, 3) runs packed.
+template <bool TAIL, bool STATS>
+__device__ __forceinline__ void lj_pass_packed(const int4 e4, int nvalid, const float4* __restrict__ pos, int i,
+                                               const float4& pi, float rc2, const float4* shift,
+                                               const LJParams& p, PackedAcc& a) {
+  int ee[4] = {e4.x, e4.y, e4.z, e4.w};
+  if (TAIL) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) ee[u] = 8 * u < nvalid ? ee[u] : -1;
+  }
+  float4 pj[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) pj[u] = __ldg(pos + ((!TAIL || ee[u] != -1) ? (ee[u] & 0x03FFFFFF) : i));
+  const F2 pxy = f2(pi.x, pi.y);
+  const F2 sig2 = f2(p.sig2f, p.sig2f), eps4 = f2(p.eps4f, p.eps4f);
+  const F2 m12 = f2(-12.f, -12.f), six = f2(6.f, 6.f), mone = f2(-1.f, -1.f);
+  float bx = 0.f, bz = 0.f, by = 0.f;
+  F2 bxy = f2(0.f, 0.f);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    F2 dxy[2];
+    float dz[2], r2m[2];
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const int u = 2 * h + v;
+      const float4 sh = shift[(unsigned)ee[u] >> 26];
+      dxy[v] = f2_sub(f2_sub(f2(pj[u].x, pj[u].y), pxy), f2(sh.x, sh.y));
+      dz[v] = __fsub_rn(__fsub_rn(pj[u].z, pi.z), sh.z);
+      float sx, sy;
+      f2_split(f2_mul(dxy[v], dxy[v]), sx, sy);
+      const float r2 = __fadd_rn(__fadd_rn(sx, sy), __fmul_rn(dz[v], dz[v]));
+      const bool in = (!TAIL || ee[u] != -1) && r2 < rc2;
+      r2m[v] = in ? r2 : 1e30f;
+      if (STATS) a.cnt += in ? 1 : 0;
+    }
+    const F2 ri2 = f2(__fdividef(1.0f, r2m[0]), __fdividef(1.0f, r2m[1]));
+    const F2 s2 = f2_mul(sig2, ri2);
+    const F2 s6 = f2_mul(f2_mul(s2, s2), s2);
+    // 4 eps (6 s^6 - 12 s^12) / r^2 = (4 eps / r^2) s^6 (6 - 12 s^6)
+    const F2 fs = f2_mul(f2_mul(f2_mul(eps4, ri2), s6), f2_fma(m12, s6, six));
+    float fs0, fs1;
+    f2_split(fs, fs0, fs1);
+    bxy = f2_fma(f2(fs0, fs0), dxy[0], bxy);
+    bz = fmaf(fs0, dz[0], bz);
+    bxy = f2_fma(f2(fs1, fs1), dxy[1], bxy);
+    bz = fmaf(fs1, dz[1], bz);
+    if (STATS) {
+      // 4 eps (s^12 - s^6); the shift is added per interacting pair at the end;
+      // (dx^2, dy^2) recomputed rather than kept live
+      a.e2 = f2_fma(eps4, f2_fma(s6, s6, f2_mul(s6, mone)), a.e2);
+      a.vxy = f2_fma(f2(fs0, fs0), f2_mul(dxy[0], dxy[0]), a.vxy);
+      a.vz = fmaf(fs0, __fmul_rn(dz[0], dz[0]), a.vz);
+      a.vxy = f2_fma(f2(fs1, fs1), f2_mul(dxy[1], dxy[1]), a.vxy);
+      a.vz = fmaf(fs1, __fmul_rn(dz[1], dz[1]), a.vz);
+    }
+  }
+  f2_split(bxy, bx, by);
+  a.fx.add(bx);
+  a.fy.add(by);
+  a.fz.add(bz);
+}
+
+// threads per block of the non-bonded kernels, and the resident 256-thread
+// blocks per SM the plain mixed kernel is compiled for (its register cap)
+#ifndef MD_LJ_THREADS
+#define MD_LJ_THREADS 256
+#endif
+#ifndef MD_LJ_MINB
+#define MD_LJ_MINB 4
+#endif
+
 template <int G, bool STATS, bool COUL, bool TYPES>
-__global__ void __launch_bounds__(256, (COUL || TYPES) ? 4 : 5)
+__global__ void __launch_bounds__(MD_LJ_THREADS, ((COUL || TYPES) ? 4 : MD_LJ_MINB) * 256 / MD_LJ_THREADS)
 k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut,
            const int* __restrict__ list, const int* __restrict__ nnb, int cap,
            const DevState* __restrict__ st, LJParams p, double4a* __restrict__ force, int overwrite,
@@ -291,7 +432,8 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
   if (TYPES)
     for (int c = threadIdx.x; c < 3 * nt * nt; c += blockDim.x) tab[c] = reinterpret_cast<const float4*>(ptab)[c];
   __syncthreads();
-  MixedAcc a;
+  constexpr bool PACK = MD_LJ_PACKED && !COUL && !TYPES;
+  typename std::conditional<PACK, PackedAcc, MixedAcc>::type a;
   if (i < N) {
     const float4 pi = pos[i];
     const float4* trow = TYPES ? tab + 3 * nt * (int)type[i] : tab;
@@ -303,33 +445,36 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
     // transposed line layout (nl_slot) the vector of lane l holds logical
     // entries 32q + l + 8u, u = 0..3, so for each u the 8 lanes gather 8
     // consecutive neighbours.  Rows hold whole lines (cap is a multiple of
-    // 32), so every vector read stays inside the row.  The next pass's vector
-    // is loaded before the current one is processed.
+    // 32), so every vector read stays inside the row.
     static_assert(G * 4 == 32, "8 lanes x 4 entries per pass");
     const int4* row4 = reinterpret_cast<const int4*>(list + (size_t)i * cap);
     const int npass = (n + 31) >> 5;
-    if (npass > 0) {
-#if MD_LJ_PREFETCH
-      int4 cur = load_list4(row4 + lane);
-#endif
-      for (int q = 0; q < npass; ++q) {
-#if MD_LJ_PREFETCH
-        int4 nxt = cur;
+    // plain LJ: the next pass's vector is loaded before the current pass is
+    // processed (the list comes from DRAM, the positions mostly from L1)
+    constexpr bool PF = MD_LJ_PREFETCH && PACK;
+    int4 nxt = make_int4(0, 0, 0, 0);
+    if (PF && npass > 0) nxt = load_list4(row4 + lane);
+    for (int q = 0; q < npass; ++q) {
+      int4 cur;
+      if constexpr (PF) {
+        cur = nxt;
         if (q + 1 < npass) nxt = load_list4(row4 + (q + 1) * G + lane);
-#else
-        const int4 cur = load_list4(row4 + q * G + lane);
-#endif
-        const int rem = n - (32 * q + lane);  // entry u is inside the row when 8u < rem
+      } else {
+        cur = load_list4(row4 + q * G + lane);
+      }
+      const int rem = n - (32 * q + lane);  // entry u is inside the row when 8u < rem
+      if constexpr (PACK) {
+        if (rem > 24) lj_pass_packed<false, STATS>(cur, rem, pos, i, pi, rc2, shift, p, a);
+        else if (rem > 0) lj_pass_packed<true, STATS>(cur, rem, pos, i, pi, rc2, shift, p, a);
+      } else {
         if (rem > 24) lj_pass_mixed<4, false, STATS, COUL, TYPES>(cur, rem, pos, i, pi, rc2, shift, p, a, type, trow);
         else if (rem > 0) lj_pass_mixed<4, true, STATS, COUL, TYPES>(cur, rem, pos, i, pi, rc2, shift, p, a, type, trow);
-#if MD_LJ_PREFETCH
-        cur = nxt;
-#endif
       }
     }
   }
   Kahan& fx = a.fx; Kahan& fy = a.fy; Kahan& fz = a.fz;
-  const float e = a.e, vx = a.vx, vy = a.vy, vz = a.vz, ec = a.ec;
+  float e, vx, vy, vz, ec;
+  acc_stats(a, p, e, vx, vy, vz, ec);
   double Fx = group_sum<G>(fx.value()), Fy = group_sum<G>(fy.value()), Fz = group_sum<G>(fz.value());
   if (i < N && lane == 0) {
     double4a f = overwrite ? double4a{0, 0, 0, 0} : force[i];
@@ -499,7 +644,7 @@ int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats,
   int cap = nl->cap;
   if (cap % 32 != 0) { md_set_error("neighbour-list capacity %d is not a multiple of 32", cap); return MD_ERR_BADARG; }
   int ow = overwrite ? 1 : 0;
-  const int threads = 256;
+  const int threads = MD_LJ_THREADS;
   dim3 grid(ceil_div((long long)N * kLanes, threads));
   if ((int)grid.x > sys->max_partial_blocks) { md_set_error("partials buffer too small"); return MD_ERR_BADARG; }
   DevState* st = sys->st;

@@ -214,6 +214,10 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
   __syncthreads();
   const bool glob = !stage;
   const unsigned ltmask = (1u << lane) - 1u;
+  const unsigned lemask = (2u << lane) - 1u;  // lanes 0..lane (all 32 for lane 31)
+  // per-warp table of the current run group's non-empty runs (rank order)
+  __shared__ int wdelta[8][32];
+  __shared__ T4 wshift[8][32];
   // When the stencil spans less than the box along every axis, each cell
   // appears in exactly one run, at that run's periodic image k_run, and
   // 2 rlist < L.  For any pair within rlist the reference's image
@@ -302,9 +306,12 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
       }
       // the candidate ranges of the surviving runs, packed end to end into
       // 32-lane chunks: lane l of a chunk takes candidate c = t0 + l, owned by
-      // the last run whose range starts at or before c (found by a 5-step
-      // search over the warp's exclusive prefix sums; an empty range never
-      // owns a candidate)
+      // the last non-empty run whose range starts at or before c.  The
+      // non-empty runs are compacted (in run order) into the warp's table:
+      // the offset taking c to its tile (or zord) index, and the run's image
+      // shift k L with its code.  Within a chunk the owner's rank is the number
+      // of non-empty runs starting before the chunk plus those starting inside
+      // it at or before c (a 32-bit start mask).
       const int len = keep ? tel - tbl : 0;
       int incl = len;
 #pragma unroll
@@ -314,36 +321,44 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
       }
       const int total = __shfl_sync(0xffffffffu, incl, 31);
       const int excl = incl - len;
+      const bool ne = len > 0;
+      const unsigned nem = __ballot_sync(0xffffffffu, ne);
+      __syncwarp();  // the previous group's table has been read
+      if (ne) {
+        const int r = rb + lane;
+        const int k = __popc(nem & ltmask);
+        wdelta[warp][k] = (glob ? rt.jb[r] : rt.off[r]) + tbl - excl;
+        const int rsx = rt.sx[r], rsy = rt.sy[r], rsz = rt.sz[r];
+        wshift[warp][k] = T4{mul_rn((R)rsx, L[0]), mul_rn((R)rsy, L[1]), mul_rn((R)rsz, L[2]),
+                             slot_as_w<R>(img_code(rsx, rsy, rsz))};
+      }
+      __syncwarp();
+      int before = 0;  // non-empty runs starting before the chunk
       for (int t0 = 0; t0 < total; t0 += 32) {
         const int cidx = t0 + lane;
-        int own = 0;
-#pragma unroll
-        for (int step = 16; step > 0; step >>= 1) {
-          const int e = __shfl_sync(0xffffffffu, excl, own + step < 32 ? own + step : 31);
-          if (own + step < 32 && e <= cidx) own += step;
-        }
-        const int oexcl = __shfl_sync(0xffffffffu, excl, own);
-        const int otb = __shfl_sync(0xffffffffu, tbl, own);
+        const unsigned smask =
+            __reduce_or_sync(0xffffffffu, (ne && excl >= t0 && excl < t0 + 32) ? (1u << (excl - t0)) : 0u);
+        const int k = before + __popc(smask & lemask) - 1;
+        before += __popc(smask);
         bool ok = false;
         int j = 0, code = 0;
         if (cidx < total) {
-          const int r = rb + own;
-          const int rjb = rt.jb[r], roff = rt.off[r], rsx = rt.sx[r], rsy = rt.sy[r], rsz = rt.sz[r];
-          const int t = otb + (cidx - oexcl);
+          const int x = cidx + wdelta[warp][k];
           T4 pj;
           if (glob) {
-            j = (int)zord[rjb + t];
+            j = (int)zord[x];
             pj = pos[j];
           } else {
-            pj = tile[roff + t];
+            pj = tile[x];
             j = slot_of_w<R>(pj.w);
           }
+          const T4 sh = wshift[warp][k];
           R dx, dy, dz;
           if (runshift) {
-            dx = sub_rn(sub_rn(pj.x, pi.x), mul_rn((R)rsx, L[0]));
-            dy = sub_rn(sub_rn(pj.y, pi.y), mul_rn((R)rsy, L[1]));
-            dz = sub_rn(sub_rn(pj.z, pi.z), mul_rn((R)rsz, L[2]));
-            code = img_code(rsx, rsy, rsz);
+            dx = sub_rn(sub_rn(pj.x, pi.x), sh.x);
+            dy = sub_rn(sub_rn(pj.y, pi.y), sh.y);
+            dz = sub_rn(sub_rn(pj.z, pi.z), sh.z);
+            code = slot_of_w<R>(sh.w);
           } else {
             const R rx = sub_rn(pj.x, pi.x), ry = sub_rn(pj.y, pi.y), rz = sub_rn(pj.z, pi.z);
             const R kx = floor_r(add_rn(mul_rn(rx, Li[0]), R(0.5)));
@@ -354,9 +369,9 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
               dy = sub_rn(ry, mul_rn(ky, L[1]));
               dz = sub_rn(rz, mul_rn(kz, L[2]));
             } else {
-              dx = sub_rn(sub_rn(pj.x, mul_rn((R)rsx, L[0])), pi.x);
-              dy = sub_rn(sub_rn(pj.y, mul_rn((R)rsy, L[1])), pi.y);
-              dz = sub_rn(sub_rn(pj.z, mul_rn((R)rsz, L[2])), pi.z);
+              dx = sub_rn(sub_rn(pj.x, sh.x), pi.x);
+              dy = sub_rn(sub_rn(pj.y, sh.y), pi.y);
+              dz = sub_rn(sub_rn(pj.z, sh.z), pi.z);
             }
             code = img_code((int)kx, (int)ky, (int)kz);
           }
