@@ -377,7 +377,7 @@ def reference_loop(pairs_per_step):
                       "test or periodic images; one copy per core"}
 
 
-WORKLOADS = ("lj_slab", "lj_fluid", "charged_fluid", "charged_slab", "lj_slab_lfc")
+WORKLOADS = ("lj_slab", "lj_fluid", "charged_fluid", "charged_slab", "lj_slab_lfc", "spme_adjoint")
 
 
 def run_workload(args):
@@ -610,6 +610,99 @@ def sampled_electrostatics_error(mdf, s, pos, lattice, arc_kw, coul, nsample=409
     return out
 
 
+def run_spme_adjoint(args):
+    """The SPME adjoint on a batch of interpolation bases: 20736 unit charges
+    (the charged fluid), mesh 64^3, beta 0.95, the Hermite basis of the
+    B-spline of order 4 and of order 6 (support CC = order/2, 16 bins: 32
+    coefficients) plus N(0, 0.1) perturbations, 8 candidates per call.  One
+    step is one call of the energy with dE/dq, dE/dr, dE/dc and one of the
+    force-error functional (against the unperturbed basis's forces) with
+    dL/dq, dL/dr, dL/dc for all 8 candidates, FP64.  value: candidates per
+    second at order 6 (device time, inputs resident, L2 flushed between
+    steps); e2e: the same through pinned host arrays copied in and every
+    gradient copied out inside the timed region."""
+    rank, world, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    import mdforce as mdf
+    s = mdf.systems.charged_fluid()
+    dev = torch.device("cuda", local)
+    K, beta, nbin, ncand = (64, 64, 64), 0.95, 16, 8
+    rng = np.random.default_rng(7)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    per_order = {}
+    for order in (4, 6):
+        CC = order / 2.0
+        hs = mdf.optibasis.HermiteSPME(s.n, K, s.box, beta, CC, nbin)
+        base = mdf.optibasis.bspline_initial_basis(CC, nbin, order)
+        cand = base[None, :] + rng.normal(0.0, 0.1, size=(ncand, base.size))
+        q = torch.tensor(s.charge, dtype=torch.float64, device=dev)
+        r = torch.tensor(s.pos, dtype=torch.float64, device=dev)
+        c = torch.tensor(cand, dtype=torch.float64, device=dev)
+        fref = hs.energy(q, r, torch.tensor(base, dtype=torch.float64, device=dev), forces=True)["forces"][0].clone()
+
+        def step():
+            a = hs.energy(q, r, c, grads=True)
+            b = hs.force_error(q, r, c, fref, grads=True)
+            return a, b
+
+        for _ in range(max(args.warmup, 3)):
+            step()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for x, y in ev:
+            flush.fill_(1)
+            x.record(stream)
+            step()
+            y.record(stream)
+        torch.cuda.synchronize()
+        t_dev = sum(x.elapsed_time(y) for x, y in ev) / 1e3 / len(ev)
+        # end to end: host inputs in, gradients out, every step
+        hq = torch.tensor(s.charge, dtype=torch.float64).pin_memory()
+        hr = torch.tensor(s.pos, dtype=torch.float64).pin_memory()
+        hc = torch.tensor(cand, dtype=torch.float64).pin_memory()
+        hf = fref.cpu().pin_memory()
+        outs = {k: torch.empty(sh, dtype=torch.float64).pin_memory() for k, sh in
+                (("e", (ncand,)), ("gq", (ncand, s.n)), ("gr", (ncand, s.n, 3)), ("gc", (ncand, hs.ncoef)),
+                 ("l", (ncand,)), ("lq", (ncand, s.n)), ("lr", (ncand, s.n, 3)), ("lc", (ncand, hs.ncoef)))}
+        h2d = sum(t.numel() * 8 for t in (hq, hr, hc, hf))
+        d2h = sum(t.numel() * 8 for t in outs.values())
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(args.steps):
+            dq, dr, dc, df = (hq.to(dev, non_blocking=True), hr.to(dev, non_blocking=True),
+                              hc.to(dev, non_blocking=True), hf.to(dev, non_blocking=True))
+            A = hs.energy(dq, dr, dc, grads=True)
+            Bv = hs.force_error(dq, dr, dc, df, grads=True)
+            for k, v in (("e", A["energy"]), ("gq", A["dE_dq"]), ("gr", A["dE_dr"]), ("gc", A["dE_dc"]),
+                         ("l", Bv["loss"]), ("lq", Bv["dL_dq"]), ("lr", Bv["dL_dr"]), ("lc", Bv["dL_dc"])):
+                outs[k].copy_(v, non_blocking=True)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        t_e2e = a0.elapsed_time(a1) / 1e3 / args.steps
+        per_order[order] = {"device_ms_per_step": t_dev * 1e3, "candidates_per_s": ncand / t_dev,
+                            "e2e_candidates_per_s": ncand / t_e2e, "h2d_bytes_per_step": h2d,
+                            "d2h_bytes_per_step": d2h, "ncoef": hs.ncoef}
+        del hs
+    if rank == 0:
+        o6 = per_order[6]
+        line = {"metric": "SPME adjoint candidate evaluations/s (energy and force-error gradients in q, r, basis)",
+                "value": o6["candidates_per_s"], "unit": "candidates/s", "n_gpus": world, "steps": args.steps,
+                "warmup": max(args.warmup, 3), "ms_per_step": o6["device_ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "spme_adjoint", "n_atoms": s.n, "box": s.box.tolist(), "mesh": list(K),
+                           "beta": beta, "basis": f"Hermite, {nbin} bins, B-spline order 4 and 6 + N(0, 0.1)",
+                           "candidates_per_call": ncand, "l2": "flushed (256 MB write) between timed steps"},
+                "e2e": {"value": o6["e2e_candidates_per_s"], "unit": "candidates/s",
+                        "h2d_bytes_per_step": o6["h2d_bytes_per_step"], "d2h_bytes_per_step": o6["d2h_bytes_per_step"]},
+                "per_order": per_order}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args):
     """The reference arm: the same workload, config, metric and unit on the host
     cores, without the GPU engine (libmdforce is never loaded).  The reference's
@@ -655,6 +748,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "spme_adjoint":
+        return run_spme_adjoint(args)
     if args.workload != "lj_slab":
         return run_workload(args)
     rank, world, local = dist_env()

@@ -53,6 +53,8 @@ constexpr int HS_MAX_S = 16;      // stencil points per axis (2 ceil(CC))
 constexpr int HS_MAX_NBIN = 64;
 constexpr int HS_MAX_COEF = 2 * HS_MAX_NBIN;
 constexpr int HS_THREADS = 128;
+constexpr int HS_G = 8;                        // lanes per atom in the spread and gather
+constexpr int HS_ATOMS = HS_THREADS / HS_G;    // atoms per spread / gather block
 
 struct HsGeom {
   int K[3];
@@ -118,21 +120,38 @@ __device__ __forceinline__ long mesh_index(const HsGeom& g, const int k[3]) {
   return (long)k[2] + (long)g.K[2] * ((long)k[1] + (long)g.K[1] * k[0]);
 }
 
-// stencil of atom i: first point k0_d and weights per axis
-struct Stencil {
+// stencil of one atom, shared by its HS_G lanes: first point k0_d and the
+// weights phi and phi' per axis; the lanes evaluate the 3 S entries between
+// them.  u_d is returned to every lane (the coefficient derivatives are
+// re-evaluated from it at the end).
+struct GroupStencil {
   int k0[3];
-  PhiEval w[3][HS_MAX_S];
+  double v[3][HS_MAX_S], dv[3][HS_MAX_S];
 };
 
-__device__ void make_stencil(const HsGeom& g, const double* c, const double* r, Stencil& s) {
+__device__ void group_stencil(const HsGeom& g, const double* c, const double* r, int sub, GroupStencil& s,
+                              double u[3], int k0[3]) {
   for (int d = 0; d < 3; ++d) {
     double f = r[d] / g.L[d];
     f -= floor(f);
-    const double u = g.K[d] * f;
-    const int k0 = (int)floor(u) - g.half + 1;
-    s.k0[d] = k0;
-    for (int j = 0; j < g.S; ++j) s.w[d][j] = phi_eval(g, c, u - (double)(k0 + j));
+    u[d] = g.K[d] * f;
+    k0[d] = (int)floor(u[d]) - g.half + 1;
   }
+  if (sub == 0)
+    for (int d = 0; d < 3; ++d) s.k0[d] = k0[d];
+  for (int t = sub; t < 3 * g.S; t += HS_G) {
+    const int d = t / g.S, j = t - d * g.S;
+    const PhiEval e = phi_eval(g, c, u[d] - (double)(k0[d] + j));
+    s.v[d][j] = e.v;
+    s.dv[d][j] = e.dv;
+  }
+}
+
+template <int W>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, W);
+  return v;
 }
 
 __device__ __forceinline__ int wrap(int k, int K) {
@@ -161,33 +180,33 @@ __global__ void k_hs_factor(HsGeom g, const double* __restrict__ c, double* __re
   for (int t = 0; t < g.ncoef; ++t) dbfac[((long)d * g.ncoef + t) * Kmax + m] = db[t];
 }
 
-// spread: mode 0: Q += q_i W_i; mode 1: B_a -= q_i R_i,a W_i (three meshes)
+// spread: mode 0: Q += q_i W_i; mode 1: B_a -= q_i R_i,a W_i (three meshes).
+// HS_G lanes per atom share its S^3 stencil points (lane l: points l, l + HS_G, ...).
 __global__ void __launch_bounds__(HS_THREADS)
 k_hs_spread(HsGeom g, int N, const double* __restrict__ q, const double* __restrict__ r,
             const double* __restrict__ c, int mode, const double* __restrict__ R, double2* __restrict__ mesh) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  Stencil s;
-  make_stencil(g, c, r + 3 * (long)i, s);
+  __shared__ GroupStencil gs[HS_ATOMS];
+  const int grp = threadIdx.x / HS_G, sub = threadIdx.x % HS_G;
+  const int i = blockIdx.x * HS_ATOMS + grp;
+  if (i >= N) return;  // whole groups leave together; no block barrier below
+  GroupStencil& s = gs[grp];
+  double u[3];
+  int k0[3];
+  group_stencil(g, c, r + 3 * (long)i, sub, s, u, k0);
+  __syncwarp(((1u << HS_G) - 1u) << (threadIdx.x & 31 & ~(HS_G - 1)));  // the group's lanes
   double a[3] = {q[i], 0.0, 0.0};
   if (mode == 1) for (int d = 0; d < 3; ++d) a[d] = -q[i] * R[3 * (long)i + d];
-  for (int j0 = 0; j0 < g.S; ++j0) {
-    const double w0 = s.w[0][j0].v;
-    if (w0 == 0.0) continue;
-    for (int j1 = 0; j1 < g.S; ++j1) {
-      const double w01 = w0 * s.w[1][j1].v;
-      if (w01 == 0.0) continue;
-      for (int j2 = 0; j2 < g.S; ++j2) {
-        const double w = w01 * s.w[2][j2].v;
-        if (w == 0.0) continue;
-        const int k[3] = {wrap(s.k0[0] + j0, g.K[0]), wrap(s.k0[1] + j1, g.K[1]), wrap(s.k0[2] + j2, g.K[2])};
-        const long p = mesh_index(g, k);
-        if (mode == 0) {
-          atomicAdd(&mesh[p].x, a[0] * w);
-        } else {
-          for (int d = 0; d < 3; ++d) atomicAdd(&mesh[d * g.Kt + p].x, a[d] * w);
-        }
-      }
+  const int S = g.S, S2 = S * S, S3 = S2 * S;
+  for (int t = sub; t < S3; t += HS_G) {
+    const int j0 = t / S2, j1 = (t / S) % S, j2 = t % S;
+    const double w = s.v[0][j0] * s.v[1][j1] * s.v[2][j2];
+    if (w == 0.0) continue;
+    const int k[3] = {wrap(k0[0] + j0, g.K[0]), wrap(k0[1] + j1, g.K[1]), wrap(k0[2] + j2, g.K[2])};
+    const long p = mesh_index(g, k);
+    if (mode == 0) {
+      atomicAdd(&mesh[p].x, a[0] * w);
+    } else {
+      for (int d = 0; d < 3; ++d) atomicAdd(&mesh[d * g.Kt + p].x, a[d] * w);
     }
   }
 }
@@ -285,70 +304,88 @@ __global__ void k_hs_kspace_adj(HsGeom g, const double2* __restrict__ Qh, const 
 }
 
 // Gather.  mode 0 (energy): F_i, dE/dq_i, dE/dr_i, dE/dc partials from the
-// field meshes E_a (fld[0..2]) and the potential (fld[3]).  mode 1 (loss, first pass): F_i only (into F).  mode 2 (loss,
-// adjoint): dL/dq_i, dL/dr_i, dL/dc partials from Lam (lam) and the fields.
+// field meshes E_a (fld[0..2]) and the potential (fld[3]).  mode 1 (loss, first
+// pass): F_i only (into F).  mode 2 (loss, adjoint): dL/dq_i, dL/dr_i, dL/dc
+// partials from Lam (lam) and the fields.  HS_G lanes per atom split its S^3
+// stencil points; their sums are combined by shuffles in a fixed order.
 __global__ void __launch_bounds__(HS_THREADS)
 k_hs_gather(HsGeom g, int N, const double* __restrict__ q, const double* __restrict__ r,
             const double* __restrict__ c, int mode, const double2* __restrict__ fld, const double2* __restrict__ lam,
             const double* __restrict__ R, double* __restrict__ F, double* __restrict__ dq, double* __restrict__ dr,
             double* __restrict__ cpart) {
   __shared__ double csum[HS_MAX_COEF];
+  __shared__ GroupStencil gs[HS_ATOMS];
   for (int t = threadIdx.x; t < g.ncoef; t += blockDim.x) csum[t] = 0.0;
+  const int grp = threadIdx.x / HS_G, sub = threadIdx.x % HS_G;
+  const int i = blockIdx.x * HS_ATOMS + grp;
+  const bool live = i < N;
+  GroupStencil& s = gs[grp];
+  double u[3] = {0, 0, 0};
+  int k0[3] = {0, 0, 0};
+  if (live) group_stencil(g, c, r + 3 * (long)i, sub, s, u, k0);
   __syncthreads();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < N) {
-    Stencil s;
-    make_stencil(g, c, r + 3 * (long)i, s);
-    const double qi = q[i];
-    double Ri[3] = {0, 0, 0};
-    if (mode == 2)
-      for (int d = 0; d < 3; ++d) Ri[d] = R[3 * (long)i + d];
-    double Ef[3] = {0, 0, 0};  // sum W E_a
-    double pot = 0.0;          // sum W phi (mode 0) or sum W Lam (mode 2)
-    double gpot[3] = {0, 0, 0};  // sum grad W phi / Lam
-    double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};  // sum d_b W E_a
-    // partial contractions per axis for the coefficient gradient: T[d][j] =
-    // sum over the other two axes of (scalar field) prod_{d' != d} w
-    double T[3][HS_MAX_S];
+  const int S = g.S, S2 = S * S, S3 = S2 * S;
+  const double qi = live ? q[i] : 0.0;
+  double Ri[3] = {0, 0, 0};
+  if (live && mode == 2)
+    for (int d = 0; d < 3; ++d) Ri[d] = R[3 * (long)i + d];
+  double Ef[3] = {0, 0, 0};    // sum W E_a
+  double pot = 0.0;            // sum W phi (mode 0) or sum W Lam (mode 2)
+  double gpot[3] = {0, 0, 0};  // sum grad W phi / Lam
+  double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};  // sum d_b W E_a
+  // partial contractions per axis for the coefficient gradient: T[d][j] =
+  // sum over the other two axes of (scalar field) prod_{d' != d} w
+  double T[3][HS_MAX_S];
+  for (int d = 0; d < 3; ++d)
+    for (int j = 0; j < S; ++j) T[d][j] = 0.0;
+  const double kl[3] = {g.K[0] / g.L[0], g.K[1] / g.L[1], g.K[2] / g.L[2]};
+  if (live)
+    for (int t = sub; t < S3; t += HS_G) {
+      const int j0 = t / S2, j1 = (t / S) % S, j2 = t % S;
+      const double av = s.v[0][j0], adv = s.dv[0][j0], bv = s.v[1][j1], bdv = s.dv[1][j1];
+      const double ev = s.v[2][j2], edv = s.dv[2][j2];
+      const bool any = (av != 0.0 || adv != 0.0) && (bv != 0.0 || bdv != 0.0) && (ev != 0.0 || edv != 0.0);
+      if (!any) continue;
+      const double w12 = bv * ev, w02 = av * ev, w01 = av * bv;
+      const double w = av * w12;
+      const int k[3] = {wrap(k0[0] + j0, g.K[0]), wrap(k0[1] + j1, g.K[1]), wrap(k0[2] + j2, g.K[2])};
+      const long p = mesh_index(g, k);
+      const double gw[3] = {adv * kl[0] * w12, bdv * kl[1] * w02, edv * kl[2] * w01};
+      double E3[3];
+      for (int d = 0; d < 3; ++d) E3[d] = fld[d * g.Kt + p].x;
+      for (int d = 0; d < 3; ++d) Ef[d] += w * E3[d];
+      double sc = 0.0;  // the scalar field whose coefficient contraction is needed
+      if (mode == 0) {
+        const double ph = fld[3 * g.Kt + p].x;
+        pot += w * ph;
+        for (int d = 0; d < 3; ++d) gpot[d] += gw[d] * ph;
+        sc = ph;
+      } else if (mode == 2) {
+        const double lm = lam[p].x;
+        pot += w * lm;
+        for (int d = 0; d < 3; ++d) gpot[d] += gw[d] * lm;
+        for (int a2 = 0; a2 < 3; ++a2)
+          for (int b2 = 0; b2 < 3; ++b2) M[a2][b2] += gw[b2] * E3[a2];
+        sc = lm - (Ri[0] * E3[0] + Ri[1] * E3[1] + Ri[2] * E3[2]);
+      }
+      if (mode != 1) {
+        T[0][j0] += sc * w12;
+        T[1][j1] += sc * w02;
+        T[2][j2] += sc * w01;
+      }
+    }
+  // group sums (every lane of the group ends with the totals)
+  for (int d = 0; d < 3; ++d) Ef[d] = group_sum<HS_G>(Ef[d]);
+  if (mode != 1) {
+    pot = group_sum<HS_G>(pot);
+    for (int d = 0; d < 3; ++d) gpot[d] = group_sum<HS_G>(gpot[d]);
     for (int d = 0; d < 3; ++d)
-      for (int j = 0; j < g.S; ++j) T[d][j] = 0.0;
-    const double kl[3] = {g.K[0] / g.L[0], g.K[1] / g.L[1], g.K[2] / g.L[2]};
-    for (int j0 = 0; j0 < g.S; ++j0)
-      for (int j1 = 0; j1 < g.S; ++j1)
-        for (int j2 = 0; j2 < g.S; ++j2) {
-          const PhiEval& a = s.w[0][j0];
-          const PhiEval& b = s.w[1][j1];
-          const PhiEval& e = s.w[2][j2];
-          const double w12 = b.v * e.v, w02 = a.v * e.v, w01 = a.v * b.v;
-          const double w = a.v * w12;
-          const bool any = (a.v != 0.0 || a.dv != 0.0) && (b.v != 0.0 || b.dv != 0.0) && (e.v != 0.0 || e.dv != 0.0);
-          if (!any) continue;
-          const int k[3] = {wrap(s.k0[0] + j0, g.K[0]), wrap(s.k0[1] + j1, g.K[1]), wrap(s.k0[2] + j2, g.K[2])};
-          const long p = mesh_index(g, k);
-          const double gw[3] = {a.dv * kl[0] * w12, b.dv * kl[1] * w02, e.dv * kl[2] * w01};
-          double E3[3];
-          for (int d = 0; d < 3; ++d) E3[d] = fld[d * g.Kt + p].x;
-          for (int d = 0; d < 3; ++d) Ef[d] += w * E3[d];
-          double sc = 0.0;  // the scalar field whose coefficient contraction is needed
-          if (mode == 0) {
-            const double ph = fld[3 * g.Kt + p].x;
-            pot += w * ph;
-            for (int d = 0; d < 3; ++d) gpot[d] += gw[d] * ph;
-            sc = ph;
-          } else if (mode == 2) {
-            const double lm = lam[p].x;
-            pot += w * lm;
-            for (int d = 0; d < 3; ++d) gpot[d] += gw[d] * lm;
-            for (int a2 = 0; a2 < 3; ++a2)
-              for (int b2 = 0; b2 < 3; ++b2) M[a2][b2] += gw[b2] * E3[a2];
-            sc = lm - (Ri[0] * E3[0] + Ri[1] * E3[1] + Ri[2] * E3[2]);
-          }
-          if (mode != 1) {
-            T[0][j0] += sc * w12;
-            T[1][j1] += sc * w02;
-            T[2][j2] += sc * w01;
-          }
-        }
+      for (int j = 0; j < S; ++j) T[d][j] = group_sum<HS_G>(T[d][j]);
+  }
+  if (mode == 2)
+    for (int a2 = 0; a2 < 3; ++a2)
+      for (int b2 = 0; b2 < 3; ++b2) M[a2][b2] = group_sum<HS_G>(M[a2][b2]);
+  if (live && sub == 0) {
     if (mode == 0 || mode == 1)
       for (int d = 0; d < 3; ++d) F[3 * (long)i + d] = -qi * Ef[d];
     if (mode == 0) {
@@ -364,15 +401,17 @@ k_hs_gather(HsGeom g, int N, const double* __restrict__ q, const double* __restr
           dr[3 * (long)i + b2] = -qi * v + qi * gpot[b2];
         }
     }
-    if (mode != 1 && cpart) {
-      for (int d = 0; d < 3; ++d)
-        for (int j = 0; j < g.S; ++j) {
-          const PhiEval& e = s.w[d][j];
-          const double tv = qi * T[d][j];
-          if (tv == 0.0) continue;
-          for (int t = 0; t < 4; ++t)
-            if (e.idx[t] >= 0) atomicAdd(&csum[e.idx[t]], tv * e.dc[t]);
-        }
+  }
+  if (live && mode != 1 && cpart) {
+    // the group's lanes split the 3 S stencil entries, re-evaluating which
+    // coefficients each weight depends on
+    for (int t = sub; t < 3 * S; t += HS_G) {
+      const int d = t / S, j = t - d * S;
+      const double tv = qi * T[d][j];
+      if (tv == 0.0) continue;
+      const PhiEval e = phi_eval(g, c, u[d] - (double)(k0[d] + j));
+      for (int b2 = 0; b2 < 4; ++b2)
+        if (e.idx[b2] >= 0) atomicAdd(&csum[e.idx[b2]], tv * e.dc[b2]);
     }
   }
   __syncthreads();
@@ -489,7 +528,7 @@ extern "C" int md_hspme_create(md_hspme** out, int natoms, const int K[3], const
   g.Kt = (long)K[0] * K[1] * K[2];
   h->Kmax = std::max(K[0], std::max(K[1], K[2]));
   const long Kt = g.Kt;
-  const long nkb = (Kt + 255) / 256, nab = (natoms + HS_THREADS - 1) / HS_THREADS;
+  const long nkb = (Kt + 255) / 256, nab = (natoms + HS_ATOMS - 1) / HS_ATOMS;
   bool ok = cudaMalloc(&h->mesh, sizeof(double2) * Kt) == cudaSuccess &&
             cudaMalloc(&h->fld, sizeof(double2) * 4 * Kt) == cudaSuccess &&
             cudaMalloc(&h->bmesh, sizeof(double2) * 3 * Kt) == cudaSuccess &&
@@ -531,7 +570,7 @@ static int hs_forward(md_hspme* h, const double* q, const double* r, const doubl
                       bool want_marg) {
   HsGeom& g = h->g;
   const long Kt = g.Kt;
-  const int nab = (h->N + HS_THREADS - 1) / HS_THREADS;
+  const int nab = (h->N + HS_ATOMS - 1) / HS_ATOMS;
   const int nkb = (int)((Kt + 255) / 256);
   k_hs_factor<<<dim3((h->Kmax + 63) / 64, 3), 64, 0, s>>>(g, c, h->bfac, h->dbfac, h->Kmax);
   MD_CHECK_LAUNCH("hspme factor");
@@ -554,7 +593,7 @@ extern "C" int md_hspme_energy(md_hspme* h, const double* q, const double* r, co
   cudaStream_t s = (cudaStream_t)stream;
   HsGeom& g = h->g;
   const int N = h->N;
-  const int nab = (N + HS_THREADS - 1) / HS_THREADS;
+  const int nab = (N + HS_ATOMS - 1) / HS_ATOMS;
   const int nkb = (int)((g.Kt + 255) / 256);
   for (int b = 0; b < C; ++b) {
     const double* c = coeffs + (long)b * g.ncoef;
@@ -585,7 +624,8 @@ extern "C" int md_hspme_force_error(md_hspme* h, const double* q, const double* 
   HsGeom& g = h->g;
   const int N = h->N;
   const long Kt = g.Kt;
-  const int nab = (N + HS_THREADS - 1) / HS_THREADS;
+  const int nab = (N + HS_ATOMS - 1) / HS_ATOMS;       // spread / gather blocks
+  const int nrb = (N + HS_THREADS - 1) / HS_THREADS;   // residual blocks
   const int nkb = (int)((Kt + 255) / 256);
   const bool grads = dL_dq || dL_dr || dL_dc;
   for (int b = 0; b < C; ++b) {
@@ -594,9 +634,9 @@ extern "C" int md_hspme_force_error(md_hspme* h, const double* q, const double* 
     k_hs_gather<<<nab, HS_THREADS, 0, s>>>(g, N, q, r, c, 1, h->fld, nullptr, nullptr, h->Fw, nullptr, nullptr,
                                            nullptr);
     MD_CHECK_LAUNCH("hspme gather");
-    k_hs_residual<<<nab, HS_THREADS, 0, s>>>(N, h->Fw, fref, h->R, h->epart);
+    k_hs_residual<<<nrb, HS_THREADS, 0, s>>>(N, h->Fw, fref, h->R, h->epart);
     MD_CHECK_LAUNCH("hspme residual");
-    k_hs_sum<<<1, 32, 0, s>>>(h->epart, nab, loss + b);
+    k_hs_sum<<<1, 32, 0, s>>>(h->epart, nrb, loss + b);
     MD_CHECK_LAUNCH("hspme loss");
     if (!grads) continue;
     // adjoint: residuals spread, transformed, Lam and the factor marginals

@@ -163,15 +163,17 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return s;  // valid in thread 0
 }
 
-// one block per candidate basis: phi_d = hat0_d + c . hats_d in shared memory,
-// then every thread takes (axis, m) pairs; value and gradient block-reduced
-// in a fixed order
+// block (c, y): candidate c; y = 0 its value, y = 1 + b its gradient in
+// coefficient b.  Every block forms phi_d = hat0_d + c . hats_d in shared
+// memory and the value sum over the (axis, m) pairs (a gradient block needs it
+// for the square root's derivative); sums are block-reduced in a fixed order.
 __global__ void __launch_bounds__(IK_THREADS)
 k_ikerr_eval(IkEval e, const double* __restrict__ coeff, double* __restrict__ value,
              double* __restrict__ grad) {
   extern __shared__ double phi[];  // concatenated phi_0, phi_1, phi_2
   __shared__ double sh[IK_THREADS / 32];
   const int c = blockIdx.x;
+  if (blockIdx.y > 0 && !grad) return;
   const double* cc = coeff + (size_t)c * e.ncoef;
   for (int d = 0; d < 3; ++d)
     for (int k = threadIdx.x; k <= e.kmax[d]; k += blockDim.x) {
@@ -206,13 +208,14 @@ k_ikerr_eval(IkEval e, const double* __restrict__ coeff, double* __restrict__ va
   __shared__ double s_o1;
   if (threadIdx.x == 0) {
     s_o1 = s_tot * e.norm;
-    value[c] = sqrt(s_o1) * e.scale;
+    if (blockIdx.y == 0) value[c] = sqrt(s_o1) * e.scale;
   }
   __syncthreads();
-  if (!grad) return;
+  if (blockIdx.y == 0) return;
   // d T / d c_b = sum_l 2 phi_l B_l / phi_0^2 - 2 phi_l^2 B_0 / phi_0^3
   const double gpref = e.norm * 0.5 / sqrt(s_o1) * e.scale;
-  for (int b = 0; b < e.ncoef; ++b) {
+  {
+    const int b = blockIdx.y - 1;
     double g = 0.0;
     for (int p = threadIdx.x; p < npair; p += blockDim.x) {
       int d, m;
@@ -390,7 +393,7 @@ static int ikerr_launch(md_ikerr* h, int C, const double* d_coeff, double* d_val
   const double V = h->L[0] * h->L[1] * h->L[2];
   e.norm = 1.0 / (2. * M_PI * V * 2. * M_PI * V);
   e.scale = sqrt(h->q2 * h->q2 / h->natoms) * 138.93545756169981341199;
-  k_ikerr_eval<<<C, IK_THREADS, h->smem, s>>>(e, d_coeff, d_val, d_grad);
+  k_ikerr_eval<<<dim3(C, d_grad ? 1 + h->ncoef : 1), IK_THREADS, h->smem, s>>>(e, d_coeff, d_val, d_grad);
   MD_CHECK_LAUNCH("k_ikerr_eval");
   return MD_OK;
 }

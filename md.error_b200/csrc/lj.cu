@@ -279,36 +279,6 @@ __device__ __forceinline__ void lj_pass_mixed(const int4 e4, int nvalid, const f
   a.fz.add(bz);
 }
 
-// Packed binary32 pairs (sm_100 f32x2): one instruction applies the same
-// round-to-nearest binary32 operation to both halves, so every half equals
-// the scalar .rn result.
-struct F2 {
-  unsigned long long v;
-};
-__device__ __forceinline__ F2 f2(float lo, float hi) {
-  F2 r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(lo), "f"(hi));
-  return r;
-}
-__device__ __forceinline__ void f2_split(F2 a, float& lo, float& hi) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a.v));
-}
-__device__ __forceinline__ F2 f2_sub(F2 a, F2 b) {
-  F2 r;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-  return r;
-}
-__device__ __forceinline__ F2 f2_mul(F2 a, F2 b) {
-  F2 r;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-  return r;
-}
-__device__ __forceinline__ F2 f2_fma(F2 a, F2 b, F2 c) {
-  F2 r;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
-  return r;
-}
-
 // Accumulators of the packed pass: energy as (pair, pair) halves without the
 // shift, which is added once per interacting pair at the end (cnt); virial
 // (xx, yy) packed and zz.

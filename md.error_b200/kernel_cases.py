@@ -14,7 +14,8 @@ Cases:
             back, z order) and one neighbour-list build on the slab start
             (radius rc_i + 0.6)
   lj        LJ forces over that list, 3 launches
-  arc       one AdaptRCut deposit + update on the slab start
+  arc       AdaptRCut on the slab start: construction (the kernel tables),
+            one deposit, update, assign and pressure correction
   errmap    the ik error map of the 20,736-atom charged fluid, K 32^3
   ikerr     the optiBasis functional, 8 candidates, K 64^3
   bonded    harmonic bonds + angles on the LJ fcc crystal
@@ -83,8 +84,9 @@ def main():
         nvtx.range_pop()
     elif a.case == "arc":
         s, sys_ = slab_system(0)
-        arc = mdf.AdaptRCutEstimator(sys_, refh=1.0, rcmin=B.RC_MIN, rcmax=B.RC_MAX, rcstep=B.RC_STEP)
+        torch.cuda.synchronize()
         nvtx.range_push("measure")
+        arc = mdf.AdaptRCutEstimator(sys_, refh=1.0, rcmin=B.RC_MIN, rcmax=B.RC_MAX, rcstep=B.RC_STEP)
         arc.deposite()
         arc.update(B.TARGET_PREC)
         arc.assign()
