@@ -33,6 +33,7 @@ struct md_adapt_rcut {
   double* s1k = nullptr;      // [nrc][nele] real
   double* s2k = nullptr;      // [3][nrc][nele] imaginary
   double* pck = nullptr;      // [3][nrc][nele] real (pressure-correction kernels)
+  double* ints = nullptr;     // [4][nrc][octant points] radial integrals of the tables
   double2* work = nullptr;    // [4*nrc][nele]
   double* error = nullptr;    // [nrc][nele]
   double* rcut = nullptr;     // [nele]
@@ -110,36 +111,66 @@ __device__ __forceinline__ long lin(const int n[3], int x, int y, int z) { retur
 
 struct ArcDims { int n[3]; int nrc; double box[3]; };
 
-// one thread per octant point (ax, ay, az) >= 0
-__global__ void k_arc_tables(ArcDims g, const double* rc, double* s1k, double* s2k, double* pck, unsigned* flags) {
+__device__ __forceinline__ double oct_k(const ArcDims& g, int t) {
+  const int hy = g.n[1] / 2 + 1, hz = g.n[2] / 2 + 1;
+  const int az = t % hz, ay = (t / hz) % hy, ax = t / (hz * hy);
+  const double kx0 = ax / g.box[0], ky0 = ay / g.box[1], kz0 = az / g.box[2];
+  return sqrt(kx0 * kx0 + ky0 * ky0 + kz0 * kz0);
+}
+
+// The radial integrals of the tables, one thread per (integrand, cutoff
+// interval, octant point): the integrand kinds 13, 5, 1 and 25 over
+// [rc_c, rc_{c+1}] (the last up to 30) with the reference's tolerances.
+// A warp covers 32 octant points of one (kind, interval).
+__global__ void k_arc_integrals(ArcDims g, const double* rc, double* ints, unsigned* flags) {
+  const int noct = (g.n[0] / 2 + 1) * (g.n[1] / 2 + 1) * (g.n[2] / 2 + 1);
+  const int nrc = g.nrc;
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= 4L * nrc * noct) return;
+  const int pt = (int)(t % noct), c = (int)((t / noct) % nrc), kind = (int)(t / ((long)noct * nrc));
+  const double k = oct_k(g, pt);
+  double v = 0.0;
+  if (k != 0) {
+    const double hi = (c == nrc - 1) ? 30.0 : rc[c + 1];
+    const int kinds[4] = {13, 5, 1, 25};
+    const double tols[4] = {1e-12, 1e-16, 1e-7, 1e-7};
+    v = g4_adaptive(kinds[kind], k, rc[c], hi, tols[kind], flags);
+  }
+  ints[t] = v;
+}
+
+// one thread per octant point (ax, ay, az) >= 0: the cumulative sums of the
+// radial integrals and the angular factors, written to every sign image
+__global__ void k_arc_tables(ArcDims g, const double* rc, const double* ints, double* s1k, double* s2k,
+                             double* pck) {
   const int hx = g.n[0] / 2 + 1, hy = g.n[1] / 2 + 1, hz = g.n[2] / 2 + 1;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= hx * hy * hz) return;
+  const int noct = hx * hy * hz;
+  if (t >= noct) return;
   const int az = t % hz, ay = (t / hz) % hy, ax = t / (hz * hy);
   const int nrc = g.nrc;
   const long nele = (long)g.n[0] * g.n[1] * g.n[2];
   const double eps = 1.0, sigma = 1.0;
   const double pref = 16. * 36. * pow_int_d(sigma, 12) * eps;
   const double pre = 8. * eps * pow_int_d(sigma, 6);
-  const double kx0 = ax / g.box[0], ky0 = ay / g.box[1], kz0 = az / g.box[2];
-  const double k = sqrt(kx0 * kx0 + ky0 * ky0 + kz0 * kz0);
+  const double k = oct_k(g, t);
   const int MAXRC = 32;
   double S1[MAXRC], T[MAXRC], I1[MAXRC], I5[MAXRC];
+  auto integral = [&](int kind, int c) { return ints[((long)kind * nrc + c) * noct + t]; };
   // cumulative integrals from the top interval [rc_last, 30] down
   double cum13 = 0, cum5 = 0;
   for (int c = nrc - 1; c >= 0; --c) {
-    const double hi = (c == nrc - 1) ? 30.0 : rc[c + 1];
     if (k != 0) {
-      cum13 += 2. / k * pref * g4_adaptive(13, k, rc[c], hi, 1e-12, flags);
+      cum13 += 2. / k * pref * integral(0, c);
       S1[c] = cum13;
-      cum5 += g4_adaptive(5, k, rc[c], hi, 1e-16, flags) * pre / k * 2 * M_PI;
+      cum5 += integral(1, c) * pre / k * 2 * M_PI;
       const double r = rc[c], r6 = pow_int_d(r, 6);
       const double e = 2. * M_PI * k * r;
       double size = -2. * M_PI * r * r * (4. * eps * pow_int_d(sigma, 6) / r6) * (2. * cos(e) / e - 2. * sin(e) / (e * e));
       size /= k;
       T[c] = cum5 + size;
-      I1[c] = g4_adaptive(1, k, rc[c], hi, 1e-7, flags);
-      I5[c] = g4_adaptive(25, k, rc[c], hi, 1e-7, flags);
+      I1[c] = integral(2, c);
+      I5[c] = integral(3, c);
     } else {
       S1[c] = 4. * M_PI * pref / 11. * pow_int_d(rc[c], -11);
       T[c] = 0;
@@ -447,7 +478,10 @@ static int build_tables(md_adapt_rcut* a) {
   for (int d = 0; d < 3; ++d) { g.n[d] = a->n[d]; g.box[d] = hs.L[d]; a->box_tab[d] = hs.L[d]; }
   g.nrc = a->nrc;
   int oct = (g.n[0] / 2 + 1) * (g.n[1] / 2 + 1) * (g.n[2] / 2 + 1);
-  k_arc_tables<<<ceil_div(oct, 64), 64, 0, a->sys->stream>>>(g, a->d_rc, a->s1k, a->s2k, a->pck, &a->sys->st->flags);
+  k_arc_integrals<<<ceil_div(4L * g.nrc * oct, 128), 128, 0, a->sys->stream>>>(g, a->d_rc, a->ints,
+                                                                              &a->sys->st->flags);
+  MD_CHECK_LAUNCH("arc integrals");
+  k_arc_tables<<<ceil_div(oct, 64), 64, 0, a->sys->stream>>>(g, a->d_rc, a->ints, a->s1k, a->s2k, a->pck);
   MD_CHECK_LAUNCH("arc tables");
   return MD_OK;
 }
@@ -486,6 +520,8 @@ extern "C" int md_arc_create(md_adapt_rcut** out, md_system* sys, double refh, d
             cudaMalloc(&a->s1k, sizeof(double) * nrc * ne) == cudaSuccess &&
             cudaMalloc(&a->s2k, sizeof(double) * 3 * nrc * ne) == cudaSuccess &&
             cudaMalloc(&a->pck, sizeof(double) * 3 * nrc * ne) == cudaSuccess &&
+            cudaMalloc(&a->ints, sizeof(double) * 4 * nrc * (size_t)((a->n[0] / 2 + 1) * (a->n[1] / 2 + 1) *
+                                                                    (a->n[2] / 2 + 1))) == cudaSuccess &&
             cudaMalloc(&a->work, sizeof(double2) * 4 * nrc * ne) == cudaSuccess &&
             cudaMalloc(&a->error, sizeof(double) * nrc * ne) == cudaSuccess &&
             cudaMalloc(&a->rcut, sizeof(double) * ne) == cudaSuccess &&
@@ -509,7 +545,7 @@ extern "C" int md_arc_create(md_adapt_rcut** out, md_system* sys, double refh, d
 
 extern "C" int md_arc_destroy(md_adapt_rcut* a) {
   if (!a) return MD_OK;
-  void* p[] = {a->d_rc, a->counts, a->rho, a->rhok, a->s1k, a->s2k, a->pck, a->work,
+  void* p[] = {a->d_rc, a->counts, a->rho, a->rhok, a->s1k, a->s2k, a->pck, a->ints, a->work,
                a->error, a->rcut, a->rcidx, a->rcidx2, a->rerr, a->pcorr};
   for (void* q : p) if (q) cudaFree(q);
   delete a;

@@ -22,6 +22,7 @@
 // the force loop forms d - k L with the reference's exact operations.
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include "device_common.cuh"
 
 struct NlGeom {
@@ -78,8 +79,6 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
   const R Li[3] = {boxLi<R>(st, 0), boxLi<R>(st, 1), boxLi<R>(st, 2)};
   const bool minimg = (MODE == MD_NL_MINIMAGE) || force_minimage;
   const int hc[3] = {c / (g.nc[2] * g.nc[1]), (c / g.nc[2]) % g.nc[1], c % g.nc[2]};
-  double h[3];
-  for (int d = 0; d < 3; ++d) h[d] = st->L[d] / g.nc[d];
 
   // largest list radius among the home atoms
   if (threadIdx.x == 0) rl_max_sh = 0.f;
@@ -94,25 +93,33 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
   }
   __syncthreads();
 
-  // runs of candidate cells: one thread per (x, y) column of the stencil
-  // computes its (at most 3) z segments; block-wide exclusive scans give
-  // each run its slot and tile offset in column order
-  int lo[3], hi[3];
-  bool full[3];
-  {
+  // the stencil of the home cell (cells per axis whose box comes within the
+  // largest radius), worked out once by thread 0
+  __shared__ double s_h[3];
+  __shared__ int s_lo[3], s_hi[3], s_full[3];
+  if (threadIdx.x == 0) {
     const double rle = (double)rl_max_sh * (1.0 + 1e-6) + 2e-3;
     for (int d = 0; d < 3; ++d) {
+      const double hd = st->L[d] / g.nc[d];
+      s_h[d] = hd;
       if (!minimg) {
-        const int reach = (h[d] >= rlist_uniform) ? 1 : (int)ceil(rlist_uniform / h[d]);
-        lo[d] = hc[d] - reach; hi[d] = hc[d] + reach; full[d] = false;
+        const int reach = (hd >= rlist_uniform) ? 1 : (int)ceil(rlist_uniform / hd);
+        s_lo[d] = hc[d] - reach; s_hi[d] = hc[d] + reach; s_full[d] = 0;
       } else {
-        lo[d] = (int)floor((hc[d] * h[d] - rle) / h[d]);
-        hi[d] = (int)floor(((hc[d] + 1) * h[d] + rle) / h[d]);
-        full[d] = (hi[d] - lo[d] + 1) >= g.nc[d];
-        if (full[d]) { lo[d] = 0; hi[d] = g.nc[d] - 1; }
+        int a = (int)floor((hc[d] * hd - rle) / hd), b = (int)floor(((hc[d] + 1) * hd + rle) / hd);
+        s_full[d] = (b - a + 1) >= g.nc[d];
+        if (s_full[d]) { a = 0; b = g.nc[d] - 1; }
+        s_lo[d] = a; s_hi[d] = b;
       }
     }
   }
+  __syncthreads();
+  // runs of candidate cells: one thread per (x, y) column of the stencil
+  // computes its (at most 3) z segments; block-wide exclusive scans give
+  // each run its slot and tile offset in column order
+  const double h[3] = {s_h[0], s_h[1], s_h[2]};
+  const int lo[3] = {s_lo[0], s_lo[1], s_lo[2]}, hi[3] = {s_hi[0], s_hi[1], s_hi[2]};
+  const bool full[3] = {s_full[0] != 0, s_full[1] != 0, s_full[2] != 0};
   __shared__ int scan_r[32], scan_a[32];
   __shared__ int base_r, base_a, overflow_runs;
   if (threadIdx.x == 0) { base_r = 0; base_a = 0; overflow_runs = 0; }
@@ -226,7 +233,7 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
   // d = (r_j - r_i) - k_run L repeats the reference's binary32 operations and
   // the image code is the run's.
   const bool runshift = minimg && !full[0] && !full[1] && !full[2];
-  const float hz = (float)h[2];
+  const float hz = (float)h[2], hzi = 1.0f / hz;
   const float Lzf = (float)st->L[2];
   // z of entry t of a run (z order) in the stored, wrapped frame
   auto zat = [&](int roff, int rjb, int t) -> float {
@@ -244,7 +251,7 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
     {
       const double xi[3] = {(double)pi.x, (double)pi.y, (double)pi.z};
       for (int d = 0; d < 3; ++d) {
-        double w = xi[d] - floor(xi[d] / st->L[d]) * st->L[d];
+        double w = xi[d] - floor(xi[d] * st->Li[d]) * st->L[d];
         if (!(w >= 0.0) || w >= st->L[d]) w = 0.0;
         xe[d] = (float)w;
       }
@@ -279,8 +286,10 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
         const int nzr = rt.nz[r];
         if (keep && minimg && nzr) {
           const int zc0 = rt.zc0[r];
-          const int k0 = max((int)floorf((xe[2] - wz) / hz) - zc0, 0);
-          const int k1 = min((int)floorf((xe[2] + wz) / hz) - zc0, nzr - 1);
+          // (a product with 1/h_z: its rounding, ~1e-5 cell, stays inside the
+          // window's 2e-3 margin)
+          const int k0 = max((int)floorf((xe[2] - wz) * hzi) - zc0, 0);
+          const int k1 = min((int)floorf((xe[2] + wz) * hzi) - zc0, nzr - 1);
           keep = k0 <= k1;
           if (keep) {
             const int roff = rt.off[r], rjb = rt.jb[r];
@@ -353,11 +362,20 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
             j = slot_of_w<R>(pj.w);
           }
           const T4 sh = wshift[warp][k];
-          R dx, dy, dz;
+          R dx, dy, dz, d2;
           if (runshift) {
-            dx = sub_rn(sub_rn(pj.x, pi.x), sh.x);
-            dy = sub_rn(sub_rn(pj.y, pi.y), sh.y);
             dz = sub_rn(sub_rn(pj.z, pi.z), sh.z);
+            if constexpr (std::is_same<R, float>::value) {
+              // x and y as one packed binary32 pair: the same roundings
+              const F2 dxy = f2_sub(f2_sub(f2(pj.x, pj.y), f2(pi.x, pi.y)), f2(sh.x, sh.y));
+              float sx, sy;
+              f2_split(f2_mul(dxy, dxy), sx, sy);
+              d2 = __fadd_rn(__fadd_rn(sx, sy), __fmul_rn(dz, dz));
+            } else {
+              dx = sub_rn(sub_rn(pj.x, pi.x), sh.x);
+              dy = sub_rn(sub_rn(pj.y, pi.y), sh.y);
+              d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
+            }
             code = slot_of_w<R>(sh.w);
           } else {
             const R rx = sub_rn(pj.x, pi.x), ry = sub_rn(pj.y, pi.y), rz = sub_rn(pj.z, pi.z);
@@ -374,8 +392,8 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
               dz = sub_rn(sub_rn(pj.z, sh.z), pi.z);
             }
             code = img_code((int)kx, (int)ky, (int)kz);
+            d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
           }
-          const R d2 = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
           ok = (d2 < rl2) && (j != i);
         }
         const unsigned m = __ballot_sync(0xffffffffu, ok);
