@@ -98,11 +98,23 @@ __global__ void __launch_bounds__(1024) k_scan(int n, uint32_t* count, uint32_t*
   const int T = blockDim.x;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = T >> 5;
   uint32_t carry = 0;
+  // cells 4t..4t+3 of a tile as one 16-byte load (count and start come from
+  // cudaMalloc, so 4t is 16-byte aligned), the next tile's loaded early
+  auto load4 = [&](int i0, uint32_t v[4]) {
+    if (i0 + 3 < n) {
+      const uint4 q = *reinterpret_cast<const uint4*>(count + i0);
+      v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) v[k] = (i0 + k < n) ? count[i0 + k] : 0u;
+    }
+  };
+  uint32_t nxt[4];
+  load4(4 * threadIdx.x, nxt);
   for (int base = 0; base < n; base += 4 * T) {
     const int i0 = base + 4 * threadIdx.x;
-    uint32_t v[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) v[k] = (i0 + k < n) ? count[i0 + k] : 0u;
+    uint32_t v[4] = {nxt[0], nxt[1], nxt[2], nxt[3]};
+    if (base + 4 * T < n) load4(i0 + 4 * T, nxt);
     const uint32_t tot = v[0] + v[1] + v[2] + v[3];
     uint32_t x = tot;
 #pragma unroll
@@ -123,13 +135,19 @@ __global__ void __launch_bounds__(1024) k_scan(int n, uint32_t* count, uint32_t*
     }
     __syncthreads();
     uint32_t run = carry + (wid > 0 ? wsum[wid - 1] : 0u) + x - tot;
+    if (i0 + 3 < n) {
+      const uint4 st4 = make_uint4(run, run + v[0], run + v[0] + v[1], run + v[0] + v[1] + v[2]);
+      *reinterpret_cast<uint4*>(start + i0) = st4;
+      *reinterpret_cast<uint4*>(count + i0) = make_uint4(0u, 0u, 0u, 0u);
+    } else {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (i0 + k < n) {
-        start[i0 + k] = run;
-        count[i0 + k] = 0u;
+      for (int k = 0; k < 4; ++k) {
+        if (i0 + k < n) {
+          start[i0 + k] = run;
+          count[i0 + k] = 0u;
+        }
+        run += v[k];
       }
-      run += v[k];
     }
     carry += wsum[nw - 1];
     __syncthreads();  // wsum is rewritten by the next tile

@@ -303,14 +303,23 @@ __global__ void k_hs_kspace_adj(HsGeom g, const double2* __restrict__ Qh, const 
   }
 }
 
+// The real parts of three field meshes and one scalar mesh interleaved per
+// point (one 32-byte read per stencil point in the gather)
+__global__ void k_hs_pack4(long Kt, const double2* __restrict__ a, const double2* __restrict__ s,
+                           double4a* __restrict__ out) {
+  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (p < Kt) out[p] = double4a{a[p].x, a[Kt + p].x, a[2 * Kt + p].x, s[p].x};
+}
+
 // Gather.  mode 0 (energy): F_i, dE/dq_i, dE/dr_i, dE/dc partials from the
-// field meshes E_a (fld[0..2]) and the potential (fld[3]).  mode 1 (loss, first
-// pass): F_i only (into F).  mode 2 (loss, adjoint): dL/dq_i, dL/dr_i, dL/dc
-// partials from Lam (lam) and the fields.  HS_G lanes per atom split its S^3
-// stencil points; their sums are combined by shuffles in a fixed order.
+// field meshes E_a and the potential (f4 = (E_0, E_1, E_2, phi)).  mode 1
+// (loss, first pass): F_i only (into F).  mode 2 (loss, adjoint): dL/dq_i,
+// dL/dr_i, dL/dc partials from f4 = (E_0, E_1, E_2, Lam).  HS_G lanes per atom
+// split its S^3 stencil points; their sums are combined by shuffles in a
+// fixed order.
 __global__ void __launch_bounds__(HS_THREADS)
 k_hs_gather(HsGeom g, int N, const double* __restrict__ q, const double* __restrict__ r,
-            const double* __restrict__ c, int mode, const double2* __restrict__ fld, const double2* __restrict__ lam,
+            const double* __restrict__ c, int mode, const double4a* __restrict__ f4,
             const double* __restrict__ R, double* __restrict__ F, double* __restrict__ dq, double* __restrict__ dr,
             double* __restrict__ cpart) {
   __shared__ double csum[HS_MAX_COEF];
@@ -351,17 +360,17 @@ k_hs_gather(HsGeom g, int N, const double* __restrict__ q, const double* __restr
       const int k[3] = {wrap(k0[0] + j0, g.K[0]), wrap(k0[1] + j1, g.K[1]), wrap(k0[2] + j2, g.K[2])};
       const long p = mesh_index(g, k);
       const double gw[3] = {adv * kl[0] * w12, bdv * kl[1] * w02, edv * kl[2] * w01};
-      double E3[3];
-      for (int d = 0; d < 3; ++d) E3[d] = fld[d * g.Kt + p].x;
+      const double4a fv = f4[p];  // E_0, E_1, E_2 and the scalar field (phi or Lam)
+      const double E3[3] = {fv.x, fv.y, fv.z};
       for (int d = 0; d < 3; ++d) Ef[d] += w * E3[d];
       double sc = 0.0;  // the scalar field whose coefficient contraction is needed
       if (mode == 0) {
-        const double ph = fld[3 * g.Kt + p].x;
+        const double ph = fv.w;
         pot += w * ph;
         for (int d = 0; d < 3; ++d) gpot[d] += gw[d] * ph;
         sc = ph;
       } else if (mode == 2) {
-        const double lm = lam[p].x;
+        const double lm = fv.w;
         pot += w * lm;
         for (int d = 0; d < 3; ++d) gpot[d] += gw[d] * lm;
         for (int a2 = 0; a2 < 3; ++a2)
@@ -484,6 +493,7 @@ struct md_hspme {
   double2* fld = nullptr;    // [4][Kt]
   double2* bmesh = nullptr;  // [3][Kt] residual spread / transforms
   double2* lam = nullptr;    // [Kt]
+  double4a* f4 = nullptr;    // [Kt] gather input: fields and one scalar mesh, real parts
   double* bfac = nullptr;    // [3][Kmax]
   double* dbfac = nullptr;   // [3][ncoef][Kmax]
   double* marg = nullptr;    // [3][Kmax]
@@ -494,7 +504,7 @@ struct md_hspme {
 };
 
 static void hs_free(md_hspme* h) {
-  void* p[] = {h->mesh, h->fld, h->bmesh, h->lam, h->bfac, h->dbfac, h->marg, h->epart, h->cpart, h->R, h->Fw};
+  void* p[] = {h->mesh, h->fld, h->bmesh, h->lam, h->f4, h->bfac, h->dbfac, h->marg, h->epart, h->cpart, h->R, h->Fw};
   for (void* x : p) if (x) cudaFree(x);
 }
 
@@ -533,6 +543,7 @@ extern "C" int md_hspme_create(md_hspme** out, int natoms, const int K[3], const
             cudaMalloc(&h->fld, sizeof(double2) * 4 * Kt) == cudaSuccess &&
             cudaMalloc(&h->bmesh, sizeof(double2) * 3 * Kt) == cudaSuccess &&
             cudaMalloc(&h->lam, sizeof(double2) * Kt) == cudaSuccess &&
+            cudaMalloc(&h->f4, sizeof(double4a) * Kt) == cudaSuccess &&
             cudaMalloc(&h->bfac, sizeof(double) * 3 * h->Kmax) == cudaSuccess &&
             cudaMalloc(&h->dbfac, sizeof(double) * 3 * std::max(g.ncoef, 1) * h->Kmax) == cudaSuccess &&
             cudaMalloc(&h->marg, sizeof(double) * 3 * h->Kmax) == cudaSuccess &&
@@ -599,7 +610,9 @@ extern "C" int md_hspme_energy(md_hspme* h, const double* q, const double* r, co
     const double* c = coeffs + (long)b * g.ncoef;
     if (int e = hs_forward(h, q, r, c, s, dE_dc != nullptr)) return e;
     double* F = forces ? forces + 3L * N * b : h->Fw;
-    k_hs_gather<<<nab, HS_THREADS, 0, s>>>(g, N, q, r, c, 0, h->fld, nullptr, nullptr, F,
+    k_hs_pack4<<<nkb, 256, 0, s>>>(g.Kt, h->fld, h->fld + 3 * g.Kt, h->f4);
+    MD_CHECK_LAUNCH("hspme pack");
+    k_hs_gather<<<nab, HS_THREADS, 0, s>>>(g, N, q, r, c, 0, h->f4, nullptr, F,
                                            dE_dq ? dE_dq + (long)N * b : nullptr, dE_dr ? dE_dr + 3L * N * b : nullptr,
                                            dE_dc ? h->cpart : nullptr);
     MD_CHECK_LAUNCH("hspme gather");
@@ -631,8 +644,9 @@ extern "C" int md_hspme_force_error(md_hspme* h, const double* q, const double* 
   for (int b = 0; b < C; ++b) {
     const double* c = coeffs + (long)b * g.ncoef;
     if (int e = hs_forward(h, q, r, c, s, false)) return e;
-    k_hs_gather<<<nab, HS_THREADS, 0, s>>>(g, N, q, r, c, 1, h->fld, nullptr, nullptr, h->Fw, nullptr, nullptr,
-                                           nullptr);
+    k_hs_pack4<<<nkb, 256, 0, s>>>(Kt, h->fld, h->fld + 3 * Kt, h->f4);
+    MD_CHECK_LAUNCH("hspme pack");
+    k_hs_gather<<<nab, HS_THREADS, 0, s>>>(g, N, q, r, c, 1, h->f4, nullptr, h->Fw, nullptr, nullptr, nullptr);
     MD_CHECK_LAUNCH("hspme gather");
     k_hs_residual<<<nrb, HS_THREADS, 0, s>>>(N, h->Fw, fref, h->R, h->epart);
     MD_CHECK_LAUNCH("hspme residual");
@@ -648,7 +662,9 @@ extern "C" int md_hspme_force_error(md_hspme* h, const double* q, const double* 
     k_hs_kspace_adj<<<nkb, 256, 0, s>>>(g, h->mesh, h->bmesh, h->bfac, h->Kmax, h->lam, h->marg);
     MD_CHECK_LAUNCH("hspme adjoint kspace");
     if (int e = dft3_grid(h->lam, g.K, +1, 1, s)) return e;
-    k_hs_gather<<<nab, HS_THREADS, 0, s>>>(g, N, q, r, c, 2, h->fld, h->lam, h->R, nullptr,
+    k_hs_pack4<<<nkb, 256, 0, s>>>(Kt, h->fld, h->lam, h->f4);
+    MD_CHECK_LAUNCH("hspme pack");
+    k_hs_gather<<<nab, HS_THREADS, 0, s>>>(g, N, q, r, c, 2, h->f4, h->R, nullptr,
                                            dL_dq ? dL_dq + (long)N * b : nullptr, dL_dr ? dL_dr + 3L * N * b : nullptr,
                                            dL_dc ? h->cpart : nullptr);
     MD_CHECK_LAUNCH("hspme adjoint gather");

@@ -17,7 +17,8 @@ Cases:
   arc       AdaptRCut on the slab start: construction (the kernel tables),
             one deposit, update, assign and pressure correction
   errmap    the ik error map of the 20,736-atom charged fluid, K 32^3
-  ikerr     the optiBasis functional, 8 candidates, K 64^3
+  ikerr     the optiBasis functional: construction (the basis hats on the
+            over-sampled grid) and one evaluation of 8 candidates, K 64^3
   bonded    harmonic bonds + angles on the LJ fcc crystal
   hspme     the Hermite-basis SPME of the charged fluid with all gradients, K 64^3
 --precision 0 (mixed) or 1 (FP64) for slab, nlist, lj and bonded.
@@ -103,9 +104,10 @@ def main():
         torch.cuda.synchronize()
         nvtx.range_pop()
     elif a.case == "ikerr":
-        f = mdf.optibasis.IkErrorGPU(2.0, 16, 0.95, (64, 64, 64), 20736.0, 20736, [30.0, 30.0, 30.0], l_cut=10)
         c = np.tile(mdf.optibasis.bspline_initial_basis(2.0, 16, 4), (8, 1))
+        torch.cuda.synchronize()
         nvtx.range_push("measure")
+        f = mdf.optibasis.IkErrorGPU(2.0, 16, 0.95, (64, 64, 64), 20736.0, 20736, [30.0, 30.0, 30.0], l_cut=10)
         f.evaluate(c)
         torch.cuda.synchronize()
         nvtx.range_pop()
