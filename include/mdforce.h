@@ -105,7 +105,8 @@ int md_system_create(md_system** out, int n_atoms, const double box[3],
                      const double* charge, const double* mass, int precision,
                      int device);
 int md_system_destroy(md_system* sys);
-/* cudaStream_t passed as void*; NULL = the library's own stream. */
+/* cudaStream_t passed as void*; NULL = the library's own stream (to use the
+   legacy default stream, e.g. torch's default stream, pass cudaStreamLegacy). */
 int md_system_set_stream(md_system* sys, void* cuda_stream);
 int md_system_synchronize(md_system* sys);
 int md_system_num_atoms(const md_system* sys, int* out);

@@ -17,6 +17,7 @@
 // element-wise kernels; nothing returns to the host until asked.
 #include <cmath>
 #include <cstring>
+#include <algorithm>
 #include <vector>
 #include "device_common.cuh"
 
@@ -25,7 +26,12 @@ struct md_adapt_rcut {
   long nele = 0;
   int nrc = 0;
   std::vector<double> rc;
-  double box_tab[3] = {0, 0, 0};  // box the kernel tables were built for
+  // the box at construction: DensityProfile_PiecewiseConst::reinit,
+  // AdaptRCut::reinit and PressureCorrection::reinit take it once
+  // (ENG/src/DensityProfile.cu:22-43, ENG/src/AdaptRCut.cu:96-162,
+  // ENG/src/PressureCorrection.cu:41-54) and bin, build the kernel tables and
+  // normalise with it for the whole run, also when NPT moves the box
+  double box_tab[3] = {0, 0, 0};
   double* d_rc = nullptr;
   double* counts = nullptr;   // deposited atom counts per bin
   double* rho = nullptr;      // profile (calculate)
@@ -225,39 +231,94 @@ __global__ void k_arc_tables(ArcDims g, const double* rc, const double* ints, do
 // ------------------------------------------------------------ batched DFT
 // One block per line; lines of all `batch` arrays of the grid along `axis`.
 // out[k] = sum_j in[j] exp(sign 2 pi i jk/n), in place.  n <= 1024.
-__global__ void k_dft_axis(double2* data, ArcDims g, int axis, int sign, int batch) {
+// A block takes `per` lines of one axis (several short lines per block, so
+// that lanes are not idle on 41-point lines).  A line of composite length
+// n = n1 n2 (n1 its smallest prime factor) is transformed in two stages
+// (Cooley-Tukey: n2 inner DFTs of length n1, the twiddles W_n^{j2 k1}, n1
+// DFTs of length n2), n (n1 + n2) products instead of n^2; a prime length
+// is summed directly.  All factors come from one table of W_n^m.
+__global__ void k_dft_axis(double2* data, ArcDims g, int axis, int sign, int batch, int n1, int per) {
   extern __shared__ double2 sm[];
-  double2* line = sm;
-  double2* tw = sm + g.n[axis];
-  const int n = g.n[axis];
+  const int n = g.n[axis], n2 = n / n1;
+  double2* tw = sm;                  // [n]
+  double2* lines_sm = sm + n;        // [per][n] input, then stage-1 output
+  double2* tmp = lines_sm + per * n; // [per][n] stage-1 results (two-stage only)
   const long nele = (long)g.n[0] * g.n[1] * g.n[2];
   const int a1 = (axis + 1) % 3, a2 = (axis + 2) % 3;
   const long lines = (long)g.n[a1] * g.n[a2];
-  const long lid = blockIdx.x;
-  if (lid >= lines * batch) return;
-  const int b = (int)(lid / lines);
-  const long r = lid % lines;
-  const int i1 = (int)(r / g.n[a2]), i2 = (int)(r % g.n[a2]);
   const long stride[3] = {(long)g.n[1] * g.n[2], (long)g.n[2], 1};
-  double2* base = data + (long)b * nele + i1 * stride[a1] + i2 * stride[a2];
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
-    line[j] = base[j * stride[axis]];
     double s, c;
     sincospi(2.0 * j / n, &s, &c);
     tw[j] = make_double2(c, sign * s);
   }
+  // load the block's lines
+  double2* base[8];
+  for (int q = 0; q < per; ++q) {
+    const long lid = (long)blockIdx.x * per + q;
+    base[q] = nullptr;
+    if (lid < lines * batch) {
+      const int b = (int)(lid / lines);
+      const long r = lid % lines;
+      const int i1 = (int)(r / g.n[a2]), i2 = (int)(r % g.n[a2]);
+      base[q] = data + (long)b * nele + i1 * stride[a1] + i2 * stride[a2];
+    }
+  }
+  for (int t = threadIdx.x; t < per * n; t += blockDim.x) {
+    const int q = t / n, j = t - q * n;
+    lines_sm[t] = base[q] ? base[q][j * stride[axis]] : make_double2(0.0, 0.0);
+  }
   __syncthreads();
-  for (int kk = threadIdx.x; kk < n; kk += blockDim.x) {
-    double sr = 0, si = 0;
+  auto cmul_acc = [](double2& acc, const double2 x, const double2 w) {
+    acc.x += x.x * w.x - x.y * w.y;
+    acc.y += x.x * w.y + x.y * w.x;
+  };
+  if (n1 == n) {
+    for (int t = threadIdx.x; t < per * n; t += blockDim.x) {
+      const int q = t / n, kk = t - q * n;
+      if (!base[q]) continue;
+      const double2* line = lines_sm + q * n;
+      double2 acc = make_double2(0.0, 0.0);
+      int m = 0;
+      for (int j = 0; j < n; ++j) {
+        cmul_acc(acc, line[j], tw[m]);
+        m += kk;
+        if (m >= n) m -= n;
+      }
+      base[q][kk * stride[axis]] = acc;
+    }
+    return;
+  }
+  // stage 1: y[k1][j2] = W_n^{j2 k1} sum_j1 x[n2 j1 + j2] W_n1^{j1 k1}
+  for (int t = threadIdx.x; t < per * n; t += blockDim.x) {
+    const int q = t / n, r = t - q * n, k1 = r / n2, j2 = r - k1 * n2;
+    const double2* line = lines_sm + q * n;
+    double2 acc = make_double2(0.0, 0.0);
+    const int step = (k1 * n2) % n;  // W_n1^{k1} = W_n^{k1 n2}
     int m = 0;
-    for (int j = 0; j < n; ++j) {
-      const double2 x = line[j], w = tw[m];
-      sr += x.x * w.x - x.y * w.y;
-      si += x.x * w.y + x.y * w.x;
-      m += kk;
+    for (int j1 = 0; j1 < n1; ++j1) {
+      cmul_acc(acc, line[n2 * j1 + j2], tw[m]);
+      m += step;
       if (m >= n) m -= n;
     }
-    base[kk * stride[axis]] = make_double2(sr, si);
+    const double2 w = tw[(j2 * k1) % n];
+    tmp[q * n + r] = make_double2(acc.x * w.x - acc.y * w.y, acc.x * w.y + acc.y * w.x);
+  }
+  __syncthreads();
+  // stage 2: X[k1 + n1 k2] = sum_j2 y[k1][j2] W_n2^{j2 k2}
+  for (int t = threadIdx.x; t < per * n; t += blockDim.x) {
+    const int q = t / n, r = t - q * n, k1 = r % n1, k2 = r / n1;
+    if (!base[q]) continue;
+    const double2* y = tmp + q * n + k1 * n2;
+    double2 acc = make_double2(0.0, 0.0);
+    const int step = (k2 * n1) % n;  // W_n2^{k2} = W_n^{k2 n1}
+    int m = 0;
+    for (int j2 = 0; j2 < n2; ++j2) {
+      cmul_acc(acc, y[j2], tw[m]);
+      m += step;
+      if (m >= n) m -= n;
+    }
+    base[q][(k1 + n1 * k2) * stride[axis]] = acc;
   }
 }
 
@@ -326,8 +387,12 @@ int dft3_grid(double2* data, const int n[3], int sign, int batch, cudaStream_t s
       k_fft2_axis<<<(unsigned)lines, 128, smem, stream>>>(data, g, axis, sign, batch, logn);
       MD_CHECK_LAUNCH("fft axis");
     } else {
-      size_t smem = sizeof(double2) * 2 * na;
-      k_dft_axis<<<(unsigned)lines, 128, smem, stream>>>(data, g, axis, sign, batch);
+      int n1 = na;  // smallest prime factor
+      for (int f = 2; f * f <= na; ++f)
+        if (na % f == 0) { n1 = f; break; }
+      const int per = std::max(1, std::min(8, 128 / na));  // lines per block
+      size_t smem = sizeof(double2) * (na + 2 * (size_t)per * na);
+      k_dft_axis<<<(unsigned)((lines + per - 1) / per), 128, smem, stream>>>(data, g, axis, sign, batch, n1, per);
       MD_CHECK_LAUNCH("dft axis");
     }
   }
@@ -340,14 +405,14 @@ static int dft3(md_adapt_rcut* a, double2* data, int sign, int batch) {
 
 // ------------------------------------------------------------ element-wise kernels
 template <class R>
-__global__ void k_arc_deposit(int N, const typename V4<R>::T* pos, const DevState* st, ArcDims g, double* counts) {
+__global__ void k_arc_deposit(int N, const typename V4<R>::T* pos, ArcDims g, double* counts) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const typename V4<R>::T p = pos[i];
   const double c[3] = {(double)(float)p.x, (double)(float)p.y, (double)(float)p.z};
   unsigned b[3];
   for (int d = 0; d < 3; ++d) {
-    const double L = st->L[d];
+    const double L = g.box[d];  // the profile's box (fixed at construction)
     double tmp = c[d];
     if (c[d] >= L) tmp -= L; else if (c[d] < 0) tmp += L;
     const double h = L / g.n[d];
@@ -366,6 +431,12 @@ __global__ void k_arc_profile(long nele, const double* counts, double inv, doubl
   out[i] = make_double2(r, 0.0);
 }
 
+// The four products of each cutoff, s1k rho_k and i s2k_d rho_k (d = x, y, z),
+// are Hermitian (rho real, s1k real and even, s2k real and odd), so their
+// inverse transforms are real; they go two to a complex transform, A + i B,
+// whose real part is IFFT(A) and imaginary part IFFT(B):
+//   work[2c]     = s1k r + i (i s2k_x r) = (s1k - s2k_x) r
+//   work[2c + 1] = i s2k_y r + i (i s2k_z r) = (-s2k_z + i s2k_y) r
 __global__ void k_arc_multiply(long nele, int nrc, const double2* rhok, double scale, const double* s1k,
                                const double* s2k, double2* work) {
   long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -373,11 +444,11 @@ __global__ void k_arc_multiply(long nele, int nrc, const double2* rhok, double s
   const double2 r = make_double2(rhok[i].x * scale, rhok[i].y * scale);
   for (int c = 0; c < nrc; ++c) {
     const double s = s1k[(long)c * nele + i];
-    work[(long)(4 * c) * nele + i] = make_double2(r.x * s, r.y * s);
-    for (int d = 0; d < 3; ++d) {
-      const double b = s2k[((long)d * nrc + c) * nele + i];
-      work[(long)(4 * c + 1 + d) * nele + i] = make_double2(-r.y * b, r.x * b);
-    }
+    const double bx = s2k[((long)0 * nrc + c) * nele + i];
+    const double by = s2k[((long)1 * nrc + c) * nele + i];
+    const double bz = s2k[((long)2 * nrc + c) * nele + i];
+    work[(long)(2 * c) * nele + i] = make_double2(r.x * (s - bx), r.y * (s - bx));
+    work[(long)(2 * c + 1) * nele + i] = make_double2(-by * r.y - bz * r.x, by * r.x - bz * r.y);
   }
 }
 
@@ -385,10 +456,8 @@ __global__ void k_arc_error(long nele, int nrc, const double2* work, double Vi, 
   long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= nele) return;
   for (int c = 0; c < nrc; ++c) {
-    const double e1 = work[(long)(4 * c) * nele + i].x * Vi;
-    const double ex = work[(long)(4 * c + 1) * nele + i].x * Vi;
-    const double ey = work[(long)(4 * c + 2) * nele + i].x * Vi;
-    const double ez = work[(long)(4 * c + 3) * nele + i].x * Vi;
+    const double2 a = work[(long)(2 * c) * nele + i], b = work[(long)(2 * c + 1) * nele + i];
+    const double e1 = a.x * Vi, ex = a.y * Vi, ey = b.x * Vi, ez = b.y * Vi;
     error[(long)c * nele + i] = sqrt(e1 + ex * ex + ey * ey + ez * ez);
   }
 }
@@ -430,13 +499,17 @@ __global__ void k_arc_refine(ArcDims g, const int* in, int* out, const double* r
   rerr[i] = error[(long)m * nele + i];
 }
 
+// pck_aa rho_k is Hermitian (pck real and even): xx and yy of a cutoff share
+// one complex transform, (pck_xx + i pck_yy) r in work[c], zz is work[nrc + c]
 __global__ void k_pc_multiply(long nele, int nrc, const double2* rhok, double scale, const double* pck, double2* work) {
   long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= nele) return;
   const double2 r = make_double2(rhok[i].x * scale, rhok[i].y * scale);
-  for (int t = 0; t < 3 * nrc; ++t) {
-    const double kk = pck[(long)t * nele + i];
-    work[(long)t * nele + i] = make_double2(r.x * kk, r.y * kk);
+  for (int c = 0; c < nrc; ++c) {
+    const double kx = pck[((long)0 * nrc + c) * nele + i], ky = pck[((long)1 * nrc + c) * nele + i];
+    const double kz = pck[((long)2 * nrc + c) * nele + i];
+    work[(long)c * nele + i] = make_double2(kx * r.x - ky * r.y, kx * r.y + ky * r.x);
+    work[(long)(nrc + c) * nele + i] = make_double2(r.x * kz, r.y * kz);
   }
 }
 
@@ -455,7 +528,9 @@ __global__ void k_pc_reduce(long nele, int nrc, const double2* work, const int* 
   double v[3] = {0, 0, 0};
   if (i < nele) {
     const int c = idx[i];
-    for (int d = 0; d < 3; ++d) v[d] = 0.5 * work[((long)d * nrc + c) * nele + i].x * rho[i] * fac;
+    const double2 xy = work[(long)c * nele + i];
+    const double conv[3] = {xy.x, xy.y, work[(long)(nrc + c) * nele + i].x};
+    for (int d = 0; d < 3; ++d) v[d] = 0.5 * conv[d] * rho[i] * fac;
   }
   block_reduce_finish<3>(v, partials, counter, out, false);
 }
@@ -562,12 +637,13 @@ extern "C" int md_arc_get_dims(md_adapt_rcut* a, int n[3], int* nrc) {
 extern "C" int md_arc_deposit(md_adapt_rcut* a, md_system* sys) {
   if (!a || !sys) return MD_ERR_BADARG;
   ArcDims g;
-  for (int d = 0; d < 3; ++d) g.n[d] = a->n[d];
+  for (int d = 0; d < 3; ++d) { g.n[d] = a->n[d]; g.box[d] = a->box_tab[d]; }
+  g.nrc = a->nrc;
   int nb = ceil_div(sys->N, 256);
   if (sys->prec == MD_PREC_FP64)
-    k_arc_deposit<double><<<nb, 256, 0, a->sys->stream>>>(sys->N, (double4a*)sys->pos, sys->st, g, a->counts);
+    k_arc_deposit<double><<<nb, 256, 0, a->sys->stream>>>(sys->N, (double4a*)sys->pos, g, a->counts);
   else
-    k_arc_deposit<float><<<nb, 256, 0, a->sys->stream>>>(sys->N, (float4*)sys->pos, sys->st, g, a->counts);
+    k_arc_deposit<float><<<nb, 256, 0, a->sys->stream>>>(sys->N, (float4*)sys->pos, g, a->counts);
   MD_CHECK_LAUNCH("arc deposit");
   a->ndata++;
   return MD_OK;
@@ -595,19 +671,15 @@ extern "C" int md_arc_get_profile(md_adapt_rcut* a, double* rho) {
   return MD_OK;
 }
 
-// Kernel tables for the current box (rebuilt when the box changed),
 // DensityProfile::calculate (counts / (dv * ndata), or the explicit profile)
-// and the forward transform of the profile into rhok.
-static int arc_profile_transform(md_adapt_rcut* a, DevState& hs, const char* who) {
-  if (int r = a->sys->read_state(hs)) return r;
-  bool box_changed = false;
-  for (int d = 0; d < 3; ++d) box_changed |= fabs(hs.L[d] - a->box_tab[d]) > 1e-9 * a->box_tab[d];
-  if (box_changed)
-    if (int r = build_tables(a)) return r;
+// and the forward transform of the profile into rhok; bin volume and the
+// kernel tables are those of the construction box.
+static int arc_profile_transform(md_adapt_rcut* a, const char* who) {
   const long ne = a->nele;
   const int nb = (int)((ne + 255) / 256);
+  const double* B = a->box_tab;
   if (a->ndata > 0) {
-    double dv = (hs.L[0] / a->n[0]) * (hs.L[1] / a->n[1]) * (hs.L[2] / a->n[2]);
+    double dv = (B[0] / a->n[0]) * (B[1] / a->n[1]) * (B[2] / a->n[2]);
     k_arc_profile<<<nb, 256, 0, a->sys->stream>>>(ne, a->counts, 1.0 / (dv * a->ndata), a->rho, a->rhok);
   } else if (a->ndata < 0) {
     k_arc_profile<<<nb, 256, 0, a->sys->stream>>>(ne, nullptr, 0.0, a->rho, a->rhok);
@@ -622,14 +694,14 @@ static int arc_profile_transform(md_adapt_rcut* a, DevState& hs, const char* who
 extern "C" int md_arc_update(md_adapt_rcut* a, double prec, int nrefine) {
   if (!a || !(prec > 0) || nrefine < 0) { md_set_error("md_arc_update: bad arguments"); return MD_ERR_BADARG; }
   md_system* sys = a->sys;
-  DevState hs;
-  if (int r = arc_profile_transform(a, hs, "md_arc_update")) return r;
+  if (int r = arc_profile_transform(a, "md_arc_update")) return r;
   const long ne = a->nele;
   const int nb = (int)((ne + 255) / 256);
-  const double V = hs.L[0] * hs.L[1] * hs.L[2];
+  const double* B = a->box_tab;
+  const double V = B[0] * B[1] * B[2];
   k_arc_multiply<<<nb, 256, 0, a->sys->stream>>>(ne, a->nrc, a->rhok, V / ne, a->s1k, a->s2k, a->work);
   MD_CHECK_LAUNCH("arc multiply");
-  if (int r = dft3(a, a->work, +1, 4 * a->nrc)) return r;
+  if (int r = dft3(a, a->work, +1, 2 * a->nrc)) return r;
   k_arc_error<<<nb, 256, 0, a->sys->stream>>>(ne, a->nrc, a->work, 1.0 / V, a->error);
   k_arc_rcut<<<nb, 256, 0, a->sys->stream>>>(ne, a->nrc, a->d_rc, a->error, prec, a->rcut, a->rcidx, a->rerr);
   MD_CHECK_LAUNCH("arc rcut");
@@ -643,8 +715,8 @@ extern "C" int md_arc_update(md_adapt_rcut* a, double prec, int nrefine) {
   // PressureCorrection::correction on the same profile and rc map
   k_pc_multiply<<<nb, 256, 0, a->sys->stream>>>(ne, a->nrc, a->rhok, V / ne, a->pck, a->work);
   MD_CHECK_LAUNCH("pc multiply");
-  if (int r = dft3(a, a->work, +1, 3 * a->nrc)) return r;
-  const double dv = (hs.L[0] / a->n[0]) * (hs.L[1] / a->n[1]) * (hs.L[2] / a->n[2]);
+  if (int r = dft3(a, a->work, +1, 2 * a->nrc)) return r;
+  const double dv = (B[0] / a->n[0]) * (B[1] / a->n[1]) * (B[2] / a->n[2]);
   if (nb > sys->max_partial_blocks) { md_set_error("partials buffer too small"); return MD_ERR_BADARG; }
   k_pc_carry<<<1, 32, 0, a->sys->stream>>>(a->pcorr, 1.0 / V);
   MD_CHECK_LAUNCH("pc carry");
@@ -839,11 +911,10 @@ extern "C" int md_fcorr_get_profile(md_fcorr* f, double* rho) {
 extern "C" int md_fcorr_update(md_fcorr* f) {
   if (!f) return MD_ERR_BADARG;
   md_adapt_rcut* a = f->arc;
-  DevState hs;
-  if (int r = arc_profile_transform(a, hs, "md_fcorr_update")) return r;
+  if (int r = arc_profile_transform(a, "md_fcorr_update")) return r;
   const long ne = a->nele;
   const int nb = (int)((ne + 255) / 256);
-  const double V = hs.L[0] * hs.L[1] * hs.L[2];
+  const double V = a->box_tab[0] * a->box_tab[1] * a->box_tab[2];
   k_fc_multiply<<<nb, 256, 0, a->sys->stream>>>(ne, a->rhok, V / ne, a->s2k, a->work);
   MD_CHECK_LAUNCH("fcorr multiply");
   if (int r = dft3(a, a->work, +1, 3)) return r;

@@ -48,6 +48,9 @@ NB_NULL, NB_LJ6_12, NB_LJ6_12_CAP, NB_COSTAIL, NB_COSTAIL_CAP, NB_LJ6_12B, NB_LJ
 ANGLE_HARMONIC, ANGLE_COS0 = 20000, 20001
 STAT_COUNT = 16
 
+# cudaStreamLegacy (cuda_runtime_api.h): the legacy default stream as an explicit handle
+CUDA_STREAM_LEGACY = 0x1
+
 
 class MDException(RuntimeError):
     code = -1
@@ -155,7 +158,18 @@ class MDSystem:
             self.h = None
 
     def set_stream(self, stream_ptr):
-        check(lib.md_system_set_stream(self.h, C.c_void_p(stream_ptr)), "set_stream")
+        """Issue the system's device work on the CUDA stream with this handle
+        (e.g. torch's `Stream.cuda_stream`).  0, the handle torch gives its
+        default stream, means the legacy default stream and is passed as
+        cudaStreamLegacy, since a NULL handle selects the library's own
+        stream; None goes back to the library's own stream."""
+        if stream_ptr is None:
+            h = None
+        elif int(stream_ptr) == 0:
+            h = CUDA_STREAM_LEGACY
+        else:
+            h = int(stream_ptr)
+        check(lib.md_system_set_stream(self.h, C.c_void_p(h)), "set_stream")
 
     def synchronize(self):
         check(lib.md_system_synchronize(self.h), "synchronize")

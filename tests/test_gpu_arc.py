@@ -102,3 +102,43 @@ def test_pressure_correction_carries_previous_value(mdf, orc, small):
     assert np.allclose(p1, o1, rtol=1e-6)
     assert np.allclose(p2, o1 / V + o2, rtol=1e-6)
     assert not np.allclose(p2, o2, rtol=1e-12, atol=0)  # the carried share is there
+
+
+def test_box_fixed_at_construction(mdf, orc, small):
+    """DensityProfile_PiecewiseConst, AdaptRCut and PressureCorrection take the
+    box once at reinit (ENG/src/DensityProfile.cu:22-43, ENG/src/AdaptRCut.cu:
+    96-162, ENG/src/PressureCorrection.cu:41-54) and keep it when NPT moves the
+    box: after the system's box changes, the kernel tables, the deposit bins,
+    the profile normalisation and the estimate are those of the first box."""
+    sys, box = small
+    pos0 = sys.positions()
+    arc = mdf.AdaptRCutEstimator(sys, refh=4.0, rcmin=2.5, rcmax=5.0, rcstep=0.5)
+    n = arc.n
+    t0 = arc.tables()
+    try:
+        new_box = box * np.array([1.0, 1.0, 1.03])
+        sys.set_box(new_box)
+        # deposit: binned and wrapped with the construction box
+        arc.clearData()
+        arc.deposite()
+        pos = sys.positions().astype(np.float32)
+        counts = orc.dp_deposit(pos, box, n)
+        dv = np.prod(box / np.array(n))
+        rho = slab_profile(n)
+        arc.set_profile(rho)
+        arc.update(4e-3)
+        t1 = arc.tables()
+        for a, b in zip(t0, t1):
+            assert np.array_equal(a, b)
+        o = orc.adapt_rcut(box, n, arc.rc_list, rho, 4e-3)
+        rc, _, _ = arc.rcut()
+        assert np.array_equal(rc, o["rcut"])
+        assert np.allclose(arc.pressure_correction(), o["pcorr"], rtol=1e-6)
+        # the deposit above, normalised with the construction box
+        arc.clearData()
+        arc.deposite()
+        arc.update(4e-3)
+        assert np.allclose(arc.profile(), counts / dv)
+    finally:
+        sys.set_box(box)
+        sys.set_positions(pos0)
