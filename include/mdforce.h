@@ -197,6 +197,9 @@ int md_cell_list_get_cell_index(md_cell_list* cl, md_system* sys, uint32_t* cell
 int md_nlist_create(md_nlist** out, md_system* sys, double rlist, double skin,
                     double expansion, int mode);
 int md_nlist_destroy(md_nlist* nl);
+/* Builds from the cell list as last rebuilt: call md_cell_list_rebuild after the
+   positions change and before this (as the reference app rebuilds clist before
+   nlist); the build also uses each cell's z order taken at that rebuild. */
 int md_nlist_rebuild(md_nlist* nl, md_system* sys, md_cell_list* cl);
 /* Rebuild, and if any list overflowed grow the capacity to fit and rebuild
    again (host resize-and-retry of MD_ERR_NLIST_OVERFLOW). */
