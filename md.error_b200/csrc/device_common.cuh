@@ -122,8 +122,8 @@ __device__ __forceinline__ u32x4 philox4x32_10(u32x4 ctr, uint32_t k0, uint32_t 
   }
   return ctr;
 }
-// four standard normals (Box-Muller on the two 32-bit pairs), FP64 math so
-// that both precisions draw the same numbers
+// four standard normals (Box-Muller on the two 32-bit pairs) in FP64, for
+// the FP64 path (the mixed path draws from the same Philox block in binary32)
 __device__ __forceinline__ void normals4(uint64_t seed, uint64_t step, uint32_t id, double out[4]) {
   u32x4 c{id, (uint32_t)step, (uint32_t)(step >> 32), 0x6d646672u};
   u32x4 r = philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
