@@ -181,13 +181,23 @@ __device__ __forceinline__ void lv_particle_step1(int k, typename V4<R>::T* __re
 // Closing B(dt/2) (kick = 0: no kick, used to prime the pressure), kinetic
 // tensor; the last block computes P, gives the box momentum its half kick
 // (with_box) and, with advance, runs box_advance for the next step.
+// With nb_rows, the non-bonded kernel's statistics rows (one row of 5 sums
+// per warp, nnb rows) are summed here too: thread k takes rows k, k + grid,
+// ... in that order, and the rows' totals reach the slots NB_ENERGY,
+// VIRIAL_XX..ZZ, ELEC_DIR (stored with nb_store, else added) before the
+// reciprocal terms are merged and the pressure is formed.
 template <class R>
 __global__ void __launch_bounds__(256)
 k_lv_step2(int N, typename V4<R>::T* __restrict__ vel, double4a* __restrict__ force,
            DevState* st, LvDev p, double* partials, int with_box, int kick, int advance,
-           const double4a* __restrict__ fadd, int merge_rec) {
+           const double4a* __restrict__ fadd, int merge_rec, const double* __restrict__ nb_rows, int nnb,
+           int nb_store) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  double kin[3] = {0, 0, 0};
+  double kin[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (nb_rows)
+    for (int r = k; r < nnb; r += gridDim.x * blockDim.x)
+#pragma unroll
+      for (int q = 0; q < 5; ++q) kin[3 + q] += nb_rows[(size_t)r * 5 + q];
   if (k < N) {
     typename V4<R>::T v = vel[k];
     double4a f = force[k];
@@ -208,8 +218,18 @@ k_lv_step2(int N, typename V4<R>::T* __restrict__ vel, double4a* __restrict__ fo
     kin[1] = 0.5 * m * (double)v.y * (double)v.y;
     kin[2] = 0.5 * m * (double)v.z * (double)v.z;
   }
-  const bool last = block_reduce_finish<3>(kin, partials, &st->red_counter[RED_KIN],
-                                           &st->stats[MD_STAT_KINETIC_XX], true);
+  bool last;
+  if (nb_rows) {
+    last = block_reduce_finish<8>(kin, partials, &st->red_counter[RED_KIN], st->kick_sums, true);
+    if (last) {
+      for (int d = 0; d < 3; ++d) st->stats[MD_STAT_KINETIC_XX + d] = st->kick_sums[d];
+      for (int q = 0; q < 5; ++q)
+        st->stats[MD_STAT_NB_ENERGY + q] = (nb_store ? 0.0 : st->stats[MD_STAT_NB_ENERGY + q]) + st->kick_sums[3 + q];
+    }
+  } else {
+    double kin3[3] = {kin[0], kin[1], kin[2]};
+    last = block_reduce_finish<3>(kin3, partials, &st->red_counter[RED_KIN], &st->stats[MD_STAT_KINETIC_XX], true);
+  }
   if (last && merge_rec) {
     // reciprocal energy into its slot, its diagonal virial added to the virial slots
     st->stats[MD_STAT_ELEC_REC] = st->scratch[0];
@@ -254,12 +274,15 @@ int langevin_step1_impl(md_system* sys, md_nlist* nl, Recorder* rec, bool with_b
   return rec_launch(rec, f, dim3(ceil_div(N, MD_LV_THREADS)), dim3(MD_LV_THREADS), 0, a);
 }
 
-int langevin_step2_impl(md_system* sys, Recorder* rec, int kick, int advance, const double4a* fadd, int merge_rec) {
+int langevin_step2_impl(md_system* sys, Recorder* rec, int kick, int advance, const double4a* fadd, int merge_rec,
+                        int nb_rows, int nb_store) {
   LvDev p = make_lv(sys, nullptr);
   DevState* st = sys->st;
   int N = sys->N;
   int with_box = 1;
-  void* a[] = {&N, &sys->vel, &sys->force, &st, &p, &sys->partials, &with_box, &kick, &advance, &fadd, &merge_rec};
+  const double* rows = nb_rows > 0 ? sys->nb_rows : nullptr;
+  void* a[] = {&N, &sys->vel, &sys->force, &st, &p, &sys->partials, &with_box, &kick, &advance, &fadd, &merge_rec,
+               &rows, &nb_rows, &nb_store};
   const void* f = sys->prec == MD_PREC_FP64 ? (const void*)k_lv_step2<double> : (const void*)k_lv_step2<float>;
   return rec_launch(rec, f, dim3(ceil_div(N, MD_LV_THREADS)), dim3(MD_LV_THREADS), 0, a);
 }
@@ -300,10 +323,10 @@ extern "C" int md_vv_step2(md_system* sys, double dt, int with_stats) {
   (void)with_stats;
   if (sys->prec == MD_PREC_FP64)
     k_lv_step2<double><<<nb, 256, 0, sys->stream>>>(N, (double4a*)sys->vel, sys->force, st, p, sys->partials, 0, 1, 0,
-                                                     nullptr, 0);
+                                                     nullptr, 0, nullptr, 0, 0);
   else
     k_lv_step2<float><<<nb, 256, 0, sys->stream>>>(N, (float4*)sys->vel, sys->force, st, p, sys->partials, 0, 1, 0,
-                                                    nullptr, 0);
+                                                    nullptr, 0, nullptr, 0, 0);
   MD_CHECK_LAUNCH("vv step2");
   return MD_OK;
 }

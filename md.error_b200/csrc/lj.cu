@@ -15,6 +15,7 @@
 // The plain LJ case (one type, no charges) runs its pair arithmetic branch
 // free, two entries per packed binary32 (f32x2) instruction, with the same
 // binary32 criterion.
+#include <algorithm>
 #include <cmath>
 #include <type_traits>
 #include <vector>
@@ -181,6 +182,39 @@ __device__ __forceinline__ R typed_pair(const V& A, const V& B, const V& C, R r2
   }
   e = R(0);
   return R(0);
+}
+
+// Statistics of the non-bonded kernels: each warp reduces its lanes' sums
+// (shuffles in a fixed order) and lane 0 writes them as one row of
+// rows[row][NV], row = warp index in the grid; k_rows_finish (a small grid),
+// or in the driver the step's closing kick, sums the rows in a fixed order
+// into the statistics slots.  A per-block reduction inside the force kernel
+// needed a block barrier, a fence and an atomic per block and a last-block
+// pass: 13 us of a 62 us launch on the 65,536-atom slab.
+template <int NV>
+__device__ __forceinline__ void warp_rows_out(double (&v)[NV], double* __restrict__ rows) {
+  warp_sum<NV>(v);
+  if ((threadIdx.x & 31) == 0) {
+    const size_t r = (size_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+#pragma unroll
+    for (int k = 0; k < NV; ++k) rows[r * NV + k] = v[k];
+  }
+}
+
+// The rows added up by a small grid: thread g sums rows g, g + G, ... (G the
+// grid's threads), then the blocks combine by the deterministic last-block
+// reduction; out[k] is stored (store) or added to.
+template <int NV>
+__global__ void __launch_bounds__(256) k_rows_finish(int nrows, const double* __restrict__ rows,
+                                                     double* __restrict__ out, int store, double* partials,
+                                                     unsigned* counter) {
+  double acc[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] += rows[(size_t)r * NV + k];
+  block_reduce_finish<NV>(acc, partials, counter, out, store != 0);
 }
 
 // ---------------------------------------------------------------- mixed
@@ -453,10 +487,12 @@ k_lj_mixed(int N, const float4* __restrict__ pos, const float* __restrict__ rcut
     force[i] = f;
   }
   if (STATS) {
-    // slots NB_ENERGY, VIRIAL_XX..ZZ, ELEC_DIR are contiguous; the first force
-    // term of a step (overwrite) stores them, later terms add
+    // one row of sums per warp; k_rows_finish, or the driver's closing kick,
+    // adds the rows up into the slots NB_ENERGY, VIRIAL_XX..ZZ, ELEC_DIR
+    // (stored by the first force term of a step, overwrite, added by later
+    // terms)
     double v[5] = {0.5 * (double)e, 0.5 * (double)vx, 0.5 * (double)vy, 0.5 * (double)vz, 0.5 * (double)ec};
-    block_reduce_finish<5>(v, partials, counter, stats, overwrite != 0);
+    warp_rows_out<5>(v, partials);
   }
 }
 
@@ -554,8 +590,7 @@ k_lj_fp64(int N, const double4a* __restrict__ pos, const float* __restrict__ rcu
   }
   if (STATS) {
     double v[5] = {0.5 * e, 0.5 * vx, 0.5 * vy, 0.5 * vz, 0.5 * ec};
-    // the first force term of a step (overwrite) stores the slots, later terms add
-    block_reduce_finish<5>(v, partials, counter, stats, overwrite != 0);
+    warp_rows_out<5>(v, partials);
   }
 }
 
@@ -595,8 +630,10 @@ static void cap_radius(bool bform, T eps, T sig, T shift, T rcut, T cap, T& capR
   pcapR = bform ? eps * (sri6 * sri6 - T(2) * sri6 + shift) : T(4) * eps * (sri6 * sri6 - sri6) + shift;
 }
 
+// finish_stats = false: the statistics stay as rows in sys->nb_rows for the
+// step's closing kick to add up (lj_stat_rows rows)
 int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats, bool overwrite,
-                  Recorder* rec) {
+                  Recorder* rec, bool finish_stats) {
   if (!eng->has_lj) { md_set_error("no non-bonded interaction registered"); return MD_ERR_BADARG; }
   LJParams p;
   p.eps4 = 4.0 * eng->eps;
@@ -616,7 +653,11 @@ int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats,
   int ow = overwrite ? 1 : 0;
   const int threads = MD_LJ_THREADS;
   dim3 grid(ceil_div((long long)N * kLanes, threads));
-  if ((int)grid.x > sys->max_partial_blocks) { md_set_error("partials buffer too small"); return MD_ERR_BADARG; }
+  // one row of 5 statistics per warp in sys->nb_rows
+  if ((long long)grid.x * (threads / 32) > (long long)N / 4 + 1024) {
+    md_set_error("statistics rows buffer too small");
+    return MD_ERR_BADARG;
+  }
   DevState* st = sys->st;
   unsigned* counter = &st->red_counter[RED_LJ];
   double* stats = &st->stats[MD_STAT_NB_ENERGY];
@@ -710,7 +751,7 @@ int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats,
   const uint8_t* type = sys->type;
   const void* ptab = eng->d_tab;
   void* a[] = {&N, &sys->pos, &sys->rcut, &nl->list, &nl->nnb, &cap, &st, &p, &sys->force, &ow,
-               &sys->partials, &counter, &stats, &corr, &sys->id, &type, &ptab, &nt};
+               &sys->nb_rows, &counter, &stats, &corr, &sys->id, &type, &ptab, &nt};
   const void* f;
 #define LJ_PICK(K, T)                                                                       \
   (coul ? (with_stats ? (const void*)K<kLanes, true, true, T> : (const void*)K<kLanes, false, true, T>) \
@@ -718,7 +759,15 @@ int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats,
   if (sys->prec == MD_PREC_FP64) f = typed ? LJ_PICK(k_lj_fp64, true) : LJ_PICK(k_lj_fp64, false);
   else f = typed ? LJ_PICK(k_lj_mixed, true) : LJ_PICK(k_lj_mixed, false);
 #undef LJ_PICK
-  return rec_launch(rec, f, grid, dim3(threads), 0, a);
+  if (int r = rec_launch(rec, f, grid, dim3(threads), 0, a)) return r;
+  if (!with_stats || !finish_stats) return MD_OK;
+  int nrows = (int)grid.x * (threads / 32);
+  void* b[] = {&nrows, &sys->nb_rows, &stats, &ow, &sys->partials, &counter};
+  return rec_launch(rec, (const void*)k_rows_finish<5>, dim3(std::min(64, ceil_div(nrows, 256))), dim3(256), 0, b);
+}
+
+int lj_stat_rows(const md_system* sys) {
+  return ceil_div((long long)sys->N * kLanes, MD_LJ_THREADS) * (MD_LJ_THREADS / 32);
 }
 
 // ElectrostaticInteraction_dir: real-space Ewald with splitting beta inside the

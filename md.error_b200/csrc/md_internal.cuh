@@ -58,6 +58,7 @@ struct DevState {
   double lam1[3], lam2[3]; // scale factors of the two A half steps of this step
   double Pcur[3];    // diagonal pressure at the end of the last step
   double scratch[8]; // reduction target of multi-slot sums merged afterwards
+  double kick_sums[8]; // closing kick: kinetic tensor and the non-bonded statistics rows
   double Lnext[3];   // box of the next step, committed by that step's first kernel
   int box_pending;
   int pad1;
@@ -105,6 +106,7 @@ struct md_system {
   float* t_rcut = nullptr;
   DevState* st = nullptr;   // device state
   double* partials = nullptr;  // block partial sums for reductions
+  double* nb_rows = nullptr;   // non-bonded statistics, one row of 5 sums per warp
   int max_partial_blocks = 0;
   // pinned host staging
   void* h_stage = nullptr;
@@ -199,7 +201,9 @@ int rec_launch(Recorder* r, const void* func, dim3 grid, dim3 block, size_t smem
 // kernels entry points implemented in the .cu files -------------------------
 int cells_rebuild_impl(md_cell_list* cl, md_system* sys, Recorder* rec, bool conditional);
 int nlist_build_impl(md_nlist* nl, md_system* sys, md_cell_list* cl, Recorder* rec, bool conditional);
-int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats, bool overwrite, Recorder* rec);
+int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats, bool overwrite, Recorder* rec,
+                  bool finish_stats = true);
+int lj_stat_rows(const md_system* sys);
 // bonded terms (bonded.cu): slot map refresh after a cell sort, exclusion pass
 // after a list build, the bonded force kernel; each a no-op without topology
 void topo_destroy(md_topo* t);
@@ -214,9 +218,12 @@ int langevin_step1_impl(md_system* sys, md_nlist* nl, Recorder* rec, bool with_b
                         cudaGraphConditionalHandle cond, int use_cond);
 // fadd: per-atom force of a concurrent branch (SPME), added into the force
 // array by the closing kick; merge_rec: the branch's reciprocal energy and
-// virial (DevState::scratch) are merged into the statistics by its last block
+// virial (DevState::scratch) are merged into the statistics by its last block;
+// nb_rows > 0: the non-bonded statistics rows left in sys->nb_rows
+// (lj_apply_impl without finish_stats) are added up by the kick, stored into
+// their slots with nb_store, else added
 int langevin_step2_impl(md_system* sys, Recorder* rec, int kick, int advance, const double4a* fadd = nullptr,
-                        int merge_rec = 0);
+                        int merge_rec = 0, int nb_rows = 0, int nb_store = 0);
 int clear_stats_impl(md_system* sys, Recorder* rec, int first, int count);
 int nhc_vv1_impl(md_nhc* h, md_nlist* nl, double dt, Recorder* rec, cudaGraphConditionalHandle cond,
                  int use_cond);

@@ -108,7 +108,10 @@ static int record_step(md_sim* s, Recorder* rec, bool use_graph) {
   const bool branch = s->p.spme && !nhc;
   const cudaGraphNode_t fork = rec->last;
   const bool fork_has = rec->has_last;
-  if (int r = lj_apply_impl(s->eng, sys, s->nl, true, true, rec)) return r;
+  // the Langevin closing kick adds up the non-bonded statistics rows itself
+  // when nothing else adds to those slots in between (no bonded terms)
+  const bool defer = !nhc && !topo_has_terms(sys->topo);
+  if (int r = lj_apply_impl(s->eng, sys, s->nl, true, true, rec, !defer)) return r;
   if (int r = bonded_apply_impl(sys, rec, 1)) return r;
   if (s->p.spme) {
     const cudaGraphNode_t lj = rec->last;
@@ -124,7 +127,8 @@ static int record_step(md_sim* s, Recorder* rec, bool use_graph) {
     // removal and operator_L(dt/2), as a pending velocity map
     if (int r = nhc_vv2_impl(s->nhc, s->p.lv.dt, rec, 1, 1, 1, 1)) return r;
   } else {
-    if (int r = langevin_step2_impl(sys, rec, 1, 1, branch ? spme_force_buffer(s->p.spme) : nullptr, branch ? 1 : 0))
+    if (int r = langevin_step2_impl(sys, rec, 1, 1, branch ? spme_force_buffer(s->p.spme) : nullptr, branch ? 1 : 0,
+                                    defer ? lj_stat_rows(sys) : 0, 1))
       return r;
   }
   if (s->ring) {

@@ -314,6 +314,8 @@ extern "C" int md_system_create(md_system** out, int n, const double box[3], con
   ALLOC(s->st, sizeof(DevState));
   s->max_partial_blocks = ceil_div((long long)n * 32, 128) + 1024;
   ALLOC(s->partials, sizeof(double) * 8 * (size_t)s->max_partial_blocks);
+  // one row of 5 per warp of the non-bonded kernels (8 lanes per atom)
+  ALLOC(s->nb_rows, sizeof(double) * 5 * ((size_t)n / 4 + 1024));
   ALLOC(s->type_by_id, (size_t)n); ALLOC(s->type, (size_t)n);
 #undef ALLOC
   DevState hs;
@@ -359,7 +361,7 @@ extern "C" int md_system_destroy(md_system* s) {
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   void* ptrs[] = {s->pos, s->vel, s->force, s->image, s->id, s->rcut, s->t_pos, s->t_vel,
-                  s->t_force, s->t_image, s->t_id, s->t_rcut, s->st, s->partials, s->d_lattice,
+                  s->t_force, s->t_image, s->t_id, s->t_rcut, s->st, s->partials, s->nb_rows, s->d_lattice,
                   s->type_by_id, s->type};
   for (void* p : ptrs) if (p) cudaFree(p);
   topo_destroy(s->topo);
