@@ -246,12 +246,14 @@ def time_kernels(torch, mdf, sys_, eng, stream, reps=50):
     P = int(counts.sum())
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # the force kernel as the step runs it: statistics left as per-warp rows,
+    # which the step's closing kick adds up
     with torch.cuda.stream(stream):
         for _ in range(5):
-            eng.applyNonBondedInteraction(sys_, nl, with_stats=True)
+            eng.applyNonBondedInteraction(sys_, nl, with_stats="rows")
         a.record(stream)
         for _ in range(reps):
-            eng.applyNonBondedInteraction(sys_, nl, with_stats=True)
+            eng.applyNonBondedInteraction(sys_, nl, with_stats="rows")
         b.record(stream)
     torch.cuda.synchronize()
     t_lj = a.elapsed_time(b) / 1e3 / reps

@@ -283,8 +283,12 @@ int md_nlist_apply_exclusions(md_nlist* nl, md_system* sys);
 /* registBondedInteraction: checks that n_bonds bonds were given to md_engine_set_bonds. */
 int md_engine_register_bonded(md_engine* eng, int n_bonds);
 int md_engine_clear_forces(md_engine* eng, md_system* sys);
-/* with_stats != 0 accumulates energy and diagonal virial into the FP64 slots. */
+/* with_stats 1 accumulates energy and diagonal virial into the FP64 slots;
+   with_stats 2 runs the force kernel as the step driver does, leaving its
+   statistics as per-warp rows that md_engine_finish_nonbonded_stats adds into
+   the slots (the driver's closing kick adds them itself). */
 int md_engine_apply_nonbonded(md_engine* eng, md_system* sys, md_nlist* nl, int with_stats);
+int md_engine_finish_nonbonded_stats(md_engine* eng, md_system* sys);
 /* applyBondedInteraction with statistics: adds the bonded forces to the system's forces
    (after md_engine_apply_nonbonded), stores MD_STAT_BOND_ENERGY and adds the virial;
    nothing to do without bonds or angles. */

@@ -867,9 +867,21 @@ extern "C" int md_engine_clear_forces(md_engine* e, md_system* sys) {
 }
 
 extern "C" int md_engine_apply_nonbonded(md_engine* e, md_system* sys, md_nlist* nl, int with_stats) {
-  if (!e || !sys || !nl) return MD_ERR_BADARG;
+  if (!e || !sys || !nl || with_stats < 0 || with_stats > 2) return MD_ERR_BADARG;
   if (!nl->built) { md_set_error("neighbour list not built"); return MD_ERR_BADARG; }
   Recorder rec;
   rec.stream = sys->stream;
-  return lj_apply_impl(e, sys, nl, with_stats != 0, false, &rec);
+  return lj_apply_impl(e, sys, nl, with_stats != 0, false, &rec, with_stats != 2);
+}
+
+extern "C" int md_engine_finish_nonbonded_stats(md_engine* e, md_system* sys) {
+  if (!e || !sys) return MD_ERR_BADARG;
+  int nrows = lj_stat_rows(sys);
+  double* stats = &sys->st->stats[MD_STAT_NB_ENERGY];
+  unsigned* counter = &sys->st->red_counter[RED_LJ];
+  int store = 0;
+  k_rows_finish<5><<<std::min(64, ceil_div(nrows, 256)), 256, 0, sys->stream>>>(nrows, sys->nb_rows, stats, store,
+                                                                                 sys->partials, counter);
+  MD_CHECK_LAUNCH("non-bonded statistics");
+  return MD_OK;
 }

@@ -88,6 +88,7 @@ _SIGS = {
     "md_engine_register_bonded": (i32, [vp, i32]),
     "md_engine_clear_forces": (i32, [vp, vp]),
     "md_engine_apply_nonbonded": (i32, [vp, vp, vp, i32]),
+    "md_engine_finish_nonbonded_stats": (i32, [vp, vp]),
     "md_engine_apply_bonded": (i32, [vp, vp]),
     "md_engine_set_bonds": (i32, [vp, i32, P(i32), P(i32), P(f64)]),
     "md_engine_register_lj_pair": (i32, [vp, i32, i32, f64, f64, f64]),

@@ -426,8 +426,14 @@ class InteractionEngine:
         check(lib.md_engine_clear_forces(self.h, (sys or self.sys).h), "clearInteraction")
 
     def applyNonBondedInteraction(self, sys, nlist, with_stats=True):
-        check(lib.md_engine_apply_nonbonded(self.h, sys.h, nlist.h, 1 if with_stats else 0),
-              "applyNonBondedInteraction")
+        """with_stats True / False, or "rows": the force kernel as the step
+        driver runs it, its statistics left as per-warp rows for
+        finishNonBondedStatistics."""
+        mode = 2 if with_stats == "rows" else (1 if with_stats else 0)
+        check(lib.md_engine_apply_nonbonded(self.h, sys.h, nlist.h, mode), "applyNonBondedInteraction")
+
+    def finishNonBondedStatistics(self, sys):
+        check(lib.md_engine_finish_nonbonded_stats(self.h, sys.h), "finishNonBondedStatistics")
 
     def applyBondedInteraction(self, sys):
         check(lib.md_engine_apply_bonded(self.h, sys.h), "applyBondedInteraction")

@@ -412,3 +412,31 @@ def test_stats_ring_rows_match_stepwise_reads(mdf, fluid):
     sa.set_stats_ring(None)
     with pytest.raises(ValueError):
         sa.set_stats_ring(np.zeros((3, 4)))
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_statistics_rows_and_finish(mdf, small_slab, prec):
+    """with_stats="rows" is the force kernel as the step driver runs it (one row
+    of sums per warp, added up later); finishNonBondedStatistics adds the rows
+    into the slots exactly as the one-call form does."""
+    s = small_slab
+    sys = mdf.MDSystem(s.pos, s.box, precision=prec)
+    sys.set_rcut(adaptive_rcut(s.n, seed=3))
+    cl = mdf.CellList(sys, 2.8)
+    cl.rebuild()
+    nl = mdf.NeighborList(sys, 5.3, 0.3, expansion=3.0)
+    nl.fit(sys, cl)
+    eng = mdf.InteractionEngine(sys)
+    eng.registNonBondedInteraction(1.0, 1.0, 0.0)
+    out = []
+    for mode in (True, "rows"):
+        eng.clearInteraction()
+        sys.clear_stats()
+        eng.applyNonBondedInteraction(sys, nl, with_stats=mode)
+        if mode == "rows":
+            assert not np.any(sys.stats()[:5])  # nothing added yet
+            eng.finishNonBondedStatistics(sys)
+        out.append((sys.forces(), sys.stats()[:5]))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.any(out[0][1])
