@@ -77,13 +77,18 @@ __device__ __forceinline__ void lv_particle_step1_f32(int k, float4* __restrict_
                                                       const int* __restrict__ id,
                                                       const float4* __restrict__ backup, DevState* st,
                                                       const LvDev& p) {
+  // every load first, so that the thread waits for memory once
   float4 x = pos[k], v = vel[k];
   const double4a f = force[k];
+  const uint32_t aid = (uint32_t)id[k];
+  const float4 b = backup ? backup[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const unsigned long long step = st->step;
+  const float l1[3] = {(float)st->lam1[0], (float)st->lam1[1], (float)st->lam1[2]};
+  const float l2[3] = {(float)st->lam2[0], (float)st->lam2[1], (float)st->lam2[2]};
+  const double L[3] = {st->L[0], st->L[1], st->L[2]}, Li[3] = {st->Li[0], st->Li[1], st->Li[2]};
   const float im = v.w;
   const float h = (float)(0.5 * p.dt);
   float vx = v.x + h * (float)f.x * im, vy = v.y + h * (float)f.y * im, vz = v.z + h * (float)f.z * im;  // B
-  const float l1[3] = {(float)st->lam1[0], (float)st->lam1[1], (float)st->lam1[2]};
-  const float l2[3] = {(float)st->lam2[0], (float)st->lam2[1], (float)st->lam2[2]};
   // A
   x.x = l1[0] * x.x + h * vx; vx /= l1[0];
   x.y = l1[1] * x.y + h * vy; vy /= l1[1];
@@ -91,7 +96,7 @@ __device__ __forceinline__ void lv_particle_step1_f32(int k, float4* __restrict_
   // O
   float xi[3];
   {
-    u32x4 c{(uint32_t)id[k], (uint32_t)st->step, (uint32_t)(st->step >> 32), 0x6d646672u};
+    u32x4 c{aid, (uint32_t)step, (uint32_t)(step >> 32), 0x6d646672u};
     u32x4 r = philox4x32_10(c, (uint32_t)p.seed, (uint32_t)(p.seed >> 32));
     const float inv = 5.9604644775390625e-8f;  // 2^-24
     const float u1 = ((float)(r.a >> 8) + 0.5f) * inv, u2 = ((float)(r.b >> 8) + 0.5f) * inv;
@@ -116,10 +121,9 @@ __device__ __forceinline__ void lv_particle_step1_f32(int k, float4* __restrict_
   vel[k] = v;
   // Displacement_max: rebuild when |r - r_backup| > skin/2
   if (backup) {
-    const float4 b = backup[k];
-    const double dx = min_image_exact((double)x.x - (double)b.x, st->L[0], st->Li[0]);
-    const double dy = min_image_exact((double)x.y - (double)b.y, st->L[1], st->Li[1]);
-    const double dz = min_image_exact((double)x.z - (double)b.z, st->L[2], st->Li[2]);
+    const double dx = min_image_exact((double)x.x - (double)b.x, L[0], Li[0]);
+    const double dy = min_image_exact((double)x.y - (double)b.y, L[1], Li[1]);
+    const double dz = min_image_exact((double)x.z - (double)b.z, L[2], Li[2]);
     const double d2 = dx * dx + dy * dy + dz * dz;
     const bool far = d2 > p.skin_half2;
     const unsigned m = __ballot_sync(__activemask(), far);
@@ -138,21 +142,28 @@ __device__ __forceinline__ void lv_particle_step1(int k, typename V4<R>::T* __re
     lv_particle_step1_f32(k, pos, vel, force, id, backup, st, p);
     return;
   }
-  typename V4<R>::T x = pos[k], v = vel[k];
+  typedef typename V4<R>::T R4;
+  // every load first, so that the thread waits for memory once
+  R4 x = pos[k], v = vel[k];
   const double4a f = force[k];
+  const uint32_t aid = (uint32_t)id[k];
+  R4 b{};
+  if (backup) b = backup[k];
+  const unsigned long long step = st->step;
+  const double l1[3] = {st->lam1[0], st->lam1[1], st->lam1[2]};
+  const double l2[3] = {st->lam2[0], st->lam2[1], st->lam2[2]};
+  const double L[3] = {st->L[0], st->L[1], st->L[2]}, Li[3] = {st->Li[0], st->Li[1], st->Li[2]};
   const double im = (double)v.w;
   const double h = 0.5 * p.dt;
   double vx = v.x + h * f.x * im, vy = v.y + h * f.y * im, vz = v.z + h * f.z * im;  // B
   double rx = x.x, ry = x.y, rz = x.z;
-  const double l1[3] = {st->lam1[0], st->lam1[1], st->lam1[2]};
-  const double l2[3] = {st->lam2[0], st->lam2[1], st->lam2[2]};
   // A
   rx = l1[0] * rx + h * vx; vx /= l1[0];
   ry = l1[1] * ry + h * vy; vy /= l1[1];
   rz = l1[2] * rz + h * vz; vz /= l1[2];
   // O
   double xi[4];
-  normals4(p.seed, st->step, (uint32_t)id[k], xi);
+  normals4(p.seed, step, aid, xi);
   const double sd = p.c2 * sqrt(p.kT * im);
   vx = p.c1 * vx + sd * xi[0];
   vy = p.c1 * vy + sd * xi[1];
@@ -167,10 +178,9 @@ __device__ __forceinline__ void lv_particle_step1(int k, typename V4<R>::T* __re
   vel[k] = v;
   // Displacement_max: rebuild when |r - r_backup| > skin/2
   if (backup) {
-    const typename V4<R>::T b = backup[k];
-    const double dx = min_image_exact((double)x.x - (double)b.x, st->L[0], st->Li[0]);
-    const double dy = min_image_exact((double)x.y - (double)b.y, st->L[1], st->Li[1]);
-    const double dz = min_image_exact((double)x.z - (double)b.z, st->L[2], st->Li[2]);
+    const double dx = min_image_exact((double)x.x - (double)b.x, L[0], Li[0]);
+    const double dy = min_image_exact((double)x.y - (double)b.y, L[1], Li[1]);
+    const double dz = min_image_exact((double)x.z - (double)b.z, L[2], Li[2]);
     const double d2 = dx * dx + dy * dy + dz * dz;
     const bool far = d2 > p.skin_half2;
     const unsigned m = __ballot_sync(__activemask(), far);
@@ -193,16 +203,32 @@ k_lv_step2(int N, typename V4<R>::T* __restrict__ vel, double4a* __restrict__ fo
            const double4a* __restrict__ fadd, int merge_rec, const double* __restrict__ nb_rows, int nnb,
            int nb_store) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  // the atom's loads are issued before the rows are read
+  typename V4<R>::T v{};
+  double4a f{}, g{};
+  if (k < N) {
+    v = vel[k];
+    f = force[k];
+    if (fadd) g = fadd[k];
+  }
   double kin[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (nb_rows)
     for (int r = k; r < nnb; r += gridDim.x * blockDim.x)
 #pragma unroll
       for (int q = 0; q < 5; ++q) kin[3 + q] += nb_rows[(size_t)r * 5 + q];
+  // The box normals of the coming step do not depend on this step's sums:
+  // one thread of block 0 works them out beside the kick, off the serial
+  // tail of the last block.  Block 0 signs in at the reduction counter after
+  // this store (barrier, fence, atomic), so the last block sees it.
+  const bool pre_xi = with_box && advance && p.dirs;
+  if (pre_xi && blockIdx.x == 0 && threadIdx.x == (blockDim.x > 32 ? 32u : 0u)) {
+    double xi[4];
+    box_normals(p, st->step + 1ull, xi);
+    for (int d = 0; d < 3; ++d) st->box_xi[d] = xi[d];
+    __threadfence();
+  }
   if (k < N) {
-    typename V4<R>::T v = vel[k];
-    double4a f = force[k];
     if (fadd) {
-      const double4a g = fadd[k];
       f.x += g.x;
       f.y += g.y;
       f.z += g.z;
@@ -235,7 +261,12 @@ k_lv_step2(int N, typename V4<R>::T* __restrict__ vel, double4a* __restrict__ fo
     st->stats[MD_STAT_ELEC_REC] = st->scratch[0];
     for (int d = 0; d < 3; ++d) st->stats[MD_STAT_VIRIAL_XX + d] += st->scratch[1 + d];
   }
-  if (last && with_box) lv_close(st, p, kick, advance);
+  if (last && with_box) {
+    double xi[3];
+    if (pre_xi)
+      for (int d = 0; d < 3; ++d) xi[d] = __ldcg(&st->box_xi[d]);
+    lv_close(st, p, kick, advance, pre_xi ? xi : nullptr);
+  }
 }
 
 LvDev make_lv(const md_system* sys, const md_nlist* nl) {

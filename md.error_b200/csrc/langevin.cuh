@@ -27,16 +27,29 @@ __device__ __forceinline__ void box_commit(DevState* st) {
 // commit = false: the new box waits in Lnext until the particles of the step
 // are moved (k_lv_step1 commits it), so the box read between steps always
 // matches the positions
-__device__ __forceinline__ void box_advance(DevState* st, const LvDev& p, bool commit) {
+// The box's normals of step s are those of Philox counter (s, 0xffffffff)
+// under the seed with 0x5bd1e995 mixed in (box_normals).  xi_pre: the normals
+// of the coming step computed ahead by another thread, or null to compute
+// them here.
+__device__ __forceinline__ void box_normals(const LvDev& p, unsigned long long step, double xi[4]) {
+  normals4(p.seed ^ 0x5bd1e995ull, step, 0xffffffffu, xi);
+}
+
+__device__ __forceinline__ void box_advance(DevState* st, const LvDev& p, bool commit,
+                                            const double* xi_pre = nullptr) {
   const unsigned f = st->flags;
   if (f & FLAG_REBUILD) st->rebuilds += 1ull;
   // a forced rebuild (new cutoff lattice) becomes this step's rebuild
   st->flags = (f & ~(FLAG_REBUILD | FLAG_FORCE_REBUILD)) | ((f & FLAG_FORCE_REBUILD) ? FLAG_REBUILD : 0u);
   st->step += 1ull;
-  double xi[4];
-  normals4(p.seed ^ 0x5bd1e995ull, st->step, 0xffffffffu, xi);
   for (int d = 0; d < 3; ++d) { st->lam1[d] = 1.0; st->lam2[d] = 1.0; }
   if (!p.dirs) return;
+  double xi[4];
+  if (xi_pre) {
+    for (int d = 0; d < 3; ++d) xi[d] = xi_pre[d];
+  } else {
+    box_normals(p, st->step, xi);
+  }
   const double V = st->L[0] * st->L[1] * st->L[2];
   for (int d = 0; d < 3; ++d) st->Lnext[d] = st->L[d];
   for (int d = 0; d < 3; ++d) {
@@ -62,7 +75,8 @@ __device__ __forceinline__ void box_advance(DevState* st, const LvDev& p, bool c
 // P_dd = 2/V (K_dd - W_dd/2) + tail correction (MDStatistic::pressureXX), the
 // box momentum's closing half kick (kick) and, with advance, the box part of
 // the next step's B A O A.
-__device__ __forceinline__ void lv_close(DevState* st, const LvDev& p, int kick, int advance) {
+__device__ __forceinline__ void lv_close(DevState* st, const LvDev& p, int kick, int advance,
+                                         const double* xi_pre = nullptr) {
   const double V = st->L[0] * st->L[1] * st->L[2];
   for (int d = 0; d < 3; ++d) {
     const double W = st->stats[MD_STAT_VIRIAL_XX + d];
@@ -70,7 +84,7 @@ __device__ __forceinline__ void lv_close(DevState* st, const LvDev& p, int kick,
     st->Pcur[d] = 2.0 / V * (K - 0.5 * W) + st->stats[MD_STAT_PRESSURE_CORR_XX + d];
     if (kick && (p.dirs & (1 << d))) st->ph[d] += 0.5 * p.dt * V / st->L[d] * (st->Pcur[d] - p.pref[d]);
   }
-  if (advance) box_advance(st, p, false);
+  if (advance) box_advance(st, p, false, xi_pre);
 }
 
 // integrator constants of the system's Langevin parameters (nl: list skin

@@ -60,6 +60,7 @@ struct DevState {
   double scratch[8]; // reduction target of multi-slot sums merged afterwards
   double kick_sums[8]; // closing kick: kinetic tensor and the non-bonded statistics rows
   double Lnext[3];   // box of the next step, committed by that step's first kernel
+  double box_xi[4];  // the box normals of the coming step, computed ahead in the closing kick
   int box_pending;
   int pad1;
 };
