@@ -527,6 +527,25 @@ int md_sim_run(md_sim* sim, int nsteps);
 int md_sim_counters(md_sim* sim, int64_t* steps, int64_t* rebuilds, int* device_flags);
 /* 1 when the step graph skips the rebuild chain with a device-side conditional node */
 int md_sim_uses_conditional_graph(md_sim* sim, int* out);
+/* How a step decides on the device whether to rebuild the cell and neighbour
+   lists (the reference decides on the host after reading the displacement
+   back, ENG/app/lj.nhc-xtc.cu:193-205):
+     MD_REBUILD_FUSED        one cooperative kernel (cell sort, per-slot types,
+                             list build) that returns at once unless the
+                             device's rebuild flag is set; used whenever the
+                             device supports cooperative launches and the
+                             system has no bonded topology
+     MD_REBUILD_CONDITIONAL  the chain of kernels under a conditional node of
+                             the step graph
+     MD_REBUILD_GATED        the chain of kernels, each returning at once
+                             unless the flag is set (no graph) */
+enum { MD_REBUILD_GATED = 0, MD_REBUILD_CONDITIONAL = 1, MD_REBUILD_FUSED = 2 };
+int md_sim_rebuild_kind(md_sim* sim, int* out);
+/* MD_REBUILD_FUSED (the default, where the device can) or
+   MD_REBUILD_CONDITIONAL: the chain of kernels, under a conditional node when
+   the step is a graph (gated launches otherwise).  Both give the same lists
+   and trajectories bit for bit. */
+int md_sim_set_rebuild_kind(md_sim* sim, int kind);
 /* MD_INTEG_NHC runs: md_nhc_get_state of the driver's chain (after the pending
    start-of-step half of the next step) */
 int md_sim_get_nhc_state(md_sim* sim, double out[5]);

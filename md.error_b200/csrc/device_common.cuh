@@ -44,6 +44,47 @@ __device__ __forceinline__ void warp_sum(double (&v)[NV]) {
 // thread 0 stores the block partial; the last block to finish sums the partials
 // in block order (fixed, hence bit-reproducible) and adds them into out[k]
 // (or stores when `store`).  `counter` is reset by the last block.
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Barrier over every block of a cooperative launch (all blocks resident).
+// The last block to arrive resets the count and advances the generation the
+// others wait on.  A wait is bounded: past 4 s the block sets FLAG_TIMEOUT and
+// the call returns false, and the caller leaves the kernel (the other blocks'
+// waits then end the same way).
+__device__ __forceinline__ bool grid_barrier(DevState* st) {
+  __shared__ int gb_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = &st->gbar_gen;
+    const unsigned g0 = *gen;
+    __threadfence();
+    int ok = 1;
+    if (atomicAdd(&st->gbar_count, 1u) == gridDim.x - 1) {
+      st->gbar_count = 0u;
+      __threadfence();
+      atomicAdd(&st->gbar_gen, 1u);
+    } else {
+      const unsigned long long t0 = global_ns();
+      while (*gen == g0) {
+        if (global_ns() - t0 > 4000000000ull) {
+          atomicOr(&st->flags, FLAG_TIMEOUT);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    gb_ok = ok;
+  }
+  __syncthreads();
+  return gb_ok != 0;
+}
+
 template <int NV>
 __device__ bool block_reduce_finish(double (&v)[NV], double* partials, unsigned* counter,
                                     double* out, bool store) {

@@ -37,7 +37,8 @@ enum : unsigned {
 };
 
 // reduction counters (one per kind of last-block reduction)
-enum { RED_LJ = 0, RED_KIN = 1, RED_DISP = 2, RED_SPME = 3, RED_MISC = 4, RED_BOND = 5 /* and 6 */, RED_COUNT = 8 };
+enum { RED_LJ = 0, RED_KIN = 1, RED_DISP = 2, RED_SPME = 3, RED_MISC = 4, RED_BOND = 5 /* and 6 */,
+       RED_NLWORK = 7 /* home cells handed out by the fused rebuild */, RED_COUNT = 8 };
 
 struct DevState {
   double L[3];       // box edge, FP64 master copy
@@ -62,7 +63,11 @@ struct DevState {
   double Lnext[3];   // box of the next step, committed by that step's first kernel
   double box_xi[4];  // the box normals of the coming step, computed ahead in the closing kick
   int box_pending;
-  int pad1;
+  unsigned gbar_count;  // grid barrier of the fused rebuild: blocks arrived
+  unsigned gbar_gen;    // and its generation
+  unsigned ncell_busy;  // home cells of 4 atoms or more listed by the fused rebuild
+  unsigned ncell_light; // and of 1 to 3 atoms
+  unsigned pad1;
 };
 
 // host helpers -------------------------------------------------------------
@@ -146,6 +151,7 @@ struct md_cell_list {
   // the slots of each cell ordered by z: zord[start[c] .. start[c+1]) (the list
   // build reads runs of cells in this order to cut each atom's z window exactly)
   uint32_t* zord = nullptr;
+  uint32_t* busy = nullptr;        // the fused rebuild's non-empty cells: the fuller ones from the front, the rest from the back
   bool built = false;
 };
 
@@ -198,10 +204,20 @@ struct Recorder {
   cudaStream_t stream = nullptr;
 };
 int rec_launch(Recorder* r, const void* func, dim3 grid, dim3 block, size_t smem, void** args);
+// the same as a cooperative launch (every block resident at once)
+int rec_launch_coop(Recorder* r, const void* func, dim3 grid, dim3 block, size_t smem, void** args);
 
 // kernels entry points implemented in the .cu files -------------------------
 int cells_rebuild_impl(md_cell_list* cl, md_system* sys, Recorder* rec, bool conditional);
 int nlist_build_impl(md_nlist* nl, md_system* sys, md_cell_list* cl, Recorder* rec, bool conditional);
+// The cell sort, the per-slot types and the list build as one cooperative
+// kernel that returns at once unless the device's rebuild flag is set (no
+// bonded topology: its slot map and exclusions stay separate kernels).
+// with_lv: the same kernel opens with the Langevin particle B A O A and the
+// displacement test of k_lv_step1, whose work it replaces.
+// rebuild_fused_ok tells whether the device can run it for this system.
+bool rebuild_fused_ok(const md_system* sys, const md_nlist* nl);
+int rebuild_fused_impl(md_cell_list* cl, md_nlist* nl, md_system* sys, Recorder* rec, bool with_lv);
 int lj_apply_impl(md_engine* eng, md_system* sys, md_nlist* nl, bool with_stats, bool overwrite, Recorder* rec,
                   bool finish_stats = true);
 int lj_stat_rows(const md_system* sys);

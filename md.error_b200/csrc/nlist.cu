@@ -23,7 +23,8 @@
 #include <cmath>
 #include <cstring>
 #include <type_traits>
-#include "device_common.cuh"
+#include "cells_dev.cuh"
+#include "langevin.cuh"
 
 struct NlGeom {
   int nc[3];
@@ -57,21 +58,23 @@ template <class R> __device__ __forceinline__ int slot_of_w(R w);
 template <> __device__ __forceinline__ int slot_of_w<float>(float w) { return __float_as_int(w); }
 template <> __device__ __forceinline__ int slot_of_w<double>(double w) { return (int)__double_as_longlong(w); }
 
+// The lists of the atoms of home cell c, by one block of 8 warps.  Every
+// exit is uniform over the block; the shared state is first written after a
+// block barrier, so a block may run this for one cell after another.
 template <class R, int MODE>
-__global__ void __launch_bounds__(256, 4)
-k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __restrict__ rcut,
-           const uint32_t* __restrict__ start, const uint32_t* __restrict__ zord, NlGeom g,
-           const DevState* __restrict__ st, double rlist_uniform, double skin, int cap, int* __restrict__ list,
-           int* __restrict__ nnb, typename V4<R>::T* __restrict__ backup, int force_minimage, DevState* stw,
-           int gate) {
+__device__ __forceinline__ void nl_build_cell(int c, const typename V4<R>::T* __restrict__ pos,
+                                              const float* __restrict__ rcut, const uint32_t* __restrict__ start,
+                                              const uint32_t* __restrict__ zord, NlGeom g,
+                                              const DevState* __restrict__ st, double rlist_uniform, double skin,
+                                              int cap, int* __restrict__ list, int* __restrict__ nnb,
+                                              typename V4<R>::T* __restrict__ backup, int force_minimage,
+                                              DevState* stw) {
   typedef typename V4<R>::T T4;
   extern __shared__ __align__(16) unsigned char nl_smem[];
   T4* tile = reinterpret_cast<T4*>(nl_smem);  // w carries the atom's slot (charges are not needed here)
   __shared__ RunTable rt;
   __shared__ int nruns, tile_n, use_global;
   __shared__ float rl_max_sh;
-  if (gate && !(st->flags & FLAG_REBUILD)) return;
-  const int c = blockIdx.x;
   const int i0 = (int)start[c], i1 = (int)start[c + 1];
   if (i0 == i1) return;  // empty home cell (uniform exit for the whole block)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
@@ -414,6 +417,18 @@ k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __rest
 }
 
 template <class R, int MODE>
+__global__ void __launch_bounds__(256, 4)
+k_nl_build(int N, const typename V4<R>::T* __restrict__ pos, const float* __restrict__ rcut,
+           const uint32_t* __restrict__ start, const uint32_t* __restrict__ zord, NlGeom g,
+           const DevState* __restrict__ st, double rlist_uniform, double skin, int cap, int* __restrict__ list,
+           int* __restrict__ nnb, typename V4<R>::T* __restrict__ backup, int force_minimage, DevState* stw,
+           int gate) {
+  if (gate && !(st->flags & FLAG_REBUILD)) return;
+  nl_build_cell<R, MODE>(blockIdx.x, pos, rcut, start, zord, g, st, rlist_uniform, skin, cap, list, nnb, backup,
+                         force_minimage, stw);
+}
+
+template <class R, int MODE>
 static const void* nl_kernel() {
   static bool attr = false;
   const void* f = (const void*)k_nl_build<R, MODE>;
@@ -425,25 +440,30 @@ static const void* nl_kernel() {
   return f;
 }
 
+// cell-list criterion needs >= 4 cells per direction (DecideNumCell), else the
+// reference falls back to the all-pair (minimum image) kernel
+static int nl_force_minimage(const md_nlist* nl, md_system* sys, const md_cell_list* cl, int* force_mi) {
+  *force_mi = 0;
+  if (nl->mode != MD_NL_CELLSHIFT) return MD_OK;
+  DevState hs;
+  if (int r = sys->read_state(hs)) return r;
+  for (int d = 0; d < 3; ++d) {
+    if (cl->ncell[d] < 4) *force_mi = 1;
+    double h = hs.L[d] / cl->ncell[d];
+    int reach = (h >= nl->rlist) ? 1 : (int)std::ceil(nl->rlist / h);
+    if (2 * reach + 1 > cl->ncell[d]) *force_mi = 1;
+  }
+  return MD_OK;
+}
+
 int nlist_build_impl(md_nlist* nl, md_system* sys, md_cell_list* cl, Recorder* rec, bool gated) {
   int N = sys->N;
   if (N >= (1 << 26)) { md_set_error("neighbour lists hold at most 2^26 atoms"); return MD_ERR_BADARG; }
   NlGeom g;
   for (int d = 0; d < 3; ++d) g.nc[d] = cl->ncell[d];
   int gate = gated ? 1 : 0;
-  // cell-list criterion needs >= 4 cells per direction (DecideNumCell), else the
-  // reference falls back to the all-pair (minimum image) kernel
   int force_mi = 0;
-  if (nl->mode == MD_NL_CELLSHIFT) {
-    DevState hs;
-    if (int r = sys->read_state(hs)) return r;
-    for (int d = 0; d < 3; ++d) {
-      if (cl->ncell[d] < 4) force_mi = 1;
-      double h = hs.L[d] / cl->ncell[d];
-      int reach = (h >= nl->rlist) ? 1 : (int)std::ceil(nl->rlist / h);
-      if (2 * reach + 1 > cl->ncell[d]) force_mi = 1;
-    }
-  }
+  if (int r = nl_force_minimage(nl, sys, cl, &force_mi)) return r;
   double rl = nl->rlist, skin = nl->skin;
   DevState* st = sys->st;
   int cap = nl->cap;
@@ -463,6 +483,245 @@ int nlist_build_impl(md_nlist* nl, md_system* sys, md_cell_list* cl, Recorder* r
   if (int r = topo_exclude_launch(sys, nl, rec, gated)) return r;
   nl->built = true;
   return MD_OK;
+}
+
+// ------------------------------------------------------- fused rebuild
+// The rebuild chain of cells.cu (bin, scan, scatter, order, gather, copy
+// back, z order) and the list build as the phases of one cooperative kernel,
+// separated by grid barriers, that returns at once unless the rebuild flag is
+// set.  Inside a captured step it replaces the conditional node around the
+// chain: a node that returns at once costs a few microseconds, the
+// conditional node around eight kernels about ten.  Each phase does exactly
+// the work of its kernel (the same device functions), so the sorted arrays
+// and the lists are the same bit for bit.
+template <class R>
+struct RebuildArgs {
+  typedef typename V4<R>::T T4;
+  int N, ntot;
+  CellGeom cg;
+  NlGeom ng;
+  T4 *pos, *vel, *t_pos, *t_vel;
+  double4a *force, *t_force;
+  int4 *image, *t_image;
+  int *id, *t_id;
+  float *rcut, *t_rcut;
+  uint32_t *t_cell, *slot, *count, *start, *members, *perm, *cell_of, *zord, *busy;
+  const float* lat;
+  int lat_n[3];
+  const uint8_t* type_by_id;  // null with one atom type
+  uint8_t* type;
+  DevState* st;
+  double rlist, skin;
+  int cap, force_mi;
+  int *list, *nnb;
+  T4* backup;
+};
+
+// resident blocks per SM the kernels are built for: the list tile of the
+// FP64 path (72 KB) leaves room for two
+template <class R> constexpr int rebuild_min_blocks() { return sizeof(R) == 4 ? 4 : 2; }
+
+// the phases, from the cell of every atom to the lists; every block calls
+// the atoms of this block in the per-atom phases: a contiguous share of
+// ceil(N / blocks), so that every block (and every SM) takes part
+__device__ __forceinline__ void block_atoms(int N, int& k0, int& k1) {
+  const int per = (N + (int)gridDim.x - 1) / (int)gridDim.x;
+  k0 = min(N, (int)blockIdx.x * per);
+  k1 = min(N, k0 + per);
+}
+
+template <class R, int MODE>
+__device__ __forceinline__ void rebuild_phases(const RebuildArgs<R>& a) {
+  DevState* st = a.st;
+  const int lane = threadIdx.x & 31;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+  const int gw = gt >> 5, nw = gs >> 5;
+  int k0, k1;
+  block_atoms(a.N, k0, k1);
+  // 1. cell of every atom (warp-uniform passes for the warp-aggregated count)
+  if (gt == 0) { st->red_counter[RED_NLWORK] = 0u; st->ncell_busy = 0u; st->ncell_light = 0u; }
+  for (int b = k0 + (int)(threadIdx.x & ~31u); b < k1; b += blockDim.x)
+    bin_atom<R>(b + lane, b + lane < k1, a.pos, a.image, st, a.cg, a.t_cell, a.slot, a.count);
+  if (!grid_barrier(st)) return;
+  // 2. cell starts
+  if (blockIdx.x == 0) scan_block(a.ntot, a.count, a.start);
+  if (!grid_barrier(st)) return;
+  // 3. member lists; the non-empty cells listed for the list build, cells of
+  // 4 atoms or more from the front of the list and the others from its back,
+  // so that the costly cells are handed out first and the cheap ones fill
+  // the end (a slab has many empty or near-empty vapour cells)
+  for (int i = k0 + threadIdx.x; i < k1; i += blockDim.x) scatter_atom(i, a.t_cell, a.slot, a.start, a.members);
+  for (int cb = gw * 32; cb < a.ntot; cb += nw * 32) {
+    const int c = cb + lane;
+    const uint32_t n = c < a.ntot ? a.start[c + 1] - a.start[c] : 0u;
+    const unsigned mh = __ballot_sync(0xffffffffu, n >= 4u), ml = __ballot_sync(0xffffffffu, n > 0u && n < 4u);
+    unsigned bh = 0, bl = 0;
+    if (lane == 0 && mh) bh = atomicAdd(&st->ncell_busy, (unsigned)__popc(mh));
+    if (lane == 0 && ml) bl = atomicAdd(&st->ncell_light, (unsigned)__popc(ml));
+    bh = __shfl_sync(0xffffffffu, bh, 0);
+    bl = __shfl_sync(0xffffffffu, bl, 0);
+    const unsigned below = (1u << lane) - 1u;
+    if (n >= 4u) a.busy[bh + __popc(mh & below)] = (uint32_t)c;
+    else if (n > 0u) a.busy[a.ntot - 1 - (int)(bl + __popc(ml & below))] = (uint32_t)c;
+  }
+  if (!grid_barrier(st)) return;
+  // 4. deterministic order inside each cell (warp per cell)
+  for (int c = gw; c < a.ntot; c += nw) order_cell(c, lane, a.start, a.members, a.rcut, a.perm);
+  if (!grid_barrier(st)) return;
+  // 5. permute into cell order
+  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x)
+    gather_atom<R>(k, a.perm, a.t_cell, a.cell_of, a.pos, a.vel, a.force, a.image, a.id, a.rcut, a.t_pos, a.t_vel,
+                   a.t_force, a.t_image, a.t_id, a.t_rcut, a.lat, a.lat_n[0], a.lat_n[1], a.lat_n[2], st);
+  if (!grid_barrier(st)) return;
+  // 6. copy back with the per-slot types; the z order of each cell from the
+  // gathered copy (the same values)
+  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+    copyback_atom<R>(k, a.t_pos, a.t_vel, a.t_force, a.t_image, a.t_id, a.t_rcut, a.pos, a.vel, a.force, a.image,
+                     a.id, a.rcut);
+    if (a.type) a.type[k] = a.type_by_id[a.t_id[k]];
+  }
+  for (int c = gw; c < a.ntot; c += nw) zorder_cell<R>(c, lane, a.start, a.t_pos, a.zord);
+  if (!grid_barrier(st)) return;
+  // 7. lists, the non-empty home cells handed out by a counter (cells differ
+  // in work by tens of times across a slab; the order of the cells does not
+  // change any list); the next cell is fetched while this one is built
+  const int nfull = (int)__ldcg(&st->ncell_busy);
+  const int nbusy = nfull + (int)__ldcg(&st->ncell_light);
+  __shared__ int s_work;
+  if (threadIdx.x == 0) s_work = (int)atomicAdd(&st->red_counter[RED_NLWORK], 1u);
+  __syncthreads();
+  int w = s_work;
+  while (w < nbusy) {
+    int nxt = 0;
+    if (threadIdx.x == 0) nxt = (int)atomicAdd(&st->red_counter[RED_NLWORK], 1u);
+    const int c = (int)__ldcg(&a.busy[w < nfull ? w : a.ntot - 1 - (w - nfull)]);
+    nl_build_cell<R, MODE>(c, a.pos, a.rcut, a.start, a.zord, a.ng, st, a.rlist, a.skin, a.cap, a.list, a.nnb,
+                           a.backup, a.force_mi, st);
+    __syncthreads();
+    if (threadIdx.x == 0) s_work = nxt;
+    __syncthreads();
+    w = s_work;
+  }
+}
+
+template <class R, int MODE>
+__global__ void __launch_bounds__(256, rebuild_min_blocks<R>()) k_rebuild(RebuildArgs<R> a) {
+  // FLAG_REBUILD does not change while this kernel runs (it is set by the
+  // step's first kernel and cleared by its last), so every block takes the
+  // same branch
+  if (!(a.st->flags & FLAG_REBUILD)) return;
+  rebuild_phases<R, MODE>(a);
+}
+
+// The Langevin step's first half with the rebuild folded in: the particle
+// B A O A and displacement test of k_lv_step1 (the same device function) for
+// every atom, a grid barrier, the box of the step committed, and, when an
+// atom has moved more than half the skin, the rebuild phases.  This saves the
+// step a kernel node against k_lv_step1 followed by k_rebuild.
+template <class R, int MODE>
+__global__ void __launch_bounds__(256, rebuild_min_blocks<R>())
+k_lv_step1_rebuild(typename V4<R>::T* __restrict__ vel, const double4a* __restrict__ force, LvDev p,
+                   RebuildArgs<R> a) {
+  DevState* st = a.st;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  int k0, k1;
+  block_atoms(a.N, k0, k1);
+  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x)
+    lv_particle_step1<R>(k, a.pos, vel, force, a.id, a.backup, st, p);
+  // every block is done reading the box of the last step
+  if (!grid_barrier(st)) return;
+  if (gt == 0) box_commit(st);
+  if (!(__ldcg(&st->flags) & FLAG_REBUILD)) return;
+  if (!grid_barrier(st)) return;  // the committed box, for the binning
+  rebuild_phases<R, MODE>(a);
+}
+
+// the kernel of a precision and list mode, its dynamic shared memory and
+// the blocks of one cooperative launch (0: not possible on this device)
+static const void* rebuild_kernel(int prec, int mode, size_t* smem, int* blocks, bool with_lv = false) {
+  const void* f;
+  if (prec == MD_PREC_FP64) {
+    if (with_lv)
+      f = mode == MD_NL_MINIMAGE ? (const void*)k_lv_step1_rebuild<double, MD_NL_MINIMAGE>
+                                 : (const void*)k_lv_step1_rebuild<double, MD_NL_CELLSHIFT>;
+    else
+      f = mode == MD_NL_MINIMAGE ? (const void*)k_rebuild<double, MD_NL_MINIMAGE>
+                                 : (const void*)k_rebuild<double, MD_NL_CELLSHIFT>;
+    *smem = NL_TILE_CAP * sizeof(double4a);
+  } else {
+    if (with_lv)
+      f = mode == MD_NL_MINIMAGE ? (const void*)k_lv_step1_rebuild<float, MD_NL_MINIMAGE>
+                                 : (const void*)k_lv_step1_rebuild<float, MD_NL_CELLSHIFT>;
+    else
+      f = mode == MD_NL_MINIMAGE ? (const void*)k_rebuild<float, MD_NL_MINIMAGE>
+                                 : (const void*)k_rebuild<float, MD_NL_CELLSHIFT>;
+    *smem = NL_TILE_CAP * sizeof(float4);
+  }
+  *blocks = 0;
+  int dev = 0, coop = 0, nsm = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, 256, *smem) != cudaSuccess) {
+    cudaGetLastError();
+    return f;
+  }
+  if (coop) *blocks = per_sm * nsm;
+  return f;
+}
+
+bool rebuild_fused_ok(const md_system* sys, const md_nlist* nl) {
+  if (sys->topo) return false;  // the topology's slot map and exclusions are kernels of bonded.cu
+  if (sys->N >= (1 << 26)) return false;
+  size_t smem;
+  int b1, b2;
+  rebuild_kernel(sys->prec, nl->mode, &smem, &b1, false);
+  rebuild_kernel(sys->prec, nl->mode, &smem, &b2, true);
+  return b1 > 0 && b2 > 0;
+}
+
+template <class R>
+static int rebuild_fused_t(md_cell_list* cl, md_nlist* nl, md_system* sys, Recorder* rec, bool with_lv) {
+  typedef typename V4<R>::T T4;
+  RebuildArgs<R> a;
+  memset(&a, 0, sizeof(a));
+  a.N = sys->N;
+  a.ntot = cl->ntot;
+  for (int d = 0; d < 3; ++d) { a.cg.nc[d] = cl->ncell[d]; a.ng.nc[d] = cl->ncell[d]; }
+  a.cg.ntot = cl->ntot;
+  a.pos = (T4*)sys->pos; a.vel = (T4*)sys->vel; a.t_pos = (T4*)sys->t_pos; a.t_vel = (T4*)sys->t_vel;
+  a.force = sys->force; a.t_force = sys->t_force;
+  a.image = sys->image; a.t_image = sys->t_image;
+  a.id = sys->id; a.t_id = sys->t_id;
+  a.rcut = sys->rcut; a.t_rcut = sys->t_rcut;
+  a.t_cell = cl->t_cell; a.slot = cl->slot; a.count = cl->count; a.start = cl->start;
+  a.members = cl->members; a.perm = cl->perm; a.cell_of = cl->cell_of; a.zord = cl->zord; a.busy = cl->busy;
+  a.lat = sys->d_lattice;
+  for (int d = 0; d < 3; ++d) a.lat_n[d] = sys->lat_n[d];
+  if (sys->ntypes > 1) { a.type_by_id = sys->type_by_id; a.type = sys->type; }
+  a.st = sys->st;
+  a.rlist = nl->rlist; a.skin = nl->skin; a.cap = nl->cap;
+  if (int r = nl_force_minimage(nl, sys, cl, &a.force_mi)) return r;
+  a.list = nl->list; a.nnb = nl->nnb; a.backup = (T4*)nl->backup;
+  size_t smem;
+  int blocks;
+  const void* f = rebuild_kernel(sys->prec, nl->mode, &smem, &blocks, with_lv);
+  if (blocks <= 0) { md_set_error("fused rebuild: no cooperative launch on this device"); return MD_ERR_CUDA; }
+  if (!with_lv) {
+    void* args[] = {&a};
+    return rec_launch_coop(rec, f, dim3(blocks), dim3(256), smem, args);
+  }
+  LvDev p = make_lv(sys, nl);
+  void* args[] = {&sys->vel, &sys->force, &p, &a};
+  return rec_launch_coop(rec, f, dim3(blocks), dim3(256), smem, args);
+}
+
+int rebuild_fused_impl(md_cell_list* cl, md_nlist* nl, md_system* sys, Recorder* rec, bool with_lv) {
+  if (sys->N >= (1 << 26)) { md_set_error("neighbour lists hold at most 2^26 atoms"); return MD_ERR_BADARG; }
+  int r = (sys->prec == MD_PREC_FP64) ? rebuild_fused_t<double>(cl, nl, sys, rec, with_lv)
+                                      : rebuild_fused_t<float>(cl, nl, sys, rec, with_lv);
+  if (r == MD_OK) { cl->built = true; nl->built = true; }
+  return r;
 }
 
 // ------------------------------------------------------------------ C ABI

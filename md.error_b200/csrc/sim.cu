@@ -36,6 +36,8 @@ struct md_sim {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool conditional = false;
+  bool fused = false;  // the rebuild is the flag-gated cooperative kernel
+  bool allow_fused = true;  // md_sim_set_rebuild_kind
   float* lattice_in_graph = nullptr;
   int topo_in_graph = -1;
   int64_t steps = 0;
@@ -71,18 +73,27 @@ static int record_step(md_sim* s, Recorder* rec, bool use_graph) {
   md_system* sys = s->sys;
   cudaGraphConditionalHandle h = 0;
   bool cond = false;
-  if (use_graph && rec->graph) {
+  // the rebuild as one flag-gated cooperative kernel where the device can
+  // run it, else the chain of kernels under a conditional node (or gated)
+  const bool fused = s->allow_fused && rebuild_fused_ok(sys, s->nl);
+  if (use_graph && rec->graph && !fused) {
     cudaError_t e = cudaGraphConditionalHandleCreate(&h, rec->graph, 0, 0);
     cond = (e == cudaSuccess);
     if (!cond) cudaGetLastError();
   }
   const bool nhc = s->nhc != nullptr;
-  if (nhc) {
+  if (fused && !nhc) {
+    // the Langevin first half and the rebuild in one kernel
+    if (int r = rebuild_fused_impl(s->cl, s->nl, sys, rec, true)) return r;
+  } else if (nhc) {
     if (int r = nhc_vv1_impl(s->nhc, s->nl, s->p.lv.dt, rec, h, cond ? 1 : 0)) return r;
   } else {
     if (int r = langevin_step1_impl(sys, s->nl, rec, false, h, cond ? 1 : 0)) return r;
   }
-  if (cond) {
+  if (fused && nhc) {
+    if (int r = rebuild_fused_impl(s->cl, s->nl, sys, rec, false)) return r;
+  } else if (fused) {
+  } else if (cond) {
     cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
     cp.conditional.handle = h;
     cp.conditional.type = cudaGraphCondTypeIf;
@@ -101,6 +112,7 @@ static int record_step(md_sim* s, Recorder* rec, bool use_graph) {
     if (int r = nlist_build_impl(s->nl, sys, s->cl, rec, true)) return r;
   }
   s->conditional = cond;
+  s->fused = fused;
   // Langevin with SPME: the reciprocal chain is a second branch beside the
   // real-space kernel (both depend on the rebuild); it stores its forces in
   // its own buffer and leaves its energy and virial for the closing kick,
@@ -372,6 +384,7 @@ extern "C" int md_sim_counters(md_sim* s, int64_t* steps, int64_t* rebuilds, int
     return MD_ERR_NLIST_OVERFLOW;
   }
   if (hs.flags & FLAG_NAN) { md_set_error("non-finite coordinates during the run"); return MD_ERR_BADARG; }
+  if (hs.flags & FLAG_TIMEOUT) { md_set_error("a grid barrier of the rebuild gave up waiting"); return MD_ERR_TIMEOUT; }
   return MD_OK;
 }
 
@@ -379,6 +392,23 @@ extern "C" int md_sim_get_nhc_state(md_sim* s, double out[5]) {
   if (!s || !out) return MD_ERR_BADARG;
   if (!s->nhc) { md_set_error("md_sim_get_nhc_state: the run does not use the Nose-Hoover chain"); return MD_ERR_BADARG; }
   return md_nhc_get_state(s->nhc, out);
+}
+
+extern "C" int md_sim_rebuild_kind(md_sim* s, int* out) {
+  if (!s || !out) return MD_ERR_BADARG;
+  *out = s->fused ? MD_REBUILD_FUSED : (s->exec && s->conditional) ? MD_REBUILD_CONDITIONAL : MD_REBUILD_GATED;
+  return MD_OK;
+}
+
+extern "C" int md_sim_set_rebuild_kind(md_sim* s, int kind) {
+  if (!s || (kind != MD_REBUILD_FUSED && kind != MD_REBUILD_CONDITIONAL)) {
+    md_set_error("md_sim_set_rebuild_kind: MD_REBUILD_FUSED or MD_REBUILD_CONDITIONAL");
+    return MD_ERR_BADARG;
+  }
+  s->allow_fused = kind == MD_REBUILD_FUSED;
+  if (s->exec) return build_graph(s);
+  s->fused = s->allow_fused && rebuild_fused_ok(s->sys, s->nl);
+  return MD_OK;
 }
 
 extern "C" int md_sim_uses_conditional_graph(md_sim* s, int* out) {

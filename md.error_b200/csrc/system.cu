@@ -71,6 +71,20 @@ int rec_launch(Recorder* r, const void* func, dim3 grid, dim3 block, size_t smem
   return MD_OK;
 }
 
+int rec_launch_coop(Recorder* r, const void* func, dim3 grid, dim3 block, size_t smem, void** args) {
+  if (r && r->graph) {
+    if (int e = rec_launch(r, func, grid, block, smem, args)) return e;
+    cudaLaunchAttributeValue v;
+    memset(&v, 0, sizeof(v));
+    v.cooperative = 1;
+    MD_CUDA(cudaGraphKernelNodeSetAttribute(r->last, cudaLaunchAttributeCooperative, &v));
+    return MD_OK;
+  }
+  cudaStream_t s = r ? r->stream : nullptr;
+  MD_CUDA(cudaLaunchCooperativeKernel(func, grid, block, args, smem, s));
+  return MD_OK;
+}
+
 int md_system::read_state(DevState& s) {
   MD_CUDA(cudaMemcpyAsync(&s, st, sizeof(DevState), cudaMemcpyDeviceToHost, stream));
   MD_CUDA(cudaStreamSynchronize(stream));

@@ -111,6 +111,8 @@ _SIGS = {
     "md_sim_run": (i32, [vp, i32]),
     "md_sim_counters": (i32, [vp, P(i64), P(i64), P(i32)]),
     "md_sim_uses_conditional_graph": (i32, [vp, P(i32)]),
+    "md_sim_rebuild_kind": (i32, [vp, P(i32)]),
+    "md_sim_set_rebuild_kind": (i32, [vp, i32]),
     "md_engine_register_coulomb": (i32, [vp, f64]),
     "md_spme_create": (i32, [P(vp), vp, P(i32), i32, f64, i32]),
     "md_spme_destroy": (i32, [vp]),

@@ -1068,6 +1068,21 @@ class Simulation:
         check(lib.md_sim_uses_conditional_graph(self.h, C.byref(v)), "conditional")
         return bool(v.value)
 
+    def rebuild_kind(self):
+        """How a step decides on the device whether to rebuild the lists:
+        "fused" (one cooperative kernel gated by the device's rebuild flag),
+        "conditional" (the chain of kernels under a conditional graph node) or
+        "gated" (the chain launched every step, each kernel gated)."""
+        v = C.c_int()
+        check(lib.md_sim_rebuild_kind(self.h, C.byref(v)), "rebuild kind")
+        return {0: "gated", 1: "conditional", 2: "fused"}[v.value]
+
+    def set_rebuild_kind(self, kind):
+        """"fused" (the default where the device can run it) or "conditional"
+        (the chain of kernels); both give the same lists bit for bit."""
+        k = {"fused": 2, "conditional": 1}[kind]
+        check(lib.md_sim_set_rebuild_kind(self.h, k), "set rebuild kind")
+
     def nhc_state(self):
         """xi1, xi2, vxi1, vxi2, HamiltonianContribution of the driver's chain."""
         out = np.zeros(5)

@@ -79,7 +79,7 @@ def test_sim_with_adaptive_cutoff(mdf):
     assert len(np.unique(rc)) > 1  # the estimate assigned different cutoffs
     p = sys.stats()
     assert p[mdf.STAT_PRESSURE_CORR_XX] != 0.0
-    assert sim.uses_conditional_graph()
+    assert sim.rebuild_kind() == "fused"
 
 
 def test_pressure_correction_carries_previous_value(mdf, orc, small):

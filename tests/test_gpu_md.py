@@ -440,3 +440,34 @@ def test_statistics_rows_and_finish(mdf, small_slab, prec):
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][1], out[1][1])
     assert np.any(out[0][1])
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_fused_rebuild_matches_kernel_chain(mdf, small_slab, prec, use_graph):
+    """The flag-gated cooperative rebuild (one kernel: cell sort, per-slot
+    types, lists) and the chain of kernels give the same trajectory bit for
+    bit: adaptive cutoffs, two atom types, Langevin NPT, several rebuilds."""
+    s = small_slab
+    types = np.arange(s.n) % 2
+    out = []
+    for kind in ("fused", "conditional"):
+        sys = mdf.MDSystem(s.pos, s.box, vel=s.vel, precision=prec, type=types)
+        sys.set_rcut(adaptive_rcut(s.n, seed=4))
+        eng = mdf.InteractionEngine(sys)
+        eng.registNonBondedInteractionPair(0, 0, 1.0, 1.0)
+        eng.registNonBondedInteractionPair(0, 1, 1.1, 0.95)
+        eng.registNonBondedInteractionPair(1, 1, 0.9, 1.05)
+        lv = mdf.langevin_params(dt=0.005, temperature=0.85, gamma_t=1.0, seed=9, tau_p=2.0, kappa_t=0.1,
+                                 p_ref=(0.0, 0.0, 0.0), npt_dirs=4)
+        sim = mdf.Simulation(sys, eng, skin=0.3, cell_size=2.8, lv=lv, use_graph=use_graph, max_rcut=5.0)
+        sim.set_rebuild_kind(kind)
+        want = kind if (use_graph or kind == "fused") else "gated"
+        sim.run(150)
+        assert sim.rebuild_kind() == want
+        steps, rebuilds, flags = sim.counters()
+        out.append((rebuilds, sys.positions(), sys.velocities(), sys.forces(), sys.types(), sys.stats(),
+                    sys.box()))
+    assert out[0][0] == out[1][0] and out[0][0] >= 3
+    for a, b in zip(out[0][1:], out[1][1:]):
+        assert np.array_equal(a, b)
