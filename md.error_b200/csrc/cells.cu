@@ -29,7 +29,7 @@ __global__ void k_bin(int N, typename V4<R>::T* pos, int4* image, DevState* st, 
 
 __global__ void __launch_bounds__(1024) k_scan(int n, uint32_t* count, uint32_t* start, DevState* st, int gate) {
   if (gate && !(st->flags & FLAG_REBUILD)) return;
-  scan_block(n, count, start);
+  scan_block<4>(n, count, start);
 }
 
 __global__ void k_scatter(int N, const uint32_t* t_cell, const uint32_t* slot, const uint32_t* start,

@@ -71,35 +71,43 @@ __device__ __forceinline__ void bin_atom(int i, bool valid, typename V4<R>::T* p
   t_cell[i] = cell;
 }
 
-// single-block exclusive scan (each thread owns 4 cells of a tile); zeroes
-// count for the next rebuild
-// one block, any multiple of 32 threads
+// single-block exclusive scan of the cell counts (each thread owns PER
+// consecutive cells of a tile of PER * blockDim cells, read and written as
+// 16-byte vectors: count and start come from cudaMalloc and PER is a multiple
+// of 4, so every vector is aligned); zeroes count for the next rebuild.  One
+// block, any multiple of 32 threads; the running total carries from tile to
+// tile and the next tile is loaded early.
+template <int PER>
 __device__ __forceinline__ void scan_block(int n, uint32_t* count, uint32_t* start) {
-  // exclusive scan of the cell counts (and their reset) in tiles of 4T cells:
-  // thread t of a tile holds cells 4t..4t+3, so each warp reads and writes
-  // 512 contiguous bytes; the running total carries from tile to tile
+  static_assert(PER % 4 == 0, "whole 16-byte vectors per thread");
   __shared__ uint32_t wsum[32];
   const int T = blockDim.x;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = T >> 5;
   uint32_t carry = 0;
-  // cells 4t..4t+3 of a tile as one 16-byte load (count and start come from
-  // cudaMalloc, so 4t is 16-byte aligned), the next tile's loaded early
-  auto load4 = [&](int i0, uint32_t v[4]) {
-    if (i0 + 3 < n) {
-      const uint4 q = *reinterpret_cast<const uint4*>(count + i0);
-      v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
-    } else {
+  auto loadv = [&](int i0, uint32_t (&v)[PER]) {
 #pragma unroll
-      for (int k = 0; k < 4; ++k) v[k] = (i0 + k < n) ? count[i0 + k] : 0u;
+    for (int q = 0; q < PER / 4; ++q) {
+      const int j = i0 + 4 * q;
+      if (j + 3 < n) {
+        const uint4 u = *reinterpret_cast<const uint4*>(count + j);
+        v[4 * q] = u.x; v[4 * q + 1] = u.y; v[4 * q + 2] = u.z; v[4 * q + 3] = u.w;
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[4 * q + k] = (j + k < n) ? count[j + k] : 0u;
+      }
     }
   };
-  uint32_t nxt[4];
-  load4(4 * threadIdx.x, nxt);
-  for (int base = 0; base < n; base += 4 * T) {
-    const int i0 = base + 4 * threadIdx.x;
-    uint32_t v[4] = {nxt[0], nxt[1], nxt[2], nxt[3]};
-    if (base + 4 * T < n) load4(i0 + 4 * T, nxt);
-    const uint32_t tot = v[0] + v[1] + v[2] + v[3];
+  uint32_t nxt[PER];
+  loadv(PER * threadIdx.x, nxt);
+  for (int base = 0; base < n; base += PER * T) {
+    const int i0 = base + PER * threadIdx.x;
+    uint32_t v[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) v[k] = nxt[k];
+    if (base + PER * T < n) loadv(i0 + PER * T, nxt);
+    uint32_t tot = 0;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) tot += v[k];
     uint32_t x = tot;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -119,18 +127,23 @@ __device__ __forceinline__ void scan_block(int n, uint32_t* count, uint32_t* sta
     }
     __syncthreads();
     uint32_t run = carry + (wid > 0 ? wsum[wid - 1] : 0u) + x - tot;
-    if (i0 + 3 < n) {
-      const uint4 st4 = make_uint4(run, run + v[0], run + v[0] + v[1], run + v[0] + v[1] + v[2]);
-      *reinterpret_cast<uint4*>(start + i0) = st4;
-      *reinterpret_cast<uint4*>(count + i0) = make_uint4(0u, 0u, 0u, 0u);
-    } else {
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        if (i0 + k < n) {
-          start[i0 + k] = run;
-          count[i0 + k] = 0u;
+    for (int q = 0; q < PER / 4; ++q) {
+      const int j = i0 + 4 * q;
+      if (j + 3 < n) {
+        const uint32_t s0 = run, s1 = s0 + v[4 * q], s2 = s1 + v[4 * q + 1], s3 = s2 + v[4 * q + 2];
+        *reinterpret_cast<uint4*>(start + j) = make_uint4(s0, s1, s2, s3);
+        *reinterpret_cast<uint4*>(count + j) = make_uint4(0u, 0u, 0u, 0u);
+        run = s3 + v[4 * q + 3];
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          if (j + k < n) {
+            start[j + k] = run;
+            count[j + k] = 0u;
+          }
+          run += v[4 * q + k];
         }
-        run += v[k];
       }
     }
     carry += wsum[nw - 1];
@@ -196,6 +209,62 @@ __device__ __forceinline__ void zorder_cell(int cell, int lane, const uint32_t* 
     }
     if (on) zord[s + rank] = e;
   }
+}
+
+// order_cell and, from the same members, the z order zorder_cell gives after
+// the gather: member e goes to slot s + rank(e) (perm), and its z there is
+// the binned pos[e].z, so ranking (z, new slot) here gives zord without a
+// pass over the gathered arrays.  Up to 32 members stay in registers; a
+// fuller cell reads its new order back from perm.
+template <class R>
+__device__ __forceinline__ void order_zorder_cell(int cell, int lane, const uint32_t* start, const uint32_t* members,
+                                                  const float* rcut, const typename V4<R>::T* pos, uint32_t* perm,
+                                                  uint32_t* zord) {
+  const uint32_t s = start[cell], n = start[cell + 1] - s;
+  if (n == 0) return;
+  if (n > 32) {
+    order_cell(cell, lane, start, members, rcut, perm);
+    __syncwarp();  // the warp's perm stores are visible to the warp
+    for (uint32_t b = 0; b < n; b += 32) {
+      const bool on = b + lane < n;
+      const uint32_t e = on ? s + b + lane : 0u;
+      const R ze = on ? pos[perm[e]].z : R(0);
+      uint32_t rank = 0;
+      for (uint32_t b2 = 0; b2 < n; b2 += 32) {
+        const bool on2 = b2 + lane < n;
+        const uint32_t e2 = on2 ? s + b2 + lane : 0xffffffffu;
+        const R z2 = on2 ? pos[perm[e2]].z : R(0);
+#pragma unroll 8
+        for (int t = 0; t < 32; ++t) {
+          const R zt = __shfl_sync(0xffffffffu, z2, t);
+          const uint32_t et = __shfl_sync(0xffffffffu, e2, t);
+          rank += (et != 0xffffffffu && (zt < ze || (zt == ze && et < e))) ? 1u : 0u;
+        }
+      }
+      if (on) zord[s + rank] = e;
+    }
+    return;
+  }
+  const bool on = (uint32_t)lane < n;
+  const uint32_t m = on ? members[s + lane] : 0u;
+  const unsigned long long km = on ? (((unsigned long long)__float_as_uint(rcut[m]) << 32) | m) : ~0ull;
+  const R zm = on ? pos[m].z : R(0);
+  uint32_t rank = 0;
+#pragma unroll 8
+  for (int t = 0; t < 32; ++t) {
+    const unsigned long long kt = __shfl_sync(0xffffffffu, km, t);
+    rank += (kt < km) ? 1u : 0u;
+  }
+  const uint32_t e = on ? s + rank : 0xffffffffu;  // the member's slot after the gather
+  if (on) perm[e] = m;
+  uint32_t rz = 0;
+#pragma unroll 8
+  for (int t = 0; t < 32; ++t) {
+    const R zt = __shfl_sync(0xffffffffu, zm, t);
+    const uint32_t et = __shfl_sync(0xffffffffu, e, t);
+    rz += (et != 0xffffffffu && (zt < zm || (zt == zm && et < e))) ? 1u : 0u;
+  }
+  if (on) zord[s + rz] = e;
 }
 
 // AssignRCut::assign index (ENG/src/AssignRCut.cu:93-112) in binary32

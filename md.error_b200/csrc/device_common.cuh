@@ -50,35 +50,42 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// Barrier over every block of a cooperative launch (all blocks resident).
-// The last block to arrive resets the count and advances the generation the
-// others wait on.  A wait is bounded: past 4 s the block sets FLAG_TIMEOUT and
-// the call returns false, and the caller leaves the kernel (the other blocks'
-// waits then end the same way).
+__device__ __forceinline__ unsigned long long atom_add_release_u64(unsigned long long* p, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.add.release.gpu.global.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Barrier over every block of a cooperative launch (all blocks resident), on
+// one 64-bit counter that each barrier advances by exactly GBAR_EPOCH: every
+// block adds 1 with release semantics, block 0 adds GBAR_EPOCH - (blocks - 1),
+// and each block waits (acquire loads) for the counter to pass the end of
+// the epoch it arrived in.  The counter never needs a reset and stays aligned
+// whatever the grid size.  A wait is bounded: past 4 s the block sets
+// FLAG_TIMEOUT and the call returns false, and the caller leaves the kernel
+// (the other blocks' waits then end the same way).
+constexpr unsigned long long GBAR_EPOCH = 1ull << 20;  // above any grid size
 __device__ __forceinline__ bool grid_barrier(DevState* st) {
   __shared__ int gb_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* gen = &st->gbar_gen;
-    const unsigned g0 = *gen;
-    __threadfence();
+    const unsigned long long inc = blockIdx.x == 0 ? GBAR_EPOCH - (gridDim.x - 1) : 1ull;
+    const unsigned long long old = atom_add_release_u64(&st->gbar, inc);
+    const unsigned long long target = (old & ~(GBAR_EPOCH - 1)) + GBAR_EPOCH;
     int ok = 1;
-    if (atomicAdd(&st->gbar_count, 1u) == gridDim.x - 1) {
-      st->gbar_count = 0u;
-      __threadfence();
-      atomicAdd(&st->gbar_gen, 1u);
-    } else {
-      const unsigned long long t0 = global_ns();
-      while (*gen == g0) {
-        if (global_ns() - t0 > 4000000000ull) {
-          atomicOr(&st->flags, FLAG_TIMEOUT);
-          ok = 0;
-          break;
-        }
-        __nanosleep(64);
+    const unsigned long long t0 = global_ns();
+    while ((long long)(ld_acquire_u64(&st->gbar) - target) < 0) {
+      if (global_ns() - t0 > 4000000000ull) {
+        atomicOr(&st->flags, FLAG_TIMEOUT);
+        ok = 0;
+        break;
       }
     }
-    __threadfence();
     gb_ok = ok;
   }
   __syncthreads();

@@ -63,11 +63,10 @@ struct DevState {
   double Lnext[3];   // box of the next step, committed by that step's first kernel
   double box_xi[4];  // the box normals of the coming step, computed ahead in the closing kick
   int box_pending;
-  unsigned gbar_count;  // grid barrier of the fused rebuild: blocks arrived
-  unsigned gbar_gen;    // and its generation
   unsigned ncell_busy;  // home cells of 4 atoms or more listed by the fused rebuild
   unsigned ncell_light; // and of 1 to 3 atoms
   unsigned pad1;
+  unsigned long long gbar;  // grid barrier of the fused rebuild (grid_barrier)
 };
 
 // host helpers -------------------------------------------------------------

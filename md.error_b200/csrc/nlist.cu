@@ -544,7 +544,7 @@ __device__ __forceinline__ void rebuild_phases(const RebuildArgs<R>& a) {
     bin_atom<R>(b + lane, b + lane < k1, a.pos, a.image, st, a.cg, a.t_cell, a.slot, a.count);
   if (!grid_barrier(st)) return;
   // 2. cell starts
-  if (blockIdx.x == 0) scan_block(a.ntot, a.count, a.start);
+  if (blockIdx.x == 0) scan_block<16>(a.ntot, a.count, a.start);
   if (!grid_barrier(st)) return;
   // 3. member lists; the non-empty cells listed for the list build, cells of
   // 4 atoms or more from the front of the list and the others from its back,
@@ -565,22 +565,22 @@ __device__ __forceinline__ void rebuild_phases(const RebuildArgs<R>& a) {
     else if (n > 0u) a.busy[a.ntot - 1 - (int)(bl + __popc(ml & below))] = (uint32_t)c;
   }
   if (!grid_barrier(st)) return;
-  // 4. deterministic order inside each cell (warp per cell)
-  for (int c = gw; c < a.ntot; c += nw) order_cell(c, lane, a.start, a.members, a.rcut, a.perm);
+  // 4. deterministic order inside each cell and the cell's z order (warp
+  // per cell)
+  for (int c = gw; c < a.ntot; c += nw)
+    order_zorder_cell<R>(c, lane, a.start, a.members, a.rcut, a.pos, a.perm, a.zord);
   if (!grid_barrier(st)) return;
   // 5. permute into cell order
   for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x)
     gather_atom<R>(k, a.perm, a.t_cell, a.cell_of, a.pos, a.vel, a.force, a.image, a.id, a.rcut, a.t_pos, a.t_vel,
                    a.t_force, a.t_image, a.t_id, a.t_rcut, a.lat, a.lat_n[0], a.lat_n[1], a.lat_n[2], st);
   if (!grid_barrier(st)) return;
-  // 6. copy back with the per-slot types; the z order of each cell from the
-  // gathered copy (the same values)
+  // 6. copy back with the per-slot types
   for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
     copyback_atom<R>(k, a.t_pos, a.t_vel, a.t_force, a.t_image, a.t_id, a.t_rcut, a.pos, a.vel, a.force, a.image,
                      a.id, a.rcut);
     if (a.type) a.type[k] = a.type_by_id[a.t_id[k]];
   }
-  for (int c = gw; c < a.ntot; c += nw) zorder_cell<R>(c, lane, a.start, a.t_pos, a.zord);
   if (!grid_barrier(st)) return;
   // 7. lists, the non-empty home cells handed out by a counter (cells differ
   // in work by tens of times across a slab; the order of the cells does not

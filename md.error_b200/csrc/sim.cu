@@ -155,6 +155,8 @@ static int build_graph(md_sim* s) {
   if (s->exec) { cudaGraphExecDestroy(s->exec); s->exec = nullptr; }
   if (s->graph) { cudaGraphDestroy(s->graph); s->graph = nullptr; }
   MD_CUDA(cudaGraphCreate(&s->graph, 0));
+  // the grid barrier's counter stays aligned unless a wait gave up: start clean
+  MD_CUDA(cudaMemsetAsync(&s->sys->st->gbar, 0, sizeof(unsigned long long), s->sys->stream));
   Recorder g;
   g.graph = s->graph;
   g.stream = s->sys->stream;
