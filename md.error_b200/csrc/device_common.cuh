@@ -50,6 +50,11 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
+__device__ __forceinline__ unsigned atom_add_acq_rel_u32(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
 __device__ __forceinline__ unsigned long long atom_add_release_u64(unsigned long long* p, unsigned long long v) {
   unsigned long long old;
   asm volatile("atom.add.release.gpu.global.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
@@ -114,13 +119,14 @@ __device__ bool block_reduce_finish(double (&v)[NV], double* partials, unsigned*
       for (int k = 0; k < NV; ++k) acc[k] += sh[w][k];
 #pragma unroll
     for (int k = 0; k < NV; ++k) partials[(size_t)blockIdx.x * NV + k] = acc[k];
-    __threadfence();
-    unsigned prev = atomicAdd(counter, 1u);
+    // release: this block's partials before its count; acquire: the last
+    // block sees every block's partials (its other threads through the
+    // barrier below)
+    const unsigned prev = atom_add_acq_rel_u32(counter, 1u);
     am_last = (prev == gridDim.x - 1);
   }
   __syncthreads();
   if (!am_last) return false;
-  __threadfence();
   double acc[NV];
 #pragma unroll
   for (int k = 0; k < NV; ++k) acc[k] = 0.0;
@@ -140,8 +146,7 @@ __device__ bool block_reduce_finish(double (&v)[NV], double* partials, unsigned*
       for (int w = 0; w < nw; ++w) s += sh[w][k];
       if (store) out[k] = s; else out[k] += s;
     }
-    *counter = 0u;
-    __threadfence();
+    *counter = 0u;  // read again by the next launch only
     return true;
   }
   return false;
