@@ -35,6 +35,10 @@ struct md_sim {
   md_nlist* nl = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // MD_SIM_MULTI consecutive steps in one graph, launched when no host-side
+  // work (density samples, cutoff or correction updates) falls between them
+  cudaGraph_t graph_multi = nullptr;
+  cudaGraphExec_t exec_multi = nullptr;
   bool conditional = false;
   bool fused = false;  // the rebuild is the flag-gated cooperative kernel
   bool allow_fused = true;  // md_sim_set_rebuild_kind
@@ -59,6 +63,10 @@ struct md_sim {
 };
 
 static void ring_release(md_sim* s);
+
+// steps per multi-step graph: a graph launch costs a few microseconds that a
+// step of tens of microseconds would otherwise pay each time
+constexpr int MD_SIM_MULTI = 8;
 
 // the step's statistic slots into the next row of the host ring
 __global__ void k_stats_ring(const DevState* st, double* ring, int rows, unsigned* count) {
@@ -151,9 +159,15 @@ static int record_step(md_sim* s, Recorder* rec, bool use_graph) {
   return MD_OK;
 }
 
-static int build_graph(md_sim* s) {
+static void release_graphs(md_sim* s) {
   if (s->exec) { cudaGraphExecDestroy(s->exec); s->exec = nullptr; }
   if (s->graph) { cudaGraphDestroy(s->graph); s->graph = nullptr; }
+  if (s->exec_multi) { cudaGraphExecDestroy(s->exec_multi); s->exec_multi = nullptr; }
+  if (s->graph_multi) { cudaGraphDestroy(s->graph_multi); s->graph_multi = nullptr; }
+}
+
+static int build_graph(md_sim* s) {
+  release_graphs(s);
   MD_CUDA(cudaGraphCreate(&s->graph, 0));
   // the grid barrier's counter stays aligned unless a wait gave up: start clean
   MD_CUDA(cudaMemsetAsync(&s->sys->st->gbar, 0, sizeof(unsigned long long), s->sys->stream));
@@ -162,6 +176,14 @@ static int build_graph(md_sim* s) {
   g.stream = s->sys->stream;
   if (int r = record_step(s, &g, true)) return r;
   MD_CUDA(cudaGraphInstantiate(&s->exec, s->graph, 0));
+  // the same step recorded MD_SIM_MULTI times in a row
+  MD_CUDA(cudaGraphCreate(&s->graph_multi, 0));
+  Recorder m;
+  m.graph = s->graph_multi;
+  m.stream = s->sys->stream;
+  for (int k = 0; k < MD_SIM_MULTI; ++k)
+    if (int r = record_step(s, &m, true)) return r;
+  MD_CUDA(cudaGraphInstantiate(&s->exec_multi, s->graph_multi, 0));
   s->lattice_in_graph = s->sys->d_lattice;
   s->topo_in_graph = s->sys->topo_version;
   return MD_OK;
@@ -171,8 +193,7 @@ extern "C" int md_sim_destroy(md_sim* s) {
   if (!s) return MD_OK;
   if (s->sys && s->sys->stream) cudaStreamSynchronize(s->sys->stream);
   ring_release(s);
-  if (s->exec) cudaGraphExecDestroy(s->exec);
-  if (s->graph) cudaGraphDestroy(s->graph);
+  release_graphs(s);
   md_nlist_destroy(s->nl);
   md_cell_list_destroy(s->cl);
   md_nhc_destroy(s->nhc);
@@ -317,6 +338,18 @@ extern "C" int md_sim_attach_adapt_rcut(md_sim* s, md_adapt_rcut* arc, int sampl
   return MD_OK;
 }
 
+// true when host-side work is due after any of the n steps j0 .. j0 + n - 1
+// (j = the step's index; the schedules of md_sim_run below)
+static bool host_work_within(const md_sim* s, int64_t j0, int n) {
+  for (int64_t j = j0; j < j0 + n; ++j) {
+    if (s->fcorr && (j % s->fc_assign_every == 0 || (j + 1) % s->fc_sample_every == 0 ||
+                     (j + 1) % s->fc_update_every == 0))
+      return true;
+    if (s->arc && ((j + 1) % s->sample_every == 0 || (j + 1) % s->update_every == 0)) return true;
+  }
+  return false;
+}
+
 extern "C" int md_sim_run(md_sim* s, int nsteps) {
   if (!s || nsteps < 0) return MD_ERR_BADARG;
   md_system* sys = s->sys;
@@ -330,7 +363,13 @@ extern "C" int md_sim_run(md_sim* s, int nsteps) {
     s->nhc_settled = false;
   }
   for (int i = 0; i < nsteps; ++i) {
-    if (s->exec) {
+    if (s->exec_multi && nsteps - i >= MD_SIM_MULTI && !host_work_within(s, s->steps, MD_SIM_MULTI - 1)) {
+      // steps s->steps .. s->steps + MD_SIM_MULTI - 1 in one launch; host work
+      // due after the last of them runs below as after a single step
+      MD_CUDA(cudaGraphLaunch(s->exec_multi, sys->stream));
+      s->steps += MD_SIM_MULTI - 1;
+      i += MD_SIM_MULTI - 1;
+    } else if (s->exec) {
       MD_CUDA(cudaGraphLaunch(s->exec, sys->stream));
     } else {
       Recorder rec;

@@ -471,3 +471,35 @@ def test_fused_rebuild_matches_kernel_chain(mdf, small_slab, prec, use_graph):
     assert out[0][0] == out[1][0] and out[0][0] >= 3
     for a, b in zip(out[0][1:], out[1][1:]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("with_arc", [False, True])
+def test_multi_step_graph_matches_single_steps(mdf, small_slab, with_arc):
+    """Simulation.run(n) launches several steps per graph where no host-side
+    work falls between them; the trajectory, the statistics and the cutoff
+    updates equal those of n single-step runs bit for bit."""
+    s = small_slab
+    out = []
+    for chunked in (False, True):
+        sys = mdf.MDSystem(s.pos, s.box, vel=s.vel, precision=0)
+        sys.set_rcut(np.full(s.n, 2.5, np.float32))
+        eng = mdf.InteractionEngine(sys)
+        eng.registNonBondedInteraction(1.0, 1.0, 0.0)
+        lv = mdf.langevin_params(dt=0.005, temperature=0.85, gamma_t=1.0, seed=5, tau_p=2.0, kappa_t=0.1,
+                                 p_ref=(0.0, 0.0, 0.0), npt_dirs=4)
+        sim = mdf.Simulation(sys, eng, skin=0.3, cell_size=2.8, lv=lv, max_rcut=5.0)
+        if with_arc:
+            arc = mdf.AdaptRCutEstimator(sys, refh=1.0, rcmin=2.5, rcmax=5.0, rcstep=0.5)
+            sim.attach_adapt_rcut(arc, sample_every=10, update_every=60, prec=0.02)
+        if chunked:
+            sim.run(123)
+        else:
+            for _ in range(123):
+                sim.run(1)
+        steps, rebuilds, flags = sim.counters()
+        assert steps == 123
+        out.append((rebuilds, sys.positions(), sys.velocities(), sys.forces(), sys.stats(), sys.box(),
+                    sys.rcut()))
+    assert out[0][0] == out[1][0] and out[0][0] >= 2
+    for a, b in zip(out[0][1:], out[1][1:]):
+        assert np.array_equal(a, b)
