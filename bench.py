@@ -379,7 +379,8 @@ def reference_loop(pairs_per_step):
                       "test or periodic images; one copy per core"}
 
 
-WORKLOADS = ("lj_slab", "lj_fluid", "charged_fluid", "charged_slab", "lj_slab_lfc", "spme_adjoint")
+WORKLOADS = ("lj_slab", "lj_fluid", "charged_fluid", "charged_slab", "charged_lj_slab", "lj_slab_lfc",
+             "spme_adjoint")
 
 
 def run_workload(args):
@@ -394,6 +395,11 @@ def run_workload(args):
     512 order 6, beta for a real-space error of 1e-4 at rc 3.0; adaptive
     per-atom cutoff 3.0..5.0 (AdaptRCut on 2-sigma bins of the density
     sampled during the relaxation, re-estimated on the reference's schedule).
+    charged_lj_slab: the LJ+SPME slab, the 65,536-atom slab start
+    (tests/golden/slab65536_start.npz) with half +1 and half -1 charges
+    (seeded), LJ + real-space Ewald at the per-atom adaptive cutoff 3.0..5.0
+    and ik SPME order 6, beta and the mesh chosen as for charged_slab, the
+    same relaxation, schedule and sampled error against a converged sum.
     lj_slab_lfc: the 65536-atom slab at a uniform cutoff 3.5 with the
     long-range force correction (ForceCorr on 1-sigma bins: field from the
     density sampled during the relaxation, then assigned every 40 steps,
@@ -419,11 +425,17 @@ def run_workload(args):
         s = mdf.systems.charged_fluid()
         rc, dt, T, gamma, shift = 3.0, 0.002, 1.0, 1.0, 0.0
         coul = dict(beta=0.95, K=(64, 64, 64), order=6)
+    elif w == "charged_lj_slab":
+        st = load_slab_start()
+        s = SimpleNamespace(name=w, n=st.n, pos=st.pos, vel=st.vel, box=st.box,
+                            charge=mdf.systems.charges(st.n, 7))
+        rc, dt, T, gamma, shift = 3.0, 0.002, 1.0, 1.0, 0.0
+        coul = dict(beta=None, K=(64, 64, 256), order=6)
     else:
         s = mdf.systems.charged_slab()
         rc, dt, T, gamma, shift = 3.0, 0.002, 1.0, 1.0, 0.0
         coul = dict(beta=None, K=(128, 128, 512), order=6)
-    adaptive = w == "charged_slab"
+    adaptive = w in ("charged_slab", "charged_lj_slab")
     arc_kw = dict(refh=2.0, rcmin=3.0, rcmax=5.0, rcstep=0.5)
     lattice = [None]
     lfc_profile = [None]
@@ -500,10 +512,10 @@ def run_workload(args):
     pos, vel = sys0.positions(), sys0.velocities()
     del sim0, sys0
     chosen = None
-    if w == "charged_slab":
+    if adaptive:
         # beta and the mesh from the error estimates of the relaxed charge profile
-        # (md_choose_spme_params) at a total target of 1e-4: the configuration's
-        # 128 x 128 x 512 mesh cannot meet it with the beta the real space needs
+        # (md_choose_spme_params) at a total target of 1e-4; the configuration's
+        # own mesh is reported beside it with its estimate at the chosen beta
         sysc = mdf.MDSystem(pos, s.box, charge=s.charge, precision=1)
         config_mesh = coul["K"]
         # the smallest total target the estimates can meet with order 6 within

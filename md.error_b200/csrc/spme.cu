@@ -519,15 +519,34 @@ k_fft_x_kspace(typename C2<R>::T* C, const typename C2<R>::T* __restrict__ twg, 
   T2* X = twi + n;
   T2* Y = X + LPB * LS;  // NG buffers
   R* PS = reinterpret_cast<R*>(Y + NG * LPB * LS);
-  int* lj = reinterpret_cast<int*>(PS + LPB * LS);
+  // psi = exp(-pi^2 m^2 / beta^2) / m^2 * B(m) / (pi V) factors by axis: the
+  // x factors exp(-sc m_x^2) b_x(i) for the n points of a line and, per line
+  // (j, k), exp(-sc (m_y^2 + m_z^2)) b_y(j) b_z(k) / (pi V) and m_y^2 + m_z^2,
+  // worked out once per block (FP64), leaving one reciprocal per point
+  double* EX = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(PS + LPB * LS) + 7) & ~(uintptr_t)7);
+  double* EJK = EX + n;
+  double* MJK = EJK + LPB;
+  int* lj = reinterpret_cast<int*>(MJK + LPB);
   int* lk = lj + LPB;
   load_tw<R, -1>(twf, twg, n);
   load_tw<R, 1>(twi, twg, n);
   const long line0 = (long)blockIdx.x * LPB;
+  const double sc = M_PI * M_PI / (beta * beta);
   if (threadIdx.x < LPB) {
     const long L = line0 + threadIdx.x;
-    lj[threadIdx.x] = (int)(L / K2h);
-    lk[threadIdx.x] = (int)(L % K2h);
+    const int j = (int)(L / K2h), k = (int)(L % K2h);
+    lj[threadIdx.x] = j;
+    lk[threadIdx.x] = k;
+    const int jp = j <= K1 / 2 ? j : j - K1;
+    const double my = jp * st->Li[1], mz = k * st->Li[2], mjk = my * my + mz * mz;
+    const double V = st->L[0] * st->L[1] * st->L[2];
+    MJK[threadIdx.x] = mjk;
+    EJK[threadIdx.x] = exp(-sc * mjk) * (bm[n + j] * bm[n + K1 + k]) / (M_PI * V);
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int ip = i <= n / 2 ? i : i - n;
+    const double mx = ip * st->Li[0];
+    EX[i] = exp(-sc * mx * mx) * bm[i];
   }
   const int grp = NG > 1 ? (int)threadIdx.x / FFT_THREADS : 0;
   const int gt = NG > 1 ? (int)threadIdx.x % FFT_THREADS : (int)threadIdx.x;
@@ -552,27 +571,26 @@ k_fft_x_kspace(typename C2<R>::T* C, const typename C2<R>::T* __restrict__ twg, 
   fft_stages<R, LOGN, 0, -1>((grp == 0 ? X : Y + grp * LPB * LS) + l * LS, twf, tl);
   double v[4] = {0, 0, 0, 0};
   if (grp == 0) {
-    const double V = st->L[0] * st->L[1] * st->L[2];
-    const double sc = M_PI * M_PI / (beta * beta), pv = 1.0 / (M_PI * V);
-    const double* bm1 = bm + n;
-    const double* bm2 = bm1 + K1;
 #pragma unroll
     for (int s = 0; s < EPT; ++s) {
       const int e = gt + s * FFT_THREADS, le = e % LPB, i = e / LPB;
       const long L = line0 + le;
       const int j = lj[le], k = lk[le];
-      const int ip = i <= n / 2 ? i : i - n, jp = j <= K1 / 2 ? j : j - K1, kp = k;
-      const double m[3] = {ip * st->Li[0], jp * st->Li[1], kp * st->Li[2]};
-      const double mm = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
-      const bool live = L < nlines && (ip || jp || kp);
-      const R ps = live ? (R)(exp(-sc * mm) / mm * (bm[i] * bm1[j] * bm2[k]) * pv) : R(0);
+      const int ip = i <= n / 2 ? i : i - n, jp = j <= K1 / 2 ? j : j - K1;
+      const double mx = ip * st->Li[0];
+      const double mm = mx * mx + MJK[le];
+      const bool live = L < nlines && (ip || jp || k);
+      const double inv = live ? 1.0 / mm : 0.0;
+      const R ps = live ? (R)(EX[i] * EJK[le] * inv) : R(0);
       PS[le * LS + i] = ps;
       if (with_stats && live) {
         // E = 1/2 sum_m |Q^|^2 psi over the full spectrum: interior z planes count twice
         const T2 q = X[le * LS + i];
         const double wgt = (k == 0 || (2 * k == K2)) ? 1.0 : 2.0;
         const double e2 = 0.5 * wgt * ((double)q.x * q.x + (double)q.y * q.y) * (double)ps;
-        const double f = 2.0 * (1.0 + M_PI * M_PI * mm / (beta * beta)) / mm;
+        // f = 2 (1 + pi^2 m^2 / beta^2) / m^2
+        const double f = 2.0 * inv + 2.0 * sc;
+        const double m[3] = {mx, jp * st->Li[1], k * st->Li[2]};
         v[0] += e2;
         // pressure tensor V P_aa = sum_m E_m (1 - f m_a^2); the virial slots hold W_aa = -V P_aa
 #pragma unroll
@@ -620,7 +638,7 @@ template <class R>
 static size_t fftx_smem(int logn, int method) {
   const int n = 1 << logn, tpl = n >= 8 ? n / 8 : 1, lpb = FFT_THREADS / tpl, ng = method == 0 ? 3 : 1;
   return sizeof(typename C2<R>::T) * (2 * (size_t)n + (1 + (size_t)ng) * lpb * (n + 1)) +
-         sizeof(R) * (size_t)lpb * (n + 1) + 2 * sizeof(int) * lpb;
+         sizeof(R) * (size_t)lpb * (n + 1) + 8 + sizeof(double) * ((size_t)n + 2 * lpb) + 2 * sizeof(int) * lpb;
 }
 
 // per-axis forward twiddle table exp(-2 pi i m / n), m < n, from FP64
