@@ -497,19 +497,23 @@ static size_t fftp_smem(int logn, int nbuf) {
 //   ik (METHOD 0): the three products phi_d = i (-2 pi m_d) psi Q^,
 //   (merge = 0: the sums stay in DevState::scratch for a later merge)
 //   analytic (METHOD 1): psi Q^ / 2 (FBSpline normalisation),
-// each transformed back along x and written to C[1 + d].  One group of
-// FFT_THREADS threads per product: group 0 runs the forward transform and
-// the k-space step (the other groups run the same stages on their own
-// buffers, keeping the barriers uniform), then every group forms and
-// inverts its product.  The last block merges the energy and the virial
-// into the statistics slots.
+// each transformed back along x and written to C[1 + d].  Groups of
+// FFT_THREADS threads: group 0 runs the forward transform and the k-space
+// step (group 1 runs the same stages on its own buffer, keeping the barriers
+// uniform), then for ik group 0 inverts phi_x and group 1 inverts psi Q^,
+// whose transform times -2 pi i m_y and -2 pi i m_z (constant along the
+// line) gives phi_y and phi_z.  The last block merges the energy and the
+// virial into the statistics slots.
 template <class R, int LOGN, int METHOD>
 __global__ void __launch_bounds__(FFT_THREADS * (METHOD == 0 ? 3 : 1))
 k_fft_x_kspace(typename C2<R>::T* C, const typename C2<R>::T* __restrict__ twg, const double* __restrict__ bm, int K1,
                int K2, double beta, DevState* st, double* partials, int with_stats, int merge) {
   typedef typename C2<R>::T T2;
   typedef FftGeom<LOGN> G;
-  constexpr int n = G::n, LPB = G::LPB, LS = G::LS, EPT = G::EPT, NG = METHOD == 0 ? 3 : 1;
+  // ik: group 0 transforms -2 pi i m_x psi Q^ back; m_y and m_z are constant
+  // along an x line, so group 1 transforms psi Q^ once and its result, times
+  // -2 pi i m_y and -2 pi i m_z, gives the other two products
+  constexpr int n = G::n, LPB = G::LPB, LS = G::LS, EPT = G::EPT, NG = METHOD == 0 ? 2 : 1;
   const int K2h = K2 / 2 + 1;
   const long nlines = (long)K1 * K2h, stride = nlines;
   const size_t nhalf = (size_t)n * nlines;
@@ -606,13 +610,15 @@ k_fft_x_kspace(typename C2<R>::T* C, const typename C2<R>::T* __restrict__ twg, 
     const T2 q = X[le * LS + i];
     const R ps = PS[le * LS + i];
     T2 g;
-    if (METHOD == 0) {
-      // phi_d = i (-2 pi m_d) psi Q^, d = grp, m = (i', j', k) / L (signed indices)
-      const int ix = grp == 0 ? (i <= n / 2 ? i : i - n)
-                              : grp == 1 ? (lj[le] <= K1 / 2 ? lj[le] : lj[le] - K1) : lk[le];
-      const R c = (R)(-2.0 * M_PI * (ix * st->Li[grp])) * ps;
+    if (METHOD == 0 && grp == 0) {
+      // phi_x = i (-2 pi m_x) psi Q^, m_x = i' / L_x (signed index)
+      const int ix = i <= n / 2 ? i : i - n;
+      const R c = (R)(-2.0 * M_PI * (ix * st->Li[0])) * ps;
       g.x = -q.y * c;
       g.y = q.x * c;
+    } else if (METHOD == 0) {
+      g.x = q.x * ps;
+      g.y = q.y * ps;
     } else {
       g.x = q.x * (R(0.5) * ps);
       g.y = q.y * (R(0.5) * ps);
@@ -621,11 +627,32 @@ k_fft_x_kspace(typename C2<R>::T* C, const typename C2<R>::T* __restrict__ twg, 
   }
   __syncthreads();
   fft_stages<R, LOGN, 0, 1>(Yg + l * LS, twi, tl);
-  T2* out = C + (1 + grp) * nhalf;
-  for (int e = gt; e < LPB * n; e += FFT_THREADS) {
-    const int le = e % LPB, i = e / LPB;
-    const long L = line0 + le;
-    if (L < nlines) out[L + i * stride] = Yg[le * LS + i];
+  if (METHOD == 0 && grp == 1) {
+    // phi_y and phi_z = i (-2 pi m_d) times the transform of psi Q^
+    T2* outy = C + 2 * nhalf;
+    T2* outz = C + 3 * nhalf;
+    for (int e = gt; e < LPB * n; e += FFT_THREADS) {
+      const int le = e % LPB, i = e / LPB;
+      const long L = line0 + le;
+      if (L >= nlines) continue;
+      const int jp = lj[le] <= K1 / 2 ? lj[le] : lj[le] - K1;
+      const R cy = (R)(-2.0 * M_PI * (jp * st->Li[1])), cz = (R)(-2.0 * M_PI * (lk[le] * st->Li[2]));
+      const T2 v = Yg[le * LS + i];
+      T2 a, b;
+      a.x = -v.y * cy;
+      a.y = v.x * cy;
+      b.x = -v.y * cz;
+      b.y = v.x * cz;
+      outy[L + i * stride] = a;
+      outz[L + i * stride] = b;
+    }
+  } else {
+    T2* out = C + (1 + grp) * nhalf;
+    for (int e = gt; e < LPB * n; e += FFT_THREADS) {
+      const int le = e % LPB, i = e / LPB;
+      const long L = line0 + le;
+      if (L < nlines) out[L + i * stride] = Yg[le * LS + i];
+    }
   }
   if (with_stats && block_reduce_finish<4>(v, partials, &st->red_counter[RED_SPME], st->scratch, true) && merge) {
     // reciprocal energy into its slot, its diagonal virial added to the virial slots
@@ -636,7 +663,7 @@ k_fft_x_kspace(typename C2<R>::T* C, const typename C2<R>::T* __restrict__ twg, 
 
 template <class R>
 static size_t fftx_smem(int logn, int method) {
-  const int n = 1 << logn, tpl = n >= 8 ? n / 8 : 1, lpb = FFT_THREADS / tpl, ng = method == 0 ? 3 : 1;
+  const int n = 1 << logn, tpl = n >= 8 ? n / 8 : 1, lpb = FFT_THREADS / tpl, ng = method == 0 ? 2 : 1;
   return sizeof(typename C2<R>::T) * (2 * (size_t)n + (1 + (size_t)ng) * lpb * (n + 1)) +
          sizeof(R) * (size_t)lpb * (n + 1) + 8 + sizeof(double) * ((size_t)n + 2 * lpb) + 2 * sizeof(int) * lpb;
 }
@@ -1352,7 +1379,7 @@ static int spme_run(md_spme* s, bool with_stats, Recorder* rec, bool concurrent)
     const void* twg = s->tw[0];
     int ws = with_stats ? 1 : 0, merge = concurrent ? 0 : 1;
     void* a[] = {&C, &twg, &s->bm, &K1, &K2, &beta, &st, &s->partials, &ws, &merge};
-    if (int r = rec_launch(rec, fftx_fn<R>(l0, method), dim3(nb), dim3(FFT_THREADS * (method == 0 ? 3 : 1)),
+    if (int r = rec_launch(rec, fftx_fn<R>(l0, method), dim3(nb), dim3(FFT_THREADS * (method == 0 ? 2 : 1)),
                            fftx_smem<R>(l0, method), a)) return r;
   }
   const int nconv = method == 0 ? 3 : 1;
