@@ -386,12 +386,15 @@ __device__ __forceinline__ void load_tw(typename C2<R>::T* tw, const typename C2
 // three groups of FFT_THREADS threads, and written interleaved, one Real4
 // (x, y, z, 0) per mesh point.
 template <class R, int LOGN, int MODE, int SIGN, int OUT4>
-__global__ void __launch_bounds__(FFT_THREADS * (OUT4 ? 3 : 1))
+__global__ void __launch_bounds__(FFT_THREADS * (OUT4 ? 2 : 1))
 k_fftp(const void* in, void* out, const typename C2<R>::T* __restrict__ twg, long nlines, long stride, long inner,
        long outer, long in_bs, long out_bs) {
   typedef typename C2<R>::T T2;
   typedef FftGeom<LOGN> G;
-  constexpr int n = G::n, LPB = G::LPB, LS = G::LS, NG = OUT4 ? 3 : 1, nh = n / 2 + 1;
+  // OUT4: the three Hermitian spectra become the x, y, z of one real
+  // 4-vector mesh; group 0 inverts A + iB (the x and y spectra: both results
+  // real, they come back as the real and imaginary parts), group 1 the z
+  constexpr int n = G::n, LPB = G::LPB, LS = G::LS, NG = OUT4 ? 2 : 1, nh = n / 2 + 1;
   extern __shared__ __align__(16) unsigned char fft_smem[];
   T2* tw = reinterpret_cast<T2*>(fft_smem);
   T2* X = tw + n;
@@ -405,7 +408,7 @@ k_fftp(const void* in, void* out, const typename C2<R>::T* __restrict__ twg, lon
   __syncthreads();
   const int grp = NG > 1 ? (int)threadIdx.x / FFT_THREADS : 0;
   const int gt = NG > 1 ? (int)threadIdx.x % FFT_THREADS : (int)threadIdx.x;
-  const long batch = OUT4 ? grp : blockIdx.y;
+  const long batch = OUT4 ? 2 * grp : blockIdx.y;
   T2* Xb = X + grp * LPB * LS;
   {
     // all loads of a thread are issued before any shared-memory store (and,
@@ -430,6 +433,19 @@ k_fftp(const void* in, void* out, const typename C2<R>::T* __restrict__ twg, lon
           const T2* src = reinterpret_cast<const T2*>(in) + batch * in_bs + L * nh;
           if (k < nh) v = src[k];
           else { const T2 u = src[n - k]; v.x = u.x; v.y = -u.y; }
+          if (OUT4 && grp == 0) {
+            // + i B, B the spectrum of the next batch.  A real transform
+            // ignores the imaginary parts at k = 0 and n/2 (the mirrored half
+            // carries the rest); they are dropped here, or they would cross
+            // into the other result
+            const T2* srb = src + in_bs;
+            T2 b;
+            if (k < nh) b = srb[k];
+            else { const T2 u = srb[n - k]; b.x = u.x; b.y = -u.y; }
+            if (k == 0 || k == n / 2) { v.y = R(0); b.y = R(0); }
+            v.x -= b.y;
+            v.y += b.x;
+          }
         }
       }
       vv[s] = v;
@@ -457,9 +473,10 @@ k_fftp(const void* in, void* out, const typename C2<R>::T* __restrict__ twg, lon
       const long L = line0 + l2;
       if (L >= nlines) continue;
       R4 o;
-      o.x = X[l2 * LS + k].x;
-      o.y = X[LPB * LS + l2 * LS + k].x;
-      o.z = X[2 * LPB * LS + l2 * LS + k].x;
+      const T2 xy = X[l2 * LS + k];
+      o.x = xy.x;
+      o.y = xy.y;
+      o.z = X[LPB * LS + l2 * LS + k].x;
       o.w = R(0);
       reinterpret_cast<R4*>(out)[L * n + k] = o;
     }
@@ -1252,11 +1269,11 @@ static int fft_launch(md_spme* s, Recorder* rec, const void* in, void* out, int 
     in_bs = out_bs = (long)s->nhalf;
   }
   const int logn = ilog2i(n), lpb = fft_lpb(n);
-  const size_t smem = fftp_smem<R>(logn, out4 ? 3 : 1);
+  const size_t smem = fftp_smem<R>(logn, out4 ? 2 : 1);
   dim3 grid((unsigned)((nlines + lpb - 1) / lpb), out4 ? 1 : batch);
   const void* twg = s->tw[axis];
   void* a[] = {&in, &out, &twg, &nlines, &stride, &inner, &outer, &in_bs, &out_bs};
-  return rec_launch(rec, fftp_fn<R>(logn, mode, sign, out4), grid, dim3(FFT_THREADS * (out4 ? 3 : 1)), smem, a);
+  return rec_launch(rec, fftp_fn<R>(logn, mode, sign, out4), grid, dim3(FFT_THREADS * (out4 ? 2 : 1)), smem, a);
 }
 
 // dynamic shared memory above the default 48 KB needs the opt-in attribute
@@ -1287,7 +1304,7 @@ static int spme_prepare(md_spme* s) {
   if (int r = smem_optin(spread_fn<R>(s->order), SPREAD_TILE_BYTES)) return r;
   if (int r = smem_optin(fftp_fn<R>(l2, 0, -1, 0), fftp_smem<R>(l2, 1))) return r;
   if (int r = smem_optin(fftp_fn<R>(l2, 2, 1, 0), fftp_smem<R>(l2, 1))) return r;
-  if (int r = smem_optin(fftp_fn<R>(l2, 2, 1, 1), fftp_smem<R>(l2, 3))) return r;
+  if (int r = smem_optin(fftp_fn<R>(l2, 2, 1, 1), fftp_smem<R>(l2, 2))) return r;
   for (int sg = -1; sg <= 1; sg += 2) {
     if (int r = smem_optin(fftp_fn<R>(l1, 1, sg, 0), fftp_smem<R>(l1, 1))) return r;
     if (int r = smem_optin(fftp_fn<R>(l0, 1, sg, 0), fftp_smem<R>(l0, 1))) return r;
