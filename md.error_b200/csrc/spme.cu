@@ -400,6 +400,10 @@ k_fftp(const void* in, void* out, const typename C2<R>::T* __restrict__ twg, lon
   T2* X = tw + n;
   long* lo = reinterpret_cast<long*>(X + NG * LPB * LS);
   load_tw<R, SIGN>(tw, twg, n);
+  // MODE 0: the real lines 2L and 2L + 1 go in as the real and imaginary
+  // parts of complex line L, and their half spectra are separated after the
+  // transform: A_k = (Z_k + conj Z_{n-k}) / 2, B_k = (Z_k - conj Z_{n-k}) / 2i
+  const long nlc = MODE == 0 ? (nlines + 1) / 2 : nlines;  // complex lines
   const long line0 = (long)blockIdx.x * LPB;
   if (threadIdx.x < LPB) {
     const long L = line0 + threadIdx.x;
@@ -424,9 +428,11 @@ k_fftp(const void* in, void* out, const typename C2<R>::T* __restrict__ twg, lon
       T2 v;
       v.x = R(0);
       v.y = R(0);
-      if (L < nlines) {
+      if (L < nlc) {
         if (MODE == 0) {
-          v.x = reinterpret_cast<const R*>(in)[batch * in_bs + L * n + k];
+          const R* src = reinterpret_cast<const R*>(in) + batch * in_bs;
+          v.x = src[2 * L * n + k];
+          if (2 * L + 1 < nlines) v.y = src[(2 * L + 1) * n + k];
         } else if (MODE == 1) {
           v = reinterpret_cast<const T2*>(in)[batch * in_bs + lo[l] + k * stride];
         } else {
@@ -459,7 +465,9 @@ k_fftp(const void* in, void* out, const typename C2<R>::T* __restrict__ twg, lon
       if (MODE == 0) {
         // the real mesh is consumed: cleared for the next spread
         const long L = line0 + l;
-        if (L < nlines) reinterpret_cast<R*>(const_cast<void*>(in))[batch * in_bs + L * n + k] = R(0);
+        R* src = reinterpret_cast<R*>(const_cast<void*>(in)) + batch * in_bs;
+        if (L < nlc) src[2 * L * n + k] = R(0);
+        if (2 * L + 1 < nlines) src[(2 * L + 1) * n + k] = R(0);
       }
       Xb[l * LS + k] = vv[s];
     }
@@ -487,10 +495,20 @@ k_fftp(const void* in, void* out, const typename C2<R>::T* __restrict__ twg, lon
     if (MODE == 1) { l2 = e % LPB; k = e / LPB; }
     else { l2 = e >> LOGN; k = e & (n - 1); }
     const long L = line0 + l2;
-    if (L >= nlines) continue;
+    if (L >= nlc) continue;
     const T2 v = X[l2 * LS + k];
     if (MODE == 0) {
-      if (k < nh) reinterpret_cast<T2*>(out)[batch * out_bs + L * nh + k] = v;
+      if (k < nh) {
+        const T2 w = X[l2 * LS + ((n - k) & (n - 1))];
+        T2 a, b;
+        a.x = R(0.5) * (v.x + w.x);
+        a.y = R(0.5) * (v.y - w.y);
+        b.x = R(0.5) * (v.y + w.y);
+        b.y = R(0.5) * (w.x - v.x);
+        T2* dst = reinterpret_cast<T2*>(out) + batch * out_bs;
+        dst[2 * L * nh + k] = a;
+        if (2 * L + 1 < nlines) dst[(2 * L + 1) * nh + k] = b;
+      }
     } else if (MODE == 1) {
       reinterpret_cast<T2*>(out)[batch * out_bs + lo[l2] + k * stride] = v;
     } else {
@@ -1270,7 +1288,8 @@ static int fft_launch(md_spme* s, Recorder* rec, const void* in, void* out, int 
   }
   const int logn = ilog2i(n), lpb = fft_lpb(n);
   const size_t smem = fftp_smem<R>(logn, out4 ? 2 : 1);
-  dim3 grid((unsigned)((nlines + lpb - 1) / lpb), out4 ? 1 : batch);
+  const long nlc = mode == 0 ? (nlines + 1) / 2 : nlines;  // R2C: two real lines per complex transform
+  dim3 grid((unsigned)((nlc + lpb - 1) / lpb), out4 ? 1 : batch);
   const void* twg = s->tw[axis];
   void* a[] = {&in, &out, &twg, &nlines, &stride, &inner, &outer, &in_bs, &out_bs};
   return rec_launch(rec, fftp_fn<R>(logn, mode, sign, out4), grid, dim3(FFT_THREADS * (out4 ? 2 : 1)), smem, a);
