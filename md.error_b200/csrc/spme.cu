@@ -364,6 +364,16 @@ __device__ __forceinline__ void fft_stages(typename C2<R>::T* x, const typename 
   if constexpr (LOGNS + LR < LOGN) fft_stages<R, LOGN, LOGNS + LR, SIGN>(x, tw, tl);
 }
 
+// the block barriers of fft_stages<R, LOGN, LOGNS, *> without the work: a
+// group with nothing to transform meets the others' barriers
+template <int LOGN, int LOGNS>
+__device__ __forceinline__ void fft_stage_barriers() {
+  constexpr int LR = (LOGN - LOGNS) >= 3 ? 3 : (LOGN - LOGNS);
+  __syncthreads();
+  __syncthreads();
+  if constexpr (LOGNS + LR < LOGN) fft_stage_barriers<LOGN, LOGNS + LR>();
+}
+
 template <class R, int SIGN>
 __device__ __forceinline__ void load_tw(typename C2<R>::T* tw, const typename C2<R>::T* __restrict__ twg, int n) {
   for (int m = threadIdx.x; m < n; m += blockDim.x) {
@@ -534,8 +544,8 @@ static size_t fftp_smem(int logn, int nbuf) {
 //   analytic (METHOD 1): psi Q^ / 2 (FBSpline normalisation),
 // each transformed back along x and written to C[1 + d].  Groups of
 // FFT_THREADS threads: group 0 runs the forward transform and the k-space
-// step (group 1 runs the same stages on its own buffer, keeping the barriers
-// uniform), then for ik group 0 inverts phi_x and group 1 inverts psi Q^,
+// step (group 1 meets the same barriers), then for ik group 0 inverts phi_x
+// and group 1 inverts psi Q^,
 // whose transform times -2 pi i m_y and -2 pi i m_z (constant along the
 // line) gives phi_y and phi_z.  The last block merges the energy and the
 // virial into the statistics slots.
@@ -607,7 +617,8 @@ k_fft_x_kspace(typename C2<R>::T* C, const typename C2<R>::T* __restrict__ twg, 
   }
   __syncthreads();
   const int l = gt / G::TPL, tl = gt % G::TPL;
-  fft_stages<R, LOGN, 0, -1>((grp == 0 ? X : Y + grp * LPB * LS) + l * LS, twf, tl);
+  if (grp == 0) fft_stages<R, LOGN, 0, -1>(X + l * LS, twf, tl);
+  else fft_stage_barriers<LOGN, 0>();
   double v[4] = {0, 0, 0, 0};
   if (grp == 0) {
 #pragma unroll
