@@ -265,6 +265,9 @@ extern "C" int md_sim_create(md_sim** out, md_system* sys, md_engine* eng, const
   } else if ((r = langevin_step2_impl(sys, &rec, 0, 1))) {
     return fail(r);
   }
+  // the fused rebuild's grid barrier counter starts clean (build_graph does
+  // it again whenever it records the step)
+  MD_CUDA(cudaMemsetAsync(&sys->st->gbar, 0, sizeof(unsigned long long), sys->stream));
   MD_CUDA(cudaStreamSynchronize(sys->stream));
   if (p->use_graph)
     if ((r = build_graph(s))) return fail(r);
