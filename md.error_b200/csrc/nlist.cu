@@ -522,7 +522,6 @@ struct RebuildArgs {
 // FP64 path (72 KB) leaves room for two
 template <class R> constexpr int rebuild_min_blocks() { return sizeof(R) == 4 ? 4 : 2; }
 
-// the phases, from the cell of every atom to the lists; every block calls
 // the atoms of this block in the per-atom phases: a contiguous share of
 // ceil(N / blocks), so that every block (and every SM) takes part
 __device__ __forceinline__ void block_atoms(int N, int& k0, int& k1) {
@@ -531,6 +530,7 @@ __device__ __forceinline__ void block_atoms(int N, int& k0, int& k1) {
   k1 = min(N, k0 + per);
 }
 
+// the phases, from the cell of every atom to the lists; every block calls
 template <class R, int MODE>
 __device__ __forceinline__ void rebuild_phases(const RebuildArgs<R>& a) {
   DevState* st = a.st;

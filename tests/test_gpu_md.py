@@ -444,10 +444,12 @@ def test_statistics_rows_and_finish(mdf, small_slab, prec):
 
 @pytest.mark.parametrize("prec", [0, 1])
 @pytest.mark.parametrize("use_graph", [True, False])
-def test_fused_rebuild_matches_kernel_chain(mdf, small_slab, prec, use_graph):
+@pytest.mark.parametrize("cellshift", [False, True])
+def test_fused_rebuild_matches_kernel_chain(mdf, small_slab, prec, use_graph, cellshift):
     """The flag-gated cooperative rebuild (one kernel: cell sort, per-slot
     types, lists) and the chain of kernels give the same trajectory bit for
-    bit: adaptive cutoffs, two atom types, Langevin NPT, several rebuilds."""
+    bit: adaptive cutoffs, two atom types, Langevin NPT, several rebuilds,
+    both list criteria."""
     s = small_slab
     types = np.arange(s.n) % 2
     out = []
@@ -460,7 +462,8 @@ def test_fused_rebuild_matches_kernel_chain(mdf, small_slab, prec, use_graph):
         eng.registNonBondedInteractionPair(1, 1, 0.9, 1.05)
         lv = mdf.langevin_params(dt=0.005, temperature=0.85, gamma_t=1.0, seed=9, tau_p=2.0, kappa_t=0.1,
                                  p_ref=(0.0, 0.0, 0.0), npt_dirs=4)
-        sim = mdf.Simulation(sys, eng, skin=0.3, cell_size=2.8, lv=lv, use_graph=use_graph, max_rcut=5.0)
+        sim = mdf.Simulation(sys, eng, skin=0.3, cell_size=2.8, lv=lv, use_graph=use_graph, max_rcut=5.0,
+                             nl_mode=mdf.NL_CELLSHIFT if cellshift else mdf.NL_MINIMAGE)
         sim.set_rebuild_kind(kind)
         want = kind if (use_graph or kind == "fused") else "gated"
         sim.run(150)
