@@ -546,6 +546,14 @@ int md_sim_rebuild_kind(md_sim* sim, int* out);
    the step is a graph (gated launches otherwise).  Both give the same lists
    and trajectories bit for bit. */
 int md_sim_set_rebuild_kind(md_sim* sim, int kind);
+/* A check of the fused rebuild's grid barrier (no counterpart in the
+   reference): one cooperative launch of a block per SM meets one barrier on
+   the system's state; with skip_block >= 0 that block never arrives, so the
+   others give up after limit_s (0 < limit_s <= 10), set the timeout flag and
+   return.  *timed_out reports the flag; the call then clears it and
+   realigns the barrier counter, so the system stays usable.  Blocks the
+   system's stream. */
+int md_check_grid_barrier(md_system* sys, int skip_block, double limit_s, int* timed_out);
 /* MD_INTEG_NHC runs: md_nhc_get_state of the driver's chain (after the pending
    start-of-step half of the next step) */
 int md_sim_get_nhc_state(md_sim* sim, double out[5]);

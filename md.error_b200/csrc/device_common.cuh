@@ -71,11 +71,11 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 // block adds 1 with release semantics, block 0 adds GBAR_EPOCH - (blocks - 1),
 // and each block waits (acquire loads) for the counter to pass the end of
 // the epoch it arrived in.  The counter never needs a reset and stays aligned
-// whatever the grid size.  A wait is bounded: past 4 s the block sets
-// FLAG_TIMEOUT and the call returns false, and the caller leaves the kernel
-// (the other blocks' waits then end the same way).
+// whatever the grid size.  A wait is bounded: past limit_ns (4 s by
+// default) the block sets FLAG_TIMEOUT and the call returns false, and the
+// caller leaves the kernel (the other blocks' waits then end the same way).
 constexpr unsigned long long GBAR_EPOCH = 1ull << 20;  // above any grid size
-__device__ __forceinline__ bool grid_barrier(DevState* st) {
+__device__ __forceinline__ bool grid_barrier(DevState* st, unsigned long long limit_ns = 4000000000ull) {
   __shared__ int gb_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -85,7 +85,7 @@ __device__ __forceinline__ bool grid_barrier(DevState* st) {
     int ok = 1;
     const unsigned long long t0 = global_ns();
     while ((long long)(ld_acquire_u64(&st->gbar) - target) < 0) {
-      if (global_ns() - t0 > 4000000000ull) {
+      if (global_ns() - t0 > limit_ns) {
         atomicOr(&st->flags, FLAG_TIMEOUT);
         ok = 0;
         break;

@@ -733,6 +733,48 @@ int rebuild_fused_impl(md_cell_list* cl, md_nlist* nl, md_system* sys, Recorder*
   return r;
 }
 
+// ------------------------------------------------------ barrier check
+// The fused rebuild's grid barrier on its own, for a test of its bounded
+// wait: every block meets one barrier, except block `skip` (when >= 0),
+// which returns at once, so the others wait out limit_ns, set FLAG_TIMEOUT
+// and return.
+__global__ void k_barrier_check(DevState* st, int skip, unsigned long long limit_ns) {
+  if ((int)blockIdx.x == skip) return;
+  grid_barrier(st, limit_ns);
+}
+
+// afterwards: the counter realigned and the timeout flag cleared
+__global__ void k_barrier_check_reset(DevState* st) {
+  st->gbar = 0ull;
+  st->flags &= ~FLAG_TIMEOUT;
+}
+
+extern "C" int md_check_grid_barrier(md_system* sys, int skip_block, double limit_s, int* timed_out) {
+  if (!sys || !timed_out || !(limit_s > 0.0) || limit_s > 10.0) {
+    md_set_error("md_check_grid_barrier: bad arguments (0 < limit_s <= 10)");
+    return MD_ERR_BADARG;
+  }
+  int dev = 0, coop = 0, nsm = 0;
+  MD_CUDA(cudaGetDevice(&dev));
+  MD_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  MD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  if (!coop) { md_set_error("md_check_grid_barrier: no cooperative launch on this device"); return MD_ERR_UNSUPPORTED; }
+  if (skip_block >= nsm) { md_set_error("md_check_grid_barrier: skip_block beyond the grid (%d blocks)", nsm); return MD_ERR_BADARG; }
+  DevState* st = sys->st;
+  unsigned long long limit_ns = (unsigned long long)(limit_s * 1e9);
+  // one block per SM, from a clean counter
+  MD_CUDA(cudaMemsetAsync(&st->gbar, 0, sizeof(unsigned long long), sys->stream));
+  void* a[] = {&st, &skip_block, &limit_ns};
+  MD_CUDA(cudaLaunchCooperativeKernel((const void*)k_barrier_check, dim3(nsm), dim3(256), a, 0, sys->stream));
+  DevState hs;
+  if (int r = sys->read_state(hs)) return r;
+  *timed_out = (hs.flags & FLAG_TIMEOUT) ? 1 : 0;
+  k_barrier_check_reset<<<1, 1, 0, sys->stream>>>(st);
+  MD_CHECK_LAUNCH("k_barrier_check_reset");
+  MD_CUDA(cudaStreamSynchronize(sys->stream));
+  return MD_OK;
+}
+
 // ------------------------------------------------------------------ C ABI
 static int alloc_lists(md_nlist* nl, md_system* sys) {
   if (nl->list) cudaFree(nl->list);

@@ -113,6 +113,7 @@ _SIGS = {
     "md_sim_uses_conditional_graph": (i32, [vp, P(i32)]),
     "md_sim_rebuild_kind": (i32, [vp, P(i32)]),
     "md_sim_set_rebuild_kind": (i32, [vp, i32]),
+    "md_check_grid_barrier": (i32, [vp, i32, f64, P(i32)]),
     "md_engine_register_coulomb": (i32, [vp, f64]),
     "md_spme_create": (i32, [P(vp), vp, P(i32), i32, f64, i32]),
     "md_spme_destroy": (i32, [vp]),

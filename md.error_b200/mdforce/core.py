@@ -734,6 +734,16 @@ def write_system_gro(path, sys, conf, step=0, time=0.0):
     write_gro(path, out, "# at time = %f, step = %d" % (time, step))
 
 
+def check_grid_barrier(sys, skip_block=-1, limit_s=1.0):
+    """Runs the fused rebuild's grid barrier once (a block per SM) on the
+    system's state; with skip_block >= 0 that block never arrives and the
+    others give up after limit_s.  Returns True when the barrier timed out;
+    the timeout flag is cleared again and the system stays usable."""
+    t = C.c_int()
+    check(lib.md_check_grid_barrier(sys.h, int(skip_block), float(limit_s), C.byref(t)), "check_grid_barrier")
+    return bool(t.value)
+
+
 def choose_beta(sys, rcut, target):
     b = C.c_double()
     check(lib.md_choose_beta(sys.h, float(rcut), float(target), C.byref(b)), "choose_beta")
