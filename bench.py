@@ -795,6 +795,7 @@ def main():
     with Clocks(local) as clk:
         t_mixed = time_steps(torch, sim_m, stream, args.steps, flush, nvtx_range="timed")
     steps_done, rebuilds, flags = sim_m.counters()
+    rebuild_kind = sim_m.rebuild_kind()
     rebuilds_timed = rebuilds - rebuilds0
     value, t_max = replica_rate(torch, args.steps, t_mixed, world, "cuda")
 
@@ -898,14 +899,19 @@ def main():
         raise RuntimeError("per-step statistics of the end-to-end run are missing or non-finite")
     del sim_e, arc_e, eng_e, sys_e
 
-    # step1, LJ, step2 every step; bin, scan, scatter, order, gather, copy back,
-    # z order, list build per rebuild; the density deposit every 40 steps and
-    # 3 + 3*3 DFT passes + 7 element-wise kernels per cutoff update (every 2000
-    # steps)
+    # the first half (with the rebuild folded in, when fused), LJ and the
+    # closing kick every step; with the kernel chain instead, bin, scan,
+    # scatter, order, gather, copy back, z order and list build per rebuild
+    # (every step in direct launch, gated); the density deposit every 40 steps
+    # and 3 + 3*3 DFT passes + 7 element-wise kernels per cutoff update (every
+    # 2000 steps)
     first, last = steps0, steps0 + args.steps
     n_updates = last // UPDATE_EVERY - first // UPDATE_EVERY
     n_deposits = last // SAMPLE_EVERY - first // SAMPLE_EVERY
-    rebuild_launches = 8 * (rebuilds_timed if use_graph else args.steps)
+    if rebuild_kind == "fused":
+        rebuild_launches = 0
+    else:
+        rebuild_launches = 8 * (rebuilds_timed if rebuild_kind == "conditional" else args.steps)
     launches = 3 * args.steps + rebuild_launches + n_deposits + 22 * n_updates
     cpu = loop = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -935,7 +941,7 @@ def main():
                 "what": f"RMS over atoms of |F - F_ref| (eps/sigma) on the start, F_ref = FP64 forces at a "
                         f"uniform cutoff {RC_LONG} plus the long-range force correction; the estimate is the "
                         f"AdaptRCut error of each atom's bin at its assigned cutoff"},
-            "list_rebuilds": rebuilds, "tau_per_day": value / world * DT * 86400,
+            "list_rebuilds": rebuilds, "rebuild_kind": rebuild_kind, "tau_per_day": value / world * DT * 86400,
             "schedule": {"period_steps": period, "period_device_s": period_dev, "period_wall_s": t_period,
                          "period_steps_per_s": period / t_period,
                          "arc_update_ms": 1e3 * arc_update_s, "deposit_ms": 1e3 * deposit_s,
