@@ -26,11 +26,12 @@ __global__ void k_lv_box(DevState* st, LvDev p) { box_advance(st, p, true); }
 // (lv_particle_step1, langevin.cuh).  With use_cond the last block to finish
 // writes the rebuild decision into the CUDA graph conditional that guards the
 // cell sort + list build.
-// threads per block of the driver's Langevin halves (a multiple of 32, <= 256);
-// 128 measured 0.2-0.3 % more steps/s than 256 on the 65,536-atom slab (twice
-// as many blocks for these latency-bound passes)
+// threads per block of the Langevin halves the driver launches as separate
+// kernels (a multiple of 32, <= 256): with the closing kick's reduction on
+// one acquire-release atomic per block, 256 measured 0.7 % more steps/s than
+// 128 on the 65,536-atom slab (half the blocks, partials and atomics)
 #ifndef MD_LV_THREADS
-#define MD_LV_THREADS 128
+#define MD_LV_THREADS 256
 #endif
 
 template <class R>
